@@ -1,0 +1,242 @@
+"""Pin the CPU oracle to the reference's own known-answer tests.
+
+Each test restates a check from CombinatorialSpaces.jl's test suite (file:line cited) and runs it
+against the oracle.  Indices are 0-based here (the reference is 1-based).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import csc
+
+SQ5 = math.sqrt(5.0)
+
+
+def gillette(O, center):
+    # test/DiscreteExteriorCalculus.jl:288-296: unit right triangle, true orientations.
+    m = O.Mesh()
+    m.add_vertex(0, 0, 0)
+    m.add_vertex(1, 0, 0)
+    m.add_vertex(0, 1, 0)
+    m.glue_triangle(0, 1, 2, 1)
+    m.set_edge_orientation(1)
+    return O.dualize(m, center)
+
+
+def test_dual_layout_square(O):
+    # test/DiscreteExteriorCalculus.jl:183-201
+    m = O.Mesh()
+    for _ in range(4):
+        m.add_vertex(0, 0, 0)
+    m.glue_triangle(0, 1, 2)
+    m.glue_triangle(0, 2, 3)
+    # coordinates are irrelevant for the layout; give them distinct positions
+    m = O.mesh_from_arrays(np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0]], float),
+                           m.ev0, m.ev1, m.te0, m.te1, m.te2,
+                           np.full(m.ne, -1, np.int8), np.full(m.nt, -1, np.int8))
+    d = O.dualize(m, O.BARYCENTER)
+    nv, ne, nt = m.nv, m.ne, m.nt
+    assert len(d.D_dv0) == 2 * ne + 6 * nt
+    assert len(d.D_de0) == 6 * nt
+    assert d.dual_point.shape[0] == nv + ne + nt
+    # primal_vertex(subsimplices(Tri(1))) == [1,1,2,2,3,3]
+    prim = [d.D_dv1[d.D_de2[i * nt + 0]] for i in range(6)]
+    assert prim == [0, 0, 1, 1, 2, 2]
+    # elementary_duals(1, s, 2) has one dual edge, (1, s, 3) has two, both ending at the edge center
+    for e, count in ((1, 1), (2, 2)):
+        des = np.nonzero(d.D_dv1 == nv + e)[0]
+        assert len(des) == count
+    # [length(elementary_duals(s, V(i))) for i in 1:4] == [4,2,4,2]
+    counts = [int(np.sum(d.D_dv1[d.D_de1] == v)) for v in range(4)]
+    assert counts == [4, 2, 4, 2]
+    assert d.dual_triangle_vertices(0) == (0, 6, 9)           # [1,7,10]
+    assert (int(d.D_dv0[0]), int(d.D_dv1[0])) == (4, 1)       # [5,2]
+
+
+def test_gillette_barycentric(O):
+    d = gillette(O, O.BARYCENTER)
+    # :298-302
+    np.testing.assert_allclose(d.dual_point[d.nv + d.ne + 0][:2], [1 / 3, 1 / 3], rtol=1e-14)
+    np.testing.assert_allclose(d.area, [0.5], rtol=1e-14)
+    np.testing.assert_allclose(O.hodge_diag(d, 0), [1 / 6] * 3, rtol=1e-14)
+    # :305
+    np.testing.assert_allclose(O.hodge_diag(d, 1), [SQ5 / 6, 1 / 6, SQ5 / 6], rtol=1e-14)
+    # :306-308  δ1 = ⋆0⁻¹ · dual_d(1) · ⋆1
+    delta1 = (np.diag(O.inv_hodge_diag(d, 0)) @ csc(O.dec_dual_derivative(d, 1)).toarray()
+              @ np.diag(O.hodge_diag(d, 1)))
+    np.testing.assert_allclose(delta1, [[2.236, 0, 2.236], [-2.236, 1, 0], [0, -1, -2.236]], atol=1e-3)
+    # :331-333 inverse Hodge stars
+    np.testing.assert_allclose(O.inv_hodge_diag(d, 2), [0.5], rtol=1e-14)
+    np.testing.assert_allclose(O.inv_hodge_diag(d, 1), [-6 / SQ5, -6, -6 / SQ5], rtol=1e-14)
+
+
+def test_gillette_circumcentric(O):
+    d = gillette(O, O.CIRCUMCENTER)
+    # test/DiscreteExteriorCalculus.jl:362-368
+    np.testing.assert_allclose(d.dual_point[d.nv + d.ne + 0][:2], [0.5, 0.5], rtol=1e-14)
+    np.testing.assert_allclose(O.hodge_diag(d, 0), [1 / 4, 1 / 8, 1 / 8], rtol=1e-14)
+    np.testing.assert_allclose(O.hodge_diag(d, 1), [0.5, 0.0, 0.5], atol=1e-15)
+    delta1 = (np.diag(O.inv_hodge_diag(d, 0)) @ csc(O.dec_dual_derivative(d, 1)).toarray()
+              @ np.diag(O.hodge_diag(d, 1)))
+    np.testing.assert_allclose(delta1, [[2, 0, 2], [-4, 0, 0], [0, 0, -4]], atol=1e-12)
+    # Δ(0) = δ1 d0 = -fast_laplace_beltrami
+    L = csc(O.laplace_beltrami0(d)).toarray()
+    np.testing.assert_allclose(-L, delta1 @ csc(O.dec_differential(d, 0)).toarray(), atol=1e-12)
+
+
+def test_gillette_exterior_derivative(O):
+    d = gillette(O, O.BARYCENTER)
+    d0 = csc(O.dec_differential(d, 0)).toarray()
+    d1 = csc(O.dec_differential(d, 1)).toarray()
+    np.testing.assert_array_equal(d0, [[-1, 1, 0], [0, -1, 1], [-1, 0, 1]])
+    np.testing.assert_array_equal(d1, [[1, 1, -1]])
+    np.testing.assert_array_equal(d1 @ d0, np.zeros((1, 3)))
+    np.testing.assert_array_equal(csc(O.dec_boundary(d, 1)).toarray(), d0.T)
+    np.testing.assert_array_equal(csc(O.dec_boundary(d, 2)).toarray(), d1.T)
+    np.testing.assert_array_equal(csc(O.dec_dual_derivative(d, 0)).toarray(), d1.T)
+    np.testing.assert_array_equal(csc(O.dec_dual_derivative(d, 1)).toarray(), -d0.T)
+
+
+def const_form(mesh, X):
+    # eval_constant_primal_form, DiscreteExteriorCalculus.jl:2172-2177
+    p = mesh.points
+    sg = np.where(mesh.edge_orientation == 1, 1.0, -1.0)
+    return ((p[mesh.ev0] - p[mesh.ev1]) @ np.asarray(X, float)) * sg
+
+
+def test_wedge_02_unit_area(O):
+    # test/DiscreteExteriorCalculus.jl:535-547: ∧(3, 5 dx∧dy) = 15 on a unit-area 3-4-5 triangle.
+    m = O.Mesh()
+    m.add_vertex(0, 0, 0)
+    m.add_vertex(6 / 8, 0, 0)
+    m.add_vertex(6 / 8, 8 / 3, 0)
+    m.glue_triangle(0, 1, 2, 1)
+    m.set_edge_orientation(1)
+    d = O.dualize(m, O.BARYCENTER)
+    out = O.wedge(d, 2, np.array([3.0, 3, 3]), np.array([d.area[0] * 5]))
+    np.testing.assert_allclose(out, [15.0], rtol=1e-14)
+
+
+def test_wedge_identities_grid_345(O):
+    # test/DiscreteExteriorCalculus.jl:549-570
+    d = O.dualize(O.grid_345(), O.BARYCENTER)
+    m = d.mesh
+    one = np.ones(d.nv)
+    np.testing.assert_allclose(O.wedge(d, 1, one, np.arange(1.0, d.ne + 1)), np.arange(1.0, d.ne + 1), rtol=1e-14)
+    np.testing.assert_allclose(O.wedge(d, 2, one, np.arange(1.0, d.nt + 1)), np.arange(1.0, d.nt + 1), rtol=1e-14)
+    dx = const_form(m, [1, 0, 0])
+    dy = const_form(m, [0, 1, 0])
+    np.testing.assert_allclose(O.wedge(d, 11, dx, dy), d.area, rtol=1e-14)
+    np.testing.assert_array_equal(O.wedge(d, 11, dx, dy), -O.wedge(d, 11, dy, dx))
+    np.testing.assert_array_equal(O.wedge(d, 11, 3 * dx, 2 * dy), O.wedge(d, 11, 2 * dx, 3 * dy))
+
+
+def test_wedge_orientation_flip_invariance(O):
+    # test/DiscreteExteriorCalculus.jl:560-565: flipping one edge's orientation (and the sign of
+    # the forms on it) leaves dx∧dy unchanged.
+    base = O.grid_345()
+    for i in range(base.ne):
+        eo = base.edge_orientation.copy()
+        eo[i] = 1 - eo[i]
+        m = O.mesh_from_arrays(base.points, base.ev0, base.ev1, base.te0, base.te1, base.te2,
+                               eo, base.tri_orientation)
+        d = O.dualize(m, O.BARYCENTER)
+        dx, dy = const_form(m, [1, 0, 0]), const_form(m, [0, 1, 0])
+        np.testing.assert_allclose(O.wedge(d, 11, dx, dy), d.area, rtol=1e-13)
+
+
+def test_wedge_cw_triangle(O):
+    # test/DiscreteExteriorCalculus.jl:567-570: tri_345_false gives -area.
+    d = O.dualize(O.tri_345(False), O.BARYCENTER)
+    dx, dy = const_form(d.mesh, [1, 0, 0]), const_form(d.mesh, [0, 1, 0])
+    np.testing.assert_allclose(O.wedge(d, 11, dx, dy), -d.area, rtol=1e-14)
+
+
+def test_subdivision_structure(O):
+    # test/Multigrid.jl:14-19
+    s = O.triangulated_grid(1, 1, 1, 1, False)
+    S = csc(O.subdivision_matrix(s)).toarray()
+    nv = s.nv
+    np.testing.assert_array_equal(S[:nv, :nv], np.eye(nv))
+    for e in range(s.ne):
+        col = S[:, nv + e]
+        rows = np.nonzero(col)[0]
+        assert list(rows) == [s.ev1[e], s.ev0[e]]
+        np.testing.assert_array_equal(col[rows], [0.5, 0.5])
+
+
+def test_subdivision_counts_and_orientation(O):
+    # test/Multigrid.jl:21-41 (binary): counts per round and orient! succeeds.
+    s = O.triangulated_grid(1, 1, 1, 1, False)
+    for _ in range(4):
+        t = O.refine_binary(s, 0.0)
+        assert (t.nv, t.ne, t.nt) == (s.nv + s.ne, 2 * s.ne + 3 * s.nt, 4 * s.nt)
+        assert O.orient(t)
+        s = t
+
+
+def test_icosphere_counts(O):
+    # Icosphere L_k = k binary subdivisions of the icosahedron: nv = 10·4^k + 2, nt = 20·4^k.
+    s = O.icosahedron()
+    assert (s.nv, s.ne, s.nt) == (12, 30, 20)
+    for k in range(1, 5):
+        s = O.refine_binary(s, 1.0)
+        assert (s.nv, s.ne, s.nt) == (10 * 4 ** k + 2, 30 * 4 ** k, 20 * 4 ** k)
+        np.testing.assert_allclose(np.linalg.norm(s.points, axis=1), 1.0, rtol=1e-15)
+        assert O.orient(s)
+
+
+def test_triangulated_grid_config(O):
+    # CombMeshes.jl:79-133 with (127, 127, 1.0, 1.0, Point3d, false): 128 x 128 vertices.
+    s = O.triangulated_grid(127, 127, 1.0, 1.0, False)
+    assert (s.nv, s.ne, s.nt) == (16384, 48641, 32258)
+    p = s.points
+    assert p[0].tolist() == [0, 0, 0]
+    assert p[128].tolist() == [0.5, 1.0, 0.0]     # even (1-based) rows are shifted by dx/2
+    assert s.edge_orientation.max() == 0
+    o = s.tri_orientation
+    assert o[0] == 1 and o[1] == 0 and o[254] == 0 and o[255] == 1
+
+
+def _mg_residual_setup(O, steps):
+    # test/Multigrid.jl:54-90 and :94-111: 4 binary levels over triangulated_grid(1,1,1/4,√3/8).
+    s = O.triangulated_grid(1, 1, 1 / 4, math.sqrt(3) / 2 * 1 / 4, False)
+    md = O.build_mg(s, 4, O.CIRCUMCENTER, 0.0, 0.0, steps)
+    L = csc(md.op(0))
+    rng = np.random.default_rng(0)
+    b = L @ rng.random(L.shape[0])
+    return md, L, b
+
+
+def test_multigrid_residuals(O):
+    md, L, b = _mg_residual_setup(O, 3)
+    u0 = np.zeros_like(b)
+    rel = lambda u: np.linalg.norm(L @ u - b) / np.linalg.norm(b)
+    assert rel(O.mu_cycles(md, u0, b, 5, 1)) < 1e-7   # V
+    assert rel(O.mu_cycles(md, u0, b, 5, 2)) < 1e-7   # W
+    assert rel(O.full_multigrid(md, b, 5, 1)) < 1e-6  # FMG-V
+    assert rel(O.full_multigrid(md, b, 5, 2)) < 1e-7  # FMG-W
+
+
+def test_multigrid_zero_steps(O):
+    # test/Multigrid.jl:151-170 (issue #178): steps = 0 runs no smoothing at all.
+    md0, L, b = _mg_residual_setup(O, 0)
+    md1, _, _ = _mg_residual_setup(O, 1)
+    u0 = np.zeros_like(b)
+    r0 = np.linalg.norm(L @ O.mu_cycles(md0, u0, b, 5, 1) - b)
+    r1 = np.linalg.norm(L @ O.mu_cycles(md1, u0, b, 5, 1) - b)
+    assert r1 < r0
+
+
+def test_multigrid_hierarchy_shapes(O):
+    md, L, _ = _mg_residual_setup(O, 3)
+    assert md.nlevels == 5
+    for k in range(4):
+        A = csc(md.op(k))
+        Ac = csc(md.op(k + 1))
+        R = csc(md.restriction(k))
+        P = csc(md.prolongation(k))
+        assert R.shape == (Ac.shape[0], A.shape[0])
+        assert P.shape == (A.shape[0], Ac.shape[0])
+        np.testing.assert_allclose(np.asarray(R.sum(axis=1)).ravel(), 1.0, rtol=1e-15)
