@@ -1,0 +1,414 @@
+"""dec_b200: the CombinatorialSpaces.jl DEC hot path on B200 (sm_100a).
+
+A Python mirror of the reference's backend entry points for this path, each calling the C ABI
+of ``libdec_b200.so`` (include/dec_b200.h):
+
+    dec_wedge_product(m, n, sd, dtype)          FastDEC.jl:255-289 (closure (a, b) -> a ∧ b)
+    dec_wedge_product_pd / _dp / _dd            FastDEC.jl:291-401
+    dec_differential / dec_boundary /
+      dec_dual_derivative(n, sd, dtype)         ext/CombinatorialSpacesCUDAExt.jl:30-61
+    dec_hodge_star / dec_inv_hodge_star         ext/CombinatorialSpacesCUDAExt.jl:70-96
+    laplace_beltrami(sd) / helmholtz(sd, c)     test/Multigrid.jl:46-48
+    MultigridData(s, levels, ...)               Multigrid.jl:698-797
+    multigrid_vcycles / multigrid_wcycles       Multigrid.jl:814-824
+
+Forms are torch CUDA tensors in the reference's element order; work runs on torch's current
+stream.  There is no CPU fallback: every call goes to the CUDA library and raises if it is
+missing or fails.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from ._capi import check, lib, DecError  # noqa: F401
+
+__all__ = ["Mesh", "Operator", "MultigridData", "dec_wedge_product", "dec_wedge_product_pd",
+           "dec_wedge_product_dp", "dec_wedge_product_dd", "dec_differential", "dec_boundary",
+           "dec_dual_derivative", "dec_hodge_star", "dec_inv_hodge_star", "laplace_beltrami",
+           "helmholtz", "multigrid_vcycles", "multigrid_wcycles", "DecError"]
+
+CENTERS = {"barycenter": _capi.DEC_BARYCENTER, "circumcenter": _capi.DEC_CIRCUMCENTER}
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _dtype_code(dtype):
+    torch = _torch()
+    if dtype in (torch.float64, np.float64, "f64", "float64"):
+        return _capi.DEC_F64
+    if dtype in (torch.float32, np.float32, "f32", "float32"):
+        return _capi.DEC_F32
+    raise ValueError(f"unsupported dtype {dtype}")
+
+
+def _torch_dtype(code):
+    torch = _torch()
+    return torch.float64 if code == _capi.DEC_F64 else torch.float32
+
+
+def _stream():
+    torch = _torch()
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _check_form(t, n, code, what):
+    torch = _torch()
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{what}: expected a CUDA tensor")
+    if t.dtype != _torch_dtype(code):
+        raise TypeError(f"{what}: expected {_torch_dtype(code)}, got {t.dtype}")
+    if t.numel() != n or not t.is_contiguous():
+        raise ValueError(f"{what}: expected a contiguous form of length {n}, got shape {tuple(t.shape)}")
+
+
+class Mesh:
+    """An embedded 2D delta set with its dual complex, resident on the GPU.
+
+    Arguments are host arrays: ``points`` (nv, 3), edge faces ``ev0`` (∂v0, target) and
+    ``ev1`` (∂v1, source), triangle faces ``te0, te1, te2`` (∂e0, ∂e1, ∂e2), the orientations
+    (None = unset, as after ``topo_to_mesh``) and the dual-subdivision ``center``.
+    """
+
+    def __init__(self, points, ev0, ev1, te0, te1, te2, edge_orientation=None, tri_orientation=None,
+                 center="barycenter", index_base=0):
+        self._keep = []
+
+        def arr(a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            self._keep.append(a)
+            return a.ctypes.data_as(C.c_void_p)
+
+        pts = np.ascontiguousarray(points, dtype=np.float64)
+        if pts.ndim == 2 and pts.shape[1] == 2:
+            pts = np.concatenate([pts, np.zeros((pts.shape[0], 1))], axis=1)
+        d = _capi.MeshDesc()
+        d.nv, d.ne, d.nt = pts.shape[0], len(ev0), len(te0)
+        d.index_base = index_base
+        d.points = arr(pts, np.float64)
+        d.e_v0, d.e_v1 = arr(ev0, np.int32), arr(ev1, np.int32)
+        d.t_e0, d.t_e1, d.t_e2 = arr(te0, np.int32), arr(te1, np.int32), arr(te2, np.int32)
+        d.edge_orientation = None if edge_orientation is None else arr(edge_orientation, np.int8)
+        d.tri_orientation = None if tri_orientation is None else arr(tri_orientation, np.int8)
+        d.center = CENTERS[center] if isinstance(center, str) else int(center)
+        self.desc = d
+        h = C.c_void_p()
+        check(lib().dec_mesh_create(C.byref(d), C.byref(h)))
+        self._h = h
+        self._owned = True
+        self.nv, self.ne, self.nt = int(d.nv), int(d.ne), int(d.nt)
+        self._keep = []  # host arrays were copied by the library
+        self.desc = None
+
+    @classmethod
+    def _borrow(cls, handle):
+        self = cls.__new__(cls)
+        self._h = handle
+        self._owned = False
+        nv, ne, nt = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib().dec_mesh_counts(handle, C.byref(nv), C.byref(ne), C.byref(nt)))
+        self.nv, self.ne, self.nt = nv.value, ne.value, nt.value
+        return self
+
+    @classmethod
+    def from_oracle(cls, m, center="barycenter"):
+        """Build from an object with the oracle Mesh attributes (0-based arrays)."""
+        return cls(m.points, m.ev0, m.ev1, m.te0, m.te1, m.te2, m.edge_orientation,
+                   m.tri_orientation, center=center, index_base=0)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and getattr(self, "_owned", False) and _capi._lib is not None:
+            _capi._lib.dec_mesh_destroy(h)
+            self._h = None
+
+    def orientation(self):
+        eo = np.empty(self.ne, np.int8)
+        to = np.empty(self.nt, np.int8)
+        check(lib().dec_mesh_orientation(self._h, eo.ctypes.data_as(C.c_void_p), to.ctypes.data_as(C.c_void_p)))
+        return eo, to
+
+    def geometry(self, which):
+        n = {"length": self.ne, "area": self.nt, "dual_area": 6 * self.nt, "dual_length_te": 3 * self.nt,
+             "dual_point": 3 * (self.nv + self.ne + self.nt)}[which]
+        code = {"length": 0, "area": 1, "dual_area": 2, "dual_length_te": 3, "dual_point": 4}[which]
+        out = np.empty(n, np.float64)
+        check(lib().dec_mesh_geometry(self._h, code, out.ctypes.data_as(C.c_void_p), n))
+        return out.reshape(-1, 3) if which == "dual_point" else out
+
+
+# ---- wedge products -------------------------------------------------------------------------
+
+class WedgePlan:
+    """Cached wedge coefficients on the device; calling it evaluates a ∧ b (allocating the output,
+    as dec_c_wedge_product does, or into ``out``)."""
+
+    def __init__(self, sd, kind, m, n, dtype):
+        self.sd = sd
+        self.code = _dtype_code(dtype)
+        h = C.c_void_p()
+        check(lib().dec_wedge_plan_create(sd._h, kind, m, n, self.code, C.byref(h)))
+        self._h = h
+        la, lb, lo = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib().dec_wedge_lengths(h, C.byref(la), C.byref(lb), C.byref(lo)))
+        self.len_a, self.len_b, self.len_out = la.value, lb.value, lo.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _capi._lib is not None:
+            _capi._lib.dec_wedge_plan_destroy(h)
+            self._h = None
+
+    def __call__(self, a, b, out=None):
+        torch = _torch()
+        _check_form(a, self.len_a, self.code, "wedge first form")
+        _check_form(b, self.len_b, self.code, "wedge second form")
+        if out is None:
+            out = torch.empty(self.len_out, dtype=_torch_dtype(self.code), device=a.device)
+        _check_form(out, self.len_out, self.code, "wedge output")
+        check(lib().dec_wedge_apply(self._h, _ptr(a), _ptr(b), _ptr(out), _stream()))
+        return out
+
+    def batched(self, a, b, out):
+        count = a.shape[0]
+        check(lib().dec_wedge_apply_batched(self._h, _ptr(a), _ptr(b), _ptr(out), count, _stream()))
+        return out
+
+
+def dec_wedge_product(m, n, sd, dtype="float64"):
+    """Primal-primal wedge of an m-form and an n-form (FastDEC.jl:255-289)."""
+    return WedgePlan(sd, _capi.DEC_WEDGE_PP, m, n, dtype)
+
+
+def dec_wedge_product_pd(m, n, sd, dtype="float64"):
+    """Primal m-form ∧ dual n-form (FastDEC.jl:386-395)."""
+    return WedgePlan(sd, _capi.DEC_WEDGE_PD, m, n, dtype)
+
+
+def dec_wedge_product_dp(m, n, sd, dtype="float64"):
+    """Dual m-form ∧ primal n-form (FastDEC.jl:381-384, :397-401)."""
+    return WedgePlan(sd, _capi.DEC_WEDGE_DP, m, n, dtype)
+
+
+def dec_wedge_product_dd(m, n, sd, dtype="float64"):
+    """Dual m-form ∧ dual n-form (FastDEC.jl:317-325)."""
+    return WedgePlan(sd, _capi.DEC_WEDGE_DD, m, n, dtype)
+
+
+# ---- operators ------------------------------------------------------------------------------
+
+class Operator:
+    """A sparse DEC operator on the device: ``op(x)`` / ``op @ x`` returns Op x."""
+
+    def __init__(self, sd, kind, dtype="float64", shift=0.0, handle=None):
+        self.sd = sd
+        if handle is not None:
+            self._h, self._owned = handle, False
+            self.code = _capi.DEC_F64
+        else:
+            self.code = _dtype_code(dtype)
+            h = C.c_void_p()
+            check(lib().dec_op_create(sd._h, kind, float(shift), self.code, C.byref(h)))
+            self._h, self._owned = h, True
+        r, c = C.c_int64(), C.c_int64()
+        check(lib().dec_op_shape(self._h, C.byref(r), C.byref(c)))
+        self.shape = (r.value, c.value)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and getattr(self, "_owned", False) and _capi._lib is not None:
+            _capi._lib.dec_op_destroy(h)
+            self._h = None
+
+    def apply(self, x, y=None, alpha=1.0, beta=0.0):
+        torch = _torch()
+        _check_form(x, self.shape[1], self.code, "operator input")
+        if y is None:
+            y = torch.empty(self.shape[0], dtype=_torch_dtype(self.code), device=x.device)
+        _check_form(y, self.shape[0], self.code, "operator output")
+        check(lib().dec_op_apply(self._h, _ptr(x), _ptr(y), float(alpha), float(beta), _stream()))
+        return y
+
+    __call__ = apply
+
+    def __matmul__(self, x):
+        return self.apply(x)
+
+    def csr(self):
+        """(indptr, indices, data, shape) of the operator, exported to the host."""
+        nnz = C.c_int64()
+        check(lib().dec_op_export_csr(self._h, C.byref(nnz), None, None, None))
+        rp = np.empty(self.shape[0] + 1, np.int32)
+        ci = np.empty(nnz.value, np.int32)
+        v = np.empty(nnz.value, np.float64)
+        check(lib().dec_op_export_csr(self._h, C.byref(nnz), rp.ctypes.data_as(C.c_void_p),
+                                      ci.ctypes.data_as(C.c_void_p), v.ctypes.data_as(C.c_void_p)))
+        return rp, ci, v, self.shape
+
+
+def dec_differential(n, sd, dtype="float64"):
+    return Operator(sd, {0: _capi.DEC_OP_D0, 1: _capi.DEC_OP_D1}[n], dtype)
+
+
+def dec_boundary(n, sd, dtype="float64"):
+    return Operator(sd, {1: _capi.DEC_OP_BOUNDARY1, 2: _capi.DEC_OP_BOUNDARY2}[n], dtype)
+
+
+def dec_dual_derivative(n, sd, dtype="float64"):
+    return Operator(sd, {0: _capi.DEC_OP_DUAL_D0, 1: _capi.DEC_OP_DUAL_D1}[n], dtype)
+
+
+def dec_hodge_star(n, sd, dtype="float64"):
+    """Diagonal Hodge star ⋆n as a device vector (the CuArray of the reference's CUDA backend)."""
+    return _hodge(n, sd, 0, dtype)
+
+
+def dec_inv_hodge_star(n, sd, dtype="float64"):
+    return _hodge(n, sd, 1, dtype)
+
+
+def _hodge(n, sd, inverse, dtype):
+    torch = _torch()
+    code = _dtype_code(dtype)
+    size = {0: sd.nv, 1: sd.ne, 2: sd.nt}[n]
+    out = torch.empty(size, dtype=_torch_dtype(code), device="cuda")
+    check(lib().dec_hodge_diag(sd._h, n, inverse, code, _ptr(out), _stream()))
+    return out
+
+
+def hodge_operator(n, sd, inverse=False, dtype="float64"):
+    kind = (_capi.DEC_OP_INV_STAR0 if inverse else _capi.DEC_OP_STAR0) + n
+    return Operator(sd, kind, dtype)
+
+
+def laplace_beltrami(sd, dtype="float64"):
+    """fast_laplace_beltrami(sd) = -⋆0⁻¹ dual_d(1) ⋆1 d(0) = ⋆0⁻¹ d0ᵀ ⋆1 d0 (test/Multigrid.jl:46-48)."""
+    return Operator(sd, _capi.DEC_OP_LAPLACE0, dtype)
+
+
+def helmholtz(sd, shift, dtype="float64"):
+    """laplace_beltrami(sd) + shift * I."""
+    return Operator(sd, _capi.DEC_OP_HELMHOLTZ0, dtype, shift=shift)
+
+
+# ---- multigrid ------------------------------------------------------------------------------
+
+def default_mg_options():
+    o = _capi.MGOptions()
+    lib().dec_mg_default_options(C.byref(o))
+    return o
+
+
+class MultigridData:
+    """MultigridData(s, BinarySubdivision(), levels, op = L + shift I, steps) on the device.
+
+    ``coarse`` is a host mesh description (anything with the oracle Mesh attributes or a
+    ``Mesh``-compatible tuple); options follow ``dec_mg_options``.
+    """
+
+    def __init__(self, coarse, levels, shift=0.0, center="circumcenter", project_radius=0.0, **opts):
+        o = default_mg_options()
+        o.levels = levels
+        o.center = CENTERS[center] if isinstance(center, str) else int(center)
+        o.project_radius = project_radius
+        o.shift = shift
+        for k, v in opts.items():
+            if not hasattr(o, k):
+                raise TypeError(f"unknown multigrid option {k}")
+            setattr(o, k, v)
+        self.options = o
+        keep = []
+
+        def arr(a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            keep.append(a)
+            return a.ctypes.data_as(C.c_void_p)
+
+        d = _capi.MeshDesc()
+        pts = np.ascontiguousarray(coarse.points, np.float64)
+        d.nv, d.ne, d.nt = pts.shape[0], len(coarse.ev0), len(coarse.te0)
+        d.index_base = 0
+        d.points = arr(pts, np.float64)
+        d.e_v0, d.e_v1 = arr(coarse.ev0, np.int32), arr(coarse.ev1, np.int32)
+        d.t_e0, d.t_e1, d.t_e2 = (arr(coarse.te0, np.int32), arr(coarse.te1, np.int32),
+                                  arr(coarse.te2, np.int32))
+        d.edge_orientation = arr(coarse.edge_orientation, np.int8)
+        d.tri_orientation = arr(coarse.tri_orientation, np.int8)
+        d.center = o.center
+        h = C.c_void_p()
+        check(lib().dec_mg_create(C.byref(d), C.byref(o), C.byref(h)))
+        self._h = h
+        self.nlevels = levels + 1
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _capi._lib is not None:
+            _capi._lib.dec_mg_destroy(h)
+            self._h = None
+
+    def level_info(self, level):
+        nv, ne, nt, lm = C.c_int64(), C.c_int64(), C.c_int64(), C.c_double()
+        check(lib().dec_mg_level_info(self._h, level, C.byref(nv), C.byref(ne), C.byref(nt), C.byref(lm)))
+        return nv.value, ne.value, nt.value, lm.value
+
+    def level_mesh(self, level):
+        h = C.c_void_p()
+        check(lib().dec_mg_level_mesh(self._h, level, C.byref(h)))
+        m = Mesh._borrow(h)
+        m._parent = self
+        return m
+
+    def level_op(self, level):
+        h = C.c_void_p()
+        check(lib().dec_mg_level_op(self._h, level, C.byref(h)))
+        op = Operator(None, 0, handle=h)
+        op._parent = self
+        return op
+
+    @property
+    def n(self):
+        return self.level_info(0)[0]
+
+    def cycles(self, u, b, cycles):
+        """u <- `cycles` V- (or W-) cycles on A u = b; u, b float64 CUDA tensors (n,) or (nrhs, n)."""
+        nrhs = 1 if b.dim() == 1 else b.shape[0]
+        check(lib().dec_mg_cycles(self._h, _ptr(u), _ptr(b), nrhs, cycles, _stream()))
+        return u
+
+    def solve(self, u, b, rtol=1e-8, max_iters=100):
+        nrhs = 1 if b.dim() == 1 else b.shape[0]
+        rep = _capi.SolveReport()
+        st = lib().dec_mg_solve(self._h, _ptr(u), _ptr(b), nrhs, rtol, max_iters, C.byref(rep), _stream())
+        if st not in (_capi.DEC_OK, 4):
+            check(st)
+        return u, rep
+
+    def solve_host(self, u, b, rtol=1e-8, max_iters=100):
+        """Same solve on host numpy arrays (float64, (n,) or (nrhs, n)); copies are part of the call."""
+        nrhs = 1 if b.ndim == 1 else b.shape[0]
+        rep = _capi.SolveReport()
+        st = lib().dec_mg_solve_host(self._h, u.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p),
+                                     nrhs, rtol, max_iters, C.byref(rep), _stream())
+        if st not in (_capi.DEC_OK, 4):
+            check(st)
+        return u, rep
+
+
+def multigrid_vcycles(u, b, md, cycles):
+    """multigrid_vcycles(u, b, md, cycles) (Multigrid.jl:814): returns the updated u (a copy)."""
+    u = u.clone()
+    return md.cycles(u, b, cycles)
+
+
+def multigrid_wcycles(u, b, md, cycles):
+    if md.options.mu != 2:
+        raise ValueError("build the MultigridData with mu=2 for W-cycles")
+    u = u.clone()
+    return md.cycles(u, b, cycles)

@@ -1,0 +1,217 @@
+// extern "C" entry points of libdec_b200.so (declared in include/dec_b200.h).  Each one turns
+// exceptions from the implementation into a dec_status and a thread-local message.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "mesh.cuh"
+#include "mg.cuh"
+#include "ops.cuh"
+
+// Implementations (wedge.cu, ops.cu).
+dec_wedge_plan* wedge_plan_create_impl(dec_mesh* mh, int kind, int da, int db, dec_dtype dt);
+void wedge_apply_impl(dec_wedge_plan* P, const void* a, const void* b, void* out, int count, void* stream);
+void wedge_plan_destroy_impl(dec_wedge_plan* P);
+void wedge_lengths_impl(const dec_wedge_plan* P, int64_t* la, int64_t* lb, int64_t* lo);
+dec_op* op_create_impl(dec_mesh* mh, int kind, double shift, dec_dtype dt);
+void op_apply_impl(dec_op* op, const void* x, void* y, double alpha, double beta, void* stream);
+void op_export_csr_impl(const dec_op* op, int64_t* nnz, int32_t* rowptr, int32_t* colind, double* val);
+void hodge_diag_impl(const dec_mesh* mh, int k, int inverse, dec_dtype dt, void* out, void* stream);
+
+namespace {
+thread_local std::string g_err;
+
+template <class F>
+dec_status guard(F&& f) {
+  try {
+    f();
+    g_err.clear();
+    return DEC_OK;
+  } catch (const decb::Error& e) {
+    g_err = e.what();
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    g_err = "host allocation failed";
+    return DEC_ERR_OOM;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return DEC_ERR_INVALID_ARG;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+const char* dec_last_error(void) { return g_err.c_str(); }
+int32_t dec_version(void) { return 1; }
+
+dec_status dec_mesh_create(const dec_mesh_desc* desc, dec_mesh** out) {
+  return guard([&] {
+    decb::require(desc && out, "dec_mesh_create: null argument");
+    *out = nullptr;
+    auto* m = new dec_mesh();
+    try {
+      m->m.build(*desc);
+    } catch (...) {
+      delete m;
+      throw;
+    }
+    *out = m;
+  });
+}
+
+dec_status dec_mesh_destroy(dec_mesh* m) {
+  return guard([&] { delete m; });
+}
+
+dec_status dec_mesh_counts(const dec_mesh* m, int64_t* nv, int64_t* ne, int64_t* nt) {
+  return guard([&] {
+    decb::require(m != nullptr, "dec_mesh_counts: null mesh");
+    if (nv) *nv = m->m.nv;
+    if (ne) *ne = m->m.ne;
+    if (nt) *nt = m->m.nt;
+  });
+}
+
+dec_status dec_mesh_orientation(const dec_mesh* m, int8_t* eo, int8_t* to) {
+  return guard([&] {
+    decb::require(m != nullptr, "dec_mesh_orientation: null mesh");
+    if (eo) std::memcpy(eo, m->m.h_eo.data(), m->m.h_eo.size());
+    if (to) std::memcpy(to, m->m.h_to.data(), m->m.h_to.size());
+  });
+}
+
+dec_status dec_mesh_geometry(const dec_mesh* mh, int32_t which, double* out, int64_t len) {
+  return guard([&] {
+    decb::require(mh != nullptr && out != nullptr, "dec_mesh_geometry: null argument");
+    const decb::Mesh& m = mh->m;
+    std::vector<double> v;
+    switch (which) {
+      case DEC_GEOM_LENGTH: v = m.length.download(); break;
+      case DEC_GEOM_AREA: v = m.area.download(); break;
+      case DEC_GEOM_DUAL_AREA: v = m.dual_area.download(); break;
+      case DEC_GEOM_DUAL_LENGTH_TE: v = m.dual_len_te.download(); break;
+      case DEC_GEOM_DUAL_POINT: {
+        auto tc = m.tri_center.download();
+        v.resize(3 * ((size_t)m.nv + m.ne + m.nt));
+        std::copy(m.h_pts.begin(), m.h_pts.end(), v.begin());
+        for (int e = 0; e < m.ne; ++e)
+          for (int k = 0; k < 3; ++k)
+            v[3 * ((size_t)m.nv + e) + k] = (m.h_pts[3 * (size_t)m.h_ev0[e] + k] + m.h_pts[3 * (size_t)m.h_ev1[e] + k]) / 2;
+        std::copy(tc.begin(), tc.end(), v.begin() + 3 * ((size_t)m.nv + m.ne));
+        break;
+      }
+      default: throw decb::Error(DEC_ERR_INVALID_ARG, "dec_mesh_geometry: unknown array");
+    }
+    decb::require((int64_t)v.size() == len, "dec_mesh_geometry: length mismatch (expected " + std::to_string(v.size()) + ")");
+    std::copy(v.begin(), v.end(), out);
+  });
+}
+
+dec_status dec_hodge_diag(const dec_mesh* m, int32_t k, int32_t inverse, dec_dtype dt, void* out, void* stream) {
+  return guard([&] { hodge_diag_impl(m, k, inverse, dt, out, stream); });
+}
+
+dec_status dec_wedge_plan_create(dec_mesh* m, int32_t kind, int32_t da, int32_t db, dec_dtype dt,
+                                 dec_wedge_plan** out) {
+  return guard([&] {
+    decb::require(out != nullptr, "dec_wedge_plan_create: null output");
+    *out = nullptr;
+    *out = wedge_plan_create_impl(m, kind, da, db, dt);
+  });
+}
+
+dec_status dec_wedge_apply(dec_wedge_plan* p, const void* a, const void* b, void* out, void* stream) {
+  return guard([&] { wedge_apply_impl(p, a, b, out, 1, stream); });
+}
+
+dec_status dec_wedge_apply_batched(dec_wedge_plan* p, const void* a, const void* b, void* out, int32_t count,
+                                   void* stream) {
+  return guard([&] { wedge_apply_impl(p, a, b, out, count, stream); });
+}
+
+dec_status dec_wedge_lengths(const dec_wedge_plan* p, int64_t* la, int64_t* lb, int64_t* lo) {
+  return guard([&] { wedge_lengths_impl(p, la, lb, lo); });
+}
+
+dec_status dec_wedge_plan_destroy(dec_wedge_plan* p) {
+  return guard([&] { wedge_plan_destroy_impl(p); });
+}
+
+dec_status dec_op_create(dec_mesh* m, int32_t kind, double shift, dec_dtype dt, dec_op** out) {
+  return guard([&] {
+    decb::require(out != nullptr, "dec_op_create: null output");
+    *out = nullptr;
+    *out = op_create_impl(m, kind, shift, dt);
+  });
+}
+
+dec_status dec_op_shape(const dec_op* op, int64_t* rows, int64_t* cols) {
+  return guard([&] {
+    decb::require(op != nullptr, "dec_op_shape: null operator");
+    if (rows) *rows = op->rows;
+    if (cols) *cols = op->cols;
+  });
+}
+
+dec_status dec_op_apply(dec_op* op, const void* x, void* y, double alpha, double beta, void* stream) {
+  return guard([&] { op_apply_impl(op, x, y, alpha, beta, stream); });
+}
+
+dec_status dec_op_export_csr(const dec_op* op, int64_t* nnz, int32_t* rowptr, int32_t* colind, double* val) {
+  return guard([&] { op_export_csr_impl(op, nnz, rowptr, colind, val); });
+}
+
+dec_status dec_op_destroy(dec_op* op) {
+  return guard([&] { delete op; });
+}
+
+void dec_mg_default_options(dec_mg_options* o) {
+  if (o) decb::mg_default_options(*o);
+}
+
+dec_status dec_mg_create(const dec_mesh_desc* coarse, const dec_mg_options* opts, dec_mg** out) {
+  return guard([&] {
+    decb::require(coarse && opts && out, "dec_mg_create: null argument");
+    *out = nullptr;
+    *out = decb::mg_create(*coarse, *opts);
+  });
+}
+
+dec_status dec_mg_destroy(dec_mg* mg) {
+  return guard([&] { decb::mg_destroy(mg); });
+}
+
+dec_status dec_mg_level_info(const dec_mg* mg, int32_t level, int64_t* nv, int64_t* ne, int64_t* nt, double* lmax) {
+  return guard([&] { decb::mg_level_info(mg, level, nv, ne, nt, lmax); });
+}
+
+dec_status dec_mg_level_mesh(const dec_mg* mg, int32_t level, const dec_mesh** out) {
+  return guard([&] { *out = decb::mg_level_mesh(mg, level); });
+}
+
+dec_status dec_mg_level_op(const dec_mg* mg, int32_t level, const dec_op** out) {
+  return guard([&] { *out = decb::mg_level_op(mg, level); });
+}
+
+dec_status dec_mg_cycles(dec_mg* mg, double* u, const double* b, int32_t nrhs, int32_t cycles, void* stream) {
+  return guard([&] { decb::mg_cycles(mg, u, b, nrhs, cycles, stream); });
+}
+
+dec_status dec_mg_solve(dec_mg* mg, double* u, const double* b, int32_t nrhs, double rtol, int32_t max_iters,
+                        dec_solve_report* rep, void* stream) {
+  dec_status st = DEC_OK;
+  dec_status g = guard([&] { st = decb::mg_solve(mg, u, b, nrhs, rtol, max_iters, rep, stream, false); });
+  return g != DEC_OK ? g : st;
+}
+
+dec_status dec_mg_solve_host(dec_mg* mg, double* u, const double* b, int32_t nrhs, double rtol, int32_t max_iters,
+                             dec_solve_report* rep, void* stream) {
+  dec_status st = DEC_OK;
+  dec_status g = guard([&] { st = decb::mg_solve(mg, u, b, nrhs, rtol, max_iters, rep, stream, true); });
+  return g != DEC_OK ? g : st;
+}
+
+}  // extern "C"

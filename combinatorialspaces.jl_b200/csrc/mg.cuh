@@ -1,0 +1,16 @@
+// Geometric multigrid over binary-subdivision hierarchies (declarations for the C ABI).
+#pragma once
+#include "mesh.cuh"
+#include "ops.cuh"
+
+namespace decb {
+void mg_default_options(dec_mg_options& o);
+dec_mg* mg_create(const dec_mesh_desc& coarse, const dec_mg_options& opts);
+void mg_destroy(dec_mg* mg);
+void mg_level_info(const dec_mg* mg, int level, int64_t* nv, int64_t* ne, int64_t* nt, double* lmax);
+const dec_mesh* mg_level_mesh(const dec_mg* mg, int level);
+const dec_op* mg_level_op(const dec_mg* mg, int level);
+void mg_cycles(dec_mg* mg, double* u, const double* b, int nrhs, int cycles, void* stream);
+dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rtol, int max_iters,
+                    dec_solve_report* rep, void* stream, bool host_buffers);
+}  // namespace decb

@@ -1,0 +1,24 @@
+// Operator handle shared by ops.cu, mg.cu and the C ABI.
+#pragma once
+#include "mesh.cuh"
+
+struct dec_op {
+  decb::Mesh* m = nullptr;
+  int kind = 0;
+  dec_dtype dtype = DEC_F64;
+  double shift = 0.0;
+  int64_t rows = 0, cols = 0;
+  decb::DArr<double> diag64;  // diagonal operators
+  decb::DArr<float> diag32;
+  int W = 0;                  // ELL width (Laplacian / Helmholtz)
+  decb::DArr<int32_t> col;
+  decb::DArr<double> val64;
+  decb::DArr<float> val32;
+};
+
+namespace decb {
+void hodge_into(const Mesh& m, int k, bool inverse, DArr<double>& out);
+void assemble_laplacian(const Mesh& m, double shift, int& W, DArr<int32_t>& col, DArr<double>& val);
+template <class T>
+void cast_array(const DArr<double>& a, DArr<T>& b);
+}  // namespace decb

@@ -1,0 +1,415 @@
+// Wedge products of the FastDEC hot path (src/FastDEC.jl:38-401) as sm_100a kernels.
+//
+// Layout: every per-simplex stream (indices, coefficients, the form indexed by the output
+// simplex, the output) is a separate SoA array, so a warp's loads of one stream are one
+// contiguous 128-256 B segment; only the forms addressed through an index (f[∂v], α[∂e]) are
+// gathered, and those come mostly from L2 because neighbouring simplices share faces.  Each
+// thread handles ITEMS outputs spaced one block apart, issuing all loads before any use.
+//
+// The expressions mirror the reference kernels term by term and this file is compiled without
+// FMA contraction, so FP64 / FP32 results reproduce the reference CPU arithmetic bit for bit
+// where the reference's order of operations is kept (∧01, ∧11, the pd/dd SpMV forms).
+#include <algorithm>
+
+#include "mesh.cuh"
+
+namespace decb {
+
+enum WedgeOp { W01, W10, W02, W20, W11, WDD01, WDD10, WPD01, WDP10 };
+
+template <class T>
+struct CoefSet {
+  DArr<T> c[3];
+  DArr<int32_t> idx;  // ELL indices for the sparse (pd / dd) forms
+  DArr<T> val;
+  int width = 0;
+};
+
+}  // namespace decb
+
+struct dec_wedge_plan {
+  decb::Mesh* m = nullptr;
+  int op = 0;
+  dec_dtype dtype = DEC_F64;
+  int64_t len_a = 0, len_b = 0, len_out = 0;
+  decb::CoefSet<double> c64;
+  decb::CoefSet<float> c32;
+};
+
+namespace decb {
+
+constexpr int kItems = 4;
+constexpr int kThreads = 256;
+
+// wedge_kernel_01!, FastDEC.jl:159-163: res[e] = ½ α[e] (f[∂v0 e] + f[∂v1 e]).
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_w01(int ne, const int32_t* __restrict__ ev0,
+                                                  const int32_t* __restrict__ ev1, const T* __restrict__ f,
+                                                  const T* __restrict__ a, T* __restrict__ out) {
+  const T half = T(0.5);
+  for (long long base = (long long)blockIdx.x * kThreads * kItems; base < ne;
+       base += (long long)gridDim.x * kThreads * kItems) {
+    int i0[kItems], i1[kItems];
+    T av[kItems];
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+      long long e = base + j * kThreads + threadIdx.x;
+      if (e < ne) {
+        i0[j] = __ldcs(ev0 + e);
+        i1[j] = __ldcs(ev1 + e);
+        av[j] = __ldcs(a + e);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+      long long e = base + j * kThreads + threadIdx.x;
+      if (e < ne) __stcs(out + e, half * av[j] * (__ldg(f + i0[j]) + __ldg(f + i1[j])));
+    }
+  }
+}
+
+// wedge_kernel_02!, FastDEC.jl:165-170, with the two dual triangles at each vertex folded into
+// one coefficient w_k = (dA_2k + dA_2k+1) / area: res[t] = α[t] Σ_k w_k f[v_k].
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_w02(int nt, const int32_t* __restrict__ tv0,
+                                                  const int32_t* __restrict__ tv1, const int32_t* __restrict__ tv2,
+                                                  const T* __restrict__ w0, const T* __restrict__ w1,
+                                                  const T* __restrict__ w2, const T* __restrict__ f,
+                                                  const T* __restrict__ a, T* __restrict__ out) {
+  for (long long base = (long long)blockIdx.x * kThreads * kItems; base < nt;
+       base += (long long)gridDim.x * kThreads * kItems) {
+    int v[kItems][3];
+    T w[kItems][3], av[kItems];
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+      long long t = base + j * kThreads + threadIdx.x;
+      if (t < nt) {
+        v[j][0] = __ldcs(tv0 + t);
+        v[j][1] = __ldcs(tv1 + t);
+        v[j][2] = __ldcs(tv2 + t);
+        w[j][0] = __ldcs(w0 + t);
+        w[j][1] = __ldcs(w1 + t);
+        w[j][2] = __ldcs(w2 + t);
+        av[j] = __ldcs(a + t);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+      long long t = base + j * kThreads + threadIdx.x;
+      if (t < nt)
+        __stcs(out + t, av[j] * (w[j][0] * __ldg(f + v[j][0]) + w[j][1] * __ldg(f + v[j][1]) +
+                                 w[j][2] * __ldg(f + v[j][2])));
+    }
+  }
+}
+
+// wedge_kernel_11!, FastDEC.jl:184-191.
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_w11(int nt, const int32_t* __restrict__ te0,
+                                                  const int32_t* __restrict__ te1, const int32_t* __restrict__ te2,
+                                                  const T* __restrict__ c0, const T* __restrict__ c1,
+                                                  const T* __restrict__ c2, const T* __restrict__ a,
+                                                  const T* __restrict__ b, T* __restrict__ out) {
+  for (long long base = (long long)blockIdx.x * kThreads * kItems; base < nt;
+       base += (long long)gridDim.x * kThreads * kItems) {
+    int e[kItems][3];
+    T c[kItems][3];
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+      long long t = base + j * kThreads + threadIdx.x;
+      if (t < nt) {
+        e[j][0] = __ldcs(te0 + t);
+        e[j][1] = __ldcs(te1 + t);
+        e[j][2] = __ldcs(te2 + t);
+        c[j][0] = __ldcs(c0 + t);
+        c[j][1] = __ldcs(c1 + t);
+        c[j][2] = __ldcs(c2 + t);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+      long long t = base + j * kThreads + threadIdx.x;
+      if (t < nt) {
+        T ae0 = __ldg(a + e[j][0]), ae1 = __ldg(a + e[j][1]), ae2 = __ldg(a + e[j][2]);
+        T be0 = __ldg(b + e[j][0]), be1 = __ldg(b + e[j][1]), be2 = __ldg(b + e[j][2]);
+        __stcs(out + t, (c[j][0] * (ae2 * be1 - ae1 * be2) + c[j][1] * (ae2 * be0 - ae0 * be2) +
+                         c[j][2] * (ae1 * be0 - ae0 * be1)));
+      }
+    }
+  }
+}
+
+// (M x) .* y with M a row-major ELL matrix (columns sorted, -1 = padding): the
+// "matrix then elementwise product" form of the pd / dd wedges, FastDEC.jl:317-325, :381-389.
+template <class T, int W>
+__global__ void __launch_bounds__(kThreads) k_ell_hadamard(int n, const int32_t* __restrict__ idx,
+                                                           const T* __restrict__ val, const T* __restrict__ x,
+                                                           const T* __restrict__ y, T* __restrict__ out,
+                                                           int mx_first) {
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
+    T s = T(0);
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+      int c = __ldcs(idx + (size_t)i * W + q);
+      T v = __ldcs(val + (size_t)i * W + q);
+      if (c >= 0) s += v * __ldg(x + c);
+    }
+    T yi = __ldcs(y + i);
+    __stcs(out + i, mx_first ? s * yi : yi * s);
+  }
+}
+
+// ---- coefficient set-up kernels (FP64) -----------------------------------------------------
+
+// wedge_kernel_coeffs(Val(1), Val(1)), FastDEC.jl:78-93.
+__global__ void k_coef11(int nt, const int32_t* __restrict__ te0, const int32_t* __restrict__ te1,
+                         const int32_t* __restrict__ te2, const int8_t* __restrict__ es,
+                         const int8_t* __restrict__ ts, const double* __restrict__ area,
+                         const double* __restrict__ da, double* c0, double* c1, double* c2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
+    double ar = (double)ts[i] * 2 * area[i];
+    int e0 = te0[i], e1 = te1[i], e2 = te2[i];
+    double s0 = es[e0], s1 = es[e1], s2 = es[e2];
+    c0[i] = s1 * s2 * (da[i] + da[i + (size_t)nt]) / ar;
+    c1[i] = s0 * s2 * (da[i + 2 * (size_t)nt] + da[i + 3 * (size_t)nt]) / ar;
+    c2[i] = s0 * s1 * (da[i + 4 * (size_t)nt] + da[i + 5 * (size_t)nt]) / ar;
+  }
+}
+
+// wedge_kernel_coeffs(Val(0), Val(2)), FastDEC.jl:50-62, folded per vertex.
+__global__ void k_coef02(int nt, const double* __restrict__ area, const double* __restrict__ da,
+                         double* w0, double* w1, double* w2) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+    double ar = area[t];
+    w0[t] = da[t] / ar + da[t + (size_t)nt] / ar;
+    w1[t] = da[t + 2 * (size_t)nt] / ar + da[t + 3 * (size_t)nt] / ar;
+    w2[t] = da[t + 4 * (size_t)nt] / ar + da[t + 5 * (size_t)nt] / ar;
+  }
+}
+
+// Rows of wedge_dd_01_mat (FastDEC.jl:293-305) and wedge_pd_01_mat (:329-347).  For edge e the
+// dual edges of e are its triangle-center -> edge-center dual edges in (k, t) order; the weight
+// of triangle t is dual_length / Σ dual_length.
+__global__ void k_rows_dd_pd(int ne, int nt, int pd, const int32_t* __restrict__ e2t_ptr,
+                             const int32_t* __restrict__ e2t, const double* __restrict__ dlen,
+                             const int32_t* __restrict__ ev0, const int32_t* __restrict__ ev1,
+                             const int32_t* __restrict__ tv0, const int32_t* __restrict__ tv1,
+                             const int32_t* __restrict__ tv2, int32_t* idx, double* val, int width,
+                             int* overflow) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+    int b = e2t_ptr[e], n = e2t_ptr[e + 1] - b;
+    double sum = 0.0;
+    for (int q = 0; q < n; ++q) {
+      int tk = e2t[b + q];
+      sum += dlen[(size_t)(tk % 3) * nt + tk / 3];
+    }
+    int cols[8];
+    double vals[8];
+    int cnt = 0;
+    auto add = [&](int c, double v) {  // m[e, c] += v
+      for (int q = 0; q < cnt; ++q)
+        if (cols[q] == c) { vals[q] = vals[q] + v; return; }
+      if (cnt < 8) { cols[cnt] = c; vals[cnt] = 0.0 + v; ++cnt; }
+      else atomicExch(overflow, 1);
+    };
+    int va = ev0[e], vb = ev1[e];
+    for (int q = 0; q < n; ++q) {
+      int tk = e2t[b + q], t = tk / 3;
+      double w = dlen[(size_t)(tk % 3) * nt + t] / sum;
+      if (!pd) {
+        add(t, w);
+      } else {
+        int tvs[3] = {tv0[t], tv1[t], tv2[t]};
+        int l = -1;
+        for (int k = 0; k < 3; ++k)
+          if (tvs[k] != va && tvs[k] != vb) l = tvs[k];
+        add(va, w * 5 / 12);
+        add(vb, w * 5 / 12);
+        if (l >= 0) add(l, w * 2 / 12);
+      }
+    }
+    // sort by column (the CSC SpMV order)
+    for (int i = 1; i < cnt; ++i)
+      for (int j = i; j > 0 && cols[j - 1] > cols[j]; --j) {
+        int tc = cols[j]; cols[j] = cols[j - 1]; cols[j - 1] = tc;
+        double tv = vals[j]; vals[j] = vals[j - 1]; vals[j - 1] = tv;
+      }
+    if (cnt > width) { atomicExch(overflow, 1); cnt = width; }
+    for (int q = 0; q < width; ++q) {
+      idx[(size_t)e * width + q] = q < cnt ? cols[q] : -1;
+      val[(size_t)e * width + q] = q < cnt ? vals[q] : 0.0;
+    }
+  }
+}
+
+template <class T>
+__global__ void k_cast(size_t n, const double* __restrict__ a, T* __restrict__ b) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = (T)a[i];
+}
+
+template <class T>
+static void cast_into(const DArr<double>& src, DArr<T>& dst) {
+  dst.alloc(src.n);
+  if (src.n) k_cast<T><<<grid_for((long long)src.n, 256), 256>>>(src.n, src.p, dst.p);
+  DEC_CHECK_LAUNCH();
+}
+
+// ---- plan ---------------------------------------------------------------------------------
+
+static void build_plan(dec_wedge_plan& P) {
+  Mesh& m = *P.m;
+  const int T = 256;
+  CoefSet<double>& c = P.c64;
+  if (P.op == W11) {
+    for (auto& x : c.c) x.alloc(m.nt);
+    if (m.nt)
+      k_coef11<<<grid_for(m.nt, T), T>>>(m.nt, m.te0.p, m.te1.p, m.te2.p, m.esign.p, m.tsign.p, m.area.p,
+                                         m.dual_area.p, c.c[0].p, c.c[1].p, c.c[2].p);
+  } else if (P.op == W02 || P.op == W20) {
+    for (auto& x : c.c) x.alloc(m.nt);
+    if (m.nt) k_coef02<<<grid_for(m.nt, T), T>>>(m.nt, m.area.p, m.dual_area.p, c.c[0].p, c.c[1].p, c.c[2].p);
+  } else if (P.op >= WDD01) {
+    bool pd = (P.op == WPD01 || P.op == WDP10);
+    c.width = pd ? 4 : 2;
+    c.idx.alloc((size_t)m.ne * c.width);
+    c.val.alloc((size_t)m.ne * c.width);
+    DArr<int> overflow(1);
+    DEC_CUDA(cudaMemset(overflow.p, 0, sizeof(int)));
+    if (m.ne)
+      k_rows_dd_pd<<<grid_for(m.ne, T), T>>>(m.ne, m.nt, pd, m.e2t_ptr.p, m.e2t.p, m.dual_len_te.p, m.ev0.p,
+                                             m.ev1.p, m.tv0.p, m.tv1.p, m.tv2.p, c.idx.p, c.val.p, c.width,
+                                             overflow.p);
+    DEC_CHECK_LAUNCH();
+    int of = overflow.download()[0];
+    if (of) throw Error(DEC_ERR_UNSUPPORTED, "wedge: an edge has more incident triangles than supported (non-manifold mesh)");
+  }
+  DEC_CHECK_LAUNCH();
+  if (P.dtype == DEC_F32) {
+    for (int k = 0; k < 3; ++k) cast_into(c.c[k], P.c32.c[k]);
+    if (c.width) {
+      cast_into(c.val, P.c32.val);
+      P.c32.width = c.width;
+    }
+  }
+  DEC_CUDA(cudaDeviceSynchronize());
+}
+
+template <class T>
+static void launch_plan(dec_wedge_plan& P, const CoefSet<T>& c, const void* va, const void* vb, void* vo,
+                        cudaStream_t s) {
+  Mesh& m = *P.m;
+  const T* a = (const T*)va;
+  const T* b = (const T*)vb;
+  T* o = (T*)vo;
+  const int* idx = P.c64.idx.p;
+  switch (P.op) {
+    case W01:
+    case W10: {
+      const T* f = P.op == W01 ? a : b;
+      const T* al = P.op == W01 ? b : a;
+      if (m.ne) k_w01<T><<<grid_for(m.ne, kThreads * kItems), kThreads, 0, s>>>(m.ne, m.ev0.p, m.ev1.p, f, al, o);
+      break;
+    }
+    case W02:
+    case W20: {
+      const T* f = P.op == W02 ? a : b;
+      const T* al = P.op == W02 ? b : a;
+      if (m.nt)
+        k_w02<T><<<grid_for(m.nt, kThreads * kItems), kThreads, 0, s>>>(m.nt, m.tv0.p, m.tv1.p, m.tv2.p, c.c[0].p,
+                                                                         c.c[1].p, c.c[2].p, f, al, o);
+      break;
+    }
+    case W11:
+      if (m.nt)
+        k_w11<T><<<grid_for(m.nt, kThreads * kItems), kThreads, 0, s>>>(m.nt, m.te0.p, m.te1.p, m.te2.p, c.c[0].p,
+                                                                         c.c[1].p, c.c[2].p, a, b, o);
+      break;
+    default:
+      break;
+  }
+  if (P.op >= WDD01) {
+    // x is the form that M acts on; y is multiplied elementwise:
+    //  dd(0,1)(f, g) = (M f) .* g,  pd(0,1)(g, f) = (M g) .* f   -> M acts on the first form
+    //  dd(1,0)(f, g) = f .* (M g),  dp(1,0)(f, g) = f .* (M g)   -> M acts on the second form
+    bool mfirst = (P.op == WDD01 || P.op == WPD01);
+    const T* x = mfirst ? a : b;
+    const T* y = mfirst ? b : a;
+    if (m.ne) {
+      if (c.width == 2)
+        k_ell_hadamard<T, 2><<<grid_for(m.ne, kThreads), kThreads, 0, s>>>(m.ne, idx, c.val.p, x, y, o, mfirst);
+      else
+        k_ell_hadamard<T, 4><<<grid_for(m.ne, kThreads), kThreads, 0, s>>>(m.ne, idx, c.val.p, x, y, o, mfirst);
+    }
+  }
+  DEC_CHECK_LAUNCH();
+}
+
+}  // namespace decb
+
+using namespace decb;
+
+dec_wedge_plan* wedge_plan_create_impl(dec_mesh* mh, int kind, int da, int db, dec_dtype dt) {
+  require(mh != nullptr, "wedge: null mesh");
+  require(dt == DEC_F64 || dt == DEC_F32, "wedge: dtype must be DEC_F64 or DEC_F32");
+  Mesh& m = mh->m;
+  int op = -1;
+  int64_t la = 0, lb = 0, lo = 0;
+  const int64_t nv = m.nv, ne = m.ne, nt = m.nt;
+  if (kind == DEC_WEDGE_PP) {
+    if (da == 0 && db == 1) { op = W01; la = nv; lb = ne; lo = ne; }
+    else if (da == 1 && db == 0) { op = W10; la = ne; lb = nv; lo = ne; }
+    else if (da == 0 && db == 2) { op = W02; la = nv; lb = nt; lo = nt; }
+    else if (da == 2 && db == 0) { op = W20; la = nt; lb = nv; lo = nt; }
+    else if (da == 1 && db == 1) { op = W11; la = ne; lb = ne; lo = nt; }
+  } else if (kind == DEC_WEDGE_DD) {
+    if (da == 0 && db == 1) { op = WDD01; la = nt; lb = ne; lo = ne; }
+    else if (da == 1 && db == 0) { op = WDD10; la = ne; lb = nt; lo = ne; }
+  } else if (kind == DEC_WEDGE_PD) {
+    if (da == 0 && db == 1) { op = WPD01; la = nv; lb = ne; lo = ne; }
+  } else if (kind == DEC_WEDGE_DP) {
+    if (da == 1 && db == 0) { op = WDP10; la = ne; lb = nv; lo = ne; }
+  }
+  if (op < 0)
+    throw Error(DEC_ERR_UNSUPPORTED,
+                "Unsupported combination of degrees " + std::to_string(da) + " and " + std::to_string(db) +
+                    ". Ensure that their sum is not greater than the degree of the complex.");
+  auto* P = new dec_wedge_plan();
+  P->m = &m;
+  P->op = op;
+  P->dtype = dt;
+  P->len_a = la;
+  P->len_b = lb;
+  P->len_out = lo;
+  try {
+    build_plan(*P);
+  } catch (...) {
+    delete P;
+    throw;
+  }
+  return P;
+}
+
+void wedge_apply_impl(dec_wedge_plan* P, const void* a, const void* b, void* out, int count, void* stream) {
+  require(P != nullptr, "wedge: null plan");
+  require(a && b && out, "wedge: null form pointer");
+  require(count >= 1, "wedge: count must be >= 1");
+  cudaStream_t s = as_stream(stream);
+  const size_t es = P->dtype == DEC_F64 ? 8 : 4;
+  for (int i = 0; i < count; ++i) {
+    const char* ai = (const char*)a + (size_t)i * P->len_a * es;
+    const char* bi = (const char*)b + (size_t)i * P->len_b * es;
+    char* oi = (char*)out + (size_t)i * P->len_out * es;
+    if (P->dtype == DEC_F64) launch_plan<double>(*P, P->c64, ai, bi, oi, s);
+    else launch_plan<float>(*P, P->c32, ai, bi, oi, s);
+  }
+}
+
+void wedge_plan_destroy_impl(dec_wedge_plan* P) { delete P; }
+
+void wedge_lengths_impl(const dec_wedge_plan* P, int64_t* la, int64_t* lb, int64_t* lo) {
+  require(P != nullptr, "wedge: null plan");
+  if (la) *la = P->len_a;
+  if (lb) *lb = P->len_b;
+  if (lo) *lo = P->len_out;
+}

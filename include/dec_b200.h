@@ -1,0 +1,179 @@
+/*
+ * dec_b200.h - C ABI of libdec_b200.so, the sm_100a (B200) implementation of the
+ * CombinatorialSpaces.jl DEC hot path: FastDEC wedge products, the exterior derivative /
+ * boundary / Hodge star / Laplace-Beltrami operators, and the Multigrid.jl geometric V-cycle
+ * over binary-subdivision hierarchies.
+ *
+ * Conventions
+ *  - Every entry point returns a dec_status; on failure dec_last_error() holds a message
+ *    (thread-local).  Nothing aborts or traps.
+ *  - Forms (cochains) are caller-owned DEVICE arrays in the reference's element order
+ *    (vertices, edges, triangles as numbered by the mesh description).  Work is enqueued on
+ *    the caller's stream (a cudaStream_t passed as void*, NULL = legacy default stream).
+ *  - Mesh, plan, operator and multigrid handles own their device memory.  A handle must not
+ *    be used from two host threads at once.
+ *  - Index arrays in dec_mesh_desc are int32 with a selectable base (1 for Julia callers).
+ */
+#ifndef DEC_B200_H
+#define DEC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum dec_status {
+  DEC_OK = 0,
+  DEC_ERR_INVALID_ARG = 1,
+  DEC_ERR_OOM = 2,
+  DEC_ERR_CUDA = 3,
+  DEC_ERR_NOT_CONVERGED = 4,
+  DEC_ERR_TIMEOUT = 5,
+  DEC_ERR_UNSUPPORTED = 6,
+  DEC_ERR_NON_ORIENTABLE = 7
+} dec_status;
+
+typedef enum dec_dtype { DEC_F64 = 0, DEC_F32 = 1 } dec_dtype;
+
+/* Barycenter() / Circumcenter(), src/DiscreteExteriorCalculus.jl:98-135 */
+typedef enum dec_center { DEC_BARYCENTER = 0, DEC_CIRCUMCENTER = 1 } dec_center;
+
+typedef struct dec_mesh dec_mesh;
+typedef struct dec_wedge_plan dec_wedge_plan;
+typedef struct dec_op dec_op;
+typedef struct dec_mg dec_mg;
+
+/*
+ * A primal 2D delta set with embedding, i.e. the fields of EmbeddedDeltaSet2D{Bool,Point3d}
+ * that the dual complex is built from (src/SimplicialSets.jl:221-411; the dual complex and its
+ * geometry follow src/DiscreteExteriorCalculus.jl:545-608 and :935-990).
+ */
+typedef struct dec_mesh_desc {
+  int32_t nv, ne, nt;
+  int32_t index_base;              /* 1 (Julia) or 0 */
+  const double* points;            /* nv x 3 row-major (x, y, z); host memory */
+  const int32_t* e_v0;             /* ∂v0 of each edge (its target); host */
+  const int32_t* e_v1;             /* ∂v1 of each edge (its source); host */
+  const int32_t* t_e0;             /* ∂e0, ∂e1, ∂e2 of each triangle; host */
+  const int32_t* t_e1;
+  const int32_t* t_e2;
+  const int8_t* edge_orientation;  /* ne; 1 true, 0 false, -1 unset (-> false); NULL = all unset */
+  const int8_t* tri_orientation;   /* nt; NULL or any -1 => orient!(s, Val(2)) is run */
+  int32_t center;                  /* dec_center */
+} dec_mesh_desc;
+
+const char* dec_last_error(void);
+int32_t dec_version(void);
+
+/* ---- mesh (replaces dualize(s, alg) + the per-operator host setup of FastDEC) ---------- */
+dec_status dec_mesh_create(const dec_mesh_desc* desc, dec_mesh** out);
+dec_status dec_mesh_destroy(dec_mesh* m);
+dec_status dec_mesh_counts(const dec_mesh* m, int64_t* nv, int64_t* ne, int64_t* nt);
+/* Orientation actually used (after orient!), copied to host arrays of ne / nt bytes. */
+dec_status dec_mesh_orientation(const dec_mesh* m, int8_t* edge_orientation, int8_t* tri_orientation);
+
+/* Geometry arrays copied to host (FP64), for parity checks:
+ * 0 length[ne], 1 area[nt], 2 dual_area[6nt] (dual-triangle order of the reference),
+ * 3 dual_length of the 3nt triangle-center -> edge-center dual edges, 4 dual_point[3(nv+ne+nt)] */
+typedef enum dec_geometry { DEC_GEOM_LENGTH = 0, DEC_GEOM_AREA = 1, DEC_GEOM_DUAL_AREA = 2,
+                            DEC_GEOM_DUAL_LENGTH_TE = 3, DEC_GEOM_DUAL_POINT = 4 } dec_geometry;
+dec_status dec_mesh_geometry(const dec_mesh* m, int32_t which, double* host_out, int64_t len);
+
+/* ---- Hodge star (replaces dec_hodge_star / dec_inv_hodge_star(n, sd, DiagonalHodge(),
+ *      Val(:CUDA)), ext/CombinatorialSpacesCUDAExt.jl:70-96, which return a CuArray) ------- */
+dec_status dec_hodge_diag(const dec_mesh* m, int32_t k, int32_t inverse, dec_dtype dtype,
+                          void* out, void* stream);
+
+/* ---- wedge products (replaces dec_wedge_product(m, n, sd, Val(:CUDA), CuArray, T) and
+ *      dec_c_wedge_product!, src/FastDEC.jl:217-289, and the pd / dp / dd wedges :291-401) ---- */
+typedef enum dec_wedge_kind {
+  DEC_WEDGE_PP = 0, /* primal-primal (0,1) (1,0) (0,2) (2,0) (1,1), FastDEC.jl:255-279 */
+  DEC_WEDGE_PD = 1, /* primal-dual (0,1) (1,1), FastDEC.jl:386-395 */
+  DEC_WEDGE_DP = 2, /* dual-primal (1,0) (1,1), FastDEC.jl:381-384, :397-401 */
+  DEC_WEDGE_DD = 3  /* dual-dual (0,1) (1,0), FastDEC.jl:317-325 */
+} dec_wedge_kind;
+dec_status dec_wedge_plan_create(dec_mesh* m, int32_t kind, int32_t deg_a, int32_t deg_b,
+                                 dec_dtype dtype, dec_wedge_plan** out);
+/* out = a ∧ b; a and b are device forms in the degrees given at plan creation. */
+dec_status dec_wedge_apply(dec_wedge_plan* p, const void* a, const void* b, void* out, void* stream);
+/* Lengths of the a, b and out forms of a plan. */
+dec_status dec_wedge_lengths(const dec_wedge_plan* p, int64_t* len_a, int64_t* len_b, int64_t* len_out);
+/* Batched launch: out_i = a_i ∧ b_i for `count` form pairs laid out back to back. */
+dec_status dec_wedge_apply_batched(dec_wedge_plan* p, const void* a, const void* b, void* out,
+                                   int32_t count, void* stream);
+dec_status dec_wedge_plan_destroy(dec_wedge_plan* p);
+
+/* ---- sparse operators (replaces dec_differential / dec_boundary / dec_dual_derivative(n, sd,
+ *      Val(:CUDA)), ext/CombinatorialSpacesCUDAExt.jl:30-61, the diagonal Hodge stars, and
+ *      the Laplacian fast_laplace_beltrami of test/Multigrid.jl:46-48 = ∇²(0),
+ *      src/DiscreteExteriorCalculus.jl:1889) ----------------------------------------------- */
+typedef enum dec_op_kind {
+  DEC_OP_D0 = 0, DEC_OP_D1 = 1,                 /* dec_differential(0|1), FastDEC.jl:468-524 */
+  DEC_OP_BOUNDARY1 = 2, DEC_OP_BOUNDARY2 = 3,   /* dec_boundary(1|2), FastDEC.jl:433-437 */
+  DEC_OP_DUAL_D0 = 4, DEC_OP_DUAL_D1 = 5,       /* dec_dual_derivative(0|1), FastDEC.jl:443-453 */
+  DEC_OP_STAR0 = 6, DEC_OP_STAR1 = 7, DEC_OP_STAR2 = 8,            /* FastDEC.jl:580-604 */
+  DEC_OP_INV_STAR0 = 9, DEC_OP_INV_STAR1 = 10, DEC_OP_INV_STAR2 = 11, /* FastDEC.jl:732-737 */
+  DEC_OP_LAPLACE0 = 12,   /* ⋆0⁻¹ d0ᵀ ⋆1 d0 (positive semidefinite, = -Δ(0)) */
+  DEC_OP_HELMHOLTZ0 = 13  /* ⋆0⁻¹ d0ᵀ ⋆1 d0 + shift * I */
+} dec_op_kind;
+dec_status dec_op_create(dec_mesh* m, int32_t kind, double shift, dec_dtype dtype, dec_op** out);
+dec_status dec_op_shape(const dec_op* op, int64_t* rows, int64_t* cols);
+/* y = alpha * Op x + beta * y  (beta == 0 overwrites y). */
+dec_status dec_op_apply(dec_op* op, const void* x, void* y, double alpha, double beta, void* stream);
+/* CSR export to host, two-phase: call with rowptr == NULL to get nnz. */
+dec_status dec_op_export_csr(const dec_op* op, int64_t* nnz, int32_t* rowptr, int32_t* colind, double* val);
+dec_status dec_op_destroy(dec_op* op);
+
+/* ---- geometric multigrid (replaces MultigridData(s, BinarySubdivision(), levels, op, steps;
+ *      alg), src/Multigrid.jl:698-797, and multigrid_vcycles / multigrid_wcycles /
+ *      full_multigrid, :814-855) --------------------------------------------------------- */
+typedef enum dec_smoother {
+  DEC_SMOOTH_JACOBI = 0,     /* damped Jacobi, `pre`/`post` sweeps */
+  DEC_SMOOTH_CHEBYSHEV = 1,  /* Chebyshev-Jacobi of degree `pre`/`post` */
+  DEC_SMOOTH_CG = 2          /* Krylov.jl cg with itmax = steps (the reference's smoother) */
+} dec_smoother;
+
+typedef struct dec_mg_options {
+  int32_t levels;          /* binary subdivisions above the coarse mesh */
+  int32_t center;          /* dec_center of every level's dual complex (reference default: circumcenter) */
+  double project_radius;   /* > 0: new vertices are projected onto this sphere (icospheres) */
+  double shift;            /* operator A = L + shift * I on every level */
+  int32_t smoother;        /* dec_smoother */
+  int32_t pre, post;       /* sweeps / degree / CG steps */
+  double omega;            /* Jacobi damping */
+  double cheb_ratio;       /* Chebyshev interval [lmax / ratio, lmax] */
+  int32_t coarse_solver;   /* 0: dense direct FP64 solve on the coarsest level; 1: the smoother */
+  int32_t precision;       /* 0: FP64 V-cycles; 1: FP32 V-cycles inside FP64 iterative refinement */
+  int32_t rhs_block;       /* right-hand sides per panel (1, 2, 4, 8, 16, 32; 0 = automatic) */
+  int32_t mu;              /* 1 = V-cycle, 2 = W-cycle */
+} dec_mg_options;
+
+typedef struct dec_solve_report {
+  int32_t iterations;      /* outer iterations (cycles) run */
+  int32_t converged;       /* all right-hand sides reached rtol */
+  double max_rel_residual; /* max_j ||b_j - A u_j|| / ||b_j|| at exit (FP64) */
+  double seconds;          /* device time of the solve */
+} dec_solve_report;
+
+void dec_mg_default_options(dec_mg_options* o);
+dec_status dec_mg_create(const dec_mesh_desc* coarse, const dec_mg_options* opts, dec_mg** out);
+dec_status dec_mg_destroy(dec_mg* mg);
+/* level 0 = finest. */
+dec_status dec_mg_level_info(const dec_mg* mg, int32_t level, int64_t* nv, int64_t* ne, int64_t* nt,
+                             double* lmax);
+dec_status dec_mg_level_mesh(const dec_mg* mg, int32_t level, const dec_mesh** out);
+dec_status dec_mg_level_op(const dec_mg* mg, int32_t level, const dec_op** out);
+/* u (in/out) and b: device FP64, column-major nv x nrhs (one contiguous vector per RHS). */
+dec_status dec_mg_cycles(dec_mg* mg, double* u, const double* b, int32_t nrhs, int32_t cycles, void* stream);
+dec_status dec_mg_solve(dec_mg* mg, double* u, const double* b, int32_t nrhs, double rtol,
+                        int32_t max_iters, dec_solve_report* report, void* stream);
+/* Same solve with host u / b (pinned or pageable); copies are part of the call. */
+dec_status dec_mg_solve_host(dec_mg* mg, double* u_host, const double* b_host, int32_t nrhs, double rtol,
+                             int32_t max_iters, dec_solve_report* report, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DEC_B200_H */

@@ -188,6 +188,20 @@ PYBIND11_MODULE(dec_oracle, mod) {
     return std::chrono::duration<double>(t1 - t0).count() / reps;
   });
 
+  mod.def("csc_matvec", [](py::tuple t, py::array_t<double, py::array::c_style | py::array::forcecast> x) {
+    // y = A x in the column order of the reference's SparseMatrixCSC SpMV
+    CSC a;
+    a.colptr = from_np(t[0].cast<py::array_t<int32_t, py::array::c_style | py::array::forcecast>>());
+    a.rowval = from_np(t[1].cast<py::array_t<int32_t, py::array::c_style | py::array::forcecast>>());
+    a.nzval = from_np(t[2].cast<py::array_t<double, py::array::c_style | py::array::forcecast>>());
+    auto shape = t[3].cast<py::tuple>();
+    a.m = shape[0].cast<int>();
+    a.n = shape[1].cast<int>();
+    std::vector<double> y(a.m);
+    spmv(a, x.data(), y.data());
+    return to_np(y);
+  });
+
   // Multigrid
   mod.def("refine_binary", [](const Mesh& m, double radius) {
     Topo t = topo_of(m);
