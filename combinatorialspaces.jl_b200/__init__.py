@@ -21,6 +21,7 @@ import ctypes as C
 import numpy as np
 
 from . import _capi
+from . import meshes  # noqa: F401
 from ._capi import check, lib, DecError  # noqa: F401
 
 __all__ = ["Mesh", "Operator", "MultigridData", "dec_wedge_product", "dec_wedge_product_pd",
@@ -339,8 +340,8 @@ class MultigridData:
         d.e_v0, d.e_v1 = arr(coarse.ev0, np.int32), arr(coarse.ev1, np.int32)
         d.t_e0, d.t_e1, d.t_e2 = (arr(coarse.te0, np.int32), arr(coarse.te1, np.int32),
                                   arr(coarse.te2, np.int32))
-        d.edge_orientation = arr(coarse.edge_orientation, np.int8)
-        d.tri_orientation = arr(coarse.tri_orientation, np.int8)
+        d.edge_orientation = None if coarse.edge_orientation is None else arr(coarse.edge_orientation, np.int8)
+        d.tri_orientation = None if coarse.tri_orientation is None else arr(coarse.tri_orientation, np.int8)
         d.center = o.center
         h = C.c_void_p()
         check(lib().dec_mg_create(C.byref(d), C.byref(o), C.byref(h)))
@@ -382,6 +383,18 @@ class MultigridData:
         check(lib().dec_mg_cycles(self._h, _ptr(u), _ptr(b), nrhs, cycles, _stream()))
         return u
 
+    def autotune(self, nrhs, reps=3):
+        """Pick the fastest panel width for `nrhs` right-hand sides (dec_mg_autotune)."""
+        k = C.c_int32()
+        check(lib().dec_mg_autotune(self._h, nrhs, reps, _stream(), C.byref(k)))
+        return k.value
+
+    def time_kernel(self, kernel, level, nrhs, reps=20):
+        """(ms per launch, algorithmic bytes per launch) of one V-cycle kernel (dec_mg_time_kernel)."""
+        ms, by = C.c_double(), C.c_double()
+        check(lib().dec_mg_time_kernel(self._h, kernel, level, nrhs, reps, _stream(), C.byref(ms), C.byref(by)))
+        return ms.value, by.value
+
     def solve(self, u, b, rtol=1e-8, max_iters=100):
         nrhs = 1 if b.dim() == 1 else b.shape[0]
         rep = _capi.SolveReport()
@@ -391,11 +404,15 @@ class MultigridData:
         return u, rep
 
     def solve_host(self, u, b, rtol=1e-8, max_iters=100):
-        """Same solve on host numpy arrays (float64, (n,) or (nrhs, n)); copies are part of the call."""
+        """Same solve on host float64 arrays ((n,) or (nrhs, n); numpy or pinned torch CPU tensors);
+        the host<->device copies are part of the call."""
         nrhs = 1 if b.ndim == 1 else b.shape[0]
         rep = _capi.SolveReport()
-        st = lib().dec_mg_solve_host(self._h, u.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p),
-                                     nrhs, rtol, max_iters, C.byref(rep), _stream())
+
+        def hp(a):
+            return C.c_void_p(a.data_ptr()) if hasattr(a, "data_ptr") else a.ctypes.data_as(C.c_void_p)
+
+        st = lib().dec_mg_solve_host(self._h, hp(u), hp(b), nrhs, rtol, max_iters, C.byref(rep), _stream())
         if st not in (_capi.DEC_OK, 4):
             check(st)
         return u, rep

@@ -35,7 +35,8 @@ class MGOptions(C.Structure):
 
 class SolveReport(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32),
-                ("max_rel_residual", C.c_double), ("seconds", C.c_double)]
+                ("max_rel_residual", C.c_double), ("seconds", C.c_double),
+                ("launches", C.c_int64), ("rhs_block", C.c_int32)]
 
 
 P = C.c_void_p
@@ -73,6 +74,8 @@ SIGNATURES = {
     "dec_mg_cycles": (I32, [P, P, P, I32, I32, P]),
     "dec_mg_solve": (I32, [P, P, P, I32, F64, I32, C.POINTER(SolveReport), P]),
     "dec_mg_solve_host": (I32, [P, P, P, I32, F64, I32, C.POINTER(SolveReport), P]),
+    "dec_mg_time_kernel": (I32, [P, I32, I32, I32, I32, P, PF64, PF64]),
+    "dec_mg_autotune": (I32, [P, I32, I32, P, C.POINTER(C.c_int32)]),
 }
 
 

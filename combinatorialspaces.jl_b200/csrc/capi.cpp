@@ -214,4 +214,16 @@ dec_status dec_mg_solve_host(dec_mg* mg, double* u, const double* b, int32_t nrh
   return g != DEC_OK ? g : st;
 }
 
+dec_status dec_mg_time_kernel(dec_mg* mg, int32_t kernel, int32_t level, int32_t nrhs, int32_t reps, void* stream,
+                              double* ms, double* bytes) {
+  return guard([&] { decb::mg_time_kernel(mg, kernel, level, nrhs, reps, stream, ms, bytes); });
+}
+
+dec_status dec_mg_autotune(dec_mg* mg, int32_t nrhs, int32_t reps, void* stream, int32_t* rhs_block) {
+  return guard([&] {
+    int k = decb::mg_autotune(mg, nrhs, reps, stream);
+    if (rhs_block) *rhs_block = k;
+  });
+}
+
 }  // extern "C"

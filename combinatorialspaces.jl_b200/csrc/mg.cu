@@ -461,6 +461,7 @@ struct Workspace {
   DArr<double> ucm, bcm;       // column-major device copies for host-buffer solves
   int nblocks = 0;
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};  // GraphKind
+  int64_t launches[3] = {0, 0, 0};                          // kernel nodes per graph
   ~Workspace() {
     for (auto& g : graph)
       if (g) cudaGraphExecDestroy(g);
@@ -474,6 +475,7 @@ struct dec_mg {
   std::vector<decb::Level> lv;  // 0 = finest
   decb::DArr<double> ainv;      // coarsest dense inverse (FP64)
   std::map<long long, std::unique_ptr<decb::Workspace>> ws;
+  std::map<long long, int> tuned;  // (nrhs, precision) -> panel width chosen by the autotuner
   cudaStream_t cap = nullptr;   // capture stream
   ~dec_mg() {
     ws.clear();
@@ -777,14 +779,18 @@ static void alloc_bufs(const dec_mg& mg, std::vector<LevelBufs<T>>& bufs, int K,
     bufs[l].y.alloc(n);
     bufs[l].b.alloc(n);
     bufs[l].d.alloc(n);
+    for (DArr<T>* a : {&bufs[l].x, &bufs[l].y, &bufs[l].b, &bufs[l].d})
+      DEC_CUDA(cudaMemset(a->p, 0, a->bytes()));
   }
 }
 
 static long long ws_key(int K, int np, int prec) { return ((long long)K << 40) | ((long long)np << 8) | prec; }
 
-static int choose_k(const dec_mg& mg, int nrhs) {
+static int choose_k(const dec_mg& mg, int nrhs, int prec) {
   int K = mg.opt.rhs_block;
   if (K <= 0) {
+    auto it = mg.tuned.find(((long long)nrhs << 2) | prec);
+    if (it != mg.tuned.end()) return it->second;
     K = 1;
     while (K < nrhs && K < 32) K <<= 1;
   }
@@ -833,6 +839,9 @@ static void enqueue_cycle(dec_mg& mg, Workspace& w, cudaStream_t s) {
   DEC_CHECK_LAUNCH();
 }
 
+// Vectors a smoothing sweep reads or writes once: Jacobi b, x, out; Chebyshev b, x, d (r/w), out.
+static int prm_vectors(int smoother) { return smoother == DEC_SMOOTH_JACOBI ? 3 : 5; }
+
 enum GraphKind { G_RESID = 0, G_VCYCLE = 1, G_CYCLE = 2 };
 
 template <int K>
@@ -858,6 +867,20 @@ static void dispatch(dec_mg& mg, Workspace& w, cudaStream_t s, int kind) {
   }
 }
 
+static int64_t count_kernel_nodes(cudaGraph_t g) {
+  size_t n = 0;
+  DEC_CUDA(cudaGraphGetNodes(g, nullptr, &n));
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (n) DEC_CUDA(cudaGraphGetNodes(g, nodes.data(), &n));
+  int64_t k = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    DEC_CUDA(cudaGraphNodeGetType(nd, &t));
+    if (t == cudaGraphNodeTypeKernel) ++k;
+  }
+  return k;
+}
+
 static cudaGraphExec_t capture(dec_mg& mg, Workspace& w, int kind) {
   cudaGraph_t g = nullptr;
   DEC_CUDA(cudaStreamBeginCapture(mg.cap, cudaStreamCaptureModeThreadLocal));
@@ -869,6 +892,7 @@ static cudaGraphExec_t capture(dec_mg& mg, Workspace& w, int kind) {
     throw;
   }
   DEC_CUDA(cudaStreamEndCapture(mg.cap, &g));
+  w.launches[kind] = count_kernel_nodes(g);
   cudaGraphExec_t ex = nullptr;
   cudaError_t err = cudaGraphInstantiate(&ex, g, 0);
   cudaGraphDestroy(g);
@@ -876,8 +900,7 @@ static cudaGraphExec_t capture(dec_mg& mg, Workspace& w, int kind) {
   return ex;
 }
 
-static Workspace& workspace(dec_mg& mg, int nrhs, int prec) {
-  int K = choose_k(mg, nrhs);
+static Workspace& workspace_k(dec_mg& mg, int nrhs, int prec, int K) {
   int np = (nrhs + K - 1) / K;
   long long key = ws_key(K, np, prec);
   auto it = mg.ws.find(key);
@@ -894,9 +917,15 @@ static Workspace& workspace(dec_mg& mg, int nrhs, int prec) {
   w->nblocks = (int)std::min<long long>(2LL * num_sms(), ((long long)mg.lv[0].n * K + TB - 1) / TB);
   w->partial.alloc((size_t)w->nblocks * K * np);
   w->norms.alloc((size_t)K * np);
+  DEC_CUDA(cudaMemset(w->B64.p, 0, w->B64.bytes()));
+  DEC_CUDA(cudaMemset(w->U64.p, 0, w->U64.bytes()));
   auto& ref = *w;
   mg.ws[key] = std::move(w);
   return ref;
+}
+
+static Workspace& workspace(dec_mg& mg, int nrhs, int prec) {
+  return workspace_k(mg, nrhs, prec, choose_k(mg, nrhs, prec));
 }
 
 void mg_cycles(dec_mg* mg, double* u, const double* b, int nrhs, int cycles, void* stream) {
@@ -998,8 +1027,137 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
     rep->converged = conv ? 1 : 0;
     rep->max_rel_residual = worst;
     rep->seconds = ms * 1e-3;
+    // to_panels x2, sumsq + reduce, residual graph per test, V-cycle graph per step, from_panels
+    rep->launches = 2 + 2 + (int64_t)(it + 1) * w.launches[G_RESID] + (int64_t)it * w.launches[G_VCYCLE] + 1;
+    rep->rhs_block = K;
   }
   return conv ? DEC_OK : DEC_ERR_NOT_CONVERGED;
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// Profiling and autotuning
+// ---------------------------------------------------------------------------------------------
+template <class T, int K>
+static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bufs, int kernel, int level, int reps,
+                          cudaStream_t s, double* ms, double* bytes) {
+  const Level& L = mg.lv[level];
+  const int np = w.npanels;
+  const size_t nk = (size_t)L.n * K * np;
+  const double sz = sizeof(T);
+  LevelBufs<T>& B = bufs[level];
+  cudaEvent_t e0, e1;
+  DEC_CUDA(cudaEventCreate(&e0));
+  DEC_CUDA(cudaEventCreate(&e1));
+  auto launch = [&]() {
+    if (kernel == DEC_KERNEL_SWEEP) {
+      SweepPrm<T> prm{};
+      prm.mode = mg.opt.smoother == DEC_SMOOTH_JACOBI ? S_JACOBI : S_CHEBN;
+      prm.omega = (T)mg.opt.omega;
+      prm.c1 = (T)0.5;
+      prm.c2 = (T)0.25;
+      launch_sweep<T, K>(L, B.b.p, B.x.p, B.y.p, B.d.p, prm, np, s);
+    } else if (kernel == DEC_KERNEL_RESIDUAL) {
+      dim3 g(w.nblocks, np);
+      const Level& F = mg.lv[0];
+      k_residual64<T, K, 0><<<g, TB, 0, s>>>(F.n, F.W, F.col.p, F.off64.p, F.diag64.p, w.B64.p, w.U64.p, bufs[0].b.p,
+                                             w.partial.p, (size_t)F.n * K);
+    } else if (kernel == DEC_KERNEL_RESTRICT) {
+      const Level& Cl = mg.lv[level + 1];
+      dim3 gc(grid_for((long long)Cl.n * K, TB, 8), np);
+      k_restrict<T, K><<<gc, TB, 0, s>>>(L.nc, L.Wq, L.ridx.p, L.rs.p, B.x.p, bufs[level + 1].b.p, (size_t)L.n * K,
+                                         (size_t)Cl.n * K);
+    } else {
+      const Level& Cl = mg.lv[level + 1];
+      dim3 gf(grid_for((long long)L.n * K, TB, 8), np);
+      k_prolong<T, K><<<gf, TB, 0, s>>>(L.n, L.nc, L.pa.p, L.pb.p, bufs[level + 1].x.p, B.x.p, (size_t)L.n * K,
+                                        (size_t)Cl.n * K);
+    }
+  };
+  launch();  // warm-up
+  DEC_CUDA(cudaEventRecord(e0, s));
+  for (int r = 0; r < reps; ++r) launch();
+  DEC_CUDA(cudaEventRecord(e1, s));
+  DEC_CHECK_LAUNCH();
+  DEC_CUDA(cudaEventSynchronize(e1));
+  float t = 0;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = t / reps;
+  if (kernel == DEC_KERNEL_SWEEP) {
+    double mat = (double)L.n * (L.W * (4.0 + sz) + 2 * sz);
+    int vecs = (prm_vectors(mg.opt.smoother));
+    *bytes = mat + vecs * (double)nk * sz;
+  } else if (kernel == DEC_KERNEL_RESIDUAL) {
+    const Level& F = mg.lv[0];
+    double mat = (double)F.n * (F.W * 12.0 + 8);
+    *bytes = mat + (double)F.n * K * np * (8 + 8 + sz);
+  } else if (kernel == DEC_KERNEL_RESTRICT) {
+    const Level& Cl = mg.lv[level + 1];
+    *bytes = (double)Cl.n * (L.Wq * 4.0 + 8) + (double)nk * sz + (double)Cl.n * K * np * sz;
+  } else {
+    const Level& Cl = mg.lv[level + 1];
+    *bytes = (double)(L.n - L.nc) * 8.0 + (double)Cl.n * K * np * sz + 2.0 * nk * sz;
+  }
+}
+
+template <int K>
+static void time_kernel_K(dec_mg& mg, Workspace& w, int kernel, int level, int reps, cudaStream_t s, double* ms,
+                          double* bytes) {
+  if (w.prec == 1) time_kernel_T<float, K>(mg, w, w.f32, kernel, level, reps, s, ms, bytes);
+  else time_kernel_T<double, K>(mg, w, w.f64, kernel, level, reps, s, ms, bytes);
+}
+
+void mg_time_kernel(dec_mg* mg, int kernel, int level, int nrhs, int reps, void* stream, double* ms, double* bytes) {
+  require(mg != nullptr && ms != nullptr && bytes != nullptr, "multigrid: null argument");
+  require(kernel >= 0 && kernel <= 3, "multigrid: unknown kernel");
+  require(level >= 0 && level < (int)mg->lv.size() - (kernel >= 2 ? 1 : 0), "multigrid: level out of range");
+  require(reps >= 1 && nrhs >= 1, "multigrid: reps and nrhs must be positive");
+  Workspace& w = workspace(*mg, nrhs, mg->opt.precision);
+  cudaStream_t s = as_stream(stream);
+  switch (w.K) {
+#define DEC_K(KK) \
+  case KK: time_kernel_K<KK>(*mg, w, kernel, level, reps, s, ms, bytes); break;
+    DEC_K(1) DEC_K(2) DEC_K(4) DEC_K(8) DEC_K(16) DEC_K(32)
+#undef DEC_K
+  }
+}
+
+int mg_autotune(dec_mg* mg, int nrhs, int reps, void* stream) {
+  require(mg != nullptr && nrhs >= 1 && reps >= 1, "multigrid: bad autotune arguments");
+  cudaStream_t s = as_stream(stream);
+  const int prec = mg->opt.precision;
+  int best = 0;
+  double best_t = 1e300;
+  for (int K = 1; K <= 32; K <<= 1) {
+    if (K > 1 && (K / 2) >= nrhs) break;  // wider panels would only add padding
+    Workspace& w = workspace_k(*mg, nrhs, prec, K);
+    if (!w.graph[G_VCYCLE]) w.graph[G_VCYCLE] = capture(*mg, w, G_VCYCLE);
+    cudaEvent_t e0, e1;
+    DEC_CUDA(cudaEventCreate(&e0));
+    DEC_CUDA(cudaEventCreate(&e1));
+    DEC_CUDA(cudaGraphLaunch(w.graph[G_VCYCLE], s));
+    DEC_CUDA(cudaEventRecord(e0, s));
+    for (int r = 0; r < reps; ++r) DEC_CUDA(cudaGraphLaunch(w.graph[G_VCYCLE], s));
+    DEC_CUDA(cudaEventRecord(e1, s));
+    DEC_CUDA(cudaEventSynchronize(e1));
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (t < best_t) {
+      best_t = t;
+      best = K;
+    }
+  }
+  // keep only the chosen workspace for this (nrhs, precision)
+  for (int K = 1; K <= 32; K <<= 1) {
+    if (K == best) continue;
+    int np = (nrhs + K - 1) / K;
+    mg->ws.erase(ws_key(K, np, prec));
+  }
+  mg->tuned[((long long)nrhs << 2) | prec] = best;
+  return best;
+}
 }  // namespace decb

@@ -155,6 +155,8 @@ typedef struct dec_solve_report {
   int32_t converged;       /* all right-hand sides reached rtol */
   double max_rel_residual; /* max_j ||b_j - A u_j|| / ||b_j|| at exit (FP64) */
   double seconds;          /* device time of the solve */
+  int64_t launches;        /* kernels launched by the solve */
+  int32_t rhs_block;       /* panel width used */
 } dec_solve_report;
 
 void dec_mg_default_options(dec_mg_options* o);
@@ -172,6 +174,23 @@ dec_status dec_mg_solve(dec_mg* mg, double* u, const double* b, int32_t nrhs, do
 /* Same solve with host u / b (pinned or pageable); copies are part of the call. */
 dec_status dec_mg_solve_host(dec_mg* mg, double* u_host, const double* b_host, int32_t nrhs, double rtol,
                              int32_t max_iters, dec_solve_report* report, void* stream);
+
+/* ---- profiling (no counterpart in the reference; its benchmarks print timings only,
+ *      test/Benchmarks.jl:128-140) ------------------------------------------------------ */
+typedef enum dec_mg_kernel {
+  DEC_KERNEL_SWEEP = 0,     /* Chebyshev / Jacobi smoothing sweep */
+  DEC_KERNEL_RESIDUAL = 1,  /* FP64 residual with norms */
+  DEC_KERNEL_RESTRICT = 2,
+  DEC_KERNEL_PROLONG = 3
+} dec_mg_kernel;
+/* Times `reps` back-to-back launches of one V-cycle kernel at `level`, configured as in a solve
+ * of `nrhs` right-hand sides, with CUDA events on `stream`.  Returns the mean milliseconds per
+ * launch and the algorithmic bytes one launch moves (every array read or written once). */
+dec_status dec_mg_time_kernel(dec_mg* mg, int32_t kernel, int32_t level, int32_t nrhs, int32_t reps,
+                              void* stream, double* ms_per_launch, double* bytes_per_launch);
+/* Times each candidate panel width on one V-cycle and keeps the fastest for `nrhs` right-hand
+ * sides (used when rhs_block = 0).  Returns the chosen width. */
+dec_status dec_mg_autotune(dec_mg* mg, int32_t nrhs, int32_t reps, void* stream, int32_t* rhs_block);
 
 #ifdef __cplusplus
 }

@@ -525,6 +525,18 @@ void spmv(const CSC& a, const double* x, double* y) {
   }
 }
 
+void apply(const CSC& A, const CSC* At, const double* x, double* y) {
+  if (At == nullptr || g_threads <= 1) {
+    spmv(A, x, y);
+    return;
+  }
+  parallel_for(A.m, [&](int i) {  // row i of A = column i of Aᵀ
+    double s = 0.0;
+    for (int p = At->colptr[i]; p < At->colptr[i + 1]; ++p) s += At->nzval[p] * x[At->rowval[p]];
+    y[i] = s;
+  });
+}
+
 void spmv_t(const CSC& a, const double* x, double* y) {
   for (int j = 0; j < a.n; ++j) {
     double s = 0.0;
@@ -1042,18 +1054,21 @@ MGData build_mg(const Mesh& coarse, int levels, int center, double shift, double
   md.ops = std::move(ops);
   md.meshes = std::move(meshes);
   md.steps.assign(levels + 1, steps);
+  for (auto& a : md.ops) md.ops_t.push_back(transpose(a));
+  for (auto& a : md.rs) md.rs_t.push_back(transpose(a));
+  for (auto& a : md.ps) md.ps_t.push_back(transpose(a));
   return md;
 }
 
 // Krylov.jl cg(A, b, x0; itmax) with M = I, atol = rtol = sqrt(eps): warm start solves for
 // Δx from r0 = b - A x0 and returns x0 + Δx.
 std::vector<double> krylov_cg(const CSC& A, const std::vector<double>& b,
-                              const std::vector<double>& x0, int itmax) {
+                              const std::vector<double>& x0, int itmax, const CSC* At) {
   const int n = A.m;
   const double eps = std::numeric_limits<double>::epsilon();
   const double atol = std::sqrt(eps), rtol = std::sqrt(eps);
   std::vector<double> x(n, 0.0), r(n), p(n), Ap(n);
-  spmv(A, x0.data(), r.data());
+  apply(A, At, x0.data(), r.data());
   for (int i = 0; i < n; ++i) r[i] = b[i] - r[i];
   p = r;
   double gamma = 0;
@@ -1067,7 +1082,7 @@ std::vector<double> krylov_cg(const CSC& A, const std::vector<double>& b,
   int iter = 0;
   bool zero_curvature = false;
   while (!(solved || iter >= itmax || zero_curvature)) {
-    spmv(A, p.data(), Ap.data());
+    apply(A, At, p.data(), Ap.data());
     double pAp = 0;
     for (int i = 0; i < n; ++i) pAp += p[i] * Ap[i];
     if (pAp <= eps * pNorm2 && std::fabs(pAp) <= eps * pNorm2) {
@@ -1097,21 +1112,22 @@ std::vector<double> krylov_cg(const CSC& A, const std::vector<double>& b,
 std::vector<double> mu_cycle(const std::vector<double>& u0, const std::vector<double>& b,
                              const MGData& md, int lvl, int mu) {
   const CSC& A = md.ops[lvl];
+  const CSC* At = md.ops_t.empty() ? nullptr : &md.ops_t[lvl];
   const int steps = md.steps[lvl];
-  std::vector<double> u = steps == 0 ? u0 : krylov_cg(A, b, u0, steps);
+  std::vector<double> u = steps == 0 ? u0 : krylov_cg(A, b, u0, steps, At);
   if (lvl >= (int)md.ops.size() - 1) return u;
   const CSC& R = md.rs[lvl];
   const CSC& P = md.ps[lvl];  // transpose(S): P*z = S' z
   std::vector<double> Au(A.m), rf(A.m), rc(R.m);
-  spmv(A, u.data(), Au.data());
+  apply(A, At, u.data(), Au.data());
   for (int i = 0; i < A.m; ++i) rf[i] = b[i] - Au[i];
-  spmv(R, rf.data(), rc.data());
+  apply(R, md.rs_t.empty() ? nullptr : &md.rs_t[lvl], rf.data(), rc.data());
   std::vector<double> z = mu_cycle(std::vector<double>(rc.size(), 0.0), rc, md, lvl + 1, mu);
   if (mu > 1) z = mu_cycle(z, rc, md, lvl + 1, mu - 1);
   std::vector<double> pz(A.m);
-  spmv(P, z.data(), pz.data());
+  apply(P, md.ps_t.empty() ? nullptr : &md.ps_t[lvl], z.data(), pz.data());
   for (int i = 0; i < A.m; ++i) u[i] = u[i] + pz[i];
-  return steps == 0 ? u : krylov_cg(A, b, u, steps);
+  return steps == 0 ? u : krylov_cg(A, b, u, steps, At);
 }
 
 std::vector<double> mu_cycles(std::vector<double> u, const std::vector<double>& b, const MGData& md,

@@ -147,6 +147,7 @@ Mesh topo_to_mesh(const Topo& t, const std::vector<double>& pts);    // :49-64
 
 struct MGData {  // MultigridData, :538-553 (finest level first)
   std::vector<CSC> ops, rs, ps;
+  std::vector<CSC> ops_t, rs_t, ps_t;  // transposes: row access for the threaded CPU baseline
   std::vector<int> steps;
   std::vector<Mesh> meshes;  // finest first, orientations as dualize left them
 };
@@ -156,7 +157,9 @@ MGData build_mg(const Mesh& coarse, int levels, int center, double shift, double
 
 // Krylov.jl cg(A, b, x0; itmax) (warm start, atol = rtol = sqrt(eps)).
 std::vector<double> krylov_cg(const CSC& A, const std::vector<double>& b,
-                              const std::vector<double>& x0, int itmax);
+                              const std::vector<double>& x0, int itmax, const CSC* At = nullptr);
+// y = A x; with more than one host thread and At (the CSC of Aᵀ) given, rows run in parallel.
+void apply(const CSC& A, const CSC* At, const double* x, double* y);
 std::vector<double> mu_cycle(const std::vector<double>& u, const std::vector<double>& b,
                              const MGData& md, int lvl, int mu);  // :857-872
 std::vector<double> mu_cycles(std::vector<double> u, const std::vector<double>& b,
