@@ -242,6 +242,16 @@ class Operator:
     def __matmul__(self, x):
         return self.apply(x)
 
+    def residual_norms(self, x, b):
+        """(‖b_j - Op x_j‖, ‖b_j‖) per right-hand side; x, b float64 CUDA tensors (n,) or (nrhs, n)."""
+        nrhs = 1 if b.dim() == 1 else b.shape[0]
+        r = np.empty(nrhs)
+        bn = np.empty(nrhs)
+        check(lib().dec_op_residual_norms(self._h, _ptr(x), _ptr(b), nrhs,
+                                          r.ctypes.data_as(C.POINTER(C.c_double)),
+                                          bn.ctypes.data_as(C.POINTER(C.c_double)), _stream()))
+        return r, bn
+
     def csr(self):
         """(indptr, indices, data, shape) of the operator, exported to the host."""
         nnz = C.c_int64()

@@ -144,6 +144,63 @@ __global__ void k_inv_sign(int n, const double* __restrict__ a, double sign, dou
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = (1 / a[i]) * sign;
 }
 
+// Per-block partial sums of (b - A x)² and b² for right-hand side j = blockIdx.y (column-major
+// x, b), A the FP64 ELL operator.  partial layout: [j][block] for the residual, then the same
+// for b.
+__global__ void __launch_bounds__(kResidThreads) k_resid_partials(int n, int W, const int32_t* __restrict__ col,
+                                                                  const double* __restrict__ val,
+                                                                  const double* __restrict__ x,
+                                                                  const double* __restrict__ b,
+                                                                  double* __restrict__ partial, int nrhs) {
+  const int j = blockIdx.y;
+  const double* xj = x + (size_t)j * n;
+  const double* bj = b + (size_t)j * n;
+  double sr = 0.0, sb = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int q = 0; q < W; ++q) {
+      int c = col[(size_t)i * W + q];
+      if (c >= 0) s += val[(size_t)i * W + q] * xj[c];
+    }
+    double r = bj[i] - s;
+    sr += r * r;
+    sb += bj[i] * bj[i];
+  }
+  __shared__ double shr[kResidThreads], shb[kResidThreads];
+  shr[threadIdx.x] = sr;
+  shb[threadIdx.x] = sb;
+  __syncthreads();
+  for (int st = kResidThreads / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) {
+      shr[threadIdx.x] += shr[threadIdx.x + st];
+      shb[threadIdx.x] += shb[threadIdx.x + st];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[(size_t)j * gridDim.x + blockIdx.x] = shr[0];
+    partial[(size_t)(nrhs + j) * gridDim.x + blockIdx.x] = shb[0];
+  }
+}
+
+// dnorms[j] = sqrt(Σ partial residual), dnorms[nrhs + j] = sqrt(Σ partial b), in block order.
+__global__ void k_resid_finish(int nblocks, int nrhs, const double* __restrict__ partial, double* __restrict__ dnorms) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 2 * nrhs) return;
+  double s = 0.0;
+  for (int k = 0; k < nblocks; ++k) s += partial[(size_t)q * nblocks + k];
+  dnorms[q] = sqrt(s);
+}
+
+void launch_residual_norms(const dec_op& op, const double* x, const double* b, int nrhs, double* partial,
+                           double* dnorms, cudaStream_t s) {
+  const Mesh& m = *op.m;
+  dim3 g(kResidBlocks, nrhs);
+  k_resid_partials<<<g, kResidThreads, 0, s>>>(m.nv, op.W, op.col.p, op.val64.p, x, b, partial, nrhs);
+  k_resid_finish<<<(2 * nrhs + 127) / 128, 128, 0, s>>>(kResidBlocks, nrhs, partial, dnorms);
+  DEC_CHECK_LAUNCH();
+}
+
 // ---------------------------------------------------------------------------------------------
 
 static const DArr<double>& star_of(const Mesh& m, int k) {
@@ -347,4 +404,20 @@ void hodge_diag_impl(const dec_mesh* mh, int k, int inverse, dec_dtype dt, void*
     DEC_CHECK_LAUNCH();
   }
   DEC_CUDA(cudaStreamSynchronize(s));  // tmp is released on return
+}
+
+void op_residual_norms_impl(dec_op* op, const double* x, const double* b, int nrhs, double* norms, double* bnorms,
+                            void* stream) {
+  require(op != nullptr && x != nullptr && b != nullptr && norms != nullptr, "residual norms: null argument");
+  require(op->kind == DEC_OP_LAPLACE0 || op->kind == DEC_OP_HELMHOLTZ0,
+          "residual norms: the operator must be the Laplacian or a Helmholtz operator");
+  require(nrhs >= 1 && nrhs <= 65535, "residual norms: nrhs must be in [1, 65535]");
+  cudaStream_t s = as_stream(stream);
+  DArr<double> partial((size_t)2 * kResidBlocks * nrhs), dn((size_t)2 * nrhs);
+  launch_residual_norms(*op, x, b, nrhs, partial.p, dn.p, s);
+  std::vector<double> h((size_t)2 * nrhs);
+  DEC_CUDA(cudaMemcpyAsync(h.data(), dn.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  DEC_CUDA(cudaStreamSynchronize(s));
+  std::copy(h.begin(), h.begin() + nrhs, norms);
+  if (bnorms) std::copy(h.begin() + nrhs, h.end(), bnorms);
 }

@@ -21,4 +21,13 @@ void hodge_into(const Mesh& m, int k, bool inverse, DArr<double>& out);
 void assemble_laplacian(const Mesh& m, double shift, int& W, DArr<int32_t>& col, DArr<double>& val);
 template <class T>
 void cast_array(const DArr<double>& a, DArr<T>& b);
+
+// Blocks of the residual-norm reduction (each block reduces a strided set of rows).
+constexpr int kResidBlocks = 256;
+constexpr int kResidThreads = 256;
+// Residual-norm kernels on caller-provided scratch: partial holds 2 * kResidBlocks * nrhs doubles,
+// dnorms 2 * nrhs.  Every partial slot is written before it is read, so the scratch needs no
+// clearing between calls.
+void launch_residual_norms(const dec_op& op, const double* x, const double* b, int nrhs, double* partial,
+                           double* dnorms, cudaStream_t s);
 }  // namespace decb

@@ -122,6 +122,13 @@ dec_status dec_op_create(dec_mesh* m, int32_t kind, double shift, dec_dtype dtyp
 dec_status dec_op_shape(const dec_op* op, int64_t* rows, int64_t* cols);
 /* y = alpha * Op x + beta * y  (beta == 0 overwrites y). */
 dec_status dec_op_apply(dec_op* op, const void* x, void* y, double alpha, double beta, void* stream);
+/* Residual norms ||b_j - Op x_j||_2 and ||b_j||_2 for nrhs right-hand sides (x, b: device FP64,
+ * column-major rows x nrhs; norms, bnorms: host arrays of nrhs doubles, bnorms may be NULL): the
+ * convergence test of the reference's multigrid tests, norm(L*u - b) / norm(b)
+ * (test/Multigrid.jl:67).  Square FP64 operators only.  Uses device scratch for the per-block
+ * partial sums (a deterministic two-stage reduction), allocated per call. */
+dec_status dec_op_residual_norms(dec_op* op, const double* x, const double* b, int32_t nrhs, double* norms,
+                                 double* bnorms, void* stream);
 /* CSR export to host, two-phase: call with rowptr == NULL to get nnz. */
 dec_status dec_op_export_csr(const dec_op* op, int64_t* nnz, int32_t* rowptr, int32_t* colind, double* val);
 dec_status dec_op_destroy(dec_op* op);

@@ -232,3 +232,22 @@ def test_one_based_description_matches(O, dec, cases):
     g1 = dec.Mesh(m.points, m.ev0 + 1, m.ev1 + 1, m.te0 + 1, m.te1 + 1, m.te2 + 1, m.edge_orientation,
                   m.tri_orientation, center="barycenter", index_base=1)
     np.testing.assert_array_equal(g1.geometry("dual_area"), g.geometry("dual_area"))
+
+
+@pytest.mark.parametrize("name", ["grid128_bary", "ico3_circum"])
+def test_residual_norms(O, dec, cases, name):
+    """‖b_j - A x_j‖ and ‖b_j‖ per right-hand side (the norm(L*u - b) / norm(b) test of
+    test/Multigrid.jl:67), against numpy on the oracle's operator."""
+    m, d, g = cases[name]
+    H = dec.helmholtz(g, 0.75)
+    A = csc(O.laplace_beltrami0(d)) + 0.75 * __import__("scipy.sparse", fromlist=["eye"]).eye(d.nv)
+    nrhs = 5
+    X = np.stack([uniform(40 + j, d.nv) for j in range(nrhs)])
+    B = np.stack([uniform(60 + j, d.nv) for j in range(nrhs)])
+    r, bn = H.residual_norms(cuda(X), cuda(B))
+    ref_r = np.array([np.linalg.norm(B[j] - A @ X[j]) for j in range(nrhs)])
+    ref_b = np.linalg.norm(B, axis=1)
+    np.testing.assert_allclose(r, ref_r, rtol=1e-12)
+    np.testing.assert_allclose(bn, ref_b, rtol=1e-13)
+    with pytest.raises(dec.DecError, match="Laplacian or a Helmholtz"):
+        dec.dec_differential(0, g).residual_norms(cuda(X), cuda(B))   # rejected before any device work
