@@ -65,6 +65,7 @@ SIGNATURES = {
     "dec_op_apply": (I32, [P, P, P, F64, F64, P]),
     "dec_op_export_csr": (I32, [P, PI64, P, P, P]),
     "dec_op_residual_norms": (I32, [P, P, P, I32, PF64, PF64, P]),
+    "dec_op_residual_norms_noalloc": (I32, [P, P, P, I32, PF64, PF64, P]),
     "dec_op_destroy": (I32, [P]),
     "dec_mg_default_options": (None, [C.POINTER(MGOptions)]),
     "dec_mg_create": (I32, [C.POINTER(MeshDesc), C.POINTER(MGOptions), PP]),

@@ -21,6 +21,8 @@ void op_export_csr_impl(const dec_op* op, int64_t* nnz, int32_t* rowptr, int32_t
 void hodge_diag_impl(const dec_mesh* mh, int k, int inverse, dec_dtype dt, void* out, void* stream);
 void op_residual_norms_impl(dec_op* op, const double* x, const double* b, int nrhs, double* norms, double* bnorms,
                             void* stream);
+void op_residual_norms_noalloc_impl(dec_op* op, const double* x, const double* b, int nrhs, double* norms,
+                                    double* bnorms, void* stream);
 
 namespace {
 thread_local std::string g_err;
@@ -165,6 +167,11 @@ dec_status dec_op_apply(dec_op* op, const void* x, void* y, double alpha, double
 dec_status dec_op_residual_norms(dec_op* op, const double* x, const double* b, int32_t nrhs, double* norms,
                                  double* bnorms, void* stream) {
   return guard([&] { op_residual_norms_impl(op, x, b, nrhs, norms, bnorms, stream); });
+}
+
+dec_status dec_op_residual_norms_noalloc(dec_op* op, const double* x, const double* b, int32_t nrhs,
+                                         double* norms, double* bnorms, void* stream) {
+  return guard([&] { op_residual_norms_noalloc_impl(op, x, b, nrhs, norms, bnorms, stream); });
 }
 
 dec_status dec_op_export_csr(const dec_op* op, int64_t* nnz, int32_t* rowptr, int32_t* colind, double* val) {

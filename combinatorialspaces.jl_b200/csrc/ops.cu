@@ -7,6 +7,7 @@
 // increasing column order, the order of the reference's CSC SpMV, and this file is compiled
 // without FMA contraction, so results reproduce the reference CPU arithmetic.
 #include <algorithm>
+#include <mutex>
 
 #include "mesh.cuh"
 #include "ops.cuh"
@@ -420,4 +421,46 @@ void op_residual_norms_impl(dec_op* op, const double* x, const double* b, int nr
   DEC_CUDA(cudaStreamSynchronize(s));
   std::copy(h.begin(), h.begin() + nrhs, norms);
   if (bnorms) std::copy(h.begin() + nrhs, h.end(), bnorms);
+}
+
+// ---- allocation-free residual norms ------------------------------------------------------------
+//
+// Scratch for callers that cannot allocate: the partial sums (2 * kResidBlocks per right-hand
+// side) followed by the 2 * nrhs norms, in a file-scope device array.  Every device that loads
+// the library holds it until the process exits.  In host code `g_resid_scratch` only names the
+// symbol; its device address is looked up once per device with that device current.
+static __device__ __align__(256) double
+    g_resid_scratch[2 * kResidBlocks * DEC_RESIDUAL_NOALLOC_MAX_RHS + 2 * DEC_RESIDUAL_NOALLOC_MAX_RHS];
+
+static double* resid_scratch_for_current_device() {
+  constexpr int kMaxDevices = 64;
+  static std::mutex mu;
+  static double* ptrs[kMaxDevices] = {};
+  int dev = 0;
+  DEC_CUDA(cudaGetDevice(&dev));
+  require(dev >= 0 && dev < kMaxDevices, "residual norms (no-alloc): device ordinal out of range");
+  std::lock_guard<std::mutex> lock(mu);
+  if (ptrs[dev] == nullptr) {
+    void* p = nullptr;
+    DEC_CUDA(cudaGetSymbolAddress(&p, g_resid_scratch));
+    ptrs[dev] = static_cast<double*>(p);
+  }
+  return ptrs[dev];
+}
+
+void op_residual_norms_noalloc_impl(dec_op* op, const double* x, const double* b, int nrhs, double* norms,
+                                    double* bnorms, void* stream) {
+  require(op != nullptr && x != nullptr && b != nullptr && norms != nullptr, "residual norms (no-alloc): null argument");
+  require(op->kind == DEC_OP_LAPLACE0 || op->kind == DEC_OP_HELMHOLTZ0,
+          "residual norms (no-alloc): the operator must be the Laplacian or a Helmholtz operator");
+  require(nrhs >= 1 && nrhs <= DEC_RESIDUAL_NOALLOC_MAX_RHS,
+          "residual norms (no-alloc): nrhs must be in [1, " + std::to_string(DEC_RESIDUAL_NOALLOC_MAX_RHS) +
+              "], the size of its static scratch");
+  cudaStream_t s = as_stream(stream);
+  double* partial = resid_scratch_for_current_device();
+  double* dn = partial + (size_t)2 * kResidBlocks * DEC_RESIDUAL_NOALLOC_MAX_RHS;
+  launch_residual_norms(*op, x, b, nrhs, partial, dn, s);
+  DEC_CUDA(cudaMemcpyAsync(norms, dn, (size_t)nrhs * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (bnorms) DEC_CUDA(cudaMemcpyAsync(bnorms, dn + nrhs, (size_t)nrhs * sizeof(double), cudaMemcpyDeviceToHost, s));
+  DEC_CUDA(cudaStreamSynchronize(s));
 }

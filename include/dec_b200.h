@@ -129,6 +129,22 @@ dec_status dec_op_apply(dec_op* op, const void* x, void* y, double alpha, double
  * partial sums (a deterministic two-stage reduction), allocated per call. */
 dec_status dec_op_residual_norms(dec_op* op, const double* x, const double* b, int32_t nrhs, double* norms,
                                  double* bnorms, void* stream);
+/* Allocation-free variant of dec_op_residual_norms (no counterpart in the reference).
+ * For callers that cannot allocate device memory at the point of the call: an application
+ * that hands the device a fixed memory budget up front, a real-time loop that must not enter
+ * the allocator, or code running while another thread captures a CUDA graph.  It calls no
+ * cudaMalloc / cudaFree: its scratch (the per-block partial sums) is a file-scope device array
+ * of DEC_RESIDUAL_NOALLOC_MAX_RHS * 2 * 256 + 2 * DEC_RESIDUAL_NOALLOC_MAX_RHS doubles (about
+ * 264 KiB) that every GPU which loads the library holds until the process exits.
+ *  - nrhs above DEC_RESIDUAL_NOALLOC_MAX_RHS is rejected with DEC_ERR_INVALID_ARG.
+ *  - The first call on a device looks up the array's device address (cudaGetSymbolAddress);
+ *    make that first call before any stream capture on that device.
+ *  - All calls share the one array, which keeps the last call's contents (every slot a call
+ *    reads it has written first, so nothing needs clearing): calls that overlap on the GPU
+ *    (concurrent streams or host threads) race. */
+#define DEC_RESIDUAL_NOALLOC_MAX_RHS 64
+dec_status dec_op_residual_norms_noalloc(dec_op* op, const double* x, const double* b, int32_t nrhs,
+                                         double* norms, double* bnorms, void* stream);
 /* CSR export to host, two-phase: call with rowptr == NULL to get nnz. */
 dec_status dec_op_export_csr(const dec_op* op, int64_t* nnz, int32_t* rowptr, int32_t* colind, double* val);
 dec_status dec_op_destroy(dec_op* op);
