@@ -413,16 +413,18 @@ class MultigridData:
             check(st)
         return u, rep
 
-    def solve_host(self, u, b, rtol=1e-8, max_iters=100):
+    def solve_host(self, u, b, rtol=1e-8, max_iters=100, use_initial_guess=True):
         """Same solve on host float64 arrays ((n,) or (nrhs, n); numpy or pinned torch CPU tensors);
-        the host<->device copies are part of the call."""
+        the host<->device copies are part of the call.  use_initial_guess=False starts from zero
+        and treats u as output only."""
         nrhs = 1 if b.ndim == 1 else b.shape[0]
         rep = _capi.SolveReport()
 
         def hp(a):
             return C.c_void_p(a.data_ptr()) if hasattr(a, "data_ptr") else a.ctypes.data_as(C.c_void_p)
 
-        st = lib().dec_mg_solve_host(self._h, hp(u), hp(b), nrhs, rtol, max_iters, C.byref(rep), _stream())
+        st = lib().dec_mg_solve_host(self._h, hp(u), hp(b), nrhs, rtol, max_iters, int(use_initial_guess),
+                                     C.byref(rep), _stream())
         if st not in (_capi.DEC_OK, 4):
             check(st)
         return u, rep

@@ -30,7 +30,8 @@ class MGOptions(C.Structure):
     _fields_ = [("levels", C.c_int32), ("center", C.c_int32), ("project_radius", C.c_double),
                 ("shift", C.c_double), ("smoother", C.c_int32), ("pre", C.c_int32), ("post", C.c_int32),
                 ("omega", C.c_double), ("cheb_ratio", C.c_double), ("coarse_solver", C.c_int32),
-                ("precision", C.c_int32), ("rhs_block", C.c_int32), ("mu", C.c_int32)]
+                ("precision", C.c_int32), ("rhs_block", C.c_int32), ("mu", C.c_int32),
+                ("inner_cycles", C.c_int32), ("reorder", C.c_int32), ("coarse_max", C.c_int32)]
 
 
 class SolveReport(C.Structure):
@@ -75,7 +76,7 @@ SIGNATURES = {
     "dec_mg_level_op": (I32, [P, I32, PP]),
     "dec_mg_cycles": (I32, [P, P, P, I32, I32, P]),
     "dec_mg_solve": (I32, [P, P, P, I32, F64, I32, C.POINTER(SolveReport), P]),
-    "dec_mg_solve_host": (I32, [P, P, P, I32, F64, I32, C.POINTER(SolveReport), P]),
+    "dec_mg_solve_host": (I32, [P, P, P, I32, F64, I32, I32, C.POINTER(SolveReport), P]),
     "dec_mg_time_kernel": (I32, [P, I32, I32, I32, I32, P, PF64, PF64]),
     "dec_mg_autotune": (I32, [P, I32, I32, P, C.POINTER(C.c_int32)]),
 }

@@ -217,14 +217,15 @@ dec_status dec_mg_cycles(dec_mg* mg, double* u, const double* b, int32_t nrhs, i
 dec_status dec_mg_solve(dec_mg* mg, double* u, const double* b, int32_t nrhs, double rtol, int32_t max_iters,
                         dec_solve_report* rep, void* stream) {
   dec_status st = DEC_OK;
-  dec_status g = guard([&] { st = decb::mg_solve(mg, u, b, nrhs, rtol, max_iters, rep, stream, false); });
+  dec_status g = guard([&] { st = decb::mg_solve(mg, u, b, nrhs, rtol, max_iters, rep, stream, false, true); });
   return g != DEC_OK ? g : st;
 }
 
 dec_status dec_mg_solve_host(dec_mg* mg, double* u, const double* b, int32_t nrhs, double rtol, int32_t max_iters,
-                             dec_solve_report* rep, void* stream) {
+                             int32_t use_initial_guess, dec_solve_report* rep, void* stream) {
   dec_status st = DEC_OK;
-  dec_status g = guard([&] { st = decb::mg_solve(mg, u, b, nrhs, rtol, max_iters, rep, stream, true); });
+  dec_status g = guard(
+      [&] { st = decb::mg_solve(mg, u, b, nrhs, rtol, max_iters, rep, stream, true, use_initial_guess != 0); });
   return g != DEC_OK ? g : st;
 }
 

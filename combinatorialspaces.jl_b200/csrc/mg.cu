@@ -9,17 +9,21 @@
 // of a component's first triangle is the DFS seed, so one flip per component at the first
 // refinement reproduces orient!'s result exactly.
 //
-// Solve layout: right-hand sides are processed in panels of K (1..32) stored row-major
-// ([panel][row][K]), so a row's K values are one contiguous 4K- or 8K-byte segment and each
-// neighbour gather of the SpMV is a coalesced segment shared by K lanes; the K lanes of a row
-// read the same matrix entries (one broadcast transaction).  A panel grid dimension processes
-// all panels in one launch, which keeps the coarse levels from being launch-bound.  The
-// smoothers are damped Jacobi or Chebyshev-Jacobi (bounds from a GPU power iteration); the
-// coarsest level is a dense FP64 solve with the precomputed inverse.  Mixed precision runs the
-// V-cycle in FP32 on the FP64 residual inside FP64 iterative refinement.  Each refinement step
-// (update, residual, norms, V-cycle) is one CUDA graph.
+// Solve layout.  Each level is stored internally in a locality order (vertices sorted along a
+// 3D Morton curve), so a row's neighbours sit close in memory and the gathers of the SpMV hit
+// L2; rows keep the reference's column order, so sums are unchanged, and only the finest
+// level's entry / exit kernels apply the permutation.  Right-hand sides are processed in
+// panels of K (1..32) stored [panel][row][K]: a row's K values are contiguous, each lane moves
+// V of them with one vector load (V = 4 FP32 / 2 FP64 values), and the K/V lanes of a row read
+// the same matrix entries (one broadcast transaction).  A panel grid dimension processes all
+// panels in one launch.  Smoothers: damped Jacobi or Chebyshev-Jacobi (bounds from a GPU power
+// iteration); coarsest level: dense FP64 solve with the precomputed inverse.  Mixed precision
+// runs the V-cycles in FP32 on the FP64 residual inside FP64 iterative refinement; the residual
+// step and the V-cycle step are each one CUDA graph.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <numeric>
@@ -150,6 +154,42 @@ static std::unique_ptr<dec_mesh> make_mesh(const HostLevel& h, int center) {
   return m;
 }
 
+// Locality order: vertices sorted by the 3D Morton code of their (bounding-box normalised)
+// position, 21 bits per axis.  Returns perm (new -> old).
+static uint64_t spread21(uint64_t x) {
+  x &= 0x1fffff;
+  x = (x | x << 32) & 0x1f00000000ffffull;
+  x = (x | x << 16) & 0x1f0000ff0000ffull;
+  x = (x | x << 8) & 0x100f00f00f00f00full;
+  x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+  x = (x | x << 2) & 0x1249249249249249ull;
+  return x;
+}
+
+static std::vector<int32_t> morton_order(const std::vector<double>& pts, int n) {
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], pts[3 * (size_t)i + k]);
+      hi[k] = std::max(hi[k], pts[3 * (size_t)i + k]);
+    }
+  std::vector<uint64_t> key(n);
+  const double q = (double)((1 << 21) - 1);
+  for (int i = 0; i < n; ++i) {
+    uint64_t c[3];
+    for (int k = 0; k < 3; ++k) {
+      double span = hi[k] - lo[k];
+      double t = span > 0 ? (pts[3 * (size_t)i + k] - lo[k]) / span : 0.0;
+      c[k] = (uint64_t)std::llround(t * q);
+    }
+    key[i] = spread21(c[0]) | (spread21(c[1]) << 1) | (spread21(c[2]) << 2);
+  }
+  std::vector<int32_t> perm(n);
+  std::iota(perm.begin(), perm.end(), 0);
+  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return key[a] < key[b]; });
+  return perm;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Kernels
 // ---------------------------------------------------------------------------------------------
@@ -158,13 +198,80 @@ enum SweepMode { S_RESID = 0, S_JACOBI = 1, S_CHEB0 = 2, S_CHEBN = 3 };
 template <class T>
 struct SweepPrm {
   int mode;
-  int zero_x;  // x is known to be zero: A x is skipped
-  T omega;     // Jacobi
-  T inv_theta; // Chebyshev first step
-  T c1, c2;    // Chebyshev recurrence
+  int zero_x;   // x is known to be zero: A x is skipped
+  int write_d;  // Chebyshev: store the direction (not needed after the last sweep)
+  int d_is_x;   // Chebyshev: the direction equals x (first step from zero), so d is not read
+  T omega;      // Jacobi
+  T inv_theta;  // Chebyshev first step
+  T c1, c2;     // Chebyshev recurrence
 };
 
 constexpr int TB = 256;
+
+// Programmatic dependent launch: every kernel of a cycle is launched with the
+// programmatic-serialization attribute, waits for its predecessor's results with
+// griddepcontrol.wait before touching memory, and lets its successor start launching at once.
+// The launches of a cycle then overlap the tails of the kernels before them.
+__device__ __forceinline__ void pdl_enter() {
+#if __CUDA_ARCH__ >= 900
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
+#endif
+}
+
+// The attribute is off unless DEC_B200_PDL=1: measured on B200, the early launch of dependents
+// overlaps small kernels' launch latency but takes SM slots from the large finest-level kernels,
+// and the whole solve ran about 4% slower with it.
+static bool pdl_enabled() {
+  static const bool on = [] {
+    const char* v = std::getenv("DEC_B200_PDL");
+    return v && v[0] == '1';
+  }();
+  return on;
+}
+
+template <class... KArgs, class... Args>
+static void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  DEC_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
+}
+
+template <class T, int V> struct VecT;
+template <> struct VecT<float, 1> { using t = float; };
+template <> struct VecT<float, 2> { using t = float2; };
+template <> struct VecT<float, 4> { using t = float4; };
+template <> struct VecT<double, 1> { using t = double; };
+template <> struct VecT<double, 2> { using t = double2; };
+
+template <class T, int V>
+__device__ __forceinline__ void ldv(const T* p, T (&r)[V]) {
+  using VT = typename VecT<T, V>::t;
+  VT t = *reinterpret_cast<const VT*>(p);
+  memcpy(r, &t, sizeof(VT));
+}
+template <class T, int V>
+__device__ __forceinline__ void stv(T* p, const T (&r)[V]) {
+  using VT = typename VecT<T, V>::t;
+  VT t;
+  memcpy(&t, r, sizeof(VT));
+  *reinterpret_cast<VT*>(p) = t;
+}
+
+template <class T, int K>
+struct Lanes {
+  static constexpr int V = std::is_same<T, float>::value ? (K >= 4 ? 4 : K) : (K >= 2 ? 2 : 1);
+  static constexpr int LPR = K / V;        // lanes per row
+  static constexpr int RPB = TB / LPR;     // rows per block
+};
 
 // One smoothing sweep / residual on all panels: r = b - A x, then
 //   S_RESID : out = r
@@ -177,171 +284,270 @@ __global__ void __launch_bounds__(TB) k_sweep(int n, int Wr, const int32_t* __re
                                               const T* __restrict__ dinv, const T* __restrict__ b,
                                               const T* __restrict__ x, T* __restrict__ out, T* __restrict__ d,
                                               SweepPrm<T> prm, size_t pstride) {
+  using Ln = Lanes<T, K>;
+  pdl_enter();
+  constexpr int V = Ln::V;
   const int w = W > 0 ? W : Wr;
-  const int k = threadIdx.x % K;
-  const size_t po = (size_t)blockIdx.y * pstride;
-  const int rows_per_grid = gridDim.x * (TB / K);
-  for (int i = blockIdx.x * (TB / K) + threadIdx.x / K; i < n; i += rows_per_grid) {
-    const size_t ik = po + (size_t)i * K + k;
-    T r = b[ik];
-    T xi = T(0);
+  const int lane = threadIdx.x % Ln::LPR;
+  const size_t po = (size_t)blockIdx.y * pstride + (size_t)lane * V;
+  for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < n; i += gridDim.x * Ln::RPB) {
+    const size_t ik = po + (size_t)i * K;
+    T r[V], xi[V];
+    ldv<T, V>(b + ik, r);
     if (!prm.zero_x) {
-      xi = x[ik];
-      T acc = diag[i] * xi;
+      ldv<T, V>(x + ik, xi);
+      const T dg = diag[i];
+      T acc[V];
+#pragma unroll
+      for (int q = 0; q < V; ++q) acc[q] = dg * xi[q];
       const int32_t* c = col + (size_t)i * w;
       const T* v = off + (size_t)i * w;
+      if constexpr (W > 0) {
+        int cs[W];
+        T vs[W];
 #pragma unroll
-      for (int s = 0; s < (W > 0 ? W : 1); ++s) {
-        if (W > 0) acc += v[s] * x[po + (size_t)c[s] * K + k];
+        for (int s = 0; s < W; ++s) {
+          cs[s] = c[s];
+          vs[s] = v[s];
+        }
+#pragma unroll
+        for (int s = 0; s < W; ++s) {
+          T nb[V];
+          ldv<T, V>(x + po + (size_t)cs[s] * K, nb);
+#pragma unroll
+          for (int q = 0; q < V; ++q) acc[q] += vs[s] * nb[q];
+        }
+      } else {
+        for (int s = 0; s < w; ++s) {
+          T nb[V];
+          ldv<T, V>(x + po + (size_t)c[s] * K, nb);
+          const T vv = v[s];
+#pragma unroll
+          for (int q = 0; q < V; ++q) acc[q] += vv * nb[q];
+        }
       }
-      if (W == 0)
-        for (int s = 0; s < w; ++s) acc += v[s] * x[po + (size_t)c[s] * K + k];
-      r = r - acc;
+#pragma unroll
+      for (int q = 0; q < V; ++q) r[q] = r[q] - acc[q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < V; ++q) xi[q] = T(0);
     }
     if (prm.mode == S_RESID) {
-      out[ik] = r;
-    } else if (prm.mode == S_JACOBI) {
-      out[ik] = xi + prm.omega * (dinv[i] * r);
-    } else if (prm.mode == S_CHEB0) {
-      T dn = (dinv[i] * r) * prm.inv_theta;
-      d[ik] = dn;
-      out[ik] = xi + dn;
-    } else {
-      T dn = prm.c1 * d[ik] + prm.c2 * (dinv[i] * r);
-      d[ik] = dn;
-      out[ik] = xi + dn;
+      stv<T, V>(out + ik, r);
+      continue;
     }
+    const T di = dinv[i];
+    T o[V];
+    if (prm.mode == S_JACOBI) {
+#pragma unroll
+      for (int q = 0; q < V; ++q) o[q] = xi[q] + prm.omega * (di * r[q]);
+    } else if (prm.mode == S_CHEB0) {
+      T dn[V];
+#pragma unroll
+      for (int q = 0; q < V; ++q) {
+        dn[q] = (di * r[q]) * prm.inv_theta;
+        o[q] = xi[q] + dn[q];
+      }
+      if (prm.write_d) stv<T, V>(d + ik, dn);
+    } else {
+      T dn[V];
+      if (prm.d_is_x) {
+#pragma unroll
+        for (int q = 0; q < V; ++q) dn[q] = xi[q];
+      } else {
+        ldv<T, V>(d + ik, dn);
+      }
+#pragma unroll
+      for (int q = 0; q < V; ++q) {
+        dn[q] = prm.c1 * dn[q] + prm.c2 * (di * r[q]);
+        o[q] = xi[q] + dn[q];
+      }
+      if (prm.write_d) stv<T, V>(d + ik, dn);
+    }
+    stv<T, V>(out + ik, o);
   }
 }
 
 // Restriction R = row-normalised S (make_restriction, Multigrid.jl:595-612):
-// rc[i] = (1/rs_i) rf[i] + Σ_e (0.5/rs_i) rf[nc+e], rs_i = 1 + deg_i / 2.
+// rc[i] = (1/rs_i) rf[self_i] + Σ_e (0.5/rs_i) rf[mid_e], rs_i = 1 + deg_i / 2, terms in the
+// reference's column order.
 template <class T, int K>
-__global__ void __launch_bounds__(TB) k_restrict(int nc, int Wq, const int32_t* __restrict__ ridx,
-                                                 const double* __restrict__ rs, const T* __restrict__ rf,
-                                                 T* __restrict__ rc, size_t fstride, size_t cstride) {
-  const int k = threadIdx.x % K;
-  const int rows_per_grid = gridDim.x * (TB / K);
-  const T* f = rf + (size_t)blockIdx.y * fstride;
-  T* c = rc + (size_t)blockIdx.y * cstride;
-  for (int i = blockIdx.x * (TB / K) + threadIdx.x / K; i < nc; i += rows_per_grid) {
+__global__ void __launch_bounds__(TB) k_restrict(int nc, int Wq, const int32_t* __restrict__ rself,
+                                                 const int32_t* __restrict__ ridx, const double* __restrict__ rs,
+                                                 const T* __restrict__ rf, T* __restrict__ rc, size_t fstride,
+                                                 size_t cstride) {
+  using Ln = Lanes<T, K>;
+  pdl_enter();
+  constexpr int V = Ln::V;
+  const int lane = threadIdx.x % Ln::LPR;
+  const T* f = rf + (size_t)blockIdx.y * fstride + (size_t)lane * V;
+  T* c = rc + (size_t)blockIdx.y * cstride + (size_t)lane * V;
+  for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < nc; i += gridDim.x * Ln::RPB) {
     const double s = rs[i];
     const T w1 = (T)(1.0 / s), wh = (T)(0.5 / s);
-    T acc = w1 * f[(size_t)i * K + k];
-    for (int q = 0; q < Wq; ++q) {
-      int m = ridx[(size_t)i * Wq + q];
-      if (m >= 0) acc += wh * f[(size_t)m * K + k];
+    T acc[V], v[V];
+    ldv<T, V>(f + (size_t)rself[i] * K, v);
+#pragma unroll
+    for (int q = 0; q < V; ++q) acc[q] = w1 * v[q];
+    for (int e = 0; e < Wq; ++e) {
+      int m = ridx[(size_t)i * Wq + e];
+      if (m < 0) break;
+      ldv<T, V>(f + (size_t)m * K, v);
+#pragma unroll
+      for (int q = 0; q < V; ++q) acc[q] += wh * v[q];
     }
-    c[(size_t)i * K + k] = acc;
+    stv<T, V>(c + (size_t)i * K, acc);
   }
 }
 
-// Prolongation and correction x_f += P z (P = Sᵀ, Multigrid.jl:774).
+// Prolongation and correction x_f += P z (P = Sᵀ, Multigrid.jl:774): every fine row takes
+// ½ z[pa] + ½ z[pb] (pa = pb for a coarse vertex, which gives z exactly).
 template <class T, int K>
-__global__ void __launch_bounds__(TB) k_prolong(int nf, int nc, const int32_t* __restrict__ pa,
-                                                const int32_t* __restrict__ pb, const T* __restrict__ z,
-                                                T* __restrict__ x, size_t fstride, size_t cstride) {
-  const int k = threadIdx.x % K;
-  const int rows_per_grid = gridDim.x * (TB / K);
-  const T* zc = z + (size_t)blockIdx.y * cstride;
-  T* xf = x + (size_t)blockIdx.y * fstride;
-  for (int j = blockIdx.x * (TB / K) + threadIdx.x / K; j < nf; j += rows_per_grid) {
-    T pz;
-    if (j < nc) {
-      pz = zc[(size_t)j * K + k];
-    } else {
-      int e = j - nc;
-      pz = T(0.5) * zc[(size_t)pa[e] * K + k] + T(0.5) * zc[(size_t)pb[e] * K + k];
-    }
-    xf[(size_t)j * K + k] += pz;
+__global__ void __launch_bounds__(TB) k_prolong(int nf, const int32_t* __restrict__ pa, const int32_t* __restrict__ pb,
+                                                const T* __restrict__ z, T* __restrict__ x, size_t fstride,
+                                                size_t cstride) {
+  using Ln = Lanes<T, K>;
+  pdl_enter();
+  constexpr int V = Ln::V;
+  const int lane = threadIdx.x % Ln::LPR;
+  const T* zc = z + (size_t)blockIdx.y * cstride + (size_t)lane * V;
+  T* xf = x + (size_t)blockIdx.y * fstride + (size_t)lane * V;
+  for (int j = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; j < nf; j += gridDim.x * Ln::RPB) {
+    T za[V], zb[V], xv[V];
+    ldv<T, V>(zc + (size_t)pa[j] * K, za);
+    ldv<T, V>(zc + (size_t)pb[j] * K, zb);
+    ldv<T, V>(xf + (size_t)j * K, xv);
+#pragma unroll
+    for (int q = 0; q < V; ++q) xv[q] += T(0.5) * za[q] + T(0.5) * zb[q];
+    stv<T, V>(xf + (size_t)j * K, xv);
   }
 }
 
-// Coarsest level: x = A⁻¹ b with the dense FP64 inverse (one CTA per panel).
+// Coarsest level: x = A⁻¹ b with the dense FP64 inverse; one thread per (row, right-hand side),
+// the row of A⁻¹ shared (broadcast) by a row's K lanes.
 template <class T, int K>
 __global__ void __launch_bounds__(TB) k_coarse(int n, const double* __restrict__ ainv, const T* __restrict__ b,
                                                T* __restrict__ x, size_t pstride) {
-  const T* bb = b + (size_t)blockIdx.x * pstride;
-  T* xx = x + (size_t)blockIdx.x * pstride;
-  for (int q = threadIdx.x; q < n * K; q += blockDim.x) {
-    int i = q / K, k = q % K;
+  pdl_enter();
+  const T* bb = b + (size_t)blockIdx.y * pstride;
+  T* xx = x + (size_t)blockIdx.y * pstride;
+  const int k = threadIdx.x % K;
+  for (int i = blockIdx.x * (TB / K) + threadIdx.x / K; i < n; i += gridDim.x * (TB / K)) {
+    const double* a = ainv + (size_t)i * n;
     double s = 0.0;
-    for (int j = 0; j < n; ++j) s += ainv[(size_t)i * n + j] * (double)bb[(size_t)j * K + k];
+    for (int j = 0; j < n; ++j) s += a[j] * (double)bb[(size_t)j * K + k];
     xx[(size_t)i * K + k] = (T)s;
   }
 }
 
-// Column-major RHS block (nrhs vectors of length n) <-> panels of K.
+// Column-major RHS block (nrhs vectors of length n, reference vertex order) -> panels of K in
+// the level's internal order (perm: internal -> reference), and back.
 template <class T, class S>
-__global__ void k_to_panels(int n, int nrhs, int K, int npanels, const S* __restrict__ src, T* __restrict__ dst) {
+__global__ void k_to_panels(int n, int nrhs, int K, int npanels, const int32_t* __restrict__ perm,
+                            const S* __restrict__ src, T* __restrict__ dst) {
   size_t total = (size_t)n * K * npanels;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
     size_t p = q / ((size_t)n * K), rem = q % ((size_t)n * K);
     int i = (int)(rem / K), k = (int)(rem % K);
     int j = (int)p * K + k;
-    dst[q] = j < nrhs ? (T)src[(size_t)j * n + i] : T(0);
+    dst[q] = j < nrhs ? (T)src[(size_t)j * n + perm[i]] : T(0);
   }
 }
 
 template <class T, class S>
-__global__ void k_from_panels(int n, int nrhs, int K, const S* __restrict__ src, T* __restrict__ dst) {
+__global__ void k_from_panels(int n, int nrhs, int K, const int32_t* __restrict__ iperm, const S* __restrict__ src,
+                              T* __restrict__ dst) {
   size_t total = (size_t)n * nrhs;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
     int j = (int)(q / n), i = (int)(q % n);
     int p = j / K, k = j % K;
-    dst[q] = (T)src[(size_t)p * n * K + (size_t)i * K + k];
+    dst[q] = (T)src[(size_t)p * n * K + (size_t)iperm[i] * K + k];
   }
 }
 
 // u += (double) z on the panels.
 template <class T>
 __global__ void k_axpy_update(size_t total, const T* __restrict__ z, double* __restrict__ u) {
+  pdl_enter();
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x)
     u[q] += (double)z[q];
 }
 
-// FP64 residual r = b - A u on the panels, written both as FP64 and in the inner precision T,
-// with per-block partial sums of r² per right-hand side (deterministic two-stage reduction).
+// FP64 residual r = b - A u on the panels, written in the inner precision T, with per-block
+// partial sums of r² per right-hand side (deterministic two-stage reduction).
 template <class T, int K, int W>
 __global__ void __launch_bounds__(TB) k_residual64(int n, int Wr, const int32_t* __restrict__ col,
                                                    const double* __restrict__ off, const double* __restrict__ diag,
                                                    const double* __restrict__ b, const double* __restrict__ u,
                                                    T* __restrict__ rT, double* __restrict__ partial, size_t pstride) {
+  using Ln = Lanes<double, K>;
+  pdl_enter();
+  constexpr int V = Ln::V;
   const int w = W > 0 ? W : Wr;
-  const int k = threadIdx.x % K;
-  const size_t po = (size_t)blockIdx.y * pstride;
-  double ss = 0.0;
-  const int rows_per_grid = gridDim.x * (TB / K);
-  for (int i = blockIdx.x * (TB / K) + threadIdx.x / K; i < n; i += rows_per_grid) {
-    const size_t ik = po + (size_t)i * K + k;
-    double acc = diag[i] * u[ik];
+  const int lane = threadIdx.x % Ln::LPR;
+  const size_t po = (size_t)blockIdx.y * pstride + (size_t)lane * V;
+  double ss[V];
+#pragma unroll
+  for (int q = 0; q < V; ++q) ss[q] = 0.0;
+  for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < n; i += gridDim.x * Ln::RPB) {
+    const size_t ik = po + (size_t)i * K;
+    double ui[V], acc[V], bv[V];
+    ldv<double, V>(u + ik, ui);
+    ldv<double, V>(b + ik, bv);
+    const double dg = diag[i];
+#pragma unroll
+    for (int q = 0; q < V; ++q) acc[q] = dg * ui[q];
     const int32_t* c = col + (size_t)i * w;
     const double* v = off + (size_t)i * w;
-    for (int s = 0; s < w; ++s) acc += v[s] * u[po + (size_t)c[s] * K + k];
-    double r = b[ik] - acc;
-    rT[ik] = (T)r;
-    ss += r * r;
+    for (int s = 0; s < w; ++s) {
+      double nb[V];
+      ldv<double, V>(u + po + (size_t)c[s] * K, nb);
+      const double vv = v[s];
+#pragma unroll
+      for (int q = 0; q < V; ++q) acc[q] += vv * nb[q];
+    }
+#pragma unroll
+    for (int q = 0; q < V; ++q) {
+      double r = bv[q] - acc[q];
+      rT[ik + q] = (T)r;
+      ss[q] += r * r;
+    }
   }
-  // reduce over the TB/K rows of this block for lane k
-  __shared__ double sh[TB];
-  sh[threadIdx.x] = ss;
+  // reduce over the rows of this block per right-hand side (column lane*V + q)
+  __shared__ double sh[TB * V];
+#pragma unroll
+  for (int q = 0; q < V; ++q) sh[threadIdx.x * V + q] = ss[q];
   __syncthreads();
-  for (int stride = TB / 2; stride >= K; stride >>= 1) {
-    if (threadIdx.x < stride) sh[threadIdx.x] += sh[threadIdx.x + stride];
+  for (int stride = TB / 2; stride >= Ln::LPR; stride >>= 1) {
+    if (threadIdx.x < stride)
+#pragma unroll
+      for (int q = 0; q < V; ++q) sh[threadIdx.x * V + q] += sh[(threadIdx.x + stride) * V + q];
     __syncthreads();
   }
-  if (threadIdx.x < K) partial[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * K + threadIdx.x] = sh[threadIdx.x];
+  if (threadIdx.x < Ln::LPR)
+#pragma unroll
+    for (int q = 0; q < V; ++q)
+      partial[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * K + threadIdx.x * V + q] = sh[threadIdx.x * V + q];
 }
 
-// Σ over blocks of the partial sums: out[p*K + k] (one thread per (panel, lane)).
-__global__ void k_reduce_partials(int nblocks, int K, int npanels, const double* __restrict__ partial,
-                                  double* __restrict__ out) {
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= K * npanels) return;
-  int p = q / K, k = q % K;
+// Σ over blocks of the partial sums: out[p*K + k], one CTA per (panel, lane), tree-reduced in a
+// fixed order (deterministic).
+__global__ void __launch_bounds__(256) k_reduce_partials(int nblocks, int K, int npanels,
+                                                         const double* __restrict__ partial,
+                                                         double* __restrict__ out) {
+  pdl_enter();
+  const int q = blockIdx.x;
+  const int p = q / K, k = q % K;
   double s = 0.0;
-  for (int bq = 0; bq < nblocks; ++bq) s += partial[((size_t)p * nblocks + bq) * K + k];
-  out[q] = s;
+  for (int bq = threadIdx.x; bq < nblocks; bq += blockDim.x) s += partial[((size_t)p * nblocks + bq) * K + k];
+  __shared__ double sh[256];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[q] = sh[0];
 }
 
 // Per-block partial sums of x² per right-hand side over the panels (same layout as k_residual64).
@@ -375,9 +581,10 @@ __global__ void k_dinv_a(int n, int W, const int32_t* __restrict__ col, const do
   }
 }
 
-__global__ void k_hash_init(int n, double* x) {
+// Start vector of the power iteration: a hash of each vertex's reference index.
+__global__ void k_hash_init(int n, const int32_t* __restrict__ perm, double* x) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    uint64_t z = (uint64_t)i * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+    uint64_t z = (uint64_t)perm[i] * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
     z ^= z >> 31;
@@ -402,22 +609,25 @@ __global__ void k_scale(int n, double a, double* x) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] *= a;
 }
 
-// Split layout of the level operator: diagonal + W off-diagonal slots (padding: own column,
-// value 0) from the sorted ELL rows.
+// Split layout of the level operator in the internal order: row i' (reference row perm[i'])
+// gets its diagonal and W off-diagonal slots (reference column order kept, columns mapped
+// through iperm; padding: own row, value 0).
 __global__ void k_split(int n, int Wf, const int32_t* __restrict__ fcol, const double* __restrict__ fval, int W,
+                        const int32_t* __restrict__ perm, const int32_t* __restrict__ iperm,
                         int32_t* __restrict__ col, double* __restrict__ off, double* __restrict__ diag,
                         double* __restrict__ dinv) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int r = perm[i];
     int q = 0;
     double dg = 0.0;
     for (int s = 0; s < Wf; ++s) {
-      int c = fcol[(size_t)i * Wf + s];
+      int c = fcol[(size_t)r * Wf + s];
       if (c < 0) continue;
-      if (c == i) {
-        dg += fval[(size_t)i * Wf + s];
+      if (c == r) {
+        dg += fval[(size_t)r * Wf + s];
       } else if (q < W) {
-        col[(size_t)i * W + q] = c;
-        off[(size_t)i * W + q] = fval[(size_t)i * Wf + s];
+        col[(size_t)i * W + q] = iperm[c];
+        off[(size_t)i * W + q] = fval[(size_t)r * Wf + s];
         ++q;
       }
     }
@@ -435,15 +645,17 @@ __global__ void k_split(int n, int Wf, const int32_t* __restrict__ fcol, const d
 // ---------------------------------------------------------------------------------------------
 struct Level {
   std::unique_ptr<dec_mesh> mesh;
-  std::unique_ptr<dec_op> op;  // A = L + shift I (sorted ELL, FP64): exports and parity
+  std::unique_ptr<dec_op> op;  // A = L + shift I (reference order, sorted ELL, FP64): exports, parity
   int n = 0, W = 0;
+  std::vector<int32_t> perm, iperm;  // internal -> reference, reference -> internal
+  DArr<int32_t> dperm, diperm;
   DArr<int32_t> col;
   DArr<double> off64, diag64, dinv64;
   DArr<float> off32, diag32, dinv32;
   double lmax = 0.0;
-  // transfer to the next coarser level
+  // transfer to the next coarser level (internal numbering on both sides)
   int nc = 0, Wq = 0;
-  DArr<int32_t> ridx, pa, pb;
+  DArr<int32_t> rself, ridx, pa, pb;
   DArr<double> rs;
 };
 
@@ -456,9 +668,9 @@ struct Workspace {
   int K = 0, npanels = 0, prec = 0;
   std::vector<LevelBufs<float>> f32;
   std::vector<LevelBufs<double>> f64;
-  DArr<double> B64, U64, R64;  // finest FP64 panels
+  DArr<double> B64, U64;      // finest FP64 panels
   DArr<double> partial, norms;
-  DArr<double> ucm, bcm;       // column-major device copies for host-buffer solves
+  DArr<double> ucm, bcm;      // column-major device copies for host-buffer solves
   int nblocks = 0;
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};  // GraphKind
   int64_t launches[3] = {0, 0, 0};                          // kernel nodes per graph
@@ -473,10 +685,11 @@ struct Workspace {
 struct dec_mg {
   dec_mg_options opt{};
   std::vector<decb::Level> lv;  // 0 = finest
-  decb::DArr<double> ainv;      // coarsest dense inverse (FP64)
+  decb::DArr<double> ainv;      // dense inverse of level lc (FP64, internal order)
+  int lc = 0;                   // level at which cycles solve directly
   std::map<long long, std::unique_ptr<decb::Workspace>> ws;
   std::map<long long, int> tuned;  // (nrhs, precision) -> panel width chosen by the autotuner
-  cudaStream_t cap = nullptr;   // capture stream
+  cudaStream_t cap = nullptr;      // capture stream
   ~dec_mg() {
     ws.clear();
     if (cap) cudaStreamDestroy(cap);
@@ -500,13 +713,16 @@ void mg_default_options(dec_mg_options& o) {
   o.precision = 0;
   o.rhs_block = 0;
   o.mu = 1;
+  o.inner_cycles = 1;
+  o.reorder = 1;
+  o.coarse_max = 0;
 }
 
 static double power_lmax(const Level& L) {
   if (L.n < 2) return 1.0;
   DArr<double> x(L.n), y(L.n), s(1);
   const int T = 256;
-  k_hash_init<<<grid_for(L.n, T), T>>>(L.n, x.p);
+  k_hash_init<<<grid_for(L.n, T), T>>>(L.n, L.dperm.p, x.p);
   double lam = 1.0;
   for (int it = 0; it < 30; ++it) {
     k_sumsq<<<1, 256>>>(L.n, x.p, s.p);
@@ -521,95 +737,115 @@ static double power_lmax(const Level& L) {
   return lam * 1.05;  // power iteration approaches λmax from below
 }
 
-// Dense inverse of the coarsest operator (Gauss-Jordan, partial pivoting).
+// Dense inverse of the coarsest operator (Gauss-Jordan, partial pivoting), reference order.
 static std::vector<double> dense_inverse(const dec_op& op, int n) {
-  {
-    auto c = op.col.download();
-    auto vv = op.val64.download();
-    std::vector<double> A((size_t)n * n, 0.0), Ainv((size_t)n * n, 0.0);
-    for (int i = 0; i < n; ++i)
-      for (int q = 0; q < op.W; ++q) {
-        int j = c[(size_t)i * op.W + q];
-        if (j >= 0) A[(size_t)i * n + j] += vv[(size_t)i * op.W + q];
-      }
-    for (int i = 0; i < n; ++i) Ainv[(size_t)i * n + i] = 1.0;
-    double amax = 0.0;
-    for (double a : A) amax = std::max(amax, std::fabs(a));
-    for (int k = 0; k < n; ++k) {
-      int p = k;
-      for (int i = k + 1; i < n; ++i)
-        if (std::fabs(A[(size_t)i * n + k]) > std::fabs(A[(size_t)p * n + k])) p = i;
-      if (std::fabs(A[(size_t)p * n + k]) <= 1e-13 * amax)
-        throw Error(DEC_ERR_INVALID_ARG,
-                    "multigrid: the coarsest operator is singular; use a positive shift or coarse_solver = 1");
-      if (p != k)
-        for (int j = 0; j < n; ++j) {
-          std::swap(A[(size_t)k * n + j], A[(size_t)p * n + j]);
-          std::swap(Ainv[(size_t)k * n + j], Ainv[(size_t)p * n + j]);
-        }
-      double piv = A[(size_t)k * n + k];
+  auto c = op.col.download();
+  auto vv = op.val64.download();
+  std::vector<double> A((size_t)n * n, 0.0), Ainv((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int q = 0; q < op.W; ++q) {
+      int j = c[(size_t)i * op.W + q];
+      if (j >= 0) A[(size_t)i * n + j] += vv[(size_t)i * op.W + q];
+    }
+  for (int i = 0; i < n; ++i) Ainv[(size_t)i * n + i] = 1.0;
+  double amax = 0.0;
+  for (double a : A) amax = std::max(amax, std::fabs(a));
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    for (int i = k + 1; i < n; ++i)
+      if (std::fabs(A[(size_t)i * n + k]) > std::fabs(A[(size_t)p * n + k])) p = i;
+    if (std::fabs(A[(size_t)p * n + k]) <= 1e-13 * amax)
+      throw Error(DEC_ERR_INVALID_ARG,
+                  "multigrid: the coarsest operator is singular; use a positive shift or coarse_solver = 1");
+    if (p != k)
       for (int j = 0; j < n; ++j) {
-        A[(size_t)k * n + j] /= piv;
-        Ainv[(size_t)k * n + j] /= piv;
+        std::swap(A[(size_t)k * n + j], A[(size_t)p * n + j]);
+        std::swap(Ainv[(size_t)k * n + j], Ainv[(size_t)p * n + j]);
       }
-      for (int i = 0; i < n; ++i) {
-        if (i == k) continue;
-        double f = A[(size_t)i * n + k];
-        if (f == 0.0) continue;
-        for (int j = 0; j < n; ++j) {
-          A[(size_t)i * n + j] -= f * A[(size_t)k * n + j];
-          Ainv[(size_t)i * n + j] -= f * Ainv[(size_t)k * n + j];
-        }
+    double piv = A[(size_t)k * n + k];
+    for (int j = 0; j < n; ++j) {
+      A[(size_t)k * n + j] /= piv;
+      Ainv[(size_t)k * n + j] /= piv;
+    }
+    for (int i = 0; i < n; ++i) {
+      if (i == k) continue;
+      double f = A[(size_t)i * n + k];
+      if (f == 0.0) continue;
+      for (int j = 0; j < n; ++j) {
+        A[(size_t)i * n + j] -= f * A[(size_t)k * n + j];
+        Ainv[(size_t)i * n + j] -= f * Ainv[(size_t)k * n + j];
       }
     }
-    return Ainv;
   }
+  return Ainv;
 }
 
-static void build_level_operator(Level& L, double shift) {
+static void build_level_operator(Level& L, double shift, bool reorder) {
   L.op.reset(op_create_impl(L.mesh.get(), DEC_OP_HELMHOLTZ0, shift, DEC_F64));
   L.n = L.mesh->m.nv;
+  if (reorder) {
+    L.perm = morton_order(L.mesh->m.h_pts, L.n);
+  } else {
+    L.perm.resize(L.n);
+    std::iota(L.perm.begin(), L.perm.end(), 0);
+  }
+  L.iperm.resize(L.n);
+  for (int i = 0; i < L.n; ++i) L.iperm[L.perm[i]] = i;
+  L.dperm.upload(L.perm);
+  L.diperm.upload(L.iperm);
   L.W = std::max(1, L.op->W - 1);
   L.col.alloc((size_t)L.n * L.W);
   L.off64.alloc((size_t)L.n * L.W);
   L.diag64.alloc(L.n);
   L.dinv64.alloc(L.n);
-  k_split<<<grid_for(L.n, 256), 256>>>(L.n, L.op->W, L.op->col.p, L.op->val64.p, L.W, L.col.p, L.off64.p,
-                                       L.diag64.p, L.dinv64.p);
+  k_split<<<grid_for(L.n, 256), 256>>>(L.n, L.op->W, L.op->col.p, L.op->val64.p, L.W, L.dperm.p, L.diperm.p,
+                                       L.col.p, L.off64.p, L.diag64.p, L.dinv64.p);
   DEC_CHECK_LAUNCH();
   cast_array(L.off64, L.off32);
   cast_array(L.diag64, L.diag32);
   cast_array(L.dinv64, L.dinv32);
 }
 
-// Transfers between fine level L and its coarse level (host topology of the coarse level).
-static void build_transfers(Level& L, const HostLevel& c) {
-  L.nc = c.nv;
-  std::vector<int32_t> pa(c.ne), pb(c.ne);
-  std::vector<std::vector<int32_t>> inc(c.nv);
+// Transfers between fine level F and its coarse level C (host topology c of the coarse mesh),
+// in the internal numbering of both.
+static void build_transfers(Level& F, const Level& C, const HostLevel& c) {
+  F.nc = c.nv;
+  std::vector<std::vector<int32_t>> inc(c.nv);  // coarse vertex -> fine midpoints (reference)
   for (int e = 0; e < c.ne; ++e) {
-    pa[e] = std::min(c.ev0[e], c.ev1[e]);
-    pb[e] = std::max(c.ev0[e], c.ev1[e]);
     inc[c.ev0[e]].push_back(c.nv + e);
     if (c.ev1[e] != c.ev0[e]) inc[c.ev1[e]].push_back(c.nv + e);
   }
   int Wq = 1;
   for (auto& v : inc) Wq = std::max<int>(Wq, (int)v.size());
-  std::vector<int32_t> ridx((size_t)c.nv * Wq, -1);
+  std::vector<int32_t> rself(c.nv), ridx((size_t)c.nv * Wq, -1);
   std::vector<double> rs(c.nv);
-  for (int i = 0; i < c.nv; ++i) {
-    double s = 1.0;  // row sum of S in column order: 1.0 then 0.5 per incident edge
+  for (int ic = 0; ic < c.nv; ++ic) {   // internal coarse row
+    int i = C.perm[ic];                 // reference coarse vertex
+    rself[ic] = F.iperm[i];             // the vertex's copy on the fine level (reference index i)
+    double s = 1.0;                     // row sum of S in column order: 1.0 then 0.5 per edge
     for (size_t q = 0; q < inc[i].size(); ++q) {
-      ridx[(size_t)i * Wq + q] = inc[i][q];
+      ridx[(size_t)ic * Wq + q] = F.iperm[inc[i][q]];
       s += 0.5;
     }
-    rs[i] = s;
+    rs[ic] = s;
   }
-  L.Wq = Wq;
-  L.ridx.upload(ridx);
-  L.rs.upload(rs);
-  L.pa.upload(pa);
-  L.pb.upload(pb);
+  std::vector<int32_t> pa(F.n), pb(F.n);
+  for (int jf = 0; jf < F.n; ++jf) {    // internal fine row
+    int j = F.perm[jf];
+    if (j < c.nv) {
+      pa[jf] = pb[jf] = C.iperm[j];
+    } else {
+      int e = j - c.nv;
+      pa[jf] = C.iperm[std::min(c.ev0[e], c.ev1[e])];
+      pb[jf] = C.iperm[std::max(c.ev0[e], c.ev1[e])];
+    }
+  }
+  F.Wq = Wq;
+  F.rself.upload(rself);
+  F.ridx.upload(ridx);
+  F.rs.upload(rs);
+  F.pa.upload(pa);
+  F.pb.upload(pb);
 }
 
 dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
@@ -619,9 +855,10 @@ dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
   require(o.mu == 1 || o.mu == 2, "multigrid: mu must be 1 (V) or 2 (W)");
   require(o.precision == 0 || o.precision == 1, "multigrid: precision must be 0 or 1");
   require(o.cheb_ratio > 1.0, "multigrid: cheb_ratio must exceed 1");
+  require(o.inner_cycles >= 1 && o.inner_cycles <= 8, "multigrid: inner_cycles must be in [1, 8]");
+  require(o.coarse_max >= 0 && o.coarse_max <= 1024, "multigrid: coarse_max must be in [0, 1024]");
   auto mg = std::make_unique<dec_mg>();
   mg->opt = o;
-  // Coarse level from the description (orientation resolved by Mesh::build).
   std::vector<HostLevel> hl(o.levels + 1);
   {
     auto m = std::make_unique<dec_mesh>();
@@ -650,14 +887,27 @@ dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
     hl[l] = refine_level(hl[l - 1], o.project_radius, l == 1 ? &flip : nullptr);
     mg->lv[o.levels - l].mesh = make_mesh(hl[l], o.center);
   }
+  for (int l = 0; l <= o.levels; ++l) build_level_operator(mg->lv[l], o.shift, o.reorder != 0);
   for (int l = 0; l <= o.levels; ++l) {
     Level& L = mg->lv[l];
-    build_level_operator(L, o.shift);
-    if (l < o.levels) build_transfers(L, hl[o.levels - l - 1]);
+    if (l < o.levels) build_transfers(L, mg->lv[l + 1], hl[o.levels - l - 1]);
     L.lmax = power_lmax(L);
   }
-  const Level& C = mg->lv[o.levels];
-  if (o.coarse_solver == 0) mg->ainv.upload(dense_inverse(*C.op, C.n));
+  mg->lc = o.levels;
+  if (o.coarse_max > 0)
+    for (int l = 0; l <= o.levels; ++l)
+      if (mg->lv[l].n <= o.coarse_max) {
+        mg->lc = l;
+        break;
+      }
+  const Level& C = mg->lv[mg->lc];
+  if (o.coarse_solver == 0) {
+    auto ai = dense_inverse(*C.op, C.n);
+    std::vector<double> ap((size_t)C.n * C.n);
+    for (int i = 0; i < C.n; ++i)
+      for (int j = 0; j < C.n; ++j) ap[(size_t)i * C.n + j] = ai[(size_t)C.perm[i] * C.n + C.perm[j]];
+    mg->ainv.upload(ap);
+  }
   DEC_CUDA(cudaStreamCreateWithFlags(&mg->cap, cudaStreamNonBlocking));
   DEC_CUDA(cudaDeviceSynchronize());
   return mg.release();
@@ -692,17 +942,22 @@ static const T* pick(const DArr<double>& a64, const DArr<float>& a32) {
 }
 
 template <class T, int K>
+static dim3 row_grid(int n, int np) {
+  return dim3(grid_for((long long)n, Lanes<T, K>::RPB, 8), np);
+}
+
+template <class T, int K>
 static void launch_sweep(const Level& L, const T* b, const T* x, T* out, T* d, SweepPrm<T> prm, int np,
                          cudaStream_t s) {
   size_t ps = (size_t)L.n * K;
-  dim3 grid(grid_for((long long)L.n * K, TB, 8), np);
+  dim3 grid = row_grid<T, K>(L.n, np);
   const T* off = pick<T>(L.off64, L.off32);
   const T* dg = pick<T>(L.diag64, L.diag32);
   const T* di = pick<T>(L.dinv64, L.dinv32);
   if (L.W == 6)
-    k_sweep<T, K, 6><<<grid, TB, 0, s>>>(L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps);
+    launch_pdl(k_sweep<T, K, 6>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps);
   else
-    k_sweep<T, K, 0><<<grid, TB, 0, s>>>(L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps);
+    launch_pdl(k_sweep<T, K, 0>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps);
 }
 
 // Smooth `sweeps` times starting from x (zero if zero_x); returns the buffer holding the result.
@@ -714,9 +969,13 @@ static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool z
   const double hi = L.lmax, lo = L.lmax / o.cheb_ratio;
   const double theta = (hi + lo) / 2, delta = (hi - lo) / 2, sigma = theta / delta;
   double rho = 1 / sigma;
+  const bool started_at_zero = zero_x;
   for (int it = 0; it < sweeps; ++it) {
     SweepPrm<T> prm{};
     prm.zero_x = zero_x ? 1 : 0;
+    // the direction is needed only by a later sweep; after a first step from zero it equals x
+    prm.write_d = (it + 1 < sweeps) && !(it == 0 && started_at_zero) ? 1 : 0;
+    prm.d_is_x = (it == 1 && started_at_zero) ? 1 : 0;
     if (o.smoother == DEC_SMOOTH_JACOBI) {
       prm.mode = S_JACOBI;
       prm.omega = (T)o.omega;
@@ -743,9 +1002,9 @@ static T* mu_cycle(const dec_mg& mg, std::vector<LevelBufs<T>>& bufs, int l, T* 
                    cudaStream_t s) {
   const Level& L = mg.lv[l];
   LevelBufs<T>& B = bufs[l];
-  const int last = (int)mg.lv.size() - 1;
-  if (l == last) {
-    k_coarse<T, K><<<np, TB, 0, s>>>(L.n, mg.ainv.p, B.b.p, B.x.p, (size_t)L.n * K);
+  if (l == mg.lc) {
+    launch_pdl(k_coarse<T, K>, dim3(grid_for(L.n, TB / K, 64), np), dim3(TB), s, L.n, (const double*)mg.ainv.p,
+               (const T*)B.b.p, B.x.p, (size_t)L.n * K);
     return B.x.p;
   }
   x = smooth<T, K>(mg, L, B, x, zero_x, mg.opt.pre, np, s);
@@ -758,15 +1017,16 @@ static T* mu_cycle(const dec_mg& mg, std::vector<LevelBufs<T>>& bufs, int l, T* 
   launch_sweep<T, K>(L, B.b.p, x, r, nullptr, prm, np, s);
   const Level& Cl = mg.lv[l + 1];
   LevelBufs<T>& Cb = bufs[l + 1];
-  dim3 gc(grid_for((long long)Cl.n * K, TB, 8), np);
-  k_restrict<T, K><<<gc, TB, 0, s>>>(L.nc, L.Wq, L.ridx.p, L.rs.p, r, Cb.b.p, (size_t)L.n * K, (size_t)Cl.n * K);
+  launch_pdl(k_restrict<T, K>, row_grid<T, K>(Cl.n, np), dim3(TB), s, L.nc, L.Wq, (const int32_t*)L.rself.p,
+             (const int32_t*)L.ridx.p, (const double*)L.rs.p, (const T*)r, Cb.b.p, (size_t)L.n * K,
+             (size_t)Cl.n * K);
   T* z = mu_cycle<T, K>(mg, bufs, l + 1, Cb.x.p, true, mu, np, s);
   if (mu > 1) z = mu_cycle<T, K>(mg, bufs, l + 1, z, false, mu - 1, np, s);
-  dim3 gf(grid_for((long long)L.n * K, TB, 8), np);
   if (zero_x) {  // x is all zero: start it from the prolonged correction
     DEC_CUDA(cudaMemsetAsync(x, 0, (size_t)L.n * K * np * sizeof(T), s));
   }
-  k_prolong<T, K><<<gf, TB, 0, s>>>(L.n, L.nc, L.pa.p, L.pb.p, z, x, (size_t)L.n * K, (size_t)Cl.n * K);
+  launch_pdl(k_prolong<T, K>, row_grid<T, K>(L.n, np), dim3(TB), s, L.n, (const int32_t*)L.pa.p,
+             (const int32_t*)L.pb.p, (const T*)z, x, (size_t)L.n * K, (size_t)Cl.n * K);
   return smooth<T, K>(mg, L, B, x, false, mg.opt.post, np, s);
 }
 
@@ -805,23 +1065,29 @@ static void enqueue_resid_T(dec_mg& mg, Workspace& w, cudaStream_t s, std::vecto
   const Level& F = mg.lv[0];
   const int np = w.npanels;
   const size_t total = (size_t)F.n * K * np;
-  k_axpy_update<T><<<grid_for((long long)total, 256), 256, 0, s>>>(total, bufs[0].x.p, w.U64.p);
+  launch_pdl(k_axpy_update<T>, dim3(grid_for((long long)total, 256)), dim3(256), s, total, (const T*)bufs[0].x.p,
+             w.U64.p);
   dim3 g(w.nblocks, np);
   if (F.W == 6)
-    k_residual64<T, K, 6><<<g, TB, 0, s>>>(F.n, F.W, F.col.p, F.off64.p, F.diag64.p, w.B64.p, w.U64.p, bufs[0].b.p,
-                                           w.partial.p, (size_t)F.n * K);
+    launch_pdl(k_residual64<T, K, 6>, g, dim3(TB), s, F.n, F.W, (const int32_t*)F.col.p, (const double*)F.off64.p,
+               (const double*)F.diag64.p, (const double*)w.B64.p, (const double*)w.U64.p, bufs[0].b.p, w.partial.p,
+               (size_t)F.n * K);
   else
-    k_residual64<T, K, 0><<<g, TB, 0, s>>>(F.n, F.W, F.col.p, F.off64.p, F.diag64.p, w.B64.p, w.U64.p, bufs[0].b.p,
-                                           w.partial.p, (size_t)F.n * K);
-  k_reduce_partials<<<(K * np + 127) / 128, 128, 0, s>>>(w.nblocks, K, np, w.partial.p, w.norms.p);
+    launch_pdl(k_residual64<T, K, 0>, g, dim3(TB), s, F.n, F.W, (const int32_t*)F.col.p, (const double*)F.off64.p,
+               (const double*)F.diag64.p, (const double*)w.B64.p, (const double*)w.U64.p, bufs[0].b.p, w.partial.p,
+               (size_t)F.n * K);
+  launch_pdl(k_reduce_partials, dim3(K * np), dim3(256), s, w.nblocks, K, np, (const double*)w.partial.p,
+             w.norms.p);
   DEC_CHECK_LAUNCH();
 }
 
-// Refinement step, part 2: e = V(r) from a zero initial guess, left in bufs[0].x.
+// Refinement step, part 2: e = V^c(r) (c = inner_cycles) from a zero initial guess, left in
+// bufs[0].x.
 template <class T, int K>
 static void enqueue_vcycle_T(dec_mg& mg, Workspace& w, cudaStream_t s, std::vector<LevelBufs<T>>& bufs) {
   const size_t total = (size_t)mg.lv[0].n * K * w.npanels;
-  T* e = mu_cycle<T, K>(mg, bufs, 0, bufs[0].x.p, true, mg.opt.mu, w.npanels, s);
+  T* e = bufs[0].x.p;
+  for (int c = 0; c < mg.opt.inner_cycles; ++c) e = mu_cycle<T, K>(mg, bufs, 0, e, c == 0, mg.opt.mu, w.npanels, s);
   if (e != bufs[0].x.p)
     DEC_CUDA(cudaMemcpyAsync(bufs[0].x.p, e, total * sizeof(T), cudaMemcpyDeviceToDevice, s));
   DEC_CHECK_LAUNCH();
@@ -914,7 +1180,7 @@ static Workspace& workspace_k(dec_mg& mg, int nrhs, int prec, int K) {
   else alloc_bufs(mg, w->f64, K, np);
   w->B64.alloc(total);
   w->U64.alloc(total);
-  w->nblocks = (int)std::min<long long>(2LL * num_sms(), ((long long)mg.lv[0].n * K + TB - 1) / TB);
+  w->nblocks = (int)std::max<long long>(1, std::min<long long>(8LL * num_sms(), ((long long)mg.lv[0].n * K + TB - 1) / TB));
   w->partial.alloc((size_t)w->nblocks * K * np);
   w->norms.alloc((size_t)K * np);
   DEC_CUDA(cudaMemset(w->B64.p, 0, w->B64.bytes()));
@@ -933,24 +1199,29 @@ void mg_cycles(dec_mg* mg, double* u, const double* b, int nrhs, int cycles, voi
   require(nrhs >= 1 && cycles >= 0, "multigrid: bad nrhs / cycles");
   cudaStream_t s = as_stream(stream);
   Workspace& w = workspace(*mg, nrhs, 0);
-  const int n = mg->lv[0].n;
+  const Level& F = mg->lv[0];
+  const int n = F.n;
   const size_t total = (size_t)n * w.K * w.npanels;
-  k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, w.K, w.npanels, b, w.B64.p);
-  k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, w.K, w.npanels, u, w.U64.p);
+  k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, w.K, w.npanels, F.dperm.p, b,
+                                                                               w.B64.p);
+  k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, w.K, w.npanels, F.dperm.p, u,
+                                                                               w.U64.p);
   DEC_CHECK_LAUNCH();
   if (!w.graph[G_CYCLE]) w.graph[G_CYCLE] = capture(*mg, w, G_CYCLE);
   for (int c = 0; c < cycles; ++c) DEC_CUDA(cudaGraphLaunch(w.graph[G_CYCLE], s));
-  k_from_panels<double, double><<<grid_for((long long)n * nrhs, 256), 256, 0, s>>>(n, nrhs, w.K, w.U64.p, u);
+  k_from_panels<double, double><<<grid_for((long long)n * nrhs, 256), 256, 0, s>>>(n, nrhs, w.K, F.diperm.p,
+                                                                                    w.U64.p, u);
   DEC_CHECK_LAUNCH();
 }
 
 dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rtol, int max_iters,
-                    dec_solve_report* rep, void* stream, bool host_buffers) {
+                    dec_solve_report* rep, void* stream, bool host_buffers, bool use_initial_guess) {
   require(mg != nullptr && u != nullptr && b != nullptr, "multigrid: null argument");
   require(nrhs >= 1 && max_iters >= 1 && rtol > 0, "multigrid: bad nrhs / max_iters / rtol");
   cudaStream_t s = as_stream(stream);
   Workspace& w = workspace(*mg, nrhs, mg->opt.precision);
-  const int n = mg->lv[0].n;
+  const Level& F = mg->lv[0];
+  const int n = F.n;
   const int K = w.K, np = w.npanels;
   const size_t total = (size_t)n * K * np;
   cudaEvent_t e0, e1;
@@ -965,13 +1236,16 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
       w.bcm.alloc((size_t)n * nrhs);
     }
     DEC_CUDA(cudaMemcpyAsync(w.bcm.p, b, (size_t)n * nrhs * 8, cudaMemcpyHostToDevice, s));
-    DEC_CUDA(cudaMemcpyAsync(w.ucm.p, u, (size_t)n * nrhs * 8, cudaMemcpyHostToDevice, s));
+    if (use_initial_guess) DEC_CUDA(cudaMemcpyAsync(w.ucm.p, u, (size_t)n * nrhs * 8, cudaMemcpyHostToDevice, s));
     bd = w.bcm.p;
     ud = w.ucm.p;
   }
-  k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, K, np, bd, w.B64.p);
-  k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, K, np, ud, w.U64.p);
-  // the first step adds e = 0
+  k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, K, np, F.dperm.p, bd, w.B64.p);
+  if (use_initial_guess)
+    k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, K, np, F.dperm.p, ud, w.U64.p);
+  else
+    DEC_CUDA(cudaMemsetAsync(w.U64.p, 0, total * sizeof(double), s));
+  // the first refinement step adds e = 0
   if (w.prec == 1) DEC_CUDA(cudaMemsetAsync(w.f32[0].x.p, 0, total * sizeof(float), s));
   else DEC_CUDA(cudaMemsetAsync(w.f64[0].x.p, 0, total * sizeof(double), s));
   DEC_CHECK_LAUNCH();
@@ -985,7 +1259,7 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
       DEC_K(1) DEC_K(2) DEC_K(4) DEC_K(8) DEC_K(16) DEC_K(32)
 #undef DEC_K
     }
-    k_reduce_partials<<<(K * np + 127) / 128, 128, 0, s>>>(w.nblocks, K, np, w.partial.p, w.norms.p);
+    k_reduce_partials<<<K * np, 256, 0, s>>>(w.nblocks, K, np, w.partial.p, w.norms.p);
     DEC_CHECK_LAUNCH();
     DEC_CUDA(cudaMemcpyAsync(bn.data(), w.norms.p, bn.size() * 8, cudaMemcpyDeviceToHost, s));
     DEC_CUDA(cudaStreamSynchronize(s));
@@ -1013,7 +1287,7 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
     DEC_CUDA(cudaGraphLaunch(w.graph[G_VCYCLE], s));  // e = V(r)
     ++it;
   }
-  k_from_panels<double, double><<<grid_for((long long)n * nrhs, 256), 256, 0, s>>>(n, nrhs, K, w.U64.p, ud);
+  k_from_panels<double, double><<<grid_for((long long)n * nrhs, 256), 256, 0, s>>>(n, nrhs, K, F.diperm.p, w.U64.p, ud);
   DEC_CHECK_LAUNCH();
   if (host_buffers) DEC_CUDA(cudaMemcpyAsync(u, ud, (size_t)n * nrhs * 8, cudaMemcpyDeviceToHost, s));
   DEC_CUDA(cudaEventRecord(e1, s));
@@ -1034,7 +1308,6 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
   return conv ? DEC_OK : DEC_ERR_NOT_CONVERGED;
 }
 
-
 // ---------------------------------------------------------------------------------------------
 // Profiling and autotuning
 // ---------------------------------------------------------------------------------------------
@@ -1053,6 +1326,7 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
     if (kernel == DEC_KERNEL_SWEEP) {
       SweepPrm<T> prm{};
       prm.mode = mg.opt.smoother == DEC_SMOOTH_JACOBI ? S_JACOBI : S_CHEBN;
+      prm.write_d = 1;  // a middle Chebyshev step: reads and writes the direction
       prm.omega = (T)mg.opt.omega;
       prm.c1 = (T)0.5;
       prm.c2 = (T)0.25;
@@ -1064,14 +1338,13 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
                                              w.partial.p, (size_t)F.n * K);
     } else if (kernel == DEC_KERNEL_RESTRICT) {
       const Level& Cl = mg.lv[level + 1];
-      dim3 gc(grid_for((long long)Cl.n * K, TB, 8), np);
-      k_restrict<T, K><<<gc, TB, 0, s>>>(L.nc, L.Wq, L.ridx.p, L.rs.p, B.x.p, bufs[level + 1].b.p, (size_t)L.n * K,
-                                         (size_t)Cl.n * K);
+      k_restrict<T, K><<<row_grid<T, K>(Cl.n, np), TB, 0, s>>>(L.nc, L.Wq, L.rself.p, L.ridx.p, L.rs.p, B.x.p,
+                                                                bufs[level + 1].b.p, (size_t)L.n * K,
+                                                                (size_t)Cl.n * K);
     } else {
       const Level& Cl = mg.lv[level + 1];
-      dim3 gf(grid_for((long long)L.n * K, TB, 8), np);
-      k_prolong<T, K><<<gf, TB, 0, s>>>(L.n, L.nc, L.pa.p, L.pb.p, bufs[level + 1].x.p, B.x.p, (size_t)L.n * K,
-                                        (size_t)Cl.n * K);
+      k_prolong<T, K><<<row_grid<T, K>(L.n, np), TB, 0, s>>>(L.n, L.pa.p, L.pb.p, bufs[level + 1].x.p, B.x.p,
+                                                              (size_t)L.n * K, (size_t)Cl.n * K);
     }
   };
   launch();  // warm-up
@@ -1087,18 +1360,17 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
   *ms = t / reps;
   if (kernel == DEC_KERNEL_SWEEP) {
     double mat = (double)L.n * (L.W * (4.0 + sz) + 2 * sz);
-    int vecs = (prm_vectors(mg.opt.smoother));
-    *bytes = mat + vecs * (double)nk * sz;
+    *bytes = mat + prm_vectors(mg.opt.smoother) * (double)nk * sz;
   } else if (kernel == DEC_KERNEL_RESIDUAL) {
     const Level& F = mg.lv[0];
     double mat = (double)F.n * (F.W * 12.0 + 8);
     *bytes = mat + (double)F.n * K * np * (8 + 8 + sz);
   } else if (kernel == DEC_KERNEL_RESTRICT) {
     const Level& Cl = mg.lv[level + 1];
-    *bytes = (double)Cl.n * (L.Wq * 4.0 + 8) + (double)nk * sz + (double)Cl.n * K * np * sz;
+    *bytes = (double)Cl.n * ((L.Wq + 1) * 4.0 + 8) + (double)nk * sz + (double)Cl.n * K * np * sz;
   } else {
     const Level& Cl = mg.lv[level + 1];
-    *bytes = (double)(L.n - L.nc) * 8.0 + (double)Cl.n * K * np * sz + 2.0 * nk * sz;
+    *bytes = (double)L.n * 8.0 + (double)Cl.n * K * np * sz + 2.0 * nk * sz;
   }
 }
 
@@ -1130,28 +1402,33 @@ int mg_autotune(dec_mg* mg, int nrhs, int reps, void* stream) {
   const int prec = mg->opt.precision;
   int best = 0;
   double best_t = 1e300;
+  cudaEvent_t e0, e1;
+  DEC_CUDA(cudaEventCreate(&e0));
+  DEC_CUDA(cudaEventCreate(&e1));
   for (int K = 1; K <= 32; K <<= 1) {
     if (K > 1 && (K / 2) >= nrhs) break;  // wider panels would only add padding
     Workspace& w = workspace_k(*mg, nrhs, prec, K);
     if (!w.graph[G_VCYCLE]) w.graph[G_VCYCLE] = capture(*mg, w, G_VCYCLE);
-    cudaEvent_t e0, e1;
-    DEC_CUDA(cudaEventCreate(&e0));
-    DEC_CUDA(cudaEventCreate(&e1));
     DEC_CUDA(cudaGraphLaunch(w.graph[G_VCYCLE], s));
-    DEC_CUDA(cudaEventRecord(e0, s));
-    for (int r = 0; r < reps; ++r) DEC_CUDA(cudaGraphLaunch(w.graph[G_VCYCLE], s));
-    DEC_CUDA(cudaEventRecord(e1, s));
-    DEC_CUDA(cudaEventSynchronize(e1));
-    float t = 0;
-    cudaEventElapsedTime(&t, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    std::vector<float> ts;
+    for (int r = 0; r < std::max(3, reps); ++r) {  // median of single-launch timings
+      DEC_CUDA(cudaEventRecord(e0, s));
+      DEC_CUDA(cudaGraphLaunch(w.graph[G_VCYCLE], s));
+      DEC_CUDA(cudaEventRecord(e1, s));
+      DEC_CUDA(cudaEventSynchronize(e1));
+      float t = 0;
+      cudaEventElapsedTime(&t, e0, e1);
+      ts.push_back(t);
+    }
+    std::sort(ts.begin(), ts.end());
+    double t = ts[ts.size() / 2];
     if (t < best_t) {
       best_t = t;
       best = K;
     }
   }
-  // keep only the chosen workspace for this (nrhs, precision)
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   for (int K = 1; K <= 32; K <<= 1) {
     if (K == best) continue;
     int np = (nrhs + K - 1) / K;
@@ -1160,4 +1437,5 @@ int mg_autotune(dec_mg* mg, int nrhs, int reps, void* stream) {
   mg->tuned[((long long)nrhs << 2) | prec] = best;
   return best;
 }
+
 }  // namespace decb

@@ -12,7 +12,7 @@ const dec_mesh* mg_level_mesh(const dec_mg* mg, int level);
 const dec_op* mg_level_op(const dec_mg* mg, int level);
 void mg_cycles(dec_mg* mg, double* u, const double* b, int nrhs, int cycles, void* stream);
 dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rtol, int max_iters,
-                    dec_solve_report* rep, void* stream, bool host_buffers);
+                    dec_solve_report* rep, void* stream, bool host_buffers, bool use_initial_guess);
 void mg_time_kernel(dec_mg* mg, int kernel, int level, int nrhs, int reps, void* stream, double* ms,
                     double* bytes);
 int mg_autotune(dec_mg* mg, int nrhs, int reps, void* stream);

@@ -171,6 +171,10 @@ typedef struct dec_mg_options {
   int32_t precision;       /* 0: FP64 V-cycles; 1: FP32 V-cycles inside FP64 iterative refinement */
   int32_t rhs_block;       /* right-hand sides per panel (1, 2, 4, 8, 16, 32; 0 = automatic) */
   int32_t mu;              /* 1 = V-cycle, 2 = W-cycle */
+  int32_t inner_cycles;    /* cycles per refinement step of dec_mg_solve (>= 1) */
+  int32_t reorder;         /* 1: store each level in a locality (Morton) order internally */
+  int32_t coarse_max;      /* > 0: cycles stop at the first level with at most this many vertices
+                              (<= 1024) and solve it directly; 0: at the hierarchy's coarsest level */
 } dec_mg_options;
 
 typedef struct dec_solve_report {
@@ -194,9 +198,11 @@ dec_status dec_mg_level_op(const dec_mg* mg, int32_t level, const dec_op** out);
 dec_status dec_mg_cycles(dec_mg* mg, double* u, const double* b, int32_t nrhs, int32_t cycles, void* stream);
 dec_status dec_mg_solve(dec_mg* mg, double* u, const double* b, int32_t nrhs, double rtol,
                         int32_t max_iters, dec_solve_report* report, void* stream);
-/* Same solve with host u / b (pinned or pageable); copies are part of the call. */
+/* Same solve with host u / b (pinned or pageable); copies are part of the call.  With
+ * use_initial_guess = 0 the solve starts from u = 0 and u_host is output only (not copied in). */
 dec_status dec_mg_solve_host(dec_mg* mg, double* u_host, const double* b_host, int32_t nrhs, double rtol,
-                             int32_t max_iters, dec_solve_report* report, void* stream);
+                             int32_t max_iters, int32_t use_initial_guess, dec_solve_report* report,
+                             void* stream);
 
 /* ---- profiling (no counterpart in the reference; its benchmarks print timings only,
  *      test/Benchmarks.jl:128-140) ------------------------------------------------------ */
