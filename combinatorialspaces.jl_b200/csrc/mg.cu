@@ -640,6 +640,195 @@ __global__ void k_split(int n, int Wf, const int32_t* __restrict__ fcol, const d
   }
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// Krylov-CG smoother (the reference's smoother: Krylov.jl cg(A, b, u; itmax = steps) with warm
+// start, atol = rtol = sqrt(eps), called at Multigrid.jl:860 / :871), FP64, one lane per
+// right-hand side.  Every right-hand side j keeps its own scalars in scal[f * ntot + j]:
+enum CgField { CG_GAMMA = 0, CG_PNORM2, CG_EPS, CG_ALPHA, CG_BETA, CG_ACTIVE, CG_UPDP, CG_ITER, CG_NFIELDS };
+// and a kernel sequence per iteration: q = A p (+ p·q partials); reduce + decide α; Δx += α p,
+// r -= α q (+ r·r partials); reduce + decide β; p = r + β p.
+
+template <int K>
+__device__ __forceinline__ void block_partials(double v, double* partial) {
+  __shared__ double sh[TB];
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int st = TB / 2; st >= K; st >>= 1) {
+    if (threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x < K) partial[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * K + threadIdx.x] = sh[threadIdx.x];
+}
+
+// r = b - A x0 (x0 = 0 when zero_x), p = r, Δx = 0; partial r·r.
+template <int K, int W>
+__global__ void __launch_bounds__(TB) k_cg_init(int n, int Wr, const int32_t* __restrict__ col,
+                                                const double* __restrict__ off, const double* __restrict__ diag,
+                                                const double* __restrict__ b, const double* __restrict__ x0,
+                                                int zero_x, double* __restrict__ r, double* __restrict__ p,
+                                                double* __restrict__ dx, double* __restrict__ partial, size_t ps) {
+  const int w = W > 0 ? W : Wr;
+  const int k = threadIdx.x % K;
+  const size_t po = (size_t)blockIdx.y * ps + k;
+  double ss = 0.0;
+  for (int i = blockIdx.x * (TB / K) + threadIdx.x / K; i < n; i += gridDim.x * (TB / K)) {
+    const size_t ik = po + (size_t)i * K;
+    double rv = b[ik];
+    if (!zero_x) {
+      double acc = diag[i] * x0[ik];
+      for (int s = 0; s < w; ++s) acc += off[(size_t)i * w + s] * x0[po + (size_t)col[(size_t)i * w + s] * K];
+      rv = rv - acc;
+    }
+    r[ik] = rv;
+    p[ik] = rv;
+    dx[ik] = 0.0;
+    ss += rv * rv;
+  }
+  block_partials<K>(ss, partial);
+}
+
+// q = A p for active right-hand sides; partial p·q.
+template <int K, int W>
+__global__ void __launch_bounds__(TB) k_cg_spmv(int n, int Wr, const int32_t* __restrict__ col,
+                                                const double* __restrict__ off, const double* __restrict__ diag,
+                                                const double* __restrict__ p, double* __restrict__ q,
+                                                const double* __restrict__ scal, int ntot, double* __restrict__ partial,
+                                                size_t ps) {
+  const int w = W > 0 ? W : Wr;
+  const int k = threadIdx.x % K;
+  const int j = blockIdx.y * K + k;
+  const bool active = scal[CG_ACTIVE * ntot + j] != 0.0;
+  const size_t po = (size_t)blockIdx.y * ps + k;
+  double ss = 0.0;
+  if (active)
+    for (int i = blockIdx.x * (TB / K) + threadIdx.x / K; i < n; i += gridDim.x * (TB / K)) {
+      const size_t ik = po + (size_t)i * K;
+      double pi = p[ik];
+      double acc = diag[i] * pi;
+      for (int s = 0; s < w; ++s) acc += off[(size_t)i * w + s] * p[po + (size_t)col[(size_t)i * w + s] * K];
+      q[ik] = acc;
+      ss += pi * acc;
+    }
+  block_partials<K>(ss, partial);
+}
+
+// Δx += α p, r -= α q for active right-hand sides; partial r·r.
+template <int K>
+__global__ void __launch_bounds__(TB) k_cg_axpy(int n, const double* __restrict__ p, const double* __restrict__ q,
+                                                double* __restrict__ dx, double* __restrict__ r,
+                                                const double* __restrict__ scal, int ntot, double* __restrict__ partial,
+                                                size_t ps) {
+  const int k = threadIdx.x % K;
+  const int j = blockIdx.y * K + k;
+  const bool active = scal[CG_ACTIVE * ntot + j] != 0.0;
+  const double a = scal[CG_ALPHA * ntot + j];
+  const size_t po = (size_t)blockIdx.y * ps + k;
+  double ss = 0.0;
+  if (active)
+    for (int i = blockIdx.x * (TB / K) + threadIdx.x / K; i < n; i += gridDim.x * (TB / K)) {
+      const size_t ik = po + (size_t)i * K;
+      dx[ik] += a * p[ik];
+      double rv = r[ik] + (-a) * q[ik];
+      r[ik] = rv;
+      ss += rv * rv;
+    }
+  block_partials<K>(ss, partial);
+}
+
+// p = r + β p where the right-hand side continues.
+template <int K>
+__global__ void __launch_bounds__(TB) k_cg_pupd(int n, const double* __restrict__ r, double* __restrict__ p,
+                                                const double* __restrict__ scal, int ntot, size_t ps) {
+  const int k = threadIdx.x % K;
+  const int j = blockIdx.y * K + k;
+  if (scal[CG_UPDP * ntot + j] == 0.0) return;
+  const double bt = scal[CG_BETA * ntot + j];
+  const size_t po = (size_t)blockIdx.y * ps + k;
+  for (int i = blockIdx.x * (TB / K) + threadIdx.x / K; i < n; i += gridDim.x * (TB / K)) {
+    const size_t ik = po + (size_t)i * K;
+    p[ik] = r[ik] + bt * p[ik];
+  }
+}
+
+// x = Δx + x0 (Krylov adds the warm start back at the end).
+template <int K>
+__global__ void __launch_bounds__(TB) k_cg_finish(int n, const double* __restrict__ x0, int zero_x,
+                                                  const double* __restrict__ dx, double* __restrict__ out, size_t ps) {
+  const int k = threadIdx.x % K;
+  const size_t po = (size_t)blockIdx.y * ps + k;
+  for (int i = blockIdx.x * (TB / K) + threadIdx.x / K; i < n; i += gridDim.x * (TB / K)) {
+    const size_t ik = po + (size_t)i * K;
+    out[ik] = zero_x ? dx[ik] : dx[ik] + x0[ik];
+  }
+}
+
+enum CgPhase { CG_PH_INIT = 0, CG_PH_ALPHA = 1, CG_PH_BETA = 2 };
+
+// One CTA per right-hand side: sum the block partials (fixed tree order) and take the CG
+// decisions of Krylov.jl's cg for that phase.
+__global__ void __launch_bounds__(256) k_cg_scalar(int phase, int nb, int K, int ntot, int itmax,
+                                                   const double* __restrict__ partial, double* __restrict__ scal) {
+  const int j = blockIdx.x;
+  const int pnl = j / K, k = j % K;
+  double s = 0.0;
+  for (int bq = threadIdx.x; bq < nb; bq += blockDim.x) s += partial[((size_t)pnl * nb + bq) * K + k];
+  __shared__ double sh[256];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  const double v = sh[0];
+  const double eps = 2.220446049250313e-16, rt = 1.4901161193847656e-08;  // eps(Float64), sqrt(eps)
+  double* S = scal;
+  auto F = [&](int f) -> double& { return S[(size_t)f * ntot + j]; };
+  if (phase == CG_PH_INIT) {
+    const double gamma = v;
+    F(CG_GAMMA) = gamma;
+    F(CG_ITER) = 0.0;
+    F(CG_UPDP) = 0.0;
+    F(CG_ALPHA) = 0.0;
+    if (gamma == 0.0) {  // x0 is a zero-residual solution: return it
+      F(CG_ACTIVE) = 0.0;
+      return;
+    }
+    const double rnorm = sqrt(gamma);
+    F(CG_EPS) = rt + rt * rnorm;
+    F(CG_PNORM2) = gamma;
+    const bool solved = rnorm <= F(CG_EPS);
+    F(CG_ACTIVE) = (!solved && itmax > 0) ? 1.0 : 0.0;
+  } else if (phase == CG_PH_ALPHA) {
+    if (F(CG_ACTIVE) == 0.0) return;
+    const double pAp = v, pn2 = F(CG_PNORM2);
+    if (pAp <= eps * pn2 && fabs(pAp) <= eps * pn2) {  // zero curvature
+      F(CG_ACTIVE) = 0.0;
+      F(CG_ALPHA) = 0.0;
+      return;
+    }
+    F(CG_ALPHA) = F(CG_GAMMA) / pAp;
+  } else {
+    F(CG_UPDP) = 0.0;
+    if (F(CG_ACTIVE) == 0.0) return;
+    const double gnext = v;
+    const double rnorm = sqrt(gnext);
+    const bool solved = (rnorm <= F(CG_EPS)) || (rnorm + 1.0 <= 1.0);
+    const double iter = F(CG_ITER) + 1.0;
+    F(CG_ITER) = iter;
+    if (!solved) {
+      const double beta = gnext / F(CG_GAMMA);
+      F(CG_BETA) = beta;
+      F(CG_PNORM2) = gnext + beta * beta * F(CG_PNORM2);
+      F(CG_GAMMA) = gnext;
+    }
+    const bool more = !solved && iter < (double)itmax;
+    F(CG_UPDP) = more ? 1.0 : 0.0;
+    F(CG_ACTIVE) = more ? 1.0 : 0.0;
+  }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Hierarchy
 // ---------------------------------------------------------------------------------------------
@@ -662,6 +851,7 @@ struct Level {
 template <class T>
 struct LevelBufs {
   DArr<T> x, y, b, d;  // x / y ping-pong, b right-hand side, d Chebyshev direction
+  DArr<T> q, e;        // CG smoother: A p and the accumulated correction Δx (CG mode only)
 };
 
 struct Workspace {
@@ -670,6 +860,7 @@ struct Workspace {
   std::vector<LevelBufs<double>> f64;
   DArr<double> B64, U64;      // finest FP64 panels
   DArr<double> partial, norms;
+  DArr<double> scal;          // CG smoother: per-right-hand-side scalars (CgField x K*npanels)
   DArr<double> ucm, bcm;      // column-major device copies for host-buffer solves
   int nblocks = 0;
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};  // GraphKind
@@ -850,7 +1041,8 @@ static void build_transfers(Level& F, const Level& C, const HostLevel& c) {
 
 dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
   require(o.levels >= 0 && o.levels <= 12, "multigrid: levels must be in [0, 12]");
-  require(o.smoother >= 0 && o.smoother <= 1, "multigrid: smoother must be DEC_SMOOTH_JACOBI or DEC_SMOOTH_CHEBYSHEV");
+  require(o.smoother >= 0 && o.smoother <= 2, "multigrid: unknown smoother");
+  require(o.smoother != DEC_SMOOTH_CG || o.precision == 0, "multigrid: the CG smoother runs in FP64 (precision 0)");
   require(o.pre >= 0 && o.post >= 0 && o.pre <= 16 && o.post <= 16, "multigrid: sweeps must be in [0, 16]");
   require(o.mu == 1 || o.mu == 2, "multigrid: mu must be 1 (V) or 2 (W)");
   require(o.precision == 0 || o.precision == 1, "multigrid: precision must be 0 or 1");
@@ -900,8 +1092,9 @@ dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
         mg->lc = l;
         break;
       }
+  if (o.smoother == DEC_SMOOTH_CG) mg->lc = o.levels;  // the reference runs CG on its coarsest level
   const Level& C = mg->lv[mg->lc];
-  if (o.coarse_solver == 0) {
+  if (o.coarse_solver == 0 && o.smoother != DEC_SMOOTH_CG) {
     auto ai = dense_inverse(*C.op, C.n);
     std::vector<double> ap((size_t)C.n * C.n);
     for (int i = 0; i < C.n; ++i)
@@ -996,12 +1189,91 @@ static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool z
   return x;
 }
 
+
+// steps iterations of the Krylov CG smoother on level L from x (zero if zero_x); returns the
+// buffer holding x.  FP64 only.
+template <int K>
+static double* cg_smooth(const dec_mg& mg, Workspace& w, const Level& L, LevelBufs<double>& B, double* x, bool zero_x,
+                         int steps, int np, cudaStream_t s) {
+  if (steps == 0) return x;  // steps == 0 skips the smoother (Multigrid.jl:860, issue #178)
+  const int ntot = K * np;
+  const size_t ps = (size_t)L.n * K;
+  dim3 g(grid_for(L.n, TB / K, 8), np);
+  const int nb = (int)g.x;
+  double* r = (x == B.x.p) ? B.y.p : B.x.p;  // r in the free ping-pong buffer
+  double* pp = B.d.p;
+  if (L.W == 6)
+    k_cg_init<K, 6><<<g, TB, 0, s>>>(L.n, L.W, L.col.p, L.off64.p, L.diag64.p, B.b.p, x, zero_x ? 1 : 0, r, pp,
+                                     B.e.p, w.partial.p, ps);
+  else
+    k_cg_init<K, 0><<<g, TB, 0, s>>>(L.n, L.W, L.col.p, L.off64.p, L.diag64.p, B.b.p, x, zero_x ? 1 : 0, r, pp,
+                                     B.e.p, w.partial.p, ps);
+  k_cg_scalar<<<ntot, 256, 0, s>>>(CG_PH_INIT, nb, K, ntot, steps, w.partial.p, w.scal.p);
+  for (int it = 0; it < steps; ++it) {
+    if (L.W == 6)
+      k_cg_spmv<K, 6><<<g, TB, 0, s>>>(L.n, L.W, L.col.p, L.off64.p, L.diag64.p, pp, B.q.p, w.scal.p, ntot,
+                                       w.partial.p, ps);
+    else
+      k_cg_spmv<K, 0><<<g, TB, 0, s>>>(L.n, L.W, L.col.p, L.off64.p, L.diag64.p, pp, B.q.p, w.scal.p, ntot,
+                                       w.partial.p, ps);
+    k_cg_scalar<<<ntot, 256, 0, s>>>(CG_PH_ALPHA, nb, K, ntot, steps, w.partial.p, w.scal.p);
+    k_cg_axpy<K><<<g, TB, 0, s>>>(L.n, pp, B.q.p, B.e.p, r, w.scal.p, ntot, w.partial.p, ps);
+    k_cg_scalar<<<ntot, 256, 0, s>>>(CG_PH_BETA, nb, K, ntot, steps, w.partial.p, w.scal.p);
+    if (it + 1 < steps) k_cg_pupd<K><<<g, TB, 0, s>>>(L.n, r, pp, w.scal.p, ntot, ps);
+  }
+  // x + Δx goes into the residual buffer (free again), which becomes the result
+  k_cg_finish<K><<<g, TB, 0, s>>>(L.n, x, zero_x ? 1 : 0, B.e.p, r, ps);
+  DEC_CHECK_LAUNCH();
+  return r;
+}
+
+
+template <class T, int K>
+static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bufs, int l, T* x, bool zero_x, int mu,
+                   int np, cudaStream_t s);
+
+// _multigrid_μ_cycle, Multigrid.jl:857-872, with the Krylov CG smoother: CG (steps) ; if the
+// coarsest level, return ; r = b - A u ; restrict ; recurse (twice for μ = 2) ; u += P z ; CG.
+template <int K>
+static double* cg_mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<double>>& bufs, int l, double* x,
+                           bool zero_x, int mu, int np, cudaStream_t s) {
+  const Level& L = mg.lv[l];
+  LevelBufs<double>& B = bufs[l];
+  const int last = (int)mg.lv.size() - 1;
+  const int steps_pre = mg.opt.pre, steps_post = mg.opt.post;
+  x = cg_smooth<K>(mg, w, L, B, x, zero_x, steps_pre, np, s);
+  if (steps_pre > 0) zero_x = false;
+  if (l >= last) {
+    if (zero_x) DEC_CUDA(cudaMemsetAsync(x, 0, (size_t)L.n * K * np * sizeof(double), s));
+    return x;
+  }
+  double* r = (x == B.x.p) ? B.y.p : B.x.p;
+  SweepPrm<double> prm{};
+  prm.mode = S_RESID;
+  prm.zero_x = zero_x ? 1 : 0;
+  launch_sweep<double, K>(L, B.b.p, x, r, nullptr, prm, np, s);
+  const Level& Cl = mg.lv[l + 1];
+  LevelBufs<double>& Cb = bufs[l + 1];
+  launch_pdl(k_restrict<double, K>, row_grid<double, K>(Cl.n, np), dim3(TB), s, L.nc, L.Wq,
+             (const int32_t*)L.rself.p, (const int32_t*)L.ridx.p, (const double*)L.rs.p, (const double*)r, Cb.b.p,
+             (size_t)L.n * K, (size_t)Cl.n * K);
+  double* z = cg_mu_cycle<K>(mg, w, bufs, l + 1, Cb.x.p, true, mu, np, s);
+  if (mu > 1) z = cg_mu_cycle<K>(mg, w, bufs, l + 1, z, false, mu - 1, np, s);
+  if (zero_x) DEC_CUDA(cudaMemsetAsync(x, 0, (size_t)L.n * K * np * sizeof(double), s));
+  launch_pdl(k_prolong<double, K>, row_grid<double, K>(L.n, np), dim3(TB), s, L.n, (const int32_t*)L.pa.p,
+             (const int32_t*)L.pb.p, (const double*)z, x, (size_t)L.n * K, (size_t)Cl.n * K);
+  return cg_smooth<K>(mg, w, L, B, x, false, steps_post, np, s);
+}
+
 // One μ-cycle at level l on (b = B[l].b, initial guess x); returns the buffer with the result.
 template <class T, int K>
-static T* mu_cycle(const dec_mg& mg, std::vector<LevelBufs<T>>& bufs, int l, T* x, bool zero_x, int mu, int np,
-                   cudaStream_t s) {
+static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bufs, int l, T* x, bool zero_x, int mu,
+                   int np, cudaStream_t s) {
   const Level& L = mg.lv[l];
   LevelBufs<T>& B = bufs[l];
+  if constexpr (std::is_same<T, double>::value) {
+    if (mg.opt.smoother == DEC_SMOOTH_CG) return cg_mu_cycle<K>(mg, w, bufs, l, x, zero_x, mu, np, s);
+  }
   if (l == mg.lc) {
     launch_pdl(k_coarse<T, K>, dim3(grid_for(L.n, TB / K, 64), np), dim3(TB), s, L.n, (const double*)mg.ainv.p,
                (const T*)B.b.p, B.x.p, (size_t)L.n * K);
@@ -1020,8 +1292,8 @@ static T* mu_cycle(const dec_mg& mg, std::vector<LevelBufs<T>>& bufs, int l, T* 
   launch_pdl(k_restrict<T, K>, row_grid<T, K>(Cl.n, np), dim3(TB), s, L.nc, L.Wq, (const int32_t*)L.rself.p,
              (const int32_t*)L.ridx.p, (const double*)L.rs.p, (const T*)r, Cb.b.p, (size_t)L.n * K,
              (size_t)Cl.n * K);
-  T* z = mu_cycle<T, K>(mg, bufs, l + 1, Cb.x.p, true, mu, np, s);
-  if (mu > 1) z = mu_cycle<T, K>(mg, bufs, l + 1, z, false, mu - 1, np, s);
+  T* z = mu_cycle<T, K>(mg, w, bufs, l + 1, Cb.x.p, true, mu, np, s);
+  if (mu > 1) z = mu_cycle<T, K>(mg, w, bufs, l + 1, z, false, mu - 1, np, s);
   if (zero_x) {  // x is all zero: start it from the prolonged correction
     DEC_CUDA(cudaMemsetAsync(x, 0, (size_t)L.n * K * np * sizeof(T), s));
   }
@@ -1041,6 +1313,12 @@ static void alloc_bufs(const dec_mg& mg, std::vector<LevelBufs<T>>& bufs, int K,
     bufs[l].d.alloc(n);
     for (DArr<T>* a : {&bufs[l].x, &bufs[l].y, &bufs[l].b, &bufs[l].d})
       DEC_CUDA(cudaMemset(a->p, 0, a->bytes()));
+    if (mg.opt.smoother == DEC_SMOOTH_CG) {
+      bufs[l].q.alloc(n);
+      bufs[l].e.alloc(n);
+      DEC_CUDA(cudaMemset(bufs[l].q.p, 0, bufs[l].q.bytes()));
+      DEC_CUDA(cudaMemset(bufs[l].e.p, 0, bufs[l].e.bytes()));
+    }
   }
 }
 
@@ -1087,7 +1365,7 @@ template <class T, int K>
 static void enqueue_vcycle_T(dec_mg& mg, Workspace& w, cudaStream_t s, std::vector<LevelBufs<T>>& bufs) {
   const size_t total = (size_t)mg.lv[0].n * K * w.npanels;
   T* e = bufs[0].x.p;
-  for (int c = 0; c < mg.opt.inner_cycles; ++c) e = mu_cycle<T, K>(mg, bufs, 0, e, c == 0, mg.opt.mu, w.npanels, s);
+  for (int c = 0; c < mg.opt.inner_cycles; ++c) e = mu_cycle<T, K>(mg, w, bufs, 0, e, c == 0, mg.opt.mu, w.npanels, s);
   if (e != bufs[0].x.p)
     DEC_CUDA(cudaMemcpyAsync(bufs[0].x.p, e, total * sizeof(T), cudaMemcpyDeviceToDevice, s));
   DEC_CHECK_LAUNCH();
@@ -1100,7 +1378,7 @@ static void enqueue_cycle(dec_mg& mg, Workspace& w, cudaStream_t s) {
   const size_t total = (size_t)mg.lv[0].n * K * w.npanels;
   DEC_CUDA(cudaMemcpyAsync(bufs[0].b.p, w.B64.p, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
   DEC_CUDA(cudaMemcpyAsync(bufs[0].x.p, w.U64.p, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  double* x = mu_cycle<double, K>(mg, bufs, 0, bufs[0].x.p, false, mg.opt.mu, w.npanels, s);
+  double* x = mu_cycle<double, K>(mg, w, bufs, 0, bufs[0].x.p, false, mg.opt.mu, w.npanels, s);
   DEC_CUDA(cudaMemcpyAsync(w.U64.p, x, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
   DEC_CHECK_LAUNCH();
 }
@@ -1183,6 +1461,10 @@ static Workspace& workspace_k(dec_mg& mg, int nrhs, int prec, int K) {
   w->nblocks = (int)std::max<long long>(1, std::min<long long>(8LL * num_sms(), ((long long)mg.lv[0].n * K + TB - 1) / TB));
   w->partial.alloc((size_t)w->nblocks * K * np);
   w->norms.alloc((size_t)K * np);
+  if (mg.opt.smoother == DEC_SMOOTH_CG) {
+    w->scal.alloc((size_t)CG_NFIELDS * K * np);
+    DEC_CUDA(cudaMemset(w->scal.p, 0, w->scal.bytes()));
+  }
   DEC_CUDA(cudaMemset(w->B64.p, 0, w->B64.bytes()));
   DEC_CUDA(cudaMemset(w->U64.p, 0, w->U64.bytes()));
   auto& ref = *w;

@@ -157,3 +157,65 @@ def test_singular_coarse_operator_is_reported(O, dec):
     coarse = O.icosahedron()
     with pytest.raises(dec.DecError, match="singular"):
         dec.MultigridData(coarse, 1, shift=0.0, center="circumcenter", project_radius=1.0)
+
+
+# ---- the reference's own algorithm on the GPU: V/W-cycles with the Krylov CG smoother ----------
+
+def _ref_grid_setup(O, dec, steps, mu):
+    # test/Multigrid.jl:54-90: triangulated_grid(1,1,1/4,√3/8), 4 binary levels, circumcentric
+    # duals, the singular Laplacian (shift 0), steps CG iterations per smoothing.
+    s = O.triangulated_grid(1, 1, 1 / 4, np.sqrt(3) / 8, False)
+    md = O.build_mg(s, 4, O.CIRCUMCENTER, 0.0, 0.0, steps)
+    mg = dec.MultigridData(s, 4, shift=0.0, center="circumcenter", smoother=2, pre=steps, post=steps, mu=mu)
+    L = csc(md.op(0))
+    return md, mg, L
+
+
+@pytest.mark.parametrize("mu", [1, 2])
+def test_cg_cycles_match_oracle(O, dec, mu):
+    """GPU mu-cycles with the Krylov CG smoother against the oracle's restatement of
+    _multigrid_μ_cycle + Krylov.jl cg (reduction order differs: 1e-9 relative)."""
+    md, mg, L = _ref_grid_setup(O, dec, 3, mu)
+    n = L.shape[0]
+    b = L @ ((uniform(0, n) + 1) / 2)
+    u0 = np.zeros(n)
+    for cycles in (1, 2, 4):
+        ref = O.mu_cycles(md, u0, b, cycles, mu)
+        u = mg.cycles(torch.zeros(n, dtype=torch.float64, device="cuda"), torch.tensor(b, device="cuda"), cycles)
+        np.testing.assert_allclose(u.cpu().numpy(), ref, rtol=1e-9, atol=1e-9 * np.abs(ref).max())
+
+
+def test_cg_cycles_reference_thresholds(O, dec):
+    """test/Multigrid.jl:67-78 on the GPU: 5 V-cycles and 5 W-cycles reach < 1e-7."""
+    for mu in (1, 2):
+        md, mg, L = _ref_grid_setup(O, dec, 3, mu)
+        n = L.shape[0]
+        b = L @ ((uniform(0, n) + 1) / 2)
+        u = mg.cycles(torch.zeros(n, dtype=torch.float64, device="cuda"), torch.tensor(b, device="cuda"), 5)
+        u = u.cpu().numpy()
+        assert np.linalg.norm(L @ u - b) / np.linalg.norm(b) < 1e-7
+
+
+def test_cg_zero_steps_does_no_smoothing(O, dec):
+    """Issue #178 (test/Multigrid.jl:151-170): steps = 0 skips the smoother entirely."""
+    md0, mg0, L = _ref_grid_setup(O, dec, 0, 1)
+    md1, mg1, _ = _ref_grid_setup(O, dec, 1, 1)
+    n = L.shape[0]
+    b = L @ ((uniform(0, n) + 1) / 2)
+    z = torch.zeros(n, dtype=torch.float64, device="cuda")
+    bt = torch.tensor(b, device="cuda")
+    r0 = np.linalg.norm(L @ mg0.cycles(z.clone(), bt, 5).cpu().numpy() - b)
+    r1 = np.linalg.norm(L @ mg1.cycles(z.clone(), bt, 5).cpu().numpy() - b)
+    assert r1 < r0
+    np.testing.assert_allclose(mg0.cycles(z.clone(), bt, 5).cpu().numpy(), O.mu_cycles(md0, np.zeros(n), b, 5, 1),
+                               rtol=1e-12, atol=1e-12)
+
+
+def test_cg_cycles_multi_rhs_match_single(O, dec):
+    md, mg, L = _ref_grid_setup(O, dec, 3, 1)
+    n = L.shape[0]
+    B = np.stack([L @ ((uniform(10 + j, n) + 1) / 2) for j in range(3)])
+    U = mg.cycles(torch.zeros((3, n), dtype=torch.float64, device="cuda"), torch.tensor(B, device="cuda"), 3)
+    for j in range(3):
+        ref = O.mu_cycles(md, np.zeros(n), B[j], 3, 1)
+        np.testing.assert_allclose(U[j].cpu().numpy(), ref, rtol=1e-9, atol=1e-9 * np.abs(ref).max())
