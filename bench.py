@@ -126,6 +126,101 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def measure_operators(dec, peak):
+    """HBM roofline of the DEC operator kernels: each kernel timed alone with CUDA events, L2
+    flushed (a 256 MB write) before every launch, on icosphere L9 (circumcentric duals) and a
+    2049x2049 grid (barycentric duals, a 9x9 triangulated grid binary-refined 8 times), FP64 and
+    FP32.  Algorithmic bytes: every streamed array once, each gathered form once (int32 indices)."""
+    import torch
+
+    flush = torch.empty(64 * 2 ** 20, dtype=torch.float32, device="cuda")
+
+    def time_op(fn, reps=10):
+        fn()
+        tot = 0.0
+        for _ in range(reps):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot / reps
+
+    big_grid = dec.meshes.triangulated_grid(8, 8, 1.0, 1.0, False)
+    for _ in range(8):
+        big_grid = dec.meshes.refine_binary(big_grid)
+    cases = [("icosphere_L9", dec.meshes.icosphere(9), "circumcenter"), ("grid_2049x2049", big_grid, "barycenter")]
+    out = {}
+    for name, m, center in cases:
+        g = dec.Mesh(m.points, m.ev0, m.ev1, m.te0, m.te1, m.te2, m.edge_orientation, m.tri_orientation,
+                     center=center)
+        nv, ne, nt = g.nv, g.ne, g.nt
+        width = int(np.bincount(np.concatenate([m.ev0, m.ev1]), minlength=nv).max()) + 1
+        res = {"nv": nv, "ne": ne, "nt": nt}
+        for dt, tdt, sz in (("float64", torch.float64, 8), ("float32", torch.float32, 4)):
+            f = torch.rand(nv, dtype=tdt, device="cuda")
+            a = torch.rand(ne, dtype=tdt, device="cuda")
+            b = torch.rand(ne, dtype=tdt, device="cuda")
+            tt = torch.rand(nt, dtype=tdt, device="cuda")
+            oe = torch.empty(ne, dtype=tdt, device="cuda")
+            ot = torch.empty(nt, dtype=tdt, device="cuda")
+            ov = torch.empty(nv, dtype=tdt, device="cuda")
+            w01 = dec.dec_wedge_product(0, 1, g, dt)
+            w11 = dec.dec_wedge_product(1, 1, g, dt)
+            w02 = dec.dec_wedge_product(0, 2, g, dt)
+            d0 = dec.dec_differential(0, g, dt)
+            d1 = dec.dec_differential(1, g, dt)
+            L = dec.laplace_beltrami(g, dt)
+            s1 = dec.hodge_operator(1, g, dtype=dt)
+            ops = {
+                "wedge01": (lambda: w01(f, a, oe), ne * (8 + 2 * sz) + nv * sz),
+                "wedge11": (lambda: w11(a, b, ot), nt * (12 + 4 * sz) + 2 * ne * sz),
+                "wedge02": (lambda: w02(f, tt, ot), nt * (12 + 5 * sz) + nv * sz),
+                "d0": (lambda: d0.apply(f, oe), ne * (9 + sz) + nv * sz),
+                "d1": (lambda: d1.apply(a, ot), nt * (13 + sz) + ne * sz),
+                "laplacian": (lambda: L.apply(f, ov), nv * width * (4 + sz) + 2 * nv * sz),
+                "star1": (lambda: s1.apply(a, oe), 3 * ne * sz),
+            }
+            for op, (fn, by) in ops.items():
+                ms = time_op(fn)
+                gbs = by / (ms * 1e-3) / 1e9
+                res[f"{op}_{dt}"] = {"us": round(ms * 1e3, 2), "GB/s": round(gbs, 1), "frac": round(gbs / peak, 3)}
+        out[name] = res
+        del g
+        torch.cuda.empty_cache()
+
+    # BASELINE config 1: 128 x 128 grid, barycentric duals, FP64, 100 repetitions each
+    # (L2-resident: µs per operation, not an HBM figure).
+    m = dec.meshes.triangulated_grid(127, 127, 1.0, 1.0, False)
+    g = dec.Mesh(m.points, m.ev0, m.ev1, m.te0, m.te1, m.te2, m.edge_orientation, m.tri_orientation,
+                 center="barycenter")
+    f = torch.tensor(dec.meshes.uniform(0, g.nv), device="cuda")
+    al = torch.tensor(dec.meshes.uniform(1, g.ne), device="cuda")
+    be = torch.tensor(dec.meshes.uniform(2, g.ne), device="cuda")
+    w01, w11, w02 = (dec.dec_wedge_product(0, 1, g), dec.dec_wedge_product(1, 1, g),
+                     dec.dec_wedge_product(0, 2, g))
+    d1, L = dec.dec_differential(1, g), dec.laplace_beltrami(g)
+    d1a = torch.empty(g.nt, dtype=torch.float64, device="cuda")
+    cfg1 = {}
+    for name, fn in (("wedge01(f,alpha)", lambda: w01(f, al)), ("wedge11(alpha,beta)", lambda: w11(al, be)),
+                     ("wedge02(f,d1 alpha)", lambda: w02(f, d1.apply(al, d1a))), ("laplacian f", lambda: L.apply(f))):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(100):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        cfg1[name] = round(e0.elapsed_time(e1) * 10, 2)  # µs per op (ms / 100 * 1000)
+    out["grid_128x128_config1_us_per_op"] = cfg1
+    return out
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -324,6 +419,9 @@ def run_ours(args):
     achieved = algo_bytes / (ms * 1e-3) / 1e9
     traffic = traffic_per_launch("k_sweep")
 
+    # --- DEC operator kernels (wedges, d, star, Laplacian) at full size ---
+    operators = measure_operators(dec, peak) if (rank == 0 and not args.no_ops) else None
+
     # --- CPU baseline (rank 0, N = 1 only): the reference algorithm on the host cores ---
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -367,6 +465,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": bytes_vec},
             "gpu_launches": launches,
             "clocks": clocks,
+            "operators": operators,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -385,6 +484,7 @@ def main():
     ap.add_argument("--coarse-max", type=int, default=170, dest="coarse_max")
     ap.add_argument("--rhs-block", type=int, default=0, dest="rhs_block")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ops", action="store_true", help="skip the operator-kernel roofline section")
     ap.add_argument("--profile", action="store_true",
                     help="run only the timed mixed-precision solves (inside an NVTX range 'timed')")
     args = ap.parse_args()

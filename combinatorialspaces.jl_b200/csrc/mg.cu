@@ -984,7 +984,7 @@ static void build_level_operator(Level& L, double shift, bool reorder) {
   for (int i = 0; i < L.n; ++i) L.iperm[L.perm[i]] = i;
   L.dperm.upload(L.perm);
   L.diperm.upload(L.iperm);
-  L.W = std::max(1, L.op->W - 1);
+  L.W = std::max(1, L.mesh->m.max_v2e);  // off-diagonal slots: the maximum vertex degree
   L.col.alloc((size_t)L.n * L.W);
   L.off64.alloc((size_t)L.n * L.W);
   L.diag64.alloc(L.n);

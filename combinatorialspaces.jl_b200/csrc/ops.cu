@@ -20,11 +20,18 @@ __device__ __forceinline__ T epilogue(T s, T yold, T alpha, T beta, bool has_bet
   return alpha * s + beta * yold;
 }
 
-// d0 x: row e = σ_e (x[∂v0] - x[∂v1]), src/FastDEC.jl:471-494.
+// Elementwise kernels handle kOpItems outputs per thread, spaced one block apart, with all
+// loads issued before any use.
+constexpr int kOpItems = 4;
+constexpr int kOpThreads = 256;
+
+// d0 x: row e = σ_e (x[∂v0] - x[∂v1]), src/FastDEC.jl:471-494.  (One edge per thread: with
+// several edges per thread these gather-bound kernels measured slower on B200.)
 template <class T>
-__global__ void k_d0(int ne, const int32_t* __restrict__ ev0, const int32_t* __restrict__ ev1,
-                     const int8_t* __restrict__ es, const T* __restrict__ x, T* __restrict__ y, T alpha,
-                     T beta, bool hb) {
+__global__ void __launch_bounds__(kOpThreads) k_d0(int ne, const int32_t* __restrict__ ev0,
+                                                   const int32_t* __restrict__ ev1, const int8_t* __restrict__ es,
+                                                   const T* __restrict__ x, T* __restrict__ y, T alpha, T beta,
+                                                   bool hb) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
     T s = (T)__ldcs(es + e) * (__ldg(x + __ldcs(ev0 + e)) - __ldg(x + __ldcs(ev1 + e)));
     y[e] = epilogue(s, hb ? y[e] : T(0), alpha, beta, hb);
@@ -34,9 +41,10 @@ __global__ void k_d0(int ne, const int32_t* __restrict__ ev0, const int32_t* __r
 // d1 x: row t = τ(σ0 x[∂e0] - σ1 x[∂e1] + σ2 x[∂e2]), src/FastDEC.jl:496-524, summed in
 // increasing edge order.
 template <class T>
-__global__ void k_d1(int nt, const int32_t* __restrict__ c0, const int32_t* __restrict__ c1,
-                     const int32_t* __restrict__ c2, const uint8_t* __restrict__ neg, const T* __restrict__ x,
-                     T* __restrict__ y, T alpha, T beta, bool hb) {
+__global__ void __launch_bounds__(kOpThreads) k_d1(int nt, const int32_t* __restrict__ c0,
+                                                   const int32_t* __restrict__ c1, const int32_t* __restrict__ c2,
+                                                   const uint8_t* __restrict__ neg, const T* __restrict__ x,
+                                                   T* __restrict__ y, T alpha, T beta, bool hb) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
     uint8_t n = __ldcs(neg + t);
     T a = __ldg(x + __ldcs(c0 + t)), b = __ldg(x + __ldcs(c1 + t)), c = __ldg(x + __ldcs(c2 + t));
@@ -64,23 +72,70 @@ __global__ void k_signed_rows(int n, const int32_t* __restrict__ ptr, const int3
 }
 
 template <class T>
-__global__ void k_diag(int n, const T* __restrict__ d, const T* __restrict__ x, T* __restrict__ y, T alpha,
-                       T beta, bool hb) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    y[i] = epilogue(__ldcs(d + i) * __ldcs(x + i), hb ? y[i] : T(0), alpha, beta, hb);
+__global__ void __launch_bounds__(kOpThreads) k_diag(int n, const T* __restrict__ d, const T* __restrict__ x,
+                                                     T* __restrict__ y, T alpha, T beta, bool hb) {
+  for (long long base = (long long)blockIdx.x * kOpThreads * kOpItems; base < n;
+       base += (long long)gridDim.x * kOpThreads * kOpItems) {
+    T dv[kOpItems], xv[kOpItems];
+#pragma unroll
+    for (int j = 0; j < kOpItems; ++j) {
+      long long i = base + j * kOpThreads + threadIdx.x;
+      if (i < n) {
+        dv[j] = __ldcs(d + i);
+        xv[j] = __ldcs(x + i);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kOpItems; ++j) {
+      long long i = base + j * kOpThreads + threadIdx.x;
+      if (i < n) y[i] = epilogue(dv[j] * xv[j], hb ? y[i] : T(0), alpha, beta, hb);
+    }
+  }
 }
 
-// Row-major ELL SpMV, one thread per row (padding: column -1).
-template <class T>
-__global__ void k_ell(int n, int W, const int32_t* __restrict__ col, const T* __restrict__ val,
-                      const T* __restrict__ x, T* __restrict__ y, T alpha, T beta, bool hb) {
+// Row-major ELL SpMV, one thread per row (padding: column -1).  Rows are padded to a multiple
+// of 4 entries so each row's columns and values come in with 16-byte vector loads; the row sum
+// runs in column order.
+template <class T, int WP>
+__global__ void __launch_bounds__(kOpThreads) k_ell(int n, int W, const int32_t* __restrict__ col,
+                                                    const T* __restrict__ val, const T* __restrict__ x,
+                                                    T* __restrict__ y, T alpha, T beta, bool hb) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     T s = T(0);
-    const int32_t* c = col + (size_t)i * W;
-    const T* v = val + (size_t)i * W;
-    for (int q = 0; q < W; ++q) {
-      int j = __ldcs(c + q);
-      if (j >= 0) s += __ldcs(v + q) * __ldg(x + j);
+    if constexpr (WP > 0) {
+      int c[WP];
+      T v[WP];
+#pragma unroll
+      for (int q = 0; q < WP; q += 4) {
+        int4 cc = __ldcs(reinterpret_cast<const int4*>(col + (size_t)i * WP + q));
+        c[q] = cc.x; c[q + 1] = cc.y; c[q + 2] = cc.z; c[q + 3] = cc.w;
+      }
+      if constexpr (sizeof(T) == 8) {
+#pragma unroll
+        for (int q = 0; q < WP; q += 2) {
+          double2 vv = __ldcs(reinterpret_cast<const double2*>(val + (size_t)i * WP + q));
+          v[q] = vv.x; v[q + 1] = vv.y;
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < WP; q += 4) {
+          float4 vv = __ldcs(reinterpret_cast<const float4*>(val + (size_t)i * WP + q));
+          v[q] = vv.x; v[q + 1] = vv.y; v[q + 2] = vv.z; v[q + 3] = vv.w;
+        }
+      }
+      T g[WP];
+#pragma unroll
+      for (int q = 0; q < WP; ++q) g[q] = c[q] >= 0 ? __ldg(x + c[q]) : T(0);
+#pragma unroll
+      for (int q = 0; q < WP; ++q)
+        if (c[q] >= 0) s += v[q] * g[q];
+    } else {
+      const int32_t* c = col + (size_t)i * W;
+      const T* v = val + (size_t)i * W;
+      for (int q = 0; q < W; ++q) {
+        int j = __ldcs(c + q);
+        if (j >= 0) s += __ldcs(v + q) * __ldg(x + j);
+      }
     }
     y[i] = epilogue(s, hb ? y[i] : T(0), alpha, beta, hb);
   }
@@ -223,7 +278,7 @@ void hodge_into(const Mesh& m, int k, bool inverse, DArr<double>& out) {
 }
 
 void assemble_laplacian(const Mesh& m, double shift, int& W, DArr<int32_t>& col, DArr<double>& val) {
-  W = m.max_v2e + 1;
+  W = (m.max_v2e + 1 + 3) / 4 * 4;  // diagonal + neighbours, padded to a multiple of 4
   col.alloc((size_t)m.nv * W);
   val.alloc((size_t)m.nv * W);
   DArr<int> overflow(1);
@@ -270,13 +325,16 @@ static void launch_op(const dec_op& op, const void* vx, void* vy, double alpha, 
     case DEC_OP_LAPLACE0:
     case DEC_OP_HELMHOLTZ0: {
       const T* val = std::is_same<T, double>::value ? (const T*)op.val64.p : (const T*)op.val32.p;
-      k_ell<T><<<grid_for(m.nv, TH), TH, 0, s>>>(m.nv, op.W, op.col.p, val, x, y, a, b, hb);
+      if (op.W == 8)
+        k_ell<T, 8><<<grid_for(m.nv, TH), TH, 0, s>>>(m.nv, op.W, op.col.p, val, x, y, a, b, hb);
+      else
+        k_ell<T, 0><<<grid_for(m.nv, TH), TH, 0, s>>>(m.nv, op.W, op.col.p, val, x, y, a, b, hb);
       break;
     }
     default: {  // diagonal stars
       const T* d = std::is_same<T, double>::value ? (const T*)op.diag64.p : (const T*)op.diag32.p;
       int n = (int)op.rows;
-      if (n) k_diag<T><<<grid_for(n, TH), TH, 0, s>>>(n, d, x, y, a, b, hb);
+      if (n) k_diag<T><<<grid_for(n, TH * kOpItems), TH, 0, s>>>(n, d, x, y, a, b, hb);
       break;
     }
   }

@@ -133,3 +133,44 @@ def uniform(seed, n, dtype=np.float64):
         z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
         z = z ^ (z >> np.uint64(31))
     return ((z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0) * 2.0 - 1.0).astype(dtype)
+
+
+def refine_binary(m, radius=0.0):
+    """refine(::BinarySubdivision) + propagate_points (src/Multigrid.jl:111-183), vectorised;
+    a positive radius projects the new vertices onto that sphere.  Orientation is left unset
+    (the library runs orient!, as dualize does on a refined mesh)."""
+    nv, ne, nt = m.nv, m.ne, m.nt
+    ev0 = np.empty(2 * ne + 3 * nt, np.int32)
+    ev1 = np.empty_like(ev0)
+    mid = nv + np.arange(ne, dtype=np.int64)
+    ev0[0:2 * ne:2] = mid
+    ev1[0:2 * ne:2] = m.ev0
+    ev0[1:2 * ne:2] = mid
+    ev1[1:2 * ne:2] = m.ev1
+    e0, e1, e2 = (np.asarray(a, np.int64) for a in (m.te0, m.te1, m.te2))
+    m0, m1, m2 = e0 + nv, e1 + nv, e2 + nv
+    base = 2 * ne + 3 * np.arange(nt, dtype=np.int64)
+    ev0[base], ev1[base] = m1, m0          # m0_m1
+    ev0[base + 1], ev1[base + 1] = m2, m1  # m1_m2
+    ev0[base + 2], ev1[base + 2] = m2, m0  # m0_m2
+    te = np.empty((4 * nt, 3), np.int32)
+    b = 4 * np.arange(nt, dtype=np.int64)
+    te[b] = np.stack([base + 1, base + 2, base], 1)
+    te[b + 1] = np.stack([base + 1, 2 * e2 + 1, 2 * e1 + 1], 1)
+    te[b + 2] = np.stack([base + 2, 2 * e2, 2 * e0 + 1], 1)
+    te[b + 3] = np.stack([base, 2 * e1, 2 * e0], 1)
+    p = np.asarray(m.points, np.float64)
+    newp = (p[m.ev0] + p[m.ev1]) / 2
+    if radius > 0:
+        newp = newp / np.linalg.norm(newp, axis=1, keepdims=True) * radius
+    return HostMesh(np.concatenate([p, newp]), ev0, ev1, te[:, 0].copy(), te[:, 1].copy(), te[:, 2].copy(),
+                    np.zeros(len(ev0), np.int8), None)
+
+
+def icosphere(k):
+    """Icosphere L_k: the unit icosahedron binary-subdivided k times, new vertices on the unit
+    sphere (nv = 10·4^k + 2)."""
+    m = icosahedron()
+    for _ in range(k):
+        m = refine_binary(m, 1.0)
+    return m
