@@ -27,7 +27,7 @@ from ._capi import check, lib, DecError  # noqa: F401
 __all__ = ["Mesh", "Operator", "MultigridData", "dec_wedge_product", "dec_wedge_product_pd",
            "dec_wedge_product_dp", "dec_wedge_product_dd", "dec_differential", "dec_boundary",
            "dec_dual_derivative", "dec_hodge_star", "dec_inv_hodge_star", "laplace_beltrami",
-           "helmholtz", "multigrid_vcycles", "multigrid_wcycles", "DecError"]
+           "helmholtz", "multigrid_vcycles", "multigrid_wcycles", "SmootherMLP", "DecError"]
 
 CENTERS = {"barycenter": _capi.DEC_BARYCENTER, "circumcenter": _capi.DEC_CIRCUMCENTER}
 
@@ -126,7 +126,7 @@ class Mesh:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and getattr(self, "_owned", False) and _capi._lib is not None:
+        if h and getattr(self, "_owned", False) and _capi is not None and _capi._lib is not None:
             _capi._lib.dec_mesh_destroy(h)
             self._h = None
 
@@ -163,7 +163,7 @@ class WedgePlan:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and _capi._lib is not None:
+        if h and _capi is not None and _capi._lib is not None:
             _capi._lib.dec_wedge_plan_destroy(h)
             self._h = None
 
@@ -224,7 +224,7 @@ class Operator:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and getattr(self, "_owned", False) and _capi._lib is not None:
+        if h and getattr(self, "_owned", False) and _capi is not None and _capi._lib is not None:
             _capi._lib.dec_op_destroy(h)
             self._h = None
 
@@ -360,7 +360,7 @@ class MultigridData:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and _capi._lib is not None:
+        if h and _capi is not None and _capi._lib is not None:
             _capi._lib.dec_mg_destroy(h)
             self._h = None
 
@@ -399,6 +399,11 @@ class MultigridData:
         check(lib().dec_mg_autotune(self._h, nrhs, reps, _stream(), C.byref(k)))
         return k.value
 
+    def set_smoother_mlp(self, mlp):
+        """Attach the learned smoother network used by smoother=DEC_SMOOTH_LEARNED (None detaches)."""
+        check(lib().dec_mg_set_smoother_mlp(self._h, None if mlp is None else mlp._h))
+        self._mlp = mlp  # keep the network alive while the hierarchy uses it
+
     def time_kernel(self, kernel, level, nrhs, reps=20):
         """(ms per launch, algorithmic bytes per launch) of one V-cycle kernel (dec_mg_time_kernel)."""
         ms, by = C.c_double(), C.c_double()
@@ -428,6 +433,97 @@ class MultigridData:
         if st not in (_capi.DEC_OK, 4):
             check(st)
         return u, rep
+
+
+class SmootherMLP:
+    """The learned smoother's network (dec_mlp_*): per-vertex MLP 16 -> 64 -> 64 -> 1, ReLU,
+    BF16 weights and activations on the tensor cores with FP32 accumulation, FP32 master
+    parameters trained with Adam by the library's own forward / backward kernels."""
+
+    NPARAM = _capi.DEC_MLP_NPARAM
+
+    def __init__(self, seed=4):
+        h = C.c_void_p()
+        check(lib().dec_mlp_create(C.c_uint64(seed), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _capi is not None and _capi._lib is not None:
+            _capi._lib.dec_mlp_destroy(h)
+            self._h = None
+
+    @property
+    def params(self):
+        p = np.empty(self.NPARAM, np.float32)
+        check(lib().dec_mlp_get_params(self._h, p.ctypes.data_as(C.c_void_p)))
+        return p
+
+    @params.setter
+    def params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        if p.size != self.NPARAM:
+            raise ValueError(f"expected {self.NPARAM} parameters")
+        check(lib().dec_mlp_set_params(self._h, p.ctypes.data_as(C.c_void_p)))
+
+    @property
+    def step(self):
+        s = C.c_int64()
+        check(lib().dec_mlp_step(self._h, C.byref(s)))
+        return s.value
+
+    def eval(self, x, tensor_cores=True):
+        """y = MLP(x) for x a float32 CUDA tensor (n, 16)."""
+        torch = _torch()
+        x = x.contiguous()
+        y = torch.empty(x.shape[0], dtype=torch.float32, device=x.device)
+        check(lib().dec_mlp_eval(self._h, _ptr(x), x.shape[0], _ptr(y), int(tensor_cores), _stream()))
+        return y
+
+    def grad(self, x, dy):
+        """Σ_q dy_q ∂MLP(x_q)/∂params as a float32 CUDA tensor (NPARAM,)."""
+        torch = _torch()
+        g = torch.empty(self.NPARAM, dtype=torch.float32, device=x.device)
+        check(lib().dec_mlp_grad(self._h, _ptr(x.contiguous()), _ptr(dy.contiguous()), x.shape[0], _ptr(g),
+                                 _stream()))
+        return g
+
+    @staticmethod
+    def features(op, r):
+        """(features (n*S, 16), scales s/a_ii (n*S,)) of residual fields r (S, n) float64."""
+        torch = _torch()
+        S = 1 if r.dim() == 1 else r.shape[0]
+        n = op.shape[0]
+        f = torch.empty((n * S, 16), dtype=torch.float32, device=r.device)
+        sc = torch.empty(n * S, dtype=torch.float32, device=r.device)
+        check(lib().dec_mlp_features(op._h, _ptr(r.contiguous()), S, _ptr(f), _ptr(sc), _stream()))
+        return f, sc
+
+    def loss_grad(self, op, r, grad=True):
+        """(energy-norm loss, full parameter gradient or None) on residual fields r (S, n)."""
+        torch = _torch()
+        S = 1 if r.dim() == 1 else r.shape[0]
+        loss = C.c_double()
+        g = torch.empty(self.NPARAM, dtype=torch.float32, device=r.device) if grad else None
+        check(lib().dec_mlp_loss_grad(self._h, op._h, _ptr(r.contiguous()), S, C.byref(loss),
+                                      None if g is None else _ptr(g), _stream()))
+        return loss.value, g
+
+    def train(self, op, r, steps, lr=1e-3, batch=65536, seed=4, record_loss=False):
+        """`steps` Adam steps on residual fields r (S, n) of op's mesh; returns the per-step losses
+        (before each update) when record_loss, else None."""
+        S = 1 if r.dim() == 1 else r.shape[0]
+        losses = np.empty(steps) if record_loss else None
+        check(lib().dec_mlp_train(self._h, op._h, _ptr(r.contiguous()), S, steps, float(lr), int(batch),
+                                  C.c_uint64(seed), None if losses is None else losses.ctypes.data_as(C.c_void_p),
+                                  _stream()))
+        return losses
+
+    def save(self, path):
+        check(lib().dec_mlp_save(self._h, str(path).encode()))
+
+    def load(self, path):
+        check(lib().dec_mlp_load(self._h, str(path).encode()))
 
 
 def multigrid_vcycles(u, b, md, cycles):

@@ -15,7 +15,9 @@ DEC_WEDGE_PP, DEC_WEDGE_PD, DEC_WEDGE_DP, DEC_WEDGE_DD = 0, 1, 2, 3
  DEC_OP_STAR0, DEC_OP_STAR1, DEC_OP_STAR2, DEC_OP_INV_STAR0, DEC_OP_INV_STAR1, DEC_OP_INV_STAR2,
  DEC_OP_LAPLACE0, DEC_OP_HELMHOLTZ0) = range(14)
 DEC_GEOM_LENGTH, DEC_GEOM_AREA, DEC_GEOM_DUAL_AREA, DEC_GEOM_DUAL_LENGTH_TE, DEC_GEOM_DUAL_POINT = range(5)
-DEC_SMOOTH_JACOBI, DEC_SMOOTH_CHEBYSHEV, DEC_SMOOTH_CG = 0, 1, 2
+DEC_SMOOTH_JACOBI, DEC_SMOOTH_CHEBYSHEV, DEC_SMOOTH_CG, DEC_SMOOTH_LEARNED = 0, 1, 2, 3
+DEC_KERNEL_SWEEP, DEC_KERNEL_RESIDUAL, DEC_KERNEL_RESTRICT, DEC_KERNEL_PROLONG, DEC_KERNEL_MLP = range(5)
+DEC_MLP_NPARAM = 5313
 
 
 class MeshDesc(C.Structure):
@@ -31,13 +33,14 @@ class MGOptions(C.Structure):
                 ("shift", C.c_double), ("smoother", C.c_int32), ("pre", C.c_int32), ("post", C.c_int32),
                 ("omega", C.c_double), ("cheb_ratio", C.c_double), ("coarse_solver", C.c_int32),
                 ("precision", C.c_int32), ("rhs_block", C.c_int32), ("mu", C.c_int32),
-                ("inner_cycles", C.c_int32), ("reorder", C.c_int32), ("coarse_max", C.c_int32)]
+                ("inner_cycles", C.c_int32), ("reorder", C.c_int32), ("coarse_max", C.c_int32),
+                ("fallback_rho", C.c_double)]
 
 
 class SolveReport(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32),
                 ("max_rel_residual", C.c_double), ("seconds", C.c_double),
-                ("launches", C.c_int64), ("rhs_block", C.c_int32)]
+                ("launches", C.c_int64), ("rhs_block", C.c_int32), ("fallback_iteration", C.c_int32)]
 
 
 P = C.c_void_p
@@ -79,6 +82,19 @@ SIGNATURES = {
     "dec_mg_solve_host": (I32, [P, P, P, I32, F64, I32, I32, C.POINTER(SolveReport), P]),
     "dec_mg_time_kernel": (I32, [P, I32, I32, I32, I32, P, PF64, PF64]),
     "dec_mg_autotune": (I32, [P, I32, I32, P, C.POINTER(C.c_int32)]),
+    "dec_mg_set_smoother_mlp": (I32, [P, P]),
+    "dec_mlp_create": (I32, [C.c_uint64, PP]),
+    "dec_mlp_destroy": (I32, [P]),
+    "dec_mlp_get_params": (I32, [P, P]),
+    "dec_mlp_set_params": (I32, [P, P]),
+    "dec_mlp_step": (I32, [P, PI64]),
+    "dec_mlp_eval": (I32, [P, P, I64, P, I32, P]),
+    "dec_mlp_grad": (I32, [P, P, P, I64, P, P]),
+    "dec_mlp_features": (I32, [P, P, I32, P, P, P]),
+    "dec_mlp_loss_grad": (I32, [P, P, P, I32, PF64, P, P]),
+    "dec_mlp_train": (I32, [P, P, P, I32, I32, F64, I64, C.c_uint64, P, P]),
+    "dec_mlp_save": (I32, [P, C.c_char_p]),
+    "dec_mlp_load": (I32, [P, C.c_char_p]),
 }
 
 

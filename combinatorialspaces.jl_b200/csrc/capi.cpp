@@ -21,6 +21,18 @@ void op_export_csr_impl(const dec_op* op, int64_t* nnz, int32_t* rowptr, int32_t
 void hodge_diag_impl(const dec_mesh* mh, int k, int inverse, dec_dtype dt, void* out, void* stream);
 void op_residual_norms_impl(dec_op* op, const double* x, const double* b, int nrhs, double* norms, double* bnorms,
                             void* stream);
+dec_mlp* mlp_create_impl(uint64_t seed);
+void mlp_destroy_impl(dec_mlp* m);
+void mlp_params_impl(dec_mlp* m, float* out, const float* in);
+int64_t mlp_step_impl(const dec_mlp* m);
+void mlp_eval_impl(dec_mlp* m, const float* x, int64_t n, float* y, int tensor_cores, void* stream);
+void mlp_grad_impl(dec_mlp* m, const float* x, const float* dy, int64_t n, float* grad, void* stream);
+void mlp_features_impl(const dec_op* op, const double* r, int S, float* feat, float* dscale, void* stream);
+void mlp_loss_grad_impl(dec_mlp* m, dec_op* op, const double* r, int S, double* loss, float* grad, void* stream);
+void mlp_train_impl(dec_mlp* m, dec_op* op, const double* r, int S, int steps, double lr, int64_t batch,
+                    uint64_t seed, double* losses, void* stream);
+void mlp_save_impl(const dec_mlp* m, const char* path);
+void mlp_load_impl(dec_mlp* m, const char* path);
 void op_residual_norms_noalloc_impl(dec_op* op, const double* x, const double* b, int nrhs, double* norms,
                                     double* bnorms, void* stream);
 
@@ -239,6 +251,68 @@ dec_status dec_mg_autotune(dec_mg* mg, int32_t nrhs, int32_t reps, void* stream,
     int k = decb::mg_autotune(mg, nrhs, reps, stream);
     if (rhs_block) *rhs_block = k;
   });
+}
+
+dec_status dec_mg_set_smoother_mlp(dec_mg* mg, const dec_mlp* mlp) {
+  return guard([&] { decb::mg_set_smoother_mlp(mg, mlp); });
+}
+
+dec_status dec_mlp_create(uint64_t seed, dec_mlp** out) {
+  return guard([&] {
+    decb::require(out != nullptr, "dec_mlp_create: null argument");
+    *out = nullptr;
+    *out = mlp_create_impl(seed);
+  });
+}
+
+dec_status dec_mlp_destroy(dec_mlp* mlp) {
+  return guard([&] { mlp_destroy_impl(mlp); });
+}
+
+dec_status dec_mlp_get_params(const dec_mlp* mlp, float* params) {
+  return guard([&] { mlp_params_impl(const_cast<dec_mlp*>(mlp), params, nullptr); });
+}
+
+dec_status dec_mlp_set_params(dec_mlp* mlp, const float* params) {
+  return guard([&] { mlp_params_impl(mlp, nullptr, params); });
+}
+
+dec_status dec_mlp_step(const dec_mlp* mlp, int64_t* step) {
+  return guard([&] {
+    decb::require(step != nullptr, "dec_mlp_step: null argument");
+    *step = mlp_step_impl(mlp);
+  });
+}
+
+dec_status dec_mlp_eval(dec_mlp* mlp, const float* x, int64_t n, float* y, int32_t tensor_cores, void* stream) {
+  return guard([&] { mlp_eval_impl(mlp, x, n, y, tensor_cores, stream); });
+}
+
+dec_status dec_mlp_grad(dec_mlp* mlp, const float* x, const float* dy, int64_t n, float* grad, void* stream) {
+  return guard([&] { mlp_grad_impl(mlp, x, dy, n, grad, stream); });
+}
+
+dec_status dec_mlp_features(const dec_op* op, const double* r, int32_t S, float* features, float* scales,
+                            void* stream) {
+  return guard([&] { mlp_features_impl(op, r, S, features, scales, stream); });
+}
+
+dec_status dec_mlp_loss_grad(dec_mlp* mlp, dec_op* op, const double* r, int32_t S, double* loss, float* grad,
+                             void* stream) {
+  return guard([&] { mlp_loss_grad_impl(mlp, op, r, S, loss, grad, stream); });
+}
+
+dec_status dec_mlp_train(dec_mlp* mlp, dec_op* op, const double* r, int32_t S, int32_t steps, double lr,
+                         int64_t batch, uint64_t seed, double* losses, void* stream) {
+  return guard([&] { mlp_train_impl(mlp, op, r, S, steps, lr, batch, seed, losses, stream); });
+}
+
+dec_status dec_mlp_save(const dec_mlp* mlp, const char* path) {
+  return guard([&] { mlp_save_impl(mlp, path); });
+}
+
+dec_status dec_mlp_load(dec_mlp* mlp, const char* path) {
+  return guard([&] { mlp_load_impl(mlp, path); });
 }
 
 }  // extern "C"

@@ -29,8 +29,10 @@
 #include <numeric>
 
 #include "mg.cuh"
+#include "mlp.cuh"
 
 dec_op* op_create_impl(dec_mesh* mh, int kind, double shift, dec_dtype dt);
+decb::MlpWeights mlp_weights(const dec_mlp* m);
 
 namespace decb {
 
@@ -863,12 +865,16 @@ struct Workspace {
   DArr<double> scal;          // CG smoother: per-right-hand-side scalars (CgField x K*npanels)
   DArr<double> ucm, bcm;      // column-major device copies for host-buffer solves
   int nblocks = 0;
-  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};  // GraphKind
-  int64_t launches[3] = {0, 0, 0};                          // kernel nodes per graph
-  ~Workspace() {
-    for (auto& g : graph)
+  DArr<double> Ubak;          // learned smoother: the iterate before a refinement step
+  cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};  // GraphKind
+  int64_t launches[4] = {0, 0, 0, 0};                               // kernel nodes per graph
+  void drop_graphs() {
+    for (auto& g : graph) {
       if (g) cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
   }
+  ~Workspace() { drop_graphs(); }
 };
 
 }  // namespace decb
@@ -881,6 +887,8 @@ struct dec_mg {
   std::map<long long, std::unique_ptr<decb::Workspace>> ws;
   std::map<long long, int> tuned;  // (nrhs, precision) -> panel width chosen by the autotuner
   cudaStream_t cap = nullptr;      // capture stream
+  const dec_mlp* mlp = nullptr;    // learned smoother network (not owned)
+  bool force_plain = false;        // set while capturing the plain-smoother fallback cycle
   ~dec_mg() {
     ws.clear();
     if (cap) cudaStreamDestroy(cap);
@@ -907,6 +915,7 @@ void mg_default_options(dec_mg_options& o) {
   o.inner_cycles = 1;
   o.reorder = 1;
   o.coarse_max = 0;
+  o.fallback_rho = 0.5;
 }
 
 static double power_lmax(const Level& L) {
@@ -1041,7 +1050,9 @@ static void build_transfers(Level& F, const Level& C, const HostLevel& c) {
 
 dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
   require(o.levels >= 0 && o.levels <= 12, "multigrid: levels must be in [0, 12]");
-  require(o.smoother >= 0 && o.smoother <= 2, "multigrid: unknown smoother");
+  require(o.smoother >= 0 && o.smoother <= 3, "multigrid: unknown smoother");
+  require(o.smoother != DEC_SMOOTH_LEARNED || (o.fallback_rho > 0 && o.fallback_rho <= 1),
+          "multigrid: fallback_rho must be in (0, 1]");
   require(o.smoother != DEC_SMOOTH_CG || o.precision == 0, "multigrid: the CG smoother runs in FP64 (precision 0)");
   require(o.pre >= 0 && o.post >= 0 && o.pre <= 16 && o.post <= 16, "multigrid: sweeps must be in [0, 16]");
   require(o.mu == 1 || o.mu == 2, "multigrid: mu must be 1 (V) or 2 (W)");
@@ -1049,6 +1060,7 @@ dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
   require(o.cheb_ratio > 1.0, "multigrid: cheb_ratio must exceed 1");
   require(o.inner_cycles >= 1 && o.inner_cycles <= 8, "multigrid: inner_cycles must be in [1, 8]");
   require(o.coarse_max >= 0 && o.coarse_max <= 1024, "multigrid: coarse_max must be in [0, 1024]");
+  require(o.coarse_solver == 0 || o.coarse_solver == 1, "multigrid: coarse_solver must be 0 or 1");
   auto mg = std::make_unique<dec_mg>();
   mg->opt = o;
   std::vector<HostLevel> hl(o.levels + 1);
@@ -1159,6 +1171,24 @@ static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool z
                  cudaStream_t s) {
   const dec_mg_options& o = mg.opt;
   T* other = (x == B.x.p) ? B.y.p : B.x.p;
+  if (o.smoother == DEC_SMOOTH_LEARNED && !mg.force_plain) {
+    // learned sweep: r = b - A x (skipped from zero: r = b), then x + (s / a_ii) MLP(features(r))
+    const MlpWeights wts = mlp_weights(mg.mlp);
+    for (int it = 0; it < sweeps; ++it) {
+      const T* r = B.b.p;
+      if (!zero_x) {
+        SweepPrm<T> prm{};
+        prm.mode = S_RESID;
+        launch_sweep<T, K>(L, B.b.p, x, B.d.p, nullptr, prm, np, s);
+        r = B.d.p;
+      }
+      launch_mlp_smooth<T, K>(wts, L.n, L.W, L.col.p, pick<T>(L.off64, L.off32), pick<T>(L.diag64, L.diag32), r, x,
+                              zero_x ? 1 : 0, other, np, s);
+      std::swap(x, other);
+      zero_x = false;
+    }
+    return x;
+  }
   const double hi = L.lmax, lo = L.lmax / o.cheb_ratio;
   const double theta = (hi + lo) / 2, delta = (hi - lo) / 2, sigma = theta / delta;
   double rho = 1 / sigma;
@@ -1275,6 +1305,8 @@ static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bu
     if (mg.opt.smoother == DEC_SMOOTH_CG) return cg_mu_cycle<K>(mg, w, bufs, l, x, zero_x, mu, np, s);
   }
   if (l == mg.lc) {
+    if (mg.opt.coarse_solver == 1)  // the smoother on the coarsest level (pre + post sweeps)
+      return smooth<T, K>(mg, L, B, x, zero_x, std::max(1, mg.opt.pre + mg.opt.post), np, s);
     launch_pdl(k_coarse<T, K>, dim3(grid_for(L.n, TB / K, 64), np), dim3(TB), s, L.n, (const double*)mg.ainv.p,
                (const T*)B.b.p, B.x.p, (size_t)L.n * K);
     return B.x.p;
@@ -1386,7 +1418,7 @@ static void enqueue_cycle(dec_mg& mg, Workspace& w, cudaStream_t s) {
 // Vectors a smoothing sweep reads or writes once: Jacobi b, x, out; Chebyshev b, x, d (r/w), out.
 static int prm_vectors(int smoother) { return smoother == DEC_SMOOTH_JACOBI ? 3 : 5; }
 
-enum GraphKind { G_RESID = 0, G_VCYCLE = 1, G_CYCLE = 2 };
+enum GraphKind { G_RESID = 0, G_VCYCLE = 1, G_CYCLE = 2, G_VCYCLE_PLAIN = 3 };  // plain: learned-smoother fallback
 
 template <int K>
 static void enqueue_kind(dec_mg& mg, Workspace& w, cudaStream_t s, int kind) {
@@ -1427,14 +1459,19 @@ static int64_t count_kernel_nodes(cudaGraph_t g) {
 
 static cudaGraphExec_t capture(dec_mg& mg, Workspace& w, int kind) {
   cudaGraph_t g = nullptr;
+  require(mg.opt.smoother != DEC_SMOOTH_LEARNED || mg.mlp != nullptr || kind == G_VCYCLE_PLAIN || kind == G_RESID,
+          "multigrid: the learned smoother needs a network (dec_mg_set_smoother_mlp)");
   DEC_CUDA(cudaStreamBeginCapture(mg.cap, cudaStreamCaptureModeThreadLocal));
+  mg.force_plain = kind == G_VCYCLE_PLAIN;
   try {
     dispatch(mg, w, mg.cap, kind);
   } catch (...) {
+    mg.force_plain = false;
     cudaStreamEndCapture(mg.cap, &g);
     if (g) cudaGraphDestroy(g);
     throw;
   }
+  mg.force_plain = false;
   DEC_CUDA(cudaStreamEndCapture(mg.cap, &g));
   w.launches[kind] = count_kernel_nodes(g);
   cudaGraphExec_t ex = nullptr;
@@ -1547,26 +1584,53 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
     DEC_CUDA(cudaStreamSynchronize(s));
     for (auto& x : bn) x = std::sqrt(x);
   }
+  const bool learned = mg->opt.smoother == DEC_SMOOTH_LEARNED;
   if (!w.graph[G_RESID]) w.graph[G_RESID] = capture(*mg, w, G_RESID);
   if (!w.graph[G_VCYCLE]) w.graph[G_VCYCLE] = capture(*mg, w, G_VCYCLE);
-  int it = 0;
-  double worst = 0.0;
-  bool conv = false;
-  for (;;) {
-    DEC_CUDA(cudaGraphLaunch(w.graph[G_RESID], s));  // u += e; r = b - A u; norms
+  if (learned) {
+    if (!w.graph[G_VCYCLE_PLAIN]) w.graph[G_VCYCLE_PLAIN] = capture(*mg, w, G_VCYCLE_PLAIN);
+    if (w.Ubak.n < total) w.Ubak.alloc(total);
+  }
+  int64_t nl = (use_initial_guess ? 2 : 1) + 2;  // to_panels, ||b|| partials + reduce
+  auto residual = [&]() {                        // u += e; r = b - A u; worst relative residual
+    DEC_CUDA(cudaGraphLaunch(w.graph[G_RESID], s));
+    nl += w.launches[G_RESID];
     DEC_CUDA(cudaMemcpyAsync(rn.data(), w.norms.p, rn.size() * 8, cudaMemcpyDeviceToHost, s));
     DEC_CUDA(cudaStreamSynchronize(s));
-    worst = 0.0;
+    double wr = 0.0;
     for (int j = 0; j < nrhs; ++j) {
-      double rel = bn[j] > 0 ? std::sqrt(rn[j]) / bn[j] : std::sqrt(rn[j]);
-      worst = std::max(worst, rel);
+      const double rel = bn[j] > 0 ? std::sqrt(rn[j]) / bn[j] : std::sqrt(rn[j]);
+      if (!std::isfinite(rel)) return HUGE_VAL;
+      wr = std::max(wr, rel);
+    }
+    return wr;
+  };
+  int it = 0, fallback_at = -1;
+  double worst = 0.0, prev = 0.0;
+  bool conv = false, plain = !learned;
+  for (;;) {
+    const bool check = !plain && it > 0;
+    if (check) DEC_CUDA(cudaMemcpyAsync(w.Ubak.p, w.U64.p, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    worst = residual();
+    if (check && !(worst <= mg->opt.fallback_rho * prev)) {
+      // the learned step fell behind: undo it (u from before the step, e = 0, same residual)
+      // and continue with the plain smoother
+      DEC_CUDA(cudaMemcpyAsync(w.U64.p, w.Ubak.p, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      if (w.prec == 1) DEC_CUDA(cudaMemsetAsync(w.f32[0].x.p, 0, total * sizeof(float), s));
+      else DEC_CUDA(cudaMemsetAsync(w.f64[0].x.p, 0, total * sizeof(double), s));
+      worst = residual();
+      plain = true;
+      fallback_at = it;
     }
     if (worst <= rtol) {
       conv = true;
       break;
     }
     if (it >= max_iters) break;
-    DEC_CUDA(cudaGraphLaunch(w.graph[G_VCYCLE], s));  // e = V(r)
+    prev = worst;
+    const int kind = learned && plain ? G_VCYCLE_PLAIN : G_VCYCLE;
+    DEC_CUDA(cudaGraphLaunch(w.graph[kind], s));  // e = V(r)
+    nl += w.launches[kind];
     ++it;
   }
   k_from_panels<double, double><<<grid_for((long long)n * nrhs, 256), 256, 0, s>>>(n, nrhs, K, F.diperm.p, w.U64.p, ud);
@@ -1583,9 +1647,9 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
     rep->converged = conv ? 1 : 0;
     rep->max_rel_residual = worst;
     rep->seconds = ms * 1e-3;
-    // to_panels x2, sumsq + reduce, residual graph per test, V-cycle graph per step, from_panels
-    rep->launches = 2 + 2 + (int64_t)(it + 1) * w.launches[G_RESID] + (int64_t)it * w.launches[G_VCYCLE] + 1;
+    rep->launches = nl + 1;  // + from_panels
     rep->rhs_block = K;
+    rep->fallback_iteration = fallback_at;
   }
   return conv ? DEC_OK : DEC_ERR_NOT_CONVERGED;
 }
@@ -1613,6 +1677,9 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
       prm.c1 = (T)0.5;
       prm.c2 = (T)0.25;
       launch_sweep<T, K>(L, B.b.p, B.x.p, B.y.p, B.d.p, prm, np, s);
+    } else if (kernel == DEC_KERNEL_MLP) {
+      launch_mlp_smooth<T, K>(mlp_weights(mg.mlp), L.n, L.W, L.col.p, pick<T>(L.off64, L.off32),
+                              pick<T>(L.diag64, L.diag32), B.b.p, B.x.p, 0, B.y.p, np, s);
     } else if (kernel == DEC_KERNEL_RESIDUAL) {
       dim3 g(w.nblocks, np);
       const Level& F = mg.lv[0];
@@ -1643,6 +1710,8 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
   if (kernel == DEC_KERNEL_SWEEP) {
     double mat = (double)L.n * (L.W * (4.0 + sz) + 2 * sz);
     *bytes = mat + prm_vectors(mg.opt.smoother) * (double)nk * sz;
+  } else if (kernel == DEC_KERNEL_MLP) {
+    *bytes = (double)L.n * (L.W * (4.0 + sz) + sz) + 3.0 * (double)nk * sz;  // operator, r, x, out
   } else if (kernel == DEC_KERNEL_RESIDUAL) {
     const Level& F = mg.lv[0];
     double mat = (double)F.n * (F.W * 12.0 + 8);
@@ -1665,8 +1734,10 @@ static void time_kernel_K(dec_mg& mg, Workspace& w, int kernel, int level, int r
 
 void mg_time_kernel(dec_mg* mg, int kernel, int level, int nrhs, int reps, void* stream, double* ms, double* bytes) {
   require(mg != nullptr && ms != nullptr && bytes != nullptr, "multigrid: null argument");
-  require(kernel >= 0 && kernel <= 3, "multigrid: unknown kernel");
-  require(level >= 0 && level < (int)mg->lv.size() - (kernel >= 2 ? 1 : 0), "multigrid: level out of range");
+  require(kernel >= 0 && kernel <= 4, "multigrid: unknown kernel");
+  require(kernel != DEC_KERNEL_MLP || mg->mlp != nullptr, "multigrid: no learned smoother network set");
+  require(level >= 0 && level < (int)mg->lv.size() - (kernel == 2 || kernel == 3 ? 1 : 0),
+          "multigrid: level out of range");
   require(reps >= 1 && nrhs >= 1, "multigrid: reps and nrhs must be positive");
   Workspace& w = workspace(*mg, nrhs, mg->opt.precision);
   cudaStream_t s = as_stream(stream);
@@ -1676,6 +1747,13 @@ void mg_time_kernel(dec_mg* mg, int kernel, int level, int nrhs, int reps, void*
     DEC_K(1) DEC_K(2) DEC_K(4) DEC_K(8) DEC_K(16) DEC_K(32)
 #undef DEC_K
   }
+}
+
+void mg_set_smoother_mlp(dec_mg* mg, const dec_mlp* mlp) {
+  require(mg != nullptr, "multigrid: null argument");
+  if (mg->mlp == mlp) return;
+  mg->mlp = mlp;
+  for (auto& kv : mg->ws) kv.second->drop_graphs();  // captured cycles hold the old weights' addresses
 }
 
 int mg_autotune(dec_mg* mg, int nrhs, int reps, void* stream) {

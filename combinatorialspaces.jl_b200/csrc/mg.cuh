@@ -16,4 +16,5 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
 void mg_time_kernel(dec_mg* mg, int kernel, int level, int nrhs, int reps, void* stream, double* ms,
                     double* bytes);
 int mg_autotune(dec_mg* mg, int nrhs, int reps, void* stream);
+void mg_set_smoother_mlp(dec_mg* mg, const dec_mlp* mlp);
 }  // namespace decb

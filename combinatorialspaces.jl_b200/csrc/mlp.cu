@@ -1,0 +1,856 @@
+// The learned multigrid smoother: a per-vertex MLP 16 -> 64 -> 64 -> 1 (ReLU) over scale-free
+// 1-ring features (the vertex's and its neighbours' residuals over their largest magnitude, the
+// couplings a_ij / a_ii, the diagonal margin, the valence).  Its output y gives the correction
+// x_i += (s_i / a_ii) y_i, s_i the residual scale, so damped Jacobi is the network y = ω f_0.
+//
+// Inference runs on the tensor cores: one warp evaluates 32 samples with mma.sync m16n8k16
+// (BF16 operands, FP32 accumulation); the first layer's accumulator fragments become the
+// second layer's A fragments in registers, and the last layer is a quad shuffle reduction.
+//
+// Training minimises the energy-norm error left by one smoothing step.  With r = A e and ⋆0 A
+// symmetric positive definite, ||e - δ||²_{⋆0 A} = ||e||²_{⋆0 A} + δᵀ ⋆0 A δ - 2 δᵀ ⋆0 r, so every
+// (residual, error) pair enters through its residual alone:
+//   L = (1/S) Σ_s (δ_sᵀ ⋆0 A δ_s - 2 δ_sᵀ ⋆0 r_s) / n_s,  n_s = Σ_i ⋆0_i r_si² / a_ii,
+//   dL/dδ = 2 ⋆0 (A δ - r) / (S n_s).
+// The forward pass over every vertex of the fields is the inference kernel; the backward pass
+// recomputes the forward in FP32 on the CUDA cores (same BF16 roundings; gradients reach the FP32
+// master weights straight through) for a batch of vertex samples, drawn with replacement when the
+// fields hold more vertices than the batch; the parameter gradient is reduced in a fixed order;
+// Adam updates the masters and refreshes the BF16 copies.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "mlp.cuh"
+#include "ops.cuh"
+
+void op_apply_impl(dec_op* op, const void* x, void* y, double alpha, double beta, void* stream);
+
+namespace decb {
+
+// ---------------------------------------------------------------------------------------------
+// tensor-core inference
+// ---------------------------------------------------------------------------------------------
+constexpr int kMlpThreads = 256;  // 8 warps
+constexpr int kMlpWarps = kMlpThreads / 32;
+constexpr int kTile = 32;         // samples per warp tile (two m16 row tiles)
+// Shared-memory row strides in BF16 elements, padded so that the fragment loads of a warp hit
+// 32 distinct banks: 12 words per feature / W1 row, 36 words per W2 row.
+constexpr int kXsStride = 24, kW1Stride = 24, kW2Stride = 72;
+
+struct MlpSmem {
+  __align__(16) __nv_bfloat16 w1[kMlpH * kW1Stride];
+  __align__(16) __nv_bfloat16 w2[kMlpH * kW2Stride];
+  float b1[kMlpH], b2[kMlpH], w3[kMlpH], b3;
+};
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ void load_weights(MlpSmem& sm, const MlpWeights& w) {
+  for (int i = threadIdx.x; i < kMlpH * kMlpIn; i += blockDim.x) sm.w1[(i / kMlpIn) * kW1Stride + i % kMlpIn] = w.w1[i];
+  for (int i = threadIdx.x; i < kMlpH * kMlpH; i += blockDim.x) sm.w2[(i / kMlpH) * kW2Stride + i % kMlpH] = w.w2[i];
+  for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
+    sm.b1[i] = w.b1[i];
+    sm.b2[i] = w.b2[i];
+    sm.w3[i] = w.w3[i];
+  }
+  if (threadIdx.x == 0) sm.b3 = w.b3[0];
+  __syncthreads();
+}
+
+// Stores one sample's 16 features as a BF16 row of the warp's tile.
+__device__ __forceinline__ void store_row(__nv_bfloat16* xs, int row, const float (&f)[16]) {
+  uint4 lo, hi;
+  lo.x = pack_bf16(f[0], f[1]);
+  lo.y = pack_bf16(f[2], f[3]);
+  lo.z = pack_bf16(f[4], f[5]);
+  lo.w = pack_bf16(f[6], f[7]);
+  hi.x = pack_bf16(f[8], f[9]);
+  hi.y = pack_bf16(f[10], f[11]);
+  hi.z = pack_bf16(f[12], f[13]);
+  hi.w = pack_bf16(f[14], f[15]);
+  uint4* p = reinterpret_cast<uint4*>(xs + row * kXsStride);
+  p[0] = lo;
+  p[1] = hi;
+}
+
+// The MLP on one warp tile of 32 samples (rows of xs).  Returns, in every lane, y of the lane's
+// own row.
+__device__ __forceinline__ float mlp_tile32(const MlpSmem& sm, const __nv_bfloat16* xs) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const uint32_t* X = reinterpret_cast<const uint32_t*>(xs);
+  const uint32_t* W1 = reinterpret_cast<const uint32_t*>(sm.w1);
+  const uint32_t* W2 = reinterpret_cast<const uint32_t*>(sm.w2);
+  constexpr int XW = kXsStride / 2, W1W = kW1Stride / 2, W2W = kW2Stride / 2;  // words per row
+  uint32_t a[2][4];
+#pragma unroll
+  for (int m = 0; m < 2; ++m) {
+    const int r0 = 16 * m + g;
+    a[m][0] = X[r0 * XW + t];
+    a[m][1] = X[(r0 + 8) * XW + t];
+    a[m][2] = X[r0 * XW + t + 4];
+    a[m][3] = X[(r0 + 8) * XW + t + 4];
+  }
+  // layer 1: z1 = W1 x + b1 on 8 column tiles of 8 units; relu + BF16 pack into layer-2 A
+  uint32_t a2[2][4][4];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const uint32_t b0 = W1[(8 * j + g) * W1W + t], b1 = W1[(8 * j + g) * W1W + t + 4];
+    const float bb0 = sm.b1[8 * j + 2 * t], bb1 = sm.b1[8 * j + 2 * t + 1];
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      float c[4] = {bb0, bb1, bb0, bb1};
+      mma16816(c, a[m], b0, b1);
+      const uint32_t lo = pack_bf16(fmaxf(c[0], 0.f), fmaxf(c[1], 0.f));
+      const uint32_t hi = pack_bf16(fmaxf(c[2], 0.f), fmaxf(c[3], 0.f));
+      if ((j & 1) == 0) {
+        a2[m][j >> 1][0] = lo;
+        a2[m][j >> 1][1] = hi;
+      } else {
+        a2[m][j >> 1][2] = lo;
+        a2[m][j >> 1][3] = hi;
+      }
+    }
+  }
+  // layers 2 and 3: y = w3 · relu(W2 h1 + b2) + b3
+  float p[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+#pragma unroll
+  for (int jt = 0; jt < 8; ++jt) {
+    const float bb0 = sm.b2[8 * jt + 2 * t], bb1 = sm.b2[8 * jt + 2 * t + 1];
+    float c[2][4] = {{bb0, bb1, bb0, bb1}, {bb0, bb1, bb0, bb1}};
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      const uint32_t b0 = W2[(8 * jt + g) * W2W + 8 * kk + t], b1 = W2[(8 * jt + g) * W2W + 8 * kk + t + 4];
+#pragma unroll
+      for (int m = 0; m < 2; ++m) mma16816(c[m], a2[m][kk], b0, b1);
+    }
+    const float w0 = sm.w3[8 * jt + 2 * t], w1 = sm.w3[8 * jt + 2 * t + 1];
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      p[m][0] += fmaxf(c[m][0], 0.f) * w0 + fmaxf(c[m][1], 0.f) * w1;
+      p[m][1] += fmaxf(c[m][2], 0.f) * w0 + fmaxf(c[m][3], 0.f) * w1;
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < 2; ++m)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      p[m][h] += __shfl_xor_sync(0xffffffffu, p[m][h], 1);
+      p[m][h] += __shfl_xor_sync(0xffffffffu, p[m][h], 2);
+    }
+  // row 16m + 8h + g' lives in quad g' as p[m][h]; lane L takes row L
+  const int src = (lane & 7) * 4, m = lane >> 4, h = (lane >> 3) & 1;
+  const float v00 = __shfl_sync(0xffffffffu, p[0][0], src), v01 = __shfl_sync(0xffffffffu, p[0][1], src);
+  const float v10 = __shfl_sync(0xffffffffu, p[1][0], src), v11 = __shfl_sync(0xffffffffu, p[1][1], src);
+  const float v = m == 0 ? (h == 0 ? v00 : v01) : (h == 0 ? v10 : v11);
+  return v + sm.b3;
+}
+
+// y = MLP(x) for n samples of 16 FP32 features (tensor cores).
+__global__ void __launch_bounds__(kMlpThreads) k_mlp_eval_tc(int64_t n, const float* __restrict__ x,
+                                                             float* __restrict__ y, MlpWeights w) {
+  __shared__ MlpSmem sm;
+  __shared__ __align__(16) __nv_bfloat16 xs[kMlpWarps][kTile * kXsStride];
+  load_weights(sm, w);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t ntiles = (n + kTile - 1) / kTile;
+  for (int64_t tile = (int64_t)blockIdx.x * kMlpWarps + warp; tile < ntiles; tile += (int64_t)gridDim.x * kMlpWarps) {
+    const int64_t q = tile * kTile + lane;
+    float f[16];
+    if (q < n) {
+      const float4* src = reinterpret_cast<const float4*>(x + q * 16);
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const float4 t4 = src[v];
+        f[4 * v] = t4.x;
+        f[4 * v + 1] = t4.y;
+        f[4 * v + 2] = t4.z;
+        f[4 * v + 3] = t4.w;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) f[k] = 0.f;
+    }
+    store_row(xs[warp], lane, f);
+    __syncwarp();
+    const float yv = mlp_tile32(sm, xs[warp]);
+    if (q < n) y[q] = yv;
+    __syncwarp();
+  }
+}
+
+// Learned smoothing step on a multigrid level (panel layout [panel][row][K]; split operator:
+// diagonal + W off-diagonal slots in the reference's column order, padding = own column with
+// value 0): out = x + (s_i / a_ii) MLP(features(r)), x taken as zero when zero_x.
+template <class T, int K>
+__global__ void __launch_bounds__(kMlpThreads) k_mlp_smooth(MlpWeights w, int n, int W, const int32_t* __restrict__ col,
+                                                            const T* __restrict__ off, const T* __restrict__ diag,
+                                                            const T* __restrict__ r, const T* __restrict__ x,
+                                                            int zero_x, T* __restrict__ out, size_t pstride) {
+  __shared__ MlpSmem sm;
+  __shared__ __align__(16) __nv_bfloat16 xs[kMlpWarps][kTile * kXsStride];
+  load_weights(sm, w);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t po = (size_t)blockIdx.y * pstride;
+  const int64_t nq = (int64_t)n * K;
+  const int64_t ntiles = (nq + kTile - 1) / kTile;
+  for (int64_t tile = (int64_t)blockIdx.x * kMlpWarps + warp; tile < ntiles; tile += (int64_t)gridDim.x * kMlpWarps) {
+    const int64_t q = tile * kTile + lane;
+    float f[16];
+    float dsc = 0.f;
+    T xv = T(0);
+    if (q < nq) {
+      const int i = (int)(q / K), k = (int)(q % K);
+      const float di = (float)diag[i];
+      float nb[6], cp[6], sabs = 0.f;
+      int nn = 0;
+      for (int s = 0; s < W; ++s) {
+        const int c = col[(size_t)i * W + s];
+        const float o = (float)off[(size_t)i * W + s];
+        if (c == i && o == 0.f) continue;  // padding slot
+        sabs += fabsf(o);
+        if (nn < 6) {
+          nb[nn] = (float)r[po + (size_t)c * K + k];
+          cp[nn] = o / di;
+          ++nn;
+        }
+      }
+      float scale;
+      mlp_features((float)r[po + q], nb, cp, nn, 1.f - sabs / di, f, &scale);
+      dsc = scale / di;
+      if (!zero_x) xv = x[po + q];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) f[k] = 0.f;
+    }
+    store_row(xs[warp], lane, f);
+    __syncwarp();
+    const float yv = mlp_tile32(sm, xs[warp]);
+    if (q < nq) out[po + q] = xv + (T)(dsc * yv);
+    __syncwarp();
+  }
+}
+
+template <class T, int K>
+void launch_mlp_smooth(const MlpWeights& w, int n, int W, const int32_t* col, const T* off, const T* diag, const T* r,
+                       const T* x, int zero_x, T* out, int np, cudaStream_t s) {
+  const long long tiles = ((long long)n * K + kTile - 1) / kTile;
+  const long long want = (tiles + kMlpWarps - 1) / kMlpWarps;
+  const long long cap = std::max<long long>(1, (long long)num_sms() * 4 / std::max(1, np));
+  dim3 grid((unsigned)std::max<long long>(1, std::min(want, cap)), np);
+  k_mlp_smooth<T, K><<<grid, kMlpThreads, 0, s>>>(w, n, W, col, off, diag, r, x, zero_x, out, (size_t)n * K);
+  DEC_CHECK_LAUNCH();
+}
+
+#define DEC_INST(T, K)                                                                                             \
+  template void launch_mlp_smooth<T, K>(const MlpWeights&, int, int, const int32_t*, const T*, const T*, const T*, \
+                                        const T*, int, T*, int, cudaStream_t);
+DEC_INST(float, 1) DEC_INST(float, 2) DEC_INST(float, 4) DEC_INST(float, 8) DEC_INST(float, 16) DEC_INST(float, 32)
+DEC_INST(double, 1) DEC_INST(double, 2) DEC_INST(double, 4) DEC_INST(double, 8) DEC_INST(double, 16)
+DEC_INST(double, 32)
+#undef DEC_INST
+
+// ---------------------------------------------------------------------------------------------
+// CUDA-core forward (FP32, the inference roundings) and the training kernels
+// ---------------------------------------------------------------------------------------------
+__device__ float mlp_forward_cc(const float* f, const __nv_bfloat16* __restrict__ w1b,
+                                const __nv_bfloat16* __restrict__ w2b, const float* __restrict__ p) {
+  float x0[kMlpIn], h1[kMlpH];
+  for (int k = 0; k < kMlpIn; ++k) x0[k] = __bfloat162float(__float2bfloat16_rn(f[k]));
+  for (int j = 0; j < kMlpH; ++j) {
+    float s = p[kOffB1 + j];
+#pragma unroll
+    for (int k = 0; k < kMlpIn; ++k) s += __bfloat162float(w1b[j * kMlpIn + k]) * x0[k];
+    h1[j] = __bfloat162float(__float2bfloat16_rn(fmaxf(s, 0.f)));
+  }
+  float y = p[kOffB3];
+  for (int j = 0; j < kMlpH; ++j) {
+    float s = p[kOffB2 + j];
+    for (int i = 0; i < kMlpH; ++i) s += __bfloat162float(w2b[j * kMlpH + i]) * h1[i];
+    y += p[kOffW3 + j] * fmaxf(s, 0.f);
+  }
+  return y;
+}
+
+__global__ void k_mlp_eval_cc(int64_t n, const float* __restrict__ x, float* __restrict__ y,
+                              const __nv_bfloat16* __restrict__ w1b, const __nv_bfloat16* __restrict__ w2b,
+                              const float* __restrict__ p) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    y[q] = mlp_forward_cc(x + q * 16, w1b, w2b, p);
+}
+
+// Activations of the backward batch, structure of arrays [row][batch]: x0 (16 rows),
+// h1 = bf16(relu(z1)) (64), relu(z2) (64), dz1 (64), dz2 (64).
+constexpr int kActX0 = 0, kActH1 = 16, kActR2 = 80, kActDz1 = 144, kActDz2 = 208, kActRows = 272;
+
+// Forward + backward of one sample: stores its activations in batch column j and dL/dy in dyb[j].
+// The ReLU masks are z1 > 0 and z2 > 0.
+__device__ void backward_sample(const float* f, float d, const __nv_bfloat16* __restrict__ w1b,
+                                const __nv_bfloat16* __restrict__ w2b, const float* __restrict__ p,
+                                float* __restrict__ act, int64_t j, int64_t B, float* __restrict__ dyb) {
+  float x0[kMlpIn], z1[kMlpH], h1[kMlpH], dz2[kMlpH];
+  for (int k = 0; k < kMlpIn; ++k) x0[k] = __bfloat162float(__float2bfloat16_rn(f[k]));
+  for (int jj = 0; jj < kMlpH; ++jj) {
+    float s = p[kOffB1 + jj];
+#pragma unroll
+    for (int k = 0; k < kMlpIn; ++k) s += __bfloat162float(w1b[jj * kMlpIn + k]) * x0[k];
+    z1[jj] = s;
+    h1[jj] = __bfloat162float(__float2bfloat16_rn(fmaxf(s, 0.f)));
+  }
+  for (int k = 0; k < kMlpIn; ++k) act[(size_t)(kActX0 + k) * B + j] = x0[k];
+  for (int jj = 0; jj < kMlpH; ++jj) {
+    float s = p[kOffB2 + jj];
+    for (int i = 0; i < kMlpH; ++i) s += __bfloat162float(w2b[jj * kMlpH + i]) * h1[i];
+    dz2[jj] = s > 0.f ? d * p[kOffW3 + jj] : 0.f;
+    act[(size_t)(kActH1 + jj) * B + j] = h1[jj];
+    act[(size_t)(kActR2 + jj) * B + j] = fmaxf(s, 0.f);
+    act[(size_t)(kActDz2 + jj) * B + j] = dz2[jj];
+  }
+  for (int i = 0; i < kMlpH; ++i) {
+    float dh = 0.f;
+    for (int jj = 0; jj < kMlpH; ++jj) dh += __bfloat162float(w2b[jj * kMlpH + i]) * dz2[jj];
+    act[(size_t)(kActDz1 + i) * B + j] = z1[i] > 0.f ? dh : 0.f;
+  }
+  dyb[j] = d;
+}
+
+// Backward of n given feature rows with given dL/dy (the gradient check entry point).
+__global__ void k_bwd_direct(int64_t n, const float* __restrict__ x, const float* __restrict__ dy,
+                             const __nv_bfloat16* __restrict__ w1b, const __nv_bfloat16* __restrict__ w2b,
+                             const float* __restrict__ p, float* __restrict__ act, float* __restrict__ dyb) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    backward_sample(x + q * 16, dy[q], w1b, w2b, p, act, q, n, dyb);
+}
+
+// Features of sample (vertex i, field rs) on a reference-ordered Laplacian / Helmholtz operator
+// (sorted ELL with the diagonal inside, padding column -1).
+__device__ void op_features(int i, int Wf, const int32_t* __restrict__ col, const double* __restrict__ val,
+                            const double* __restrict__ rs, float* f, float* dsc) {
+  double di = 0.0;
+  for (int q = 0; q < Wf; ++q)
+    if (col[(size_t)i * Wf + q] == i) di += val[(size_t)i * Wf + q];
+  float nb[6], cp[6], sabs = 0.f;
+  int nn = 0;
+  const float dif = (float)di;
+  for (int q = 0; q < Wf; ++q) {
+    const int c = col[(size_t)i * Wf + q];
+    if (c < 0 || c == i) continue;
+    const float o = (float)val[(size_t)i * Wf + q];
+    sabs += fabsf(o);
+    if (nn < 6) {
+      nb[nn] = (float)rs[c];
+      cp[nn] = o / dif;
+      ++nn;
+    }
+  }
+  float scale;
+  mlp_features((float)rs[i], nb, cp, nn, 1.f - sabs / dif, f, &scale);
+  *dsc = scale / dif;
+}
+
+__global__ void k_op_features(int n, int S, int Wf, const int32_t* __restrict__ col, const double* __restrict__ val,
+                              const double* __restrict__ r, float* __restrict__ feat, float* __restrict__ dscale) {
+  const int64_t N = (int64_t)n * S;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < N; q += (int64_t)gridDim.x * blockDim.x) {
+    const int s = (int)(q / n), i = (int)(q % n);
+    float f[16], dsc;
+    op_features(i, Wf, col, val, r + (size_t)s * n, f, &dsc);
+    for (int k = 0; k < 16; ++k) feat[q * 16 + k] = f[k];
+    dscale[q] = dsc;
+  }
+}
+
+// δ = dscale · MLP(features) for all n·S samples (tensor cores, the inference kernel's numerics).
+__global__ void __launch_bounds__(kMlpThreads) k_train_fwd(int n, int S, int Wf, const int32_t* __restrict__ col,
+                                                           const double* __restrict__ val, const double* __restrict__ r,
+                                                           MlpWeights w, double* __restrict__ delta,
+                                                           float* __restrict__ dscale) {
+  __shared__ MlpSmem sm;
+  __shared__ __align__(16) __nv_bfloat16 xs[kMlpWarps][kTile * kXsStride];
+  load_weights(sm, w);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t N = (int64_t)n * S;
+  const int64_t ntiles = (N + kTile - 1) / kTile;
+  for (int64_t tile = (int64_t)blockIdx.x * kMlpWarps + warp; tile < ntiles; tile += (int64_t)gridDim.x * kMlpWarps) {
+    const int64_t q = tile * kTile + lane;
+    float f[16], dsc = 0.f;
+    if (q < N) {
+      const int s = (int)(q / n), i = (int)(q % n);
+      op_features(i, Wf, col, val, r + (size_t)s * n, f, &dsc);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) f[k] = 0.f;
+    }
+    store_row(xs[warp], lane, f);
+    __syncwarp();
+    const float yv = mlp_tile32(sm, xs[warp]);
+    if (q < N) {
+      delta[q] = (double)(dsc * yv);
+      dscale[q] = dsc;
+    }
+    __syncwarp();
+  }
+}
+
+// n_s = Σ_i ⋆0_i r_si² / a_ii per field (one CTA per field).
+__global__ void __launch_bounds__(256) k_train_norms(int n, int Wf, const int32_t* __restrict__ col,
+                                                     const double* __restrict__ val, const double* __restrict__ star0,
+                                                     const double* __restrict__ r, double* __restrict__ nrm) {
+  const double* rs = r + (size_t)blockIdx.x * n;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double di = 0.0;
+    for (int q = 0; q < Wf; ++q)
+      if (col[(size_t)i * Wf + q] == i) di += val[(size_t)i * Wf + q];
+    acc += star0[i] * rs[i] * rs[i] / di;
+  }
+  __shared__ double sh[256];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) nrm[blockIdx.x] = sh[0] > 0 ? sh[0] : 1.0;
+}
+
+// dL/dδ = 2 w (A δ - r), w = ⋆0_i / (S n_s); dy = dL/dδ · dscale; loss partials Σ w δ (A δ - 2 r).
+constexpr int kLossBlocks = 512;
+__global__ void __launch_bounds__(256) k_train_loss(int n, int S, const double* __restrict__ r,
+                                                    const double* __restrict__ aq, const double* __restrict__ delta,
+                                                    const double* __restrict__ star0, const double* __restrict__ nrm,
+                                                    const float* __restrict__ dscale, double* __restrict__ dy,
+                                                    double* __restrict__ lpart) {
+  const int64_t N = (int64_t)n * S;
+  double acc = 0.0;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < N; k += (int64_t)gridDim.x * blockDim.x) {
+    const int s = (int)(k / n), i = (int)(k % n);
+    const double w = star0[i] / (nrm[s] * S);
+    dy[k] = 2.0 * w * (aq[k] - r[k]) * (double)dscale[k];
+    acc += w * delta[k] * (aq[k] - 2.0 * r[k]);
+  }
+  __shared__ double sh[256];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) lpart[blockIdx.x] = sh[0];
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// Backward over the batch: column j is sample j when the fields hold at most B samples, else a
+// sample drawn uniformly with replacement from (seed, step, j); dL/dy is scaled by N / B so the
+// batch gradient estimates the full one.
+__global__ void k_train_bwd(int n, int S, int64_t B, uint64_t seed, int64_t step, int Wf,
+                            const int32_t* __restrict__ col, const double* __restrict__ val,
+                            const double* __restrict__ r, const __nv_bfloat16* __restrict__ w1b,
+                            const __nv_bfloat16* __restrict__ w2b, const float* __restrict__ p,
+                            const double* __restrict__ dy, float* __restrict__ act, float* __restrict__ dyb) {
+  const int64_t N = (int64_t)n * S;
+  const bool sample = N > B;
+  const int64_t Bn = sample ? B : N;
+  const double scale = sample ? (double)N / (double)B : 1.0;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < Bn; j += (int64_t)gridDim.x * blockDim.x) {
+    int64_t q = j;
+    if (sample) {
+      const uint64_t h = mix64(seed + 0x9E3779B97F4A7C15ull * (uint64_t)(step + 1) + 0xD1B54A32D192ED03ull * (uint64_t)j);
+      q = (int64_t)(h % (uint64_t)N);
+    }
+    const int s = (int)(q / n), i = (int)(q % n);
+    float f[16], dsc;
+    op_features(i, Wf, col, val, r + (size_t)s * n, f, &dsc);
+    backward_sample(f, (float)(dy[q] * scale), w1b, w2b, p, act, j, Bn, dyb);
+  }
+}
+
+// Parameter gradient partials over one chunk of batch columns per CTA, in a fixed order:
+// dW1 = Σ dz1 x0ᵀ, db1 = Σ dz1, dW2 = Σ dz2 h1ᵀ, db2 = Σ dz2, dw3 = Σ dy relu(z2), db3 = Σ dy.
+constexpr int kGradThreads = 256, kGradTile = 16, kGradChunk = 256, kMaxChunks = 1024;
+__global__ void __launch_bounds__(kGradThreads) k_train_grad(int64_t B, int64_t chunk, const float* __restrict__ act,
+                                                             const float* __restrict__ dyb, float* __restrict__ gpart) {
+  __shared__ float sx0[kMlpIn][kGradTile], sh1[kMlpH][kGradTile], sr2[kMlpH][kGradTile];
+  __shared__ float sdz1[kMlpH][kGradTile], sdz2[kMlpH][kGradTile], sdy[kGradTile];
+  constexpr int kPer = (kMlpNParam + kGradThreads - 1) / kGradThreads;
+  float acc[kPer];
+#pragma unroll
+  for (int m = 0; m < kPer; ++m) acc[m] = 0.f;
+  const int64_t lo = blockIdx.x * chunk, hi = min(B, lo + chunk);
+  for (int64_t b = lo; b < hi; b += kGradTile) {
+    for (int e = threadIdx.x; e < kGradTile * (kActRows + 1); e += kGradThreads) {
+      const int c = e % kGradTile, row = e / kGradTile;
+      const int64_t q = b + c;
+      const bool ok = q < hi;
+      const float v = ok ? (row < kActRows ? act[(size_t)row * B + q] : dyb[q]) : 0.f;
+      if (row < kActH1) sx0[row][c] = v;
+      else if (row < kActR2) sh1[row - kActH1][c] = v;
+      else if (row < kActDz1) sr2[row - kActR2][c] = v;
+      else if (row < kActDz2) sdz1[row - kActDz1][c] = v;
+      else if (row < kActRows) sdz2[row - kActDz2][c] = v;
+      else sdy[c] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < kPer; ++m) {
+      const int pi = threadIdx.x + m * kGradThreads;
+      if (pi >= kMlpNParam) break;
+      float s = 0.f;
+      if (pi < kOffB1) {
+        const int i = pi / kMlpIn, k = pi % kMlpIn;
+#pragma unroll
+        for (int c = 0; c < kGradTile; ++c) s += sdz1[i][c] * sx0[k][c];
+      } else if (pi < kOffW2) {
+#pragma unroll
+        for (int c = 0; c < kGradTile; ++c) s += sdz1[pi - kOffB1][c];
+      } else if (pi < kOffB2) {
+        const int j = (pi - kOffW2) / kMlpH, i = (pi - kOffW2) % kMlpH;
+#pragma unroll
+        for (int c = 0; c < kGradTile; ++c) s += sdz2[j][c] * sh1[i][c];
+      } else if (pi < kOffW3) {
+#pragma unroll
+        for (int c = 0; c < kGradTile; ++c) s += sdz2[pi - kOffB2][c];
+      } else if (pi < kOffB3) {
+#pragma unroll
+        for (int c = 0; c < kGradTile; ++c) s += sdy[c] * sr2[pi - kOffW3][c];
+      } else {
+#pragma unroll
+        for (int c = 0; c < kGradTile; ++c) s += sdy[c];
+      }
+      acc[m] += s;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int m = 0; m < kPer; ++m) {
+    const int pi = threadIdx.x + m * kGradThreads;
+    if (pi < kMlpNParam) gpart[(size_t)blockIdx.x * kMlpNParam + pi] = acc[m];
+  }
+}
+
+__global__ void k_grad_reduce(int nchunks, const float* __restrict__ gpart, float* __restrict__ grad) {
+  for (int pi = blockIdx.x * blockDim.x + threadIdx.x; pi < kMlpNParam; pi += gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int c = 0; c < nchunks; ++c) s += gpart[(size_t)c * kMlpNParam + pi];
+    grad[pi] = s;
+  }
+}
+
+__global__ void k_refresh_bf16(const float* __restrict__ p, __nv_bfloat16* __restrict__ w1b,
+                               __nv_bfloat16* __restrict__ w2b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kMlpH * kMlpH; i += gridDim.x * blockDim.x) {
+    if (i < kMlpH * kMlpIn) w1b[i] = __float2bfloat16_rn(p[kOffW1 + i]);
+    w2b[i] = __float2bfloat16_rn(p[kOffW2 + i]);
+  }
+}
+
+// Adam (β1 = 0.9, β2 = 0.999, ε = 1e-8, bias-corrected) on the FP32 masters.
+__global__ void k_adam(int64_t t, float lr, const float* __restrict__ g, float* __restrict__ p, float* __restrict__ m,
+                       float* __restrict__ v) {
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  const float c1 = 1.f - powf(b1, (float)t), c2 = 1.f - powf(b2, (float)t);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kMlpNParam; i += gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  }
+}
+
+static uint64_t splitmix(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+static unsigned eval_grid(long long samples) {
+  const long long tiles = (samples + kTile - 1) / kTile;
+  return (unsigned)std::max<long long>(1, std::min<long long>((tiles + kMlpWarps - 1) / kMlpWarps, num_sms() * 4LL));
+}
+
+static void ensure_scratch(dec_mlp& m, size_t N, size_t B, int S) {
+  if (m.cap_n < N) {
+    m.delta.alloc(N);
+    m.q.alloc(N);
+    m.dy.alloc(N);
+    m.dsc.alloc(N);
+    m.cap_n = N;
+  }
+  if (m.cap_b < B) {
+    m.act.alloc((size_t)kActRows * B);
+    m.dyb.alloc(B);
+    m.cap_b = B;
+  }
+  if (m.nrm.n < (size_t)S) m.nrm.alloc(std::max<size_t>(S, 64));
+  if (m.lpart.n < (size_t)kLossBlocks) m.lpart.alloc(kLossBlocks);
+  if (m.gpart.n < (size_t)kMaxChunks * kMlpNParam) m.gpart.alloc((size_t)kMaxChunks * kMlpNParam);
+}
+
+static int grad_chunks(int64_t B, int64_t* chunk) {
+  int nch = (int)std::min<int64_t>(kMaxChunks, std::max<int64_t>(1, (B + kGradChunk - 1) / kGradChunk));
+  *chunk = (B + nch - 1) / nch;
+  return nch;
+}
+
+static void reduce_grad(dec_mlp& m, int64_t B, float* grad, cudaStream_t s) {
+  int64_t chunk;
+  const int nch = grad_chunks(B, &chunk);
+  k_train_grad<<<nch, kGradThreads, 0, s>>>(B, chunk, m.act.p, m.dyb.p, m.gpart.p);
+  k_grad_reduce<<<(kMlpNParam + 255) / 256, 256, 0, s>>>(nch, m.gpart.p, grad);
+  DEC_CHECK_LAUNCH();
+}
+
+static void check_train_op(const dec_op* op) {
+  require(op != nullptr, "mlp: null operator");
+  require(op->kind == DEC_OP_LAPLACE0 || op->kind == DEC_OP_HELMHOLTZ0,
+          "mlp: training needs a Laplacian / Helmholtz operator");
+  require(op->dtype == DEC_F64, "mlp: training needs an FP64 operator");
+}
+
+// δ, A δ, dL/dy and the loss partials of S fields on the operator's mesh.
+static void loss_and_dy(dec_mlp& m, dec_op* op, const double* r, int S, cudaStream_t s) {
+  const int n = op->m->nv;
+  const int64_t N = (int64_t)n * S;
+  k_train_fwd<<<eval_grid(N), kMlpThreads, 0, s>>>(n, S, op->W, op->col.p, op->val64.p, r, m.view(), m.delta.p,
+                                                   m.dsc.p);
+  DEC_CHECK_LAUNCH();
+  for (int j = 0; j < S; ++j) op_apply_impl(op, m.delta.p + (size_t)j * n, m.q.p + (size_t)j * n, 1.0, 0.0, s);
+  k_train_loss<<<kLossBlocks, 256, 0, s>>>(n, S, r, m.q.p, m.delta.p, op->m->star0.p, m.nrm.p, m.dsc.p, m.dy.p,
+                                           m.lpart.p);
+  DEC_CHECK_LAUNCH();
+}
+
+static double host_loss(dec_mlp& m, cudaStream_t s) {
+  std::vector<double> lp(kLossBlocks);
+  DEC_CUDA(cudaMemcpyAsync(lp.data(), m.lpart.p, kLossBlocks * sizeof(double), cudaMemcpyDeviceToHost, s));
+  DEC_CUDA(cudaStreamSynchronize(s));
+  double tot = 0;
+  for (double v : lp) tot += v;
+  return tot;
+}
+
+// CRC-32 (IEEE 802.3, reflected polynomial 0xEDB88320), bitwise.
+static uint32_t crc32(const unsigned char* p, size_t n) {
+  uint32_t c = 0xFFFFFFFFu;
+  for (size_t i = 0; i < n; ++i) {
+    c ^= p[i];
+    for (int k = 0; k < 8; ++k) c = (c >> 1) ^ (0xEDB88320u & (0u - (c & 1u)));
+  }
+  return ~c;
+}
+
+}  // namespace decb
+
+using namespace decb;
+
+dec_mlp* mlp_create_impl(uint64_t seed) {
+  auto* m = new dec_mlp();
+  try {
+    // Xavier (Glorot) uniform U(-a, a), a = sqrt(6 / (fan_in + fan_out)), from the splitmix64
+    // stream of the seed; biases zero.
+    std::vector<float> p(kMlpNParam, 0.f);
+    uint64_t st = seed;
+    auto fill = [&](int off, int cnt, int fin, int fout) {
+      const double a = std::sqrt(6.0 / (fin + fout));
+      for (int i = 0; i < cnt; ++i) {
+        const double u = (double)(splitmix(st) >> 11) * (1.0 / 9007199254740992.0);
+        p[off + i] = (float)((2.0 * u - 1.0) * a);
+      }
+    };
+    fill(kOffW1, kMlpH * kMlpIn, kMlpIn, kMlpH);
+    fill(kOffW2, kMlpH * kMlpH, kMlpH, kMlpH);
+    fill(kOffW3, kMlpH, kMlpH, 1);
+    m->master.upload(p);
+    m->adam_m.alloc(kMlpNParam);
+    m->adam_v.alloc(kMlpNParam);
+    DEC_CUDA(cudaMemset(m->adam_m.p, 0, m->adam_m.bytes()));
+    DEC_CUDA(cudaMemset(m->adam_v.p, 0, m->adam_v.bytes()));
+    m->grad.alloc(kMlpNParam);
+    m->w1b.alloc(kMlpH * kMlpIn);
+    m->w2b.alloc(kMlpH * kMlpH);
+    k_refresh_bf16<<<16, 256>>>(m->master.p, m->w1b.p, m->w2b.p);
+    DEC_CHECK_LAUNCH();
+    DEC_CUDA(cudaDeviceSynchronize());
+  } catch (...) {
+    delete m;
+    throw;
+  }
+  return m;
+}
+
+void mlp_destroy_impl(dec_mlp* m) { delete m; }
+
+void mlp_params_impl(dec_mlp* m, float* out, const float* in) {
+  require(m != nullptr, "mlp: null handle");
+  if (out) DEC_CUDA(cudaMemcpy(out, m->master.p, m->master.bytes(), cudaMemcpyDeviceToHost));
+  if (in) {
+    DEC_CUDA(cudaMemcpy(m->master.p, in, m->master.bytes(), cudaMemcpyHostToDevice));
+    k_refresh_bf16<<<16, 256>>>(m->master.p, m->w1b.p, m->w2b.p);
+    DEC_CHECK_LAUNCH();
+    DEC_CUDA(cudaDeviceSynchronize());
+  }
+}
+
+int64_t mlp_step_impl(const dec_mlp* m) {
+  require(m != nullptr, "mlp: null handle");
+  return m->step;
+}
+
+MlpWeights mlp_weights(const dec_mlp* m) {
+  require(m != nullptr, "mlp: null handle");
+  return m->view();
+}
+
+void mlp_eval_impl(dec_mlp* m, const float* x, int64_t n, float* y, int tensor_cores, void* stream) {
+  require(m != nullptr && n >= 0 && (n == 0 || (x != nullptr && y != nullptr)), "mlp: bad eval arguments");
+  require((reinterpret_cast<uintptr_t>(x) & 15) == 0, "mlp: features must be 16-byte aligned");
+  if (n == 0) return;
+  cudaStream_t s = as_stream(stream);
+  if (tensor_cores) k_mlp_eval_tc<<<eval_grid(n), kMlpThreads, 0, s>>>(n, x, y, m->view());
+  else k_mlp_eval_cc<<<grid_for(n, 128), 128, 0, s>>>(n, x, y, m->w1b.p, m->w2b.p, m->master.p);
+  DEC_CHECK_LAUNCH();
+}
+
+void mlp_grad_impl(dec_mlp* m, const float* x, const float* dy, int64_t n, float* grad, void* stream) {
+  require(m != nullptr && x != nullptr && dy != nullptr && grad != nullptr && n > 0, "mlp: bad grad arguments");
+  cudaStream_t s = as_stream(stream);
+  ensure_scratch(*m, 1, (size_t)n, 1);
+  k_bwd_direct<<<grid_for(n, 128), 128, 0, s>>>(n, x, dy, m->w1b.p, m->w2b.p, m->master.p, m->act.p, m->dyb.p);
+  DEC_CHECK_LAUNCH();
+  reduce_grad(*m, n, grad, s);
+}
+
+void mlp_features_impl(const dec_op* op, const double* r, int S, float* feat, float* dscale, void* stream) {
+  check_train_op(op);
+  require(r != nullptr && feat != nullptr && dscale != nullptr && S >= 1, "mlp: bad feature arguments");
+  const int n = op->m->nv;
+  k_op_features<<<grid_for((long long)n * S, 128), 128, 0, as_stream(stream)>>>(n, S, op->W, op->col.p, op->val64.p, r,
+                                                                                 feat, dscale);
+  DEC_CHECK_LAUNCH();
+}
+
+void mlp_loss_grad_impl(dec_mlp* m, dec_op* op, const double* r, int S, double* loss, float* grad, void* stream) {
+  require(m != nullptr && r != nullptr && S >= 1, "mlp: bad loss arguments");
+  check_train_op(op);
+  cudaStream_t s = as_stream(stream);
+  const int n = op->m->nv;
+  const int64_t N = (int64_t)n * S;
+  ensure_scratch(*m, (size_t)N, (size_t)N, S);
+  k_train_norms<<<S, 256, 0, s>>>(n, op->W, op->col.p, op->val64.p, op->m->star0.p, r, m->nrm.p);
+  loss_and_dy(*m, op, r, S, s);
+  if (grad) {
+    k_train_bwd<<<grid_for(N, 128), 128, 0, s>>>(n, S, N, 0, 0, op->W, op->col.p, op->val64.p, r, m->w1b.p, m->w2b.p,
+                                                 m->master.p, m->dy.p, m->act.p, m->dyb.p);
+    DEC_CHECK_LAUNCH();
+    reduce_grad(*m, N, grad, s);
+  }
+  if (loss) *loss = host_loss(*m, s);
+}
+
+void mlp_train_impl(dec_mlp* m, dec_op* op, const double* r, int S, int steps, double lr, int64_t batch,
+                    uint64_t seed, double* losses, void* stream) {
+  require(m != nullptr && r != nullptr && S >= 1 && steps >= 0 && batch >= 1 && lr > 0, "mlp: bad train arguments");
+  check_train_op(op);
+  cudaStream_t s = as_stream(stream);
+  const int n = op->m->nv;
+  const int64_t N = (int64_t)n * S;
+  const int64_t Bn = std::min<int64_t>(batch, N);
+  ensure_scratch(*m, (size_t)N, (size_t)Bn, S);
+  k_train_norms<<<S, 256, 0, s>>>(n, op->W, op->col.p, op->val64.p, op->m->star0.p, r, m->nrm.p);
+  for (int it = 0; it < steps; ++it) {
+    loss_and_dy(*m, op, r, S, s);
+    k_train_bwd<<<grid_for(Bn, 128), 128, 0, s>>>(n, S, batch, seed, m->step, op->W, op->col.p, op->val64.p, r,
+                                                  m->w1b.p, m->w2b.p, m->master.p, m->dy.p, m->act.p, m->dyb.p);
+    DEC_CHECK_LAUNCH();
+    reduce_grad(*m, Bn, m->grad.p, s);
+    ++m->step;
+    k_adam<<<(kMlpNParam + 255) / 256, 256, 0, s>>>(m->step, (float)lr, m->grad.p, m->master.p, m->adam_m.p,
+                                                    m->adam_v.p);
+    k_refresh_bf16<<<16, 256, 0, s>>>(m->master.p, m->w1b.p, m->w2b.p);
+    DEC_CHECK_LAUNCH();
+    if (losses) losses[it] = host_loss(*m, s);  // the loss before this step's update
+  }
+}
+
+// Checkpoint: "DECMLP01" | u32 version | u32 nparam | i64 step | f32 master, adam_m, adam_v
+// (nparam each) | u32 CRC-32 of everything before it.
+static constexpr char kMagic[8] = {'D', 'E', 'C', 'M', 'L', 'P', '0', '1'};
+
+void mlp_save_impl(const dec_mlp* m, const char* path) {
+  require(m != nullptr && path != nullptr, "mlp: bad save arguments");
+  DEC_CUDA(cudaDeviceSynchronize());
+  std::vector<unsigned char> buf;
+  auto put = [&](const void* p, size_t n) {
+    const unsigned char* c = static_cast<const unsigned char*>(p);
+    buf.insert(buf.end(), c, c + n);
+  };
+  const uint32_t version = 1, np = kMlpNParam;
+  put(kMagic, 8);
+  put(&version, 4);
+  put(&np, 4);
+  put(&m->step, 8);
+  for (const DArr<float>* a : {&m->master, &m->adam_m, &m->adam_v}) {
+    std::vector<float> h = a->download();
+    put(h.data(), h.size() * 4);
+  }
+  const uint32_t crc = crc32(buf.data(), buf.size());
+  put(&crc, 4);
+  FILE* f = std::fopen(path, "wb");
+  require(f != nullptr, std::string("mlp: cannot open ") + path + " for writing");
+  const size_t w = std::fwrite(buf.data(), 1, buf.size(), f);
+  const int rc = std::fclose(f);
+  require(w == buf.size() && rc == 0, std::string("mlp: short write to ") + path);
+}
+
+void mlp_load_impl(dec_mlp* m, const char* path) {
+  require(m != nullptr && path != nullptr, "mlp: bad load arguments");
+  FILE* f = std::fopen(path, "rb");
+  require(f != nullptr, std::string("mlp: cannot open ") + path);
+  std::vector<unsigned char> buf;
+  unsigned char tmp[65536];
+  size_t k;
+  while ((k = std::fread(tmp, 1, sizeof(tmp), f)) > 0) buf.insert(buf.end(), tmp, tmp + k);
+  std::fclose(f);
+  const size_t body = 8 + 4 + 4 + 8 + 3 * (size_t)kMlpNParam * 4;
+  require(buf.size() == body + 4, "mlp: checkpoint has the wrong size");
+  require(std::memcmp(buf.data(), kMagic, 8) == 0, "mlp: not a checkpoint");
+  uint32_t version, np, crc;
+  int64_t step;
+  std::memcpy(&version, buf.data() + 8, 4);
+  std::memcpy(&np, buf.data() + 12, 4);
+  std::memcpy(&step, buf.data() + 16, 8);
+  std::memcpy(&crc, buf.data() + body, 4);
+  require(version == 1 && np == (uint32_t)kMlpNParam, "mlp: unsupported checkpoint version / shape");
+  require(crc32(buf.data(), body) == crc, "mlp: checkpoint CRC mismatch");
+  const unsigned char* p = buf.data() + 24;
+  for (DArr<float>* a : {&m->master, &m->adam_m, &m->adam_v}) {
+    DEC_CUDA(cudaMemcpy(a->p, p, (size_t)kMlpNParam * 4, cudaMemcpyHostToDevice));
+    p += (size_t)kMlpNParam * 4;
+  }
+  m->step = step;
+  k_refresh_bf16<<<16, 256>>>(m->master.p, m->w1b.p, m->w2b.p);
+  DEC_CHECK_LAUNCH();
+  DEC_CUDA(cudaDeviceSynchronize());
+}

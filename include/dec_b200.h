@@ -44,6 +44,7 @@ typedef struct dec_mesh dec_mesh;
 typedef struct dec_wedge_plan dec_wedge_plan;
 typedef struct dec_op dec_op;
 typedef struct dec_mg dec_mg;
+typedef struct dec_mlp dec_mlp;
 
 /*
  * A primal 2D delta set with embedding, i.e. the fields of EmbeddedDeltaSet2D{Bool,Point3d}
@@ -155,7 +156,9 @@ dec_status dec_op_destroy(dec_op* op);
 typedef enum dec_smoother {
   DEC_SMOOTH_JACOBI = 0,     /* damped Jacobi, `pre`/`post` sweeps */
   DEC_SMOOTH_CHEBYSHEV = 1,  /* Chebyshev-Jacobi of degree `pre`/`post` */
-  DEC_SMOOTH_CG = 2          /* Krylov.jl cg with itmax = steps (the reference's smoother) */
+  DEC_SMOOTH_CG = 2,         /* Krylov.jl cg with itmax = steps (the reference's smoother) */
+  DEC_SMOOTH_LEARNED = 3     /* per-vertex MLP correction on the tensor cores (dec_mg_set_smoother_mlp),
+                                `pre`/`post` sweeps; Chebyshev-Jacobi is the fallback */
 } dec_smoother;
 
 typedef struct dec_mg_options {
@@ -175,6 +178,10 @@ typedef struct dec_mg_options {
   int32_t reorder;         /* 1: store each level in a locality (Morton) order internally */
   int32_t coarse_max;      /* > 0: cycles stop at the first level with at most this many vertices
                               (<= 1024) and solve it directly; 0: at the hierarchy's coarsest level */
+  double fallback_rho;     /* learned smoother: dec_mg_solve switches to the plain smoother for the
+                              rest of the solve when a refinement step reduces the worst relative
+                              residual by less than this factor (or it is not finite); that step is
+                              undone and redone with the plain smoother */
 } dec_mg_options;
 
 typedef struct dec_solve_report {
@@ -184,6 +191,8 @@ typedef struct dec_solve_report {
   double seconds;          /* device time of the solve */
   int64_t launches;        /* kernels launched by the solve */
   int32_t rhs_block;       /* panel width used */
+  int32_t fallback_iteration; /* learned smoother: refinement step at which the plain smoother took
+                                 over, -1 if it did not */
 } dec_solve_report;
 
 void dec_mg_default_options(dec_mg_options* o);
@@ -204,13 +213,59 @@ dec_status dec_mg_solve_host(dec_mg* mg, double* u_host, const double* b_host, i
                              int32_t max_iters, int32_t use_initial_guess, dec_solve_report* report,
                              void* stream);
 
+/* Learned smoother for DEC_SMOOTH_LEARNED: the hierarchy reads the network's weights at every
+ * cycle (the network must outlive its use; retraining takes effect at the next cycle).  NULL
+ * detaches it. */
+dec_status dec_mg_set_smoother_mlp(dec_mg* mg, const dec_mlp* mlp);
+
+/* ---- learned smoother network (no counterpart in the reference): per-vertex MLP 16 -> 64 -> 64
+ *      -> 1 with ReLU; parameters flat FP32 W1[64][16] | b1[64] | W2[64][64] | b2[64] | w3[64] | b3;
+ *      inference with W1, W2, the features and the first hidden layer in BF16, FP32 accumulation.
+ *      Features of vertex i from the residual field r and operator row i (Laplacian/Helmholtz):
+ *      r_i/s, six neighbour residuals r_j/s, six couplings a_ij/a_ii (column order, zero-padded),
+ *      1 - sum_j |a_ij|/a_ii, valence/6, 0; s = max |r| over the 1-ring.  The smoother applies
+ *      x_i += (s / a_ii) y_i. ---------------------------------------------------------------- */
+#define DEC_MLP_NPARAM 5313
+/* Xavier-uniform weights (splitmix64 stream of `seed`), zero biases, Adam state zero. */
+dec_status dec_mlp_create(uint64_t seed, dec_mlp** out);
+dec_status dec_mlp_destroy(dec_mlp* mlp);
+/* Host copies of the FP32 master parameters (DEC_MLP_NPARAM floats); either pointer may be NULL. */
+dec_status dec_mlp_get_params(const dec_mlp* mlp, float* params);
+dec_status dec_mlp_set_params(dec_mlp* mlp, const float* params);
+dec_status dec_mlp_step(const dec_mlp* mlp, int64_t* step);
+/* y[n] = MLP(x[n][16]) on device memory; tensor_cores = 0 evaluates on the CUDA cores. */
+dec_status dec_mlp_eval(dec_mlp* mlp, const float* x, int64_t n, float* y, int32_t tensor_cores, void* stream);
+/* grad[DEC_MLP_NPARAM] (device) = sum_q dy[q] d MLP(x_q) / d params. */
+dec_status dec_mlp_grad(dec_mlp* mlp, const float* x, const float* dy, int64_t n, float* grad, void* stream);
+/* Features (n*S x 16) and the correction scales s / a_ii (n*S) of S residual fields r (device,
+ * column-major n x S) on an FP64 Laplacian / Helmholtz operator. */
+dec_status dec_mlp_features(const dec_op* op, const double* r, int32_t S, float* features, float* scales,
+                            void* stream);
+/* Energy-norm loss of one smoothing step on S residual fields, and its full parameter gradient
+ * (device, may be NULL):
+ *   L = (1/S) sum_s (d_s' M A d_s - 2 d_s' M r_s) / n_s,  d = (s/a_ii) MLP(features),
+ *   M = diag(star0), n_s = sum_i star0_i r_si^2 / a_ii. */
+dec_status dec_mlp_loss_grad(dec_mlp* mlp, dec_op* op, const double* r, int32_t S, double* loss, float* grad,
+                             void* stream);
+/* `steps` Adam steps (lr; beta 0.9 / 0.999, eps 1e-8) on S residual fields; each step's gradient
+ * comes from `batch` vertex samples (all of them when n*S <= batch, else drawn with replacement
+ * from the stream of (seed, step)).  losses (host, may be NULL) receives each step's loss before
+ * its update and then synchronises the stream every step. */
+dec_status dec_mlp_train(dec_mlp* mlp, dec_op* op, const double* r, int32_t S, int32_t steps, double lr,
+                         int64_t batch, uint64_t seed, double* losses, void* stream);
+/* Checkpoint of parameters, Adam moments and step counter ("DECMLP01", version 1, CRC-32). */
+dec_status dec_mlp_save(const dec_mlp* mlp, const char* path);
+dec_status dec_mlp_load(dec_mlp* mlp, const char* path);
+
 /* ---- profiling (no counterpart in the reference; its benchmarks print timings only,
  *      test/Benchmarks.jl:128-140) ------------------------------------------------------ */
 typedef enum dec_mg_kernel {
   DEC_KERNEL_SWEEP = 0,     /* Chebyshev / Jacobi smoothing sweep */
   DEC_KERNEL_RESIDUAL = 1,  /* FP64 residual with norms */
   DEC_KERNEL_RESTRICT = 2,
-  DEC_KERNEL_PROLONG = 3
+  DEC_KERNEL_PROLONG = 3,
+  DEC_KERNEL_MLP = 4        /* learned smoothing step (the MLP kernel alone; 10,368 FLOP per sample,
+                               10,240 of them on the tensor cores) */
 } dec_mg_kernel;
 /* Times `reps` back-to-back launches of one V-cycle kernel at `level`, configured as in a solve
  * of `nrhs` right-hand sides, with CUDA events on `stream`.  Returns the mean milliseconds per

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <limits>
 #include <numeric>
+#include <cstring>
 
 #include <thread>
 
@@ -1252,6 +1253,92 @@ std::vector<double> plain_vcycle(const std::vector<double>& u0, const std::vecto
   spmv(md.ps[lvl], z.data(), pz.data());
   for (int i = 0; i < n; ++i) u[i] = u[i] + pz[i];
   return smooth(A, b, u, o.post, o, o.lmax.at(lvl));
+}
+
+}  // namespace orc
+
+namespace orc {
+
+float round_bf16(float x) {
+  uint32_t u;
+  std::memcpy(&u, &x, 4);
+  u += 0x7fffu + ((u >> 16) & 1u);
+  u &= 0xffff0000u;
+  float r;
+  std::memcpy(&r, &u, 4);
+  return r;
+}
+
+namespace {
+struct MlpView {
+  const float *W1, *b1, *W2, *b2, *w3, *b3;
+  explicit MlpView(const std::vector<float>& p) {
+    W1 = p.data();
+    b1 = W1 + MLP_H * MLP_IN;
+    W2 = b1 + MLP_H;
+    b2 = W2 + MLP_H * MLP_H;
+    w3 = b2 + MLP_H;
+    b3 = w3 + MLP_H;
+  }
+};
+// One sample: returns y and fills x0 (rounded), z1, h1 (rounded), z2.
+// With bf16 = false every rounding is skipped and the network is evaluated in FP64 (used to
+// check the backward pass against finite differences).
+double mlp_one(const MlpView& v, const float* x, double* x0, double* z1, double* h1, double* z2, bool bf16) {
+  auto rd = [bf16](float a) { return bf16 ? (double)round_bf16(a) : (double)a; };
+  for (int k = 0; k < MLP_IN; ++k) x0[k] = rd(x[k]);
+  for (int j = 0; j < MLP_H; ++j) {
+    double s = v.b1[j];
+    for (int k = 0; k < MLP_IN; ++k) s += rd(v.W1[j * MLP_IN + k]) * x0[k];
+    z1[j] = s;
+    h1[j] = bf16 ? (double)round_bf16((float)std::max(s, 0.0)) : std::max(s, 0.0);
+  }
+  double y = v.b3[0];
+  for (int j = 0; j < MLP_H; ++j) {
+    double s = v.b2[j];
+    for (int i = 0; i < MLP_H; ++i) s += rd(v.W2[j * MLP_H + i]) * h1[i];
+    z2[j] = s;
+    y += (double)v.w3[j] * std::max(s, 0.0);
+  }
+  return y;
+}
+}  // namespace
+
+void mlp_forward(const std::vector<float>& p, const float* x, int S, double* y, bool bf16) {
+  MlpView v(p);
+  double x0[MLP_IN], h1[MLP_H], z1[MLP_H], z2[MLP_H];
+  for (int s = 0; s < S; ++s) y[s] = mlp_one(v, x + (size_t)s * MLP_IN, x0, z1, h1, z2, bf16);
+}
+
+void mlp_backward(const std::vector<float>& p, const float* x, const double* dy, int S, std::vector<double>& g,
+                  bool bf16) {
+  MlpView v(p);
+  g.assign(MLP_NPARAM, 0.0);
+  double* gW1 = g.data();
+  double* gb1 = gW1 + MLP_H * MLP_IN;
+  double* gW2 = gb1 + MLP_H;
+  double* gb2 = gW2 + MLP_H * MLP_H;
+  double* gw3 = gb2 + MLP_H;
+  double* gb3 = gw3 + MLP_H;
+  double x0[MLP_IN], h1[MLP_H], z1[MLP_H], z2[MLP_H], dz2[MLP_H];
+  for (int s = 0; s < S; ++s) {
+    mlp_one(v, x + (size_t)s * MLP_IN, x0, z1, h1, z2, bf16);
+    const double d = dy[s];
+    gb3[0] += d;
+    for (int j = 0; j < MLP_H; ++j) {
+      gw3[j] += d * std::max(z2[j], 0.0);
+      dz2[j] = z2[j] > 0 ? d * v.w3[j] : 0.0;
+      gb2[j] += dz2[j];
+      for (int i = 0; i < MLP_H; ++i) gW2[j * MLP_H + i] += dz2[j] * h1[i];
+    }
+    for (int i = 0; i < MLP_H; ++i) {
+      double dh = 0.0;
+      for (int j = 0; j < MLP_H; ++j) dh += (bf16 ? (double)round_bf16(v.W2[j * MLP_H + i]) : v.W2[j * MLP_H + i]) * dz2[j];
+      double dz1 = z1[i] > 0 ? dh : 0.0;
+      gb1[i] += dz1;
+      for (int k = 0; k < MLP_IN; ++k) gW1[i * MLP_IN + k] += dz1 * x0[k];
+    }
+  }
 }
 
 }  // namespace orc

@@ -181,3 +181,21 @@ std::vector<double> plain_vcycle(const std::vector<double>& u, const std::vector
 std::vector<double> dense_solve(const CSC& A, const std::vector<double>& b);  // LU, partial pivot
 
 }  // namespace orc
+
+namespace orc {
+// ---------------------------------------------------------------------------------------------
+// The learned smoother's per-vertex MLP 16 -> 64 -> 64 -> 1 (ReLU), as the library evaluates it:
+// features, W1 and W2 rounded to BF16 (round to nearest even), the first hidden layer rounded
+// to BF16 before the second product, FP32-or-wider accumulation.  Parameters are one flat vector:
+// W1[64][16] | b1[64] | W2[64][64] | b2[64] | w3[64] | b3.  Gradients flow to the FP32 master
+// parameters through the rounding (straight-through).
+// ---------------------------------------------------------------------------------------------
+constexpr int MLP_IN = 16, MLP_H = 64;
+constexpr int MLP_NPARAM = MLP_H * MLP_IN + MLP_H + MLP_H * MLP_H + MLP_H + MLP_H + 1;
+float round_bf16(float x);
+// bf16 = false: no rounding, FP64 throughout (for finite-difference checks of the backward pass)
+void mlp_forward(const std::vector<float>& p, const float* x, int S, double* y, bool bf16 = true);
+// grad += d(Σ_s dy_s y_s)/dp
+void mlp_backward(const std::vector<float>& p, const float* x, const double* dy, int S, std::vector<double>& grad,
+                  bool bf16 = true);
+}  // namespace orc

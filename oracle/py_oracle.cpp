@@ -202,6 +202,24 @@ PYBIND11_MODULE(dec_oracle, mod) {
     return to_np(y);
   });
 
+  mod.attr("MLP_NPARAM") = MLP_NPARAM;
+  mod.def("mlp_forward", [](py::array_t<float, py::array::c_style | py::array::forcecast> p,
+                            py::array_t<float, py::array::c_style | py::array::forcecast> x, bool bf16) {
+    std::vector<float> pv(p.data(), p.data() + p.size());
+    int S = (int)(x.size() / MLP_IN);
+    py::array_t<double> y(S);
+    mlp_forward(pv, x.data(), S, y.mutable_data(), bf16);
+    return y;
+  }, py::arg("p"), py::arg("x"), py::arg("bf16") = true);
+  mod.def("mlp_backward", [](py::array_t<float, py::array::c_style | py::array::forcecast> p,
+                             py::array_t<float, py::array::c_style | py::array::forcecast> x,
+                             py::array_t<double, py::array::c_style | py::array::forcecast> dy, bool bf16) {
+    std::vector<float> pv(p.data(), p.data() + p.size());
+    std::vector<double> g;
+    mlp_backward(pv, x.data(), dy.data(), (int)dy.size(), g, bf16);
+    return to_np(g);
+  }, py::arg("p"), py::arg("x"), py::arg("dy"), py::arg("bf16") = true);
+
   // Multigrid
   mod.def("refine_binary", [](const Mesh& m, double radius) {
     Topo t = topo_of(m);
