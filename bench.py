@@ -221,6 +221,58 @@ def measure_operators(dec, peak):
     return out
 
 
+def measure_learned(dec, args, B, U64, common, timed):
+    """The learned smoother: trained on the GPU (Adam, lr 1e-3, batch 65,536 vertex samples, seed
+    4) on V-cycle (residual, error) pairs of icospheres L5-L7, then used as the smoother at every
+    level of FP32 V-cycles in FP64 refinement: on the L8 workload (against the FP64 solution
+    U64) and on icosphere L9 (2,621,442 vertices) against the plain Chebyshev smoother, with
+    the plain smoother as fallback."""
+    import torch
+    from dec_b200 import learned
+    t0 = time.perf_counter()
+    mlp, losses = learned.train_smoother(steps=args.train_steps, lr=1e-3, batch=65536, seed=4, shift=SHIFT)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    ico = dec.meshes.icosahedron()
+    out = {"train": {"steps": args.train_steps, "seconds": train_s, "final_losses": [round(l, 4) for _, _, l in losses[-3:]]}}
+
+    def run(level, smoother, sweeps, Bm, Uref=None):
+        opts = dict(common, smoother=smoother, pre=sweeps, post=sweeps)
+        mg = dec.MultigridData(ico, level, precision=1, **opts)
+        if smoother == 3:
+            mg.set_smoother_mlp(mlp)
+        U = torch.zeros_like(Bm)
+
+        def solve():
+            U.zero_()
+            return mg.solve(U, Bm, rtol=RTOL, max_iters=100)[1]
+
+        t, reps = timed(solve, max(1, args.steps), 1)
+        rep = reps[-1]
+        res = {"solves_per_s": Bm.shape[0] * max(1, args.steps) / t, "v_cycles_per_solve": int(rep.iterations),
+               "converged": bool(rep.converged), "fallback_iteration": int(rep.fallback_iteration),
+               "sweeps": sweeps}
+        if Uref is not None:
+            res["max_rel_error_vs_fp64_solve"] = float(((U - Uref).norm(dim=1) / Uref.norm(dim=1)).max())
+        if smoother == 3:
+            ms, _ = mg.time_kernel(4, 0, Bm.shape[0], reps=5)
+            nv = mg.level_info(0)[0]
+            res["mlp_kernel_ms"] = ms
+            res["mlp_tensor_tflops"] = 10240.0 * nv * Bm.shape[0] / (ms * 1e-3) / 1e12
+        del mg
+        torch.cuda.empty_cache()
+        return res
+
+    out["L8_learned_fp32"] = {f"V({k},{k})": run(LEVEL, 3, k, B, U64) for k in (1, 2)}
+    n9 = 10 * 4 ** 9 + 2
+    B9 = torch.tensor(np.stack([dec.meshes.uniform(200 + j, n9) for j in range(NRHS)]), device="cuda")
+    out["L9_learned_fp32"] = {f"V({k},{k})": run(9, 3, k, B9) for k in (1, 2)}
+    out["L9_plain_fp32"] = {f"V({k},{k})": run(9, 1, k, B9) for k in (2, 3)}
+    del B9
+    torch.cuda.empty_cache()
+    return out
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -365,11 +417,21 @@ def run_ours(args):
         solve32()
     barrier()
     torch.cuda.synchronize()
+
+    def load_for(seconds):  # the same solves, untimed, so the sampler sees the GPU under this load
+        t_end = time.perf_counter() + seconds
+        while time.perf_counter() < t_end:
+            solve32()
+        torch.cuda.synchronize()
+
     sampler.start()
+    load_for(0.6)
     torch.cuda.nvtx.range_push("timed")
     t_ours, reps = timed(solve32, args.steps, 0)
     torch.cuda.nvtx.range_pop()
+    load_for(0.6)
     clocks = sampler.stop()
+    clocks["window"] = "0.6 s of the same solves before and after the timed region, and the timed region"
     if args.profile:
         if rank == 0:
             print(json.dumps({"profile_run": True, "solves_per_s": NRHS * world * args.steps / t_ours,
@@ -419,6 +481,9 @@ def run_ours(args):
     achieved = algo_bytes / (ms * 1e-3) / 1e9
     traffic = traffic_per_launch("k_sweep")
 
+    # --- learned smoother (trained here), L8 and L9 ---
+    learned_res = measure_learned(dec, args, B, U64, common, timed) if args.train_steps > 0 else None
+
     # --- DEC operator kernels (wedges, d, star, Laplacian) at full size ---
     operators = measure_operators(dec, peak) if (rank == 0 and not args.no_ops) else None
 
@@ -466,11 +531,37 @@ def run_ours(args):
             "gpu_launches": launches,
             "clocks": clocks,
             "operators": operators,
+            "learned_smoother": learned_res,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def run_kernel(args):
+    """One V-cycle kernel alone (dec_mg_time_kernel) on icosphere L`mesh_level` with NRHS
+    right-hand sides: the entry point for ncu captures of a single kernel."""
+    import torch
+    dec = load_package()
+    kinds = {"sweep": 0, "residual": 1, "restrict": 2, "prolong": 3, "mlp": 4}
+    kind = kinds[args.kernel]
+    mg = dec.MultigridData(dec.meshes.icosahedron(), args.mesh_level, shift=SHIFT, center="circumcenter",
+                           project_radius=1.0, smoother=3 if kind == 4 else 1, pre=args.sweeps, post=args.sweeps,
+                           precision=1, rhs_block=32, coarse_max=args.coarse_max)
+    if kind == 4:
+        mlp = dec.SmootherMLP(4)
+        mg.set_smoother_mlp(mlp)
+    for _ in range(args.warmup):
+        mg.time_kernel(kind, 0, NRHS, reps=1)
+    ms, by = mg.time_kernel(kind, 0, NRHS, reps=args.steps)
+    torch.cuda.synchronize()
+    nv = mg.level_info(0)[0]
+    line = {"kernel": args.kernel, "mesh_level": args.mesh_level, "nrhs": NRHS, "ms_per_launch": ms,
+            "algorithmic_bytes": by, "GB/s": by / (ms * 1e-3) / 1e9}
+    if kind == 4:
+        line["tensor_TFLOP/s"] = 10240.0 * nv * NRHS / (ms * 1e-3) / 1e12
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -487,8 +578,15 @@ def main():
     ap.add_argument("--no-ops", action="store_true", help="skip the operator-kernel roofline section")
     ap.add_argument("--profile", action="store_true",
                     help="run only the timed mixed-precision solves (inside an NVTX range 'timed')")
+    ap.add_argument("--kernel", choices=["sweep", "residual", "restrict", "prolong", "mlp"],
+                    help="time one V-cycle kernel alone (steps launches after warmup) and exit")
+    ap.add_argument("--mesh-level", type=int, default=LEVEL, dest="mesh_level")
+    ap.add_argument("--train-steps", type=int, default=20000, dest="train_steps",
+                    help="Adam steps of the learned smoother (0 skips the learned-smoother section)")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.kernel:
+        run_kernel(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

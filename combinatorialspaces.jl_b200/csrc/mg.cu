@@ -843,6 +843,7 @@ struct Level {
   DArr<int32_t> col;
   DArr<double> off64, diag64, dinv64;
   DArr<float> off32, diag32, dinv32;
+  DArr<float4> mtab;  // learned smoother: per-row coupling features
   double lmax = 0.0;
   // transfer to the next coarser level (internal numbering on both sides)
   int nc = 0, Wq = 0;
@@ -1182,8 +1183,8 @@ static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool z
         launch_sweep<T, K>(L, B.b.p, x, B.d.p, nullptr, prm, np, s);
         r = B.d.p;
       }
-      launch_mlp_smooth<T, K>(wts, L.n, L.W, L.col.p, pick<T>(L.off64, L.off32), pick<T>(L.diag64, L.diag32), r, x,
-                              zero_x ? 1 : 0, other, np, s);
+      launch_mlp_smooth<T, K>(wts, L.n, L.W, L.col.p, L.mtab.p, pick<T>(L.diag64, L.diag32), r, x, zero_x ? 1 : 0,
+                              other, np, s);
       std::swap(x, other);
       zero_x = false;
     }
@@ -1678,8 +1679,8 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
       prm.c2 = (T)0.25;
       launch_sweep<T, K>(L, B.b.p, B.x.p, B.y.p, B.d.p, prm, np, s);
     } else if (kernel == DEC_KERNEL_MLP) {
-      launch_mlp_smooth<T, K>(mlp_weights(mg.mlp), L.n, L.W, L.col.p, pick<T>(L.off64, L.off32),
-                              pick<T>(L.diag64, L.diag32), B.b.p, B.x.p, 0, B.y.p, np, s);
+      launch_mlp_smooth<T, K>(mlp_weights(mg.mlp), L.n, L.W, L.col.p, L.mtab.p, pick<T>(L.diag64, L.diag32), B.b.p,
+                              B.x.p, 0, B.y.p, np, s);
     } else if (kernel == DEC_KERNEL_RESIDUAL) {
       dim3 g(w.nblocks, np);
       const Level& F = mg.lv[0];
@@ -1752,6 +1753,9 @@ void mg_time_kernel(dec_mg* mg, int kernel, int level, int nrhs, int reps, void*
 void mg_set_smoother_mlp(dec_mg* mg, const dec_mlp* mlp) {
   require(mg != nullptr, "multigrid: null argument");
   if (mg->mlp == mlp) return;
+  if (mlp)  // the per-row coupling features the network reads on every level
+    for (Level& L : mg->lv)
+      if (!L.mtab.p) build_mlp_table(L.n, L.W, L.col.p, L.off64.p, L.diag64.p, L.mtab);
   mg->mlp = mlp;
   for (auto& kv : mg->ws) kv.second->drop_graphs();  // captured cycles hold the old weights' addresses
 }

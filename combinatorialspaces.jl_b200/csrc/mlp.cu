@@ -126,23 +126,43 @@ __device__ __forceinline__ float mlp_tile32(const MlpSmem& sm, const __nv_bfloat
       }
     }
   }
-  // layers 2 and 3: y = w3 · relu(W2 h1 + b2) + b3
+  // layers 2 and 3: y = w3 · relu(W2 h1 + b2) + b3, two column tiles at a time (four
+  // independent accumulator chains per k step)
   float p[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
 #pragma unroll
-  for (int jt = 0; jt < 8; ++jt) {
-    const float bb0 = sm.b2[8 * jt + 2 * t], bb1 = sm.b2[8 * jt + 2 * t + 1];
-    float c[2][4] = {{bb0, bb1, bb0, bb1}, {bb0, bb1, bb0, bb1}};
+  for (int jp = 0; jp < 4; ++jp) {
+    float c[2][2][4];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int jt = 2 * jp + u;
+      const float bb0 = sm.b2[8 * jt + 2 * t], bb1 = sm.b2[8 * jt + 2 * t + 1];
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        c[u][m][0] = bb0;
+        c[u][m][1] = bb1;
+        c[u][m][2] = bb0;
+        c[u][m][3] = bb1;
+      }
+    }
 #pragma unroll
     for (int kk = 0; kk < 4; ++kk) {
-      const uint32_t b0 = W2[(8 * jt + g) * W2W + 8 * kk + t], b1 = W2[(8 * jt + g) * W2W + 8 * kk + t + 4];
 #pragma unroll
-      for (int m = 0; m < 2; ++m) mma16816(c[m], a2[m][kk], b0, b1);
+      for (int u = 0; u < 2; ++u) {
+        const int jt = 2 * jp + u;
+        const uint32_t b0 = W2[(8 * jt + g) * W2W + 8 * kk + t], b1 = W2[(8 * jt + g) * W2W + 8 * kk + t + 4];
+#pragma unroll
+        for (int m = 0; m < 2; ++m) mma16816(c[u][m], a2[m][kk], b0, b1);
+      }
     }
-    const float w0 = sm.w3[8 * jt + 2 * t], w1 = sm.w3[8 * jt + 2 * t + 1];
 #pragma unroll
-    for (int m = 0; m < 2; ++m) {
-      p[m][0] += fmaxf(c[m][0], 0.f) * w0 + fmaxf(c[m][1], 0.f) * w1;
-      p[m][1] += fmaxf(c[m][2], 0.f) * w0 + fmaxf(c[m][3], 0.f) * w1;
+    for (int u = 0; u < 2; ++u) {
+      const int jt = 2 * jp + u;
+      const float w0 = sm.w3[8 * jt + 2 * t], w1 = sm.w3[8 * jt + 2 * t + 1];
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        p[m][0] += fmaxf(c[u][m][0], 0.f) * w0 + fmaxf(c[u][m][1], 0.f) * w1;
+        p[m][1] += fmaxf(c[u][m][2], 0.f) * w0 + fmaxf(c[u][m][3], 0.f) * w1;
+      }
     }
   }
 #pragma unroll
@@ -193,12 +213,41 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_eval_tc(int64_t n, const fl
   }
 }
 
-// Learned smoothing step on a multigrid level (panel layout [panel][row][K]; split operator:
-// diagonal + W off-diagonal slots in the reference's column order, padding = own column with
-// value 0): out = x + (s_i / a_ii) MLP(features(r)), x taken as zero when zero_x.
+// Per-row feature table of a multigrid level (split operator: diagonal + W off-diagonal slots in
+// the reference's column order, real slots first, padding = own column with value 0):
+// tab[2i] = (c0, c1, c2, c3), tab[2i+1] = (c4, c5, 1 - Σ_j |a_ij| / a_ii, nn / 6) with
+// c_s = a_ij / a_ii of the first nn = min(6, real slots) slots, zero beyond; the same float
+// arithmetic as the per-sample feature function.
+__global__ void k_mlp_table(int n, int W, const int32_t* __restrict__ col, const double* __restrict__ off,
+                            const double* __restrict__ diag, float4* __restrict__ tab) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float di = (float)diag[i];
+    float cp[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, sabs = 0.f;
+    int nn = 0;
+    for (int s = 0; s < W; ++s) {
+      const int c = col[(size_t)i * W + s];
+      const float o = (float)off[(size_t)i * W + s];
+      if (c == i && o == 0.f) continue;
+      sabs += fabsf(o);
+      if (nn < 6) cp[nn++] = o / di;
+    }
+    tab[2 * (size_t)i] = make_float4(cp[0], cp[1], cp[2], cp[3]);
+    tab[2 * (size_t)i + 1] = make_float4(cp[4], cp[5], 1.f - sabs / di, (float)nn * (1.0f / 6.0f));
+  }
+}
+
+void build_mlp_table(int n, int W, const int32_t* col, const double* off, const double* diag, DArr<float4>& tab) {
+  tab.alloc(2 * (size_t)n);
+  k_mlp_table<<<grid_for(n, 256), 256>>>(n, W, col, off, diag, tab.p);
+  DEC_CHECK_LAUNCH();
+}
+
+// Learned smoothing step on a multigrid level (panel layout [panel][row][K]):
+// out = x + (s_i / a_ii) MLP(features(r)), x taken as zero when zero_x.  The coupling features
+// come from the level's table; the residual features are gathered per sample.
 template <class T, int K>
-__global__ void __launch_bounds__(kMlpThreads) k_mlp_smooth(MlpWeights w, int n, int W, const int32_t* __restrict__ col,
-                                                            const T* __restrict__ off, const T* __restrict__ diag,
+__global__ void __launch_bounds__(kMlpThreads, 3) k_mlp_smooth(MlpWeights w, int n, int W, const int32_t* __restrict__ col,
+                                                            const float4* __restrict__ tab, const T* __restrict__ diag,
                                                             const T* __restrict__ r, const T* __restrict__ x,
                                                             int zero_x, T* __restrict__ out, size_t pstride) {
   __shared__ MlpSmem sm;
@@ -215,23 +264,31 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_smooth(MlpWeights w, int n,
     T xv = T(0);
     if (q < nq) {
       const int i = (int)(q / K), k = (int)(q % K);
-      const float di = (float)diag[i];
-      float nb[6], cp[6], sabs = 0.f;
-      int nn = 0;
-      for (int s = 0; s < W; ++s) {
-        const int c = col[(size_t)i * W + s];
-        const float o = (float)off[(size_t)i * W + s];
-        if (c == i && o == 0.f) continue;  // padding slot
-        sabs += fabsf(o);
-        if (nn < 6) {
-          nb[nn] = (float)r[po + (size_t)c * K + k];
-          cp[nn] = o / di;
-          ++nn;
-        }
+      const float4 t0 = tab[2 * (size_t)i], t1 = tab[2 * (size_t)i + 1];
+      const int nn = __float2int_rn(t1.w * 6.0f);
+      const float ri = (float)r[po + q];
+      float nb[6];
+      float s = fabsf(ri);
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        nb[j] = j < nn ? (float)r[po + (size_t)col[(size_t)i * W + j] * K + k] : 0.f;
+        s = fmaxf(s, fabsf(nb[j]));
       }
-      float scale;
-      mlp_features((float)r[po + q], nb, cp, nn, 1.f - sabs / di, f, &scale);
-      dsc = scale / di;
+      if (s == 0.0f) s = 1.0f;
+      const float inv = 1.0f / s;
+      f[0] = ri * inv;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) f[1 + j] = nb[j] * inv;
+      f[7] = t0.x;
+      f[8] = t0.y;
+      f[9] = t0.z;
+      f[10] = t0.w;
+      f[11] = t1.x;
+      f[12] = t1.y;
+      f[13] = t1.z;
+      f[14] = t1.w;
+      f[15] = 0.0f;
+      dsc = s / (float)diag[i];
       if (!zero_x) xv = x[po + q];
     } else {
 #pragma unroll
@@ -246,19 +303,19 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_smooth(MlpWeights w, int n,
 }
 
 template <class T, int K>
-void launch_mlp_smooth(const MlpWeights& w, int n, int W, const int32_t* col, const T* off, const T* diag, const T* r,
-                       const T* x, int zero_x, T* out, int np, cudaStream_t s) {
+void launch_mlp_smooth(const MlpWeights& w, int n, int W, const int32_t* col, const float4* tab, const T* diag,
+                       const T* r, const T* x, int zero_x, T* out, int np, cudaStream_t s) {
   const long long tiles = ((long long)n * K + kTile - 1) / kTile;
   const long long want = (tiles + kMlpWarps - 1) / kMlpWarps;
   const long long cap = std::max<long long>(1, (long long)num_sms() * 4 / std::max(1, np));
   dim3 grid((unsigned)std::max<long long>(1, std::min(want, cap)), np);
-  k_mlp_smooth<T, K><<<grid, kMlpThreads, 0, s>>>(w, n, W, col, off, diag, r, x, zero_x, out, (size_t)n * K);
+  k_mlp_smooth<T, K><<<grid, kMlpThreads, 0, s>>>(w, n, W, col, tab, diag, r, x, zero_x, out, (size_t)n * K);
   DEC_CHECK_LAUNCH();
 }
 
 #define DEC_INST(T, K)                                                                                             \
-  template void launch_mlp_smooth<T, K>(const MlpWeights&, int, int, const int32_t*, const T*, const T*, const T*, \
-                                        const T*, int, T*, int, cudaStream_t);
+  template void launch_mlp_smooth<T, K>(const MlpWeights&, int, int, const int32_t*, const float4*, const T*, \
+                                        const T*, const T*, int, T*, int, cudaStream_t);
 DEC_INST(float, 1) DEC_INST(float, 2) DEC_INST(float, 4) DEC_INST(float, 8) DEC_INST(float, 16) DEC_INST(float, 32)
 DEC_INST(double, 1) DEC_INST(double, 2) DEC_INST(double, 4) DEC_INST(double, 8) DEC_INST(double, 16)
 DEC_INST(double, 32)

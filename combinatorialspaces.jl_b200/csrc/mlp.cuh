@@ -72,7 +72,10 @@ namespace decb {
 // Launches the learned smoothing step on a multigrid level (panel layout [panel][row][K]):
 // out = x + (s_i / a_ii) MLP(features(r)) with x taken as zero when zero_x.
 // T = float / double level arrays.  Defined in mlp.cu.
+// tab: the level's per-row feature table (build_mlp_table).
 template <class T, int K>
-void launch_mlp_smooth(const MlpWeights& w, int n, int W, const int32_t* col, const T* off, const T* diag,
+void launch_mlp_smooth(const MlpWeights& w, int n, int W, const int32_t* col, const float4* tab, const T* diag,
                        const T* r, const T* x, int zero_x, T* out, int np, cudaStream_t s);
+// Per-row coupling features of a level's split operator (2 float4 per row).
+void build_mlp_table(int n, int W, const int32_t* col, const double* off, const double* diag, DArr<float4>& tab);
 }  // namespace decb
