@@ -273,6 +273,94 @@ def measure_learned(dec, args, B, U64, common, timed):
     return out
 
 
+def measure_batched(dec, args):
+    """The batched uneven workload: 512 Helmholtz solves (L + c I) u = b, c log-uniform in [0.1, 10]
+    and the mesh drawn uniformly from 8 types (icospheres L4-L7; planar grids 65^2, 129^2, 257^2,
+    513^2 = a 9x9 triangulated grid refined 3-6 times), seed 3; FP32 Chebyshev V(3,3) cycles in
+    FP64 refinement to 1e-8, every refinement step of all 8 groups one CUDA graph, panel widths
+    per group from the autotuner.  Then 1,024 wedge products ∧(1,1) of FP32 uniform[-1,1] 1-form
+    pairs on icosphere L7 in one batched launch."""
+    import torch
+    rng = np.random.default_rng(3)
+    ico = dec.meshes.icosahedron()
+    grid9 = dec.meshes.triangulated_grid(8, 8, 1.0, 1.0, False)
+    types = [("icosphere_L4", ico, 4, 1.0), ("icosphere_L5", ico, 5, 1.0), ("icosphere_L6", ico, 6, 1.0),
+             ("icosphere_L7", ico, 7, 1.0), ("grid_65x65", grid9, 3, 0.0), ("grid_129x129", grid9, 4, 0.0),
+             ("grid_257x257", grid9, 5, 0.0), ("grid_513x513", grid9, 6, 0.0)]
+    draw = rng.integers(0, len(types), 512)
+    cs = np.exp(rng.uniform(np.log(0.1), np.log(10.0), 512))
+    t0 = time.perf_counter()
+    mgs, nrhs, shifts, Bs = [], [], [], []
+    for t, (name, coarse, levels, radius) in enumerate(types):
+        mg = dec.MultigridData(coarse, levels, shift=0.0, center="circumcenter", project_radius=radius,
+                               smoother=1, pre=3, post=3, precision=1, coarse_solver=2, coarse_max=170,
+                               inner_cycles=2)
+        idx = np.nonzero(draw == t)[0]
+        mgs.append(mg)
+        nrhs.append(len(idx))
+        shifts.append(cs[idx])
+        Bs.append(torch.tensor(np.stack([dec.meshes.uniform(1000 + int(i), mg.n) for i in idx]), device="cuda"))
+    batch = dec.Batch(mgs)
+    batch.autotune(nrhs, reps=3)
+    setup_s = time.perf_counter() - t0
+    Us = [torch.zeros_like(B) for B in Bs]
+
+    def solve():
+        for U in Us:
+            U.zero_()
+        return batch.solve(Us, Bs, shifts=shifts, rtol=RTOL, max_iters=60)
+
+    for _ in range(max(1, args.warmup)):
+        solve()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    steps = max(1, args.steps)
+    e0.record()
+    outs = [solve() for _ in range(steps)]
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    reps, tot = outs[-1]
+    groups = {}
+    for (name, _, _, _), mg, r, k in zip(types, mgs, reps, nrhs):
+        groups[name] = {"vertices": mg.n, "solves": k, "refinement_steps": int(r.iterations),
+                        "converged": bool(r.converged), "panel_width": int(r.rhs_block)}
+    res = {"solves": 512, "solves_per_s": 512 * steps / t, "ms_per_batch": 1e3 * t / steps,
+           "refinement_steps": int(tot.iterations), "converged": bool(tot.converged),
+           "max_rel_residual": tot.max_rel_residual, "kernels_per_batch": int(tot.launches),
+           "setup_seconds": setup_s, "groups": groups}
+    del Us, Bs, batch, mgs
+    torch.cuda.empty_cache()
+
+    # 1,024 wedge products on icosphere L7 (FP32), one batched launch
+    m7 = dec.meshes.icosphere(7)
+    g7 = dec.Mesh(m7.points, m7.ev0, m7.ev1, m7.te0, m7.te1, m7.te2, m7.edge_orientation, m7.tri_orientation,
+                  center="circumcenter")
+    ne, nt = g7.ne, g7.nt
+    w11 = dec.dec_wedge_product(1, 1, g7, "float32")
+    count = 1024
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(3)
+    a = torch.rand((count, ne), dtype=torch.float32, device="cuda", generator=gen) * 2 - 1
+    b = torch.rand((count, ne), dtype=torch.float32, device="cuda", generator=gen) * 2 - 1
+    out = torch.empty((count, nt), dtype=torch.float32, device="cuda")
+    w11.batched(a, b, out)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        w11.batched(a, b, out)
+    e1.record()
+    torch.cuda.synchronize()
+    tw = e0.elapsed_time(e1) / 1e3 / steps
+    by = count * (2.0 * ne * 4 + nt * 4) + nt * (12 + 3 * 4)
+    res["wedge11_L7_fp32_x1024"] = {"ms": 1e3 * tw, "wedges_per_s": count / tw, "GB/s": by / tw / 1e9,
+                                    "bytes": by}
+    del a, b, out
+    torch.cuda.empty_cache()
+    return res
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -481,6 +569,9 @@ def run_ours(args):
     achieved = algo_bytes / (ms * 1e-3) / 1e9
     traffic = traffic_per_launch("k_sweep")
 
+    # --- batched uneven workload (512 solves over 8 meshes, one graph per step) ---
+    batched = measure_batched(dec, args) if (rank == 0 and not args.no_batch) else None
+
     # --- learned smoother (trained here), L8 and L9 ---
     learned_res = measure_learned(dec, args, B, U64, common, timed) if args.train_steps > 0 else None
 
@@ -532,6 +623,7 @@ def run_ours(args):
             "clocks": clocks,
             "operators": operators,
             "learned_smoother": learned_res,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -581,6 +673,7 @@ def main():
     ap.add_argument("--kernel", choices=["sweep", "residual", "restrict", "prolong", "mlp"],
                     help="time one V-cycle kernel alone (steps launches after warmup) and exit")
     ap.add_argument("--mesh-level", type=int, default=LEVEL, dest="mesh_level")
+    ap.add_argument("--no-batch", action="store_true", dest="no_batch", help="skip the batched-workload section")
     ap.add_argument("--train-steps", type=int, default=20000, dest="train_steps",
                     help="Adam steps of the learned smoother (0 skips the learned-smoother section)")
     args = ap.parse_args()

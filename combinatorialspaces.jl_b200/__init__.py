@@ -27,7 +27,7 @@ from ._capi import check, lib, DecError  # noqa: F401
 __all__ = ["Mesh", "Operator", "MultigridData", "dec_wedge_product", "dec_wedge_product_pd",
            "dec_wedge_product_dp", "dec_wedge_product_dd", "dec_differential", "dec_boundary",
            "dec_dual_derivative", "dec_hodge_star", "dec_inv_hodge_star", "laplace_beltrami",
-           "helmholtz", "multigrid_vcycles", "multigrid_wcycles", "SmootherMLP", "DecError"]
+           "helmholtz", "multigrid_vcycles", "multigrid_wcycles", "SmootherMLP", "Batch", "DecError"]
 
 CENTERS = {"barycenter": _capi.DEC_BARYCENTER, "circumcenter": _capi.DEC_CIRCUMCENTER}
 
@@ -178,7 +178,13 @@ class WedgePlan:
         return out
 
     def batched(self, a, b, out):
+        """out[j] = a[j] ∧ b[j] for j < count, one launch (a, b, out: (count, len) CUDA tensors)."""
         count = a.shape[0]
+        for t, ln, what in ((a, self.len_a, "first forms"), (b, self.len_b, "second forms"),
+                            (out, self.len_out, "outputs")):
+            if tuple(t.shape) != (count, ln):
+                raise ValueError(f"wedge batch {what}: expected shape {(count, ln)}, got {tuple(t.shape)}")
+            _check_form(t, count * ln, self.code, f"wedge batch {what}")
         check(lib().dec_wedge_apply_batched(self._h, _ptr(a), _ptr(b), _ptr(out), count, _stream()))
         return out
 
@@ -410,9 +416,20 @@ class MultigridData:
         check(lib().dec_mg_time_kernel(self._h, kernel, level, nrhs, reps, _stream(), C.byref(ms), C.byref(by)))
         return ms.value, by.value
 
-    def solve(self, u, b, rtol=1e-8, max_iters=100):
+    def solve(self, u, b, rtol=1e-8, max_iters=100, shifts=None):
+        """FP64-refined solve of A u = b (u in/out); with `shifts` (coarse_solver=2 hierarchies)
+        right-hand side j solves (L + (shift + shifts[j]) I) u_j = b_j."""
         nrhs = 1 if b.dim() == 1 else b.shape[0]
         rep = _capi.SolveReport()
+        if shifts is not None:
+            sh = np.ascontiguousarray(shifts, np.float64)
+            if sh.size != nrhs:
+                raise ValueError("one shift per right-hand side")
+            st = lib().dec_mg_solve_shifted(self._h, _ptr(u), _ptr(b), nrhs, sh.ctypes.data_as(C.c_void_p), rtol,
+                                            max_iters, C.byref(rep), _stream())
+            if st not in (_capi.DEC_OK, 4):
+                check(st)
+            return u, rep
         st = lib().dec_mg_solve(self._h, _ptr(u), _ptr(b), nrhs, rtol, max_iters, C.byref(rep), _stream())
         if st not in (_capi.DEC_OK, 4):
             check(st)
@@ -433,6 +450,55 @@ class MultigridData:
         if st not in (_capi.DEC_OK, 4):
             check(st)
         return u, rep
+
+
+class Batch:
+    """Batched solves over several MultigridData hierarchies (dec_batch_*): each refinement step
+    of every group runs as one CUDA graph with a concurrent branch per group."""
+
+    def __init__(self, groups):
+        self.groups = list(groups)
+        arr = (C.c_void_p * len(self.groups))(*[g._h.value for g in self.groups])
+        h = C.c_void_p()
+        check(lib().dec_batch_create(arr, len(self.groups), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _capi is not None and _capi._lib is not None:
+            _capi._lib.dec_batch_destroy(h)
+            self._h = None
+
+    def autotune(self, nrhs, reps=3):
+        n = (C.c_int32 * len(nrhs))(*nrhs)
+        check(lib().dec_batch_autotune(self._h, n, reps, _stream()))
+
+    def solve(self, us, bs, shifts=None, rtol=1e-8, max_iters=100):
+        """us, bs: per group float64 CUDA tensors (nrhs_g, n_g) (us in/out); shifts: per group
+        host arrays or None.  Returns (per-group reports, total report)."""
+        G = len(self.groups)
+        nrhs = [1 if b.dim() == 1 else b.shape[0] for b in bs]
+        up = (C.c_void_p * G)(*[u.data_ptr() for u in us])
+        bp = (C.c_void_p * G)(*[b.data_ptr() for b in bs])
+        nr = (C.c_int32 * G)(*nrhs)
+        keep = []
+        sp = None
+        if shifts is not None:
+            ptrs = []
+            for sh in shifts:
+                if sh is None:
+                    ptrs.append(None)
+                else:
+                    a = np.ascontiguousarray(sh, np.float64)
+                    keep.append(a)
+                    ptrs.append(a.ctypes.data)
+            sp = (C.c_void_p * G)(*ptrs)
+        reps = (_capi.SolveReport * G)()
+        tot = _capi.SolveReport()
+        st = lib().dec_batch_solve(self._h, up, bp, nr, sp, rtol, max_iters, reps, C.byref(tot), _stream())
+        if st not in (_capi.DEC_OK, 4):
+            check(st)
+        return list(reps), tot
 
 
 class SmootherMLP:

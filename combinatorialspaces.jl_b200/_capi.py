@@ -83,6 +83,11 @@ SIGNATURES = {
     "dec_mg_time_kernel": (I32, [P, I32, I32, I32, I32, P, PF64, PF64]),
     "dec_mg_autotune": (I32, [P, I32, I32, P, C.POINTER(C.c_int32)]),
     "dec_mg_set_smoother_mlp": (I32, [P, P]),
+    "dec_mg_solve_shifted": (I32, [P, P, P, I32, P, F64, I32, C.POINTER(SolveReport), P]),
+    "dec_batch_create": (I32, [P, I32, PP]),
+    "dec_batch_destroy": (I32, [P]),
+    "dec_batch_autotune": (I32, [P, P, I32, P]),
+    "dec_batch_solve": (I32, [P, P, P, P, P, F64, I32, P, C.POINTER(SolveReport), P]),
     "dec_mlp_create": (I32, [C.c_uint64, PP]),
     "dec_mlp_destroy": (I32, [P]),
     "dec_mlp_get_params": (I32, [P, P]),

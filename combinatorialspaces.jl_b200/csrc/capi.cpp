@@ -253,6 +253,41 @@ dec_status dec_mg_autotune(dec_mg* mg, int32_t nrhs, int32_t reps, void* stream,
   });
 }
 
+dec_status dec_mg_solve_shifted(dec_mg* mg, double* u, const double* b, int32_t nrhs, const double* shifts,
+                                double rtol, int32_t max_iters, dec_solve_report* rep, void* stream) {
+  dec_status st = DEC_OK;
+  dec_status g = guard([&] {
+    decb::require(shifts != nullptr, "dec_mg_solve_shifted: null shifts");
+    st = decb::mg_solve(mg, u, b, nrhs, rtol, max_iters, rep, stream, false, true, shifts);
+  });
+  return g != DEC_OK ? g : st;
+}
+
+dec_status dec_batch_create(dec_mg* const* groups, int32_t ngroups, dec_batch** out) {
+  return guard([&] {
+    decb::require(out != nullptr, "dec_batch_create: null argument");
+    *out = nullptr;
+    *out = decb::batch_create(groups, ngroups);
+  });
+}
+
+dec_status dec_batch_destroy(dec_batch* batch) {
+  return guard([&] { decb::batch_destroy(batch); });
+}
+
+dec_status dec_batch_autotune(dec_batch* batch, const int32_t* nrhs, int32_t reps, void* stream) {
+  return guard([&] { decb::batch_autotune(batch, nrhs, reps, stream); });
+}
+
+dec_status dec_batch_solve(dec_batch* batch, double* const* u, const double* const* rhs, const int32_t* nrhs,
+                           const double* const* shifts, double rtol, int32_t max_iters, dec_solve_report* reports,
+                           dec_solve_report* total, void* stream) {
+  dec_status st = DEC_OK;
+  dec_status g = guard(
+      [&] { st = decb::batch_solve(batch, u, rhs, nrhs, shifts, rtol, max_iters, reports, total, stream); });
+  return g != DEC_OK ? g : st;
+}
+
 dec_status dec_mg_set_smoother_mlp(dec_mg* mg, const dec_mlp* mlp) {
   return guard([&] { decb::mg_set_smoother_mlp(mg, mlp); });
 }

@@ -280,18 +280,21 @@ struct Lanes {
 //   S_JACOBI: out = x + ω D⁻¹ r
 //   S_CHEB0 : d = D⁻¹ r / θ; out = x + d
 //   S_CHEBN : d = c1 d + c2 D⁻¹ r; out = x + d
-template <class T, int K, int W>
+// SH: right-hand side j of panel p has its own operator A + cs[p*K + j] I (D likewise).
+template <class T, int K, int W, bool SH>
 __global__ void __launch_bounds__(TB) k_sweep(int n, int Wr, const int32_t* __restrict__ col,
                                               const T* __restrict__ off, const T* __restrict__ diag,
                                               const T* __restrict__ dinv, const T* __restrict__ b,
                                               const T* __restrict__ x, T* __restrict__ out, T* __restrict__ d,
-                                              SweepPrm<T> prm, size_t pstride) {
+                                              SweepPrm<T> prm, size_t pstride, const T* __restrict__ cs) {
   using Ln = Lanes<T, K>;
   pdl_enter();
   constexpr int V = Ln::V;
   const int w = W > 0 ? W : Wr;
   const int lane = threadIdx.x % Ln::LPR;
   const size_t po = (size_t)blockIdx.y * pstride + (size_t)lane * V;
+  T csv[V];
+  if constexpr (SH) ldv<T, V>(cs + (size_t)blockIdx.y * K + (size_t)lane * V, csv);
   for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < n; i += gridDim.x * Ln::RPB) {
     const size_t ik = po + (size_t)i * K;
     T r[V], xi[V];
@@ -301,7 +304,10 @@ __global__ void __launch_bounds__(TB) k_sweep(int n, int Wr, const int32_t* __re
       const T dg = diag[i];
       T acc[V];
 #pragma unroll
-      for (int q = 0; q < V; ++q) acc[q] = dg * xi[q];
+      for (int q = 0; q < V; ++q) {
+        if constexpr (SH) acc[q] = (dg + csv[q]) * xi[q];
+        else acc[q] = dg * xi[q];
+      }
       const int32_t* c = col + (size_t)i * w;
       const T* v = off + (size_t)i * w;
       if constexpr (W > 0) {
@@ -338,16 +344,21 @@ __global__ void __launch_bounds__(TB) k_sweep(int n, int Wr, const int32_t* __re
       stv<T, V>(out + ik, r);
       continue;
     }
-    const T di = dinv[i];
+    T di[V];
+#pragma unroll
+    for (int q = 0; q < V; ++q) {
+      if constexpr (SH) di[q] = T(1) / (diag[i] + csv[q]);
+      else di[q] = dinv[i];
+    }
     T o[V];
     if (prm.mode == S_JACOBI) {
 #pragma unroll
-      for (int q = 0; q < V; ++q) o[q] = xi[q] + prm.omega * (di * r[q]);
+      for (int q = 0; q < V; ++q) o[q] = xi[q] + prm.omega * (di[q] * r[q]);
     } else if (prm.mode == S_CHEB0) {
       T dn[V];
 #pragma unroll
       for (int q = 0; q < V; ++q) {
-        dn[q] = (di * r[q]) * prm.inv_theta;
+        dn[q] = (di[q] * r[q]) * prm.inv_theta;
         o[q] = xi[q] + dn[q];
       }
       if (prm.write_d) stv<T, V>(d + ik, dn);
@@ -361,7 +372,7 @@ __global__ void __launch_bounds__(TB) k_sweep(int n, int Wr, const int32_t* __re
       }
 #pragma unroll
       for (int q = 0; q < V; ++q) {
-        dn[q] = prm.c1 * dn[q] + prm.c2 * (di * r[q]);
+        dn[q] = prm.c1 * dn[q] + prm.c2 * (di[q] * r[q]);
         o[q] = xi[q] + dn[q];
       }
       if (prm.write_d) stv<T, V>(d + ik, dn);
@@ -442,6 +453,42 @@ __global__ void __launch_bounds__(TB) k_coarse(int n, const double* __restrict__
   }
 }
 
+// Coarsest-level solve for per-right-hand-side shifts c (coarse_solver 2): with
+// L = M⁻¹ K (M = ⋆0, K symmetric) and M^{1/2} L M^{-1/2} = Q Λ Qᵀ,
+// (L + c I)⁻¹ = E (Λ + c)⁻¹ F,  E = M^{-1/2} Q,  F = Qᵀ M^{1/2}.
+// Phase 1: y = (Λ + c)⁻¹ F b (FP64 scratch); phase 2: x = E y.
+template <class T, int K>
+__global__ void __launch_bounds__(TB) k_coarse_eig1(int n, const double* __restrict__ F, const double* __restrict__ lam,
+                                                    const double* __restrict__ cs, const T* __restrict__ b,
+                                                    double* __restrict__ y, size_t pstride) {
+  pdl_enter();
+  const T* bb = b + (size_t)blockIdx.y * pstride;
+  double* yy = y + (size_t)blockIdx.y * pstride;
+  const int k = threadIdx.x % K;
+  const double c = cs[(size_t)blockIdx.y * K + k];
+  for (int i = blockIdx.x * (TB / K) + threadIdx.x / K; i < n; i += gridDim.x * (TB / K)) {
+    const double* a = F + (size_t)i * n;
+    double s = 0.0;
+    for (int j = 0; j < n; ++j) s += a[j] * (double)bb[(size_t)j * K + k];
+    yy[(size_t)i * K + k] = s / (lam[i] + c);
+  }
+}
+
+template <class T, int K>
+__global__ void __launch_bounds__(TB) k_coarse_eig2(int n, const double* __restrict__ E, const double* __restrict__ y,
+                                                    T* __restrict__ x, size_t pstride) {
+  pdl_enter();
+  const double* yy = y + (size_t)blockIdx.y * pstride;
+  T* xx = x + (size_t)blockIdx.y * pstride;
+  const int k = threadIdx.x % K;
+  for (int i = blockIdx.x * (TB / K) + threadIdx.x / K; i < n; i += gridDim.x * (TB / K)) {
+    const double* a = E + (size_t)i * n;
+    double s = 0.0;
+    for (int j = 0; j < n; ++j) s += a[j] * yy[(size_t)j * K + k];
+    xx[(size_t)i * K + k] = (T)s;
+  }
+}
+
 // Column-major RHS block (nrhs vectors of length n, reference vertex order) -> panels of K in
 // the level's internal order (perm: internal -> reference), and back.
 template <class T, class S>
@@ -477,20 +524,22 @@ __global__ void k_axpy_update(size_t total, const T* __restrict__ z, double* __r
 
 // FP64 residual r = b - A u on the panels, written in the inner precision T, with per-block
 // partial sums of r² per right-hand side (deterministic two-stage reduction).
-template <class T, int K, int W>
+template <class T, int K, int W, bool SH>
 __global__ void __launch_bounds__(TB) k_residual64(int n, int Wr, const int32_t* __restrict__ col,
                                                    const double* __restrict__ off, const double* __restrict__ diag,
                                                    const double* __restrict__ b, const double* __restrict__ u,
-                                                   T* __restrict__ rT, double* __restrict__ partial, size_t pstride) {
+                                                   T* __restrict__ rT, double* __restrict__ partial, size_t pstride,
+                                                   const double* __restrict__ cs) {
   using Ln = Lanes<double, K>;
   pdl_enter();
   constexpr int V = Ln::V;
   const int w = W > 0 ? W : Wr;
   const int lane = threadIdx.x % Ln::LPR;
   const size_t po = (size_t)blockIdx.y * pstride + (size_t)lane * V;
-  double ss[V];
+  double ss[V], csv[V];
 #pragma unroll
   for (int q = 0; q < V; ++q) ss[q] = 0.0;
+  if constexpr (SH) ldv<double, V>(cs + (size_t)blockIdx.y * K + (size_t)lane * V, csv);
   for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < n; i += gridDim.x * Ln::RPB) {
     const size_t ik = po + (size_t)i * K;
     double ui[V], acc[V], bv[V];
@@ -498,7 +547,10 @@ __global__ void __launch_bounds__(TB) k_residual64(int n, int Wr, const int32_t*
     ldv<double, V>(b + ik, bv);
     const double dg = diag[i];
 #pragma unroll
-    for (int q = 0; q < V; ++q) acc[q] = dg * ui[q];
+    for (int q = 0; q < V; ++q) {
+      if constexpr (SH) acc[q] = (dg + csv[q]) * ui[q];
+      else acc[q] = dg * ui[q];
+    }
     const int32_t* c = col + (size_t)i * w;
     const double* v = off + (size_t)i * w;
     for (int s = 0; s < w; ++s) {
@@ -855,6 +907,7 @@ template <class T>
 struct LevelBufs {
   DArr<T> x, y, b, d;  // x / y ping-pong, b right-hand side, d Chebyshev direction
   DArr<T> q, e;        // CG smoother: A p and the accumulated correction Δx (CG mode only)
+  const T* cs = nullptr;  // per-RHS shifts (coarse_solver 2), K * npanels, shared by all levels
 };
 
 struct Workspace {
@@ -867,6 +920,11 @@ struct Workspace {
   DArr<double> ucm, bcm;      // column-major device copies for host-buffer solves
   int nblocks = 0;
   DArr<double> Ubak;          // learned smoother: the iterate before a refinement step
+  DArr<double> cs64;          // coarse_solver 2: per-RHS total shifts (K * npanels)
+  DArr<float> cs32;
+  DArr<double> ceig;          // coarse_solver 2: FP64 scratch of the coarsest solve
+  std::vector<double> hcs64;  // host staging of the shifts
+  std::vector<float> hcs32;
   cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};  // GraphKind
   int64_t launches[4] = {0, 0, 0, 0};                               // kernel nodes per graph
   void drop_graphs() {
@@ -884,11 +942,13 @@ struct dec_mg {
   dec_mg_options opt{};
   std::vector<decb::Level> lv;  // 0 = finest
   decb::DArr<double> ainv;      // dense inverse of level lc (FP64, internal order)
+  decb::DArr<double> eigE, eigF, eigL;  // coarse_solver 2: (L + c I)⁻¹ = E (Λ + c)⁻¹ F on level lc
   int lc = 0;                   // level at which cycles solve directly
   std::map<long long, std::unique_ptr<decb::Workspace>> ws;
   std::map<long long, int> tuned;  // (nrhs, precision) -> panel width chosen by the autotuner
   cudaStream_t cap = nullptr;      // capture stream
   const dec_mlp* mlp = nullptr;    // learned smoother network (not owned)
+  uint64_t epoch = 0;              // bumped whenever workspaces or their graphs are dropped
   bool force_plain = false;        // set while capturing the plain-smoother fallback cycle
   ~dec_mg() {
     ws.clear();
@@ -981,6 +1041,81 @@ static std::vector<double> dense_inverse(const dec_op& op, int n) {
   return Ainv;
 }
 
+// Eigendecomposition of a symmetric matrix (row-major n x n, overwritten) by the cyclic Jacobi
+// method: rotations zero each off-diagonal entry in turn until the off-diagonal mass is below
+// 1e-30 of the total.  Returns the eigenvalues; Q (row-major) holds the eigenvectors as columns.
+static std::vector<double> symmetric_eigen(std::vector<double>& A, int n, std::vector<double>& Q) {
+  Q.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) Q[(size_t)i * n + i] = 1.0;
+  auto at = [&](int i, int j) -> double& { return A[(size_t)i * n + j]; };
+  double total = 0.0;
+  for (double a : A) total += a * a;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double offm = 0.0;
+    for (int i = 0; i < n; ++i)
+      for (int j = i + 1; j < n; ++j) offm += 2.0 * at(i, j) * at(i, j);
+    if (offm <= 1e-30 * total) break;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = at(p, q);
+        if (apq == 0.0) continue;
+        const double theta = (at(q, q) - at(p, p)) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+        for (int k = 0; k < n; ++k) {  // A <- A J (columns p, q)
+          const double akp = at(k, p), akq = at(k, q);
+          at(k, p) = c * akp - sn * akq;
+          at(k, q) = sn * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {  // A <- Jᵀ A (rows p, q)
+          const double apk = at(p, k), aqk = at(q, k);
+          at(p, k) = c * apk - sn * aqk;
+          at(q, k) = sn * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {  // Q <- Q J
+          const double qkp = Q[(size_t)k * n + p], qkq = Q[(size_t)k * n + q];
+          Q[(size_t)k * n + p] = c * qkp - sn * qkq;
+          Q[(size_t)k * n + q] = sn * qkp + c * qkq;
+        }
+      }
+  }
+  std::vector<double> lam(n);
+  for (int i = 0; i < n; ++i) lam[i] = at(i, i);
+  return lam;
+}
+
+// Coarse solver 2: with M = ⋆0 of the level and S = M^{1/2} L M^{-1/2} = Q Λ Qᵀ (symmetrised),
+// E = M^{-1/2} Q and F = Qᵀ M^{1/2}, permuted to the level's internal order.
+static void build_eigen_coarse(dec_mg& mg, const Level& C) {
+  const int n = C.n;
+  auto c = C.op->col.download();
+  auto vv = C.op->val64.download();
+  auto m0 = C.mesh->m.star0.download();
+  std::vector<double> S((size_t)n * n, 0.0), Q;
+  for (int i = 0; i < n; ++i)
+    for (int q = 0; q < C.op->W; ++q) {
+      const int j = c[(size_t)i * C.op->W + q];
+      if (j >= 0) S[(size_t)i * n + j] += std::sqrt(m0[i]) * vv[(size_t)i * C.op->W + q] / std::sqrt(m0[j]);
+    }
+  for (int i = 0; i < n; ++i)
+    for (int j = i + 1; j < n; ++j) {
+      const double a = 0.5 * (S[(size_t)i * n + j] + S[(size_t)j * n + i]);
+      S[(size_t)i * n + j] = S[(size_t)j * n + i] = a;
+    }
+  std::vector<double> lam = symmetric_eigen(S, n, Q);
+  std::vector<double> E((size_t)n * n), F((size_t)n * n);
+  for (int ii = 0; ii < n; ++ii) {  // internal row / column ii <-> reference perm[ii]
+    const int r = C.perm[ii];
+    for (int k = 0; k < n; ++k) {
+      E[(size_t)ii * n + k] = Q[(size_t)r * n + k] / std::sqrt(m0[r]);
+      F[(size_t)k * n + ii] = Q[(size_t)r * n + k] * std::sqrt(m0[r]);
+    }
+  }
+  mg.eigE.upload(E);
+  mg.eigF.upload(F);
+  mg.eigL.upload(lam);
+}
+
 static void build_level_operator(Level& L, double shift, bool reorder) {
   L.op.reset(op_create_impl(L.mesh.get(), DEC_OP_HELMHOLTZ0, shift, DEC_F64));
   L.n = L.mesh->m.nv;
@@ -1061,7 +1196,9 @@ dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
   require(o.cheb_ratio > 1.0, "multigrid: cheb_ratio must exceed 1");
   require(o.inner_cycles >= 1 && o.inner_cycles <= 8, "multigrid: inner_cycles must be in [1, 8]");
   require(o.coarse_max >= 0 && o.coarse_max <= 1024, "multigrid: coarse_max must be in [0, 1024]");
-  require(o.coarse_solver == 0 || o.coarse_solver == 1, "multigrid: coarse_solver must be 0 or 1");
+  require(o.coarse_solver >= 0 && o.coarse_solver <= 2, "multigrid: coarse_solver must be 0, 1 or 2");
+  require(o.coarse_solver != 2 || (o.smoother == DEC_SMOOTH_JACOBI || o.smoother == DEC_SMOOTH_CHEBYSHEV),
+          "multigrid: per-RHS shifts (coarse_solver 2) need the Jacobi or Chebyshev smoother");
   auto mg = std::make_unique<dec_mg>();
   mg->opt = o;
   std::vector<HostLevel> hl(o.levels + 1);
@@ -1092,7 +1229,9 @@ dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
     hl[l] = refine_level(hl[l - 1], o.project_radius, l == 1 ? &flip : nullptr);
     mg->lv[o.levels - l].mesh = make_mesh(hl[l], o.center);
   }
-  for (int l = 0; l <= o.levels; ++l) build_level_operator(mg->lv[l], o.shift, o.reorder != 0);
+  // coarse_solver 2 keeps every level's operator the Laplacian; the shifts come per RHS
+  for (int l = 0; l <= o.levels; ++l)
+    build_level_operator(mg->lv[l], o.coarse_solver == 2 ? 0.0 : o.shift, o.reorder != 0);
   for (int l = 0; l <= o.levels; ++l) {
     Level& L = mg->lv[l];
     if (l < o.levels) build_transfers(L, mg->lv[l + 1], hl[o.levels - l - 1]);
@@ -1107,6 +1246,10 @@ dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
       }
   if (o.smoother == DEC_SMOOTH_CG) mg->lc = o.levels;  // the reference runs CG on its coarsest level
   const Level& C = mg->lv[mg->lc];
+  if (o.coarse_solver == 2) {
+    require(C.n <= 640, "multigrid: coarse_solver 2 needs a coarsest level of at most 640 vertices (coarse_max)");
+    build_eigen_coarse(*mg, C);
+  }
   if (o.coarse_solver == 0 && o.smoother != DEC_SMOOTH_CG) {
     auto ai = dense_inverse(*C.op, C.n);
     std::vector<double> ap((size_t)C.n * C.n);
@@ -1154,16 +1297,22 @@ static dim3 row_grid(int n, int np) {
 
 template <class T, int K>
 static void launch_sweep(const Level& L, const T* b, const T* x, T* out, T* d, SweepPrm<T> prm, int np,
-                         cudaStream_t s) {
+                         cudaStream_t s, const T* cs) {
   size_t ps = (size_t)L.n * K;
   dim3 grid = row_grid<T, K>(L.n, np);
   const T* off = pick<T>(L.off64, L.off32);
   const T* dg = pick<T>(L.diag64, L.diag32);
   const T* di = pick<T>(L.dinv64, L.dinv32);
-  if (L.W == 6)
-    launch_pdl(k_sweep<T, K, 6>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps);
-  else
-    launch_pdl(k_sweep<T, K, 0>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps);
+  if (cs) {
+    if (L.W == 6)
+      launch_pdl(k_sweep<T, K, 6, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+    else
+      launch_pdl(k_sweep<T, K, 0, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+  } else if (L.W == 6) {
+    launch_pdl(k_sweep<T, K, 6, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+  } else {
+    launch_pdl(k_sweep<T, K, 0, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+  }
 }
 
 // Smooth `sweeps` times starting from x (zero if zero_x); returns the buffer holding the result.
@@ -1180,7 +1329,7 @@ static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool z
       if (!zero_x) {
         SweepPrm<T> prm{};
         prm.mode = S_RESID;
-        launch_sweep<T, K>(L, B.b.p, x, B.d.p, nullptr, prm, np, s);
+        launch_sweep<T, K>(L, B.b.p, x, B.d.p, nullptr, prm, np, s, B.cs);
         r = B.d.p;
       }
       launch_mlp_smooth<T, K>(wts, L.n, L.W, L.col.p, L.mtab.p, pick<T>(L.diag64, L.diag32), r, x, zero_x ? 1 : 0,
@@ -1213,7 +1362,7 @@ static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool z
       prm.c2 = (T)(2 * rho_new / delta);
       rho = rho_new;
     }
-    launch_sweep<T, K>(L, B.b.p, x, other, B.d.p, prm, np, s);
+    launch_sweep<T, K>(L, B.b.p, x, other, B.d.p, prm, np, s, B.cs);
     std::swap(x, other);
     zero_x = false;
   }
@@ -1282,7 +1431,7 @@ static double* cg_mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs
   SweepPrm<double> prm{};
   prm.mode = S_RESID;
   prm.zero_x = zero_x ? 1 : 0;
-  launch_sweep<double, K>(L, B.b.p, x, r, nullptr, prm, np, s);
+  launch_sweep<double, K>(L, B.b.p, x, r, nullptr, prm, np, s, B.cs);
   const Level& Cl = mg.lv[l + 1];
   LevelBufs<double>& Cb = bufs[l + 1];
   launch_pdl(k_restrict<double, K>, row_grid<double, K>(Cl.n, np), dim3(TB), s, L.nc, L.Wq,
@@ -1308,6 +1457,14 @@ static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bu
   if (l == mg.lc) {
     if (mg.opt.coarse_solver == 1)  // the smoother on the coarsest level (pre + post sweeps)
       return smooth<T, K>(mg, L, B, x, zero_x, std::max(1, mg.opt.pre + mg.opt.post), np, s);
+    if (mg.opt.coarse_solver == 2) {  // per-RHS shifted solve through the eigendecomposition
+      const dim3 g(grid_for(L.n, TB / K, 64), np);
+      launch_pdl(k_coarse_eig1<T, K>, g, dim3(TB), s, L.n, (const double*)mg.eigF.p, (const double*)mg.eigL.p,
+                 (const double*)w.cs64.p, (const T*)B.b.p, w.ceig.p, (size_t)L.n * K);
+      launch_pdl(k_coarse_eig2<T, K>, g, dim3(TB), s, L.n, (const double*)mg.eigE.p, (const double*)w.ceig.p, B.x.p,
+                 (size_t)L.n * K);
+      return B.x.p;
+    }
     launch_pdl(k_coarse<T, K>, dim3(grid_for(L.n, TB / K, 64), np), dim3(TB), s, L.n, (const double*)mg.ainv.p,
                (const T*)B.b.p, B.x.p, (size_t)L.n * K);
     return B.x.p;
@@ -1319,7 +1476,7 @@ static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bu
   SweepPrm<T> prm{};
   prm.mode = S_RESID;
   prm.zero_x = zero_x ? 1 : 0;
-  launch_sweep<T, K>(L, B.b.p, x, r, nullptr, prm, np, s);
+  launch_sweep<T, K>(L, B.b.p, x, r, nullptr, prm, np, s, B.cs);
   const Level& Cl = mg.lv[l + 1];
   LevelBufs<T>& Cb = bufs[l + 1];
   launch_pdl(k_restrict<T, K>, row_grid<T, K>(Cl.n, np), dim3(TB), s, L.nc, L.Wq, (const int32_t*)L.rself.p,
@@ -1379,14 +1536,20 @@ static void enqueue_resid_T(dec_mg& mg, Workspace& w, cudaStream_t s, std::vecto
   launch_pdl(k_axpy_update<T>, dim3(grid_for((long long)total, 256)), dim3(256), s, total, (const T*)bufs[0].x.p,
              w.U64.p);
   dim3 g(w.nblocks, np);
-  if (F.W == 6)
-    launch_pdl(k_residual64<T, K, 6>, g, dim3(TB), s, F.n, F.W, (const int32_t*)F.col.p, (const double*)F.off64.p,
+  const double* cs = w.cs64.p;
+  auto go = [&](auto kern) {
+    launch_pdl(kern, g, dim3(TB), s, F.n, F.W, (const int32_t*)F.col.p, (const double*)F.off64.p,
                (const double*)F.diag64.p, (const double*)w.B64.p, (const double*)w.U64.p, bufs[0].b.p, w.partial.p,
-               (size_t)F.n * K);
-  else
-    launch_pdl(k_residual64<T, K, 0>, g, dim3(TB), s, F.n, F.W, (const int32_t*)F.col.p, (const double*)F.off64.p,
-               (const double*)F.diag64.p, (const double*)w.B64.p, (const double*)w.U64.p, bufs[0].b.p, w.partial.p,
-               (size_t)F.n * K);
+               (size_t)F.n * K, cs);
+  };
+  if (cs) {
+    if (F.W == 6) go(k_residual64<T, K, 6, true>);
+    else go(k_residual64<T, K, 0, true>);
+  } else if (F.W == 6) {
+    go(k_residual64<T, K, 6, false>);
+  } else {
+    go(k_residual64<T, K, 0, false>);
+  }
   launch_pdl(k_reduce_partials, dim3(K * np), dim3(256), s, w.nblocks, K, np, (const double*)w.partial.p,
              w.norms.p);
   DEC_CHECK_LAUNCH();
@@ -1503,6 +1666,17 @@ static Workspace& workspace_k(dec_mg& mg, int nrhs, int prec, int K) {
     w->scal.alloc((size_t)CG_NFIELDS * K * np);
     DEC_CUDA(cudaMemset(w->scal.p, 0, w->scal.bytes()));
   }
+  if (mg.opt.coarse_solver == 2) {
+    w->cs64.alloc((size_t)K * np);
+    w->cs32.alloc((size_t)K * np);
+    w->ceig.alloc((size_t)mg.lv[mg.lc].n * K * np);
+    w->hcs64.assign((size_t)K * np, mg.opt.shift > 0 ? mg.opt.shift : 1.0);
+    w->hcs32.assign((size_t)K * np, (float)w->hcs64[0]);
+    DEC_CUDA(cudaMemcpy(w->cs64.p, w->hcs64.data(), w->cs64.bytes(), cudaMemcpyHostToDevice));
+    DEC_CUDA(cudaMemcpy(w->cs32.p, w->hcs32.data(), w->cs32.bytes(), cudaMemcpyHostToDevice));
+    for (auto& b : w->f32) b.cs = w->cs32.p;
+    for (auto& b : w->f64) b.cs = w->cs64.p;
+  }
   DEC_CUDA(cudaMemset(w->B64.p, 0, w->B64.bytes()));
   DEC_CUDA(cudaMemset(w->U64.p, 0, w->U64.bytes()));
   auto& ref = *w;
@@ -1514,11 +1688,29 @@ static Workspace& workspace(dec_mg& mg, int nrhs, int prec) {
   return workspace_k(mg, nrhs, prec, choose_k(mg, nrhs, prec));
 }
 
+// coarse_solver 2: RHS j gets the operator L + (shift + c_j) I (c_j = 0 without `shifts`).
+static void set_shifts(const dec_mg& mg, Workspace& w, const double* shifts, int nrhs, cudaStream_t s) {
+  if (mg.opt.coarse_solver != 2) {
+    require(shifts == nullptr, "multigrid: per-RHS shifts need coarse_solver = 2");
+    return;
+  }
+  for (size_t j = 0; j < w.hcs64.size(); ++j) {
+    double c = mg.opt.shift + (shifts && (int)j < nrhs ? shifts[j] : 0.0);
+    if ((int)j >= nrhs) c = 1.0;  // padding columns (zero right-hand sides)
+    require(c > 0.0 && std::isfinite(c), "multigrid: every total shift must be positive and finite");
+    w.hcs64[j] = c;
+    w.hcs32[j] = (float)c;
+  }
+  DEC_CUDA(cudaMemcpyAsync(w.cs64.p, w.hcs64.data(), w.cs64.bytes(), cudaMemcpyHostToDevice, s));
+  DEC_CUDA(cudaMemcpyAsync(w.cs32.p, w.hcs32.data(), w.cs32.bytes(), cudaMemcpyHostToDevice, s));
+}
+
 void mg_cycles(dec_mg* mg, double* u, const double* b, int nrhs, int cycles, void* stream) {
   require(mg != nullptr && u != nullptr && b != nullptr, "multigrid: null argument");
   require(nrhs >= 1 && cycles >= 0, "multigrid: bad nrhs / cycles");
   cudaStream_t s = as_stream(stream);
   Workspace& w = workspace(*mg, nrhs, 0);
+  set_shifts(*mg, w, nullptr, nrhs, s);
   const Level& F = mg->lv[0];
   const int n = F.n;
   const size_t total = (size_t)n * w.K * w.npanels;
@@ -1535,11 +1727,13 @@ void mg_cycles(dec_mg* mg, double* u, const double* b, int nrhs, int cycles, voi
 }
 
 dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rtol, int max_iters,
-                    dec_solve_report* rep, void* stream, bool host_buffers, bool use_initial_guess) {
+                    dec_solve_report* rep, void* stream, bool host_buffers, bool use_initial_guess,
+                    const double* shifts) {
   require(mg != nullptr && u != nullptr && b != nullptr, "multigrid: null argument");
   require(nrhs >= 1 && max_iters >= 1 && rtol > 0, "multigrid: bad nrhs / max_iters / rtol");
   cudaStream_t s = as_stream(stream);
   Workspace& w = workspace(*mg, nrhs, mg->opt.precision);
+  set_shifts(*mg, w, shifts, nrhs, s);
   const Level& F = mg->lv[0];
   const int n = F.n;
   const int K = w.K, np = w.npanels;
@@ -1677,15 +1871,15 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
       prm.omega = (T)mg.opt.omega;
       prm.c1 = (T)0.5;
       prm.c2 = (T)0.25;
-      launch_sweep<T, K>(L, B.b.p, B.x.p, B.y.p, B.d.p, prm, np, s);
+      launch_sweep<T, K>(L, B.b.p, B.x.p, B.y.p, B.d.p, prm, np, s, B.cs);
     } else if (kernel == DEC_KERNEL_MLP) {
       launch_mlp_smooth<T, K>(mlp_weights(mg.mlp), L.n, L.W, L.col.p, L.mtab.p, pick<T>(L.diag64, L.diag32), B.b.p,
                               B.x.p, 0, B.y.p, np, s);
     } else if (kernel == DEC_KERNEL_RESIDUAL) {
       dim3 g(w.nblocks, np);
       const Level& F = mg.lv[0];
-      k_residual64<T, K, 0><<<g, TB, 0, s>>>(F.n, F.W, F.col.p, F.off64.p, F.diag64.p, w.B64.p, w.U64.p, bufs[0].b.p,
-                                             w.partial.p, (size_t)F.n * K);
+      k_residual64<T, K, 0, false><<<g, TB, 0, s>>>(F.n, F.W, F.col.p, F.off64.p, F.diag64.p, w.B64.p, w.U64.p,
+                                                    bufs[0].b.p, w.partial.p, (size_t)F.n * K, nullptr);
     } else if (kernel == DEC_KERNEL_RESTRICT) {
       const Level& Cl = mg.lv[level + 1];
       k_restrict<T, K><<<row_grid<T, K>(Cl.n, np), TB, 0, s>>>(L.nc, L.Wq, L.rself.p, L.ridx.p, L.rs.p, B.x.p,
@@ -1758,6 +1952,7 @@ void mg_set_smoother_mlp(dec_mg* mg, const dec_mlp* mlp) {
       if (!L.mtab.p) build_mlp_table(L.n, L.W, L.col.p, L.off64.p, L.diag64.p, L.mtab);
   mg->mlp = mlp;
   for (auto& kv : mg->ws) kv.second->drop_graphs();  // captured cycles hold the old weights' addresses
+  ++mg->epoch;
 }
 
 int mg_autotune(dec_mg* mg, int nrhs, int reps, void* stream) {
@@ -1798,8 +1993,241 @@ int mg_autotune(dec_mg* mg, int nrhs, int reps, void* stream) {
     int np = (nrhs + K - 1) / K;
     mg->ws.erase(ws_key(K, np, prec));
   }
+  ++mg->epoch;
   mg->tuned[((long long)nrhs << 2) | prec] = best;
   return best;
+}
+
+}  // namespace decb
+
+// ---------------------------------------------------------------------------------------------
+// Batched solves over several hierarchies (meshes of uneven sizes): every refinement step of all
+// groups is one CUDA graph whose branches (one per group, on forked streams) run concurrently;
+// the host reads all groups' residual norms with one copy per step.
+// ---------------------------------------------------------------------------------------------
+struct dec_batch {
+  std::vector<dec_mg*> groups;                 // not owned
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t fork = nullptr;
+  cudaStream_t cap = nullptr;
+  decb::DArr<double> norms;                    // all groups' squared residual norms
+  std::vector<size_t> off;                     // group g's norms at norms[off[g]]
+  std::vector<decb::Workspace*> used;          // workspaces the graphs were captured on
+  std::vector<uint64_t> epochs;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // 0: residual of all groups, 1: V-cycle + residual
+  int64_t launches[2] = {0, 0};
+  void drop_graphs() {
+    for (auto& g : graph) {
+      if (g) cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  }
+  ~dec_batch() {
+    drop_graphs();
+    for (auto st : streams) cudaStreamDestroy(st);
+    for (auto e : join) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (cap) cudaStreamDestroy(cap);
+  }
+};
+
+namespace decb {
+
+dec_batch* batch_create(dec_mg* const* groups, int ngroups) {
+  require(groups != nullptr && ngroups >= 1 && ngroups <= 256, "batch: need 1..256 hierarchies");
+  auto b = std::make_unique<dec_batch>();
+  for (int g = 0; g < ngroups; ++g) {
+    require(groups[g] != nullptr, "batch: null hierarchy");
+    for (int h = 0; h < g; ++h) require(groups[h] != groups[g], "batch: a hierarchy appears twice");
+    const int sm = groups[g]->opt.smoother;
+    require(sm == DEC_SMOOTH_JACOBI || sm == DEC_SMOOTH_CHEBYSHEV, "batch: groups need the Jacobi or Chebyshev smoother");
+    b->groups.push_back(groups[g]);
+    cudaStream_t st;
+    DEC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    b->streams.push_back(st);
+    cudaEvent_t e;
+    DEC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->join.push_back(e);
+  }
+  DEC_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+  DEC_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+  return b.release();
+}
+
+void batch_destroy(dec_batch* b) { delete b; }
+
+// kind 0: the residual step of every group; kind 1: V-cycle then residual of every group.  Each
+// group's norms are copied into the batch's array at the end of its branch.
+static cudaGraphExec_t batch_capture(dec_batch& bt, int kind) {
+  cudaGraph_t g = nullptr;
+  DEC_CUDA(cudaStreamBeginCapture(bt.cap, cudaStreamCaptureModeThreadLocal));
+  try {
+    DEC_CUDA(cudaEventRecord(bt.fork, bt.cap));
+    for (size_t q = 0; q < bt.groups.size(); ++q) {
+      dec_mg& mg = *bt.groups[q];
+      Workspace& w = *bt.used[q];
+      cudaStream_t st = bt.streams[q];
+      DEC_CUDA(cudaStreamWaitEvent(st, bt.fork, 0));
+      if (kind == 1) dispatch(mg, w, st, G_VCYCLE);
+      dispatch(mg, w, st, G_RESID);
+      DEC_CUDA(cudaMemcpyAsync(bt.norms.p + bt.off[q], w.norms.p, w.norms.bytes(), cudaMemcpyDeviceToDevice, st));
+      DEC_CUDA(cudaEventRecord(bt.join[q], st));
+      DEC_CUDA(cudaStreamWaitEvent(bt.cap, bt.join[q], 0));
+    }
+  } catch (...) {
+    cudaStreamEndCapture(bt.cap, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  DEC_CUDA(cudaStreamEndCapture(bt.cap, &g));
+  bt.launches[kind] = count_kernel_nodes(g);
+  cudaGraphExec_t ex = nullptr;
+  cudaError_t err = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  DEC_CUDA(err);
+  return ex;
+}
+
+void batch_autotune(dec_batch* b, const int* nrhs, int reps, void* stream) {
+  require(b != nullptr && nrhs != nullptr, "batch: null argument");
+  for (size_t q = 0; q < b->groups.size(); ++q) mg_autotune(b->groups[q], nrhs[q], reps, stream);
+  b->drop_graphs();
+}
+
+dec_status batch_solve(dec_batch* b, double* const* u, const double* const* rhs, const int* nrhs,
+                       const double* const* shifts, double rtol, int max_iters, dec_solve_report* reps,
+                       dec_solve_report* total, void* stream) {
+  require(b != nullptr && u != nullptr && rhs != nullptr && nrhs != nullptr, "batch: null argument");
+  require(max_iters >= 1 && rtol > 0, "batch: bad max_iters / rtol");
+  const size_t G = b->groups.size();
+  cudaStream_t s = as_stream(stream);
+  // workspaces (autotuned panel widths), shifts, panels, initial e = 0
+  std::vector<Workspace*> ws(G);
+  std::vector<uint64_t> ep(G);
+  size_t nn = 0;
+  std::vector<size_t> off(G);
+  for (size_t q = 0; q < G; ++q) {
+    dec_mg& mg = *b->groups[q];
+    require(u[q] != nullptr && rhs[q] != nullptr && nrhs[q] >= 1, "batch: bad group arguments");
+    ws[q] = &workspace(mg, nrhs[q], mg.opt.precision);
+    ep[q] = mg.epoch;
+    off[q] = nn;
+    nn += ws[q]->norms.n;
+  }
+  if (ws != b->used || ep != b->epochs || b->off != off) {
+    b->drop_graphs();
+    b->used = ws;
+    b->epochs = ep;
+    b->off = off;
+    if (b->norms.n < nn) b->norms.alloc(nn);
+  }
+  cudaEvent_t e0, e1;
+  DEC_CUDA(cudaEventCreate(&e0));
+  DEC_CUDA(cudaEventCreate(&e1));
+  DEC_CUDA(cudaEventRecord(e0, s));
+  std::vector<std::vector<double>> bn(G);
+  int64_t nl = 0;
+  for (size_t q = 0; q < G; ++q) {
+    dec_mg& mg = *b->groups[q];
+    Workspace& w = *ws[q];
+    set_shifts(mg, w, shifts ? shifts[q] : nullptr, nrhs[q], s);
+    const Level& F = mg.lv[0];
+    const int n = F.n, K = w.K, np = w.npanels;
+    const size_t tot = (size_t)n * K * np;
+    k_to_panels<double, double><<<grid_for((long long)tot, 256), 256, 0, s>>>(n, nrhs[q], K, np, F.dperm.p, rhs[q], w.B64.p);
+    k_to_panels<double, double><<<grid_for((long long)tot, 256), 256, 0, s>>>(n, nrhs[q], K, np, F.dperm.p, u[q], w.U64.p);
+    if (w.prec == 1) DEC_CUDA(cudaMemsetAsync(w.f32[0].x.p, 0, tot * sizeof(float), s));
+    else DEC_CUDA(cudaMemsetAsync(w.f64[0].x.p, 0, tot * sizeof(double), s));
+    dim3 g(w.nblocks, np);
+    switch (K) {
+#define DEC_K(KK) \
+  case KK: k_panel_sumsq<KK><<<g, TB, 0, s>>>(n, w.B64.p, w.partial.p, (size_t)n * KK); break;
+      DEC_K(1) DEC_K(2) DEC_K(4) DEC_K(8) DEC_K(16) DEC_K(32)
+#undef DEC_K
+    }
+    k_reduce_partials<<<K * np, 256, 0, s>>>(w.nblocks, K, np, w.partial.p, b->norms.p + off[q]);
+    DEC_CHECK_LAUNCH();
+    nl += 5;
+  }
+  std::vector<double> hn(nn);
+  auto fetch = [&]() {
+    DEC_CUDA(cudaMemcpyAsync(hn.data(), b->norms.p, nn * sizeof(double), cudaMemcpyDeviceToHost, s));
+    DEC_CUDA(cudaStreamSynchronize(s));
+  };
+  fetch();
+  for (size_t q = 0; q < G; ++q) {
+    bn[q].resize(nrhs[q]);
+    for (int j = 0; j < nrhs[q]; ++j) bn[q][j] = std::sqrt(hn[off[q] + j]);
+  }
+  if (!b->graph[0]) b->graph[0] = batch_capture(*b, 0);
+  if (!b->graph[1]) b->graph[1] = batch_capture(*b, 1);
+  std::vector<double> worst(G, 0.0);
+  std::vector<int> conv_at(G, -1);
+  auto check = [&](int it) {
+    fetch();
+    bool all = true;
+    for (size_t q = 0; q < G; ++q) {
+      double wr = 0.0;
+      for (int j = 0; j < nrhs[q]; ++j) {
+        const double r = std::sqrt(hn[off[q] + j]);
+        const double rel = bn[q][j] > 0 ? r / bn[q][j] : r;
+        wr = std::isfinite(rel) ? std::max(wr, rel) : HUGE_VAL;
+      }
+      worst[q] = wr;
+      if (conv_at[q] < 0 && wr <= rtol) conv_at[q] = it;
+      all = all && conv_at[q] >= 0;
+    }
+    return all;
+  };
+  DEC_CUDA(cudaGraphLaunch(b->graph[0], s));
+  nl += b->launches[0];
+  int it = 0;
+  bool all = check(0);
+  while (!all && it < max_iters) {
+    DEC_CUDA(cudaGraphLaunch(b->graph[1], s));
+    nl += b->launches[1];
+    ++it;
+    all = check(it);
+  }
+  for (size_t q = 0; q < G; ++q) {
+    dec_mg& mg = *b->groups[q];
+    Workspace& w = *ws[q];
+    const Level& F = mg.lv[0];
+    k_from_panels<double, double><<<grid_for((long long)F.n * nrhs[q], 256), 256, 0, s>>>(F.n, nrhs[q], w.K, F.diperm.p,
+                                                                                           w.U64.p, u[q]);
+    ++nl;
+  }
+  DEC_CHECK_LAUNCH();
+  DEC_CUDA(cudaEventRecord(e1, s));
+  DEC_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  double wmax = 0.0;
+  for (size_t q = 0; q < G; ++q) {
+    wmax = std::max(wmax, worst[q]);
+    if (reps) {
+      reps[q].iterations = conv_at[q] >= 0 ? conv_at[q] : it;
+      reps[q].converged = conv_at[q] >= 0 ? 1 : 0;
+      reps[q].max_rel_residual = worst[q];
+      reps[q].seconds = ms * 1e-3;
+      reps[q].launches = 0;
+      reps[q].rhs_block = ws[q]->K;
+      reps[q].fallback_iteration = -1;
+    }
+  }
+  if (total) {
+    total->iterations = it;
+    total->converged = all ? 1 : 0;
+    total->max_rel_residual = wmax;
+    total->seconds = ms * 1e-3;
+    total->launches = nl;
+    total->rhs_block = 0;
+    total->fallback_iteration = -1;
+  }
+  return all ? DEC_OK : DEC_ERR_NOT_CONVERGED;
 }
 
 }  // namespace decb

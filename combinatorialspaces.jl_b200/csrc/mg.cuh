@@ -12,9 +12,16 @@ const dec_mesh* mg_level_mesh(const dec_mg* mg, int level);
 const dec_op* mg_level_op(const dec_mg* mg, int level);
 void mg_cycles(dec_mg* mg, double* u, const double* b, int nrhs, int cycles, void* stream);
 dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rtol, int max_iters,
-                    dec_solve_report* rep, void* stream, bool host_buffers, bool use_initial_guess);
+                    dec_solve_report* rep, void* stream, bool host_buffers, bool use_initial_guess,
+                    const double* shifts = nullptr);
 void mg_time_kernel(dec_mg* mg, int kernel, int level, int nrhs, int reps, void* stream, double* ms,
                     double* bytes);
 int mg_autotune(dec_mg* mg, int nrhs, int reps, void* stream);
 void mg_set_smoother_mlp(dec_mg* mg, const dec_mlp* mlp);
+dec_batch* batch_create(dec_mg* const* groups, int ngroups);
+void batch_destroy(dec_batch* b);
+void batch_autotune(dec_batch* b, const int* nrhs, int reps, void* stream);
+dec_status batch_solve(dec_batch* b, double* const* u, const double* const* rhs, const int* nrhs,
+                       const double* const* shifts, double rtol, int max_iters, dec_solve_report* reps,
+                       dec_solve_report* total, void* stream);
 }  // namespace decb

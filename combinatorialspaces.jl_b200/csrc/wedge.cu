@@ -9,6 +9,10 @@
 // The expressions mirror the reference kernels term by term and this file is compiled without
 // FMA contraction, so FP64 / FP32 results reproduce the reference CPU arithmetic bit for bit
 // where the reference's order of operations is kept (∧01, ∧11, the pd/dd SpMV forms).
+//
+// Batched application: blockIdx.y selects the form pair; each kernel offsets its form pointers
+// by blockIdx.y times the form lengths, so a batch is one launch whose index and coefficient
+// streams stay resident in L2 across the pairs.
 #include <algorithm>
 
 #include "mesh.cuh"
@@ -45,7 +49,11 @@ constexpr int kThreads = 256;
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_w01(int ne, const int32_t* __restrict__ ev0,
                                                   const int32_t* __restrict__ ev1, const T* __restrict__ f,
-                                                  const T* __restrict__ a, T* __restrict__ out) {
+                                                  const T* __restrict__ a, T* __restrict__ out, size_t sf, size_t sa,
+                                                  size_t so) {
+  f += blockIdx.y * sf;
+  a += blockIdx.y * sa;
+  out += blockIdx.y * so;
   const T half = T(0.5);
   for (long long base = (long long)blockIdx.x * kThreads * kItems; base < ne;
        base += (long long)gridDim.x * kThreads * kItems) {
@@ -75,7 +83,11 @@ __global__ void __launch_bounds__(kThreads) k_w02(int nt, const int32_t* __restr
                                                   const int32_t* __restrict__ tv1, const int32_t* __restrict__ tv2,
                                                   const T* __restrict__ w0, const T* __restrict__ w1,
                                                   const T* __restrict__ w2, const T* __restrict__ f,
-                                                  const T* __restrict__ a, T* __restrict__ out) {
+                                                  const T* __restrict__ a, T* __restrict__ out, size_t sf, size_t sa,
+                                                  size_t so) {
+  f += blockIdx.y * sf;
+  a += blockIdx.y * sa;
+  out += blockIdx.y * so;
   for (long long base = (long long)blockIdx.x * kThreads * kItems; base < nt;
        base += (long long)gridDim.x * kThreads * kItems) {
     int v[kItems][3];
@@ -109,7 +121,11 @@ __global__ void __launch_bounds__(kThreads) k_w11(int nt, const int32_t* __restr
                                                   const int32_t* __restrict__ te1, const int32_t* __restrict__ te2,
                                                   const T* __restrict__ c0, const T* __restrict__ c1,
                                                   const T* __restrict__ c2, const T* __restrict__ a,
-                                                  const T* __restrict__ b, T* __restrict__ out) {
+                                                  const T* __restrict__ b, T* __restrict__ out, size_t sa, size_t sb,
+                                                  size_t so) {
+  a += blockIdx.y * sa;
+  b += blockIdx.y * sb;
+  out += blockIdx.y * so;
   for (long long base = (long long)blockIdx.x * kThreads * kItems; base < nt;
        base += (long long)gridDim.x * kThreads * kItems) {
     int e[kItems][3];
@@ -145,7 +161,10 @@ template <class T, int W>
 __global__ void __launch_bounds__(kThreads) k_ell_hadamard(int n, const int32_t* __restrict__ idx,
                                                            const T* __restrict__ val, const T* __restrict__ x,
                                                            const T* __restrict__ y, T* __restrict__ out,
-                                                           int mx_first) {
+                                                           int mx_first, size_t sx, size_t sy, size_t so) {
+  x += blockIdx.y * sx;
+  y += blockIdx.y * sy;
+  out += blockIdx.y * so;
   for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
     T s = T(0);
 #pragma unroll
@@ -295,54 +314,74 @@ static void build_plan(dec_wedge_plan& P) {
   DEC_CUDA(cudaDeviceSynchronize());
 }
 
+// `count` form pairs (a, b, out consecutive with the plan's lengths), one launch per kind.
 template <class T>
-static void launch_plan(dec_wedge_plan& P, const CoefSet<T>& c, const void* va, const void* vb, void* vo,
+static void launch_plan(dec_wedge_plan& P, const CoefSet<T>& c, const void* va, const void* vb, void* vo, int count,
                         cudaStream_t s) {
   Mesh& m = *P.m;
   const T* a = (const T*)va;
   const T* b = (const T*)vb;
   T* o = (T*)vo;
+  const size_t sa = P.len_a, sb = P.len_b, so = P.len_out;
   const int* idx = P.c64.idx.p;
-  switch (P.op) {
-    case W01:
-    case W10: {
-      const T* f = P.op == W01 ? a : b;
-      const T* al = P.op == W01 ? b : a;
-      if (m.ne) k_w01<T><<<grid_for(m.ne, kThreads * kItems), kThreads, 0, s>>>(m.ne, m.ev0.p, m.ev1.p, f, al, o);
-      break;
+  // the batch is grid.y (at most 65,535 pairs per launch) and every pair keeps the single-pair
+  // grid: CTAs are dispatched x-fastest, so a few pairs at a time stream through L2 and each form
+  // value shared by neighbouring simplices is read from DRAM once
+  auto grid2 = [&](long long n, int per, int cnt) { return dim3(grid_for(n, per), (unsigned)cnt); };
+  for (int done = 0; done < count;) {
+    const int cnt = std::min(count - done, 65535);
+    const T* ab = a + (size_t)done * sa;
+    const T* bb = b + (size_t)done * sb;
+    T* ob = o + (size_t)done * so;
+    switch (P.op) {
+      case W01:
+      case W10: {
+        const T* f = P.op == W01 ? ab : bb;
+        const T* al = P.op == W01 ? bb : ab;
+        const size_t sf = P.op == W01 ? sa : sb, sl = P.op == W01 ? sb : sa;
+        if (m.ne)
+          k_w01<T><<<grid2(m.ne, kThreads * kItems, cnt), kThreads, 0, s>>>(m.ne, m.ev0.p, m.ev1.p, f, al, ob, sf, sl,
+                                                                              so);
+        break;
+      }
+      case W02:
+      case W20: {
+        const T* f = P.op == W02 ? ab : bb;
+        const T* al = P.op == W02 ? bb : ab;
+        const size_t sf = P.op == W02 ? sa : sb, sl = P.op == W02 ? sb : sa;
+        if (m.nt)
+          k_w02<T><<<grid2(m.nt, kThreads * kItems, cnt), kThreads, 0, s>>>(m.nt, m.tv0.p, m.tv1.p, m.tv2.p, c.c[0].p,
+                                                                              c.c[1].p, c.c[2].p, f, al, ob, sf, sl, so);
+        break;
+      }
+      case W11:
+        if (m.nt)
+          k_w11<T><<<grid2(m.nt, kThreads * kItems, cnt), kThreads, 0, s>>>(m.nt, m.te0.p, m.te1.p, m.te2.p, c.c[0].p,
+                                                                              c.c[1].p, c.c[2].p, ab, bb, ob, sa, sb, so);
+        break;
+      default:
+        break;
     }
-    case W02:
-    case W20: {
-      const T* f = P.op == W02 ? a : b;
-      const T* al = P.op == W02 ? b : a;
-      if (m.nt)
-        k_w02<T><<<grid_for(m.nt, kThreads * kItems), kThreads, 0, s>>>(m.nt, m.tv0.p, m.tv1.p, m.tv2.p, c.c[0].p,
-                                                                         c.c[1].p, c.c[2].p, f, al, o);
-      break;
+    if (P.op >= WDD01) {
+      // x is the form that M acts on; y is multiplied elementwise:
+      //  dd(0,1)(f, g) = (M f) .* g,  pd(0,1)(g, f) = (M g) .* f   -> M acts on the first form
+      //  dd(1,0)(f, g) = f .* (M g),  dp(1,0)(f, g) = f .* (M g)   -> M acts on the second form
+      const bool mfirst = (P.op == WDD01 || P.op == WPD01);
+      const T* x = mfirst ? ab : bb;
+      const T* y = mfirst ? bb : ab;
+      const size_t sx = mfirst ? sa : sb, sy = mfirst ? sb : sa;
+      if (m.ne) {
+        if (c.width == 2)
+          k_ell_hadamard<T, 2><<<grid2(m.ne, kThreads, cnt), kThreads, 0, s>>>(m.ne, idx, c.val.p, x, y, ob, mfirst,
+                                                                               sx, sy, so);
+        else
+          k_ell_hadamard<T, 4><<<grid2(m.ne, kThreads, cnt), kThreads, 0, s>>>(m.ne, idx, c.val.p, x, y, ob, mfirst,
+                                                                               sx, sy, so);
+      }
     }
-    case W11:
-      if (m.nt)
-        k_w11<T><<<grid_for(m.nt, kThreads * kItems), kThreads, 0, s>>>(m.nt, m.te0.p, m.te1.p, m.te2.p, c.c[0].p,
-                                                                         c.c[1].p, c.c[2].p, a, b, o);
-      break;
-    default:
-      break;
+    DEC_CHECK_LAUNCH();
+    done += cnt;
   }
-  if (P.op >= WDD01) {
-    // x is the form that M acts on; y is multiplied elementwise:
-    //  dd(0,1)(f, g) = (M f) .* g,  pd(0,1)(g, f) = (M g) .* f   -> M acts on the first form
-    //  dd(1,0)(f, g) = f .* (M g),  dp(1,0)(f, g) = f .* (M g)   -> M acts on the second form
-    bool mfirst = (P.op == WDD01 || P.op == WPD01);
-    const T* x = mfirst ? a : b;
-    const T* y = mfirst ? b : a;
-    if (m.ne) {
-      if (c.width == 2)
-        k_ell_hadamard<T, 2><<<grid_for(m.ne, kThreads), kThreads, 0, s>>>(m.ne, idx, c.val.p, x, y, o, mfirst);
-      else
-        k_ell_hadamard<T, 4><<<grid_for(m.ne, kThreads), kThreads, 0, s>>>(m.ne, idx, c.val.p, x, y, o, mfirst);
-    }
-  }
-  DEC_CHECK_LAUNCH();
 }
 
 }  // namespace decb
@@ -395,14 +434,8 @@ void wedge_apply_impl(dec_wedge_plan* P, const void* a, const void* b, void* out
   require(a && b && out, "wedge: null form pointer");
   require(count >= 1, "wedge: count must be >= 1");
   cudaStream_t s = as_stream(stream);
-  const size_t es = P->dtype == DEC_F64 ? 8 : 4;
-  for (int i = 0; i < count; ++i) {
-    const char* ai = (const char*)a + (size_t)i * P->len_a * es;
-    const char* bi = (const char*)b + (size_t)i * P->len_b * es;
-    char* oi = (char*)out + (size_t)i * P->len_out * es;
-    if (P->dtype == DEC_F64) launch_plan<double>(*P, P->c64, ai, bi, oi, s);
-    else launch_plan<float>(*P, P->c32, ai, bi, oi, s);
-  }
+  if (P->dtype == DEC_F64) launch_plan<double>(*P, P->c64, a, b, out, count, s);
+  else launch_plan<float>(*P, P->c32, a, b, out, count, s);
 }
 
 void wedge_plan_destroy_impl(dec_wedge_plan* P) { delete P; }

@@ -45,6 +45,7 @@ typedef struct dec_wedge_plan dec_wedge_plan;
 typedef struct dec_op dec_op;
 typedef struct dec_mg dec_mg;
 typedef struct dec_mlp dec_mlp;
+typedef struct dec_batch dec_batch;
 
 /*
  * A primal 2D delta set with embedding, i.e. the fields of EmbeddedDeltaSet2D{Bool,Point3d}
@@ -170,7 +171,11 @@ typedef struct dec_mg_options {
   int32_t pre, post;       /* sweeps / degree / CG steps */
   double omega;            /* Jacobi damping */
   double cheb_ratio;       /* Chebyshev interval [lmax / ratio, lmax] */
-  int32_t coarse_solver;   /* 0: dense direct FP64 solve on the coarsest level; 1: the smoother */
+  int32_t coarse_solver;   /* 0: dense direct FP64 solve on the coarsest level; 1: the smoother;
+                              2: exact solve through the coarsest Laplacian's eigendecomposition, which
+                              admits a shift per right-hand side (every level then stores the
+                              Laplacian, and RHS j solves (L + (shift + c_j) I) u = b; see
+                              dec_mg_solve_shifted); Jacobi / Chebyshev smoothers only */
   int32_t precision;       /* 0: FP64 V-cycles; 1: FP32 V-cycles inside FP64 iterative refinement */
   int32_t rhs_block;       /* right-hand sides per panel (1, 2, 4, 8, 16, 32; 0 = automatic) */
   int32_t mu;              /* 1 = V-cycle, 2 = W-cycle */
@@ -212,6 +217,30 @@ dec_status dec_mg_solve(dec_mg* mg, double* u, const double* b, int32_t nrhs, do
 dec_status dec_mg_solve_host(dec_mg* mg, double* u_host, const double* b_host, int32_t nrhs, double rtol,
                              int32_t max_iters, int32_t use_initial_guess, dec_solve_report* report,
                              void* stream);
+
+/* dec_mg_solve with a shift per right-hand side (coarse_solver 2): RHS j solves
+ * (L + (shift + shifts[j]) I) u_j = b_j; shifts is a host array of nrhs values (total shifts must
+ * be positive). */
+dec_status dec_mg_solve_shifted(dec_mg* mg, double* u, const double* b, int32_t nrhs, const double* shifts,
+                                double rtol, int32_t max_iters, dec_solve_report* report, void* stream);
+
+/* ---- batched solves over several hierarchies (meshes of uneven sizes; no counterpart in the
+ *      reference): every refinement step of all groups is one CUDA graph with a concurrent branch
+ *      per group (FP32 or FP64 V-cycles per each hierarchy's options, FP64 refinement), one
+ *      residual-norm read-back per step for all groups.  Groups use the Jacobi or Chebyshev smoother.
+ * ------------------------------------------------------------------------------------------ */
+/* The hierarchies are not owned and must outlive the batch. */
+dec_status dec_batch_create(dec_mg* const* groups, int32_t ngroups, dec_batch** out);
+dec_status dec_batch_destroy(dec_batch* batch);
+/* Runs dec_mg_autotune on every group for its nrhs (panel width per group). */
+dec_status dec_batch_autotune(dec_batch* batch, const int32_t* nrhs, int32_t reps, void* stream);
+/* Group g: u[g] (in/out initial guess) and rhs[g] device FP64 column-major n_g x nrhs[g];
+ * shifts[g] host per-RHS shifts (coarse_solver 2 groups) or NULL (shifts itself may be NULL).
+ * Every group runs until all groups reach rtol or max_iters refinement steps; reports[g] gives the
+ * step at which group g converged, total the whole batch (device seconds, kernels launched). */
+dec_status dec_batch_solve(dec_batch* batch, double* const* u, const double* const* rhs, const int32_t* nrhs,
+                           const double* const* shifts, double rtol, int32_t max_iters,
+                           dec_solve_report* reports, dec_solve_report* total, void* stream);
 
 /* Learned smoother for DEC_SMOOTH_LEARNED: the hierarchy reads the network's weights at every
  * cycle (the network must outlive its use; retraining takes effect at the next cycle).  NULL
