@@ -128,18 +128,20 @@ class ClockSampler:
 
 def measure_operators(dec, peak):
     """HBM roofline of the DEC operator kernels: each kernel timed alone with CUDA events, L2
-    flushed (a 256 MB write) before every launch, on icosphere L9 (circumcentric duals) and a
+    flushed before every launch by reading a 256 MB buffer (a read leaves L2 holding clean lines,
+    so the timed kernel pays no write-back of the flush), on icosphere L9 (circumcentric duals) and a
     2049x2049 grid (barycentric duals, a 9x9 triangulated grid binary-refined 8 times), FP64 and
     FP32.  Algorithmic bytes: every streamed array once, each gathered form once (int32 indices)."""
     import torch
 
-    flush = torch.empty(64 * 2 ** 20, dtype=torch.float32, device="cuda")
+    flush = torch.ones(64 * 2 ** 20, dtype=torch.float32, device="cuda")
+    sink = torch.empty((), dtype=torch.float32, device="cuda")
 
     def time_op(fn, reps=10):
         fn()
         tot = 0.0
         for _ in range(reps):
-            flush.fill_(1.0)
+            torch.sum(flush, dim=0, out=sink)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()

@@ -675,13 +675,13 @@ __global__ void k_split(int n, int Wf, const int32_t* __restrict__ fcol, const d
     int q = 0;
     double dg = 0.0;
     for (int s = 0; s < Wf; ++s) {
-      int c = fcol[(size_t)r * Wf + s];
+      int c = fcol[(size_t)s * n + r];
       if (c < 0) continue;
       if (c == r) {
-        dg += fval[(size_t)r * Wf + s];
+        dg += fval[(size_t)s * n + r];
       } else if (q < W) {
         col[(size_t)i * W + q] = iperm[c];
-        off[(size_t)i * W + q] = fval[(size_t)r * Wf + s];
+        off[(size_t)i * W + q] = fval[(size_t)s * n + r];
         ++q;
       }
     }
@@ -1005,8 +1005,8 @@ static std::vector<double> dense_inverse(const dec_op& op, int n) {
   std::vector<double> A((size_t)n * n, 0.0), Ainv((size_t)n * n, 0.0);
   for (int i = 0; i < n; ++i)
     for (int q = 0; q < op.W; ++q) {
-      int j = c[(size_t)i * op.W + q];
-      if (j >= 0) A[(size_t)i * n + j] += vv[(size_t)i * op.W + q];
+      int j = c[(size_t)q * n + i];
+      if (j >= 0) A[(size_t)i * n + j] += vv[(size_t)q * n + i];
     }
   for (int i = 0; i < n; ++i) Ainv[(size_t)i * n + i] = 1.0;
   double amax = 0.0;
@@ -1094,8 +1094,8 @@ static void build_eigen_coarse(dec_mg& mg, const Level& C) {
   std::vector<double> S((size_t)n * n, 0.0), Q;
   for (int i = 0; i < n; ++i)
     for (int q = 0; q < C.op->W; ++q) {
-      const int j = c[(size_t)i * C.op->W + q];
-      if (j >= 0) S[(size_t)i * n + j] += std::sqrt(m0[i]) * vv[(size_t)i * C.op->W + q] / std::sqrt(m0[j]);
+      const int j = c[(size_t)q * n + i];
+      if (j >= 0) S[(size_t)i * n + j] += std::sqrt(m0[i]) * vv[(size_t)q * n + i] / std::sqrt(m0[j]);
     }
   for (int i = 0; i < n; ++i)
     for (int j = i + 1; j < n; ++j) {

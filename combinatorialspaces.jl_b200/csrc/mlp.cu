@@ -393,20 +393,20 @@ __global__ void k_bwd_direct(int64_t n, const float* __restrict__ x, const float
     backward_sample(x + q * 16, dy[q], w1b, w2b, p, act, q, n, dyb);
 }
 
-// Features of sample (vertex i, field rs) on a reference-ordered Laplacian / Helmholtz operator
-// (sorted ELL with the diagonal inside, padding column -1).
-__device__ void op_features(int i, int Wf, const int32_t* __restrict__ col, const double* __restrict__ val,
+// Features of sample (vertex i, field rs) on a reference-ordered Laplacian / Helmholtz operator of
+// n rows (slot-major ELL, columns sorted, the diagonal inside, padding column -1).
+__device__ void op_features(int i, int n, int Wf, const int32_t* __restrict__ col, const double* __restrict__ val,
                             const double* __restrict__ rs, float* f, float* dsc) {
   double di = 0.0;
   for (int q = 0; q < Wf; ++q)
-    if (col[(size_t)i * Wf + q] == i) di += val[(size_t)i * Wf + q];
+    if (col[(size_t)q * n + i] == i) di += val[(size_t)q * n + i];
   float nb[6], cp[6], sabs = 0.f;
   int nn = 0;
   const float dif = (float)di;
   for (int q = 0; q < Wf; ++q) {
-    const int c = col[(size_t)i * Wf + q];
+    const int c = col[(size_t)q * n + i];
     if (c < 0 || c == i) continue;
-    const float o = (float)val[(size_t)i * Wf + q];
+    const float o = (float)val[(size_t)q * n + i];
     sabs += fabsf(o);
     if (nn < 6) {
       nb[nn] = (float)rs[c];
@@ -425,7 +425,7 @@ __global__ void k_op_features(int n, int S, int Wf, const int32_t* __restrict__ 
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < N; q += (int64_t)gridDim.x * blockDim.x) {
     const int s = (int)(q / n), i = (int)(q % n);
     float f[16], dsc;
-    op_features(i, Wf, col, val, r + (size_t)s * n, f, &dsc);
+    op_features(i, n, Wf, col, val, r + (size_t)s * n, f, &dsc);
     for (int k = 0; k < 16; ++k) feat[q * 16 + k] = f[k];
     dscale[q] = dsc;
   }
@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_train_fwd(int n, int S, int Wf,
     float f[16], dsc = 0.f;
     if (q < N) {
       const int s = (int)(q / n), i = (int)(q % n);
-      op_features(i, Wf, col, val, r + (size_t)s * n, f, &dsc);
+      op_features(i, n, Wf, col, val, r + (size_t)s * n, f, &dsc);
     } else {
 #pragma unroll
       for (int k = 0; k < 16; ++k) f[k] = 0.f;
@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(256) k_train_norms(int n, int Wf, const int32_
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     double di = 0.0;
     for (int q = 0; q < Wf; ++q)
-      if (col[(size_t)i * Wf + q] == i) di += val[(size_t)i * Wf + q];
+      if (col[(size_t)q * n + i] == i) di += val[(size_t)q * n + i];
     acc += star0[i] * rs[i] * rs[i] / di;
   }
   __shared__ double sh[256];
@@ -536,7 +536,7 @@ __global__ void k_train_bwd(int n, int S, int64_t B, uint64_t seed, int64_t step
     }
     const int s = (int)(q / n), i = (int)(q % n);
     float f[16], dsc;
-    op_features(i, Wf, col, val, r + (size_t)s * n, f, &dsc);
+    op_features(i, n, Wf, col, val, r + (size_t)s * n, f, &dsc);
     backward_sample(f, (float)(dy[q] * scale), w1b, w2b, p, act, j, Bn, dyb);
   }
 }

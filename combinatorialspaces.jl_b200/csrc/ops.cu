@@ -8,6 +8,7 @@
 // without FMA contraction, so results reproduce the reference CPU arithmetic.
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 
 #include "mesh.cuh"
 #include "ops.cuh"
@@ -55,6 +56,88 @@ __global__ void __launch_bounds__(kOpThreads) k_d1(int nt, const int32_t* __rest
   }
 }
 
+// Four consecutive rows per thread with 16-byte index loads, one 32-bit load of the four sign
+// bytes and vector stores (y 16-byte aligned); the arithmetic per row is that of k_d0 / k_d1.
+template <class T>
+__device__ __forceinline__ void store4(T* y, int g, const T (&v)[4]) {
+  if constexpr (sizeof(T) == 4) {
+    __stcs(reinterpret_cast<float4*>(y) + g, make_float4(v[0], v[1], v[2], v[3]));
+  } else {
+    __stcs(reinterpret_cast<double2*>(y) + 2 * g, make_double2(v[0], v[1]));
+    __stcs(reinterpret_cast<double2*>(y) + 2 * g + 1, make_double2(v[2], v[3]));
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kOpThreads) k_d0v(int ne, const int32_t* __restrict__ ev0,
+                                                    const int32_t* __restrict__ ev1, const int8_t* __restrict__ es,
+                                                    const T* __restrict__ x, T* __restrict__ y, T alpha, T beta,
+                                                    bool hb) {
+  const int ng = ne / 4;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+    const int4 a = __ldcs(reinterpret_cast<const int4*>(ev0) + g);
+    const int4 b = __ldcs(reinterpret_cast<const int4*>(ev1) + g);
+    const int sg = __ldcs(reinterpret_cast<const int*>(es) + g);
+    const int ia[4] = {a.x, a.y, a.z, a.w}, ib[4] = {b.x, b.y, b.z, b.w};
+    T xa[4], xb[4], o[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      xa[k] = __ldg(x + ia[k]);
+      xb[k] = __ldg(x + ib[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const T sv = (T)(int8_t)((sg >> (8 * k)) & 0xff);
+      const T sk = sv * (xa[k] - xb[k]);
+      o[k] = epilogue(sk, hb ? y[4 * (size_t)g + k] : T(0), alpha, beta, hb);
+    }
+    store4(y, g, o);
+  }
+  for (int e = 4 * ng + blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+    const T sk = (T)es[e] * (__ldg(x + ev0[e]) - __ldg(x + ev1[e]));
+    y[e] = epilogue(sk, hb ? y[e] : T(0), alpha, beta, hb);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kOpThreads) k_d1v(int nt, const int32_t* __restrict__ c0,
+                                                    const int32_t* __restrict__ c1, const int32_t* __restrict__ c2,
+                                                    const uint8_t* __restrict__ neg, const T* __restrict__ x,
+                                                    T* __restrict__ y, T alpha, T beta, bool hb) {
+  const int ng = nt / 4;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+    const int4 p = __ldcs(reinterpret_cast<const int4*>(c0) + g);
+    const int4 q = __ldcs(reinterpret_cast<const int4*>(c1) + g);
+    const int4 r = __ldcs(reinterpret_cast<const int4*>(c2) + g);
+    const unsigned ng4 = (unsigned)__ldcs(reinterpret_cast<const int*>(neg) + g);
+    const int i0[4] = {p.x, p.y, p.z, p.w}, i1[4] = {q.x, q.y, q.z, q.w}, i2[4] = {r.x, r.y, r.z, r.w};
+    T va[4], vb[4], vc[4], o[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      va[k] = __ldg(x + i0[k]);
+      vb[k] = __ldg(x + i1[k]);
+      vc[k] = __ldg(x + i2[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const unsigned n = (ng4 >> (8 * k)) & 0xffu;
+      T sk = (n & 1) ? -va[k] : va[k];
+      sk = sk + ((n & 2) ? -vb[k] : vb[k]);
+      sk = sk + ((n & 4) ? -vc[k] : vc[k]);
+      o[k] = epilogue(sk, hb ? y[4 * (size_t)g + k] : T(0), alpha, beta, hb);
+    }
+    store4(y, g, o);
+  }
+  for (int t = 4 * ng + blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+    const uint8_t n = neg[t];
+    const T a = __ldg(x + c0[t]), b = __ldg(x + c1[t]), c = __ldg(x + c2[t]);
+    T sk = (n & 1) ? -a : a;
+    sk = sk + ((n & 2) ? -b : b);
+    sk = sk + ((n & 4) ? -c : c);
+    y[t] = epilogue(sk, hb ? y[t] : T(0), alpha, beta, hb);
+  }
+}
+
 // Transposed incidence rows: entry ±(j+1) contributes ±x[j].
 template <class T>
 __global__ void k_signed_rows(int n, const int32_t* __restrict__ ptr, const int32_t* __restrict__ ent,
@@ -93,48 +176,32 @@ __global__ void __launch_bounds__(kOpThreads) k_diag(int n, const T* __restrict_
   }
 }
 
-// Row-major ELL SpMV, one thread per row (padding: column -1).  Rows are padded to a multiple
-// of 4 entries so each row's columns and values come in with 16-byte vector loads; the row sum
-// runs in column order.
-template <class T, int WP>
+// Slot-major ELL SpMV (entry (i, q) at q * n + i; padding: column -1), one thread per row: the
+// q-th loads of a warp are 32 consecutive rows, one contiguous segment per slot.  All loads of a
+// row are issued before the products; the row sum runs in slot (= column) order.
+template <class T, int WC>
 __global__ void __launch_bounds__(kOpThreads) k_ell(int n, int W, const int32_t* __restrict__ col,
                                                     const T* __restrict__ val, const T* __restrict__ x,
                                                     T* __restrict__ y, T alpha, T beta, bool hb) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     T s = T(0);
-    if constexpr (WP > 0) {
-      int c[WP];
-      T v[WP];
+    if constexpr (WC > 0) {
+      int c[WC];
+      T v[WC], g[WC];
 #pragma unroll
-      for (int q = 0; q < WP; q += 4) {
-        int4 cc = __ldcs(reinterpret_cast<const int4*>(col + (size_t)i * WP + q));
-        c[q] = cc.x; c[q + 1] = cc.y; c[q + 2] = cc.z; c[q + 3] = cc.w;
+      for (int q = 0; q < WC; ++q) {
+        c[q] = __ldcs(col + (size_t)q * n + i);
+        v[q] = __ldcs(val + (size_t)q * n + i);
       }
-      if constexpr (sizeof(T) == 8) {
 #pragma unroll
-        for (int q = 0; q < WP; q += 2) {
-          double2 vv = __ldcs(reinterpret_cast<const double2*>(val + (size_t)i * WP + q));
-          v[q] = vv.x; v[q + 1] = vv.y;
-        }
-      } else {
+      for (int q = 0; q < WC; ++q) g[q] = c[q] >= 0 ? __ldg(x + c[q]) : T(0);
 #pragma unroll
-        for (int q = 0; q < WP; q += 4) {
-          float4 vv = __ldcs(reinterpret_cast<const float4*>(val + (size_t)i * WP + q));
-          v[q] = vv.x; v[q + 1] = vv.y; v[q + 2] = vv.z; v[q + 3] = vv.w;
-        }
-      }
-      T g[WP];
-#pragma unroll
-      for (int q = 0; q < WP; ++q) g[q] = c[q] >= 0 ? __ldg(x + c[q]) : T(0);
-#pragma unroll
-      for (int q = 0; q < WP; ++q)
+      for (int q = 0; q < WC; ++q)
         if (c[q] >= 0) s += v[q] * g[q];
     } else {
-      const int32_t* c = col + (size_t)i * W;
-      const T* v = val + (size_t)i * W;
       for (int q = 0; q < W; ++q) {
-        int j = __ldcs(c + q);
-        if (j >= 0) s += __ldcs(v + q) * __ldg(x + j);
+        const int j = __ldcs(col + (size_t)q * n + i);
+        if (j >= 0) s += __ldcs(val + (size_t)q * n + i) * __ldg(x + j);
       }
     }
     y[i] = epilogue(s, hb ? y[i] : T(0), alpha, beta, hb);
@@ -153,8 +220,8 @@ __global__ void k_laplace_rows(int nv, int W, const int32_t* __restrict__ ptr, c
     const double h = (1 / star0[i]) * 1.0;
     double diag = 0.0;
     int cnt = 0;
-    int32_t* c = col + (size_t)i * W;
-    double* v = val + (size_t)i * W;
+    auto c = [&](int q) -> int32_t& { return col[(size_t)q * nv + i]; };  // slot-major
+    auto v = [&](int q) -> double& { return val[(size_t)q * nv + i]; };
     for (int q = ptr[i]; q < ptr[i + 1]; ++q) {
       int ent = v2e[q];
       int e = ent > 0 ? ent - 1 : -ent - 1;
@@ -162,29 +229,29 @@ __global__ void k_laplace_rows(int nv, int W, const int32_t* __restrict__ ptr, c
       double w = h * star1[e];
       diag += w;
       int k = 0;
-      while (k < cnt && c[k] != j) ++k;
+      while (k < cnt && c(k) != j) ++k;
       if (k < cnt) {
-        v[k] = v[k] + (-w);
+        v(k) = v(k) + (-w);
       } else if (cnt < W - 1) {
-        c[cnt] = j;
-        v[cnt] = 0.0 + (-w);
+        c(cnt) = j;
+        v(cnt) = 0.0 + (-w);
         ++cnt;
       } else {
         atomicExch(overflow, 1);
       }
     }
     if (shift != 0.0) diag = diag + shift;
-    c[cnt] = i;
-    v[cnt] = diag;
+    c(cnt) = i;
+    v(cnt) = diag;
     ++cnt;
     for (int a = 1; a < cnt; ++a)
-      for (int b = a; b > 0 && c[b - 1] > c[b]; --b) {
-        int tc = c[b]; c[b] = c[b - 1]; c[b - 1] = tc;
-        double tv = v[b]; v[b] = v[b - 1]; v[b - 1] = tv;
+      for (int b = a; b > 0 && c(b - 1) > c(b); --b) {
+        int tc = c(b); c(b) = c(b - 1); c(b - 1) = tc;
+        double tv = v(b); v(b) = v(b - 1); v(b - 1) = tv;
       }
     for (int q = cnt; q < W; ++q) {
-      c[q] = -1;
-      v[q] = 0.0;
+      c(q) = -1;
+      v(q) = 0.0;
     }
   }
 }
@@ -215,8 +282,8 @@ __global__ void __launch_bounds__(kResidThreads) k_resid_partials(int n, int W, 
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double s = 0.0;
     for (int q = 0; q < W; ++q) {
-      int c = col[(size_t)i * W + q];
-      if (c >= 0) s += val[(size_t)i * W + q] * xj[c];
+      int c = col[(size_t)q * n + i];
+      if (c >= 0) s += val[(size_t)q * n + i] * xj[c];
     }
     double r = bj[i] - s;
     sr += r * r;
@@ -278,7 +345,7 @@ void hodge_into(const Mesh& m, int k, bool inverse, DArr<double>& out) {
 }
 
 void assemble_laplacian(const Mesh& m, double shift, int& W, DArr<int32_t>& col, DArr<double>& val) {
-  W = (m.max_v2e + 1 + 3) / 4 * 4;  // diagonal + neighbours, padded to a multiple of 4
+  W = m.max_v2e + 1;  // diagonal + neighbours
   col.alloc((size_t)m.nv * W);
   val.alloc((size_t)m.nv * W);
   DArr<int> overflow(1);
@@ -297,6 +364,8 @@ void cast_array(const DArr<double>& a, DArr<T>& b) {
 }
 template void cast_array<float>(const DArr<double>&, DArr<float>&);
 
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 template <class T>
 static void launch_op(const dec_op& op, const void* vx, void* vy, double alpha, double beta, cudaStream_t s) {
   const Mesh& m = *op.m;
@@ -307,10 +376,18 @@ static void launch_op(const dec_op& op, const void* vx, void* vy, double alpha, 
   const int TH = 256;
   switch (op.kind) {
     case DEC_OP_D0:
-      if (m.ne) k_d0<T><<<grid_for(m.ne, TH), TH, 0, s>>>(m.ne, m.ev0.p, m.ev1.p, m.esign.p, x, y, a, b, hb);
+      if (!m.ne) break;
+      if (sizeof(T) == 4 && aligned16(y))  // FP64 measured faster one row per thread
+        k_d0v<T><<<grid_for(m.ne / 4 + 1, TH), TH, 0, s>>>(m.ne, m.ev0.p, m.ev1.p, m.esign.p, x, y, a, b, hb);
+      else
+        k_d0<T><<<grid_for(m.ne, TH), TH, 0, s>>>(m.ne, m.ev0.p, m.ev1.p, m.esign.p, x, y, a, b, hb);
       break;
     case DEC_OP_D1:
-      if (m.nt)
+      if (!m.nt) break;
+      if (aligned16(y))
+        k_d1v<T><<<grid_for(m.nt / 4 + 1, TH), TH, 0, s>>>(m.nt, m.d1c0.p, m.d1c1.p, m.d1c2.p, m.d1neg.p, x, y, a, b,
+                                                            hb);
+      else
         k_d1<T><<<grid_for(m.nt, TH), TH, 0, s>>>(m.nt, m.d1c0.p, m.d1c1.p, m.d1c2.p, m.d1neg.p, x, y, a, b, hb);
       break;
     case DEC_OP_BOUNDARY1:  // ∂1 = d0ᵀ
@@ -325,8 +402,8 @@ static void launch_op(const dec_op& op, const void* vx, void* vy, double alpha, 
     case DEC_OP_LAPLACE0:
     case DEC_OP_HELMHOLTZ0: {
       const T* val = std::is_same<T, double>::value ? (const T*)op.val64.p : (const T*)op.val32.p;
-      if (op.W == 8)
-        k_ell<T, 8><<<grid_for(m.nv, TH), TH, 0, s>>>(m.nv, op.W, op.col.p, val, x, y, a, b, hb);
+      if (op.W == 7)
+        k_ell<T, 7><<<grid_for(m.nv, TH), TH, 0, s>>>(m.nv, op.W, op.col.p, val, x, y, a, b, hb);
       else
         k_ell<T, 0><<<grid_for(m.nv, TH), TH, 0, s>>>(m.nv, op.W, op.col.p, val, x, y, a, b, hb);
       break;
@@ -431,7 +508,7 @@ void op_export_csr_impl(const dec_op* op, int64_t* nnz, int32_t* rowptr, int32_t
       auto v = op->val64.download();
       for (int i = 0; i < m.nv; ++i) {
         for (int q = 0; q < op->W; ++q)
-          if (c[(size_t)i * op->W + q] >= 0) push(c[(size_t)i * op->W + q], v[(size_t)i * op->W + q]);
+          if (c[(size_t)q * m.nv + i] >= 0) push(c[(size_t)q * m.nv + i], v[(size_t)q * m.nv + i]);
         rp[i + 1] = (int32_t)ci.size();
       }
       break;

@@ -155,6 +155,109 @@ __global__ void __launch_bounds__(kThreads) k_w11(int nt, const int32_t* __restr
   }
 }
 
+// FP32 variants with four consecutive outputs per thread: 16-byte loads of the streamed index,
+// coefficient and form arrays and 16-byte stores, the per-output expressions unchanged.  Used
+// when every streamed pointer of every pair is 16-byte aligned; n4 = n / 4 vector groups, the
+// remaining n % 4 outputs by the scalar expression.
+__device__ __forceinline__ void f4(const float4& v, float (&o)[4]) {
+  o[0] = v.x;
+  o[1] = v.y;
+  o[2] = v.z;
+  o[3] = v.w;
+}
+__device__ __forceinline__ void i4(const int4& v, int (&o)[4]) {
+  o[0] = v.x;
+  o[1] = v.y;
+  o[2] = v.z;
+  o[3] = v.w;
+}
+
+__global__ void __launch_bounds__(kThreads) k_w01v(int ne, const int32_t* __restrict__ ev0,
+                                                   const int32_t* __restrict__ ev1, const float* __restrict__ f,
+                                                   const float* __restrict__ a, float* __restrict__ out, size_t sf,
+                                                   size_t sa, size_t so) {
+  f += blockIdx.y * sf;
+  a += blockIdx.y * sa;
+  out += blockIdx.y * so;
+  const float half = 0.5f;
+  const int n4 = ne / 4;
+  for (int g = blockIdx.x * kThreads + threadIdx.x; g < n4; g += gridDim.x * kThreads) {
+    int i0[4], i1[4];
+    float av[4], o[4];
+    i4(__ldcs(reinterpret_cast<const int4*>(ev0) + g), i0);
+    i4(__ldcs(reinterpret_cast<const int4*>(ev1) + g), i1);
+    f4(__ldcs(reinterpret_cast<const float4*>(a) + g), av);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) o[k] = half * av[k] * (__ldg(f + i0[k]) + __ldg(f + i1[k]));
+    __stcs(reinterpret_cast<float4*>(out) + g, make_float4(o[0], o[1], o[2], o[3]));
+  }
+  for (int e = 4 * n4 + blockIdx.x * kThreads + threadIdx.x; e < ne; e += gridDim.x * kThreads)
+    out[e] = half * a[e] * (__ldg(f + ev0[e]) + __ldg(f + ev1[e]));
+}
+
+__global__ void __launch_bounds__(kThreads) k_w02v(int nt, const int32_t* __restrict__ tv0,
+                                                   const int32_t* __restrict__ tv1, const int32_t* __restrict__ tv2,
+                                                   const float* __restrict__ w0, const float* __restrict__ w1,
+                                                   const float* __restrict__ w2, const float* __restrict__ f,
+                                                   const float* __restrict__ a, float* __restrict__ out, size_t sf,
+                                                   size_t sa, size_t so) {
+  f += blockIdx.y * sf;
+  a += blockIdx.y * sa;
+  out += blockIdx.y * so;
+  const int n4 = nt / 4;
+  for (int g = blockIdx.x * kThreads + threadIdx.x; g < n4; g += gridDim.x * kThreads) {
+    int v0[4], v1[4], v2[4];
+    float c0[4], c1[4], c2[4], av[4], o[4];
+    i4(__ldcs(reinterpret_cast<const int4*>(tv0) + g), v0);
+    i4(__ldcs(reinterpret_cast<const int4*>(tv1) + g), v1);
+    i4(__ldcs(reinterpret_cast<const int4*>(tv2) + g), v2);
+    f4(__ldcs(reinterpret_cast<const float4*>(w0) + g), c0);
+    f4(__ldcs(reinterpret_cast<const float4*>(w1) + g), c1);
+    f4(__ldcs(reinterpret_cast<const float4*>(w2) + g), c2);
+    f4(__ldcs(reinterpret_cast<const float4*>(a) + g), av);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      o[k] = av[k] * (c0[k] * __ldg(f + v0[k]) + c1[k] * __ldg(f + v1[k]) + c2[k] * __ldg(f + v2[k]));
+    __stcs(reinterpret_cast<float4*>(out) + g, make_float4(o[0], o[1], o[2], o[3]));
+  }
+  for (int t = 4 * n4 + blockIdx.x * kThreads + threadIdx.x; t < nt; t += gridDim.x * kThreads)
+    out[t] = a[t] * (w0[t] * __ldg(f + tv0[t]) + w1[t] * __ldg(f + tv1[t]) + w2[t] * __ldg(f + tv2[t]));
+}
+
+__global__ void __launch_bounds__(kThreads) k_w11v(int nt, const int32_t* __restrict__ te0,
+                                                   const int32_t* __restrict__ te1, const int32_t* __restrict__ te2,
+                                                   const float* __restrict__ cf0, const float* __restrict__ cf1,
+                                                   const float* __restrict__ cf2, const float* __restrict__ a,
+                                                   const float* __restrict__ b, float* __restrict__ out, size_t sa,
+                                                   size_t sb, size_t so) {
+  a += blockIdx.y * sa;
+  b += blockIdx.y * sb;
+  out += blockIdx.y * so;
+  const int n4 = nt / 4;
+  for (int g = blockIdx.x * kThreads + threadIdx.x; g < n4; g += gridDim.x * kThreads) {
+    int e0[4], e1[4], e2[4];
+    float c0[4], c1[4], c2[4], o[4];
+    i4(__ldcs(reinterpret_cast<const int4*>(te0) + g), e0);
+    i4(__ldcs(reinterpret_cast<const int4*>(te1) + g), e1);
+    i4(__ldcs(reinterpret_cast<const int4*>(te2) + g), e2);
+    f4(__ldcs(reinterpret_cast<const float4*>(cf0) + g), c0);
+    f4(__ldcs(reinterpret_cast<const float4*>(cf1) + g), c1);
+    f4(__ldcs(reinterpret_cast<const float4*>(cf2) + g), c2);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float ae0 = __ldg(a + e0[k]), ae1 = __ldg(a + e1[k]), ae2 = __ldg(a + e2[k]);
+      const float be0 = __ldg(b + e0[k]), be1 = __ldg(b + e1[k]), be2 = __ldg(b + e2[k]);
+      o[k] = (c0[k] * (ae2 * be1 - ae1 * be2) + c1[k] * (ae2 * be0 - ae0 * be2) + c2[k] * (ae1 * be0 - ae0 * be1));
+    }
+    __stcs(reinterpret_cast<float4*>(out) + g, make_float4(o[0], o[1], o[2], o[3]));
+  }
+  for (int t = 4 * n4 + blockIdx.x * kThreads + threadIdx.x; t < nt; t += gridDim.x * kThreads) {
+    const float ae0 = __ldg(a + te0[t]), ae1 = __ldg(a + te1[t]), ae2 = __ldg(a + te2[t]);
+    const float be0 = __ldg(b + te0[t]), be1 = __ldg(b + te1[t]), be2 = __ldg(b + te2[t]);
+    out[t] = (cf0[t] * (ae2 * be1 - ae1 * be2) + cf1[t] * (ae2 * be0 - ae0 * be2) + cf2[t] * (ae1 * be0 - ae0 * be1));
+  }
+}
+
 // (M x) .* y with M a row-major ELL matrix (columns sorted, -1 = padding): the
 // "matrix then elementwise product" form of the pd / dd wedges, FastDEC.jl:317-325, :381-389.
 template <class T, int W>
@@ -328,6 +431,9 @@ static void launch_plan(dec_wedge_plan& P, const CoefSet<T>& c, const void* va, 
   // grid: CTAs are dispatched x-fastest, so a few pairs at a time stream through L2 and each form
   // value shared by neighbouring simplices is read from DRAM once
   auto grid2 = [&](long long n, int per, int cnt) { return dim3(grid_for(n, per), (unsigned)cnt); };
+  auto al16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  // the FP32 vector kernels need every pair's streamed pointers 16-byte aligned
+  const bool vec = sizeof(T) == 4 && al16(va) && al16(vb) && al16(vo) && (count == 1 || (sa % 4 == 0 && sb % 4 == 0 && so % 4 == 0));
   for (int done = 0; done < count;) {
     const int cnt = std::min(count - done, 65535);
     const T* ab = a + (size_t)done * sa;
@@ -339,9 +445,16 @@ static void launch_plan(dec_wedge_plan& P, const CoefSet<T>& c, const void* va, 
         const T* f = P.op == W01 ? ab : bb;
         const T* al = P.op == W01 ? bb : ab;
         const size_t sf = P.op == W01 ? sa : sb, sl = P.op == W01 ? sb : sa;
-        if (m.ne)
-          k_w01<T><<<grid2(m.ne, kThreads * kItems, cnt), kThreads, 0, s>>>(m.ne, m.ev0.p, m.ev1.p, f, al, ob, sf, sl,
-                                                                              so);
+        if (!m.ne) break;
+        if constexpr (sizeof(T) == 4) {
+          if (vec) {
+            k_w01v<<<grid2(m.ne / 4 + 1, kThreads, cnt), kThreads, 0, s>>>(m.ne, m.ev0.p, m.ev1.p, f, al, ob, sf, sl,
+                                                                             so);
+            break;
+          }
+        }
+        k_w01<T><<<grid2(m.ne, kThreads * kItems, cnt), kThreads, 0, s>>>(m.ne, m.ev0.p, m.ev1.p, f, al, ob, sf, sl,
+                                                                            so);
         break;
       }
       case W02:
@@ -349,15 +462,29 @@ static void launch_plan(dec_wedge_plan& P, const CoefSet<T>& c, const void* va, 
         const T* f = P.op == W02 ? ab : bb;
         const T* al = P.op == W02 ? bb : ab;
         const size_t sf = P.op == W02 ? sa : sb, sl = P.op == W02 ? sb : sa;
-        if (m.nt)
-          k_w02<T><<<grid2(m.nt, kThreads * kItems, cnt), kThreads, 0, s>>>(m.nt, m.tv0.p, m.tv1.p, m.tv2.p, c.c[0].p,
-                                                                              c.c[1].p, c.c[2].p, f, al, ob, sf, sl, so);
+        if (!m.nt) break;
+        if constexpr (sizeof(T) == 4) {
+          if (vec) {
+            k_w02v<<<grid2(m.nt / 4 + 1, kThreads, cnt), kThreads, 0, s>>>(m.nt, m.tv0.p, m.tv1.p, m.tv2.p, c.c[0].p,
+                                                                             c.c[1].p, c.c[2].p, f, al, ob, sf, sl, so);
+            break;
+          }
+        }
+        k_w02<T><<<grid2(m.nt, kThreads * kItems, cnt), kThreads, 0, s>>>(m.nt, m.tv0.p, m.tv1.p, m.tv2.p, c.c[0].p,
+                                                                            c.c[1].p, c.c[2].p, f, al, ob, sf, sl, so);
         break;
       }
       case W11:
-        if (m.nt)
-          k_w11<T><<<grid2(m.nt, kThreads * kItems, cnt), kThreads, 0, s>>>(m.nt, m.te0.p, m.te1.p, m.te2.p, c.c[0].p,
-                                                                              c.c[1].p, c.c[2].p, ab, bb, ob, sa, sb, so);
+        if (!m.nt) break;
+        if constexpr (sizeof(T) == 4) {
+          if (vec) {
+            k_w11v<<<grid2(m.nt / 4 + 1, kThreads, cnt), kThreads, 0, s>>>(m.nt, m.te0.p, m.te1.p, m.te2.p, c.c[0].p,
+                                                                             c.c[1].p, c.c[2].p, ab, bb, ob, sa, sb, so);
+            break;
+          }
+        }
+        k_w11<T><<<grid2(m.nt, kThreads * kItems, cnt), kThreads, 0, s>>>(m.nt, m.te0.p, m.te1.p, m.te2.p, c.c[0].p,
+                                                                            c.c[1].p, c.c[2].p, ab, bb, ob, sa, sb, so);
         break;
       default:
         break;
