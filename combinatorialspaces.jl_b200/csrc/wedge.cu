@@ -19,14 +19,15 @@
 
 namespace decb {
 
-enum WedgeOp { W01, W10, W02, W20, W11, WDD01, WDD10, WPD01, WDP10 };
+enum WedgeOp { W01, W10, W02, W20, W11, WDD01, WDD10, WPD01, WDP10, WPD11, WDP11 };
 
 template <class T>
 struct CoefSet {
   DArr<T> c[3];
-  DArr<int32_t> idx;  // ELL indices for the sparse (pd / dd) forms
+  DArr<int32_t> idx;  // ELL indices for the sparse (pd / dd) forms; slot-major for ♭♯
   DArr<T> val;
   int width = 0;
+  DArr<T> tmp;        // pd / dp (1,1): ♭♯ times the dual form, one per batched pair
 };
 
 }  // namespace decb
@@ -44,6 +45,7 @@ namespace decb {
 
 constexpr int kItems = 4;
 constexpr int kThreads = 256;
+constexpr int kFlatSharpWidth = 6;  // ♭♯ row: the edges of the (at most two) incident triangles
 
 // wedge_kernel_01!, FastDEC.jl:159-163: res[e] = ½ α[e] (f[∂v0 e] + f[∂v1 e]).
 template <class T>
@@ -377,21 +379,231 @@ static void cast_into(const DArr<double>& src, DArr<T>& dst) {
   DEC_CHECK_LAUNCH();
 }
 
+// ---- ♭♯ for the primal-dual (1,1) wedges --------------------------------------------------
+// ♭♯_mat = ♭(DPPFlat) * ♯(LLSDDSharp), src/DiscreteExteriorCalculus.jl:687-714, :876-909,
+// :1992.  The dual edges of edge e are its triangle-center -> edge-center dual edges
+// (D_edges12, (k, t) order = the e2t order); the one from triangle t is the last k with
+// ∂e_k(t) = e.  Σ dual lengths per edge:
+__global__ void k_fs_sumlen(int ne, int nt, const int32_t* __restrict__ e2t_ptr, const int32_t* __restrict__ e2t,
+                            const double* __restrict__ dlen, double* __restrict__ sumlen) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+    double sum = 0.0;
+    for (int q = e2t_ptr[e]; q < e2t_ptr[e + 1]; ++q) {
+      const int tk = e2t[q];
+      sum += dlen[(size_t)(tk % 3) * nt + tk / 3];
+    }
+    sumlen[e] = sum;
+  }
+}
+
+__device__ __forceinline__ int fs_slot(int t, int e, const int32_t* te0, const int32_t* te1, const int32_t* te2) {
+  int k = -1;
+  if (te0[t] == e) k = 0;
+  if (te1[t] == e) k = 1;
+  if (te2[t] == e) k = 2;
+  return k;
+}
+
+// ♯ per triangle t: its edges sorted by index, and for edge i the 3-vector w_i pinv(X)[:, i]
+// with X[i] = σ_i (tri center - edge center) over the three dual edges, w_i = dual length /
+// Σ dual lengths of the edge; pinv(X) = B (YᵀY)⁻¹ Yᵀ, B an orthonormal basis of the triangle's
+// plane and Y = X B.
+__global__ void k_fs_sharp(int nt, const int32_t* __restrict__ te0, const int32_t* __restrict__ te1,
+                           const int32_t* __restrict__ te2, const int32_t* __restrict__ tv0,
+                           const int32_t* __restrict__ tv1, const int32_t* __restrict__ tv2,
+                           const int32_t* __restrict__ ev0, const int32_t* __restrict__ ev1,
+                           const int8_t* __restrict__ esign, const int8_t* __restrict__ tsign,
+                           const double* __restrict__ pts, const double* __restrict__ tc,
+                           const double* __restrict__ dlen, const double* __restrict__ sumlen,
+                           int32_t* __restrict__ tedges, double* __restrict__ sharp) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+    int es[3] = {te0[t], te1[t], te2[t]};
+    for (int a = 1; a < 3; ++a)
+      for (int b = a; b > 0 && es[b - 1] > es[b]; --b) {
+        const int x = es[b]; es[b] = es[b - 1]; es[b - 1] = x;
+      }
+    double X[3][3], w[3];
+    const bool to = tsign[t] > 0;
+    for (int i = 0; i < 3; ++i) {
+      const int e = es[i];
+      const int k = fs_slot(t, e, te0, te1, te2);
+      const bool ok = (k % 2 == 1) ? !to : to;
+      const double sg = ((esign[e] > 0) == ok) ? 1.0 : -1.0;
+      for (int c = 0; c < 3; ++c) {
+        const double mid = (pts[3 * (size_t)ev0[e] + c] + pts[3 * (size_t)ev1[e] + c]) / 2;
+        X[i][c] = sg * (tc[3 * (size_t)t + c] - mid);
+      }
+      w[i] = dlen[(size_t)k * nt + t] / sumlen[e];
+      tedges[3 * (size_t)t + i] = e;
+    }
+    const double* q0 = pts + 3 * (size_t)tv0[t];
+    const double* q1 = pts + 3 * (size_t)tv1[t];
+    const double* q2 = pts + 3 * (size_t)tv2[t];
+    double u[3] = {q1[0] - q0[0], q1[1] - q0[1], q1[2] - q0[2]};
+    double v[3] = {q2[0] - q0[0], q2[1] - q0[1], q2[2] - q0[2]};
+    const double nu = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    for (int c = 0; c < 3; ++c) u[c] /= nu;
+    const double uv = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+    for (int c = 0; c < 3; ++c) v[c] -= uv * u[c];
+    const double nvv = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    for (int c = 0; c < 3; ++c) v[c] /= nvv;
+    double Y[3][2];
+    for (int i = 0; i < 3; ++i) {
+      Y[i][0] = X[i][0] * u[0] + X[i][1] * u[1] + X[i][2] * u[2];
+      Y[i][1] = X[i][0] * v[0] + X[i][1] * v[1] + X[i][2] * v[2];
+    }
+    double g00 = 0, g01 = 0, g11 = 0;
+    for (int i = 0; i < 3; ++i) {
+      g00 += Y[i][0] * Y[i][0];
+      g01 += Y[i][0] * Y[i][1];
+      g11 += Y[i][1] * Y[i][1];
+    }
+    const double det = g00 * g11 - g01 * g01;
+    const double i00 = g11 / det, i01 = -g01 / det, i11 = g00 / det;
+    for (int i = 0; i < 3; ++i) {
+      const double c0 = i00 * Y[i][0] + i01 * Y[i][1];
+      const double c1 = i01 * Y[i][0] + i11 * Y[i][1];
+      for (int c = 0; c < 3; ++c) sharp[9 * (size_t)t + 3 * i + c] = w[i] * (c0 * u[c] + c1 * v[c]);
+    }
+  }
+}
+
+// ♭ rows and the product: row e sums, over its incident triangles t (increasing), the entries
+// (e, edge i of t) = (δ_t e⃗ / Σδ) · ♯_t[i], e⃗ = σ_e (p∂v0 - p∂v1), δ_t the dual length of e in t;
+// duplicate columns are added in that order, then the row is sorted by column (slot-major ELL).
+__global__ void k_fs_rows(int ne, int nt, const int32_t* __restrict__ e2t_ptr, const int32_t* __restrict__ e2t,
+                          const int32_t* __restrict__ te0, const int32_t* __restrict__ te1,
+                          const int32_t* __restrict__ te2, const int32_t* __restrict__ ev0,
+                          const int32_t* __restrict__ ev1, const int8_t* __restrict__ esign,
+                          const double* __restrict__ pts, const double* __restrict__ dlen,
+                          const int32_t* __restrict__ tedges, const double* __restrict__ sharp,
+                          int32_t* __restrict__ idx, double* __restrict__ val, int* overflow) {
+  constexpr int W = kFlatSharpWidth;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+    int tris[8];
+    int nts = 0;
+    for (int q = e2t_ptr[e]; q < e2t_ptr[e + 1]; ++q) {
+      const int t = e2t[q] / 3;
+      bool seen = false;
+      for (int j = 0; j < nts; ++j) seen |= tris[j] == t;
+      if (!seen) {
+        if (nts < 8) tris[nts++] = t;
+        else atomicExch(overflow, 1);
+      }
+    }
+    for (int a = 1; a < nts; ++a)
+      for (int b = a; b > 0 && tris[b - 1] > tris[b]; --b) {
+        const int x = tris[b]; tris[b] = tris[b - 1]; tris[b - 1] = x;
+      }
+    const double sg = esign[e] > 0 ? 1.0 : -1.0;
+    double ev[3];
+    for (int c = 0; c < 3; ++c) ev[c] = (pts[3 * (size_t)ev0[e] + c] - pts[3 * (size_t)ev1[e] + c]) * sg;
+    double dels[8], dsum = 0;
+    for (int j = 0; j < nts; ++j) {
+      const int k = fs_slot(tris[j], e, te0, te1, te2);
+      dels[j] = dlen[(size_t)k * nt + tris[j]];
+      dsum += dels[j];
+    }
+    int cols[W];
+    double vals[W];
+    int cnt = 0;
+    for (int j = 0; j < nts; ++j) {
+      const int t = tris[j];
+      double fl[3];
+      for (int c = 0; c < 3; ++c) fl[c] = dels[j] * ev[c] / dsum;
+      for (int i = 0; i < 3; ++i) {
+        const double* sv = sharp + 9 * (size_t)t + 3 * i;
+        const double x = fl[0] * sv[0] + fl[1] * sv[1] + fl[2] * sv[2];
+        const int cc = tedges[3 * (size_t)t + i];
+        int q = 0;
+        while (q < cnt && cols[q] != cc) ++q;
+        if (q < cnt) {
+          vals[q] = vals[q] + x;
+        } else if (cnt < W) {
+          cols[cnt] = cc;
+          vals[cnt] = x;
+          ++cnt;
+        } else {
+          atomicExch(overflow, 1);
+        }
+      }
+    }
+    for (int a = 1; a < cnt; ++a)
+      for (int b = a; b > 0 && cols[b - 1] > cols[b]; --b) {
+        const int tcol = cols[b]; cols[b] = cols[b - 1]; cols[b - 1] = tcol;
+        const double tv = vals[b]; vals[b] = vals[b - 1]; vals[b - 1] = tv;
+      }
+    for (int q = 0; q < W; ++q) {
+      idx[(size_t)q * ne + e] = q < cnt ? cols[q] : -1;
+      val[(size_t)q * ne + e] = q < cnt ? vals[q] : 0.0;
+    }
+  }
+}
+
+// y = ♭♯ x (slot-major ELL of width kFlatSharpWidth), row sums in column order; batched pairs
+// along grid.y.
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_fs_apply(int ne, const int32_t* __restrict__ idx,
+                                                       const T* __restrict__ val, const T* __restrict__ x,
+                                                       T* __restrict__ y, size_t sx, size_t sy) {
+  x += blockIdx.y * sx;
+  y += blockIdx.y * sy;
+  constexpr int W = kFlatSharpWidth;
+  for (int e = blockIdx.x * kThreads + threadIdx.x; e < ne; e += gridDim.x * kThreads) {
+    int c[W];
+    T v[W];
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+      c[q] = __ldcs(idx + (size_t)q * ne + e);
+      v[q] = __ldcs(val + (size_t)q * ne + e);
+    }
+    T s = T(0);
+#pragma unroll
+    for (int q = 0; q < W; ++q)
+      if (c[q] >= 0) s += v[q] * __ldg(x + c[q]);
+    y[e] = s;
+  }
+}
+
 // ---- plan ---------------------------------------------------------------------------------
 
 static void build_plan(dec_wedge_plan& P) {
   Mesh& m = *P.m;
   const int T = 256;
   CoefSet<double>& c = P.c64;
-  if (P.op == W11) {
+  if (P.op == W11 || P.op == WPD11 || P.op == WDP11) {
     for (auto& x : c.c) x.alloc(m.nt);
     if (m.nt)
       k_coef11<<<grid_for(m.nt, T), T>>>(m.nt, m.te0.p, m.te1.p, m.te2.p, m.esign.p, m.tsign.p, m.area.p,
                                          m.dual_area.p, c.c[0].p, c.c[1].p, c.c[2].p);
+  }
+  if (P.op == WPD11 || P.op == WDP11) {
+    c.width = kFlatSharpWidth;
+    c.idx.alloc((size_t)m.ne * c.width);
+    c.val.alloc((size_t)m.ne * c.width);
+    DArr<double> sumlen(m.ne), sharp((size_t)9 * m.nt);
+    DArr<int32_t> tedges((size_t)3 * m.nt);
+    DArr<int> overflow(1);
+    DEC_CUDA(cudaMemset(overflow.p, 0, sizeof(int)));
+    if (m.ne && m.nt) {
+      k_fs_sumlen<<<grid_for(m.ne, T), T>>>(m.ne, m.nt, m.e2t_ptr.p, m.e2t.p, m.dual_len_te.p, sumlen.p);
+      k_fs_sharp<<<grid_for(m.nt, T), T>>>(m.nt, m.te0.p, m.te1.p, m.te2.p, m.tv0.p, m.tv1.p, m.tv2.p, m.ev0.p,
+                                           m.ev1.p, m.esign.p, m.tsign.p, m.pts.p, m.tri_center.p, m.dual_len_te.p,
+                                           sumlen.p, tedges.p, sharp.p);
+      k_fs_rows<<<grid_for(m.ne, T), T>>>(m.ne, m.nt, m.e2t_ptr.p, m.e2t.p, m.te0.p, m.te1.p, m.te2.p, m.ev0.p,
+                                          m.ev1.p, m.esign.p, m.pts.p, m.dual_len_te.p, tedges.p, sharp.p, c.idx.p,
+                                          c.val.p, overflow.p);
+    } else if (m.ne) {
+      DEC_CUDA(cudaMemset(c.idx.p, 0xff, c.idx.bytes()));
+      DEC_CUDA(cudaMemset(c.val.p, 0, c.val.bytes()));
+    }
+    DEC_CHECK_LAUNCH();
+    if (overflow.download()[0])
+      throw Error(DEC_ERR_UNSUPPORTED, "wedge: an edge has more incident triangles than supported (non-manifold mesh)");
   } else if (P.op == W02 || P.op == W20) {
     for (auto& x : c.c) x.alloc(m.nt);
     if (m.nt) k_coef02<<<grid_for(m.nt, T), T>>>(m.nt, m.area.p, m.dual_area.p, c.c[0].p, c.c[1].p, c.c[2].p);
-  } else if (P.op >= WDD01) {
+  } else if (P.op >= WDD01 && P.op <= WDP10) {
     bool pd = (P.op == WPD01 || P.op == WDP10);
     c.width = pd ? 4 : 2;
     c.idx.alloc((size_t)m.ne * c.width);
@@ -489,7 +701,24 @@ static void launch_plan(dec_wedge_plan& P, const CoefSet<T>& c, const void* va, 
       default:
         break;
     }
-    if (P.op >= WDD01) {
+    if (P.op == WPD11 || P.op == WDP11) {
+      // pd(1,1)(f, g) = ∧11(f, ♭♯ g); dp(1,1)(f, g) = ∧11(♭♯ f, g), FastDEC.jl:391-401
+      const bool dual_second = P.op == WPD11;
+      const T* dform = dual_second ? bb : ab;
+      const size_t sd = dual_second ? sb : sa;
+      DArr<T>& tmp = const_cast<CoefSet<T>&>(c).tmp;
+      if (tmp.n < (size_t)cnt * m.ne) tmp.alloc((size_t)cnt * m.ne);
+      if (m.ne)
+        k_fs_apply<T><<<grid2(m.ne, kThreads, cnt), kThreads, 0, s>>>(m.ne, idx, c.val.p, dform, tmp.p, sd,
+                                                                      (size_t)m.ne);
+      const T* fa = dual_second ? ab : tmp.p;
+      const T* fb = dual_second ? tmp.p : bb;
+      const size_t sfa = dual_second ? sa : (size_t)m.ne, sfb = dual_second ? (size_t)m.ne : sb;
+      if (m.nt)
+        k_w11<T><<<grid2(m.nt, kThreads * kItems, cnt), kThreads, 0, s>>>(m.nt, m.te0.p, m.te1.p, m.te2.p, c.c[0].p,
+                                                                            c.c[1].p, c.c[2].p, fa, fb, ob, sfa, sfb,
+                                                                            so);
+    } else if (P.op >= WDD01) {
       // x is the form that M acts on; y is multiplied elementwise:
       //  dd(0,1)(f, g) = (M f) .* g,  pd(0,1)(g, f) = (M g) .* f   -> M acts on the first form
       //  dd(1,0)(f, g) = f .* (M g),  dp(1,0)(f, g) = f .* (M g)   -> M acts on the second form
@@ -533,8 +762,10 @@ dec_wedge_plan* wedge_plan_create_impl(dec_mesh* mh, int kind, int da, int db, d
     else if (da == 1 && db == 0) { op = WDD10; la = ne; lb = nt; lo = ne; }
   } else if (kind == DEC_WEDGE_PD) {
     if (da == 0 && db == 1) { op = WPD01; la = nv; lb = ne; lo = ne; }
+    else if (da == 1 && db == 1) { op = WPD11; la = ne; lb = ne; lo = nt; }
   } else if (kind == DEC_WEDGE_DP) {
     if (da == 1 && db == 0) { op = WDP10; la = ne; lb = nv; lo = ne; }
+    else if (da == 1 && db == 1) { op = WDP11; la = ne; lb = ne; lo = nt; }
   }
   if (op < 0)
     throw Error(DEC_ERR_UNSUPPORTED,

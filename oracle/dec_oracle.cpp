@@ -797,6 +797,62 @@ CSC wedge_pd_01_mat(const Dual& d) {
 // :876-909, :1992.  pinv(X) of the 3x3 matrix of dual-edge vectors (which span the triangle's
 // plane, so X has rank 2 and pinv drops its third singular value) is written as
 // B (YᵀY)⁻¹ Yᵀ with B an orthonormal basis of the plane and Y = X B.
+// ⋆(Val(1), s, GeometricHodge()), DiscreteExteriorCalculus.jl:1680-1731.  Per triangle, with
+// e = (∂e2, ∂e1, ∂e0), ev_i = p∂v0 - p∂v1 of e_i and dv_i = ±(triangle center - edge center)
+// (minus for the middle edge): diagonal entries σ_t crossdot(ev_i, dv_i) / |ev_i|² times the
+// triangle's relative orientation (the sign of its first nonzero one), and off-diagonal
+// entries for the six ordered triples (p1, p2, p3):
+// rel σ_t (ev_p1·dv_p1 / |ev_p1|²) (ev_p1·ev_p3) / crossdot(ev_p2, ev_p3); zero values are
+// skipped and duplicates summed in input order.  crossdot(a, b) = |a × b| · sign((a × b)_z)
+// (+1 when that component is 0), :1667-1670.
+static double crossdot3(const double* a, const double* b) {
+  const double c0 = a[1] * b[2] - a[2] * b[1], c1 = a[2] * b[0] - a[0] * b[2], c2 = a[0] * b[1] - a[1] * b[0];
+  const double nrm = std::sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+  return nrm * (c2 == 0 ? 1.0 : (c2 > 0 ? 1.0 : -1.0));
+}
+
+CSC hodge_geometric1(const Dual& d) {
+  const Mesh& m = d.mesh;
+  std::vector<i32> I, J;
+  std::vector<double> V;
+  auto dot3 = [](const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+  for (int t = 0; t < d.nt; ++t) {
+    const int e[3] = {m.te2[t], m.te1[t], m.te0[t]};
+    double ev[3][3], dv[3][3];
+    const double* tc = &d.dual_point[3 * (size_t)d.tri_center(t)];
+    for (int i = 0; i < 3; ++i) {
+      const double* ec = &d.dual_point[3 * (size_t)d.edge_center(e[i])];
+      for (int k = 0; k < 3; ++k) {
+        ev[i][k] = m.pts[3 * (size_t)m.ev0[e[i]] + k] - m.pts[3 * (size_t)m.ev1[e[i]] + k];
+        dv[i][k] = (tc[k] - ec[k]) * (i == 1 ? -1.0 : 1.0);
+      }
+    }
+    double diag_dot[3];
+    for (int i = 0; i < 3; ++i) diag_dot[i] = dot3(ev[i], dv[i]) / dot3(ev[i], ev[i]);
+    const double st = nsign(m.to[t]);
+    double rel = 0.0;
+    for (int i = 0; i < 3; ++i) {
+      const double dc = st * crossdot3(ev[i], dv[i]) / dot3(ev[i], ev[i]);
+      if (dc != 0.0) {
+        if (rel == 0.0) rel = dc > 0 ? 1.0 : (dc < 0 ? -1.0 : 0.0);
+        I.push_back(e[i]);
+        J.push_back(e[i]);
+        V.push_back(dc * rel);
+      }
+    }
+    static const int perms[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+    for (const auto& p : perms) {
+      const double val = rel * st * diag_dot[p[0]] * dot3(ev[p[0]], ev[p[2]]) / crossdot3(ev[p[1]], ev[p[2]]);
+      if (val != 0.0) {
+        I.push_back(e[p[0]]);
+        J.push_back(e[p[1]]);
+        V.push_back(val);
+      }
+    }
+  }
+  return sparse_coo(d.ne, d.ne, I, J, V);
+}
+
 CSC flat_sharp_mat(const Dual& d) {
   const Mesh& m = d.mesh;
   auto eds = elementary_duals_1(d);

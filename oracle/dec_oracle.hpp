@@ -129,6 +129,8 @@ template <class T> void wedge11(const Dual& d, const Wedge11Cache& c, const T* a
 CSC wedge_dd_01_mat(const Dual& d);
 CSC wedge_pd_01_mat(const Dual& d);
 CSC flat_sharp_mat(const Dual& d);
+// ⋆1 with GeometricHodge (the reference default for 1-forms in 2D), DiscreteExteriorCalculus.jl:1680-1731.
+CSC hodge_geometric1(const Dual& d);
 
 // ---------------------------------------------------------------------------------------
 // Multigrid.jl

@@ -115,7 +115,8 @@ def test_batch_over_uneven_meshes(O, dec):
 
 
 @pytest.mark.parametrize("kind,m,n", [("pp", 0, 1), ("pp", 1, 0), ("pp", 0, 2), ("pp", 2, 0), ("pp", 1, 1),
-                                      ("dd", 0, 1), ("dd", 1, 0), ("pd", 0, 1), ("dp", 1, 0)])
+                                      ("dd", 0, 1), ("dd", 1, 0), ("pd", 0, 1), ("dp", 1, 0), ("pd", 1, 1),
+                                      ("dp", 1, 1)])
 @pytest.mark.parametrize("dtype", ["float64", "float32"])
 def test_batched_wedge_equals_single_applications(dec, kind, m, n, dtype):
     """dec_wedge_apply_batched (one launch, pairs along grid.y) is bit-identical to applying the

@@ -218,6 +218,30 @@ def test_pd_dd_wedges(O, dec, cases, name, dt):
     np.testing.assert_allclose(dd10, fe * (Mdd @ ft), rtol=tol, atol=tol)
 
 
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("dt", ["float64", "float32"])
+def test_pd_dp_11_wedges(O, dec, cases, name, dt):
+    """pd(1,1)(f, g) = ∧11(f, ♭♯ g) and dp(1,1)(f, g) = ∧11(♭♯ f, g) (FastDEC.jl:391-401) with
+    ♭♯ = ♭(DPP) ♯(LLS) built on the GPU: bit-exact with the oracle in FP64."""
+    m, d, g = cases[name]
+    fs = O.flat_sharp_mat(d)
+    npdt = np.float64 if dt == "float64" else np.float32
+    tdt = torch.float64 if dt == "float64" else torch.float32
+    f = uniform(21, d.ne)
+    h = uniform(22, d.ne)
+    ref_pd = O.wedge(d, 11, f, O.csc_matvec(fs, h))
+    ref_dp = O.wedge(d, 11, O.csc_matvec(fs, f), h)
+    pd = dec.dec_wedge_product_pd(1, 1, g, dt)(cuda(f.astype(npdt), tdt), cuda(h.astype(npdt), tdt)).cpu().numpy()
+    dp = dec.dec_wedge_product_dp(1, 1, g, dt)(cuda(f.astype(npdt), tdt), cuda(h.astype(npdt), tdt)).cpu().numpy()
+    if dt == "float64":
+        np.testing.assert_array_equal(pd, ref_pd)
+        np.testing.assert_array_equal(dp, ref_dp)
+    else:
+        for got, ref in ((pd, ref_pd), (dp, ref_dp)):
+            np.testing.assert_allclose(got, ref, rtol=0, atol=2e-5 * max(1.0, np.abs(ref).max()))
+
+
 def test_unsupported_degrees_raise(dec, cases):
     m, d, g = cases["grid_345_bary"]
     with pytest.raises(dec.DecError, match="Unsupported combination"):

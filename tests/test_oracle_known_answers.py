@@ -240,3 +240,42 @@ def test_multigrid_hierarchy_shapes(O):
         assert R.shape == (Ac.shape[0], A.shape[0])
         assert P.shape == (A.shape[0], Ac.shape[0])
         np.testing.assert_allclose(np.asarray(R.sum(axis=1)).ravel(), 1.0, rtol=1e-15)
+
+
+def _primal_const(m, alpha):
+    """eval_constant_primal_form (src/DiscreteExteriorCalculus.jl:2172-2177):
+    α · (p[tgt e] - p[src e]) · sign(e), tgt = ∂v0, src = ∂v1."""
+    p = np.asarray(m.points).reshape(-1, 3)
+    v = (p[np.asarray(m.ev0)] - p[np.asarray(m.ev1)]) @ np.asarray(alpha, float)
+    return v * np.where(np.asarray(m.edge_orientation) > 0, 1.0, -1.0)
+
+
+def _dual_const(O, d, alpha):
+    """eval_constant_dual_form (:2189-2193): hodge_star(1, s) -- the geometric ⋆1, the default
+    for 1-forms in 2D (:1650) -- applied to the primal form of (α₂, -α₁, α₃)."""
+    return csc(O.hodge_geometric1(d)) @ _primal_const(d.mesh, [alpha[1], -alpha[0], alpha[2]])
+
+
+@pytest.mark.parametrize("mesh", ["tri_345", "grid_345"])
+def test_flat_sharp_and_pd_wedges(O, mesh):
+    """test/DiscreteExteriorCalculus.jl:701-745 (flat counter-clockwise meshes, barycentric duals):
+    ♭♯ maps a constant field's dual 1-form to its primal 1-form (up to the orientation sign),
+    and the primal-dual (1,1) wedges are antisymmetric, exactly across pd and dp."""
+    d = O.dualize(getattr(O, mesh)(), O.BARYCENTER)
+    fs = csc(O.flat_sharp_mat(d))
+    X = [3 / math.sqrt(2), 1 / math.sqrt(2), 0.0]
+    Xf = _dual_const(O, d, X)
+    got = fs @ Xf
+    want = _primal_const(d.mesh, X)
+    assert np.allclose(got, want, atol=1e-13) or np.allclose(got, -want, atol=1e-13)
+    pd = lambda f, g: O.wedge(d, 11, f, fs @ g)
+    dp = lambda f, g: O.wedge(d, 11, fs @ f, g)
+    fd, gd = [2.0, 7.0, 0.0], [8.0, 1.0, 0.0]
+    f1, g1 = _primal_const(d.mesh, fd), _primal_const(d.mesh, gd)
+    f2, g2 = _dual_const(O, d, fd), _dual_const(O, d, gd)
+    np.testing.assert_allclose(pd(f1, g2), -pd(g1, f2), rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(dp(f2, g1), -dp(g2, f1), rtol=1e-12, atol=1e-12)
+    np.testing.assert_array_equal(pd(f1, g2), -dp(g2, f1))
+    np.testing.assert_array_equal(dp(f2, g1), -pd(g1, f2))
+    np.testing.assert_allclose(pd(f1, f2), 0, atol=1e-11)
+    np.testing.assert_allclose(pd(g1, g2), 0, atol=1e-11)
