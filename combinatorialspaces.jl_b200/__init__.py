@@ -300,8 +300,16 @@ def _hodge(n, sd, inverse, dtype):
     return out
 
 
-def hodge_operator(n, sd, inverse=False, dtype="float64"):
-    kind = (_capi.DEC_OP_INV_STAR0 if inverse else _capi.DEC_OP_STAR0) + n
+def hodge_operator(n, sd, inverse=False, dtype="float64", hodge="diagonal"):
+    """⋆n (or its inverse) as an operator.  hodge="geometric" with n = 1 is the sparse
+    GeometricHodge ⋆1 (FastDEC.jl:660-716); its inverse is a Krylov solve with -⋆1 (the
+    reference's dec_inv_hodge_star(1, sd, GeometricHodge()))."""
+    if hodge == "geometric" and n == 1:
+        kind = _capi.DEC_OP_INV_STAR1_GEOMETRIC if inverse else _capi.DEC_OP_STAR1_GEOMETRIC
+    elif hodge in ("diagonal", "geometric"):
+        kind = (_capi.DEC_OP_INV_STAR0 if inverse else _capi.DEC_OP_STAR0) + n
+    else:
+        raise ValueError(f"unknown hodge {hodge!r}")
     return Operator(sd, kind, dtype)
 
 

@@ -13,7 +13,7 @@ DEC_BARYCENTER, DEC_CIRCUMCENTER = 0, 1
 DEC_WEDGE_PP, DEC_WEDGE_PD, DEC_WEDGE_DP, DEC_WEDGE_DD = 0, 1, 2, 3
 (DEC_OP_D0, DEC_OP_D1, DEC_OP_BOUNDARY1, DEC_OP_BOUNDARY2, DEC_OP_DUAL_D0, DEC_OP_DUAL_D1,
  DEC_OP_STAR0, DEC_OP_STAR1, DEC_OP_STAR2, DEC_OP_INV_STAR0, DEC_OP_INV_STAR1, DEC_OP_INV_STAR2,
- DEC_OP_LAPLACE0, DEC_OP_HELMHOLTZ0) = range(14)
+ DEC_OP_LAPLACE0, DEC_OP_HELMHOLTZ0, DEC_OP_STAR1_GEOMETRIC, DEC_OP_INV_STAR1_GEOMETRIC) = range(16)
 DEC_GEOM_LENGTH, DEC_GEOM_AREA, DEC_GEOM_DUAL_AREA, DEC_GEOM_DUAL_LENGTH_TE, DEC_GEOM_DUAL_POINT = range(5)
 DEC_SMOOTH_JACOBI, DEC_SMOOTH_CHEBYSHEV, DEC_SMOOTH_CG, DEC_SMOOTH_LEARNED = 0, 1, 2, 3
 DEC_KERNEL_SWEEP, DEC_KERNEL_RESIDUAL, DEC_KERNEL_RESTRICT, DEC_KERNEL_PROLONG, DEC_KERNEL_MLP = range(5)

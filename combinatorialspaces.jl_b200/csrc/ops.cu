@@ -256,6 +256,213 @@ __global__ void k_laplace_rows(int nv, int W, const int32_t* __restrict__ ptr, c
   }
 }
 
+// ---- geometric ⋆1 (FastDEC.jl:660-716) ------------------------------------------------------
+// crossdot(a, b) = |a × b| · sign((a × b)_z), +1 when that component is 0 (DEC.jl:1667-1670).
+__device__ __forceinline__ double crossdot3(const double* a, const double* b) {
+  const double c0 = a[1] * b[2] - a[2] * b[1], c1 = a[2] * b[0] - a[0] * b[2], c2 = a[0] * b[1] - a[1] * b[0];
+  const double nrm = sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+  return nrm * (c2 == 0 ? 1.0 : (c2 > 0 ? 1.0 : -1.0));
+}
+__device__ __forceinline__ double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+// The nine candidate entries of triangle t in the reference's push order: 0..2 the diagonal of
+// its edges (∂e2, ∂e1, ∂e0), 3..8 the six ordered triples; bit k of mask set = entry present.
+__constant__ int kGeoPerm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+
+__global__ void k_geo_tri(int nt, const int32_t* __restrict__ te0, const int32_t* __restrict__ te1,
+                          const int32_t* __restrict__ te2, const int32_t* __restrict__ ev0,
+                          const int32_t* __restrict__ ev1, const double* __restrict__ pts,
+                          const double* __restrict__ tcen, double* __restrict__ coef, uint16_t* __restrict__ mask) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+    const int e[3] = {te2[t], te1[t], te0[t]};
+    double ev[3][3], dv[3][3];
+    for (int i = 0; i < 3; ++i)
+      for (int k = 0; k < 3; ++k) {
+        const double a = pts[3 * (size_t)ev0[e[i]] + k], b = pts[3 * (size_t)ev1[e[i]] + k];
+        ev[i][k] = a - b;
+        dv[i][k] = tcen[3 * (size_t)t + k] - (a + b) / 2;
+      }
+    for (int k = 0; k < 3; ++k) dv[1][k] *= -1;
+    const double cz = ev[0][0] * dv[0][1] - ev[0][1] * dv[0][0];
+    const double rel = cz == 0 ? 1.0 : (cz > 0 ? 1.0 : -1.0);
+    uint16_t mk = 0;
+    for (int i = 0; i < 3; ++i) {
+      const double dc = crossdot3(ev[i], dv[i]);
+      coef[9 * (size_t)t + i] = dc != 0.0 ? rel * dc / dot3(ev[i], ev[i]) : 0.0;
+      if (dc != 0.0) mk |= (uint16_t)(1u << i);
+    }
+    for (int q = 0; q < 6; ++q) {
+      const int p1 = kGeoPerm[q][0], p2 = kGeoPerm[q][1], p3 = kGeoPerm[q][2];
+      const double diag_dot = dot3(ev[p1], dv[p1]) / dot3(ev[p1], ev[p1]);
+      const double val = diag_dot * dot3(ev[p1], ev[p3]);
+      coef[9 * (size_t)t + 3 + q] = val != 0.0 ? rel * val / crossdot3(ev[p2], ev[p3]) : 0.0;
+      if (val != 0.0) mk |= (uint16_t)(1u << (3 + q));
+    }
+    mask[t] = mk;
+  }
+}
+
+// Row e: the present entries (e, c) of its incident triangles in increasing triangle order and
+// push order, duplicates added in that order (the first kept as is), then sorted by column;
+// slot-major ELL of width W, negated when `negate` (the inverse star solves with -⋆1).
+__global__ void k_geo_rows(int ne, int W, const int32_t* __restrict__ e2t_ptr, const int32_t* __restrict__ e2t,
+                           const int32_t* __restrict__ te0, const int32_t* __restrict__ te1,
+                           const int32_t* __restrict__ te2, const double* __restrict__ coef,
+                           const uint16_t* __restrict__ mask, int negate, int32_t* __restrict__ col,
+                           double* __restrict__ val, int* overflow) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+    int tris[8], nts = 0;
+    for (int q = e2t_ptr[e]; q < e2t_ptr[e + 1]; ++q) {
+      const int t = e2t[q] / 3;
+      bool seen = false;
+      for (int j = 0; j < nts; ++j) seen |= tris[j] == t;
+      if (!seen) {
+        if (nts < 8) tris[nts++] = t;
+        else atomicExch(overflow, 1);
+      }
+    }
+    for (int a = 1; a < nts; ++a)
+      for (int b = a; b > 0 && tris[b - 1] > tris[b]; --b) {
+        const int x = tris[b]; tris[b] = tris[b - 1]; tris[b - 1] = x;
+      }
+    int cols[8];
+    double vals[8];
+    int cnt = 0;
+    auto add = [&](int c, double v) {
+      int q = 0;
+      while (q < cnt && cols[q] != c) ++q;
+      if (q < cnt) vals[q] = vals[q] + v;
+      else if (cnt < W && cnt < 8) { cols[cnt] = c; vals[cnt] = v; ++cnt; }
+      else atomicExch(overflow, 1);
+    };
+    for (int j = 0; j < nts; ++j) {
+      const int t = tris[j];
+      const int ed[3] = {te2[t], te1[t], te0[t]};
+      const uint16_t mk = mask[t];
+      for (int i = 0; i < 3; ++i)
+        if ((mk >> i) & 1 && ed[i] == e) add(ed[i], coef[9 * (size_t)t + i]);
+      for (int q = 0; q < 6; ++q)
+        if ((mk >> (3 + q)) & 1 && ed[kGeoPerm[q][0]] == e) add(ed[kGeoPerm[q][1]], coef[9 * (size_t)t + 3 + q]);
+    }
+    for (int a = 1; a < cnt; ++a)
+      for (int b = a; b > 0 && cols[b - 1] > cols[b]; --b) {
+        const int tc = cols[b]; cols[b] = cols[b - 1]; cols[b - 1] = tc;
+        const double tv = vals[b]; vals[b] = vals[b - 1]; vals[b - 1] = tv;
+      }
+    for (int q = 0; q < W; ++q) {
+      col[(size_t)q * ne + e] = q < cnt ? cols[q] : -1;
+      val[(size_t)q * ne + e] = q < cnt ? (negate ? -vals[q] : vals[q]) : 0.0;
+    }
+  }
+}
+
+constexpr int kGeoWidth = 6;  // diagonal + the two other edges of each of two incident triangles
+
+static void assemble_geometric_star1(const Mesh& m, bool negate, int& W, DArr<int32_t>& col, DArr<double>& val) {
+  W = kGeoWidth;
+  col.alloc((size_t)m.ne * W);
+  val.alloc((size_t)m.ne * W);
+  DArr<double> coef((size_t)9 * m.nt);
+  DArr<uint16_t> mask(m.nt);
+  DArr<int> overflow(1);
+  DEC_CUDA(cudaMemset(overflow.p, 0, sizeof(int)));
+  if (m.nt)
+    k_geo_tri<<<grid_for(m.nt, 128), 128>>>(m.nt, m.te0.p, m.te1.p, m.te2.p, m.ev0.p, m.ev1.p, m.pts.p,
+                                             m.tri_center.p, coef.p, mask.p);
+  if (m.ne)
+    k_geo_rows<<<grid_for(m.ne, 128), 128>>>(m.ne, W, m.e2t_ptr.p, m.e2t.p, m.te0.p, m.te1.p, m.te2.p, coef.p,
+                                              mask.p, negate ? 1 : 0, col.p, val.p, overflow.p);
+  DEC_CHECK_LAUNCH();
+  if (overflow.download()[0])
+    throw Error(DEC_ERR_UNSUPPORTED, "geometric hodge: an edge has more incident triangles than supported");
+}
+
+// ---- inverse geometric ⋆1: Jacobi-preconditioned BiCGSTAB on A = -⋆1 (FP64) ----------------
+constexpr int kKryBlocks = 256;
+// partial sums of up to three dot products (a_k · b_k) per block, then a fixed-order finish
+__global__ void __launch_bounds__(256) k_kry_dots(int n, int nd, const double* __restrict__ a0,
+                                                  const double* __restrict__ b0, const double* __restrict__ a1,
+                                                  const double* __restrict__ b1, const double* __restrict__ a2,
+                                                  const double* __restrict__ b2, double* __restrict__ partial) {
+  double s0 = 0, s1 = 0, s2 = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    s0 += a0[i] * b0[i];
+    if (nd > 1) s1 += a1[i] * b1[i];
+    if (nd > 2) s2 += a2[i] * b2[i];
+  }
+  __shared__ double sh[3][256];
+  sh[0][threadIdx.x] = s0;
+  sh[1][threadIdx.x] = s1;
+  sh[2][threadIdx.x] = s2;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) partial[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = sh[threadIdx.x][0];
+}
+
+__global__ void k_kry_finish(int nb, const double* __restrict__ partial, double* __restrict__ out) {
+  const int k = threadIdx.x;
+  if (k < 3) {
+    double s = 0;
+    for (int b = 0; b < nb; ++b) s += partial[(size_t)k * nb + b];
+    out[k] = s;
+  }
+}
+
+// p = r + β (p - ω v); ph = dinv ∘ p
+__global__ void k_kry_p(int n, double beta, double omega, const double* __restrict__ r, const double* __restrict__ v,
+                        const double* __restrict__ dinv, double* __restrict__ p, double* __restrict__ ph) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double pi = r[i] + beta * (p[i] - omega * v[i]);
+    p[i] = pi;
+    ph[i] = dinv[i] * pi;
+  }
+}
+// s = r - α v; x += α ph; sh = dinv ∘ s
+__global__ void k_kry_s(int n, double alpha, const double* __restrict__ r, const double* __restrict__ v,
+                        const double* __restrict__ ph, const double* __restrict__ dinv, double* __restrict__ s,
+                        double* __restrict__ x, double* __restrict__ shat) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double si = r[i] - alpha * v[i];
+    s[i] = si;
+    x[i] += alpha * ph[i];
+    shat[i] = dinv[i] * si;
+  }
+}
+// x += ω sh; r = s - ω t
+__global__ void k_kry_x(int n, double omega, const double* __restrict__ s, const double* __restrict__ t,
+                        const double* __restrict__ shat, double* __restrict__ x, double* __restrict__ r) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] += omega * shat[i];
+    r[i] = s[i] - omega * t[i];
+  }
+}
+__global__ void k_kry_sub(int n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = a[i] - b[i];
+}
+__global__ void k_ell_diag_inv(int n, int W, const int32_t* __restrict__ col, const double* __restrict__ val,
+                               double* __restrict__ dinv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double d = 0.0;
+    for (int q = 0; q < W; ++q)
+      if (col[(size_t)q * n + i] == i) d += val[(size_t)q * n + i];
+    dinv[i] = d != 0.0 ? 1.0 / d : 1.0;
+  }
+}
+template <class S, class T>
+__global__ void k_conv(size_t n, const S* __restrict__ a, T* __restrict__ b) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = (T)a[i];
+}
+template <class T>
+__global__ void k_epi(size_t n, const double* __restrict__ s, T* __restrict__ y, double alpha, double beta, int hb) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    y[i] = hb ? (T)(alpha * s[i] + beta * (double)y[i]) : (T)(alpha * s[i]);
+}
+
 template <class T>
 __global__ void k_cast_op(size_t n, const double* __restrict__ a, T* __restrict__ b) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -367,6 +574,97 @@ template void cast_array<float>(const DArr<double>&, DArr<float>&);
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
 template <class T>
+static void launch_ell(int n, int W, const int32_t* col, const T* val, const T* x, T* y, T a, T b, bool hb,
+                       cudaStream_t s) {
+  if (W == 7) k_ell<T, 7><<<grid_for(n, kOpThreads), kOpThreads, 0, s>>>(n, W, col, val, x, y, a, b, hb);
+  else if (W == 6) k_ell<T, 6><<<grid_for(n, kOpThreads), kOpThreads, 0, s>>>(n, W, col, val, x, y, a, b, hb);
+  else k_ell<T, 0><<<grid_for(n, kOpThreads), kOpThreads, 0, s>>>(n, W, col, val, x, y, a, b, hb);
+}
+
+// y = alpha (-⋆1)⁻¹ x + beta y: BiCGSTAB with the Jacobi preconditioner on A = -⋆1 (stored),
+// FP64, from x0 = 0 to ||b - A x|| <= 1e-14 ||b|| (or 1e-12 once it stagnates).
+static void inverse_geometric_star(dec_op& op, const void* vx, void* vy, double alpha, double beta, cudaStream_t s) {
+  const int n = (int)op.rows;
+  if (n == 0) return;
+  const size_t N = (size_t)n;
+  if (op.kry.n < 10 * N + 4 * kKryBlocks) op.kry.alloc(10 * N + 4 * kKryBlocks);
+  double* b = op.kry.p;
+  double* x = b + N;
+  double* r = x + N;
+  double* rh = r + N;
+  double* p = rh + N;
+  double* v = p + N;
+  double* ph = v + N;
+  double* sv = ph + N;
+  double* t = sv + N;
+  double* dinv = t + N;
+  double* partial = dinv + N;
+  double* dres = partial + 3 * kKryBlocks;
+  const unsigned g = grid_for(n, 256);
+  if (op.dtype == DEC_F64) DEC_CUDA(cudaMemcpyAsync(b, vx, N * 8, cudaMemcpyDeviceToDevice, s));
+  else k_conv<float, double><<<g, 256, 0, s>>>(N, (const float*)vx, b);
+  k_ell_diag_inv<<<g, 256, 0, s>>>(n, op.W, op.col.p, op.val64.p, dinv);
+  DEC_CUDA(cudaMemsetAsync(x, 0, N * 8, s));
+  DEC_CUDA(cudaMemcpyAsync(r, b, N * 8, cudaMemcpyDeviceToDevice, s));
+  DEC_CUDA(cudaMemcpyAsync(rh, b, N * 8, cudaMemcpyDeviceToDevice, s));
+  DEC_CUDA(cudaMemsetAsync(p, 0, N * 8, s));
+  DEC_CUDA(cudaMemsetAsync(v, 0, N * 8, s));
+  double h[3];
+  auto dots = [&](int nd, const double* a0, const double* b0, const double* a1, const double* b1, const double* a2,
+                  const double* b2) {
+    k_kry_dots<<<kKryBlocks, 256, 0, s>>>(n, nd, a0, b0, a1, b1, a2, b2, partial);
+    k_kry_finish<<<1, 32, 0, s>>>(kKryBlocks, partial, dres);
+    DEC_CHECK_LAUNCH();
+    DEC_CUDA(cudaMemcpyAsync(h, dres, sizeof(h), cudaMemcpyDeviceToHost, s));
+    DEC_CUDA(cudaStreamSynchronize(s));
+  };
+  dots(1, b, b, nullptr, nullptr, nullptr, nullptr);
+  const double bnorm = std::sqrt(h[0]);
+  double rho_old = 1, alpha_k = 1, omega = 1, best = HUGE_VAL;
+  int stall = 0;
+  bool done = bnorm == 0.0;
+  for (int it = 0; it < 1000 && !done; ++it) {
+    dots(1, rh, r, nullptr, nullptr, nullptr, nullptr);
+    const double rho = h[0];
+    if (rho == 0.0) break;
+    const double beta_k = (rho / rho_old) * (alpha_k / omega);
+    k_kry_p<<<g, 256, 0, s>>>(n, beta_k, omega, r, v, dinv, p, ph);
+    launch_ell<double>(n, op.W, op.col.p, op.val64.p, ph, v, 1.0, 0.0, false, s);
+    dots(1, rh, v, nullptr, nullptr, nullptr, nullptr);
+    if (h[0] == 0.0) break;
+    alpha_k = rho / h[0];
+    k_kry_s<<<g, 256, 0, s>>>(n, alpha_k, r, v, ph, dinv, sv, x, ph);  // ph now holds dinv ∘ s
+    dots(1, sv, sv, nullptr, nullptr, nullptr, nullptr);
+    if (std::sqrt(h[0]) <= 1e-14 * bnorm) break;
+    launch_ell<double>(n, op.W, op.col.p, op.val64.p, ph, t, 1.0, 0.0, false, s);
+    dots(2, t, sv, t, t, nullptr, nullptr);
+    if (h[1] == 0.0) break;
+    omega = h[0] / h[1];
+    k_kry_x<<<g, 256, 0, s>>>(n, omega, sv, t, ph, x, r);
+    dots(1, r, r, nullptr, nullptr, nullptr, nullptr);
+    const double rn = std::sqrt(h[0]);
+    if (rn <= 1e-14 * bnorm) break;
+    if (rn < 0.5 * best) {
+      best = rn;
+      stall = 0;
+    } else if (++stall > 20 && rn <= 1e-12 * bnorm) {
+      break;
+    }
+    rho_old = rho;
+    if (omega == 0.0) break;
+  }
+  // final check on the true residual
+  launch_ell<double>(n, op.W, op.col.p, op.val64.p, x, t, 1.0, 0.0, false, s);
+  k_kry_sub<<<g, 256, 0, s>>>(n, b, t, r);
+  dots(1, r, r, nullptr, nullptr, nullptr, nullptr);
+  if (!(std::sqrt(h[0]) <= 1e-10 * std::max(bnorm, 1e-300)) && bnorm != 0.0)
+    throw Error(DEC_ERR_NOT_CONVERGED, "inverse geometric hodge: the Krylov solve did not converge");
+  if (op.dtype == DEC_F64) k_epi<double><<<g, 256, 0, s>>>(N, x, (double*)vy, alpha, beta, beta != 0.0);
+  else k_epi<float><<<g, 256, 0, s>>>(N, x, (float*)vy, alpha, beta, beta != 0.0);
+  DEC_CHECK_LAUNCH();
+}
+
+template <class T>
 static void launch_op(const dec_op& op, const void* vx, void* vy, double alpha, double beta, cudaStream_t s) {
   const Mesh& m = *op.m;
   const T* x = (const T*)vx;
@@ -400,14 +698,15 @@ static void launch_op(const dec_op& op, const void* vx, void* vy, double alpha, 
       if (m.ne) k_signed_rows<T><<<grid_for(m.ne, TH), TH, 0, s>>>(m.ne, m.e2ts_ptr.p, m.e2ts.p, x, y, false, a, b, hb);
       break;
     case DEC_OP_LAPLACE0:
-    case DEC_OP_HELMHOLTZ0: {
+    case DEC_OP_HELMHOLTZ0:
+    case DEC_OP_STAR1_GEOMETRIC: {
       const T* val = std::is_same<T, double>::value ? (const T*)op.val64.p : (const T*)op.val32.p;
-      if (op.W == 7)
-        k_ell<T, 7><<<grid_for(m.nv, TH), TH, 0, s>>>(m.nv, op.W, op.col.p, val, x, y, a, b, hb);
-      else
-        k_ell<T, 0><<<grid_for(m.nv, TH), TH, 0, s>>>(m.nv, op.W, op.col.p, val, x, y, a, b, hb);
+      if (op.rows) launch_ell<T>((int)op.rows, op.W, op.col.p, val, x, y, a, b, hb, s);
       break;
     }
+    case DEC_OP_INV_STAR1_GEOMETRIC:
+      inverse_geometric_star(const_cast<dec_op&>(op), vx, vy, alpha, beta, s);
+      break;
     default: {  // diagonal stars
       const T* d = std::is_same<T, double>::value ? (const T*)op.diag64.p : (const T*)op.diag32.p;
       int n = (int)op.rows;
@@ -425,7 +724,7 @@ using namespace decb;
 dec_op* op_create_impl(dec_mesh* mh, int kind, double shift, dec_dtype dt) {
   require(mh != nullptr, "op: null mesh");
   require(dt == DEC_F64 || dt == DEC_F32, "op: dtype must be DEC_F64 or DEC_F32");
-  require(kind >= DEC_OP_D0 && kind <= DEC_OP_HELMHOLTZ0, "op: unknown operator kind");
+  require(kind >= DEC_OP_D0 && kind <= DEC_OP_INV_STAR1_GEOMETRIC, "op: unknown operator kind");
   Mesh& m = mh->m;
   auto* op = new dec_op();
   op->m = &m;
@@ -439,7 +738,8 @@ dec_op* op_create_impl(dec_mesh* mh, int kind, double shift, dec_dtype dt) {
       case DEC_OP_BOUNDARY1: case DEC_OP_DUAL_D1: op->rows = m.nv; op->cols = m.ne; break;
       case DEC_OP_BOUNDARY2: case DEC_OP_DUAL_D0: op->rows = m.ne; op->cols = m.nt; break;
       case DEC_OP_STAR0: case DEC_OP_INV_STAR0: op->rows = op->cols = m.nv; break;
-      case DEC_OP_STAR1: case DEC_OP_INV_STAR1: op->rows = op->cols = m.ne; break;
+      case DEC_OP_STAR1: case DEC_OP_INV_STAR1: case DEC_OP_STAR1_GEOMETRIC: case DEC_OP_INV_STAR1_GEOMETRIC:
+        op->rows = op->cols = m.ne; break;
       case DEC_OP_STAR2: case DEC_OP_INV_STAR2: op->rows = op->cols = m.nt; break;
       default: op->rows = op->cols = m.nv; break;
     }
@@ -450,6 +750,9 @@ dec_op* op_create_impl(dec_mesh* mh, int kind, double shift, dec_dtype dt) {
     } else if (kind == DEC_OP_LAPLACE0 || kind == DEC_OP_HELMHOLTZ0) {
       assemble_laplacian(m, op->shift, op->W, op->col, op->val64);
       if (dt == DEC_F32) cast_array(op->val64, op->val32);
+    } else if (kind == DEC_OP_STAR1_GEOMETRIC || kind == DEC_OP_INV_STAR1_GEOMETRIC) {
+      assemble_geometric_star1(m, kind == DEC_OP_INV_STAR1_GEOMETRIC, op->W, op->col, op->val64);
+      if (dt == DEC_F32 && kind == DEC_OP_STAR1_GEOMETRIC) cast_array(op->val64, op->val32);
     }
     DEC_CUDA(cudaDeviceSynchronize());
   } catch (...) {
@@ -503,16 +806,19 @@ void op_export_csr_impl(const dec_op* op, int64_t* nnz, int32_t* rowptr, int32_t
       }
       break;
     }
-    case DEC_OP_LAPLACE0: case DEC_OP_HELMHOLTZ0: {
+    case DEC_OP_LAPLACE0: case DEC_OP_HELMHOLTZ0: case DEC_OP_STAR1_GEOMETRIC: {
       auto c = op->col.download();
       auto v = op->val64.download();
-      for (int i = 0; i < m.nv; ++i) {
+      const size_t n = (size_t)op->rows;
+      for (size_t i = 0; i < n; ++i) {
         for (int q = 0; q < op->W; ++q)
-          if (c[(size_t)q * m.nv + i] >= 0) push(c[(size_t)q * m.nv + i], v[(size_t)q * m.nv + i]);
+          if (c[(size_t)q * n + i] >= 0) push(c[(size_t)q * n + i], v[(size_t)q * n + i]);
         rp[i + 1] = (int32_t)ci.size();
       }
       break;
     }
+    case DEC_OP_INV_STAR1_GEOMETRIC:
+      throw Error(DEC_ERR_UNSUPPORTED, "op: the inverse geometric hodge star is a solve, not a stored matrix");
     default: {
       auto d = op->diag64.download();
       for (int64_t i = 0; i < op->rows; ++i) {

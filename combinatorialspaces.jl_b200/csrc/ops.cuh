@@ -10,10 +10,11 @@ struct dec_op {
   int64_t rows = 0, cols = 0;
   decb::DArr<double> diag64;  // diagonal operators
   decb::DArr<float> diag32;
-  int W = 0;                  // ELL width (Laplacian / Helmholtz)
+  int W = 0;                  // slot-major ELL width (Laplacian / Helmholtz / geometric ⋆1)
   decb::DArr<int32_t> col;
   decb::DArr<double> val64;
   decb::DArr<float> val32;
+  decb::DArr<double> kry;     // inverse geometric ⋆1: Krylov vectors, 1/diag and reduction scratch
 };
 
 namespace decb {

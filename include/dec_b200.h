@@ -118,7 +118,13 @@ typedef enum dec_op_kind {
   DEC_OP_STAR0 = 6, DEC_OP_STAR1 = 7, DEC_OP_STAR2 = 8,            /* FastDEC.jl:580-604 */
   DEC_OP_INV_STAR0 = 9, DEC_OP_INV_STAR1 = 10, DEC_OP_INV_STAR2 = 11, /* FastDEC.jl:732-737 */
   DEC_OP_LAPLACE0 = 12,   /* ⋆0⁻¹ d0ᵀ ⋆1 d0 (positive semidefinite, = -Δ(0)) */
-  DEC_OP_HELMHOLTZ0 = 13  /* ⋆0⁻¹ d0ᵀ ⋆1 d0 + shift * I */
+  DEC_OP_HELMHOLTZ0 = 13, /* ⋆0⁻¹ d0ᵀ ⋆1 d0 + shift * I */
+  DEC_OP_STAR1_GEOMETRIC = 14,     /* dec_hodge_star(1, sd, GeometricHodge()), FastDEC.jl:660-716 (sparse
+                                      ne x ne; the diagonal ⋆1 on planar circumcentric duals) */
+  DEC_OP_INV_STAR1_GEOMETRIC = 15  /* dec_inv_hodge_star(1, sd, GeometricHodge()), FastDEC.jl:745-748,
+                                      CUDA ext :93-96: y = (-⋆1)⁻¹ x by a Jacobi-preconditioned
+                                      BiCGSTAB solve in FP64 to 1e-14 relative residual (one host
+                                      read-back per reduction; not capturable in a CUDA graph) */
 } dec_op_kind;
 dec_status dec_op_create(dec_mesh* m, int32_t kind, double shift, dec_dtype dtype, dec_op** out);
 dec_status dec_op_shape(const dec_op* op, int64_t* rows, int64_t* cols);

@@ -853,6 +853,52 @@ CSC hodge_geometric1(const Dual& d) {
   return sparse_coo(d.ne, d.ne, I, J, V);
 }
 
+// FastDEC.jl:660-716.  Per triangle, edges (∂e2, ∂e1, ∂e0); ev_i = p∂v0 - p∂v1, dv_i = triangle
+// center - edge center with dv_2 negated; rel = sign of (ev_1 × dv_1)_z (1 when 0).  Entries in
+// this order: diagonal rel crossdot(ev_i, dv_i) / |ev_i|² where crossdot ≠ 0, then for the six
+// triples (p1, p2, p3) where val = (ev_p1·dv_p1 / |ev_p1|²) (ev_p1·ev_p3) ≠ 0 the entry
+// (e_p1, e_p2) = rel val / crossdot(ev_p2, ev_p3); duplicates summed in input order.
+CSC hodge_geometric1_fast(const Dual& d) {
+  const Mesh& m = d.mesh;
+  std::vector<i32> I, J;
+  std::vector<double> V;
+  auto dot3 = [](const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+  for (int t = 0; t < d.nt; ++t) {
+    const int e[3] = {m.te2[t], m.te1[t], m.te0[t]};
+    double ev[3][3], dv[3][3];
+    const double* tc = &d.dual_point[3 * (size_t)d.tri_center(t)];
+    for (int i = 0; i < 3; ++i) {
+      const double* ec = &d.dual_point[3 * (size_t)d.edge_center(e[i])];
+      for (int k = 0; k < 3; ++k) {
+        ev[i][k] = d.dual_point[3 * (size_t)m.ev0[e[i]] + k] - d.dual_point[3 * (size_t)m.ev1[e[i]] + k];
+        dv[i][k] = tc[k] - ec[k];
+      }
+    }
+    for (int k = 0; k < 3; ++k) dv[1][k] *= -1;
+    const double cz = ev[0][0] * dv[0][1] - ev[0][1] * dv[0][0];
+    const double rel = cz == 0 ? 1.0 : (cz > 0 ? 1.0 : -1.0);
+    for (int i = 0; i < 3; ++i) {
+      const double dc = crossdot3(ev[i], dv[i]);
+      if (dc != 0.0) {
+        I.push_back(e[i]);
+        J.push_back(e[i]);
+        V.push_back(rel * dc / dot3(ev[i], ev[i]));
+      }
+    }
+    static const int perms[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+    for (const auto& p : perms) {
+      const double diag_dot = dot3(ev[p[0]], dv[p[0]]) / dot3(ev[p[0]], ev[p[0]]);
+      const double val = diag_dot * dot3(ev[p[0]], ev[p[2]]);
+      if (val != 0.0) {
+        I.push_back(e[p[0]]);
+        J.push_back(e[p[1]]);
+        V.push_back(rel * val / crossdot3(ev[p[1]], ev[p[2]]));
+      }
+    }
+  }
+  return sparse_coo(d.ne, d.ne, I, J, V);
+}
+
 CSC flat_sharp_mat(const Dual& d) {
   const Mesh& m = d.mesh;
   auto eds = elementary_duals_1(d);

@@ -131,6 +131,8 @@ CSC wedge_pd_01_mat(const Dual& d);
 CSC flat_sharp_mat(const Dual& d);
 // ⋆1 with GeometricHodge (the reference default for 1-forms in 2D), DiscreteExteriorCalculus.jl:1680-1731.
 CSC hodge_geometric1(const Dual& d);
+// FastDEC's dec_hodge_star(Val(1), sd, GeometricHodge()), FastDEC.jl:660-716 (the GPU's formulation).
+CSC hodge_geometric1_fast(const Dual& d);
 
 // ---------------------------------------------------------------------------------------
 // Multigrid.jl

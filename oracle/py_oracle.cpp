@@ -162,6 +162,7 @@ PYBIND11_MODULE(dec_oracle, mod) {
   mod.def("wedge_pd_01_mat", [](const Dual& d) { return csc_tuple(wedge_pd_01_mat(d)); });
   mod.def("flat_sharp_mat", [](const Dual& d) { return csc_tuple(flat_sharp_mat(d)); });
   mod.def("hodge_geometric1", [](const Dual& d) { return csc_tuple(hodge_geometric1(d)); });
+  mod.def("hodge_geometric1_fast", [](const Dual& d) { return csc_tuple(hodge_geometric1_fast(d)); });
   mod.def("wedge02_cache", [](const Dual& d) {
     auto c = wedge02_cache(d);
     return py::make_tuple(to_np(c.verts), to_np(c.coeffs));

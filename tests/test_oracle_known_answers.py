@@ -279,3 +279,24 @@ def test_flat_sharp_and_pd_wedges(O, mesh):
     np.testing.assert_array_equal(dp(f2, g1), -pd(g1, f2))
     np.testing.assert_allclose(pd(f1, f2), 0, atol=1e-11)
     np.testing.assert_allclose(pd(g1, g2), 0, atol=1e-11)
+
+
+@pytest.mark.parametrize("mesh,center", [("tri_345", "BARYCENTER"), ("grid_345", "BARYCENTER"),
+                                         ("grid", "BARYCENTER"), ("grid", "CIRCUMCENTER"), ("ico", "CIRCUMCENTER")])
+def test_geometric_hodge_fast_matches_dec(O, mesh, center):
+    """test/Operators.jl:184-197: FastDEC's geometric ⋆1 equals the DEC one to 1e-12 (the
+    reference compares them with rtol / atol 1e-12).  On planar circumcentric duals it is the
+    diagonal ⋆1; on a curved surface its z-axis orientation trick (crossdot,
+    DiscreteExteriorCalculus.jl:1667-1670) flips some entries, so that check is planar only."""
+    if mesh == "grid":
+        m = O.triangulated_grid(10, 7, 1.3, 0.9, True)
+    elif mesh == "ico":
+        m = O.refine_binary(O.refine_binary(O.icosahedron(), 1.0), 1.0)
+    else:
+        m = getattr(O, mesh)()
+    d = O.dualize(m, getattr(O, center))
+    fast = csc(O.hodge_geometric1_fast(d)).toarray()
+    dec = csc(O.hodge_geometric1(d)).toarray()
+    np.testing.assert_allclose(fast, dec, rtol=1e-12, atol=1e-12)
+    if center == "CIRCUMCENTER" and mesh == "grid":
+        np.testing.assert_allclose(fast, np.diag(O.hodge_diag(d, 1)), rtol=1e-12, atol=1e-12)
