@@ -633,6 +633,51 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_op(args):
+    """One DEC operator kernel alone on icosphere L`mesh_level` (circumcentric duals), `steps`
+    back-to-back applications after `warmup`, FP64 or FP32 (--dtype): the entry point for ncu
+    captures of the operator kernels."""
+    import torch
+    dec = load_package()
+    m = dec.meshes.icosphere(args.mesh_level)
+    g = dec.Mesh(m.points, m.ev0, m.ev1, m.te0, m.te1, m.te2, m.edge_orientation, m.tri_orientation,
+                 center="circumcenter")
+    tdt = torch.float64 if args.dtype == "float64" else torch.float32
+    f = torch.rand(g.nv, dtype=tdt, device="cuda")
+    a = torch.rand(g.ne, dtype=tdt, device="cuda")
+    b = torch.rand(g.ne, dtype=tdt, device="cuda")
+    t = torch.rand(g.nt, dtype=tdt, device="cuda")
+    ops = {
+        "laplacian": (dec.laplace_beltrami(g, args.dtype), f),
+        "d0": (dec.dec_differential(0, g, args.dtype), f),
+        "d1": (dec.dec_differential(1, g, args.dtype), a),
+        "star1_geometric": (dec.hodge_operator(1, g, dtype=args.dtype, hodge="geometric"), a),
+    }
+    wedges = {"wedge01": (dec.dec_wedge_product(0, 1, g, args.dtype), f, a),
+              "wedge11": (dec.dec_wedge_product(1, 1, g, args.dtype), a, b),
+              "wedge02": (dec.dec_wedge_product(0, 2, g, args.dtype), f, t)}
+    if args.op in ops:
+        op, x = ops[args.op]
+        y = torch.empty(op.shape[0], dtype=tdt, device="cuda")
+        fn = lambda: op.apply(x, y)
+    else:
+        w, x1, x2 = wedges[args.op]
+        y = torch.empty(w.len_out, dtype=tdt, device="cuda")
+        fn = lambda: w(x1, x2, y)
+    for _ in range(args.warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"op": args.op, "dtype": args.dtype, "mesh_level": args.mesh_level, "nv": g.nv, "ne": g.ne,
+                      "nt": g.nt, "us_per_launch": 1e3 * e0.elapsed_time(e1) / args.steps}), flush=True)
+
+
 def run_kernel(args):
     """One V-cycle kernel alone (dec_mg_time_kernel) on icosphere L`mesh_level` with NRHS
     right-hand sides: the entry point for ncu captures of a single kernel."""
@@ -675,11 +720,16 @@ def main():
     ap.add_argument("--kernel", choices=["sweep", "residual", "restrict", "prolong", "mlp"],
                     help="time one V-cycle kernel alone (steps launches after warmup) and exit")
     ap.add_argument("--mesh-level", type=int, default=LEVEL, dest="mesh_level")
+    ap.add_argument("--op", choices=["laplacian", "d0", "d1", "star1_geometric", "wedge01", "wedge11", "wedge02"],
+                    help="time one DEC operator kernel alone (steps launches after warmup) and exit")
+    ap.add_argument("--dtype", default="float64", choices=["float64", "float32"])
     ap.add_argument("--no-batch", action="store_true", dest="no_batch", help="skip the batched-workload section")
     ap.add_argument("--train-steps", type=int, default=20000, dest="train_steps",
                     help="Adam steps of the learned smoother (0 skips the learned-smoother section)")
     args = ap.parse_args()
-    if args.kernel:
+    if args.op:
+        run_op(args)
+    elif args.kernel:
         run_kernel(args)
     elif args.impl == "reference":
         run_reference(args)
