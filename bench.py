@@ -710,7 +710,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--sweeps", type=int, default=3)
-    ap.add_argument("--inner-cycles", type=int, default=2, dest="inner_cycles")
+    ap.add_argument("--inner-cycles", type=int, default=3, dest="inner_cycles")
     ap.add_argument("--coarse-max", type=int, default=170, dest="coarse_max")
     ap.add_argument("--rhs-block", type=int, default=0, dest="rhs_block")
     ap.add_argument("--no-cpu", action="store_true")

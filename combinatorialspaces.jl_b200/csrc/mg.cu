@@ -28,6 +28,8 @@
 #include <memory>
 #include <numeric>
 
+#include <cuda_fp16.h>
+
 #include "mg.cuh"
 #include "mlp.cuh"
 
@@ -247,30 +249,75 @@ static void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStre
   DEC_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
 }
 
+// Storage type T of the panel vectors and the type C the kernels compute in: FP16 storage
+// (precision 2) computes in FP32.
+template <class T> struct Cmp { using t = T; };
+template <> struct Cmp<__half> { using t = float; };
+template <class T> using CT = typename Cmp<T>::t;
+
 template <class T, int V> struct VecT;
 template <> struct VecT<float, 1> { using t = float; };
 template <> struct VecT<float, 2> { using t = float2; };
 template <> struct VecT<float, 4> { using t = float4; };
 template <> struct VecT<double, 1> { using t = double; };
 template <> struct VecT<double, 2> { using t = double2; };
+template <> struct VecT<__half, 1> { using t = unsigned short; };
+template <> struct VecT<__half, 2> { using t = unsigned; };
+template <> struct VecT<__half, 4> { using t = uint2; };
+template <> struct VecT<__half, 8> { using t = uint4; };
 
-template <class T, int V>
-__device__ __forceinline__ void ldv(const T* p, T (&r)[V]) {
-  using VT = typename VecT<T, V>::t;
+// V consecutive values of storage type S as one vector load, converted to the compute type C.
+template <class S, int V, class C>
+__device__ __forceinline__ void ldv(const S* p, C (&r)[V]) {
+  if constexpr (!std::is_same<S, __half>::value && sizeof(S) * V > 16) {  // several 16-byte loads
+    constexpr int H = 16 / sizeof(S);
+    static_assert(V % H == 0, "vector width");
+#pragma unroll
+    for (int c = 0; c < V / H; ++c) {
+      S t[H];
+      ldv<S, H>(p + c * H, t);
+#pragma unroll
+      for (int k = 0; k < H; ++k) r[c * H + k] = t[k];
+    }
+    return;
+  } else {
+  using VT = typename VecT<S, V>::t;
   VT t = *reinterpret_cast<const VT*>(p);
-  memcpy(r, &t, sizeof(VT));
+  if constexpr (std::is_same<S, __half>::value) {
+    __half h[V];
+    memcpy(h, &t, sizeof(VT));
+#pragma unroll
+    for (int q = 0; q < V; ++q) r[q] = __half2float(h[q]);
+  } else {
+    memcpy(r, &t, sizeof(VT));
+  }
+  }
 }
-template <class T, int V>
-__device__ __forceinline__ void stv(T* p, const T (&r)[V]) {
-  using VT = typename VecT<T, V>::t;
+template <class S, int V, class C>
+__device__ __forceinline__ void stv(S* p, const C (&r)[V]) {
+  using VT = typename VecT<S, V>::t;
   VT t;
-  memcpy(&t, r, sizeof(VT));
+  if constexpr (std::is_same<S, __half>::value) {
+    __half h[V];
+#pragma unroll
+    for (int q = 0; q < V; ++q) h[q] = __float2half_rn(r[q]);
+    memcpy(&t, h, sizeof(VT));
+  } else {
+    memcpy(&t, r, sizeof(VT));
+  }
   *reinterpret_cast<VT*>(p) = t;
 }
+template <class T> __device__ __forceinline__ double to_d(T v) { return (double)v; }
+template <> __device__ __forceinline__ double to_d<__half>(__half v) { return (double)__half2float(v); }
+template <class T> __device__ __forceinline__ T from_d(double v) { return (T)v; }
+template <> __device__ __forceinline__ __half from_d<__half>(double v) { return __float2half_rn((float)v); }
 
+// Lanes per row: each lane moves one 16-byte vector (or the whole row when K is smaller).
 template <class T, int K>
 struct Lanes {
-  static constexpr int V = std::is_same<T, float>::value ? (K >= 4 ? 4 : K) : (K >= 2 ? 2 : 1);
+  static constexpr int V = std::is_same<T, float>::value    ? (K >= 4 ? 4 : K)
+                           : std::is_same<T, __half>::value ? (K >= 8 ? 8 : K)
+                                                            : (K >= 2 ? 2 : 1);
   static constexpr int LPR = K / V;        // lanes per row
   static constexpr int RPB = TB / LPR;     // rows per block
 };
@@ -283,36 +330,37 @@ struct Lanes {
 // SH: right-hand side j of panel p has its own operator A + cs[p*K + j] I (D likewise).
 template <class T, int K, int W, bool SH>
 __global__ void __launch_bounds__(TB) k_sweep(int n, int Wr, const int32_t* __restrict__ col,
-                                              const T* __restrict__ off, const T* __restrict__ diag,
-                                              const T* __restrict__ dinv, const T* __restrict__ b,
+                                              const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
+                                              const CT<T>* __restrict__ dinv, const T* __restrict__ b,
                                               const T* __restrict__ x, T* __restrict__ out, T* __restrict__ d,
-                                              SweepPrm<T> prm, size_t pstride, const T* __restrict__ cs) {
+                                              SweepPrm<CT<T>> prm, size_t pstride, const CT<T>* __restrict__ shf) {
   using Ln = Lanes<T, K>;
+  using C = CT<T>;
   pdl_enter();
   constexpr int V = Ln::V;
   const int w = W > 0 ? W : Wr;
   const int lane = threadIdx.x % Ln::LPR;
   const size_t po = (size_t)blockIdx.y * pstride + (size_t)lane * V;
-  T csv[V];
-  if constexpr (SH) ldv<T, V>(cs + (size_t)blockIdx.y * K + (size_t)lane * V, csv);
+  C csv[V];
+  if constexpr (SH) ldv<C, V>(shf + (size_t)blockIdx.y * K + (size_t)lane * V, csv);
   for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < n; i += gridDim.x * Ln::RPB) {
     const size_t ik = po + (size_t)i * K;
-    T r[V], xi[V];
+    C r[V], xi[V];
     ldv<T, V>(b + ik, r);
     if (!prm.zero_x) {
       ldv<T, V>(x + ik, xi);
-      const T dg = diag[i];
-      T acc[V];
+      const C dg = diag[i];
+      C acc[V];
 #pragma unroll
       for (int q = 0; q < V; ++q) {
         if constexpr (SH) acc[q] = (dg + csv[q]) * xi[q];
         else acc[q] = dg * xi[q];
       }
       const int32_t* c = col + (size_t)i * w;
-      const T* v = off + (size_t)i * w;
+      const C* v = off + (size_t)i * w;
       if constexpr (W > 0) {
         int cs[W];
-        T vs[W];
+        C vs[W];
 #pragma unroll
         for (int s = 0; s < W; ++s) {
           cs[s] = c[s];
@@ -320,16 +368,16 @@ __global__ void __launch_bounds__(TB) k_sweep(int n, int Wr, const int32_t* __re
         }
 #pragma unroll
         for (int s = 0; s < W; ++s) {
-          T nb[V];
+          C nb[V];
           ldv<T, V>(x + po + (size_t)cs[s] * K, nb);
 #pragma unroll
           for (int q = 0; q < V; ++q) acc[q] += vs[s] * nb[q];
         }
       } else {
         for (int s = 0; s < w; ++s) {
-          T nb[V];
+          C nb[V];
           ldv<T, V>(x + po + (size_t)c[s] * K, nb);
-          const T vv = v[s];
+          const C vv = v[s];
 #pragma unroll
           for (int q = 0; q < V; ++q) acc[q] += vv * nb[q];
         }
@@ -338,24 +386,24 @@ __global__ void __launch_bounds__(TB) k_sweep(int n, int Wr, const int32_t* __re
       for (int q = 0; q < V; ++q) r[q] = r[q] - acc[q];
     } else {
 #pragma unroll
-      for (int q = 0; q < V; ++q) xi[q] = T(0);
+      for (int q = 0; q < V; ++q) xi[q] = C(0);
     }
     if (prm.mode == S_RESID) {
       stv<T, V>(out + ik, r);
       continue;
     }
-    T di[V];
+    C di[V];
 #pragma unroll
     for (int q = 0; q < V; ++q) {
-      if constexpr (SH) di[q] = T(1) / (diag[i] + csv[q]);
+      if constexpr (SH) di[q] = C(1) / (diag[i] + csv[q]);
       else di[q] = dinv[i];
     }
-    T o[V];
+    C o[V];
     if (prm.mode == S_JACOBI) {
 #pragma unroll
       for (int q = 0; q < V; ++q) o[q] = xi[q] + prm.omega * (di[q] * r[q]);
     } else if (prm.mode == S_CHEB0) {
-      T dn[V];
+      C dn[V];
 #pragma unroll
       for (int q = 0; q < V; ++q) {
         dn[q] = (di[q] * r[q]) * prm.inv_theta;
@@ -363,7 +411,7 @@ __global__ void __launch_bounds__(TB) k_sweep(int n, int Wr, const int32_t* __re
       }
       if (prm.write_d) stv<T, V>(d + ik, dn);
     } else {
-      T dn[V];
+      C dn[V];
       if (prm.d_is_x) {
 #pragma unroll
         for (int q = 0; q < V; ++q) dn[q] = xi[q];
@@ -390,6 +438,7 @@ __global__ void __launch_bounds__(TB) k_restrict(int nc, int Wq, const int32_t* 
                                                  const T* __restrict__ rf, T* __restrict__ rc, size_t fstride,
                                                  size_t cstride) {
   using Ln = Lanes<T, K>;
+  using C = CT<T>;
   pdl_enter();
   constexpr int V = Ln::V;
   const int lane = threadIdx.x % Ln::LPR;
@@ -397,8 +446,8 @@ __global__ void __launch_bounds__(TB) k_restrict(int nc, int Wq, const int32_t* 
   T* c = rc + (size_t)blockIdx.y * cstride + (size_t)lane * V;
   for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < nc; i += gridDim.x * Ln::RPB) {
     const double s = rs[i];
-    const T w1 = (T)(1.0 / s), wh = (T)(0.5 / s);
-    T acc[V], v[V];
+    const C w1 = (C)(1.0 / s), wh = (C)(0.5 / s);
+    C acc[V], v[V];
     ldv<T, V>(f + (size_t)rself[i] * K, v);
 #pragma unroll
     for (int q = 0; q < V; ++q) acc[q] = w1 * v[q];
@@ -420,18 +469,19 @@ __global__ void __launch_bounds__(TB) k_prolong(int nf, const int32_t* __restric
                                                 const T* __restrict__ z, T* __restrict__ x, size_t fstride,
                                                 size_t cstride) {
   using Ln = Lanes<T, K>;
+  using C = CT<T>;
   pdl_enter();
   constexpr int V = Ln::V;
   const int lane = threadIdx.x % Ln::LPR;
   const T* zc = z + (size_t)blockIdx.y * cstride + (size_t)lane * V;
   T* xf = x + (size_t)blockIdx.y * fstride + (size_t)lane * V;
   for (int j = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; j < nf; j += gridDim.x * Ln::RPB) {
-    T za[V], zb[V], xv[V];
+    C za[V], zb[V], xv[V];
     ldv<T, V>(zc + (size_t)pa[j] * K, za);
     ldv<T, V>(zc + (size_t)pb[j] * K, zb);
     ldv<T, V>(xf + (size_t)j * K, xv);
 #pragma unroll
-    for (int q = 0; q < V; ++q) xv[q] += T(0.5) * za[q] + T(0.5) * zb[q];
+    for (int q = 0; q < V; ++q) xv[q] += C(0.5) * za[q] + C(0.5) * zb[q];
     stv<T, V>(xf + (size_t)j * K, xv);
   }
 }
@@ -448,8 +498,8 @@ __global__ void __launch_bounds__(TB) k_coarse(int n, const double* __restrict__
   for (int i = blockIdx.x * (TB / K) + threadIdx.x / K; i < n; i += gridDim.x * (TB / K)) {
     const double* a = ainv + (size_t)i * n;
     double s = 0.0;
-    for (int j = 0; j < n; ++j) s += a[j] * (double)bb[(size_t)j * K + k];
-    xx[(size_t)i * K + k] = (T)s;
+    for (int j = 0; j < n; ++j) s += a[j] * to_d(bb[(size_t)j * K + k]);
+    xx[(size_t)i * K + k] = from_d<T>(s);
   }
 }
 
@@ -469,7 +519,7 @@ __global__ void __launch_bounds__(TB) k_coarse_eig1(int n, const double* __restr
   for (int i = blockIdx.x * (TB / K) + threadIdx.x / K; i < n; i += gridDim.x * (TB / K)) {
     const double* a = F + (size_t)i * n;
     double s = 0.0;
-    for (int j = 0; j < n; ++j) s += a[j] * (double)bb[(size_t)j * K + k];
+    for (int j = 0; j < n; ++j) s += a[j] * to_d(bb[(size_t)j * K + k]);
     yy[(size_t)i * K + k] = s / (lam[i] + c);
   }
 }
@@ -485,7 +535,7 @@ __global__ void __launch_bounds__(TB) k_coarse_eig2(int n, const double* __restr
     const double* a = E + (size_t)i * n;
     double s = 0.0;
     for (int j = 0; j < n; ++j) s += a[j] * yy[(size_t)j * K + k];
-    xx[(size_t)i * K + k] = (T)s;
+    xx[(size_t)i * K + k] = from_d<T>(s);
   }
 }
 
@@ -522,6 +572,35 @@ __global__ void k_axpy_update(size_t total, const T* __restrict__ z, double* __r
     u[q] += (double)z[q];
 }
 
+// FP16 storage: u += (double) z · escale[j] (z holds the correction of the scaled right-hand side).
+template <int K>
+__global__ void k_axpy_scaled(size_t total, size_t pstride, const __half* __restrict__ z,
+                              const double* __restrict__ esc, double* __restrict__ u) {
+  pdl_enter();
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x)
+    u[q] += (double)__half2float(z[q]) * esc[(q / pstride) * K + q % K];
+}
+
+// FP16 storage: the finest right-hand side is the FP64 residual (rounded to FP32) over its RMS,
+// b_j = r_j / rms_j, rms_j = sqrt(Σ r_j² / n) (1 for a zero residual), so the V-cycle works on
+// values of order one; escale_j = rms_j undoes it in the next update.
+template <int K>
+__global__ void k_scale_half(int n, int np, const float* __restrict__ r, const double* __restrict__ norms,
+                             __half* __restrict__ b, double* __restrict__ esc) {
+  pdl_enter();
+  auto rms_of = [&](int c) {
+    const double v = sqrt(norms[c] / n);
+    return (v > 0.0 && isfinite(v)) ? v : 1.0;
+  };
+  if (blockIdx.x == 0)
+    for (int c = threadIdx.x; c < K * np; c += blockDim.x) esc[c] = rms_of(c);
+  const size_t pstride = (size_t)n * K, total = pstride * np;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)((q / pstride) * K + q % K);
+    b[q] = __float2half_rn((float)((double)r[q] / rms_of(c)));
+  }
+}
+
 // FP64 residual r = b - A u on the panels, written in the inner precision T, with per-block
 // partial sums of r² per right-hand side (deterministic two-stage reduction).
 template <class T, int K, int W, bool SH>
@@ -553,12 +632,28 @@ __global__ void __launch_bounds__(TB) k_residual64(int n, int Wr, const int32_t*
     }
     const int32_t* c = col + (size_t)i * w;
     const double* v = off + (size_t)i * w;
-    for (int s = 0; s < w; ++s) {
-      double nb[V];
-      ldv<double, V>(u + po + (size_t)c[s] * K, nb);
-      const double vv = v[s];
+    if constexpr (W > 0) {  // all index, value and neighbour loads before the products
+      int cc[W];
+      double vs[W], nb[W][V];
 #pragma unroll
-      for (int q = 0; q < V; ++q) acc[q] += vv * nb[q];
+      for (int s = 0; s < W; ++s) {
+        cc[s] = c[s];
+        vs[s] = v[s];
+      }
+#pragma unroll
+      for (int s = 0; s < W; ++s) ldv<double, V>(u + po + (size_t)cc[s] * K, nb[s]);
+#pragma unroll
+      for (int s = 0; s < W; ++s)
+#pragma unroll
+        for (int q = 0; q < V; ++q) acc[q] += vs[s] * nb[s][q];
+    } else {
+      for (int s = 0; s < w; ++s) {
+        double nb[V];
+        ldv<double, V>(u + po + (size_t)c[s] * K, nb);
+        const double vv = v[s];
+#pragma unroll
+        for (int q = 0; q < V; ++q) acc[q] += vv * nb[q];
+      }
     }
 #pragma unroll
     for (int q = 0; q < V; ++q) {
@@ -907,13 +1002,16 @@ template <class T>
 struct LevelBufs {
   DArr<T> x, y, b, d;  // x / y ping-pong, b right-hand side, d Chebyshev direction
   DArr<T> q, e;        // CG smoother: A p and the accumulated correction Δx (CG mode only)
-  const T* cs = nullptr;  // per-RHS shifts (coarse_solver 2), K * npanels, shared by all levels
+  const CT<T>* cs = nullptr;  // per-RHS shifts (coarse_solver 2), K * npanels, shared by all levels
 };
 
 struct Workspace {
   int K = 0, npanels = 0, prec = 0;
   std::vector<LevelBufs<float>> f32;
   std::vector<LevelBufs<double>> f64;
+  std::vector<LevelBufs<__half>> f16;  // precision 2: FP16 panels, FP32 arithmetic
+  DArr<float> r32;                     // precision 2: the FP64 residual rounded to FP32
+  DArr<double> escale;                 // precision 2: per-RHS scale of the FP16 right-hand side
   DArr<double> B64, U64;      // finest FP64 panels
   DArr<double> partial, norms;
   DArr<double> scal;          // CG smoother: per-right-hand-side scalars (CgField x K*npanels)
@@ -1192,7 +1290,9 @@ dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
   require(o.smoother != DEC_SMOOTH_CG || o.precision == 0, "multigrid: the CG smoother runs in FP64 (precision 0)");
   require(o.pre >= 0 && o.post >= 0 && o.pre <= 16 && o.post <= 16, "multigrid: sweeps must be in [0, 16]");
   require(o.mu == 1 || o.mu == 2, "multigrid: mu must be 1 (V) or 2 (W)");
-  require(o.precision == 0 || o.precision == 1, "multigrid: precision must be 0 or 1");
+  require(o.precision >= 0 && o.precision <= 2, "multigrid: precision must be 0, 1 or 2");
+  require(o.precision != 2 || o.smoother == DEC_SMOOTH_JACOBI || o.smoother == DEC_SMOOTH_CHEBYSHEV,
+          "multigrid: FP16 storage (precision 2) needs the Jacobi or Chebyshev smoother");
   require(o.cheb_ratio > 1.0, "multigrid: cheb_ratio must exceed 1");
   require(o.inner_cycles >= 1 && o.inner_cycles <= 8, "multigrid: inner_cycles must be in [1, 8]");
   require(o.coarse_max >= 0 && o.coarse_max <= 1024, "multigrid: coarse_max must be in [0, 1024]");
@@ -1284,8 +1384,9 @@ const dec_op* mg_level_op(const dec_mg* mg, int level) { return level_at(mg, lev
 // ---------------------------------------------------------------------------------------------
 // Cycle enqueue
 // ---------------------------------------------------------------------------------------------
+// The level's operator arrays in the compute type of storage type T (FP32 for FP16 storage).
 template <class T>
-static const T* pick(const DArr<double>& a64, const DArr<float>& a32) {
+static const CT<T>* pick(const DArr<double>& a64, const DArr<float>& a32) {
   if constexpr (std::is_same<T, double>::value) return a64.p;
   else return a32.p;
 }
@@ -1296,13 +1397,13 @@ static dim3 row_grid(int n, int np) {
 }
 
 template <class T, int K>
-static void launch_sweep(const Level& L, const T* b, const T* x, T* out, T* d, SweepPrm<T> prm, int np,
-                         cudaStream_t s, const T* cs) {
+static void launch_sweep(const Level& L, const T* b, const T* x, T* out, T* d, SweepPrm<CT<T>> prm, int np,
+                         cudaStream_t s, const CT<T>* cs) {
   size_t ps = (size_t)L.n * K;
   dim3 grid = row_grid<T, K>(L.n, np);
-  const T* off = pick<T>(L.off64, L.off32);
-  const T* dg = pick<T>(L.diag64, L.diag32);
-  const T* di = pick<T>(L.dinv64, L.dinv32);
+  const CT<T>* off = pick<T>(L.off64, L.off32);
+  const CT<T>* dg = pick<T>(L.diag64, L.diag32);
+  const CT<T>* di = pick<T>(L.dinv64, L.dinv32);
   if (cs) {
     if (L.W == 6)
       launch_pdl(k_sweep<T, K, 6, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
@@ -1321,13 +1422,14 @@ static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool z
                  cudaStream_t s) {
   const dec_mg_options& o = mg.opt;
   T* other = (x == B.x.p) ? B.y.p : B.x.p;
+  if constexpr (!std::is_same<T, __half>::value) {
   if (o.smoother == DEC_SMOOTH_LEARNED && !mg.force_plain) {
     // learned sweep: r = b - A x (skipped from zero: r = b), then x + (s / a_ii) MLP(features(r))
     const MlpWeights wts = mlp_weights(mg.mlp);
     for (int it = 0; it < sweeps; ++it) {
       const T* r = B.b.p;
       if (!zero_x) {
-        SweepPrm<T> prm{};
+        SweepPrm<CT<T>> prm{};
         prm.mode = S_RESID;
         launch_sweep<T, K>(L, B.b.p, x, B.d.p, nullptr, prm, np, s, B.cs);
         r = B.d.p;
@@ -1339,27 +1441,29 @@ static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool z
     }
     return x;
   }
+  }
+  using C = CT<T>;
   const double hi = L.lmax, lo = L.lmax / o.cheb_ratio;
   const double theta = (hi + lo) / 2, delta = (hi - lo) / 2, sigma = theta / delta;
   double rho = 1 / sigma;
   const bool started_at_zero = zero_x;
   for (int it = 0; it < sweeps; ++it) {
-    SweepPrm<T> prm{};
+    SweepPrm<C> prm{};
     prm.zero_x = zero_x ? 1 : 0;
     // the direction is needed only by a later sweep; after a first step from zero it equals x
     prm.write_d = (it + 1 < sweeps) && !(it == 0 && started_at_zero) ? 1 : 0;
     prm.d_is_x = (it == 1 && started_at_zero) ? 1 : 0;
     if (o.smoother == DEC_SMOOTH_JACOBI) {
       prm.mode = S_JACOBI;
-      prm.omega = (T)o.omega;
+      prm.omega = (C)o.omega;
     } else if (it == 0) {
       prm.mode = S_CHEB0;
-      prm.inv_theta = (T)(1.0 / theta);
+      prm.inv_theta = (C)(1.0 / theta);
     } else {
       double rho_new = 1 / (2 * sigma - rho);
       prm.mode = S_CHEBN;
-      prm.c1 = (T)(rho_new * rho);
-      prm.c2 = (T)(2 * rho_new / delta);
+      prm.c1 = (C)(rho_new * rho);
+      prm.c2 = (C)(2 * rho_new / delta);
       rho = rho_new;
     }
     launch_sweep<T, K>(L, B.b.p, x, other, B.d.p, prm, np, s, B.cs);
@@ -1473,7 +1577,7 @@ static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bu
   zero_x = zero_x && mg.opt.pre == 0;
   // residual into the free buffer, then restrict into the coarse right-hand side
   T* r = (x == B.x.p) ? B.y.p : B.x.p;
-  SweepPrm<T> prm{};
+  SweepPrm<CT<T>> prm{};
   prm.mode = S_RESID;
   prm.zero_x = zero_x ? 1 : 0;
   launch_sweep<T, K>(L, B.b.p, x, r, nullptr, prm, np, s, B.cs);
@@ -1533,25 +1637,38 @@ static void enqueue_resid_T(dec_mg& mg, Workspace& w, cudaStream_t s, std::vecto
   const Level& F = mg.lv[0];
   const int np = w.npanels;
   const size_t total = (size_t)F.n * K * np;
-  launch_pdl(k_axpy_update<T>, dim3(grid_for((long long)total, 256)), dim3(256), s, total, (const T*)bufs[0].x.p,
-             w.U64.p);
+  constexpr bool H = std::is_same<T, __half>::value;
+  using R = typename std::conditional<H, float, T>::type;  // the residual kernel's output type
+  R* rout;
+  if constexpr (H) {
+    launch_pdl(k_axpy_scaled<K>, dim3(grid_for((long long)total, 256)), dim3(256), s, total, (size_t)F.n * K,
+               (const __half*)bufs[0].x.p, (const double*)w.escale.p, w.U64.p);
+    rout = w.r32.p;
+  } else {
+    launch_pdl(k_axpy_update<T>, dim3(grid_for((long long)total, 256)), dim3(256), s, total, (const T*)bufs[0].x.p,
+               w.U64.p);
+    rout = bufs[0].b.p;
+  }
   dim3 g(w.nblocks, np);
   const double* cs = w.cs64.p;
   auto go = [&](auto kern) {
     launch_pdl(kern, g, dim3(TB), s, F.n, F.W, (const int32_t*)F.col.p, (const double*)F.off64.p,
-               (const double*)F.diag64.p, (const double*)w.B64.p, (const double*)w.U64.p, bufs[0].b.p, w.partial.p,
+               (const double*)F.diag64.p, (const double*)w.B64.p, (const double*)w.U64.p, rout, w.partial.p,
                (size_t)F.n * K, cs);
   };
   if (cs) {
-    if (F.W == 6) go(k_residual64<T, K, 6, true>);
-    else go(k_residual64<T, K, 0, true>);
+    if (F.W == 6) go(k_residual64<R, K, 6, true>);
+    else go(k_residual64<R, K, 0, true>);
   } else if (F.W == 6) {
-    go(k_residual64<T, K, 6, false>);
+    go(k_residual64<R, K, 6, false>);
   } else {
-    go(k_residual64<T, K, 0, false>);
+    go(k_residual64<R, K, 0, false>);
   }
   launch_pdl(k_reduce_partials, dim3(K * np), dim3(256), s, w.nblocks, K, np, (const double*)w.partial.p,
              w.norms.p);
+  if constexpr (H)
+    launch_pdl(k_scale_half<K>, dim3(grid_for((long long)total, 256)), dim3(256), s, F.n, np, (const float*)w.r32.p,
+               (const double*)w.norms.p, (__half*)bufs[0].b.p, w.escale.p);
   DEC_CHECK_LAUNCH();
 }
 
@@ -1588,6 +1705,9 @@ template <int K>
 static void enqueue_kind(dec_mg& mg, Workspace& w, cudaStream_t s, int kind) {
   if (kind == G_CYCLE) {
     enqueue_cycle<K>(mg, w, s);
+  } else if (w.prec == 2) {
+    if (kind == G_RESID) enqueue_resid_T<__half, K>(mg, w, s, w.f16);
+    else enqueue_vcycle_T<__half, K>(mg, w, s, w.f16);
   } else if (w.prec == 1) {
     if (kind == G_RESID) enqueue_resid_T<float, K>(mg, w, s, w.f32);
     else enqueue_vcycle_T<float, K>(mg, w, s, w.f32);
@@ -1655,7 +1775,14 @@ static Workspace& workspace_k(dec_mg& mg, int nrhs, int prec, int K) {
   w->npanels = np;
   w->prec = prec;
   const size_t total = (size_t)mg.lv[0].n * K * np;
-  if (prec == 1) alloc_bufs(mg, w->f32, K, np);
+  if (prec == 2) {
+    alloc_bufs(mg, w->f16, K, np);
+    w->r32.alloc(total);
+    std::vector<double> ones((size_t)K * np, 1.0);
+    w->escale.upload(ones);
+  } else if (prec == 1) {
+    alloc_bufs(mg, w->f32, K, np);
+  }
   else alloc_bufs(mg, w->f64, K, np);
   w->B64.alloc(total);
   w->U64.alloc(total);
@@ -1675,6 +1802,7 @@ static Workspace& workspace_k(dec_mg& mg, int nrhs, int prec, int K) {
     DEC_CUDA(cudaMemcpy(w->cs64.p, w->hcs64.data(), w->cs64.bytes(), cudaMemcpyHostToDevice));
     DEC_CUDA(cudaMemcpy(w->cs32.p, w->hcs32.data(), w->cs32.bytes(), cudaMemcpyHostToDevice));
     for (auto& b : w->f32) b.cs = w->cs32.p;
+    for (auto& b : w->f16) b.cs = w->cs32.p;
     for (auto& b : w->f64) b.cs = w->cs64.p;
   }
   DEC_CUDA(cudaMemset(w->B64.p, 0, w->B64.bytes()));
@@ -1760,7 +1888,8 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
   else
     DEC_CUDA(cudaMemsetAsync(w.U64.p, 0, total * sizeof(double), s));
   // the first refinement step adds e = 0
-  if (w.prec == 1) DEC_CUDA(cudaMemsetAsync(w.f32[0].x.p, 0, total * sizeof(float), s));
+  if (w.prec == 2) DEC_CUDA(cudaMemsetAsync(w.f16[0].x.p, 0, total * sizeof(__half), s));
+  else if (w.prec == 1) DEC_CUDA(cudaMemsetAsync(w.f32[0].x.p, 0, total * sizeof(float), s));
   else DEC_CUDA(cudaMemsetAsync(w.f64[0].x.p, 0, total * sizeof(double), s));
   DEC_CHECK_LAUNCH();
   // ||b|| per right-hand side.
@@ -1811,7 +1940,8 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
       // the learned step fell behind: undo it (u from before the step, e = 0, same residual)
       // and continue with the plain smoother
       DEC_CUDA(cudaMemcpyAsync(w.U64.p, w.Ubak.p, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
-      if (w.prec == 1) DEC_CUDA(cudaMemsetAsync(w.f32[0].x.p, 0, total * sizeof(float), s));
+      if (w.prec == 2) DEC_CUDA(cudaMemsetAsync(w.f16[0].x.p, 0, total * sizeof(__half), s));
+  else if (w.prec == 1) DEC_CUDA(cudaMemsetAsync(w.f32[0].x.p, 0, total * sizeof(float), s));
       else DEC_CUDA(cudaMemsetAsync(w.f64[0].x.p, 0, total * sizeof(double), s));
       worst = residual();
       plain = true;
@@ -1865,21 +1995,30 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
   DEC_CUDA(cudaEventCreate(&e1));
   auto launch = [&]() {
     if (kernel == DEC_KERNEL_SWEEP) {
-      SweepPrm<T> prm{};
+      SweepPrm<CT<T>> prm{};
       prm.mode = mg.opt.smoother == DEC_SMOOTH_JACOBI ? S_JACOBI : S_CHEBN;
       prm.write_d = 1;  // a middle Chebyshev step: reads and writes the direction
-      prm.omega = (T)mg.opt.omega;
-      prm.c1 = (T)0.5;
-      prm.c2 = (T)0.25;
+      prm.omega = (CT<T>)mg.opt.omega;
+      prm.c1 = (CT<T>)0.5;
+      prm.c2 = (CT<T>)0.25;
       launch_sweep<T, K>(L, B.b.p, B.x.p, B.y.p, B.d.p, prm, np, s, B.cs);
     } else if (kernel == DEC_KERNEL_MLP) {
-      launch_mlp_smooth<T, K>(mlp_weights(mg.mlp), L.n, L.W, L.col.p, L.mtab.p, pick<T>(L.diag64, L.diag32), B.b.p,
-                              B.x.p, 0, B.y.p, np, s);
+      if constexpr (!std::is_same<T, __half>::value)
+        launch_mlp_smooth<T, K>(mlp_weights(mg.mlp), L.n, L.W, L.col.p, L.mtab.p, pick<T>(L.diag64, L.diag32),
+                                B.b.p, B.x.p, 0, B.y.p, np, s);
     } else if (kernel == DEC_KERNEL_RESIDUAL) {
       dim3 g(w.nblocks, np);
       const Level& F = mg.lv[0];
-      k_residual64<T, K, 0, false><<<g, TB, 0, s>>>(F.n, F.W, F.col.p, F.off64.p, F.diag64.p, w.B64.p, w.U64.p,
-                                                    bufs[0].b.p, w.partial.p, (size_t)F.n * K, nullptr);
+      using R = typename std::conditional<std::is_same<T, __half>::value, float, T>::type;
+      R* rout;
+      if constexpr (std::is_same<T, __half>::value) rout = w.r32.p;
+      else rout = bufs[0].b.p;
+      if (F.W == 6)  // the variant the solve launches
+        k_residual64<R, K, 6, false><<<g, TB, 0, s>>>(F.n, F.W, F.col.p, F.off64.p, F.diag64.p, w.B64.p, w.U64.p,
+                                                      rout, w.partial.p, (size_t)F.n * K, nullptr);
+      else
+        k_residual64<R, K, 0, false><<<g, TB, 0, s>>>(F.n, F.W, F.col.p, F.off64.p, F.diag64.p, w.B64.p, w.U64.p,
+                                                      rout, w.partial.p, (size_t)F.n * K, nullptr);
     } else if (kernel == DEC_KERNEL_RESTRICT) {
       const Level& Cl = mg.lv[level + 1];
       k_restrict<T, K><<<row_grid<T, K>(Cl.n, np), TB, 0, s>>>(L.nc, L.Wq, L.rself.p, L.ridx.p, L.rs.p, B.x.p,
@@ -1923,7 +2062,8 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
 template <int K>
 static void time_kernel_K(dec_mg& mg, Workspace& w, int kernel, int level, int reps, cudaStream_t s, double* ms,
                           double* bytes) {
-  if (w.prec == 1) time_kernel_T<float, K>(mg, w, w.f32, kernel, level, reps, s, ms, bytes);
+  if (w.prec == 2) time_kernel_T<__half, K>(mg, w, w.f16, kernel, level, reps, s, ms, bytes);
+  else if (w.prec == 1) time_kernel_T<float, K>(mg, w, w.f32, kernel, level, reps, s, ms, bytes);
   else time_kernel_T<double, K>(mg, w, w.f64, kernel, level, reps, s, ms, bytes);
 }
 
@@ -2137,7 +2277,8 @@ dec_status batch_solve(dec_batch* b, double* const* u, const double* const* rhs,
     const size_t tot = (size_t)n * K * np;
     k_to_panels<double, double><<<grid_for((long long)tot, 256), 256, 0, s>>>(n, nrhs[q], K, np, F.dperm.p, rhs[q], w.B64.p);
     k_to_panels<double, double><<<grid_for((long long)tot, 256), 256, 0, s>>>(n, nrhs[q], K, np, F.dperm.p, u[q], w.U64.p);
-    if (w.prec == 1) DEC_CUDA(cudaMemsetAsync(w.f32[0].x.p, 0, tot * sizeof(float), s));
+    if (w.prec == 2) DEC_CUDA(cudaMemsetAsync(w.f16[0].x.p, 0, tot * sizeof(__half), s));
+    else if (w.prec == 1) DEC_CUDA(cudaMemsetAsync(w.f32[0].x.p, 0, tot * sizeof(float), s));
     else DEC_CUDA(cudaMemsetAsync(w.f64[0].x.p, 0, tot * sizeof(double), s));
     dim3 g(w.nblocks, np);
     switch (K) {

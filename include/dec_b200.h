@@ -182,7 +182,9 @@ typedef struct dec_mg_options {
                               admits a shift per right-hand side (every level then stores the
                               Laplacian, and RHS j solves (L + (shift + c_j) I) u = b; see
                               dec_mg_solve_shifted); Jacobi / Chebyshev smoothers only */
-  int32_t precision;       /* 0: FP64 V-cycles; 1: FP32 V-cycles inside FP64 iterative refinement */
+  int32_t precision;       /* 0: FP64 V-cycles; 1: FP32 V-cycles inside FP64 iterative refinement;
+                              2: FP16-stored panels (FP32 arithmetic) inside FP64 refinement, each
+                              step's residual scaled to unit RMS per RHS (Jacobi / Chebyshev only) */
   int32_t rhs_block;       /* right-hand sides per panel (1, 2, 4, 8, 16, 32; 0 = automatic) */
   int32_t mu;              /* 1 = V-cycle, 2 = W-cycle */
   int32_t inner_cycles;    /* cycles per refinement step of dec_mg_solve (>= 1) */

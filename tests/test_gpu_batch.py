@@ -51,8 +51,9 @@ def _check_solutions(L, B, U, shifts, rtol):
 
 
 @pytest.mark.parametrize("name", list(GROUPS))
-def test_shifted_solve_matches_direct(O, dec, name):
-    md, mg = _pair(O, dec, name)
+@pytest.mark.parametrize("precision", [1, 2])
+def test_shifted_solve_matches_direct(O, dec, name, precision):
+    md, mg = _pair(O, dec, name, precision)
     L = csc(md.op(0))
     # every level stores the Laplacian itself
     ref = L.tocsr()

@@ -105,8 +105,10 @@ def test_wcycle_matches_oracle_structure(O, dec, built):
     assert rw < 1e-2
 
 
-@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("precision", [0, 1, 2])
 def test_solve_reaches_tolerance(O, dec, built, precision):
+    """FP64, FP32 and FP16-storage V-cycles inside FP64 refinement all reach the requested residual
+    and the direct FP64 solution."""
     import scipy.sparse.linalg as spla
     coarse, md, _ = built["ico4_circum"]
     mg = dec.MultigridData(coarse, 4, shift=1.0, center="circumcenter", project_radius=1.0, precision=precision)
