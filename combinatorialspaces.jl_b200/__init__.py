@@ -27,7 +27,8 @@ from ._capi import check, lib, DecError  # noqa: F401
 __all__ = ["Mesh", "Operator", "MultigridData", "dec_wedge_product", "dec_wedge_product_pd",
            "dec_wedge_product_dp", "dec_wedge_product_dd", "dec_differential", "dec_boundary",
            "dec_dual_derivative", "dec_hodge_star", "dec_inv_hodge_star", "laplace_beltrami",
-           "helmholtz", "multigrid_vcycles", "multigrid_wcycles", "SmootherMLP", "Batch", "DecError"]
+           "helmholtz", "multigrid_vcycles", "multigrid_wcycles", "full_multigrid", "SmootherMLP", "Batch",
+           "DecError"]
 
 CENTERS = {"barycenter": _capi.DEC_BARYCENTER, "circumcenter": _capi.DEC_CIRCUMCENTER}
 
@@ -604,6 +605,16 @@ def multigrid_vcycles(u, b, md, cycles):
     """multigrid_vcycles(u, b, md, cycles) (Multigrid.jl:814): returns the updated u (a copy)."""
     u = u.clone()
     return md.cycles(u, b, cycles)
+
+
+def full_multigrid(b, md, cycles):
+    """full_multigrid(b, md, cycles, alg, μ) (Multigrid.jl:826-855): returns u; μ is the
+    hierarchy's `mu` option."""
+    torch = _torch()
+    u = torch.empty_like(b)
+    nrhs = 1 if b.dim() == 1 else b.shape[0]
+    check(lib().dec_mg_full_multigrid(md._h, _ptr(u), _ptr(b.contiguous()), nrhs, cycles, _stream()))
+    return u
 
 
 def multigrid_wcycles(u, b, md, cycles):

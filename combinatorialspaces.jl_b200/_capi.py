@@ -78,6 +78,7 @@ SIGNATURES = {
     "dec_mg_level_mesh": (I32, [P, I32, PP]),
     "dec_mg_level_op": (I32, [P, I32, PP]),
     "dec_mg_cycles": (I32, [P, P, P, I32, I32, P]),
+    "dec_mg_full_multigrid": (I32, [P, P, P, I32, I32, P]),
     "dec_mg_solve": (I32, [P, P, P, I32, F64, I32, C.POINTER(SolveReport), P]),
     "dec_mg_solve_host": (I32, [P, P, P, I32, F64, I32, I32, C.POINTER(SolveReport), P]),
     "dec_mg_time_kernel": (I32, [P, I32, I32, I32, I32, P, PF64, PF64]),

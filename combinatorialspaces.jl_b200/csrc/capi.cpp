@@ -226,6 +226,10 @@ dec_status dec_mg_cycles(dec_mg* mg, double* u, const double* b, int32_t nrhs, i
   return guard([&] { decb::mg_cycles(mg, u, b, nrhs, cycles, stream); });
 }
 
+dec_status dec_mg_full_multigrid(dec_mg* mg, double* u, const double* b, int32_t nrhs, int32_t cycles, void* stream) {
+  return guard([&] { decb::mg_full_multigrid(mg, u, b, nrhs, cycles, stream); });
+}
+
 dec_status dec_mg_solve(dec_mg* mg, double* u, const double* b, int32_t nrhs, double rtol, int32_t max_iters,
                         dec_solve_report* rep, void* stream) {
   dec_status st = DEC_OK;

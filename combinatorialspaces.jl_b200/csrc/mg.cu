@@ -1854,6 +1854,74 @@ void mg_cycles(dec_mg* mg, double* u, const double* b, int nrhs, int cycles, voi
   DEC_CHECK_LAUNCH();
 }
 
+// full_multigrid (Multigrid.jl:826-855) at level l, b_l in bufs[l].b: restrict b to the next
+// level, solve there recursively, prolong the result as the initial guess (P z onto zero), then
+// `cycles` μ-cycles.  The recursion stops at the level the cycles solve directly.  Returns the
+// buffer holding z_l.
+template <class T, int K>
+static T* fmg_T(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bufs, int l, int cycles, int np,
+                cudaStream_t s) {
+  const Level& L = mg.lv[l];
+  LevelBufs<T>& B = bufs[l];
+  const int last = mg.opt.smoother == DEC_SMOOTH_CG ? (int)mg.lv.size() - 1 : mg.lc;
+  T* z = B.x.p;
+  bool zero = true;
+  if (l < last) {
+    const Level& Cl = mg.lv[l + 1];
+    LevelBufs<T>& Cb = bufs[l + 1];
+    launch_pdl(k_restrict<T, K>, row_grid<T, K>(Cl.n, np), dim3(TB), s, L.nc, L.Wq, (const int32_t*)L.rself.p,
+               (const int32_t*)L.ridx.p, (const double*)L.rs.p, (const T*)B.b.p, Cb.b.p, (size_t)L.n * K,
+               (size_t)Cl.n * K);
+    T* zc = fmg_T<T, K>(mg, w, bufs, l + 1, cycles, np, s);
+    DEC_CUDA(cudaMemsetAsync(z, 0, (size_t)L.n * K * np * sizeof(T), s));
+    launch_pdl(k_prolong<T, K>, row_grid<T, K>(L.n, np), dim3(TB), s, L.n, (const int32_t*)L.pa.p,
+               (const int32_t*)L.pb.p, (const T*)zc, z, (size_t)L.n * K, (size_t)Cl.n * K);
+    zero = false;
+  }
+  for (int c = 0; c < cycles; ++c) {
+    z = mu_cycle<T, K>(mg, w, bufs, l, z, zero, mg.opt.mu, np, s);
+    zero = false;
+  }
+  if (zero) DEC_CUDA(cudaMemsetAsync(z, 0, (size_t)L.n * K * np * sizeof(T), s));
+  return z;
+}
+
+template <int K>
+static void fmg_K(dec_mg& mg, Workspace& w, int cycles, cudaStream_t s) {
+  auto& bufs = w.f64;
+  const size_t total = (size_t)mg.lv[0].n * K * w.npanels;
+  DEC_CUDA(cudaMemcpyAsync(bufs[0].b.p, w.B64.p, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  double* z = fmg_T<double, K>(mg, w, bufs, 0, cycles, w.npanels, s);
+  DEC_CUDA(cudaMemcpyAsync(w.U64.p, z, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  DEC_CHECK_LAUNCH();
+}
+
+void mg_full_multigrid(dec_mg* mg, double* u, const double* b, int nrhs, int cycles, void* stream) {
+  require(mg != nullptr && u != nullptr && b != nullptr, "multigrid: null argument");
+  require(nrhs >= 1 && cycles >= 0, "multigrid: bad nrhs / cycles");
+  require(mg->opt.smoother != DEC_SMOOTH_LEARNED || mg->mlp != nullptr,
+          "multigrid: the learned smoother needs a network (dec_mg_set_smoother_mlp)");
+  cudaStream_t s = as_stream(stream);
+  Workspace& w = workspace(*mg, nrhs, 0);
+  set_shifts(*mg, w, nullptr, nrhs, s);
+  const Level& F = mg->lv[0];
+  const int n = F.n;
+  const size_t total = (size_t)n * w.K * w.npanels;
+  k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, w.K, w.npanels, F.dperm.p, b,
+                                                                               w.B64.p);
+  DEC_CHECK_LAUNCH();
+  switch (w.K) {
+#define DEC_K(KK) \
+  case KK: fmg_K<KK>(*mg, w, cycles, s); break;
+    DEC_K(1) DEC_K(2) DEC_K(4) DEC_K(8) DEC_K(16) DEC_K(32)
+#undef DEC_K
+    default: throw Error(DEC_ERR_INVALID_ARG, "multigrid: bad panel width");
+  }
+  k_from_panels<double, double><<<grid_for((long long)n * nrhs, 256), 256, 0, s>>>(n, nrhs, w.K, F.diperm.p,
+                                                                                    w.U64.p, u);
+  DEC_CHECK_LAUNCH();
+}
+
 dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rtol, int max_iters,
                     dec_solve_report* rep, void* stream, bool host_buffers, bool use_initial_guess,
                     const double* shifts) {

@@ -11,6 +11,7 @@ void mg_level_info(const dec_mg* mg, int level, int64_t* nv, int64_t* ne, int64_
 const dec_mesh* mg_level_mesh(const dec_mg* mg, int level);
 const dec_op* mg_level_op(const dec_mg* mg, int level);
 void mg_cycles(dec_mg* mg, double* u, const double* b, int nrhs, int cycles, void* stream);
+void mg_full_multigrid(dec_mg* mg, double* u, const double* b, int nrhs, int cycles, void* stream);
 dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rtol, int max_iters,
                     dec_solve_report* rep, void* stream, bool host_buffers, bool use_initial_guess,
                     const double* shifts = nullptr);

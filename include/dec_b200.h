@@ -218,6 +218,11 @@ dec_status dec_mg_level_mesh(const dec_mg* mg, int32_t level, const dec_mesh** o
 dec_status dec_mg_level_op(const dec_mg* mg, int32_t level, const dec_op** out);
 /* u (in/out) and b: device FP64, column-major nv x nrhs (one contiguous vector per RHS). */
 dec_status dec_mg_cycles(dec_mg* mg, double* u, const double* b, int32_t nrhs, int32_t cycles, void* stream);
+/* full_multigrid(b, md, cycles, alg, μ) (Multigrid.jl:826-855): b restricted to the coarsest
+ * level, then on the way up each level's solution is prolonged as the next level's initial guess
+ * followed by `cycles` μ-cycles there; u (output) gets the finest level's result.  FP64. */
+dec_status dec_mg_full_multigrid(dec_mg* mg, double* u, const double* b, int32_t nrhs, int32_t cycles,
+                                 void* stream);
 dec_status dec_mg_solve(dec_mg* mg, double* u, const double* b, int32_t nrhs, double rtol,
                         int32_t max_iters, dec_solve_report* report, void* stream);
 /* Same solve with host u / b (pinned or pageable); copies are part of the call.  With

@@ -221,3 +221,40 @@ def test_cg_cycles_multi_rhs_match_single(O, dec):
     for j in range(3):
         ref = O.mu_cycles(md, np.zeros(n), B[j], 3, 1)
         np.testing.assert_allclose(U[j].cpu().numpy(), ref, rtol=1e-9, atol=1e-9 * np.abs(ref).max())
+
+
+# ---- full multigrid (Multigrid.jl:826-855) ---------------------------------------------------
+
+@pytest.mark.parametrize("mu", [1, 2])
+def test_full_multigrid_cg_matches_oracle(O, dec, mu):
+    """FMG with the reference's CG smoother against the oracle's full_multigrid, and the
+    reference's thresholds (test/Multigrid.jl:79-83: FMG-V < 1e-6, FMG-W < 1e-7 after 5 cycles).
+    The operator is the singular Laplacian (shift 0): constants are its null space, which the CG
+    iterations leave to rounding, so the iterates are compared modulo a constant (1e-8)."""
+    md, mg, L = _ref_grid_setup(O, dec, 3, mu)
+    n = L.shape[0]
+    b = L @ ((uniform(0, n) + 1) / 2)
+    bt = torch.tensor(b, device="cuda")
+    for cycles in (1, 5):
+        ref = O.full_multigrid(md, b, cycles, mu)
+        u = dec.full_multigrid(bt, mg, cycles).cpu().numpy()
+        du, dr = u - u.mean(), ref - ref.mean()
+        assert np.linalg.norm(du - dr) <= 1e-8 * np.linalg.norm(dr)
+        assert np.linalg.norm(L @ (u - ref)) <= 1e-8 * np.linalg.norm(b)
+    assert np.linalg.norm(L @ u - b) / np.linalg.norm(b) < (1e-6 if mu == 1 else 1e-7)
+
+
+def test_full_multigrid_chebyshev(O, dec):
+    """FMG with the stationary smoother and the dense coarsest solve: one FMG-V(3,3) pass on
+    icosphere L5 Helmholtz already reduces the residual below 1e-2, and more cycles keep going."""
+    coarse = O.icosahedron()
+    md = O.build_mg(coarse, 5, O.CIRCUMCENTER, 1.0, 1.0, 3)
+    mg = dec.MultigridData(coarse, 5, shift=1.0, center="circumcenter", project_radius=1.0, precision=0)
+    A = csc(md.op(0))
+    n = A.shape[0]
+    B = np.stack([uniform(600 + j, n) for j in range(3)])
+    rel = []
+    for cycles in (1, 3):
+        U = dec.full_multigrid(torch.tensor(B, device="cuda"), mg, cycles).cpu().numpy()
+        rel.append(max(np.linalg.norm(B[j] - A @ U[j]) / np.linalg.norm(B[j]) for j in range(3)))
+    assert rel[0] < 1e-2 and rel[1] < rel[0] * 1e-2
