@@ -238,10 +238,11 @@ def measure_learned(dec, args, B, U64, common, timed):
     ico = dec.meshes.icosahedron()
     out = {"train": {"steps": args.train_steps, "seconds": train_s, "final_losses": [round(l, 4) for _, _, l in losses[-3:]]}}
 
-    def run(level, smoother, sweeps, Bm, Uref=None):
+    def run(level, smoother, sweeps, Bm, Uref=None, engine="tcgen05"):
         opts = dict(common, smoother=smoother, pre=sweeps, post=sweeps)
         mg = dec.MultigridData(ico, level, precision=1, **opts)
         if smoother == 3:
+            mlp.set_engine(engine)
             mg.set_smoother_mlp(mlp)
         U = torch.zeros_like(Bm)
 
@@ -254,6 +255,8 @@ def measure_learned(dec, args, B, U64, common, timed):
         res = {"solves_per_s": Bm.shape[0] * max(1, args.steps) / t, "v_cycles_per_solve": int(rep.iterations),
                "converged": bool(rep.converged), "fallback_iteration": int(rep.fallback_iteration),
                "sweeps": sweeps}
+        if smoother == 3:
+            res["mlp_engine"] = engine
         if Uref is not None:
             res["max_rel_error_vs_fp64_solve"] = float(((U - Uref).norm(dim=1) / Uref.norm(dim=1)).max())
         if smoother == 3:
@@ -266,9 +269,11 @@ def measure_learned(dec, args, B, U64, common, timed):
         return res
 
     out["L8_learned_fp32"] = {f"V({k},{k})": run(LEVEL, 3, k, B, U64) for k in (1, 2)}
+    out["L8_learned_fp32_mma_sync"] = {"V(1,1)": run(LEVEL, 3, 1, B, U64, engine="mma")}
     n9 = 10 * 4 ** 9 + 2
     B9 = torch.tensor(np.stack([dec.meshes.uniform(200 + j, n9) for j in range(NRHS)]), device="cuda")
     out["L9_learned_fp32"] = {f"V({k},{k})": run(9, 3, k, B9) for k in (1, 2)}
+    out["L9_learned_fp32_mma_sync"] = {"V(1,1)": run(9, 3, 1, B9, engine="mma")}
     out["L9_plain_fp32"] = {f"V({k},{k})": run(9, 1, k, B9) for k in (2, 3)}
     del B9
     torch.cuda.empty_cache()
@@ -690,6 +695,7 @@ def run_kernel(args):
                            precision=1, rhs_block=32, coarse_max=args.coarse_max)
     if kind == 4:
         mlp = dec.SmootherMLP(4)
+        mlp.set_engine(args.mlp_engine)
         mg.set_smoother_mlp(mlp)
     for _ in range(args.warmup):
         mg.time_kernel(kind, 0, NRHS, reps=1)
@@ -700,6 +706,7 @@ def run_kernel(args):
             "algorithmic_bytes": by, "GB/s": by / (ms * 1e-3) / 1e9}
     if kind == 4:
         line["tensor_TFLOP/s"] = 10240.0 * nv * NRHS / (ms * 1e-3) / 1e12
+        line["mlp_engine"] = args.mlp_engine
     print(json.dumps(line), flush=True)
 
 
@@ -724,6 +731,8 @@ def main():
                     help="time one DEC operator kernel alone (steps launches after warmup) and exit")
     ap.add_argument("--dtype", default="float64", choices=["float64", "float32"])
     ap.add_argument("--no-batch", action="store_true", dest="no_batch", help="skip the batched-workload section")
+    ap.add_argument("--mlp-engine", default="tcgen05", choices=["mma", "tcgen05"], dest="mlp_engine",
+                    help="kernel engine of the learned smoothing step for --kernel mlp")
     ap.add_argument("--train-steps", type=int, default=20000, dest="train_steps",
                     help="Adam steps of the learned smoother (0 skips the learned-smoother section)")
     args = ap.parse_args()

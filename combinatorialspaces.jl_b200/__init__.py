@@ -548,12 +548,17 @@ class SmootherMLP:
         return s.value
 
     def eval(self, x, tensor_cores=True):
-        """y = MLP(x) for x a float32 CUDA tensor (n, 16)."""
+        """y = MLP(x) for x a float32 CUDA tensor (n, 16); tensor_cores: False (CUDA cores),
+        True / 1 (mma.sync) or 2 (tcgen05 with TMEM accumulators)."""
         torch = _torch()
         x = x.contiguous()
         y = torch.empty(x.shape[0], dtype=torch.float32, device=x.device)
         check(lib().dec_mlp_eval(self._h, _ptr(x), x.shape[0], _ptr(y), int(tensor_cores), _stream()))
         return y
+
+    def set_engine(self, engine):
+        """Kernel engine of the learned smoothing step: "mma" (mma.sync) or "tcgen05"."""
+        check(lib().dec_mlp_set_engine(self._h, {"mma": 0, "tcgen05": 1}[engine]))
 
     def grad(self, x, dy):
         """Σ_q dy_q ∂MLP(x_q)/∂params as a float32 CUDA tensor (NPARAM,)."""

@@ -100,6 +100,7 @@ SIGNATURES = {
     "dec_mlp_loss_grad": (I32, [P, P, P, I32, PF64, P, P]),
     "dec_mlp_train": (I32, [P, P, P, I32, I32, F64, I64, C.c_uint64, P, P]),
     "dec_mlp_save": (I32, [P, C.c_char_p]),
+    "dec_mlp_set_engine": (I32, [P, I32]),
     "dec_mlp_load": (I32, [P, C.c_char_p]),
 }
 

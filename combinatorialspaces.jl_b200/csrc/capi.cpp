@@ -32,6 +32,7 @@ void mlp_loss_grad_impl(dec_mlp* m, dec_op* op, const double* r, int S, double* 
 void mlp_train_impl(dec_mlp* m, dec_op* op, const double* r, int S, int steps, double lr, int64_t batch,
                     uint64_t seed, double* losses, void* stream);
 void mlp_save_impl(const dec_mlp* m, const char* path);
+void mlp_set_engine_impl(dec_mlp* m, int engine);
 void mlp_load_impl(dec_mlp* m, const char* path);
 void op_residual_norms_noalloc_impl(dec_op* op, const double* x, const double* b, int nrhs, double* norms,
                                     double* bnorms, void* stream);
@@ -344,6 +345,10 @@ dec_status dec_mlp_loss_grad(dec_mlp* mlp, dec_op* op, const double* r, int32_t 
 dec_status dec_mlp_train(dec_mlp* mlp, dec_op* op, const double* r, int32_t S, int32_t steps, double lr,
                          int64_t batch, uint64_t seed, double* losses, void* stream) {
   return guard([&] { mlp_train_impl(mlp, op, r, S, steps, lr, batch, seed, losses, stream); });
+}
+
+dec_status dec_mlp_set_engine(dec_mlp* mlp, int32_t engine) {
+  return guard([&] { mlp_set_engine_impl(mlp, engine); });
 }
 
 dec_status dec_mlp_save(const dec_mlp* mlp, const char* path) {

@@ -35,6 +35,7 @@
 
 dec_op* op_create_impl(dec_mesh* mh, int kind, double shift, dec_dtype dt);
 decb::MlpWeights mlp_weights(const dec_mlp* m);
+void mlp_check_error(const dec_mlp* m, cudaStream_t s);
 
 namespace decb {
 
@@ -1048,6 +1049,7 @@ struct dec_mg {
   const dec_mlp* mlp = nullptr;    // learned smoother network (not owned)
   uint64_t epoch = 0;              // bumped whenever workspaces or their graphs are dropped
   bool force_plain = false;        // set while capturing the plain-smoother fallback cycle
+  int mlp_engine = -1;             // kernel engine of the network when the graphs were captured
   ~dec_mg() {
     ws.clear();
     if (cap) cudaStreamDestroy(cap);
@@ -1766,6 +1768,11 @@ static cudaGraphExec_t capture(dec_mg& mg, Workspace& w, int kind) {
 }
 
 static Workspace& workspace_k(dec_mg& mg, int nrhs, int prec, int K) {
+  if (mg.mlp && mg.mlp->engine != mg.mlp_engine) {  // captured cycles hold the other engine's kernels
+    for (auto& kv : mg.ws) kv.second->drop_graphs();
+    ++mg.epoch;
+    mg.mlp_engine = mg.mlp->engine;
+  }
   int np = (nrhs + K - 1) / K;
   long long key = ws_key(K, np, prec);
   auto it = mg.ws.find(key);
@@ -2035,6 +2042,7 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (learned) mlp_check_error(mg->mlp, s);  // a tcgen05 smoothing step whose wait timed out
   if (rep) {
     rep->iterations = it;
     rep->converged = conv ? 1 : 0;

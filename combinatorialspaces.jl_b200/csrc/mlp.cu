@@ -302,15 +302,342 @@ __global__ void __launch_bounds__(kMlpThreads, 3) k_mlp_smooth(MlpWeights w, int
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// tcgen05 inference (sm_100a): 128 samples per tile, one per thread and TMEM lane.  The
+// features (layer-1 A, 128 x 16) and the first hidden layer (layer-2 A, 128 x 64) are written to
+// shared memory in the canonical K-major layout without swizzle (8-row groups of 16-byte core
+// rows: byte (r / 8) * SBO + (k / 8) * 128 + (r % 8) * 16 + (k % 8) * 2, SBO = K / 8 * 128); W1 and
+// W2 are staged the same way as the B operands (N x K).  One thread issues
+//   tcgen05.mma.cta_group::1.kind::f16  D1[128 x 64] = A1 W1ᵀ            (TMEM columns 0..63)
+//   tcgen05.mma ... x4                   D2[128 x 64] = Σ_s A2_s W2_sᵀ    (columns 64..127)
+// (BF16 operands, FP32 accumulation) and commits to an mbarrier; each thread reads its own row
+// with tcgen05.ld 32x32b.x64, so the bias, ReLU, BF16 rounding and the last layer are per-thread.
+// Every mbarrier wait is bounded: on time-out the block agrees (__syncthreads_and), sets *err,
+// stops, frees its TMEM and returns.
+// ---------------------------------------------------------------------------------------------
+constexpr int kTc5Rows = 128;
+constexpr uint32_t kTc5Cols = 128;
+
+struct __align__(128) Tc5Smem {
+  __align__(128) __nv_bfloat16 a1[kTc5Rows * kMlpIn];
+  __align__(128) __nv_bfloat16 a2[kTc5Rows * kMlpH];
+  __align__(128) __nv_bfloat16 w1[kMlpH * kMlpIn];
+  __align__(128) __nv_bfloat16 w2[kMlpH * kMlpH];
+  float b1[kMlpH], b2[kMlpH], w3[kMlpH], b3;
+  __align__(8) uint64_t mbar;
+  uint32_t tmem;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+// byte offset of element (r, k) of a K-major no-swizzle operand with K columns
+__device__ __forceinline__ uint32_t kmaj(int r, int k, int K) {
+  return (uint32_t)((r >> 3) * (K * 16) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+// shared-memory matrix descriptor: start >> 4, LBO >> 4 at 16, SBO >> 4 at 32, version 1 at 46,
+// no swizzle
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// instruction descriptor: F32 accumulator, BF16 A and B, both K-major, N = 64, M = 128
+constexpr uint32_t kTc5Idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(64 >> 3) << 17) |
+                               ((uint32_t)(128 >> 4) << 24);
+
+__device__ __forceinline__ void tc5_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(kTc5Idesc), "r"(acc));
+}
+__device__ __forceinline__ void tc5_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
+  for (int it = 0; it < (1 << 20); ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void tc5_ld64(uint32_t taddr, float (&v)[64]) {
+  uint32_t r[64];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,"
+      "%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+        "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+        "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+        "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+        "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 64; ++j) v[j] = __uint_as_float(r[j]);
+}
+__device__ __forceinline__ void tc5_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc5_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Writes one sample's 16 features (row r of A1).
+__device__ __forceinline__ void tc5_store_features(Tc5Smem& sm, int r, const float (&f)[16]) {
+  uint4 lo, hi;
+  lo.x = pack_bf16(f[0], f[1]);
+  lo.y = pack_bf16(f[2], f[3]);
+  lo.z = pack_bf16(f[4], f[5]);
+  lo.w = pack_bf16(f[6], f[7]);
+  hi.x = pack_bf16(f[8], f[9]);
+  hi.y = pack_bf16(f[10], f[11]);
+  hi.z = pack_bf16(f[12], f[13]);
+  hi.w = pack_bf16(f[14], f[15]);
+  char* base = reinterpret_cast<char*>(sm.a1);
+  *reinterpret_cast<uint4*>(base + kmaj(r, 0, kMlpIn)) = lo;
+  *reinterpret_cast<uint4*>(base + kmaj(r, 8, kMlpIn)) = hi;
+}
+
+__device__ void tc5_setup(Tc5Smem& sm, const MlpWeights& w) {
+  char* w1 = reinterpret_cast<char*>(sm.w1);
+  char* w2 = reinterpret_cast<char*>(sm.w2);
+  for (int i = threadIdx.x; i < kMlpH * kMlpIn; i += blockDim.x)
+    *reinterpret_cast<__nv_bfloat16*>(w1 + kmaj(i / kMlpIn, i % kMlpIn, kMlpIn)) = w.w1[i];
+  for (int i = threadIdx.x; i < kMlpH * kMlpH; i += blockDim.x)
+    *reinterpret_cast<__nv_bfloat16*>(w2 + kmaj(i / kMlpH, i % kMlpH, kMlpH)) = w.w2[i];
+  for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
+    sm.b1[i] = w.b1[i];
+    sm.b2[i] = w.b2[i];
+    sm.w3[i] = w.w3[i];
+  }
+  if (threadIdx.x == 0) {
+    sm.b3 = w.b3[0];
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sm.mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (threadIdx.x < 32) {  // warp 0 allocates the accumulator columns
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem)),
+                 "r"(kTc5Cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_async_smem();
+  tc5_fence_before();
+  __syncthreads();
+  tc5_fence_after();
+}
+
+__device__ void tc5_teardown(Tc5Smem& sm) {
+  tc5_fence_before();
+  __syncthreads();
+  tc5_fence_after();
+  if (threadIdx.x < 32)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sm.tmem), "r"(kTc5Cols));
+}
+
+// The MLP on the CTA's tile (A1 written): returns y of this thread's row, or false on time-out.
+__device__ __forceinline__ bool tc5_tile(Tc5Smem& sm, uint32_t& phase, float& y) {
+  const int r = threadIdx.x;
+  const uint32_t mbar = smem_u32(&sm.mbar);
+  const uint32_t lane_addr = sm.tmem + ((uint32_t)(r & ~31) << 16);
+  fence_async_smem();
+  tc5_fence_before();
+  __syncthreads();
+  if (r == 0) {
+    tc5_fence_after();
+    tc5_mma(sm.tmem, smem_desc(smem_u32(sm.a1), 128, 256), smem_desc(smem_u32(sm.w1), 128, 256), 0);
+    tc5_commit(mbar);
+  }
+  bool ok = __syncthreads_and(mbar_wait(mbar, phase));
+  if (!ok) {  // one more bounded wait for the MMA in flight before the TMEM is freed
+    mbar_wait(mbar, phase);
+    return false;
+  }
+  phase ^= 1;
+  tc5_fence_after();
+  float z[64];
+  tc5_ld64(lane_addr, z);
+  char* a2 = reinterpret_cast<char*>(sm.a2);
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    uint4 v;
+    v.x = pack_bf16(fmaxf(z[8 * c + 0] + sm.b1[8 * c + 0], 0.f), fmaxf(z[8 * c + 1] + sm.b1[8 * c + 1], 0.f));
+    v.y = pack_bf16(fmaxf(z[8 * c + 2] + sm.b1[8 * c + 2], 0.f), fmaxf(z[8 * c + 3] + sm.b1[8 * c + 3], 0.f));
+    v.z = pack_bf16(fmaxf(z[8 * c + 4] + sm.b1[8 * c + 4], 0.f), fmaxf(z[8 * c + 5] + sm.b1[8 * c + 5], 0.f));
+    v.w = pack_bf16(fmaxf(z[8 * c + 6] + sm.b1[8 * c + 6], 0.f), fmaxf(z[8 * c + 7] + sm.b1[8 * c + 7], 0.f));
+    *reinterpret_cast<uint4*>(a2 + kmaj(r, 8 * c, kMlpH)) = v;
+  }
+  fence_async_smem();
+  tc5_fence_before();
+  __syncthreads();
+  if (r == 0) {
+    tc5_fence_after();
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks)
+      tc5_mma(sm.tmem + 64, smem_desc(smem_u32(sm.a2) + 256 * ks, 128, 1024),
+              smem_desc(smem_u32(sm.w2) + 256 * ks, 128, 1024), ks > 0 ? 1u : 0u);
+    tc5_commit(mbar);
+  }
+  ok = __syncthreads_and(mbar_wait(mbar, phase));
+  if (!ok) {
+    mbar_wait(mbar, phase);
+    return false;
+  }
+  phase ^= 1;
+  tc5_fence_after();
+  tc5_ld64(lane_addr + 64, z);
+  float acc = sm.b3;
+#pragma unroll
+  for (int j = 0; j < 64; ++j) acc += sm.w3[j] * fmaxf(z[j] + sm.b2[j], 0.f);
+  y = acc;
+  return true;
+}
+
+// y = MLP(x) for n samples of 16 FP32 features (tcgen05).
+__global__ void __launch_bounds__(kTc5Rows) k_mlp_eval_tc5(int64_t n, const float* __restrict__ x,
+                                                           float* __restrict__ y, MlpWeights w, int* err) {
+  __shared__ Tc5Smem sm;
+  tc5_setup(sm, w);
+  uint32_t phase = 0;
+  const int64_t ntiles = (n + kTc5Rows - 1) / kTc5Rows;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t q = tile * kTc5Rows + threadIdx.x;
+    float f[16];
+    if (q < n) {
+      const float4* src = reinterpret_cast<const float4*>(x + q * 16);
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const float4 t4 = src[v];
+        f[4 * v] = t4.x;
+        f[4 * v + 1] = t4.y;
+        f[4 * v + 2] = t4.z;
+        f[4 * v + 3] = t4.w;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) f[k] = 0.f;
+    }
+    tc5_store_features(sm, threadIdx.x, f);
+    float yv;
+    if (!tc5_tile(sm, phase, yv)) {
+      if (threadIdx.x == 0) atomicExch(err, 1);
+      break;
+    }
+    if (q < n) y[q] = yv;
+  }
+  tc5_teardown(sm);
+}
+
+// Learned smoothing step with the tcgen05 MLP (same features and update as k_mlp_smooth).
+template <class T, int K>
+__global__ void __launch_bounds__(kTc5Rows) k_mlp_smooth_tc5(MlpWeights w, int n, int W,
+                                                             const int32_t* __restrict__ col,
+                                                             const float4* __restrict__ tab,
+                                                             const T* __restrict__ diag, const T* __restrict__ r,
+                                                             const T* __restrict__ x, int zero_x, T* __restrict__ out,
+                                                             size_t pstride, int np, int* err) {
+  __shared__ Tc5Smem sm;
+  tc5_setup(sm, w);
+  uint32_t phase = 0;
+  const int64_t nq = (int64_t)n * K;
+  const int64_t tiles_per_panel = (nq + kTc5Rows - 1) / kTc5Rows;
+  const int64_t ntiles = tiles_per_panel * np;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const size_t po = (size_t)(tile / tiles_per_panel) * pstride;
+    const int64_t q = (tile % tiles_per_panel) * kTc5Rows + threadIdx.x;
+    float f[16];
+    float dsc = 0.f;
+    T xv = T(0);
+    if (q < nq) {
+      const int i = (int)(q / K), k = (int)(q % K);
+      const float4 t0 = tab[2 * (size_t)i], t1 = tab[2 * (size_t)i + 1];
+      const int nn = __float2int_rn(t1.w * 6.0f);
+      const float ri = (float)r[po + q];
+      float nb[6];
+      float s = fabsf(ri);
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        nb[j] = j < nn ? (float)r[po + (size_t)col[(size_t)i * W + j] * K + k] : 0.f;
+        s = fmaxf(s, fabsf(nb[j]));
+      }
+      if (s == 0.0f) s = 1.0f;
+      const float inv = 1.0f / s;
+      f[0] = ri * inv;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) f[1 + j] = nb[j] * inv;
+      f[7] = t0.x;
+      f[8] = t0.y;
+      f[9] = t0.z;
+      f[10] = t0.w;
+      f[11] = t1.x;
+      f[12] = t1.y;
+      f[13] = t1.z;
+      f[14] = t1.w;
+      f[15] = 0.0f;
+      dsc = s / (float)diag[i];
+      if (!zero_x) xv = x[po + q];
+    } else {
+#pragma unroll
+      for (int k2 = 0; k2 < 16; ++k2) f[k2] = 0.f;
+    }
+    tc5_store_features(sm, threadIdx.x, f);
+    float yv;
+    if (!tc5_tile(sm, phase, yv)) {
+      if (threadIdx.x == 0) atomicExch(err, 1);
+      break;
+    }
+    if (q < nq) out[po + q] = xv + (T)(dsc * yv);
+  }
+  tc5_teardown(sm);
+}
+
+// Dynamic shared memory that caps the tcgen05 kernels at 4 resident CTAs per SM, so the
+// 4 x 128 TMEM columns they allocate always fit (no CTA waits in tcgen05.alloc).
+constexpr int kTc5PadSmem = 24 * 1024;
+
+static unsigned tc5_grid(long long tiles) {
+  return (unsigned)std::max<long long>(1, std::min<long long>(tiles, (long long)num_sms() * 4));
+}
+
+// Static + padding shared memory exceeds 48 KB, which needs the kernel's opt-in.
+template <class F>
+static void tc5_opt_in(F* kernel) {
+  DEC_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTc5PadSmem));
+}
+
 template <class T, int K>
 void launch_mlp_smooth(const MlpWeights& w, int n, int W, const int32_t* col, const float4* tab, const T* diag,
                        const T* r, const T* x, int zero_x, T* out, int np, cudaStream_t s) {
+  if (w.engine == 1) {
+    const long long tiles = ((long long)n * K + kTc5Rows - 1) / kTc5Rows * np;
+    k_mlp_smooth_tc5<T, K><<<tc5_grid(tiles), kTc5Rows, kTc5PadSmem, s>>>(w, n, W, col, tab, diag, r, x, zero_x, out,
+                                                                          (size_t)n * K, np, w.err);
+    DEC_CHECK_LAUNCH();
+    return;
+  }
   const long long tiles = ((long long)n * K + kTile - 1) / kTile;
   const long long want = (tiles + kMlpWarps - 1) / kMlpWarps;
   const long long cap = std::max<long long>(1, (long long)num_sms() * 4 / std::max(1, np));
   dim3 grid((unsigned)std::max<long long>(1, std::min(want, cap)), np);
   k_mlp_smooth<T, K><<<grid, kMlpThreads, 0, s>>>(w, n, W, col, tab, diag, r, x, zero_x, out, (size_t)n * K);
   DEC_CHECK_LAUNCH();
+}
+
+// Opts every tcgen05 kernel into its shared-memory padding on the current device.
+void tc5_opt_in_all() {
+  tc5_opt_in(k_mlp_eval_tc5);
+#define DEC_OPT(T, K) tc5_opt_in(k_mlp_smooth_tc5<T, K>);
+  DEC_OPT(float, 1) DEC_OPT(float, 2) DEC_OPT(float, 4) DEC_OPT(float, 8) DEC_OPT(float, 16) DEC_OPT(float, 32)
+  DEC_OPT(double, 1) DEC_OPT(double, 2) DEC_OPT(double, 4) DEC_OPT(double, 8) DEC_OPT(double, 16)
+  DEC_OPT(double, 32)
+#undef DEC_OPT
 }
 
 #define DEC_INST(T, K)                                                                                             \
@@ -747,6 +1074,8 @@ dec_mlp* mlp_create_impl(uint64_t seed) {
     m->grad.alloc(kMlpNParam);
     m->w1b.alloc(kMlpH * kMlpIn);
     m->w2b.alloc(kMlpH * kMlpH);
+    m->err.alloc(1);
+    DEC_CUDA(cudaMemset(m->err.p, 0, sizeof(int)));
     k_refresh_bf16<<<16, 256>>>(m->master.p, m->w1b.p, m->w2b.p);
     DEC_CHECK_LAUNCH();
     DEC_CUDA(cudaDeviceSynchronize());
@@ -780,11 +1109,36 @@ MlpWeights mlp_weights(const dec_mlp* m) {
   return m->view();
 }
 
+// Reads and clears the tcgen05 kernels' error flag (synchronises the stream).
+void mlp_check_error(const dec_mlp* m, cudaStream_t s) {
+  int h = 0;
+  DEC_CUDA(cudaMemcpyAsync(&h, m->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DEC_CUDA(cudaStreamSynchronize(s));
+  if (h) {
+    DEC_CUDA(cudaMemsetAsync(m->err.p, 0, sizeof(int), s));
+    throw Error(DEC_ERR_TIMEOUT, "mlp: a tcgen05 kernel timed out waiting for its MMA");
+  }
+}
+
+void mlp_set_engine_impl(dec_mlp* m, int engine) {
+  require(m != nullptr, "mlp: null handle");
+  require(engine == 0 || engine == 1, "mlp: engine must be 0 (mma.sync) or 1 (tcgen05)");
+  if (engine == 1) tc5_opt_in_all();  // outside any stream capture
+  m->engine = engine;
+}
+
 void mlp_eval_impl(dec_mlp* m, const float* x, int64_t n, float* y, int tensor_cores, void* stream) {
   require(m != nullptr && n >= 0 && (n == 0 || (x != nullptr && y != nullptr)), "mlp: bad eval arguments");
   require((reinterpret_cast<uintptr_t>(x) & 15) == 0, "mlp: features must be 16-byte aligned");
   if (n == 0) return;
   cudaStream_t s = as_stream(stream);
+  if (tensor_cores == 2) {
+    tc5_opt_in(k_mlp_eval_tc5);
+    k_mlp_eval_tc5<<<tc5_grid((n + kTc5Rows - 1) / kTc5Rows), kTc5Rows, kTc5PadSmem, s>>>(n, x, y, m->view(), m->err.p);
+    DEC_CHECK_LAUNCH();
+    mlp_check_error(m, s);
+    return;
+  }
   if (tensor_cores) k_mlp_eval_tc<<<eval_grid(n), kMlpThreads, 0, s>>>(n, x, y, m->view());
   else k_mlp_eval_cc<<<grid_for(n, 128), 128, 0, s>>>(n, x, y, m->w1b.p, m->w2b.p, m->master.p);
   DEC_CHECK_LAUNCH();

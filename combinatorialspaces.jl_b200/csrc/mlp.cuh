@@ -21,6 +21,8 @@ struct MlpWeights {
   const float* b2;          // 64
   const float* w3;          // 64
   const float* b3;          // 1
+  int engine;               // 0: mma.sync kernels, 1: tcgen05 / TMEM kernels
+  int* err;                 // set by a kernel whose bounded wait timed out
 };
 
 // Features of one vertex sample from its residual and its 1-ring (used by inference and
@@ -62,9 +64,11 @@ struct dec_mlp {
   decb::DArr<float> dyb;      // dL/dy of the backward batch
   decb::DArr<float> gpart;    // per-chunk gradient partials
   decb::DArr<double> lpart, nrm;
+  decb::DArr<int> err;        // device error flag of the tcgen05 kernels
+  int engine = 0;
   decb::MlpWeights view() const {
     return {w1b.p, w2b.p, master.p + decb::kOffB1, master.p + decb::kOffB2, master.p + decb::kOffW3,
-            master.p + decb::kOffB3};
+            master.p + decb::kOffB3, engine, err.p};
   }
 };
 

@@ -1,8 +1,9 @@
 """The learned smoother on the GPU against the oracle.
 
 * Initialisation: Xavier-uniform from the splitmix64 stream of the seed, bit for bit.
-* Inference (tensor cores, mma.sync BF16 / FP32 accumulation) and the CUDA-core forward agree
-  with the oracle's mlp_forward (same BF16 roundings; FP32 against FP64 accumulation).
+* Inference on the tensor cores (mma.sync, and tcgen05 with TMEM accumulators; BF16 operands,
+  FP32 accumulation) and the CUDA-core forward agree with the oracle's mlp_forward (same BF16
+  roundings; FP32 against FP64 accumulation); the two tensor-core engines agree with each other.
 * The backward kernels' parameter gradient agrees with the oracle's mlp_backward, both for
   given (features, dL/dy) and for the full energy-norm training loss on a mesh.
 * The features of a residual field are bit-exact with a float32 numpy statement of them.
@@ -75,7 +76,7 @@ def test_xavier_init_bit_exact(dec):
     assert not np.array_equal(dec.SmootherMLP(5).params, m.params)
 
 
-@pytest.mark.parametrize("tensor_cores", [True, False])
+@pytest.mark.parametrize("tensor_cores", [True, False, 2])
 def test_forward_matches_oracle(O, dec, tensor_cores):
     m = dec.SmootherMLP(4)
     rng = np.random.default_rng(3)
@@ -97,14 +98,33 @@ def test_forward_matches_oracle(O, dec, tensor_cores):
     assert np.median(err) <= 2e-5 * scale
 
 
-def test_jacobi_network_on_tensor_cores(dec):
+@pytest.mark.parametrize("tensor_cores", [1, 2])
+def test_jacobi_network_on_tensor_cores(dec, tensor_cores):
     m = dec.SmootherMLP(4)
     m.params = jacobi_net(np.float32(0.8))
-    x = torch.zeros((100, 16), dtype=torch.float32, device="cuda")
-    x[:, 0] = torch.linspace(-1, 1, 100, device="cuda")
-    y = m.eval(x).cpu().numpy()
+    x = torch.zeros((300, 16), dtype=torch.float32, device="cuda")
+    x[:, 0] = torch.linspace(-1, 1, 300, device="cuda")
+    y = m.eval(x, tensor_cores=tensor_cores).cpu().numpy()
     f0 = x[:, 0].to(torch.bfloat16).float().cpu().numpy()
     np.testing.assert_allclose(y, np.float32(0.8) * f0, rtol=0, atol=1e-7)
+
+
+def test_tcgen05_matches_mma_sync(dec):
+    """Both engines round the same products to BF16 and accumulate in FP32; only the order of
+    the FP32 sums differs, so the outputs agree to a few FP32 ulps of the hidden sums except
+    where a BF16 rounding of a hidden unit flips."""
+    m = dec.SmootherMLP(7)
+    rng = np.random.default_rng(8)
+    for n in (1, 127, 128, 129, 70001):
+        x = torch.tensor(rng.uniform(-1, 1, (n, 16)).astype(np.float32), device="cuda")
+        y1 = m.eval(x, tensor_cores=1).cpu().numpy()
+        y2 = m.eval(x, tensor_cores=2).cpu().numpy()
+        d = np.abs(y1 - y2)
+        scale = max(np.abs(y1).max(), 1e-30)
+        assert d.max() <= 2e-3 * scale
+        assert np.mean(d <= 1e-5 * scale) >= 0.99
+    with pytest.raises(dec.DecError, match="engine"):
+        dec.check(dec.lib().dec_mlp_set_engine(m._h, 2))
 
 
 def test_grad_matches_oracle(O, dec):
@@ -175,7 +195,8 @@ def _learned_sweep(O, p, A, x, b):
     return x + dsc.astype(np.float64) * O.mlp_forward(p, F)
 
 
-def test_learned_vcycle_matches_numpy(O, dec):
+@pytest.mark.parametrize("engine", ["mma", "tcgen05"])
+def test_learned_vcycle_matches_numpy(O, dec, engine):
     coarse = O.icosahedron()
     md = O.build_mg(coarse, 2, O.CIRCUMCENTER, 1.0, 1.0, 3)
     mg = dec.MultigridData(coarse, 2, shift=1.0, center="circumcenter", project_radius=1.0, precision=0,
@@ -184,6 +205,7 @@ def test_learned_vcycle_matches_numpy(O, dec):
     p = mlp.params
     p[OFF_W3:OFF_B3] *= 0.3
     mlp.params = p
+    mlp.set_engine(engine)
     mg.set_smoother_mlp(mlp)
     ops = [csc(md.op(l)).tocsr() for l in range(3)]
     Rs = [csc(md.restriction(l)).tocsr() for l in range(2)]
@@ -261,9 +283,11 @@ def test_trained_network_beats_jacobi(O, dec, trained):
     assert rel_learned < 0.5 * rel_jacobi
 
 
-def test_learned_solve_converges_without_fallback(O, dec, trained):
+@pytest.mark.parametrize("engine", ["mma", "tcgen05"])
+def test_learned_solve_converges_without_fallback(O, dec, trained, engine):
     import scipy.sparse.linalg as spla
     mlp = trained[0]
+    mlp.set_engine(engine)
     coarse = O.icosahedron()
     md = O.build_mg(coarse, 4, O.CIRCUMCENTER, 1.0, 1.0, 3)
     mg = dec.MultigridData(coarse, 4, shift=1.0, center="circumcenter", project_radius=1.0, precision=1,
@@ -279,6 +303,26 @@ def test_learned_solve_converges_without_fallback(O, dec, trained):
     for j in range(2):
         exact = spla.spsolve(A, B[j])
         assert np.linalg.norm(U[j] - exact) / np.linalg.norm(exact) < 1e-7
+    mlp.set_engine("mma")
+
+
+def test_engine_switch_recaptures_cycles(O, dec, trained):
+    """A multigrid object that has captured its cycles with one engine runs the other after
+    set_engine: the two cycle results differ only by the engines' FP32 summation order."""
+    mlp = trained[0]
+    coarse = O.icosahedron()
+    mg = dec.MultigridData(coarse, 4, shift=1.0, center="circumcenter", project_radius=1.0, precision=1,
+                           smoother=3, pre=2, post=2)
+    mg.set_smoother_mlp(mlp)
+    n = mg.n
+    B = torch.tensor(np.stack([uniform(97 + j, n) for j in range(3)]), device="cuda")
+    out = {}
+    for engine in ("mma", "tcgen05", "mma"):
+        mlp.set_engine(engine)
+        out.setdefault(engine, []).append(mg.cycles(torch.zeros_like(B), B, 2).cpu().numpy())
+    np.testing.assert_array_equal(out["mma"][0], out["mma"][1])
+    a, b = out["mma"][0], out["tcgen05"][0]
+    assert np.linalg.norm(a - b) <= 1e-3 * np.linalg.norm(a)
 
 
 def test_diverging_network_falls_back(O, dec):
