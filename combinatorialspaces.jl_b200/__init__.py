@@ -460,6 +460,36 @@ class MultigridData:
             check(st)
         return u, rep
 
+    def solve_host_submit(self, u, b, rtol=1e-8, max_iters=100, use_initial_guess=True):
+        """Pipelined solve_host: enqueues the copies and the solve on the hierarchy's own streams
+        and returns a PendingSolve at once; three may be in flight, so neighbouring solves'
+        host<->device copies overlap each one's compute (pinned torch CPU tensors give the
+        overlap).  u and b must stay alive until PendingSolve.wait()."""
+        nrhs = 1 if b.ndim == 1 else b.shape[0]
+        hp = (lambda a: C.c_void_p(a.data_ptr()) if hasattr(a, "data_ptr") else a.ctypes.data_as(C.c_void_p))
+        t = C.c_uint64()
+        check(lib().dec_mg_solve_host_submit(self._h, hp(u), hp(b), nrhs, rtol, max_iters, int(use_initial_guess),
+                                             C.byref(t)))
+        return PendingSolve(self, t.value, u, b)
+
+
+class PendingSolve:
+    """A submitted host-buffer solve (MultigridData.solve_host_submit)."""
+
+    def __init__(self, mg, ticket, u, b):
+        self.mg, self.ticket, self.u, self.b = mg, ticket, u, b
+        self.report = None
+
+    def wait(self):
+        """Blocks until u holds the solution; returns (u, SolveReport)."""
+        if self.report is None:
+            rep = _capi.SolveReport()
+            st = lib().dec_mg_solve_host_wait(self.mg._h, self.ticket, C.byref(rep))
+            if st not in (_capi.DEC_OK, 4):
+                check(st)
+            self.report = rep
+        return self.u, self.report
+
 
 class Batch:
     """Batched solves over several MultigridData hierarchies (dec_batch_*): each refinement step

@@ -81,6 +81,8 @@ SIGNATURES = {
     "dec_mg_full_multigrid": (I32, [P, P, P, I32, I32, P]),
     "dec_mg_solve": (I32, [P, P, P, I32, F64, I32, C.POINTER(SolveReport), P]),
     "dec_mg_solve_host": (I32, [P, P, P, I32, F64, I32, I32, C.POINTER(SolveReport), P]),
+    "dec_mg_solve_host_submit": (I32, [P, P, P, I32, F64, I32, I32, C.POINTER(C.c_uint64)]),
+    "dec_mg_solve_host_wait": (I32, [P, C.c_uint64, C.POINTER(SolveReport)]),
     "dec_mg_time_kernel": (I32, [P, I32, I32, I32, I32, P, PF64, PF64]),
     "dec_mg_autotune": (I32, [P, I32, I32, P, C.POINTER(C.c_int32)]),
     "dec_mg_set_smoother_mlp": (I32, [P, P]),

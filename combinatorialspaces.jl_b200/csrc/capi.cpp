@@ -246,6 +246,20 @@ dec_status dec_mg_solve_host(dec_mg* mg, double* u, const double* b, int32_t nrh
   return g != DEC_OK ? g : st;
 }
 
+dec_status dec_mg_solve_host_submit(dec_mg* mg, double* u, const double* b, int32_t nrhs, double rtol,
+                                    int32_t max_iters, int32_t use_initial_guess, uint64_t* ticket) {
+  return guard([&] {
+    decb::require(ticket != nullptr, "dec_mg_solve_host_submit: null ticket");
+    *ticket = decb::mg_solve_submit(mg, u, b, nrhs, rtol, max_iters, use_initial_guess != 0);
+  });
+}
+
+dec_status dec_mg_solve_host_wait(dec_mg* mg, uint64_t ticket, dec_solve_report* rep) {
+  dec_status st = DEC_OK;
+  dec_status g = guard([&] { st = decb::mg_solve_wait(mg, ticket, rep); });
+  return g != DEC_OK ? g : st;
+}
+
 dec_status dec_mg_time_kernel(dec_mg* mg, int32_t kernel, int32_t level, int32_t nrhs, int32_t reps, void* stream,
                               double* ms, double* bytes) {
   return guard([&] { decb::mg_time_kernel(mg, kernel, level, nrhs, reps, stream, ms, bytes); });

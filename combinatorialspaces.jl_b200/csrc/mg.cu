@@ -213,6 +213,17 @@ struct SweepPrm {
 
 constexpr int TB = 256;
 
+// State of the refinement loop that runs on the device (graph with a conditional WHILE node).
+struct LoopState {
+  int it;         // refinement steps run
+  int conv;       // every right-hand side reached rtol
+  int nrhs;       // right-hand sides in use (the rest of the panels is padding)
+  int max_iters;
+  double rtol;
+  double worst;   // max_j ||b_j - A u_j|| / ||b_j|| at the last test
+};
+
+
 // Programmatic dependent launch: every kernel of a cycle is launched with the
 // programmatic-serialization attribute, waits for its predecessor's results with
 // griddepcontrol.wait before touching memory, and lets its successor start launching at once.
@@ -700,6 +711,52 @@ __global__ void __launch_bounds__(256) k_reduce_partials(int nblocks, int K, int
   if (threadIdx.x == 0) out[q] = sh[0];
 }
 
+__global__ void k_loop_init(LoopState* st, int nrhs, int max_iters, double rtol) {
+  st->it = 0;
+  st->conv = 0;
+  st->nrhs = nrhs;
+  st->max_iters = max_iters;
+  st->rtol = rtol;
+  st->worst = 0.0;
+}
+
+// The refinement loop's test on the device: the worst relative residual over the right-hand
+// sides (sqrt(r²) / sqrt(b²), sqrt(r²) where b = 0; a non-finite one counts as infinite), then
+// the WHILE node's condition: another step when it is above rtol and max_iters is not reached.
+__global__ void __launch_bounds__(256) k_ir_check(cudaGraphConditionalHandle h, const double* __restrict__ norms,
+                                                  const double* __restrict__ bn2, LoopState* st) {
+  const int nrhs = st->nrhs;
+  double w = 0.0;
+  int bad = 0;
+  for (int j = threadIdx.x; j < nrhs; j += blockDim.x) {
+    const double bn = sqrt(bn2[j]);
+    const double rel = bn > 0 ? sqrt(norms[j]) / bn : sqrt(norms[j]);
+    if (!isfinite(rel)) bad = 1;
+    else w = fmax(w, rel);
+  }
+  __shared__ double sw[256];
+  __shared__ int sb[256];
+  sw[threadIdx.x] = w;
+  sb[threadIdx.x] = bad;
+  __syncthreads();
+  for (int k = 128; k > 0; k >>= 1) {
+    if (threadIdx.x < k) {
+      sw[threadIdx.x] = fmax(sw[threadIdx.x], sw[threadIdx.x + k]);
+      sb[threadIdx.x] |= sb[threadIdx.x + k];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double worst = sb[0] ? HUGE_VAL : sw[0];
+    st->worst = worst;
+    const bool conv = worst <= st->rtol;
+    st->conv = conv ? 1 : 0;
+    const bool more = !conv && st->it < st->max_iters;
+    if (more) ++st->it;
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+  }
+}
+
 // Per-block partial sums of x² per right-hand side over the panels (same layout as k_residual64).
 template <int K>
 __global__ void __launch_bounds__(TB) k_panel_sumsq(int n, const double* __restrict__ x, double* __restrict__ partial,
@@ -1017,6 +1074,11 @@ struct Workspace {
   DArr<double> partial, norms;
   DArr<double> scal;          // CG smoother: per-right-hand-side scalars (CgField x K*npanels)
   DArr<double> ucm, bcm;      // column-major device copies for host-buffer solves
+  DArr<double> pu[3], pb[3];  // staging slots of pipelined host-buffer solves
+  DArr<double> bn2;           // ||b_j||² (device refinement loop)
+  DArr<LoopState> loop;       // device refinement loop state
+  cudaGraphExec_t solve_graph = nullptr;  // the whole refinement loop (Jacobi / Chebyshev)
+  int64_t solve_pre = 0, solve_body = 0;  // kernel nodes before / inside its loop
   int nblocks = 0;
   DArr<double> Ubak;          // learned smoother: the iterate before a refinement step
   DArr<double> cs64;          // coarse_solver 2: per-RHS total shifts (K * npanels)
@@ -1031,6 +1093,8 @@ struct Workspace {
       if (g) cudaGraphExecDestroy(g);
       g = nullptr;
     }
+    if (solve_graph) cudaGraphExecDestroy(solve_graph);
+    solve_graph = nullptr;
   }
   ~Workspace() { drop_graphs(); }
 };
@@ -1050,8 +1114,30 @@ struct dec_mg {
   uint64_t epoch = 0;              // bumped whenever workspaces or their graphs are dropped
   bool force_plain = false;        // set while capturing the plain-smoother fallback cycle
   int mlp_engine = -1;             // kernel engine of the network when the graphs were captured
+  // Pipelined host-buffer solves (submit / wait): copy-in, compute and copy-out streams, per
+  // staging slot the events start, copied in, computed, copied out, and the loop state read back.
+  static constexpr int kSlots = 3;
+  cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t pev[kSlots][4] = {};
+  decb::LoopState* hstate = nullptr;  // pinned, one per slot
+  struct Pending {
+    bool active = false;
+    uint64_t ticket = 0;
+    decb::Workspace* w = nullptr;
+    int nrhs = 0;
+    bool guess = false;
+  } pend[kSlots];
+  uint64_t next_ticket = 1;
   ~dec_mg() {
+    for (cudaStream_t p : pipe)
+      if (p) cudaStreamSynchronize(p);
     ws.clear();
+    for (auto& sl : pev)
+      for (cudaEvent_t e : sl)
+        if (e) cudaEventDestroy(e);
+    for (cudaStream_t p : pipe)
+      if (p) cudaStreamDestroy(p);
+    if (hstate) cudaFreeHost(hstate);
     if (cap) cudaStreamDestroy(cap);
   }
 };
@@ -1737,7 +1823,12 @@ static int64_t count_kernel_nodes(cudaGraph_t g) {
   int64_t k = 0;
   for (auto nd : nodes) {
     cudaGraphNodeType t;
-    DEC_CUDA(cudaGraphNodeGetType(nd, &t));
+    if (cudaGraphNodeGetType(nd, &t) != cudaSuccess) {
+      // the CUDA 12.9 runtime on a CUDA 13 driver does not name a conditional node's type; the
+      // error is not sticky and the node is not a kernel
+      (void)cudaGetLastError();
+      continue;
+    }
     if (t == cudaGraphNodeTypeKernel) ++k;
   }
   return k;
@@ -1767,7 +1858,14 @@ static cudaGraphExec_t capture(dec_mg& mg, Workspace& w, int kind) {
   return ex;
 }
 
-static Workspace& workspace_k(dec_mg& mg, int nrhs, int prec, int K) {
+// Waits for the pipelined host-buffer solves still running on the hierarchy's workspaces.
+static void drain_pipeline(dec_mg& mg) {
+  for (cudaStream_t p : mg.pipe)
+    if (p) DEC_CUDA(cudaStreamSynchronize(p));
+}
+
+static Workspace& workspace_k(dec_mg& mg, int nrhs, int prec, int K, bool drain = true) {
+  if (drain) drain_pipeline(mg);
   if (mg.mlp && mg.mlp->engine != mg.mlp_engine) {  // captured cycles hold the other engine's kernels
     for (auto& kv : mg.ws) kv.second->drop_graphs();
     ++mg.epoch;
@@ -1819,8 +1917,120 @@ static Workspace& workspace_k(dec_mg& mg, int nrhs, int prec, int K) {
   return ref;
 }
 
-static Workspace& workspace(dec_mg& mg, int nrhs, int prec) {
-  return workspace_k(mg, nrhs, prec, choose_k(mg, nrhs, prec));
+static Workspace& workspace(dec_mg& mg, int nrhs, int prec, bool drain = true) {
+  return workspace_k(mg, nrhs, prec, choose_k(mg, nrhs, prec), drain);
+}
+
+// ||b_j||² of the FP64 right-hand-side panels into `out` (K * npanels).
+static void enqueue_bnorms(const dec_mg& mg, Workspace& w, cudaStream_t s, double* out) {
+  const int n = mg.lv[0].n, K = w.K, np = w.npanels;
+  dim3 g(w.nblocks, np);
+  switch (K) {
+#define DEC_K(KK) \
+  case KK: k_panel_sumsq<KK><<<g, TB, 0, s>>>(n, w.B64.p, w.partial.p, (size_t)n * KK); break;
+    DEC_K(1) DEC_K(2) DEC_K(4) DEC_K(8) DEC_K(16) DEC_K(32)
+#undef DEC_K
+  }
+  k_reduce_partials<<<K * np, 256, 0, s>>>(w.nblocks, K, np, w.partial.p, out);
+  DEC_CHECK_LAUNCH();
+}
+
+// e = 0 on the finest level (the correction the first refinement step adds).
+static void zero_correction(const dec_mg& mg, Workspace& w, cudaStream_t s) {
+  const size_t total = (size_t)mg.lv[0].n * w.K * w.npanels;
+  if (w.prec == 2) DEC_CUDA(cudaMemsetAsync(w.f16[0].x.p, 0, total * sizeof(__half), s));
+  else if (w.prec == 1) DEC_CUDA(cudaMemsetAsync(w.f32[0].x.p, 0, total * sizeof(float), s));
+  else DEC_CUDA(cudaMemsetAsync(w.f64[0].x.p, 0, total * sizeof(double), s));
+}
+
+// The whole refinement loop of a Jacobi / Chebyshev solve as one graph, from the FP64 panels
+// (B64, U64) and the loop state (k_loop_init):
+//   ||b||²; e = 0; [u += e; r = b - A u; test]; WHILE (test): { e = V^c(r); u += e; r = b - A u; test }
+// The test (k_ir_check) sets the WHILE node's condition, so the solve needs no host round trip.
+static void capture_solve(dec_mg& mg, Workspace& w) {
+  if (w.bn2.n < (size_t)w.K * w.npanels) w.bn2.alloc((size_t)w.K * w.npanels);
+  if (!w.loop.p) w.loop.alloc(1);
+  cudaGraph_t g = nullptr;
+  DEC_CUDA(cudaGraphCreate(&g, 0));
+  auto fail = [&]() {
+    cudaGraph_t junk = nullptr;
+    cudaStreamCaptureStatus cs;
+    if (cudaStreamIsCapturing(mg.cap, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+      cudaStreamEndCapture(mg.cap, &junk);
+    cudaGraphDestroy(g);
+  };
+  try {
+    cudaGraphConditionalHandle h;
+    DEC_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+    DEC_CUDA(cudaStreamBeginCaptureToGraph(mg.cap, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    enqueue_bnorms(mg, w, mg.cap, w.bn2.p);
+    zero_correction(mg, w, mg.cap);
+    dispatch(mg, w, mg.cap, G_RESID);
+    k_ir_check<<<1, 256, 0, mg.cap>>>(h, w.norms.p, w.bn2.p, w.loop.p);
+    DEC_CHECK_LAUNCH();
+    cudaStreamCaptureStatus st;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    DEC_CUDA(cudaStreamGetCaptureInfo(mg.cap, &st, nullptr, &cg, &deps, &ndeps));
+    cudaGraphNodeParams prm = {};
+    prm.type = cudaGraphNodeTypeConditional;
+    prm.conditional.handle = h;
+    prm.conditional.type = cudaGraphCondTypeWhile;
+    prm.conditional.size = 1;
+    cudaGraphNode_t loop_node;
+    DEC_CUDA(cudaGraphAddNode(&loop_node, cg, deps, ndeps, &prm));
+    DEC_CUDA(cudaStreamUpdateCaptureDependencies(mg.cap, &loop_node, 1, cudaStreamSetCaptureDependencies));
+    DEC_CUDA(cudaStreamEndCapture(mg.cap, &g));
+    cudaGraph_t body = prm.conditional.phGraph_out[0];
+    DEC_CUDA(cudaStreamBeginCaptureToGraph(mg.cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    dispatch(mg, w, mg.cap, G_VCYCLE);
+    dispatch(mg, w, mg.cap, G_RESID);
+    k_ir_check<<<1, 256, 0, mg.cap>>>(h, w.norms.p, w.bn2.p, w.loop.p);
+    DEC_CHECK_LAUNCH();
+    DEC_CUDA(cudaStreamEndCapture(mg.cap, &body));
+    w.solve_pre = count_kernel_nodes(g);
+    w.solve_body = count_kernel_nodes(body);
+    cudaGraphExec_t ex = nullptr;
+    DEC_CUDA(cudaGraphInstantiate(&ex, g, 0));
+    w.solve_graph = ex;
+  } catch (...) {
+    fail();
+    throw;
+  }
+  cudaGraphDestroy(g);
+}
+
+// Panels in (b, and u or zero), the loop graph, panels out: the device part of a Jacobi /
+// Chebyshev solve, enqueued on s (bd / ud device column-major).
+static void enqueue_solve(dec_mg& mg, Workspace& w, const double* bd, double* ud, int nrhs, double rtol,
+                          int max_iters, bool use_initial_guess, cudaStream_t s) {
+  const Level& F = mg.lv[0];
+  const int n = F.n, K = w.K, np = w.npanels;
+  const size_t total = (size_t)n * K * np;
+  if (!w.solve_graph) capture_solve(mg, w);
+  k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, K, np, F.dperm.p, bd, w.B64.p);
+  if (use_initial_guess)
+    k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, K, np, F.dperm.p, ud, w.U64.p);
+  else
+    DEC_CUDA(cudaMemsetAsync(w.U64.p, 0, total * sizeof(double), s));
+  k_loop_init<<<1, 1, 0, s>>>(w.loop.p, nrhs, max_iters, rtol);
+  DEC_CHECK_LAUNCH();
+  DEC_CUDA(cudaGraphLaunch(w.solve_graph, s));
+  k_from_panels<double, double><<<grid_for((long long)n * nrhs, 256), 256, 0, s>>>(n, nrhs, K, F.diperm.p, w.U64.p, ud);
+  DEC_CHECK_LAUNCH();
+}
+
+static void fill_report(const Workspace& w, const LoopState& st, bool guess, float ms, dec_solve_report* rep) {
+  if (!rep) return;
+  rep->iterations = st.it;
+  rep->converged = st.conv;
+  rep->max_rel_residual = st.worst;
+  rep->seconds = ms * 1e-3;
+  // to_panels (b, and u), loop init, the graph's kernels, from_panels
+  rep->launches = (guess ? 2 : 1) + 1 + w.solve_pre + (int64_t)st.it * w.solve_body + 1;
+  rep->rhs_block = w.K;
+  rep->fallback_iteration = -1;
 }
 
 // coarse_solver 2: RHS j gets the operator L + (shift + c_j) I (c_j = 0 without `shifts`).
@@ -1957,6 +2167,21 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
     bd = w.bcm.p;
     ud = w.ucm.p;
   }
+  if (mg->opt.smoother != DEC_SMOOTH_LEARNED) {  // the refinement loop runs on the device
+    enqueue_solve(*mg, w, bd, ud, nrhs, rtol, max_iters, use_initial_guess, s);
+    if (host_buffers) DEC_CUDA(cudaMemcpyAsync(u, ud, (size_t)n * nrhs * 8, cudaMemcpyDeviceToHost, s));
+    DEC_CUDA(cudaEventRecord(e1, s));
+    LoopState st;
+    DEC_CUDA(cudaMemcpyAsync(&st, w.loop.p, sizeof(LoopState), cudaMemcpyDeviceToHost, s));
+    DEC_CUDA(cudaEventSynchronize(e1));
+    DEC_CUDA(cudaStreamSynchronize(s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    fill_report(w, st, use_initial_guess, ms, rep);
+    return st.conv ? DEC_OK : DEC_ERR_NOT_CONVERGED;
+  }
   k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, K, np, F.dperm.p, bd, w.B64.p);
   if (use_initial_guess)
     k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, K, np, F.dperm.p, ud, w.U64.p);
@@ -2053,6 +2278,79 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
     rep->fallback_iteration = fallback_at;
   }
   return conv ? DEC_OK : DEC_ERR_NOT_CONVERGED;
+}
+
+// Pipelined host-buffer solves.  Submit enqueues, on the hierarchy's own streams, the copy of b
+// (and u) into the ticket's staging slot, the device solve (panels, loop graph, panels) and the
+// copy of u back, and returns; three tickets may be in flight, so the copies of the solves
+// before and after one overlap its compute.  Wait blocks on the ticket's copy-out and returns
+// its report.
+static void ensure_pipeline(dec_mg& mg) {
+  if (mg.pipe[0]) return;
+  for (cudaStream_t& p : mg.pipe) DEC_CUDA(cudaStreamCreateWithFlags(&p, cudaStreamNonBlocking));
+  for (auto& sl : mg.pev)
+    for (cudaEvent_t& e : sl) DEC_CUDA(cudaEventCreate(&e));
+  DEC_CUDA(cudaMallocHost(&mg.hstate, dec_mg::kSlots * sizeof(LoopState)));
+}
+
+uint64_t mg_solve_submit(dec_mg* mg, double* u, const double* b, int nrhs, double rtol, int max_iters,
+                         bool use_initial_guess) {
+  require(mg != nullptr && u != nullptr && b != nullptr, "multigrid: null argument");
+  require(nrhs >= 1 && max_iters >= 1 && rtol > 0, "multigrid: bad nrhs / max_iters / rtol");
+  require(mg->opt.smoother != DEC_SMOOTH_LEARNED,
+          "multigrid: pipelined solves run the Jacobi or Chebyshev smoother (the learned smoother's "
+          "fallback test runs on the host)");
+  const uint64_t ticket = mg->next_ticket;
+  const int slot = (int)(ticket % dec_mg::kSlots);
+  require(!mg->pend[slot].active, "multigrid: three pipelined solves are in flight; wait for the oldest one first");
+  ensure_pipeline(*mg);
+  cudaStream_t hin = mg->pipe[0], comp = mg->pipe[1], hout = mg->pipe[2];
+  Workspace& w = workspace(*mg, nrhs, mg->opt.precision, false);
+  set_shifts(*mg, w, nullptr, nrhs, comp);
+  if (!w.solve_graph) capture_solve(*mg, w);
+  const size_t len = (size_t)mg->lv[0].n * nrhs;
+  DArr<double>& bs = w.pb[slot];
+  DArr<double>& us = w.pu[slot];
+  if (bs.n < len || us.n < len) {
+    DEC_CUDA(cudaStreamSynchronize(comp));  // other slots' solves may still read the workspace
+    if (bs.n < len) bs.alloc(len);
+    if (us.n < len) us.alloc(len);
+  }
+  cudaEvent_t* ev = mg->pev[slot];
+  DEC_CUDA(cudaEventRecord(ev[0], hin));
+  DEC_CUDA(cudaMemcpyAsync(bs.p, b, len * 8, cudaMemcpyHostToDevice, hin));
+  if (use_initial_guess) DEC_CUDA(cudaMemcpyAsync(us.p, u, len * 8, cudaMemcpyHostToDevice, hin));
+  DEC_CUDA(cudaEventRecord(ev[1], hin));
+  DEC_CUDA(cudaStreamWaitEvent(comp, ev[1], 0));
+  enqueue_solve(*mg, w, bs.p, us.p, nrhs, rtol, max_iters, use_initial_guess, comp);
+  DEC_CUDA(cudaMemcpyAsync(mg->hstate + slot, w.loop.p, sizeof(LoopState), cudaMemcpyDeviceToHost, comp));
+  DEC_CUDA(cudaEventRecord(ev[2], comp));
+  DEC_CUDA(cudaStreamWaitEvent(hout, ev[2], 0));
+  DEC_CUDA(cudaMemcpyAsync(u, us.p, len * 8, cudaMemcpyDeviceToHost, hout));
+  DEC_CUDA(cudaEventRecord(ev[3], hout));
+  auto& pd = mg->pend[slot];
+  pd.active = true;
+  pd.ticket = ticket;
+  pd.w = &w;
+  pd.nrhs = nrhs;
+  pd.guess = use_initial_guess;
+  ++mg->next_ticket;
+  return ticket;
+}
+
+dec_status mg_solve_wait(dec_mg* mg, uint64_t ticket, dec_solve_report* rep) {
+  require(mg != nullptr, "multigrid: null argument");
+  const int slot = (int)(ticket % dec_mg::kSlots);
+  auto& pd = mg->pend[slot];
+  require(pd.active && pd.ticket == ticket, "multigrid: unknown or already collected ticket");
+  pd.active = false;
+  cudaEvent_t* ev = mg->pev[slot];
+  DEC_CUDA(cudaEventSynchronize(ev[3]));
+  const LoopState st = mg->hstate[slot];
+  float ms = 0;
+  DEC_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[3]));
+  fill_report(*pd.w, st, pd.guess, ms, rep);
+  return st.conv ? DEC_OK : DEC_ERR_NOT_CONVERGED;
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -15,6 +15,9 @@ void mg_full_multigrid(dec_mg* mg, double* u, const double* b, int nrhs, int cyc
 dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rtol, int max_iters,
                     dec_solve_report* rep, void* stream, bool host_buffers, bool use_initial_guess,
                     const double* shifts = nullptr);
+uint64_t mg_solve_submit(dec_mg* mg, double* u, const double* b, int nrhs, double rtol, int max_iters,
+                         bool use_initial_guess);
+dec_status mg_solve_wait(dec_mg* mg, uint64_t ticket, dec_solve_report* rep);
 void mg_time_kernel(dec_mg* mg, int kernel, int level, int nrhs, int reps, void* stream, double* ms,
                     double* bytes);
 int mg_autotune(dec_mg* mg, int nrhs, int reps, void* stream);

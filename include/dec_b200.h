@@ -231,6 +231,17 @@ dec_status dec_mg_solve_host(dec_mg* mg, double* u_host, const double* b_host, i
                              int32_t max_iters, int32_t use_initial_guess, dec_solve_report* report,
                              void* stream);
 
+/* Pipelined form of dec_mg_solve_host (Jacobi / Chebyshev smoothers): submit enqueues the copy of
+ * b_host (and u_host) to the device, the solve and the copy of u back on the hierarchy's own
+ * streams and returns a ticket at once; wait blocks until u_host holds the ticket's solution and
+ * returns its report (seconds: first copy in to last copy out).  Three tickets may be in flight,
+ * so the copies of neighbouring solves overlap each solve's compute; the host buffers must stay
+ * valid (and, for the overlap, pinned) until the wait.  Other calls on the hierarchy first wait
+ * for the pipeline. */
+dec_status dec_mg_solve_host_submit(dec_mg* mg, double* u_host, const double* b_host, int32_t nrhs, double rtol,
+                                    int32_t max_iters, int32_t use_initial_guess, uint64_t* ticket);
+dec_status dec_mg_solve_host_wait(dec_mg* mg, uint64_t ticket, dec_solve_report* report);
+
 /* dec_mg_solve with a shift per right-hand side (coarse_solver 2): RHS j solves
  * (L + (shift + shifts[j]) I) u_j = b_j; shifts is a host array of nrhs values (total shifts must
  * be positive). */

@@ -155,6 +155,73 @@ def test_host_buffer_solve_matches_device(dec, built):
     np.testing.assert_array_equal(Uh, Ud.cpu().numpy())
 
 
+def test_device_refinement_loop_steps(O, dec, built):
+    """The refinement loop runs on the device (a graph whose WHILE node the residual test sets):
+    the step count it reports is the first k at which a k-step solve meets rtol, a capped solve
+    reports not-converged with the residual of the u it returns, and b = 0 needs no step."""
+    coarse, md, _ = built["ico4_circum"]
+    mg = dec.MultigridData(coarse, 4, shift=1.0, center="circumcenter", project_radius=1.0, precision=1)
+    n = mg.n
+    A = csc(md.op(0)).tocsc()
+    B = np.stack([uniform(150 + j, n) for j in range(3)])
+    Bd = torch.tensor(B, device="cuda")
+    rtol = 1e-9
+    U, rep = mg.solve(torch.zeros_like(Bd), Bd, rtol=rtol, max_iters=60)
+    assert rep.converged == 1 and rep.iterations >= 2
+    worst = []
+    for k in range(1, rep.iterations + 1):
+        Uk, rk = mg.solve(torch.zeros_like(Bd), Bd, rtol=rtol, max_iters=k)
+        Uk = Uk.cpu().numpy()
+        rel = max(np.linalg.norm(B[j] - A @ Uk[j]) / np.linalg.norm(B[j]) for j in range(3))
+        assert rk.iterations == k
+        assert rk.max_rel_residual == pytest.approx(rel, rel=1e-6)
+        assert rk.converged == (1 if k == rep.iterations else 0)
+        worst.append(rel)
+    assert all(w > rtol for w in worst[:-1]) and worst[-1] <= rtol * 1.0001
+    np.testing.assert_array_equal(Uk, U.cpu().numpy())
+    Z, rz = mg.solve(torch.zeros_like(Bd), torch.zeros_like(Bd), rtol=rtol)
+    assert rz.converged == 1 and rz.iterations == 0 and rz.max_rel_residual == 0.0
+    assert float(Z.abs().max()) == 0.0
+
+
+def test_pipelined_host_solves_match_synchronous(dec, built):
+    """solve_host_submit / wait: three solves in flight on the hierarchy's own streams give the
+    same bits as the synchronous host-buffer solve; a fourth submit before a wait, a second wait on
+    a ticket and the learned smoother are refused."""
+    coarse, md, _ = built["ico4_circum"]
+    mg = dec.MultigridData(coarse, 4, shift=1.0, center="circumcenter", project_radius=1.0, precision=1)
+    n = mg.n
+    sizes = [2, 3, 2, 1, 4]
+    Bs = [torch.tensor(np.stack([uniform(700 + 10 * q + j, n) for j in range(m)])).pin_memory()
+          for q, m in enumerate(sizes)]
+    Us = [torch.zeros_like(B).pin_memory() for B in Bs]
+    p0 = mg.solve_host_submit(Us[0], Bs[0], rtol=1e-9, use_initial_guess=False)
+    p1 = mg.solve_host_submit(Us[1], Bs[1], rtol=1e-9, use_initial_guess=False)
+    p2 = mg.solve_host_submit(Us[2], Bs[2], rtol=1e-9, use_initial_guess=False)
+    with pytest.raises(dec.DecError, match="in flight"):
+        mg.solve_host_submit(Us[3], Bs[3])
+    _, r0 = p0.wait()
+    p3 = mg.solve_host_submit(Us[3], Bs[3], rtol=1e-9, use_initial_guess=False)
+    _, r1 = p1.wait()
+    p4 = mg.solve_host_submit(Us[4], Bs[4], rtol=1e-9, use_initial_guess=False)
+    reps = [r0, r1, p2.wait()[1], p3.wait()[1], p4.wait()[1]]
+    with pytest.raises(dec.DecError, match="ticket"):
+        rep = dec._capi.SolveReport()
+        dec.check(dec.lib().dec_mg_solve_host_wait(mg._h, p4.ticket, dec._capi.C.byref(rep)))
+    for q, m in enumerate(sizes):
+        ref = np.zeros((m, n))
+        _, rr = mg.solve_host(ref, Bs[q].numpy(), rtol=1e-9, use_initial_guess=False)
+        np.testing.assert_array_equal(Us[q].numpy(), ref)
+        assert reps[q].converged == 1 and reps[q].iterations == rr.iterations
+        assert reps[q].max_rel_residual == rr.max_rel_residual and reps[q].seconds > 0
+    # starting from the solution: no refinement step
+    _, rg = mg.solve_host_submit(Us[0], Bs[0], rtol=1e-9, use_initial_guess=True).wait()
+    assert rg.converged == 1 and rg.iterations == 0
+    learned = dec.MultigridData(coarse, 2, shift=1.0, center="circumcenter", project_radius=1.0, smoother=3)
+    with pytest.raises(dec.DecError, match="learned"):
+        learned.solve_host_submit(np.zeros(learned.n), np.ones(learned.n))
+
+
 def test_singular_coarse_operator_is_reported(O, dec):
     coarse = O.icosahedron()
     with pytest.raises(dec.DecError, match="singular"):
