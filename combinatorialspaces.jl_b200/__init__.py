@@ -210,6 +210,28 @@ def dec_wedge_product_dd(m, n, sd, dtype="float64"):
     return WedgePlan(sd, _capi.DEC_WEDGE_DD, m, n, dtype)
 
 
+def dec_c_wedge_product(j, k, a, b, p, c, n_out, out=None, index_base=0):
+    """dec_c_wedge_product!(Val(j), Val(k), res, α, β, p, c) (FastDEC.jl:217-232): the wedge kernel
+    on caller caches (the reference's cache_wedge matrices; p an int32 CUDA tensor, c a CUDA tensor
+    of the forms' dtype or None for (0,1)), for (0,1), (0,2), (0,3), (1,1) and (2,1).  p, c are
+    passed in Julia's column-major order: a (R, n_out) torch tensor's transpose-contiguous layout,
+    i.e. shape (n_out, R) row-major (for (0,1): shape (2, n_out))."""
+    torch = _torch()
+    code = _dtype_code(a.dtype)
+    if out is None:
+        out = torch.empty(n_out, dtype=a.dtype, device=a.device)
+    for t, what in ((a, "α"), (b, "β"), (out, "result")):
+        if t.dtype != a.dtype or not t.is_contiguous():
+            raise ValueError(f"c_wedge: {what} must be contiguous {a.dtype}")
+    if p.dtype != torch.int32 or not p.is_contiguous():
+        raise ValueError("c_wedge: p must be a contiguous int32 tensor")
+    if c is not None and (c.dtype != a.dtype or not c.is_contiguous()):
+        raise ValueError("c_wedge: c must be a contiguous tensor of the forms' dtype")
+    check(lib().dec_c_wedge_apply(j, k, n_out, _ptr(p), _ptr(c) if c is not None else None, code, _ptr(a),
+                                  _ptr(b), _ptr(out), index_base, _stream()))
+    return out
+
+
 # ---- operators ------------------------------------------------------------------------------
 
 class Operator:
@@ -322,6 +344,78 @@ def laplace_beltrami(sd, dtype="float64"):
 def helmholtz(sd, shift, dtype="float64"):
     """laplace_beltrami(sd) + shift * I."""
     return Operator(sd, _capi.DEC_OP_HELMHOLTZ0, dtype, shift=shift)
+
+
+def flat_sharp(sd, dtype="float64"):
+    """♭♯_mat(sd) (DiscreteExteriorCalculus.jl:1992): dual 1-form -> primal 1-form, as an operator."""
+    return Operator(sd, _capi.DEC_OP_FLAT_SHARP, dtype)
+
+
+# ---- dual-dual interior product, Lie derivative and dual Laplacians (2D) ----------------------
+# The reference composes these from its operators (FastDEC.jl:762-853); so does this mirror, with
+# every factor a device operator of this library.  GeometricHodge throughout: ⋆1 is the sparse
+# geometric star and its inverse the (-⋆1)⁻¹ Krylov solve; ⋆0, ⋆2 and their inverses are diagonal.
+
+def _diag(v):
+    return lambda x: v * x
+
+
+def interior_product_dd(m, n, sd):
+    """interior_product_dd(Val(m), Val(n), sd) (FastDEC.jl:765-790), FP64.
+    (1,1): (f, g) -> ⋆2 ∧pd11(⋆1⁻¹ g, f), dual 1-forms f, g -> dual 0-form.
+    (1,2): (f, g) -> ⋆1 ♭♯ ((Λpd01 (⋆0⁻¹ g)) .* f), dual 1-form f, dual 2-form g -> dual 1-form."""
+    if (m, n) == (1, 1):
+        ihs1 = hodge_operator(1, sd, inverse=True, hodge="geometric")
+        w11 = dec_wedge_product_pd(1, 1, sd)
+        hs2 = _diag(dec_hodge_star(2, sd))
+        return lambda f, g: hs2(w11(ihs1(g), f))
+    if (m, n) == (1, 2):
+        ihs0 = _diag(dec_inv_hodge_star(0, sd))
+        hs1 = hodge_operator(1, sd, hodge="geometric")
+        fs = flat_sharp(sd)
+        w01 = dec_wedge_product_pd(0, 1, sd)  # (g, f) -> (Λpd01 g) .* f
+        return lambda f, g: hs1(fs(w01(ihs0(g), f)))
+    raise ValueError(f"interior_product_dd: unsupported degrees ({m}, {n})")
+
+
+def lie_derivative_dd(m, n, sd):
+    """ℒ_dd(Val(1), Val(1), sd) (FastDEC.jl:795-802): (f, g) -> -(dd0 i1(f, g)) - i2(f, dd1 g), with
+    i1 = interior_product_dd(1, 1), i2 = interior_product_dd(1, 2), ddk the dual derivatives."""
+    if (m, n) != (1, 1):
+        raise ValueError(f"lie_derivative_dd: unsupported degrees ({m}, {n})")
+    dd0, dd1 = dec_dual_derivative(0, sd), dec_dual_derivative(1, sd)
+    i1, i2 = interior_product_dd(1, 1, sd), interior_product_dd(1, 2, sd)
+
+    def lie(f, g):
+        a = dd0(i1(f, g))
+        b = i2(f, dd1(g))
+        return -a - b
+    return lie
+
+
+ℒ_dd = lie_derivative_dd
+
+
+def dual_laplacian(k, sd):
+    """Δᵈ(Val(k), sd) on a 2D complex (FastDEC.jl:812-853), FP64.
+    k = 0: x -> ⋆2 d1 ⋆1⁻¹ (dd0 x) (dual 0-forms, length nt).
+    k = 1: x -> ⋆1 d0 ⋆0⁻¹ dd1 x + dd0 ⋆2 d1 ⋆1⁻¹ x (dual 1-forms, length ne)."""
+    dd0 = dec_dual_derivative(0, sd)
+    ihs1 = hodge_operator(1, sd, inverse=True, hodge="geometric")
+    d1 = dec_differential(1, sd)
+    hs2 = _diag(dec_hodge_star(2, sd))
+    if k == 0:
+        return lambda x: hs2(d1(ihs1(dd0(x))))
+    if k == 1:
+        dd1 = dec_dual_derivative(1, sd)
+        ihs0 = _diag(dec_inv_hodge_star(0, sd))
+        d0 = dec_differential(0, sd)
+        hs1 = hodge_operator(1, sd, hodge="geometric")
+        return lambda x: hs1(d0(ihs0(dd1(x)))) + dd0(hs2(d1(ihs1(x))))
+    raise ValueError(f"dual_laplacian: unsupported degree {k}")
+
+
+Δᵈ = dual_laplacian
 
 
 # ---- multigrid ------------------------------------------------------------------------------
@@ -650,6 +744,22 @@ def full_multigrid(b, md, cycles):
     nrhs = 1 if b.dim() == 1 else b.shape[0]
     check(lib().dec_mg_full_multigrid(md._h, _ptr(u), _ptr(b.contiguous()), nrhs, cycles, _stream()))
     return u
+
+
+def dec_inverse_laplacian(k, coarse, levels, steps=3, cycles=5, mu=2, center="circumcenter", project_radius=0.0):
+    """dec_Δ⁻¹(Val(0), s; scheme=BinarySubdivision(), steps=3, cycles=5, alg=cg, μ=2)
+    (FastDEC.jl:866-869): a hierarchy of `levels` binary subdivisions of `coarse` with the
+    Laplacian ∇²(0) on every level and the reference's CG smoother, returned as
+    b -> full_multigrid(b, md, cycles, cg, μ).  The hierarchy is the closure's `md`."""
+    if k != 0:
+        raise ValueError("dec_inverse_laplacian: only 0-forms (Val(0))")
+    md = MultigridData(coarse, levels, shift=0.0, center=center, project_radius=project_radius,
+                       smoother=_capi.DEC_SMOOTH_CG, pre=steps, post=steps, mu=mu, precision=0)
+
+    def solve(b):
+        return full_multigrid(b, md, cycles)
+    solve.md = md
+    return solve
 
 
 def multigrid_wcycles(u, b, md, cycles):

@@ -13,7 +13,8 @@ DEC_BARYCENTER, DEC_CIRCUMCENTER = 0, 1
 DEC_WEDGE_PP, DEC_WEDGE_PD, DEC_WEDGE_DP, DEC_WEDGE_DD = 0, 1, 2, 3
 (DEC_OP_D0, DEC_OP_D1, DEC_OP_BOUNDARY1, DEC_OP_BOUNDARY2, DEC_OP_DUAL_D0, DEC_OP_DUAL_D1,
  DEC_OP_STAR0, DEC_OP_STAR1, DEC_OP_STAR2, DEC_OP_INV_STAR0, DEC_OP_INV_STAR1, DEC_OP_INV_STAR2,
- DEC_OP_LAPLACE0, DEC_OP_HELMHOLTZ0, DEC_OP_STAR1_GEOMETRIC, DEC_OP_INV_STAR1_GEOMETRIC) = range(16)
+ DEC_OP_LAPLACE0, DEC_OP_HELMHOLTZ0, DEC_OP_STAR1_GEOMETRIC, DEC_OP_INV_STAR1_GEOMETRIC,
+ DEC_OP_FLAT_SHARP) = range(17)
 DEC_GEOM_LENGTH, DEC_GEOM_AREA, DEC_GEOM_DUAL_AREA, DEC_GEOM_DUAL_LENGTH_TE, DEC_GEOM_DUAL_POINT = range(5)
 DEC_SMOOTH_JACOBI, DEC_SMOOTH_CHEBYSHEV, DEC_SMOOTH_CG, DEC_SMOOTH_LEARNED = 0, 1, 2, 3
 DEC_KERNEL_SWEEP, DEC_KERNEL_RESIDUAL, DEC_KERNEL_RESTRICT, DEC_KERNEL_PROLONG, DEC_KERNEL_MLP = range(5)
@@ -81,6 +82,7 @@ SIGNATURES = {
     "dec_mg_full_multigrid": (I32, [P, P, P, I32, I32, P]),
     "dec_mg_solve": (I32, [P, P, P, I32, F64, I32, C.POINTER(SolveReport), P]),
     "dec_mg_solve_host": (I32, [P, P, P, I32, F64, I32, I32, C.POINTER(SolveReport), P]),
+    "dec_c_wedge_apply": (I32, [I32, I32, I64, P, P, I32, P, P, P, I32, P]),
     "dec_mg_solve_host_submit": (I32, [P, P, P, I32, F64, I32, I32, C.POINTER(C.c_uint64)]),
     "dec_mg_solve_host_wait": (I32, [P, C.c_uint64, C.POINTER(SolveReport)]),
     "dec_mg_time_kernel": (I32, [P, I32, I32, I32, I32, P, PF64, PF64]),

@@ -15,6 +15,8 @@ dec_wedge_plan* wedge_plan_create_impl(dec_mesh* mh, int kind, int da, int db, d
 void wedge_apply_impl(dec_wedge_plan* P, const void* a, const void* b, void* out, int count, void* stream);
 void wedge_plan_destroy_impl(dec_wedge_plan* P);
 void wedge_lengths_impl(const dec_wedge_plan* P, int64_t* la, int64_t* lb, int64_t* lo);
+void c_wedge_apply_impl(int j, int k, int64_t n, const int32_t* p, const void* c, dec_dtype dt, const void* a,
+                        const void* b, void* res, int index_base, void* stream);
 dec_op* op_create_impl(dec_mesh* mh, int kind, double shift, dec_dtype dt);
 void op_apply_impl(dec_op* op, const void* x, void* y, double alpha, double beta, void* stream);
 void op_export_csr_impl(const dec_op* op, int64_t* nnz, int32_t* rowptr, int32_t* colind, double* val);
@@ -147,6 +149,11 @@ dec_status dec_wedge_apply(dec_wedge_plan* p, const void* a, const void* b, void
 dec_status dec_wedge_apply_batched(dec_wedge_plan* p, const void* a, const void* b, void* out, int32_t count,
                                    void* stream) {
   return guard([&] { wedge_apply_impl(p, a, b, out, count, stream); });
+}
+
+dec_status dec_c_wedge_apply(int32_t j, int32_t k, int64_t n_out, const int32_t* p, const void* c, dec_dtype dtype,
+                             const void* a, const void* b, void* res, int32_t index_base, void* stream) {
+  return guard([&] { c_wedge_apply_impl(j, k, n_out, p, c, dtype, a, b, res, index_base, stream); });
 }
 
 dec_status dec_wedge_lengths(const dec_wedge_plan* p, int64_t* la, int64_t* lb, int64_t* lo) {

@@ -699,7 +699,8 @@ static void launch_op(const dec_op& op, const void* vx, void* vy, double alpha, 
       break;
     case DEC_OP_LAPLACE0:
     case DEC_OP_HELMHOLTZ0:
-    case DEC_OP_STAR1_GEOMETRIC: {
+    case DEC_OP_STAR1_GEOMETRIC:
+    case DEC_OP_FLAT_SHARP: {
       const T* val = std::is_same<T, double>::value ? (const T*)op.val64.p : (const T*)op.val32.p;
       if (op.rows) launch_ell<T>((int)op.rows, op.W, op.col.p, val, x, y, a, b, hb, s);
       break;
@@ -724,7 +725,7 @@ using namespace decb;
 dec_op* op_create_impl(dec_mesh* mh, int kind, double shift, dec_dtype dt) {
   require(mh != nullptr, "op: null mesh");
   require(dt == DEC_F64 || dt == DEC_F32, "op: dtype must be DEC_F64 or DEC_F32");
-  require(kind >= DEC_OP_D0 && kind <= DEC_OP_INV_STAR1_GEOMETRIC, "op: unknown operator kind");
+  require(kind >= DEC_OP_D0 && kind <= DEC_OP_FLAT_SHARP, "op: unknown operator kind");
   Mesh& m = mh->m;
   auto* op = new dec_op();
   op->m = &m;
@@ -739,6 +740,7 @@ dec_op* op_create_impl(dec_mesh* mh, int kind, double shift, dec_dtype dt) {
       case DEC_OP_BOUNDARY2: case DEC_OP_DUAL_D0: op->rows = m.ne; op->cols = m.nt; break;
       case DEC_OP_STAR0: case DEC_OP_INV_STAR0: op->rows = op->cols = m.nv; break;
       case DEC_OP_STAR1: case DEC_OP_INV_STAR1: case DEC_OP_STAR1_GEOMETRIC: case DEC_OP_INV_STAR1_GEOMETRIC:
+      case DEC_OP_FLAT_SHARP:
         op->rows = op->cols = m.ne; break;
       case DEC_OP_STAR2: case DEC_OP_INV_STAR2: op->rows = op->cols = m.nt; break;
       default: op->rows = op->cols = m.nv; break;
@@ -753,6 +755,9 @@ dec_op* op_create_impl(dec_mesh* mh, int kind, double shift, dec_dtype dt) {
     } else if (kind == DEC_OP_STAR1_GEOMETRIC || kind == DEC_OP_INV_STAR1_GEOMETRIC) {
       assemble_geometric_star1(m, kind == DEC_OP_INV_STAR1_GEOMETRIC, op->W, op->col, op->val64);
       if (dt == DEC_F32 && kind == DEC_OP_STAR1_GEOMETRIC) cast_array(op->val64, op->val32);
+    } else if (kind == DEC_OP_FLAT_SHARP) {
+      op->W = assemble_flat_sharp(m, op->col, op->val64);
+      if (dt == DEC_F32) cast_array(op->val64, op->val32);
     }
     DEC_CUDA(cudaDeviceSynchronize());
   } catch (...) {
@@ -806,7 +811,7 @@ void op_export_csr_impl(const dec_op* op, int64_t* nnz, int32_t* rowptr, int32_t
       }
       break;
     }
-    case DEC_OP_LAPLACE0: case DEC_OP_HELMHOLTZ0: case DEC_OP_STAR1_GEOMETRIC: {
+    case DEC_OP_LAPLACE0: case DEC_OP_HELMHOLTZ0: case DEC_OP_STAR1_GEOMETRIC: case DEC_OP_FLAT_SHARP: {
       auto c = op->col.download();
       auto v = op->val64.download();
       const size_t n = (size_t)op->rows;

@@ -10,7 +10,7 @@ struct dec_op {
   int64_t rows = 0, cols = 0;
   decb::DArr<double> diag64;  // diagonal operators
   decb::DArr<float> diag32;
-  int W = 0;                  // slot-major ELL width (Laplacian / Helmholtz / geometric ⋆1)
+  int W = 0;                  // slot-major ELL width (Laplacian / Helmholtz / geometric ⋆1 / ♭♯)
   decb::DArr<int32_t> col;
   decb::DArr<double> val64;
   decb::DArr<float> val32;
@@ -20,6 +20,7 @@ struct dec_op {
 namespace decb {
 void hodge_into(const Mesh& m, int k, bool inverse, DArr<double>& out);
 void assemble_laplacian(const Mesh& m, double shift, int& W, DArr<int32_t>& col, DArr<double>& val);
+int assemble_flat_sharp(const Mesh& m, DArr<int32_t>& idx, DArr<double>& val);  // wedge.cu
 template <class T>
 void cast_array(const DArr<double>& a, DArr<T>& b);
 

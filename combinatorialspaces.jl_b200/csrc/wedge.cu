@@ -565,6 +565,34 @@ __global__ void __launch_bounds__(kThreads) k_fs_apply(int ne, const int32_t* __
   }
 }
 
+// ♭♯_mat(sd) (DiscreteExteriorCalculus.jl:1992; ♭ :687-714, ♯ :876-909) as a slot-major ELL of
+// width kFlatSharpWidth (padding column -1); returns the width.
+int assemble_flat_sharp(const Mesh& m, DArr<int32_t>& idx, DArr<double>& val) {
+  const int T = 256;
+  idx.alloc((size_t)m.ne * kFlatSharpWidth);
+  val.alloc((size_t)m.ne * kFlatSharpWidth);
+  DArr<double> sumlen(m.ne), sharp((size_t)9 * m.nt);
+  DArr<int32_t> tedges((size_t)3 * m.nt);
+  DArr<int> overflow(1);
+  DEC_CUDA(cudaMemset(overflow.p, 0, sizeof(int)));
+  if (m.ne && m.nt) {
+    k_fs_sumlen<<<grid_for(m.ne, T), T>>>(m.ne, m.nt, m.e2t_ptr.p, m.e2t.p, m.dual_len_te.p, sumlen.p);
+    k_fs_sharp<<<grid_for(m.nt, T), T>>>(m.nt, m.te0.p, m.te1.p, m.te2.p, m.tv0.p, m.tv1.p, m.tv2.p, m.ev0.p,
+                                         m.ev1.p, m.esign.p, m.tsign.p, m.pts.p, m.tri_center.p, m.dual_len_te.p,
+                                         sumlen.p, tedges.p, sharp.p);
+    k_fs_rows<<<grid_for(m.ne, T), T>>>(m.ne, m.nt, m.e2t_ptr.p, m.e2t.p, m.te0.p, m.te1.p, m.te2.p, m.ev0.p,
+                                        m.ev1.p, m.esign.p, m.pts.p, m.dual_len_te.p, tedges.p, sharp.p, idx.p,
+                                        val.p, overflow.p);
+  } else if (m.ne) {
+    DEC_CUDA(cudaMemset(idx.p, 0xff, idx.bytes()));
+    DEC_CUDA(cudaMemset(val.p, 0, val.bytes()));
+  }
+  DEC_CHECK_LAUNCH();
+  if (overflow.download()[0])
+    throw Error(DEC_ERR_UNSUPPORTED, "flat-sharp: an edge has more incident triangles than supported (non-manifold mesh)");
+  return kFlatSharpWidth;
+}
+
 // ---- plan ---------------------------------------------------------------------------------
 
 static void build_plan(dec_wedge_plan& P) {
@@ -578,28 +606,7 @@ static void build_plan(dec_wedge_plan& P) {
                                          m.dual_area.p, c.c[0].p, c.c[1].p, c.c[2].p);
   }
   if (P.op == WPD11 || P.op == WDP11) {
-    c.width = kFlatSharpWidth;
-    c.idx.alloc((size_t)m.ne * c.width);
-    c.val.alloc((size_t)m.ne * c.width);
-    DArr<double> sumlen(m.ne), sharp((size_t)9 * m.nt);
-    DArr<int32_t> tedges((size_t)3 * m.nt);
-    DArr<int> overflow(1);
-    DEC_CUDA(cudaMemset(overflow.p, 0, sizeof(int)));
-    if (m.ne && m.nt) {
-      k_fs_sumlen<<<grid_for(m.ne, T), T>>>(m.ne, m.nt, m.e2t_ptr.p, m.e2t.p, m.dual_len_te.p, sumlen.p);
-      k_fs_sharp<<<grid_for(m.nt, T), T>>>(m.nt, m.te0.p, m.te1.p, m.te2.p, m.tv0.p, m.tv1.p, m.tv2.p, m.ev0.p,
-                                           m.ev1.p, m.esign.p, m.tsign.p, m.pts.p, m.tri_center.p, m.dual_len_te.p,
-                                           sumlen.p, tedges.p, sharp.p);
-      k_fs_rows<<<grid_for(m.ne, T), T>>>(m.ne, m.nt, m.e2t_ptr.p, m.e2t.p, m.te0.p, m.te1.p, m.te2.p, m.ev0.p,
-                                          m.ev1.p, m.esign.p, m.pts.p, m.dual_len_te.p, tedges.p, sharp.p, c.idx.p,
-                                          c.val.p, overflow.p);
-    } else if (m.ne) {
-      DEC_CUDA(cudaMemset(c.idx.p, 0xff, c.idx.bytes()));
-      DEC_CUDA(cudaMemset(c.val.p, 0, c.val.bytes()));
-    }
-    DEC_CHECK_LAUNCH();
-    if (overflow.download()[0])
-      throw Error(DEC_ERR_UNSUPPORTED, "wedge: an edge has more incident triangles than supported (non-manifold mesh)");
+    c.width = assemble_flat_sharp(m, c.idx, c.val);
   } else if (P.op == W02 || P.op == W20) {
     for (auto& x : c.c) x.alloc(m.nt);
     if (m.nt) k_coef02<<<grid_for(m.nt, T), T>>>(m.nt, m.area.p, m.dual_area.p, c.c[0].p, c.c[1].p, c.c[2].p);
@@ -740,6 +747,91 @@ static void launch_plan(dec_wedge_plan& P, const CoefSet<T>& c, const void* va, 
   }
 }
 
+// ---- wedges on caller caches: dec_c_wedge_product!(Val(j), Val(k), res, α, β, p, c) ----------
+// (FastDEC.jl:217-232).  The caches are the reference's Julia matrices (column-major): every
+// output's indices / coefficients are contiguous (R x n_out), except (0,1) whose p is n_out x 2.
+// `base` is subtracted from every index (1 for Julia's 1-based caches).  Each kernel restates
+// its reference kernel's arithmetic in the same order (this file compiles without FMA
+// contraction).
+
+// wedge_kernel_01! (FastDEC.jl:159-163): res = ½ β[i] (α[p[i,1]] + α[p[i,2]]).
+template <class T>
+__global__ void k_cw01(int64_t n, const int32_t* __restrict__ p, int base, const T* __restrict__ a,
+                       const T* __restrict__ b, T* __restrict__ res) {
+  const T half = T(0.5);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    res[i] = half * b[i] * (a[p[i] - base] + a[p[n + i] - base]);
+}
+
+// wedge_kernel_02! (FastDEC.jl:165-170): res = β[i] Σ_{j=1..6} c[j,i] α[p[j,i]].
+template <class T>
+__global__ void k_cw02(int64_t n, const int32_t* __restrict__ p, const T* __restrict__ c, int base,
+                       const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ res) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t* q = p + 6 * i;
+    const T* w = c + 6 * i;
+    res[i] = b[i] * (w[0] * a[q[0] - base] + w[1] * a[q[1] - base] + w[2] * a[q[2] - base] +
+                     w[3] * a[q[3] - base] + w[4] * a[q[4] - base] + w[5] * a[q[5] - base]);
+  }
+}
+
+// wedge_kernel_03! (FastDEC.jl:172-182): res = Σ_{j=1..24} (β[i] c[j,i]) α[p[j,i]], in j order.
+template <class T>
+__global__ void k_cw03(int64_t n, const int32_t* __restrict__ p, const T* __restrict__ c, int base,
+                       const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ res) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t* q = p + 24 * i;
+    const T* w = c + 24 * i;
+    const T bv = b[i];
+    T tmp = T(0);
+#pragma unroll 8
+    for (int j = 0; j < 24; ++j) tmp += bv * w[j] * a[q[j] - base];
+    res[i] = tmp;
+  }
+}
+
+// wedge_kernel_11! (FastDEC.jl:184-191).
+template <class T>
+__global__ void k_cw11(int64_t n, const int32_t* __restrict__ p, const T* __restrict__ c, int base,
+                       const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ res) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int e0 = p[3 * i] - base, e1 = p[3 * i + 1] - base, e2 = p[3 * i + 2] - base;
+    const T c1 = c[3 * i], c2 = c[3 * i + 1], c3 = c[3 * i + 2];
+    const T ae0 = a[e0], ae1 = a[e1], ae2 = a[e2];
+    const T be0 = b[e0], be1 = b[e1], be2 = b[e2];
+    res[i] = (c1 * (ae2 * be1 - ae1 * be2) + c2 * (ae2 * be0 - ae0 * be2) + c3 * (ae1 * be0 - ae0 * be1));
+  }
+}
+
+// wedge_kernel_21! (FastDEC.jl:193-205): α a 2-form (triangles t0..t3 = p[7..10, i]), β a 1-form
+// (edges e0..e5 = p[1..6, i]), twelve coefficients.
+template <class T>
+__global__ void k_cw21(int64_t n, const int32_t* __restrict__ p, const T* __restrict__ c, int base,
+                       const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ res) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t* q = p + 10 * i;
+    const T* w = c + 12 * i;
+    const T be0 = b[q[0] - base], be1 = b[q[1] - base], be2 = b[q[2] - base], be3 = b[q[3] - base],
+            be4 = b[q[4] - base], be5 = b[q[5] - base];
+    const T at0 = a[q[6] - base], at1 = a[q[7] - base], at2 = a[q[8] - base], at3 = a[q[9] - base];
+    res[i] = w[0] * be3 * at3 - w[1] * be4 * at2 + w[2] * be5 * at1 + w[3] * be1 * at3 - w[4] * be2 * at2 +
+             w[5] * be5 * at0 + w[6] * be0 * at3 - w[7] * be2 * at1 + w[8] * be4 * at0 + w[9] * be0 * at2 -
+             w[10] * be1 * at1 + w[11] * be3 * at0;
+  }
+}
+
+template <class T>
+static void launch_cw(int j, int k, int64_t n, const int32_t* p, const T* c, int base, const T* a, const T* b, T* res,
+                      cudaStream_t s) {
+  const unsigned g = grid_for(n, kThreads);
+  if (j == 0 && k == 1) k_cw01<T><<<g, kThreads, 0, s>>>(n, p, base, a, b, res);
+  else if (j == 0 && k == 2) k_cw02<T><<<g, kThreads, 0, s>>>(n, p, c, base, a, b, res);
+  else if (j == 0 && k == 3) k_cw03<T><<<g, kThreads, 0, s>>>(n, p, c, base, a, b, res);
+  else if (j == 1 && k == 1) k_cw11<T><<<g, kThreads, 0, s>>>(n, p, c, base, a, b, res);
+  else k_cw21<T><<<g, kThreads, 0, s>>>(n, p, c, base, a, b, res);
+  DEC_CHECK_LAUNCH();
+}
+
 }  // namespace decb
 
 using namespace decb;
@@ -803,4 +895,23 @@ void wedge_lengths_impl(const dec_wedge_plan* P, int64_t* la, int64_t* lb, int64
   if (la) *la = P->len_a;
   if (lb) *lb = P->len_b;
   if (lo) *lo = P->len_out;
+}
+
+void c_wedge_apply_impl(int j, int k, int64_t n, const int32_t* p, const void* c, dec_dtype dt, const void* a,
+                        const void* b, void* res, int index_base, void* stream) {
+  const bool ok = (j == 0 && (k == 1 || k == 2 || k == 3)) || (j == 1 && k == 1) || (j == 2 && k == 1);
+  if (!ok)
+    throw Error(DEC_ERR_UNSUPPORTED,
+                "Unsupported combination of degrees " + std::to_string(j) + " and " + std::to_string(k) +
+                    ". Ensure that their sum is not greater than the degree of the complex.");
+  require(n >= 0, "c_wedge: negative output length");
+  require(dt == DEC_F64 || dt == DEC_F32, "c_wedge: dtype must be DEC_F64 or DEC_F32");
+  require(index_base == 0 || index_base == 1, "c_wedge: index_base must be 0 or 1");
+  if (n == 0) return;
+  require(p && a && b && res && (c || (j == 0 && k == 1)), "c_wedge: null pointer");
+  cudaStream_t s = as_stream(stream);
+  if (dt == DEC_F64)
+    launch_cw<double>(j, k, n, p, (const double*)c, index_base, (const double*)a, (const double*)b, (double*)res, s);
+  else
+    launch_cw<float>(j, k, n, p, (const float*)c, index_base, (const float*)a, (const float*)b, (float*)res, s);
 }

@@ -106,6 +106,17 @@ dec_status dec_wedge_lengths(const dec_wedge_plan* p, int64_t* len_a, int64_t* l
 dec_status dec_wedge_apply_batched(dec_wedge_plan* p, const void* a, const void* b, void* out,
                                    int32_t count, void* stream);
 dec_status dec_wedge_plan_destroy(dec_wedge_plan* p);
+/* dec_c_wedge_product!(Val(j), Val(k), res, α, β, p, c) (FastDEC.jl:217-232): a wedge kernel on
+ * caller caches in the reference's layout (cache_wedge output, Julia column-major), for
+ * (j,k) = (0,1), (0,2), (0,3), (1,1), (2,1) -- the 3D kernels included:
+ *   (0,1): p n_out x 2 (edge endpoints), c unused:   res[i] = ½ β[i] (α[p[i,1]] + α[p[i,2]])
+ *   (0,2): p, c 6 x n_out:                            res[i] = β[i] Σ_j c[j,i] α[p[j,i]]
+ *   (0,3): p, c 24 x n_out (tetrahedra):              res[i] = Σ_j β[i] c[j,i] α[p[j,i]]
+ *   (1,1): p, c 3 x n_out (edges of triangle i):       wedge_kernel_11!
+ *   (2,1): p 10 x n_out (6 edges, 4 triangles of tetrahedron i), c 12 x n_out: wedge_kernel_21!
+ * p: device int32, index_base 0 or 1 (Julia); c, a (α), b (β), res: device arrays of dtype. */
+dec_status dec_c_wedge_apply(int32_t j, int32_t k, int64_t n_out, const int32_t* p, const void* c, dec_dtype dtype,
+                             const void* a, const void* b, void* res, int32_t index_base, void* stream);
 
 /* ---- sparse operators (replaces dec_differential / dec_boundary / dec_dual_derivative(n, sd,
  *      Val(:CUDA)), ext/CombinatorialSpacesCUDAExt.jl:30-61, the diagonal Hodge stars, and
@@ -124,7 +135,10 @@ typedef enum dec_op_kind {
   DEC_OP_INV_STAR1_GEOMETRIC = 15  /* dec_inv_hodge_star(1, sd, GeometricHodge()), FastDEC.jl:745-748,
                                       CUDA ext :93-96: y = (-⋆1)⁻¹ x by a Jacobi-preconditioned
                                       BiCGSTAB solve in FP64 to 1e-14 relative residual (one host
-                                      read-back per reduction; not capturable in a CUDA graph) */
+                                      read-back per reduction; not capturable in a CUDA graph) */,
+  DEC_OP_FLAT_SHARP = 16           /* ♭♯_mat(sd) (DiscreteExteriorCalculus.jl:1992; ♭ :687-714, ♯ :876-909):
+                                      dual 1-form -> primal 1-form, ne x ne, <= 6 nnz per row (the
+                                      matrix inside dec_wedge_product_pd/dp(1,1), FastDEC.jl:391-401) */
 } dec_op_kind;
 dec_status dec_op_create(dec_mesh* m, int32_t kind, double shift, dec_dtype dtype, dec_op** out);
 dec_status dec_op_shape(const dec_op* op, int64_t* rows, int64_t* cols);

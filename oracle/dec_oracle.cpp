@@ -738,6 +738,46 @@ template void wedge02<float>(const Dual&, const Wedge02Cache&, const float*, con
 template void wedge11<double>(const Dual&, const Wedge11Cache&, const double*, const double*, double*);
 template void wedge11<float>(const Dual&, const Wedge11Cache&, const float*, const float*, float*);
 
+// dec_c_wedge_product!(Val(j), Val(k), res, α, β, p, c) (FastDEC.jl:217-232) on caller caches in
+// the reference's column-major layout, 0-based indices: wedge_kernel_01! (:159-163, p n x 2),
+// _02! (:165-170, p, c 6 x n), _03! (:172-182, p, c 24 x n), _11! (:184-191, p, c 3 x n) and
+// _21! (:193-205, p 10 x n, c 12 x n).  Same expressions, same order.
+template <class T>
+void c_wedge(int j, int k, int64_t n, const i32* p, const T* c, const T* a, const T* b, T* res) {
+  for (int64_t i = 0; i < n; ++i) {
+    if (j == 0 && k == 1) {
+      const T half = T(0.5);
+      res[i] = half * b[i] * (a[p[i]] + a[p[n + i]]);
+    } else if (j == 0 && k == 2) {
+      const i32* q = p + 6 * i;
+      const T* w = c + 6 * i;
+      res[i] = b[i] * (w[0] * a[q[0]] + w[1] * a[q[1]] + w[2] * a[q[2]] + w[3] * a[q[3]] + w[4] * a[q[4]] +
+                       w[5] * a[q[5]]);
+    } else if (j == 0 && k == 3) {
+      T tmp = T(0);
+      for (int r = 0; r < 24; ++r) tmp += b[i] * c[24 * i + r] * a[p[24 * i + r]];
+      res[i] = tmp;
+    } else if (j == 1 && k == 1) {
+      const i32 e0 = p[3 * i], e1 = p[3 * i + 1], e2 = p[3 * i + 2];
+      const T c1 = c[3 * i], c2 = c[3 * i + 1], c3 = c[3 * i + 2];
+      res[i] = (c1 * (a[e2] * b[e1] - a[e1] * b[e2]) + c2 * (a[e2] * b[e0] - a[e0] * b[e2]) +
+                c3 * (a[e1] * b[e0] - a[e0] * b[e1]));
+    } else if (j == 2 && k == 1) {
+      const i32* q = p + 10 * i;
+      const T* w = c + 12 * i;
+      const T be0 = b[q[0]], be1 = b[q[1]], be2 = b[q[2]], be3 = b[q[3]], be4 = b[q[4]], be5 = b[q[5]];
+      const T at0 = a[q[6]], at1 = a[q[7]], at2 = a[q[8]], at3 = a[q[9]];
+      res[i] = w[0] * be3 * at3 - w[1] * be4 * at2 + w[2] * be5 * at1 + w[3] * be1 * at3 - w[4] * be2 * at2 +
+               w[5] * be5 * at0 + w[6] * be0 * at3 - w[7] * be2 * at1 + w[8] * be4 * at0 + w[9] * be0 * at2 -
+               w[10] * be1 * at1 + w[11] * be3 * at0;
+    } else {
+      throw std::runtime_error("c_wedge: unsupported degrees");
+    }
+  }
+}
+template void c_wedge<double>(int, int, int64_t, const i32*, const double*, const double*, const double*, double*);
+template void c_wedge<float>(int, int, int64_t, const i32*, const float*, const float*, const float*, float*);
+
 // elementary_duals(1, s, e) = dual edges whose D_∂v1 is the center of e, in index order
 // (DiscreteExteriorCalculus.jl:478-479).  In a 2D dual complex they are the D_edges12 entries.
 static std::vector<std::vector<i32>> elementary_duals_1(const Dual& d) {

@@ -124,6 +124,8 @@ Wedge11Cache wedge11_cache(const Dual& d);
 template <class T> void wedge01(const Dual& d, const T* f, const T* a, T* out);
 template <class T> void wedge02(const Dual& d, const Wedge02Cache& c, const T* f, const T* a, T* out);
 template <class T> void wedge11(const Dual& d, const Wedge11Cache& c, const T* a, const T* b, T* out);
+template <class T>
+void c_wedge(int j, int k, int64_t n, const i32* p, const T* c, const T* a, const T* b, T* res);
 
 // Primal-dual / dual-dual wedge matrices, FastDEC.jl:293-347, and ♭♯ (DEC.jl:1992).
 CSC wedge_dd_01_mat(const Dual& d);

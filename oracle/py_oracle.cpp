@@ -174,6 +174,22 @@ PYBIND11_MODULE(dec_oracle, mod) {
   // kind: 1 = (0,1), 2 = (0,2), 11 = (1,1)
   mod.def("wedge", &run_wedge<double>);
   mod.def("wedge_f32", &run_wedge<float>);
+  mod.def("c_wedge", [](int j, int k, int64_t n, py::array_t<int32_t, py::array::c_style | py::array::forcecast> p,
+                        py::array_t<double, py::array::c_style | py::array::forcecast> c,
+                        py::array_t<double, py::array::c_style | py::array::forcecast> a,
+                        py::array_t<double, py::array::c_style | py::array::forcecast> b) {
+    py::array_t<double> out(n);
+    c_wedge<double>(j, k, n, p.data(), c.size() ? c.data() : nullptr, a.data(), b.data(), out.mutable_data());
+    return out;
+  });
+  mod.def("c_wedge_f32", [](int j, int k, int64_t n, py::array_t<int32_t, py::array::c_style | py::array::forcecast> p,
+                            py::array_t<float, py::array::c_style | py::array::forcecast> c,
+                            py::array_t<float, py::array::c_style | py::array::forcecast> a,
+                            py::array_t<float, py::array::c_style | py::array::forcecast> b) {
+    py::array_t<float> out(n);
+    c_wedge<float>(j, k, n, p.data(), c.size() ? c.data() : nullptr, a.data(), b.data(), out.mutable_data());
+    return out;
+  });
   mod.def("time_wedge", [](const Dual& d, int kind, py::array_t<double, py::array::c_style> a,
                            py::array_t<double, py::array::c_style> b, int reps) {
     // Seconds per evaluation of the cached kernel (caches built once, outside the timing).

@@ -300,3 +300,51 @@ def test_geometric_hodge_fast_matches_dec(O, mesh, center):
     np.testing.assert_allclose(fast, dec, rtol=1e-12, atol=1e-12)
     if center == "CIRCUMCENTER" and mesh == "grid":
         np.testing.assert_allclose(fast, np.diag(O.hodge_diag(d, 1)), rtol=1e-12, atol=1e-12)
+
+
+def _cache_meshes(O):
+    return [O.dualize(O.grid_345(), O.BARYCENTER), O.dualize(O.triangulated_grid(6, 5, 1.0, 0.8, False), O.CIRCUMCENTER)]
+
+
+def test_cached_wedge_kernels_match_mesh_wedges(O):
+    """dec_c_wedge_product! on the reference's caches (FastDEC.jl:217-232) equals the mesh-bound
+    wedges (which the reference's identities above pin) bit for bit: (0,1) with p = [∂v0 ∂v1]
+    (an ne x 2 column-major matrix), (0,2) and (1,1) with the 6 x nt / 3 x nt caches."""
+    rng = np.random.default_rng(11)
+    for d in _cache_meshes(O):
+        m = d.mesh
+        f, a, b, t = rng.uniform(-1, 1, d.nv), rng.uniform(-1, 1, d.ne), rng.uniform(-1, 1, d.ne), rng.uniform(-1, 1, d.nt)
+        p01 = np.concatenate([m.ev0, m.ev1]).astype(np.int32)
+        np.testing.assert_array_equal(O.c_wedge(0, 1, d.ne, p01, np.zeros(0), f, a), O.wedge(d, 1, f, a))
+        v, c = O.wedge02_cache(d)
+        np.testing.assert_array_equal(O.c_wedge(0, 2, d.nt, v, c, f, t), O.wedge(d, 2, f, t))
+        e, c = O.wedge11_cache(d)
+        np.testing.assert_array_equal(O.c_wedge(1, 1, d.nt, e, c, a, b), O.wedge(d, 11, a, b))
+
+
+def test_cached_3d_wedge_kernels(O):
+    """The 3D kernels wedge_kernel_03! (FastDEC.jl:172-182) and wedge_kernel_21! (:193-205) against
+    a vectorised numpy statement of the same sums, on random caches."""
+    rng = np.random.default_rng(12)
+    n, nv, ne, nt = 37, 50, 80, 60
+    p3 = rng.integers(0, nv, (n, 24)).astype(np.int32)
+    c3 = rng.uniform(-1, 1, (n, 24))
+    f, beta = rng.uniform(-1, 1, nv), rng.uniform(-1, 1, n)
+    ref3 = np.zeros(n)
+    for j in range(24):
+        ref3 = ref3 + beta * c3[:, j] * f[p3[:, j]]
+    np.testing.assert_array_equal(O.c_wedge(0, 3, n, p3, c3, f, beta), ref3)
+    p21 = np.concatenate([rng.integers(0, ne, (n, 6)), rng.integers(0, nt, (n, 4))], axis=1).astype(np.int32)
+    c21 = rng.uniform(-1, 1, (n, 12))
+    al, be = rng.uniform(-1, 1, nt), rng.uniform(-1, 1, ne)
+    B = [be[p21[:, q]] for q in range(6)]
+    A = [al[p21[:, 6 + q]] for q in range(4)]
+    w = [c21[:, q] for q in range(12)]
+    ref21 = (w[0] * B[3] * A[3] - w[1] * B[4] * A[2] + w[2] * B[5] * A[1] + w[3] * B[1] * A[3] - w[4] * B[2] * A[2]
+             + w[5] * B[5] * A[0] + w[6] * B[0] * A[3] - w[7] * B[2] * A[1] + w[8] * B[4] * A[0] + w[9] * B[0] * A[2]
+             - w[10] * B[1] * A[1] + w[11] * B[3] * A[0])
+    np.testing.assert_array_equal(O.c_wedge(2, 1, n, p21, c21, al, be), ref21)
+    # 1 ∧ β = β when every tetrahedron's coefficients sum to one
+    c1 = rng.uniform(0, 1, (n, 24))
+    c1 /= c1.sum(axis=1, keepdims=True)
+    np.testing.assert_allclose(O.c_wedge(0, 3, n, p3, c1, np.ones(nv), beta), beta, rtol=1e-14, atol=1e-15)
