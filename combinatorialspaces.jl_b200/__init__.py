@@ -433,8 +433,14 @@ class MultigridData:
     ``Mesh``-compatible tuple); options follow ``dec_mg_options``.
     """
 
-    def __init__(self, coarse, levels, shift=0.0, center="circumcenter", project_radius=0.0, **opts):
+    def __init__(self, coarse, levels, shift=0.0, center="circumcenter", project_radius=0.0, mode="direct",
+                 **opts):
+        """mode: "direct" (DirectMode: every level discretised on its own mesh) or "galerkin"
+        (GalerkinMode: coarse operators R A P, Multigrid.jl:740-748)."""
         o = default_mg_options()
+        if mode not in ("direct", "galerkin"):
+            raise ValueError(f"unknown multigrid mode {mode!r}")
+        o.galerkin = 1 if mode == "galerkin" else 0
         o.levels = levels
         o.center = CENTERS[center] if isinstance(center, str) else int(center)
         o.project_radius = project_radius

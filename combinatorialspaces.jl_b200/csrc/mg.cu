@@ -34,6 +34,8 @@
 #include "mlp.cuh"
 
 dec_op* op_create_impl(dec_mesh* mh, int kind, double shift, dec_dtype dt);
+dec_op* op_from_csr_impl(dec_mesh* mh, int n, const std::vector<int32_t>& rowptr, const std::vector<int32_t>& colind,
+                         const std::vector<double>& val);
 decb::MlpWeights mlp_weights(const dec_mlp* m);
 void mlp_check_error(const dec_mlp* m, cudaStream_t s);
 
@@ -1302,8 +1304,132 @@ static void build_eigen_coarse(dec_mg& mg, const Level& C) {
   mg.eigL.upload(lam);
 }
 
-static void build_level_operator(Level& L, double shift, bool reorder) {
-  L.op.reset(op_create_impl(L.mesh.get(), DEC_OP_HELMHOLTZ0, shift, DEC_F64));
+// ---- GalerkinMode (Multigrid.jl:740-748): A_{k+1} = R_k A_k P_k on the host ------------------
+struct HostCSC {
+  int m = 0, n = 0;
+  std::vector<int32_t> cp, ri;
+  std::vector<double> v;
+};
+
+// C = X Y column by column, as SparseArrays' spmatmul: C[i, j] = Σ_k X[i, k] Y[k, j] summed over
+// the stored entries of Y[:, j] in row order; each column's rows sorted.
+static HostCSC csc_mul(const HostCSC& X, const HostCSC& Y) {
+  require(X.n == Y.m, "multigrid: Galerkin product dimension mismatch");
+  HostCSC C;
+  C.m = X.m;
+  C.n = Y.n;
+  C.cp.assign(Y.n + 1, 0);
+  std::vector<double> acc(X.m, 0.0);
+  std::vector<int32_t> stamp(X.m, -1), rows;
+  for (int j = 0; j < Y.n; ++j) {
+    rows.clear();
+    for (int q = Y.cp[j]; q < Y.cp[j + 1]; ++q) {
+      const int k = Y.ri[q];
+      const double y = Y.v[q];
+      for (int p = X.cp[k]; p < X.cp[k + 1]; ++p) {
+        const int i = X.ri[p];
+        const double prod = X.v[p] * y;
+        if (stamp[i] != j) {
+          stamp[i] = j;
+          rows.push_back(i);
+          acc[i] = prod;
+        } else {
+          acc[i] += prod;
+        }
+      }
+    }
+    std::sort(rows.begin(), rows.end());
+    for (int i : rows) {
+      C.ri.push_back(i);
+      C.v.push_back(acc[i]);
+    }
+    C.cp[j + 1] = (int32_t)C.ri.size();
+  }
+  return C;
+}
+
+static HostCSC csc_transpose(const HostCSC& A) {
+  HostCSC T;
+  T.m = A.n;
+  T.n = A.m;
+  T.cp.assign(A.m + 1, 0);
+  for (int r : A.ri) T.cp[r + 1]++;
+  for (int i = 0; i < A.m; ++i) T.cp[i + 1] += T.cp[i];
+  T.ri.resize(A.ri.size());
+  T.v.resize(A.v.size());
+  std::vector<int32_t> pos(T.cp.begin(), T.cp.end() - 1);
+  for (int j = 0; j < A.n; ++j)
+    for (int p = A.cp[j]; p < A.cp[j + 1]; ++p) {
+      const int q = pos[A.ri[p]]++;
+      T.ri[q] = j;
+      T.v[q] = A.v[p];
+    }
+  return T;
+}
+
+// The level operator (reference numbering, sorted ELL) as a CSC.
+static HostCSC csc_of_op(const dec_op& op) {
+  const int n = (int)op.rows;
+  auto c = op.col.download();
+  auto v = op.val64.download();
+  HostCSC R;  // CSR of the rows first (as a CSC of the transpose), then transposed
+  R.m = n;
+  R.n = n;
+  R.cp.assign(n + 1, 0);
+  for (int i = 0; i < n; ++i) {
+    for (int q = 0; q < op.W; ++q)
+      if (c[(size_t)q * n + i] >= 0) {
+        R.ri.push_back(c[(size_t)q * n + i]);
+        R.v.push_back(v[(size_t)q * n + i]);
+      }
+    R.cp[i + 1] = (int32_t)R.ri.size();
+  }
+  return csc_transpose(R);
+}
+
+// subdivision_matrix(BinarySubdivision(), topo) (Multigrid.jl:191-219) of coarse topology c:
+// nv_c x (nv_c + ne_c), identity then ½ at min(∂v0, ∂v1) and max for each edge's midpoint.
+static HostCSC subdivision_csc(const HostLevel& c) {
+  HostCSC S;
+  S.m = c.nv;
+  S.n = c.nv + c.ne;
+  S.cp.assign(S.n + 1, 0);
+  for (int i = 0; i < c.nv; ++i) {
+    S.ri.push_back(i);
+    S.v.push_back(1.0);
+    S.cp[i + 1] = (int32_t)S.ri.size();
+  }
+  for (int e = 0; e < c.ne; ++e) {
+    const int a = std::min(c.ev0[e], c.ev1[e]), b = std::max(c.ev0[e], c.ev1[e]);
+    S.ri.push_back(a);
+    S.v.push_back(0.5);
+    S.ri.push_back(b);
+    S.v.push_back(0.5);
+    S.cp[c.nv + e + 1] = (int32_t)S.ri.size();
+  }
+  return S;
+}
+
+// A_coarse = R A P with R = make_restriction(S) (each S entry over its row's sum, Multigrid.jl:
+// 595-612) and P = Sᵀ, in the reference's evaluation order (R * A) * P; returned as a CSR.
+static void galerkin_product(const dec_op& A, const HostLevel& c, std::vector<int32_t>& rp,
+                             std::vector<int32_t>& ci, std::vector<double>& vv) {
+  HostCSC S = subdivision_csc(c);
+  std::vector<double> rs(S.m, 0.0);
+  for (size_t k = 0; k < S.v.size(); ++k) rs[S.ri[k]] += S.v[k];
+  HostCSC Rm = S;
+  for (size_t k = 0; k < Rm.v.size(); ++k) Rm.v[k] = S.v[k] / rs[S.ri[k]];
+  HostCSC P = csc_transpose(S);
+  HostCSC Ac = csc_mul(csc_mul(Rm, csc_of_op(A)), P);
+  HostCSC T = csc_transpose(Ac);  // rows of Ac, columns sorted
+  rp = T.cp;
+  ci = T.ri;
+  vv = T.v;
+}
+
+static void build_level_operator(Level& L, double shift, bool reorder, dec_op* given = nullptr) {
+  if (given) L.op.reset(given);
+  else L.op.reset(op_create_impl(L.mesh.get(), DEC_OP_HELMHOLTZ0, shift, DEC_F64));
   L.n = L.mesh->m.nv;
   if (reorder) {
     L.perm = morton_order(L.mesh->m.h_pts, L.n);
@@ -1315,7 +1441,8 @@ static void build_level_operator(Level& L, double shift, bool reorder) {
   for (int i = 0; i < L.n; ++i) L.iperm[L.perm[i]] = i;
   L.dperm.upload(L.perm);
   L.diperm.upload(L.iperm);
-  L.W = std::max(1, L.mesh->m.max_v2e);  // off-diagonal slots: the maximum vertex degree
+  // off-diagonal slots: the maximum vertex degree (a Galerkin operator: its widest row)
+  L.W = given ? std::max(1, L.op->W) : std::max(1, L.mesh->m.max_v2e);
   L.col.alloc((size_t)L.n * L.W);
   L.off64.alloc((size_t)L.n * L.W);
   L.diag64.alloc(L.n);
@@ -1387,6 +1514,9 @@ dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
   require(o.coarse_solver >= 0 && o.coarse_solver <= 2, "multigrid: coarse_solver must be 0, 1 or 2");
   require(o.coarse_solver != 2 || (o.smoother == DEC_SMOOTH_JACOBI || o.smoother == DEC_SMOOTH_CHEBYSHEV),
           "multigrid: per-RHS shifts (coarse_solver 2) need the Jacobi or Chebyshev smoother");
+  require(o.galerkin == 0 || o.galerkin == 1, "multigrid: galerkin must be 0 or 1");
+  require(!(o.galerkin && o.coarse_solver == 2),
+          "multigrid: per-RHS shifts (coarse_solver 2) need every level's own Laplacian (not GalerkinMode)");
   auto mg = std::make_unique<dec_mg>();
   mg->opt = o;
   std::vector<HostLevel> hl(o.levels + 1);
@@ -1418,8 +1548,17 @@ dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
     mg->lv[o.levels - l].mesh = make_mesh(hl[l], o.center);
   }
   // coarse_solver 2 keeps every level's operator the Laplacian; the shifts come per RHS
-  for (int l = 0; l <= o.levels; ++l)
-    build_level_operator(mg->lv[l], o.coarse_solver == 2 ? 0.0 : o.shift, o.reorder != 0);
+  for (int l = 0; l <= o.levels; ++l) {
+    if (o.galerkin && l > 0) {  // A_l = R A_{l-1} P over the coarse topology of level l
+      std::vector<int32_t> rp, ci;
+      std::vector<double> vv;
+      galerkin_product(*mg->lv[l - 1].op, hl[o.levels - l], rp, ci, vv);
+      dec_op* A = op_from_csr_impl(mg->lv[l].mesh.get(), hl[o.levels - l].nv, rp, ci, vv);
+      build_level_operator(mg->lv[l], 0.0, o.reorder != 0, A);
+    } else {
+      build_level_operator(mg->lv[l], o.coarse_solver == 2 ? 0.0 : o.shift, o.reorder != 0);
+    }
+  }
   for (int l = 0; l <= o.levels; ++l) {
     Level& L = mg->lv[l];
     if (l < o.levels) build_transfers(L, mg->lv[l + 1], hl[o.levels - l - 1]);

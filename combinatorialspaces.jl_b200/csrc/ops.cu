@@ -767,6 +767,36 @@ dec_op* op_create_impl(dec_mesh* mh, int kind, double shift, dec_dtype dt) {
   return op;
 }
 
+// An n x n FP64 operator from a host CSR (columns sorted within each row), stored as the
+// slot-major ELL of the Laplacian kind (apply, residual norms and export as for L + shift I).
+dec_op* op_from_csr_impl(dec_mesh* mh, int n, const std::vector<int32_t>& rowptr, const std::vector<int32_t>& colind,
+                         const std::vector<double>& val) {
+  require(mh != nullptr && (int)rowptr.size() == n + 1, "op: bad CSR");
+  auto* op = new dec_op();
+  op->m = &mh->m;
+  op->kind = DEC_OP_HELMHOLTZ0;
+  op->dtype = DEC_F64;
+  op->rows = op->cols = n;
+  int W = 1;
+  for (int i = 0; i < n; ++i) W = std::max(W, rowptr[i + 1] - rowptr[i]);
+  op->W = W;
+  std::vector<int32_t> c((size_t)W * n, -1);
+  std::vector<double> v((size_t)W * n, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int q = rowptr[i]; q < rowptr[i + 1]; ++q) {
+      c[(size_t)(q - rowptr[i]) * n + i] = colind[q];
+      v[(size_t)(q - rowptr[i]) * n + i] = val[q];
+    }
+  try {
+    op->col.upload(c);
+    op->val64.upload(v);
+  } catch (...) {
+    delete op;
+    throw;
+  }
+  return op;
+}
+
 void op_apply_impl(dec_op* op, const void* x, void* y, double alpha, double beta, void* stream) {
   require(op != nullptr && x != nullptr && y != nullptr, "op: null argument");
   if (op->dtype == DEC_F64) launch_op<double>(*op, x, y, alpha, beta, as_stream(stream));

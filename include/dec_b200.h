@@ -209,6 +209,10 @@ typedef struct dec_mg_options {
                               rest of the solve when a refinement step reduces the worst relative
                               residual by less than this factor (or it is not finite); that step is
                               undone and redone with the plain smoother */
+  int32_t galerkin;        /* 0: DirectMode (every level's operator from its own mesh); 1: GalerkinMode
+                              (Multigrid.jl:740-748): only the finest level's, the coarser ones
+                              A_{k+1} = R_k A_k P_k (host sparse products in SparseArrays' order);
+                              not with coarse_solver 2 */
 } dec_mg_options;
 
 typedef struct dec_solve_report {

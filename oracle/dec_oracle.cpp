@@ -1171,7 +1171,7 @@ static CSC level_op(const Mesh& m, int center, double shift, Mesh* oriented) {
 
 // _build_multigrid(DirectMode(), s, BinarySubdivision(), levels, op, steps, alg),
 // Multigrid.jl:752-797.
-MGData build_mg(const Mesh& coarse, int levels, int center, double shift, double radius, int steps) {
+MGData build_mg(const Mesh& coarse, int levels, int center, double shift, double radius, int steps, bool galerkin) {
   MGData md;
   std::vector<CSC> ops;
   std::vector<Mesh> meshes;
@@ -1194,6 +1194,8 @@ MGData build_mg(const Mesh& coarse, int levels, int center, double shift, double
   }
   std::reverse(ops.begin(), ops.end());
   std::reverse(meshes.begin(), meshes.end());
+  if (galerkin)  // _finalize_ops(::GalerkinMode), Multigrid.jl:740-748: ops[i+1] = rs[i] * ops[i] * ps[i]
+    for (int i = 0; i < levels; ++i) ops[i + 1] = spgemm(spgemm(md.rs[i], ops[i]), md.ps[i]);
   md.ops = std::move(ops);
   md.meshes = std::move(meshes);
   md.steps.assign(levels + 1, steps);

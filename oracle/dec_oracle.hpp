@@ -157,9 +157,9 @@ struct MGData {  // MultigridData, :538-553 (finest level first)
   std::vector<int> steps;
   std::vector<Mesh> meshes;  // finest first, orientations as dualize left them
 };
-// _build_multigrid(DirectMode, BinarySubdivision), :752-797, with op = L + shift*I.
+// _build_multigrid(DirectMode or GalerkinMode, BinarySubdivision), :740-797, with op = L + shift*I.
 MGData build_mg(const Mesh& coarse, int levels, int center, double shift, double project_radius,
-                int steps);
+                int steps, bool galerkin = false);
 
 // Krylov.jl cg(A, b, x0; itmax) (warm start, atol = rtol = sqrt(eps)).
 std::vector<double> krylov_cg(const CSC& A, const std::vector<double>& b,

@@ -255,7 +255,7 @@ PYBIND11_MODULE(dec_oracle, mod) {
       .def("set_steps", [](MGData& md, int s) { for (auto& x : md.steps) x = s; });
 
   mod.def("build_mg", &build_mg, py::arg("coarse"), py::arg("levels"), py::arg("center"),
-          py::arg("shift"), py::arg("radius"), py::arg("steps") = 3);
+          py::arg("shift"), py::arg("radius"), py::arg("steps") = 3, py::arg("galerkin") = false);
   mod.def("krylov_cg", [](const MGData& md, int lvl, py::array_t<double, py::array::c_style | py::array::forcecast> b,
                           py::array_t<double, py::array::c_style | py::array::forcecast> x0, int itmax) {
     return to_np(krylov_cg(md.ops.at(lvl), from_np(b), from_np(x0), itmax));

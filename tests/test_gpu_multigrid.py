@@ -325,3 +325,60 @@ def test_full_multigrid_chebyshev(O, dec):
         U = dec.full_multigrid(torch.tensor(B, device="cuda"), mg, cycles).cpu().numpy()
         rel.append(max(np.linalg.norm(B[j] - A @ U[j]) / np.linalg.norm(B[j]) for j in range(3)))
     assert rel[0] < 1e-2 and rel[1] < rel[0] * 1e-2
+
+
+# ---- GalerkinMode (Multigrid.jl:740-748) ------------------------------------------------------
+
+@pytest.mark.parametrize("mu", [1, 2])
+def test_galerkin_hierarchy_and_cg_cycles(O, dec, mu):
+    """Coarse operators R A P built by the library equal the oracle's bit for bit (the same
+    column-by-column products in SparseArrays' order); the CG-smoother μ-cycles on them match
+    the oracle's, and the reference's test_galerkin thresholds hold on the GPU."""
+    s = O.triangulated_grid(1, 1, 1 / 4, np.sqrt(3) / 8, False)
+    md = O.build_mg(s, 4, O.CIRCUMCENTER, 0.0, 0.0, 3, galerkin=True)
+    mg = dec.MultigridData(s, 4, shift=0.0, center="circumcenter", smoother=2, pre=3, post=3, mu=mu,
+                           mode="galerkin")
+    for k in range(5):
+        ref = csc(md.op(k)).toarray()
+        rp, ci, v, shape = mg.level_op(k).csr()
+        import scipy.sparse as sp
+        got = sp.csr_matrix((v, ci, rp), shape=shape).toarray()
+        np.testing.assert_array_equal(got, ref)
+    L = csc(md.op(0))
+    n = L.shape[0]
+    b = L @ ((uniform(0, n) + 1) / 2)
+    u = mg.cycles(torch.zeros(n, dtype=torch.float64, device="cuda"), torch.tensor(b, device="cuda"), 5)
+    u = u.cpu().numpy()
+    ref = O.mu_cycles(md, np.zeros(n), b, 5, mu)
+    assert np.linalg.norm((u - u.mean()) - (ref - ref.mean())) <= 1e-8 * np.linalg.norm(ref - ref.mean())
+    rel = np.linalg.norm(L @ u - b) / np.linalg.norm(b)
+    assert rel < (2e-6 if mu == 1 else 7e-7)
+    f = dec.full_multigrid(torch.tensor(b, device="cuda"), mg, 5).cpu().numpy()
+    assert np.linalg.norm(L @ f - b) / np.linalg.norm(b) < (1e-3 if mu == 1 else 5e-6)
+
+
+def test_galerkin_mixed_precision_solve(O, dec):
+    """GalerkinMode under the FP32-in-FP64 Chebyshev solve on an icosphere Helmholtz problem:
+    reaches the tolerance and the direct solution; per-RHS shifts are refused."""
+    import scipy.sparse.linalg as spla
+    coarse = O.icosahedron()
+    md = O.build_mg(coarse, 4, O.CIRCUMCENTER, 1.0, 1.0, 3, galerkin=True)
+    mg = dec.MultigridData(coarse, 4, shift=1.0, center="circumcenter", project_radius=1.0, precision=1,
+                           mode="galerkin")
+    for k in (1, 4):
+        rp, ci, v, shape = mg.level_op(k).csr()
+        import scipy.sparse as sp
+        np.testing.assert_array_equal(sp.csr_matrix((v, ci, rp), shape=shape).toarray(), csc(md.op(k)).toarray())
+    A = csc(md.op(0)).tocsc()
+    n = A.shape[0]
+    B = np.stack([uniform(900 + j, n) for j in range(3)])
+    U, rep = mg.solve(torch.zeros((3, n), dtype=torch.float64, device="cuda"), torch.tensor(B, device="cuda"),
+                      rtol=1e-10, max_iters=60)
+    assert rep.converged == 1
+    U = U.cpu().numpy()
+    for j in range(3):
+        exact = spla.spsolve(A, B[j])
+        assert np.linalg.norm(U[j] - exact) / np.linalg.norm(exact) < 1e-7
+    with pytest.raises(dec.DecError, match="Galerkin"):
+        dec.MultigridData(coarse, 2, shift=1.0, center="circumcenter", project_radius=1.0, coarse_solver=2,
+                          mode="galerkin")

@@ -348,3 +348,26 @@ def test_cached_3d_wedge_kernels(O):
     c1 = rng.uniform(0, 1, (n, 24))
     c1 /= c1.sum(axis=1, keepdims=True)
     np.testing.assert_allclose(O.c_wedge(0, 3, n, p3, c1, np.ones(nv), beta), beta, rtol=1e-14, atol=1e-15)
+
+
+def test_galerkin_mode_thresholds(O):
+    """test_galerkin (test/Multigrid.jl:115-142) with BinarySubdivision: coarse operators R A P
+    (GalerkinMode, Multigrid.jl:740-748), CG smoothing with 3 steps, the reference's residual
+    thresholds after 5 cycles; each coarse operator is R A P of the level above (scipy, 1e-14)."""
+    s = O.triangulated_grid(1, 1, 1 / 4, np.sqrt(3) / 8, False)
+    md = O.build_mg(s, 4, O.CIRCUMCENTER, 0.0, 0.0, 3, galerkin=True)
+    direct = O.build_mg(s, 4, O.CIRCUMCENTER, 0.0, 0.0, 3)
+    L = csc(md.op(0))
+    np.testing.assert_array_equal(L.toarray(), csc(direct.op(0)).toarray())
+    for k in range(4):
+        rap = csc(md.restriction(k)) @ csc(md.op(k)) @ csc(md.prolongation(k))
+        Ac = csc(md.op(k + 1))
+        assert abs(Ac - rap).max() <= 1e-14 * abs(rap).max()
+    rng = np.random.default_rng(0)
+    b = L @ rng.random(L.shape[0])
+    u0 = np.zeros_like(b)
+    rel = lambda u: np.linalg.norm(L @ u - b) / np.linalg.norm(b)
+    assert rel(O.mu_cycles(md, u0, b, 5, 1)) < 2e-6   # V
+    assert rel(O.mu_cycles(md, u0, b, 5, 2)) < 7e-7   # W
+    assert rel(O.full_multigrid(md, b, 5, 1)) < 1e-3  # FMG-V
+    assert rel(O.full_multigrid(md, b, 5, 2)) < 5e-6  # FMG-W
