@@ -26,8 +26,8 @@ __device__ __forceinline__ T epilogue(T s, T yold, T alpha, T beta, bool has_bet
 constexpr int kOpItems = 4;
 constexpr int kOpThreads = 256;
 
-// d0 x: row e = σ_e (x[∂v0] - x[∂v1]), src/FastDEC.jl:471-494.  (One edge per thread: with
-// several edges per thread these gather-bound kernels measured slower on B200.)
+// d0 x: row e = σ_e (x[∂v0] - x[∂v1]), src/FastDEC.jl:471-494, one edge per thread (FP32 rows
+// whose output is not 16-byte aligned).
 template <class T>
 __global__ void __launch_bounds__(kOpThreads) k_d0(int ne, const int32_t* __restrict__ ev0,
                                                    const int32_t* __restrict__ ev1, const int8_t* __restrict__ es,
@@ -36,6 +36,48 @@ __global__ void __launch_bounds__(kOpThreads) k_d0(int ne, const int32_t* __rest
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
     T s = (T)__ldcs(es + e) * (__ldg(x + __ldcs(ev0 + e)) - __ldg(x + __ldcs(ev1 + e)));
     y[e] = epilogue(s, hb ? y[e] : T(0), alpha, beta, hb);
+  }
+}
+
+// The same rows, IT edges per thread spaced one block apart (consecutive edges stay in one warp,
+// so the two gathers of edges 2e and 2e+1, which share a midpoint vertex, coalesce), every
+// index load issued before any gather: the FP64 path (0.83 of the measured HBM copy bandwidth
+// on icosphere L9 against 0.69 with one edge per thread).
+template <class T, int IT>
+__global__ void __launch_bounds__(kOpThreads) k_d0i(int ne, const int32_t* __restrict__ ev0,
+                                                    const int32_t* __restrict__ ev1, const int8_t* __restrict__ es,
+                                                    const T* __restrict__ x, T* __restrict__ y, T alpha, T beta,
+                                                    bool hb) {
+  for (long long base = (long long)blockIdx.x * kOpThreads * IT; base < ne;
+       base += (long long)gridDim.x * kOpThreads * IT) {
+    int i0[IT], i1[IT];
+    int8_t sg[IT];
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+      const long long e = base + j * kOpThreads + threadIdx.x;
+      if (e < ne) {
+        i0[j] = __ldcs(ev0 + e);
+        i1[j] = __ldcs(ev1 + e);
+        sg[j] = __ldcs(es + e);
+      }
+    }
+    T xa[IT], xb[IT];
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+      const long long e = base + j * kOpThreads + threadIdx.x;
+      if (e < ne) {
+        xa[j] = __ldg(x + i0[j]);
+        xb[j] = __ldg(x + i1[j]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+      const long long e = base + j * kOpThreads + threadIdx.x;
+      if (e < ne) {
+        const T s = (T)sg[j] * (xa[j] - xb[j]);
+        y[e] = epilogue(s, hb ? y[e] : T(0), alpha, beta, hb);
+      }
+    }
   }
 }
 
@@ -675,7 +717,9 @@ static void launch_op(const dec_op& op, const void* vx, void* vy, double alpha, 
   switch (op.kind) {
     case DEC_OP_D0:
       if (!m.ne) break;
-      if (sizeof(T) == 4 && aligned16(y))  // FP64 measured faster one row per thread
+      if (sizeof(T) == 8)  // measured: 4 edges a block apart beat 16-byte vectors for FP64 d0
+        k_d0i<T, 4><<<grid_for(m.ne, TH * 4), TH, 0, s>>>(m.ne, m.ev0.p, m.ev1.p, m.esign.p, x, y, a, b, hb);
+      else if (aligned16(y))
         k_d0v<T><<<grid_for(m.ne / 4 + 1, TH), TH, 0, s>>>(m.ne, m.ev0.p, m.ev1.p, m.esign.p, x, y, a, b, hb);
       else
         k_d0<T><<<grid_for(m.ne, TH), TH, 0, s>>>(m.ne, m.ev0.p, m.ev1.p, m.esign.p, x, y, a, b, hb);
