@@ -687,7 +687,8 @@ class SmootherMLP:
         return y
 
     def set_engine(self, engine):
-        """Kernel engine of the learned smoothing step: "mma" (mma.sync) or "tcgen05"."""
+        """Kernel engine of the learned smoothing step: "tcgen05" (the default; TMEM accumulators,
+        eight 128-sample tile chains per SM) or "mma" (mma.sync)."""
         check(lib().dec_mlp_set_engine(self._h, {"mma": 0, "tcgen05": 1}[engine]))
 
     def grad(self, x, dy):

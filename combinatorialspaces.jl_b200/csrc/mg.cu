@@ -1116,6 +1116,7 @@ struct dec_mg {
   uint64_t epoch = 0;              // bumped whenever workspaces or their graphs are dropped
   bool force_plain = false;        // set while capturing the plain-smoother fallback cycle
   int mlp_engine = -1;             // kernel engine of the network when the graphs were captured
+  uint64_t mlp_version = 0;        // its parameter version then (the tcgen05 kernels take b1 .. b3 by value)
   // Pipelined host-buffer solves (submit / wait): copy-in, compute and copy-out streams, per
   // staging slot the events start, copied in, computed, copied out, and the loop state read back.
   static constexpr int kSlots = 3;
@@ -2005,10 +2006,12 @@ static void drain_pipeline(dec_mg& mg) {
 
 static Workspace& workspace_k(dec_mg& mg, int nrhs, int prec, int K, bool drain = true) {
   if (drain) drain_pipeline(mg);
-  if (mg.mlp && mg.mlp->engine != mg.mlp_engine) {  // captured cycles hold the other engine's kernels
+  if (mg.mlp && (mg.mlp->engine != mg.mlp_engine || mg.mlp->version != mg.mlp_version)) {
+    // captured cycles hold the other engine's kernels, or the earlier per-unit vectors
     for (auto& kv : mg.ws) kv.second->drop_graphs();
     ++mg.epoch;
     mg.mlp_engine = mg.mlp->engine;
+    mg.mlp_version = mg.mlp->version;
   }
   int np = (nrhs + K - 1) / K;
   long long key = ws_key(K, np, prec);

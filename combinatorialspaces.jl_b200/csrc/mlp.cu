@@ -303,31 +303,48 @@ __global__ void __launch_bounds__(kMlpThreads, 3) k_mlp_smooth(MlpWeights w, int
 }
 
 // ---------------------------------------------------------------------------------------------
-// tcgen05 inference (sm_100a): 128 samples per tile, one per thread and TMEM lane.  The
-// features (layer-1 A, 128 x 16) and the first hidden layer (layer-2 A, 128 x 64) are written to
-// shared memory in the canonical K-major layout without swizzle (8-row groups of 16-byte core
-// rows: byte (r / 8) * SBO + (k / 8) * 128 + (r % 8) * 16 + (k % 8) * 2, SBO = K / 8 * 128); W1 and
-// W2 are staged the same way as the B operands (N x K).  One thread issues
-//   tcgen05.mma.cta_group::1.kind::f16  D1[128 x 64] = A1 W1ᵀ            (TMEM columns 0..63)
-//   tcgen05.mma ... x4                   D2[128 x 64] = Σ_s A2_s W2_sᵀ    (columns 64..127)
-// (BF16 operands, FP32 accumulation) and commits to an mbarrier; each thread reads its own row
-// with tcgen05.ld 32x32b.x64, so the bias, ReLU, BF16 rounding and the last layer are per-thread.
-// Every mbarrier wait is bounded: on time-out the block agrees (__syncthreads_and), sets *err,
-// stops, frees its TMEM and returns.
+// tcgen05 inference (sm_100a).  One persistent CTA of 1024 threads per SM runs eight independent
+// tile chains, one per warpgroup.  A warpgroup takes 128 samples at a time (one per thread and
+// TMEM lane) through
+//   features -> A1 (128 x 16, shared)   MMA1: D = A1 W1ᵀ           (the warpgroup's 64 TMEM columns)
+//   D + b1, ReLU, BF16 -> A2 (128 x 64)  MMA2: D = Σ_s A2_s W2_sᵀ   (the same columns)
+//   y = b3 + Σ_j w3_j ReLU(D_j + b2_j)   (FP32, per thread; even and odd j in two lanes)
+// with its own shared-memory stages, mbarrier and named barrier, so eight chains are in flight
+// per SM (the whole 512-column TMEM) and one chain's gathers and epilogues overlap another's
+// MMAs.  W1 and W2 are staged once per CTA; b1, b2, w3 and b3 come by value in the kernel
+// parameters, so the epilogues take them as constant operands (shared-memory broadcast loads of
+// them had kept the load/store pipe 72% busy).  The epilogues use packed FP32 pairs.  The operands are BF16 in the canonical
+// K-major layout without swizzle (8-row groups of 16-byte core rows: byte (r / 8) * SBO +
+// (k / 8) * 128 + (r % 8) * 16 + (k % 8) * 2, SBO = K / 8 * 128); one elected thread of the
+// warpgroup issues tcgen05.mma.cta_group::1.kind::f16 (FP32 accumulation) and commits to the
+// warpgroup's mbarrier; every thread reads its own TMEM lane in 16-column chunks, the next
+// chunk's load in flight while the current one is used.
+// Every mbarrier wait is bounded: on time-out the warpgroup agrees (bar.red.and), waits once more
+// (bounded) for its MMA in flight, sets *err and leaves its loop; the CTA then frees its TMEM and
+// returns.
 // ---------------------------------------------------------------------------------------------
-constexpr int kTc5Rows = 128;
-constexpr uint32_t kTc5Cols = 128;
+constexpr int kTcRows = 128;                     // samples per tile: one warpgroup
+constexpr int kTcGroups = 8;                     // tile chains per CTA
+constexpr int kTcThreads = kTcRows * kTcGroups;  // 1024
+constexpr uint32_t kTcCols = 64 * kTcGroups;     // TMEM columns of the CTA
 
-struct __align__(128) Tc5Smem {
-  __align__(128) __nv_bfloat16 a1[kTc5Rows * kMlpIn];
-  __align__(128) __nv_bfloat16 a2[kTc5Rows * kMlpH];
-  __align__(128) __nv_bfloat16 w1[kMlpH * kMlpIn];
-  __align__(128) __nv_bfloat16 w2[kMlpH * kMlpH];
-  float b1[kMlpH], b2[kMlpH], w3[kMlpH], b3;
-  __align__(8) uint64_t mbar;
-  uint32_t tmem;
+struct __align__(128) TcGroup {
+  __nv_bfloat16 a1[kTcRows * kMlpIn];  // 4 KB
+  __nv_bfloat16 a2[kTcRows * kMlpH];   // 16 KB
 };
+struct __align__(128) TcSmem {
+  __nv_bfloat16 w1[kMlpH * kMlpIn];
+  __nv_bfloat16 w2[kMlpH * kMlpH];
+  uint32_t tmem;
+  uint64_t mbar[kTcGroups];
+  TcGroup g[kTcGroups];
+};
+// dynamic shared memory per CTA (one CTA per SM), with slack to align the struct to 128 bytes
+constexpr size_t kTcSmemBytes = sizeof(TcSmem) + 128;
 
+__device__ __forceinline__ TcSmem& tc_smem(unsigned char* raw) {
+  return *reinterpret_cast<TcSmem*>((reinterpret_cast<uintptr_t>(raw) + 127) & ~uintptr_t(127));
+}
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -342,16 +359,16 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 // instruction descriptor: F32 accumulator, BF16 A and B, both K-major, N = 64, M = 128
-constexpr uint32_t kTc5Idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(64 >> 3) << 17) |
-                               ((uint32_t)(128 >> 4) << 24);
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(64 >> 3) << 17) |
+                              ((uint32_t)(128 >> 4) << 24);
 
-__device__ __forceinline__ void tc5_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
-      "l"(a), "l"(b), "r"(kTc5Idesc), "r"(acc));
+      "l"(a), "l"(b), "r"(kTcIdesc), "r"(acc));
 }
-__device__ __forceinline__ void tc5_commit(uint32_t mbar) {
+__device__ __forceinline__ void tc_commit(uint32_t mbar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
 }
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
@@ -367,31 +384,41 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
   }
   return false;
 }
-__device__ __forceinline__ void tc5_ld64(uint32_t taddr, float (&v)[64]) {
-  uint32_t r[64];
+// 16 consecutive TMEM columns of this thread's lane; the registers are valid after tc_wait16
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,"
-      "%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
-        "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
-        "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
-        "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
-        "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int j = 0; j < 64; ++j) v[j] = __uint_as_float(r[j]);
 }
-__device__ __forceinline__ void tc5_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc5_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// waits for this thread's TMEM loads; the registers are operands, so no use of them moves above it
+__device__ __forceinline__ void tc_wait16(uint32_t (&r)[16]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                 "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                 "+r"(r[15])
+               :
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// the warpgroup's named barrier (ids 1..8; 0 is __syncthreads)
+__device__ __forceinline__ void group_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+__device__ __forceinline__ bool group_all(int id, bool v) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, %2, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(out)
+      : "r"((uint32_t)v), "r"(id)
+      : "memory");
+  return out != 0;
+}
 
 // Writes one sample's 16 features (row r of A1).
-__device__ __forceinline__ void tc5_store_features(Tc5Smem& sm, int r, const float (&f)[16]) {
+__device__ __forceinline__ void tc_store_features(__nv_bfloat16* a1, int r, const float (&f)[16]) {
   uint4 lo, hi;
   lo.x = pack_bf16(f[0], f[1]);
   lo.y = pack_bf16(f[2], f[3]);
@@ -401,114 +428,164 @@ __device__ __forceinline__ void tc5_store_features(Tc5Smem& sm, int r, const flo
   hi.y = pack_bf16(f[10], f[11]);
   hi.z = pack_bf16(f[12], f[13]);
   hi.w = pack_bf16(f[14], f[15]);
-  char* base = reinterpret_cast<char*>(sm.a1);
+  char* base = reinterpret_cast<char*>(a1);
   *reinterpret_cast<uint4*>(base + kmaj(r, 0, kMlpIn)) = lo;
   *reinterpret_cast<uint4*>(base + kmaj(r, 8, kMlpIn)) = hi;
 }
 
-__device__ void tc5_setup(Tc5Smem& sm, const MlpWeights& w) {
+__device__ void tc_setup(TcSmem& sm, const MlpWeights& w) {
   char* w1 = reinterpret_cast<char*>(sm.w1);
   char* w2 = reinterpret_cast<char*>(sm.w2);
   for (int i = threadIdx.x; i < kMlpH * kMlpIn; i += blockDim.x)
     *reinterpret_cast<__nv_bfloat16*>(w1 + kmaj(i / kMlpIn, i % kMlpIn, kMlpIn)) = w.w1[i];
   for (int i = threadIdx.x; i < kMlpH * kMlpH; i += blockDim.x)
     *reinterpret_cast<__nv_bfloat16*>(w2 + kmaj(i / kMlpH, i % kMlpH, kMlpH)) = w.w2[i];
-  for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
-    sm.b1[i] = w.b1[i];
-    sm.b2[i] = w.b2[i];
-    sm.w3[i] = w.w3[i];
-  }
   if (threadIdx.x == 0) {
-    sm.b3 = w.b3[0];
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sm.mbar)) : "memory");
+    for (int g = 0; g < kTcGroups; ++g)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sm.mbar[g])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (threadIdx.x < 32) {  // warp 0 allocates the accumulator columns
+  if (threadIdx.x < 32) {  // warp 0 allocates the accumulator columns of all eight chains
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem)),
-                 "r"(kTc5Cols));
+                 "r"(kTcCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   fence_async_smem();
-  tc5_fence_before();
+  tc_fence_before();
   __syncthreads();
-  tc5_fence_after();
+  tc_fence_after();
 }
 
-__device__ void tc5_teardown(Tc5Smem& sm) {
-  tc5_fence_before();
+__device__ void tc_teardown(TcSmem& sm) {
+  tc_fence_before();
   __syncthreads();
-  tc5_fence_after();
+  tc_fence_after();
   if (threadIdx.x < 32)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sm.tmem), "r"(kTc5Cols));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sm.tmem), "r"(kTcCols));
 }
 
-// The MLP on the CTA's tile (A1 written): returns y of this thread's row, or false on time-out.
-__device__ __forceinline__ bool tc5_tile(Tc5Smem& sm, uint32_t& phase, float& y) {
-  const int r = threadIdx.x;
-  const uint32_t mbar = smem_u32(&sm.mbar);
-  const uint32_t lane_addr = sm.tmem + ((uint32_t)(r & ~31) << 16);
-  fence_async_smem();
-  tc5_fence_before();
-  __syncthreads();
-  if (r == 0) {
-    tc5_fence_after();
-    tc5_mma(sm.tmem, smem_desc(smem_u32(sm.a1), 128, 256), smem_desc(smem_u32(sm.w1), 128, 256), 0);
-    tc5_commit(mbar);
+// Packed FP32 pairs (.f32x2, two IEEE round-to-nearest lanes per instruction).
+__device__ __forceinline__ uint64_t f2(uint32_t lo, uint32_t hi) { return ((uint64_t)hi << 32) | lo; }
+__device__ __forceinline__ uint64_t f2(float lo, float hi) { return f2(__float_as_uint(lo), __float_as_uint(hi)); }
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ float lo_of(uint64_t v) { return __uint_as_float((uint32_t)v); }
+__device__ __forceinline__ float hi_of(uint64_t v) { return __uint_as_float((uint32_t)(v >> 32)); }
+
+// Layer-1 epilogue of one 16-column chunk: A2[r, c0 .. c0+15] = bf16(ReLU(D + b1)), the ReLU and
+// the round-to-nearest BF16 pair in one conversion (a NaN stays NaN there, where max(x, 0) gave 0).
+__device__ __forceinline__ void tc_epi1(const MlpSmall& hs, char* a2, int r, int c0, const uint32_t (&z)[16]) {
+  uint32_t pk[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const uint64_t v = add2(f2(z[2 * j], z[2 * j + 1]), f2(hs.b1[c0 + 2 * j], hs.b1[c0 + 2 * j + 1]));
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(pk[j]) : "f"(hi_of(v)), "f"(lo_of(v)));
   }
-  bool ok = __syncthreads_and(mbar_wait(mbar, phase));
+  *reinterpret_cast<uint4*>(a2 + kmaj(r, c0, kMlpH)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+  *reinterpret_cast<uint4*>(a2 + kmaj(r, c0 + 8, kMlpH)) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+}
+// Layer-3 partial sums of one chunk, two lanes: acc.lo += w3_j ReLU(D_j + b2_j) over even j,
+// acc.hi over odd j.
+__device__ __forceinline__ void tc_epi2(const MlpSmall& hs, int c0, const uint32_t (&z)[16], uint64_t& acc) {
+#pragma unroll
+  for (int j = 0; j < 16; j += 2) {
+    const uint64_t v = add2(f2(z[j], z[j + 1]), f2(hs.b2[c0 + j], hs.b2[c0 + j + 1]));
+    const uint64_t h = f2(fmaxf(lo_of(v), 0.f), fmaxf(hi_of(v), 0.f));
+    acc = fma2(f2(hs.w3[c0 + j], hs.w3[c0 + j + 1]), h, acc);
+  }
+}
+
+// The MLP on warpgroup g's tile (A1 written by every thread of the group): y of this thread's row,
+// or false on time-out.
+__device__ __forceinline__ bool tc_tile(TcSmem& sm, const MlpSmall& hs, int g, int r, uint32_t& phase, float& y) {
+  const int bar = 1 + g;
+  const uint32_t mbar = smem_u32(&sm.mbar[g]);
+  const uint32_t dcol = sm.tmem + 64u * g;
+  const uint32_t lane = dcol + ((uint32_t)(r & ~31) << 16);
+  TcGroup& G = sm.g[g];
+  fence_async_smem();
+  tc_fence_before();
+  group_sync(bar);
+  if (r == 0) {
+    tc_fence_after();
+    tc_mma(dcol, smem_desc(smem_u32(G.a1), 128, 256), smem_desc(smem_u32(sm.w1), 128, 256), 0);
+    tc_commit(mbar);
+  }
+  bool ok = group_all(bar, mbar_wait(mbar, phase));
   if (!ok) {  // one more bounded wait for the MMA in flight before the TMEM is freed
     mbar_wait(mbar, phase);
     return false;
   }
   phase ^= 1;
-  tc5_fence_after();
-  float z[64];
-  tc5_ld64(lane_addr, z);
-  char* a2 = reinterpret_cast<char*>(sm.a2);
-#pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    uint4 v;
-    v.x = pack_bf16(fmaxf(z[8 * c + 0] + sm.b1[8 * c + 0], 0.f), fmaxf(z[8 * c + 1] + sm.b1[8 * c + 1], 0.f));
-    v.y = pack_bf16(fmaxf(z[8 * c + 2] + sm.b1[8 * c + 2], 0.f), fmaxf(z[8 * c + 3] + sm.b1[8 * c + 3], 0.f));
-    v.z = pack_bf16(fmaxf(z[8 * c + 4] + sm.b1[8 * c + 4], 0.f), fmaxf(z[8 * c + 5] + sm.b1[8 * c + 5], 0.f));
-    v.w = pack_bf16(fmaxf(z[8 * c + 6] + sm.b1[8 * c + 6], 0.f), fmaxf(z[8 * c + 7] + sm.b1[8 * c + 7], 0.f));
-    *reinterpret_cast<uint4*>(a2 + kmaj(r, 8 * c, kMlpH)) = v;
-  }
+  tc_fence_after();
+  char* a2 = reinterpret_cast<char*>(G.a2);
+  uint32_t za[16], zb[16];
+  tc_ld16(lane, za);
+  tc_wait16(za);
+  tc_ld16(lane + 16, zb);
+  tc_epi1(hs, a2, r, 0, za);
+  tc_wait16(zb);
+  tc_ld16(lane + 32, za);
+  tc_epi1(hs, a2, r, 16, zb);
+  tc_wait16(za);
+  tc_ld16(lane + 48, zb);
+  tc_epi1(hs, a2, r, 32, za);
+  tc_wait16(zb);
+  tc_epi1(hs, a2, r, 48, zb);
   fence_async_smem();
-  tc5_fence_before();
-  __syncthreads();
+  tc_fence_before();
+  group_sync(bar);  // every lane has read D1 and written its A2 row
   if (r == 0) {
-    tc5_fence_after();
+    tc_fence_after();
 #pragma unroll
     for (int ks = 0; ks < 4; ++ks)
-      tc5_mma(sm.tmem + 64, smem_desc(smem_u32(sm.a2) + 256 * ks, 128, 1024),
-              smem_desc(smem_u32(sm.w2) + 256 * ks, 128, 1024), ks > 0 ? 1u : 0u);
-    tc5_commit(mbar);
+      tc_mma(dcol, smem_desc(smem_u32(G.a2) + 256 * ks, 128, 1024), smem_desc(smem_u32(sm.w2) + 256 * ks, 128, 1024),
+             ks > 0 ? 1u : 0u);
+    tc_commit(mbar);
   }
-  ok = __syncthreads_and(mbar_wait(mbar, phase));
+  ok = group_all(bar, mbar_wait(mbar, phase));
   if (!ok) {
     mbar_wait(mbar, phase);
     return false;
   }
   phase ^= 1;
-  tc5_fence_after();
-  tc5_ld64(lane_addr + 64, z);
-  float acc = sm.b3;
-#pragma unroll
-  for (int j = 0; j < 64; ++j) acc += sm.w3[j] * fmaxf(z[j] + sm.b2[j], 0.f);
-  y = acc;
+  tc_fence_after();
+  uint64_t acc = 0;  // two FP32 zeros
+  tc_ld16(lane, za);
+  tc_wait16(za);
+  tc_ld16(lane + 16, zb);
+  tc_epi2(hs, 0, za, acc);
+  tc_wait16(zb);
+  tc_ld16(lane + 32, za);
+  tc_epi2(hs, 16, zb, acc);
+  tc_wait16(za);
+  tc_ld16(lane + 48, zb);
+  tc_epi2(hs, 32, za, acc);
+  tc_wait16(zb);
+  tc_epi2(hs, 48, zb, acc);
+  y = hs.b3 + (lo_of(acc) + hi_of(acc));
   return true;
 }
 
 // y = MLP(x) for n samples of 16 FP32 features (tcgen05).
-__global__ void __launch_bounds__(kTc5Rows) k_mlp_eval_tc5(int64_t n, const float* __restrict__ x,
-                                                           float* __restrict__ y, MlpWeights w, int* err) {
-  __shared__ Tc5Smem sm;
-  tc5_setup(sm, w);
+__global__ void __launch_bounds__(kTcThreads, 1) k_mlp_eval_tcg(int64_t n, const float* __restrict__ x,
+                                                              float* __restrict__ y, MlpWeights w, int* err) {
+  extern __shared__ unsigned char tc_raw[];
+  TcSmem& sm = tc_smem(tc_raw);
+  tc_setup(sm, w);
+  const int g = threadIdx.x / kTcRows, rr = threadIdx.x % kTcRows;
   uint32_t phase = 0;
-  const int64_t ntiles = (n + kTc5Rows - 1) / kTc5Rows;
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int64_t q = tile * kTc5Rows + threadIdx.x;
+  const int64_t ntiles = (n + kTcRows - 1) / kTcRows;
+  for (int64_t tile = (int64_t)blockIdx.x * kTcGroups + g; tile < ntiles; tile += (int64_t)gridDim.x * kTcGroups) {
+    const int64_t q = tile * kTcRows + rr;
     float f[16];
     if (q < n) {
       const float4* src = reinterpret_cast<const float4*>(x + q * 16);
@@ -524,34 +601,37 @@ __global__ void __launch_bounds__(kTc5Rows) k_mlp_eval_tc5(int64_t n, const floa
 #pragma unroll
       for (int k = 0; k < 16; ++k) f[k] = 0.f;
     }
-    tc5_store_features(sm, threadIdx.x, f);
+    tc_store_features(sm.g[g].a1, rr, f);
     float yv;
-    if (!tc5_tile(sm, phase, yv)) {
-      if (threadIdx.x == 0) atomicExch(err, 1);
+    if (!tc_tile(sm, w.hs, g, rr, phase, yv)) {
+      if (rr == 0) atomicExch(err, 1);
       break;
     }
     if (q < n) y[q] = yv;
   }
-  tc5_teardown(sm);
+  tc_teardown(sm);
 }
 
 // Learned smoothing step with the tcgen05 MLP (same features and update as k_mlp_smooth).
 template <class T, int K>
-__global__ void __launch_bounds__(kTc5Rows) k_mlp_smooth_tc5(MlpWeights w, int n, int W,
-                                                             const int32_t* __restrict__ col,
-                                                             const float4* __restrict__ tab,
-                                                             const T* __restrict__ diag, const T* __restrict__ r,
-                                                             const T* __restrict__ x, int zero_x, T* __restrict__ out,
-                                                             size_t pstride, int np, int* err) {
-  __shared__ Tc5Smem sm;
-  tc5_setup(sm, w);
+__global__ void __launch_bounds__(kTcThreads, 1) k_mlp_smooth_tcg(MlpWeights w, int n, int W,
+                                                                const int32_t* __restrict__ col,
+                                                                const float4* __restrict__ tab,
+                                                                const T* __restrict__ diag, const T* __restrict__ r,
+                                                                const T* __restrict__ x, int zero_x,
+                                                                T* __restrict__ out, size_t pstride, int np,
+                                                                int* err) {
+  extern __shared__ unsigned char tc_raw[];
+  TcSmem& sm = tc_smem(tc_raw);
+  tc_setup(sm, w);
+  const int g = threadIdx.x / kTcRows, rr = threadIdx.x % kTcRows;
   uint32_t phase = 0;
   const int64_t nq = (int64_t)n * K;
-  const int64_t tiles_per_panel = (nq + kTc5Rows - 1) / kTc5Rows;
+  const int64_t tiles_per_panel = (nq + kTcRows - 1) / kTcRows;
   const int64_t ntiles = tiles_per_panel * np;
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  for (int64_t tile = (int64_t)blockIdx.x * kTcGroups + g; tile < ntiles; tile += (int64_t)gridDim.x * kTcGroups) {
     const size_t po = (size_t)(tile / tiles_per_panel) * pstride;
-    const int64_t q = (tile % tiles_per_panel) * kTc5Rows + threadIdx.x;
+    const int64_t q = (tile % tiles_per_panel) * kTcRows + rr;
     float f[16];
     float dsc = 0.f;
     T xv = T(0);
@@ -587,38 +667,35 @@ __global__ void __launch_bounds__(kTc5Rows) k_mlp_smooth_tc5(MlpWeights w, int n
 #pragma unroll
       for (int k2 = 0; k2 < 16; ++k2) f[k2] = 0.f;
     }
-    tc5_store_features(sm, threadIdx.x, f);
+    tc_store_features(sm.g[g].a1, rr, f);
     float yv;
-    if (!tc5_tile(sm, phase, yv)) {
-      if (threadIdx.x == 0) atomicExch(err, 1);
+    if (!tc_tile(sm, w.hs, g, rr, phase, yv)) {
+      if (rr == 0) atomicExch(err, 1);
       break;
     }
     if (q < nq) out[po + q] = xv + (T)(dsc * yv);
   }
-  tc5_teardown(sm);
+  tc_teardown(sm);
 }
 
-// Dynamic shared memory that caps the tcgen05 kernels at 4 resident CTAs per SM, so the
-// 4 x 128 TMEM columns they allocate always fit (no CTA waits in tcgen05.alloc).
-constexpr int kTc5PadSmem = 24 * 1024;
-
-static unsigned tc5_grid(long long tiles) {
-  return (unsigned)std::max<long long>(1, std::min<long long>(tiles, (long long)num_sms() * 4));
+static unsigned tc_grid(long long tiles) {
+  const long long ctas = (tiles + kTcGroups - 1) / kTcGroups;
+  return (unsigned)std::max<long long>(1, std::min<long long>(ctas, (long long)num_sms()));
 }
 
-// Static + padding shared memory exceeds 48 KB, which needs the kernel's opt-in.
+// The tcgen05 kernels' shared memory exceeds 48 KB, which needs each kernel's opt-in.
 template <class F>
-static void tc5_opt_in(F* kernel) {
-  DEC_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTc5PadSmem));
+static void tc_opt_in(F* kernel) {
+  DEC_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes));
 }
 
 template <class T, int K>
 void launch_mlp_smooth(const MlpWeights& w, int n, int W, const int32_t* col, const float4* tab, const T* diag,
                        const T* r, const T* x, int zero_x, T* out, int np, cudaStream_t s) {
   if (w.engine == 1) {
-    const long long tiles = ((long long)n * K + kTc5Rows - 1) / kTc5Rows * np;
-    k_mlp_smooth_tc5<T, K><<<tc5_grid(tiles), kTc5Rows, kTc5PadSmem, s>>>(w, n, W, col, tab, diag, r, x, zero_x, out,
-                                                                          (size_t)n * K, np, w.err);
+    const long long tiles = ((long long)n * K + kTcRows - 1) / kTcRows * np;
+    k_mlp_smooth_tcg<T, K><<<tc_grid(tiles), kTcThreads, kTcSmemBytes, s>>>(w, n, W, col, tab, diag, r, x, zero_x,
+                                                                          out, (size_t)n * K, np, w.err);
     DEC_CHECK_LAUNCH();
     return;
   }
@@ -630,10 +707,10 @@ void launch_mlp_smooth(const MlpWeights& w, int n, int W, const int32_t* col, co
   DEC_CHECK_LAUNCH();
 }
 
-// Opts every tcgen05 kernel into its shared-memory padding on the current device.
-void tc5_opt_in_all() {
-  tc5_opt_in(k_mlp_eval_tc5);
-#define DEC_OPT(T, K) tc5_opt_in(k_mlp_smooth_tc5<T, K>);
+// Opts every tcgen05 kernel into its shared memory on the current device.
+void tc_opt_in_all() {
+  tc_opt_in(k_mlp_eval_tcg);
+#define DEC_OPT(T, K) tc_opt_in(k_mlp_smooth_tcg<T, K>);
   DEC_OPT(float, 1) DEC_OPT(float, 2) DEC_OPT(float, 4) DEC_OPT(float, 8) DEC_OPT(float, 16) DEC_OPT(float, 32)
   DEC_OPT(double, 1) DEC_OPT(double, 2) DEC_OPT(double, 4) DEC_OPT(double, 8) DEC_OPT(double, 16)
   DEC_OPT(double, 32)
@@ -1049,6 +1126,17 @@ static uint32_t crc32(const unsigned char* p, size_t n) {
 
 using namespace decb;
 
+// After every change of the parameters: the host copy of the per-unit vectors, and a new
+// version (cycles captured with the old copy are captured again).
+static void refresh_small(dec_mlp* m) {
+  DEC_CUDA(cudaDeviceSynchronize());
+  DEC_CUDA(cudaMemcpy(m->hsmall.b1, m->master.p + kOffB1, kMlpH * 4, cudaMemcpyDeviceToHost));
+  DEC_CUDA(cudaMemcpy(m->hsmall.b2, m->master.p + kOffB2, kMlpH * 4, cudaMemcpyDeviceToHost));
+  DEC_CUDA(cudaMemcpy(m->hsmall.w3, m->master.p + kOffW3, kMlpH * 4, cudaMemcpyDeviceToHost));
+  DEC_CUDA(cudaMemcpy(&m->hsmall.b3, m->master.p + kOffB3, 4, cudaMemcpyDeviceToHost));
+  ++m->version;
+}
+
 dec_mlp* mlp_create_impl(uint64_t seed) {
   auto* m = new dec_mlp();
   try {
@@ -1078,7 +1166,8 @@ dec_mlp* mlp_create_impl(uint64_t seed) {
     DEC_CUDA(cudaMemset(m->err.p, 0, sizeof(int)));
     k_refresh_bf16<<<16, 256>>>(m->master.p, m->w1b.p, m->w2b.p);
     DEC_CHECK_LAUNCH();
-    DEC_CUDA(cudaDeviceSynchronize());
+    refresh_small(m);
+    tc_opt_in_all();  // the default engine's kernels, outside any stream capture
   } catch (...) {
     delete m;
     throw;
@@ -1095,7 +1184,7 @@ void mlp_params_impl(dec_mlp* m, float* out, const float* in) {
     DEC_CUDA(cudaMemcpy(m->master.p, in, m->master.bytes(), cudaMemcpyHostToDevice));
     k_refresh_bf16<<<16, 256>>>(m->master.p, m->w1b.p, m->w2b.p);
     DEC_CHECK_LAUNCH();
-    DEC_CUDA(cudaDeviceSynchronize());
+    refresh_small(m);
   }
 }
 
@@ -1123,7 +1212,7 @@ void mlp_check_error(const dec_mlp* m, cudaStream_t s) {
 void mlp_set_engine_impl(dec_mlp* m, int engine) {
   require(m != nullptr, "mlp: null handle");
   require(engine == 0 || engine == 1, "mlp: engine must be 0 (mma.sync) or 1 (tcgen05)");
-  if (engine == 1) tc5_opt_in_all();  // outside any stream capture
+  if (engine == 1) tc_opt_in_all();  // outside any stream capture
   m->engine = engine;
 }
 
@@ -1133,8 +1222,9 @@ void mlp_eval_impl(dec_mlp* m, const float* x, int64_t n, float* y, int tensor_c
   if (n == 0) return;
   cudaStream_t s = as_stream(stream);
   if (tensor_cores == 2) {
-    tc5_opt_in(k_mlp_eval_tc5);
-    k_mlp_eval_tc5<<<tc5_grid((n + kTc5Rows - 1) / kTc5Rows), kTc5Rows, kTc5PadSmem, s>>>(n, x, y, m->view(), m->err.p);
+    tc_opt_in(k_mlp_eval_tcg);
+    k_mlp_eval_tcg<<<tc_grid((n + kTcRows - 1) / kTcRows), kTcThreads, kTcSmemBytes, s>>>(n, x, y, m->view(),
+                                                                                        m->err.p);
     DEC_CHECK_LAUNCH();
     mlp_check_error(m, s);
     return;
@@ -1203,6 +1293,7 @@ void mlp_train_impl(dec_mlp* m, dec_op* op, const double* r, int S, int steps, d
     DEC_CHECK_LAUNCH();
     if (losses) losses[it] = host_loss(*m, s);  // the loss before this step's update
   }
+  if (steps > 0) refresh_small(m);
 }
 
 // Checkpoint: "DECMLP01" | u32 version | u32 nparam | i64 step | f32 master, adam_m, adam_v
@@ -1263,5 +1354,5 @@ void mlp_load_impl(dec_mlp* m, const char* path) {
   m->step = step;
   k_refresh_bf16<<<16, 256>>>(m->master.p, m->w1b.p, m->w2b.p);
   DEC_CHECK_LAUNCH();
-  DEC_CUDA(cudaDeviceSynchronize());
+  refresh_small(m);
 }

@@ -14,6 +14,12 @@ constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kMlpH * kMlpIn, kOffW2 = kOffB1 + kM
               kOffW3 = kOffB2 + kMlpH, kOffB3 = kOffW3 + kMlpH;
 
 // Device view of the inference weights: W1, W2 in BF16, the rest FP32.
+// The network's per-unit vectors, passed by value (kernel parameter space) to the tcgen05
+// kernels, whose epilogues then read them as constant operands instead of shared memory.
+struct MlpSmall {
+  float b1[kMlpH], b2[kMlpH], w3[kMlpH], b3;
+};
+
 struct MlpWeights {
   const __nv_bfloat16* w1;  // [64][16]
   const __nv_bfloat16* w2;  // [64][64]
@@ -23,6 +29,7 @@ struct MlpWeights {
   const float* b3;          // 1
   int engine;               // 0: mma.sync kernels, 1: tcgen05 / TMEM kernels
   int* err;                 // set by a kernel whose bounded wait timed out
+  MlpSmall hs;              // b1, b2, w3, b3 as of the last parameter change (host copy)
 };
 
 // Features of one vertex sample from its residual and its 1-ring (used by inference and
@@ -65,10 +72,12 @@ struct dec_mlp {
   decb::DArr<float> gpart;    // per-chunk gradient partials
   decb::DArr<double> lpart, nrm;
   decb::DArr<int> err;        // device error flag of the tcgen05 kernels
-  int engine = 0;
+  int engine = 1;             // tcgen05 (1) by default; mma.sync (0) on request
+  decb::MlpSmall hsmall{};    // host copy of b1, b2, w3, b3 (refreshed with every parameter change)
+  uint64_t version = 0;       // bumped with every parameter change (captured cycles hold hsmall)
   decb::MlpWeights view() const {
     return {w1b.p, w2b.p, master.p + decb::kOffB1, master.p + decb::kOffB2, master.p + decb::kOffW3,
-            master.p + decb::kOffB3, engine, err.p};
+            master.p + decb::kOffB3, engine, err.p, hsmall};
   }
 };
 

@@ -308,8 +308,9 @@ dec_status dec_mlp_step(const dec_mlp* mlp, int64_t* step);
  * mma.sync, 2 with tcgen05 / TMEM (this one synchronises the stream and returns DEC_ERR_TIMEOUT if
  * a bounded wait for the tensor core ran out). */
 dec_status dec_mlp_eval(dec_mlp* mlp, const float* x, int64_t n, float* y, int32_t tensor_cores, void* stream);
-/* Kernel engine of the learned smoothing step: 0 = mma.sync (m16n8k16, warp tiles of 32 samples),
- * 1 = tcgen05.mma with TMEM accumulators (CTA tiles of 128 samples). */
+/* Kernel engine of the learned smoothing step: 1 (the default) = tcgen05.mma with TMEM accumulators
+ * (one 1024-thread CTA per SM, eight chains of 128-sample tiles); 0 = mma.sync (m16n8k16, warp tiles
+ * of 32 samples). */
 dec_status dec_mlp_set_engine(dec_mlp* mlp, int32_t engine);
 /* grad[DEC_MLP_NPARAM] (device) = sum_q dy[q] d MLP(x_q) / d params. */
 dec_status dec_mlp_grad(dec_mlp* mlp, const float* x, const float* dy, int64_t n, float* grad, void* stream);
