@@ -239,7 +239,10 @@ def measure_learned(dec, args, B, U64, common, timed):
     out = {"train": {"steps": args.train_steps, "seconds": train_s, "final_losses": [round(l, 4) for _, _, l in losses[-3:]]}}
 
     def run(level, smoother, sweeps, Bm, Uref=None, engine="tcgen05"):
+        # the learned V(1,1) solve is fastest with 2 cycles per refinement step (measured 1, 2, 3)
         opts = dict(common, smoother=smoother, pre=sweeps, post=sweeps)
+        if smoother == 3:
+            opts["inner_cycles"] = 2
         mg = dec.MultigridData(ico, level, precision=1, **opts)
         if smoother == 3:
             mlp.set_engine(engine)
