@@ -35,6 +35,10 @@ struct Error : std::runtime_error {
 inline void require(bool ok, const std::string& msg) {
   if (!ok) throw Error(DEC_ERR_INVALID_ARG, msg);
 }
+// A literal message builds no string unless the check fails (checks inside per-element loops).
+inline void require(bool ok, const char* msg) {
+  if (!ok) throw Error(DEC_ERR_INVALID_ARG, msg);
+}
 
 // Owning device array.
 template <class T>

@@ -10,6 +10,8 @@
 #include <algorithm>
 #include <cmath>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "mesh.cuh"
 
 namespace decb {
@@ -187,15 +189,130 @@ static bool orient_triangles(int ne, int nt, const std::vector<int32_t>* te, std
   return true;
 }
 
-// Counting sort of (key, value) pairs, stable in insertion order.
-static void csr_from_pairs(int nkeys, const std::vector<int32_t>& keys, const std::vector<int32_t>& vals,
-                           std::vector<int32_t>& ptr, std::vector<int32_t>& out) {
-  ptr.assign(nkeys + 1, 0);
-  for (auto k : keys) ptr[k + 1]++;
-  for (int i = 0; i < nkeys; ++i) ptr[i + 1] += ptr[i];
-  out.resize(keys.size());
-  std::vector<int32_t> pos(ptr.begin(), ptr.end() - 1);
-  for (size_t q = 0; q < keys.size(); ++q) out[pos[keys[q]]++] = vals[q];
+// ---------------------------------------------------------------------------------------------
+// derived topology on the device
+// ---------------------------------------------------------------------------------------------
+// Per triangle: its vertices (∂v1∂e1, ∂v0∂e2, ∂v0∂e1) and its d1 row, the three edges sorted by
+// index (equal edges by position) with their coefficients τ(σ0, -σ1, σ2) packed as sign bits.
+__global__ void k_tri_topo(int nt, const int32_t* __restrict__ ev0, const int32_t* __restrict__ ev1,
+                           const int32_t* __restrict__ te0, const int32_t* __restrict__ te1,
+                           const int32_t* __restrict__ te2, const int8_t* __restrict__ esign,
+                           const int8_t* __restrict__ tsign, int32_t* __restrict__ tv0, int32_t* __restrict__ tv1,
+                           int32_t* __restrict__ tv2, int32_t* __restrict__ c0, int32_t* __restrict__ c1,
+                           int32_t* __restrict__ c2, uint8_t* __restrict__ neg) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+    const int es[3] = {te0[t], te1[t], te2[t]};
+    tv0[t] = ev1[es[1]];
+    tv1[t] = ev0[es[2]];
+    tv2[t] = ev0[es[1]];
+    const int ts = tsign[t];
+    const int sg[3] = {esign[es[0]] * ts, -esign[es[1]] * ts, esign[es[2]] * ts};
+    int ord[3] = {0, 1, 2};
+    for (int a = 1; a < 3; ++a)
+      for (int b = a; b > 0 && es[ord[b - 1]] > es[ord[b]]; --b) {
+        const int x = ord[b];
+        ord[b] = ord[b - 1];
+        ord[b - 1] = x;
+      }
+    c0[t] = es[ord[0]];
+    c1[t] = es[ord[1]];
+    c2[t] = es[ord[2]];
+    neg[t] = (uint8_t)((sg[ord[0]] < 0) | ((sg[ord[1]] < 0) << 1) | ((sg[ord[2]] < 0) << 2));
+  }
+}
+
+// Pairs (x_k[t], 3t+k) pushed k-major: entry k*nt + t.
+__global__ void k_pairs_tri(int nt, const int32_t* __restrict__ x0, const int32_t* __restrict__ x1,
+                            const int32_t* __restrict__ x2, int32_t* __restrict__ keys, int32_t* __restrict__ vals) {
+  const long long n = 3LL * nt;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(q / nt), t = (int)(q % nt);
+    keys[q] = k == 0 ? x0[t] : k == 1 ? x1[t] : x2[t];
+    vals[q] = 3 * t + k;
+  }
+}
+
+// Pairs (edge of d1 row t, ±(t+1)) pushed triangle-major: entry 3t+q.
+__global__ void k_pairs_d1t(int nt, const int32_t* __restrict__ c0, const int32_t* __restrict__ c1,
+                            const int32_t* __restrict__ c2, const uint8_t* __restrict__ neg,
+                            int32_t* __restrict__ keys, int32_t* __restrict__ vals) {
+  const long long n = 3LL * nt;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int t = (int)(i / 3), q = (int)(i % 3);
+    keys[i] = q == 0 ? c0[t] : q == 1 ? c1[t] : c2[t];
+    vals[i] = ((neg[t] >> q) & 1) ? -(t + 1) : (t + 1);
+  }
+}
+
+// Pairs (vertex, ±(e+1)) of d0ᵀ pushed edge-major, lower vertex first (entries 2e, 2e+1); a loop
+// edge gets the key nv (past every vertex, so it sorts last and is left out of the lists).
+__global__ void k_pairs_d0t(int ne, int nv, const int32_t* __restrict__ ev0, const int32_t* __restrict__ ev1,
+                            const int8_t* __restrict__ esign, int32_t* __restrict__ keys,
+                            int32_t* __restrict__ vals) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+    const int a = ev0[e], b = ev1[e], s = esign[e];
+    if (a == b) {
+      keys[2 * (size_t)e] = keys[2 * (size_t)e + 1] = nv;
+      vals[2 * (size_t)e] = vals[2 * (size_t)e + 1] = 0;
+      continue;
+    }
+    const int lo = min(a, b), hi = max(a, b);
+    const int slo = lo == a ? s : -s, shi = hi == a ? s : -s;
+    keys[2 * (size_t)e] = lo;
+    vals[2 * (size_t)e] = slo > 0 ? e + 1 : -(e + 1);
+    keys[2 * (size_t)e + 1] = hi;
+    vals[2 * (size_t)e + 1] = shi > 0 ? e + 1 : -(e + 1);
+  }
+}
+
+__global__ void k_iota(long long n, int32_t* __restrict__ a) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    a[q] = (int32_t)q;
+}
+__global__ void k_gather_vals(long long n, const int32_t* __restrict__ order, const int32_t* __restrict__ vals,
+                              int32_t* __restrict__ out) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    out[q] = vals[order[q]];
+}
+// Row pointers from keys sorted ascending: ptr[k] = first position whose key is >= k (keys past
+// nkeys - 1 count as nkeys), ptr[nkeys] = the pairs with a key below nkeys.
+__global__ void k_bounds(long long n, int nkeys, const int32_t* __restrict__ ks, int32_t* __restrict__ ptr) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q <= n; q += (long long)gridDim.x * blockDim.x) {
+    const int prev = q == 0 ? -1 : min(ks[q - 1], nkeys);
+    const int cur = q == n ? nkeys : min(ks[q], nkeys);
+    for (int k = prev + 1; k <= cur; ++k) ptr[k] = (int32_t)q;
+  }
+}
+__global__ void k_max_degree(int n, const int32_t* __restrict__ ptr, int* __restrict__ mx) {
+  int m = 0;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    m = max(m, ptr[v + 1] - ptr[v]);
+  if (m) atomicMax(mx, m);
+}
+
+// CSR of (key, value) pairs with each key's values in push order: a stable radix sort of the
+// keys with their push positions, then the values gathered in that order.
+static void csr_from_pairs_dev(int nkeys, long long npairs, const int32_t* keys, const int32_t* vals,
+                               DArr<int32_t>& ptr, DArr<int32_t>& out) {
+  const int T = 256;
+  ptr.alloc((size_t)nkeys + 1);
+  out.alloc(std::max<size_t>(1, (size_t)npairs));
+  if (npairs == 0) {
+    DEC_CUDA(cudaMemset(ptr.p, 0, ptr.bytes()));
+    return;
+  }
+  DArr<int32_t> idx(npairs), ks(npairs), is(npairs);
+  k_iota<<<grid_for(npairs, T), T>>>(npairs, idx.p);
+  DEC_CHECK_LAUNCH();
+  int bits = 1;
+  while (bits < 31 && (1LL << bits) <= nkeys) ++bits;  // keys lie in [0, nkeys]
+  size_t tmp_bytes = 0;
+  DEC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, ks.p, idx.p, is.p, (int)npairs, 0, bits));
+  DArr<unsigned char> tmp(std::max<size_t>(1, tmp_bytes));
+  DEC_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, keys, ks.p, idx.p, is.p, (int)npairs, 0, bits));
+  k_gather_vals<<<grid_for(npairs, T), T>>>(npairs, is.p, vals, out.p);
+  k_bounds<<<grid_for(npairs + 1, T), T>>>(npairs, nkeys, ks.p, ptr.p);
+  DEC_CHECK_LAUNCH();
 }
 
 void Mesh::build(const dec_mesh_desc& d) {
@@ -247,102 +364,55 @@ void Mesh::build(const dec_mesh_desc& d) {
       throw Error(DEC_ERR_NON_ORIENTABLE, "The 2-simplices of the given 2D delta set are non-orientable.");
   }
 
-  // Triangle vertices and the simplicial identities they rely on.
-  std::vector<int32_t> h_tv0(nt), h_tv1(nt), h_tv2(nt);
-  for (int t = 0; t < nt; ++t) {
-    h_tv0[t] = h_ev1[h_te1[t]];
-    h_tv1[t] = h_ev0[h_te2[t]];
-    h_tv2[t] = h_ev0[h_te1[t]];
-  }
-  // d1 rows sorted by edge index, with signs τ(σ0, -σ1, σ2).
-  std::vector<int32_t> c0(nt), c1(nt), c2(nt);
-  std::vector<uint8_t> neg(nt);
-  for (int t = 0; t < nt; ++t) {
-    int ts = h_to[t] ? 1 : -1;
-    int es[3] = {h_te0[t], h_te1[t], h_te2[t]};
-    int sg[3] = {(h_eo[es[0]] ? 1 : -1) * ts, -(h_eo[es[1]] ? 1 : -1) * ts, (h_eo[es[2]] ? 1 : -1) * ts};
-    int ord[3] = {0, 1, 2};
-    std::sort(ord, ord + 3, [&](int a, int b) { return es[a] < es[b] || (es[a] == es[b] && a < b); });
-    c0[t] = es[ord[0]];
-    c1[t] = es[ord[1]];
-    c2[t] = es[ord[2]];
-    neg[t] = (uint8_t)((sg[ord[0]] < 0) | ((sg[ord[1]] < 0) << 1) | ((sg[ord[2]] < 0) << 2));
-  }
-  // Incidence lists.
-  std::vector<int32_t> keys, vals, ptr, out;
-  keys.reserve(3 * (size_t)nt);
-  vals.reserve(3 * (size_t)nt);
-  for (int k = 0; k < 3; ++k)
-    for (int t = 0; t < nt; ++t) {
-      keys.push_back(k == 0 ? h_tv0[t] : k == 1 ? h_tv1[t] : h_tv2[t]);
-      vals.push_back(3 * t + k);
-    }
-  csr_from_pairs(nv, keys, vals, ptr, out);
-  v2t_ptr.upload(ptr);
-  v2t.upload(out);
-  keys.clear();
-  vals.clear();
-  for (int k = 0; k < 3; ++k)
-    for (int t = 0; t < nt; ++t) {
-      keys.push_back(k == 0 ? h_te0[t] : k == 1 ? h_te1[t] : h_te2[t]);
-      vals.push_back(3 * t + k);
-    }
-  csr_from_pairs(ne, keys, vals, ptr, out);
-  e2t_ptr.upload(ptr);
-  e2t.upload(out);
-  // d1ᵀ rows: for edge e, entries (t, coefficient of e in d1 row t), sorted by t.
-  keys.clear();
-  vals.clear();
-  for (int t = 0; t < nt; ++t) {
-    int cs[3] = {c0[t], c1[t], c2[t]};
-    for (int q = 0; q < 3; ++q) {
-      keys.push_back(cs[q]);
-      vals.push_back(((neg[t] >> q) & 1) ? -(t + 1) : (t + 1));
-    }
-  }
-  csr_from_pairs(ne, keys, vals, ptr, out);
-  e2ts_ptr.upload(ptr);
-  e2ts.upload(out);
-  // d0ᵀ rows: for vertex v, entries (e, d0[e, v]) sorted by e (d0[e,∂v0] = σ, d0[e,∂v1] = -σ).
-  keys.clear();
-  vals.clear();
-  for (int e = 0; e < ne; ++e) {
-    int s = h_eo[e] ? 1 : -1;
-    int a = h_ev0[e], b = h_ev1[e];
-    if (a == b) continue;
-    int lo = std::min(a, b), hi = std::max(a, b);
-    int slo = (lo == a) ? s : -s, shi = (hi == a) ? s : -s;
-    keys.push_back(lo);
-    vals.push_back(slo > 0 ? e + 1 : -(e + 1));
-    keys.push_back(hi);
-    vals.push_back(shi > 0 ? e + 1 : -(e + 1));
-  }
-  csr_from_pairs(nv, keys, vals, ptr, out);
-  max_v2e = 0;
-  for (int v = 0; v < nv; ++v) max_v2e = std::max(max_v2e, ptr[v + 1] - ptr[v]);
-  // entries of one vertex were pushed in increasing edge order
-  v2e_ptr.upload(ptr);
-  v2e.upload(out);
-
-  // Upload topology.
+  // Derived topology on the device, from the raw arrays only.
   ev0.upload(h_ev0);
   ev1.upload(h_ev1);
   te0.upload(h_te0);
   te1.upload(h_te1);
   te2.upload(h_te2);
-  tv0.upload(h_tv0);
-  tv1.upload(h_tv1);
-  tv2.upload(h_tv2);
-  d1c0.upload(c0);
-  d1c1.upload(c1);
-  d1c2.upload(c2);
-  d1neg.upload(neg);
   std::vector<int8_t> es(ne), ts(nt);
   for (int e = 0; e < ne; ++e) es[e] = h_eo[e] ? 1 : -1;
   for (int t = 0; t < nt; ++t) ts[t] = h_to[t] ? 1 : -1;
   esign.upload(es);
   tsign.upload(ts);
   pts.upload(h_pts);
+  tv0.alloc(nt);
+  tv1.alloc(nt);
+  tv2.alloc(nt);
+  d1c0.alloc(nt);
+  d1c1.alloc(nt);
+  d1c2.alloc(nt);
+  d1neg.alloc(nt);
+  const int T = 256;
+  if (nt)
+    k_tri_topo<<<grid_for(nt, T), T>>>(nt, ev0.p, ev1.p, te0.p, te1.p, te2.p, esign.p, tsign.p, tv0.p, tv1.p, tv2.p,
+                                       d1c0.p, d1c1.p, d1c2.p, d1neg.p);
+  DEC_CHECK_LAUNCH();
+  {
+    DArr<int32_t> keys(std::max<size_t>(1, std::max(3 * (size_t)nt, 2 * (size_t)ne)));
+    DArr<int32_t> vals(keys.n);
+    // v2t: vertex -> 3t+k pushed k-major (k, then t); e2t likewise over the triangles' edges
+    if (nt) k_pairs_tri<<<grid_for(3LL * nt, T), T>>>(nt, tv0.p, tv1.p, tv2.p, keys.p, vals.p);
+    DEC_CHECK_LAUNCH();
+    csr_from_pairs_dev(nv, 3LL * nt, keys.p, vals.p, v2t_ptr, v2t);
+    if (nt) k_pairs_tri<<<grid_for(3LL * nt, T), T>>>(nt, te0.p, te1.p, te2.p, keys.p, vals.p);
+    DEC_CHECK_LAUNCH();
+    csr_from_pairs_dev(ne, 3LL * nt, keys.p, vals.p, e2t_ptr, e2t);
+    // d1ᵀ rows: for edge e, entries ±(t+1) pushed triangle-major
+    if (nt) k_pairs_d1t<<<grid_for(3LL * nt, T), T>>>(nt, d1c0.p, d1c1.p, d1c2.p, d1neg.p, keys.p, vals.p);
+    DEC_CHECK_LAUNCH();
+    csr_from_pairs_dev(ne, 3LL * nt, keys.p, vals.p, e2ts_ptr, e2ts);
+    // d0ᵀ rows: for vertex v, entries ±(e+1) (d0[e,∂v0] = σ, d0[e,∂v1] = -σ) pushed edge-major,
+    // the lower vertex first; loops (∂v0 = ∂v1) are skipped
+    if (ne) k_pairs_d0t<<<grid_for(2LL * ne, T), T>>>(ne, nv, ev0.p, ev1.p, esign.p, keys.p, vals.p);
+    DEC_CHECK_LAUNCH();
+    csr_from_pairs_dev(nv, 2LL * ne, keys.p, vals.p, v2e_ptr, v2e);
+    DArr<int> mx(1);
+    DEC_CUDA(cudaMemset(mx.p, 0, sizeof(int)));
+    k_max_degree<<<grid_for(nv, T), T>>>(nv, v2e_ptr.p, mx.p);
+    DEC_CHECK_LAUNCH();
+    max_v2e = mx.download()[0];
+  }
 
   // Geometry.
   length.alloc(ne);
@@ -353,7 +423,6 @@ void Mesh::build(const dec_mesh_desc& d) {
   star0.alloc(nv);
   star1.alloc(ne);
   star2.alloc(nt);
-  const int T = 256;
   if (ne) k_edge_geom<<<grid_for(ne, T), T>>>(ne, ev0.p, ev1.p, pts.p, length.p);
   if (nt)
     k_tri_geom<<<grid_for(nt, T), T>>>(nt, center, ev0.p, ev1.p, te0.p, te1.p, te2.p, tv0.p, tv1.p,

@@ -28,6 +28,7 @@
 #include <memory>
 #include <numeric>
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cuda_fp16.h>
 
 #include "mg.cuh"
@@ -162,8 +163,8 @@ static std::unique_ptr<dec_mesh> make_mesh(const HostLevel& h, int center) {
 }
 
 // Locality order: vertices sorted by the 3D Morton code of their (bounding-box normalised)
-// position, 21 bits per axis.  Returns perm (new -> old).
-static uint64_t spread21(uint64_t x) {
+// position, 21 bits per axis (a stable sort, ties in vertex order).  Returns perm (new -> old).
+__host__ __device__ inline uint64_t spread21(uint64_t x) {
   x &= 0x1fffff;
   x = (x | x << 32) & 0x1f00000000ffffull;
   x = (x | x << 16) & 0x1f0000ff0000ffull;
@@ -173,28 +174,38 @@ static uint64_t spread21(uint64_t x) {
   return x;
 }
 
-static std::vector<int32_t> morton_order(const std::vector<double>& pts, int n) {
+__global__ void k_morton_keys(int n, const double* __restrict__ pts, double3 lo, double3 span,
+                              uint64_t* __restrict__ key, int32_t* __restrict__ idx) {
+  const double q = (double)((1 << 21) - 1);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double l[3] = {lo.x, lo.y, lo.z}, sp[3] = {span.x, span.y, span.z};
+    uint64_t c[3];
+    for (int k = 0; k < 3; ++k) {
+      const double t = sp[k] > 0 ? (pts[3 * (size_t)i + k] - l[k]) / sp[k] : 0.0;
+      c[k] = (uint64_t)llround(t * q);
+    }
+    key[i] = spread21(c[0]) | (spread21(c[1]) << 1) | (spread21(c[2]) << 2);
+    idx[i] = i;
+  }
+}
+
+static std::vector<int32_t> morton_order(const std::vector<double>& h_pts, const double* d_pts, int n) {
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
   for (int i = 0; i < n; ++i)
     for (int k = 0; k < 3; ++k) {
-      lo[k] = std::min(lo[k], pts[3 * (size_t)i + k]);
-      hi[k] = std::max(hi[k], pts[3 * (size_t)i + k]);
+      lo[k] = std::min(lo[k], h_pts[3 * (size_t)i + k]);
+      hi[k] = std::max(hi[k], h_pts[3 * (size_t)i + k]);
     }
-  std::vector<uint64_t> key(n);
-  const double q = (double)((1 << 21) - 1);
-  for (int i = 0; i < n; ++i) {
-    uint64_t c[3];
-    for (int k = 0; k < 3; ++k) {
-      double span = hi[k] - lo[k];
-      double t = span > 0 ? (pts[3 * (size_t)i + k] - lo[k]) / span : 0.0;
-      c[k] = (uint64_t)std::llround(t * q);
-    }
-    key[i] = spread21(c[0]) | (spread21(c[1]) << 1) | (spread21(c[2]) << 2);
-  }
-  std::vector<int32_t> perm(n);
-  std::iota(perm.begin(), perm.end(), 0);
-  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return key[a] < key[b]; });
-  return perm;
+  DArr<uint64_t> key(n), ks(n);
+  DArr<int32_t> idx(n), is(n);
+  k_morton_keys<<<grid_for(n, 256), 256>>>(n, d_pts, make_double3(lo[0], lo[1], lo[2]),
+                                           make_double3(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]), key.p, idx.p);
+  DEC_CHECK_LAUNCH();
+  size_t tmp_bytes = 0;
+  DEC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, key.p, ks.p, idx.p, is.p, n, 0, 64));
+  DArr<unsigned char> tmp(std::max<size_t>(1, tmp_bytes));
+  DEC_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, key.p, ks.p, idx.p, is.p, n, 0, 64));
+  return is.download();
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -801,10 +812,23 @@ __global__ void k_hash_init(int n, const int32_t* __restrict__ perm, double* x) 
   }
 }
 
-__global__ void k_sumsq(int n, const double* __restrict__ x, double* __restrict__ out) {
+__global__ void k_sumsq_part(int n, const double* __restrict__ x, double* __restrict__ part) {
   __shared__ double sh[256];
   double s = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s += x[i] * x[i];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += x[i] * x[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void k_sum_parts(int nb, const double* __restrict__ part, double* __restrict__ out) {
+  __shared__ double sh[256];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) s += part[i];
   sh[threadIdx.x] = s;
   __syncthreads();
   for (int st = 128; st > 0; st >>= 1) {
@@ -814,7 +838,9 @@ __global__ void k_sumsq(int n, const double* __restrict__ x, double* __restrict_
   if (threadIdx.x == 0) *out = sh[0];
 }
 
-__global__ void k_scale(int n, double a, double* x) {
+// x /= ||x|| with ||x||² read from the device
+__global__ void k_scale_inv_norm(int n, const double* __restrict__ s2, double* x) {
+  const double a = 1.0 / sqrt(*s2);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] *= a;
 }
 
@@ -1168,22 +1194,25 @@ void mg_default_options(dec_mg_options& o) {
   o.fallback_rho = 0.5;
 }
 
+// λmax(D⁻¹A) of a level: 30 power steps from a hashed start vector, all on the device (the norm
+// never leaves it until the end).
 static double power_lmax(const Level& L) {
   if (L.n < 2) return 1.0;
-  DArr<double> x(L.n), y(L.n), s(1);
   const int T = 256;
+  const int nb = (int)std::min<long long>(4LL * num_sms(), ((long long)L.n + T - 1) / T);
+  DArr<double> x(L.n), y(L.n), part(nb), s(1);
   k_hash_init<<<grid_for(L.n, T), T>>>(L.n, L.dperm.p, x.p);
-  double lam = 1.0;
   for (int it = 0; it < 30; ++it) {
-    k_sumsq<<<1, 256>>>(L.n, x.p, s.p);
-    double nx = std::sqrt(s.download()[0]);
-    k_scale<<<grid_for(L.n, T), T>>>(L.n, 1.0 / nx, x.p);
+    k_sumsq_part<<<nb, T>>>(L.n, x.p, part.p);
+    k_sum_parts<<<1, T>>>(nb, part.p, s.p);
+    k_scale_inv_norm<<<grid_for(L.n, T), T>>>(L.n, s.p, x.p);
     k_dinv_a<<<grid_for(L.n, T), T>>>(L.n, L.W, L.col.p, L.off64.p, L.diag64.p, x.p, y.p);
-    k_sumsq<<<1, 256>>>(L.n, y.p, s.p);
-    lam = std::sqrt(s.download()[0]);
     std::swap(x.p, y.p);
   }
+  k_sumsq_part<<<nb, T>>>(L.n, x.p, part.p);
+  k_sum_parts<<<1, T>>>(nb, part.p, s.p);
   DEC_CHECK_LAUNCH();
+  const double lam = std::sqrt(s.download()[0]);
   return lam * 1.05;  // power iteration approaches λmax from below
 }
 
@@ -1433,7 +1462,7 @@ static void build_level_operator(Level& L, double shift, bool reorder, dec_op* g
   else L.op.reset(op_create_impl(L.mesh.get(), DEC_OP_HELMHOLTZ0, shift, DEC_F64));
   L.n = L.mesh->m.nv;
   if (reorder) {
-    L.perm = morton_order(L.mesh->m.h_pts, L.n);
+    L.perm = morton_order(L.mesh->m.h_pts, L.mesh->m.pts.p, L.n);
   } else {
     L.perm.resize(L.n);
     std::iota(L.perm.begin(), L.perm.end(), 0);
@@ -1460,21 +1489,31 @@ static void build_level_operator(Level& L, double shift, bool reorder, dec_op* g
 // in the internal numbering of both.
 static void build_transfers(Level& F, const Level& C, const HostLevel& c) {
   F.nc = c.nv;
-  std::vector<std::vector<int32_t>> inc(c.nv);  // coarse vertex -> fine midpoints (reference)
+  // coarse vertex -> fine midpoints (reference numbering) in increasing edge order, as CSR
+  std::vector<int32_t> iptr(c.nv + 1, 0), inc;
   for (int e = 0; e < c.ne; ++e) {
-    inc[c.ev0[e]].push_back(c.nv + e);
-    if (c.ev1[e] != c.ev0[e]) inc[c.ev1[e]].push_back(c.nv + e);
+    iptr[c.ev0[e] + 1]++;
+    if (c.ev1[e] != c.ev0[e]) iptr[c.ev1[e] + 1]++;
+  }
+  for (int i = 0; i < c.nv; ++i) iptr[i + 1] += iptr[i];
+  inc.resize(iptr[c.nv]);
+  {
+    std::vector<int32_t> pos(iptr.begin(), iptr.end() - 1);
+    for (int e = 0; e < c.ne; ++e) {
+      inc[pos[c.ev0[e]]++] = c.nv + e;
+      if (c.ev1[e] != c.ev0[e]) inc[pos[c.ev1[e]]++] = c.nv + e;
+    }
   }
   int Wq = 1;
-  for (auto& v : inc) Wq = std::max<int>(Wq, (int)v.size());
+  for (int i = 0; i < c.nv; ++i) Wq = std::max<int>(Wq, iptr[i + 1] - iptr[i]);
   std::vector<int32_t> rself(c.nv), ridx((size_t)c.nv * Wq, -1);
   std::vector<double> rs(c.nv);
   for (int ic = 0; ic < c.nv; ++ic) {   // internal coarse row
     int i = C.perm[ic];                 // reference coarse vertex
     rself[ic] = F.iperm[i];             // the vertex's copy on the fine level (reference index i)
     double s = 1.0;                     // row sum of S in column order: 1.0 then 0.5 per edge
-    for (size_t q = 0; q < inc[i].size(); ++q) {
-      ridx[(size_t)ic * Wq + q] = F.iperm[inc[i][q]];
+    for (int q = iptr[i]; q < iptr[i + 1]; ++q) {
+      ridx[(size_t)ic * Wq + (q - iptr[i])] = F.iperm[inc[q]];
       s += 0.5;
     }
     rs[ic] = s;
