@@ -22,6 +22,7 @@ import numpy as np
 
 from . import _capi
 from . import meshes  # noqa: F401
+from . import mesh_io  # noqa: F401
 from ._capi import check, lib, DecError  # noqa: F401
 
 __all__ = ["Mesh", "Operator", "MultigridData", "dec_wedge_product", "dec_wedge_product_pd",
