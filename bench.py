@@ -727,7 +727,7 @@ def run_kernel(args):
     kind = kinds[args.kernel]
     mg = dec.MultigridData(dec.meshes.icosahedron(), args.mesh_level, shift=SHIFT, center="circumcenter",
                            project_radius=1.0, smoother=3 if kind == 4 else 1, pre=args.sweeps, post=args.sweeps,
-                           precision=1, rhs_block=32, coarse_max=args.coarse_max)
+                           precision=args.precision, rhs_block=32, coarse_max=args.coarse_max)
     if kind == 4:
         mlp = dec.SmootherMLP(4)
         mlp.set_engine(args.mlp_engine)
@@ -737,7 +737,8 @@ def run_kernel(args):
     ms, by = mg.time_kernel(kind, 0, NRHS, reps=args.steps)
     torch.cuda.synchronize()
     nv = mg.level_info(0)[0]
-    line = {"kernel": args.kernel, "mesh_level": args.mesh_level, "nrhs": NRHS, "ms_per_launch": ms,
+    line = {"kernel": args.kernel, "mesh_level": args.mesh_level, "precision": args.precision, "nrhs": NRHS,
+            "ms_per_launch": ms,
             "algorithmic_bytes": by, "GB/s": by / (ms * 1e-3) / 1e9}
     if kind == 4:
         line["tensor_TFLOP/s"] = 10240.0 * nv * NRHS / (ms * 1e-3) / 1e12
@@ -762,6 +763,8 @@ def main():
     ap.add_argument("--kernel", choices=["sweep", "residual", "restrict", "prolong", "mlp"],
                     help="time one V-cycle kernel alone (steps launches after warmup) and exit")
     ap.add_argument("--mesh-level", type=int, default=LEVEL, dest="mesh_level")
+    ap.add_argument("--precision", type=int, default=1, choices=[1, 2],
+                    help="V-cycle storage for --kernel: 1 FP32, 2 FP16 (FP32 arithmetic)")
     ap.add_argument("--op", choices=["laplacian", "d0", "d1", "star1_geometric", "wedge01", "wedge11", "wedge02"],
                     help="time one DEC operator kernel alone (steps launches after warmup) and exit")
     ap.add_argument("--dtype", default="float64", choices=["float64", "float32"])
