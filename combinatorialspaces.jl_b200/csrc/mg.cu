@@ -353,18 +353,13 @@ struct Lanes {
 //   S_CHEB0 : d = D⁻¹ r / θ; out = x + d
 //   S_CHEBN : d = c1 d + c2 D⁻¹ r; out = x + d
 // SH: right-hand side j of panel p has its own operator A + cs[p*K + j] I (D likewise).
-// FP16-stored sweeps carry eight values per 16-byte access; unbounded they took 72 registers
-// (3 blocks, 24 warps per SM).  Held to six 256-thread blocks per SM (40 registers, no spills;
-// seven spilled) the L8 sweep went from 4.05 to 4.58 TB/s; the grid is sized to that residency.
-template <class T>
-constexpr int kSweepMinBlocks = std::is_same<T, __half>::value ? 6 : 1;
-
 template <class T, int K, int W, bool SH>
-__global__ void __launch_bounds__(TB, kSweepMinBlocks<T>) k_sweep(int n, int Wr, const int32_t* __restrict__ col,
-                                              const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
-                                              const CT<T>* __restrict__ dinv, const T* __restrict__ b,
-                                              const T* __restrict__ x, T* __restrict__ out, T* __restrict__ d,
-                                              SweepPrm<CT<T>> prm, size_t pstride, const CT<T>* __restrict__ shf) {
+__device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restrict__ col,
+                                           const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
+                                           const CT<T>* __restrict__ dinv, const T* __restrict__ b,
+                                           const T* __restrict__ x, T* __restrict__ out, T* __restrict__ d,
+                                           const SweepPrm<CT<T>>& prm, size_t pstride,
+                                           const CT<T>* __restrict__ shf) {
   using Ln = Lanes<T, K>;
   using C = CT<T>;
   pdl_enter();
@@ -458,6 +453,29 @@ __global__ void __launch_bounds__(TB, kSweepMinBlocks<T>) k_sweep(int n, int Wr,
     }
     stv<T, V>(out + ik, o);
   }
+}
+
+template <class T, int K, int W, bool SH>
+__global__ void __launch_bounds__(TB) k_sweep(int n, int Wr, const int32_t* __restrict__ col,
+                                              const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
+                                              const CT<T>* __restrict__ dinv, const T* __restrict__ b,
+                                              const T* __restrict__ x, T* __restrict__ out, T* __restrict__ d,
+                                              SweepPrm<CT<T>> prm, size_t pstride, const CT<T>* __restrict__ shf) {
+  sweep_rows<T, K, W, SH>(n, Wr, col, off, diag, dinv, b, x, out, d, prm, pstride, shf);
+}
+
+// FP16-stored sweeps carry eight values per 16-byte access; unbounded they took 72 registers
+// (3 blocks, 24 warps per SM).  Held to six 256-thread blocks per SM (40 registers, no spills;
+// seven spilled) the L8 sweep went from 4.05 to 4.58 TB/s; the grid is sized to that residency.
+constexpr int kSweepHalfBlocks = 6;
+
+template <int K, int W, bool SH>
+__global__ void __launch_bounds__(TB, kSweepHalfBlocks) k_sweep_h(
+    int n, int Wr, const int32_t* __restrict__ col, const float* __restrict__ off, const float* __restrict__ diag,
+    const float* __restrict__ dinv, const __half* __restrict__ b, const __half* __restrict__ x,
+    __half* __restrict__ out, __half* __restrict__ d, SweepPrm<float> prm, size_t pstride,
+    const float* __restrict__ shf) {
+  sweep_rows<__half, K, W, SH>(n, Wr, col, off, diag, dinv, b, x, out, d, prm, pstride, shf);
 }
 
 // Restriction R = row-normalised S (make_restriction, Multigrid.jl:595-612):
@@ -1674,20 +1692,33 @@ static void launch_sweep(const Level& L, const T* b, const T* x, T* out, T* d, S
                          cudaStream_t s, const CT<T>* cs) {
   size_t ps = (size_t)L.n * K;
   dim3 grid = row_grid<T, K>(L.n, np);
-  if (kSweepMinBlocks<T> > 1)
-    grid.x = std::min<unsigned>(grid.x, (unsigned)(kSweepMinBlocks<T> * num_sms()));
-  const CT<T>* off = pick<T>(L.off64, L.off32);
-  const CT<T>* dg = pick<T>(L.diag64, L.diag32);
-  const CT<T>* di = pick<T>(L.dinv64, L.dinv32);
-  if (cs) {
-    if (L.W == 6)
-      launch_pdl(k_sweep<T, K, 6, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
-    else
-      launch_pdl(k_sweep<T, K, 0, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
-  } else if (L.W == 6) {
-    launch_pdl(k_sweep<T, K, 6, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+  if constexpr (std::is_same<T, __half>::value) {
+    grid.x = std::min<unsigned>(grid.x, (unsigned)(kSweepHalfBlocks * num_sms()));
+    const float* off = L.off32.p;
+    const float* dg = L.diag32.p;
+    const float* di = L.dinv32.p;
+    if (cs) {
+      if (L.W == 6) launch_pdl(k_sweep_h<K, 6, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+      else launch_pdl(k_sweep_h<K, 0, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+    } else if (L.W == 6) {
+      launch_pdl(k_sweep_h<K, 6, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+    } else {
+      launch_pdl(k_sweep_h<K, 0, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+    }
   } else {
-    launch_pdl(k_sweep<T, K, 0, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+    const CT<T>* off = pick<T>(L.off64, L.off32);
+    const CT<T>* dg = pick<T>(L.diag64, L.diag32);
+    const CT<T>* di = pick<T>(L.dinv64, L.dinv32);
+    if (cs) {
+      if (L.W == 6)
+        launch_pdl(k_sweep<T, K, 6, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+      else
+        launch_pdl(k_sweep<T, K, 0, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+    } else if (L.W == 6) {
+      launch_pdl(k_sweep<T, K, 6, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+    } else {
+      launch_pdl(k_sweep<T, K, 0, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+    }
   }
 }
 
