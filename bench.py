@@ -286,7 +286,8 @@ def measure_learned(dec, args, B, U64, common, timed):
 def measure_batched(dec, args):
     """The batched uneven workload: 512 Helmholtz solves (L + c I) u = b, c log-uniform in [0.1, 10]
     and the mesh drawn uniformly from 8 types (icospheres L4-L7; planar grids 65^2, 129^2, 257^2,
-    513^2 = a 9x9 triangulated grid refined 3-6 times), seed 3; FP32 Chebyshev V(3,3) cycles in
+    513^2 = a 9x9 triangulated grid refined 3-6 times), seed 3; FP32 Chebyshev cycles (the headline's
+    --pre / --post / --cheb-ratio / --inner-cycles) in
     FP64 refinement to 1e-8, every refinement step of all 8 groups one CUDA graph, panel widths
     per group from the autotuner.  Then 1,024 wedge products ∧(1,1) of FP32 uniform[-1,1] 1-form
     pairs on icosphere L7 in one batched launch."""
@@ -303,8 +304,8 @@ def measure_batched(dec, args):
     mgs, nrhs, shifts, Bs = [], [], [], []
     for t, (name, coarse, levels, radius) in enumerate(types):
         mg = dec.MultigridData(coarse, levels, shift=0.0, center="circumcenter", project_radius=radius,
-                               smoother=1, pre=3, post=3, precision=1, coarse_solver=2, coarse_max=170,
-                               inner_cycles=2)
+                               smoother=1, pre=args.pre, post=args.post, cheb_ratio=args.cheb_ratio, precision=1,
+                               coarse_solver=2, coarse_max=170, inner_cycles=args.inner_cycles)
         idx = np.nonzero(draw == t)[0]
         mgs.append(mg)
         nrhs.append(len(idx))
