@@ -467,7 +467,9 @@ def run_ours(args):
     common = dict(shift=SHIFT, center="circumcenter", project_radius=1.0, smoother=1, pre=args.pre,
                   post=args.post, cheb_ratio=args.cheb_ratio, rhs_block=args.rhs_block,
                   inner_cycles=args.inner_cycles, coarse_max=args.coarse_max)
-    mg = dec.MultigridData(ico, LEVEL, precision=1, **common)
+    # a profiling run drives the refinement loop from the host, so that every kernel is a graph
+    # node the profiler follows (kernels inside the device loop's conditional node are not)
+    mg = dec.MultigridData(ico, LEVEL, precision=1, **dict(common, device_loop=0 if args.profile else 1))
     mg64 = dec.MultigridData(ico, LEVEL, precision=0, **common)
     setup_s = time.perf_counter() - t_setup
     n = mg.level_info(0)[0]

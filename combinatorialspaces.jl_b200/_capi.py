@@ -35,7 +35,7 @@ class MGOptions(C.Structure):
                 ("omega", C.c_double), ("cheb_ratio", C.c_double), ("coarse_solver", C.c_int32),
                 ("precision", C.c_int32), ("rhs_block", C.c_int32), ("mu", C.c_int32),
                 ("inner_cycles", C.c_int32), ("reorder", C.c_int32), ("coarse_max", C.c_int32),
-                ("fallback_rho", C.c_double), ("galerkin", C.c_int32)]
+                ("fallback_rho", C.c_double), ("galerkin", C.c_int32), ("device_loop", C.c_int32)]
 
 
 class SolveReport(C.Structure):

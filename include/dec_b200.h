@@ -213,6 +213,10 @@ typedef struct dec_mg_options {
                               (Multigrid.jl:740-748): only the finest level's, the coarser ones
                               A_{k+1} = R_k A_k P_k (host sparse products in SparseArrays' order);
                               not with coarse_solver 2 */
+  int32_t device_loop;     /* 1 (default): dec_mg_solve runs its refinement loop on the device (one graph
+                              with a conditional WHILE node); 0: the host drives it, one graph launch
+                              per step (profilers that do not follow kernels inside conditional graph
+                              nodes see every kernel) */
 } dec_mg_options;
 
 typedef struct dec_solve_report {

@@ -184,6 +184,21 @@ def test_device_refinement_loop_steps(O, dec, built):
     assert float(Z.abs().max()) == 0.0
 
 
+def test_host_driven_loop_matches_device_loop(dec, built):
+    """device_loop = 0 (one graph launch per refinement step, the test on the host) takes the same
+    steps and gives the same bits as the loop on the device."""
+    coarse, md, _ = built["ico4_circum"]
+    out = []
+    for dl in (1, 0):
+        mg = dec.MultigridData(coarse, 4, shift=1.0, center="circumcenter", project_radius=1.0, precision=1,
+                               pre=0, post=2, cheb_ratio=3.0, inner_cycles=2, device_loop=dl)
+        B = torch.tensor(np.stack([uniform(160 + j, mg.n) for j in range(3)]), device="cuda")
+        U, rep = mg.solve(torch.zeros_like(B), B, rtol=1e-10, max_iters=60)
+        out.append((U.cpu().numpy(), rep.iterations, rep.max_rel_residual, rep.converged))
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    assert out[0][1:] == out[1][1:] and out[0][3] == 1
+
+
 def test_pipelined_host_solves_match_synchronous(dec, built):
     """solve_host_submit / wait: three solves in flight on the hierarchy's own streams give the
     same bits as the synchronous host-buffer solve; a fourth submit before a wait, a second wait on
