@@ -480,8 +480,11 @@ __global__ void __launch_bounds__(TB, kSweepHalfBlocks) k_sweep_h(
 
 // Restriction R = row-normalised S (make_restriction, Multigrid.jl:595-612):
 // rc[i] = (1/rs_i) rf[self_i] + Σ_e (0.5/rs_i) rf[mid_e], rs_i = 1 + deg_i / 2, terms in the
-// reference's column order.
-template <class T, int K>
+// reference's column order.  A row's midpoints fill the front of its ridx slots (-1 after them).
+// WQ > 0 (the slot count, known at compile time) loads every midpoint index first and issues all
+// the row's gathers before the first sum, instead of one index -> gather -> sum chain per slot;
+// the sums keep the same order, so the result is the same bit for bit.
+template <class T, int K, int WQ = 0>
 __global__ void __launch_bounds__(TB) k_restrict(int nc, int Wq, const int32_t* __restrict__ rself,
                                                  const int32_t* __restrict__ ridx, const double* __restrict__ rs,
                                                  const T* __restrict__ rf, T* __restrict__ rc, size_t fstride,
@@ -497,15 +500,36 @@ __global__ void __launch_bounds__(TB) k_restrict(int nc, int Wq, const int32_t* 
     const double s = rs[i];
     const C w1 = (C)(1.0 / s), wh = (C)(0.5 / s);
     C acc[V], v[V];
-    ldv<T, V>(f + (size_t)rself[i] * K, v);
+    if constexpr (WQ > 0) {
+      int m[WQ];
 #pragma unroll
-    for (int q = 0; q < V; ++q) acc[q] = w1 * v[q];
-    for (int e = 0; e < Wq; ++e) {
-      int m = ridx[(size_t)i * Wq + e];
-      if (m < 0) break;
-      ldv<T, V>(f + (size_t)m * K, v);
+      for (int e = 0; e < WQ; ++e) m[e] = ridx[(size_t)i * WQ + e];
+      C g[WQ][V];
+      ldv<T, V>(f + (size_t)rself[i] * K, v);
 #pragma unroll
-      for (int q = 0; q < V; ++q) acc[q] += wh * v[q];
+      for (int e = 0; e < WQ; ++e) {
+        if (m[e] >= 0) ldv<T, V>(f + (size_t)m[e] * K, g[e]);
+      }
+#pragma unroll
+      for (int q = 0; q < V; ++q) acc[q] = w1 * v[q];
+#pragma unroll
+      for (int e = 0; e < WQ; ++e) {
+        if (m[e] >= 0) {
+#pragma unroll
+          for (int q = 0; q < V; ++q) acc[q] += wh * g[e][q];
+        }
+      }
+    } else {
+      ldv<T, V>(f + (size_t)rself[i] * K, v);
+#pragma unroll
+      for (int q = 0; q < V; ++q) acc[q] = w1 * v[q];
+      for (int e = 0; e < Wq; ++e) {
+        int m = ridx[(size_t)i * Wq + e];
+        if (m < 0) break;
+        ldv<T, V>(f + (size_t)m * K, v);
+#pragma unroll
+        for (int q = 0; q < V; ++q) acc[q] += wh * v[q];
+      }
     }
     stv<T, V>(c + (size_t)i * K, acc);
   }
@@ -1216,6 +1240,7 @@ void mg_default_options(dec_mg_options& o) {
   o.reorder = 1;
   o.coarse_max = 0;
   o.fallback_rho = 0.5;
+  o.device_loop = 1;
 }
 
 // λmax(D⁻¹A) of a level: 30 power steps from a hashed start vector, all on the device (the norm
@@ -1579,6 +1604,7 @@ dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
   require(o.coarse_solver != 2 || (o.smoother == DEC_SMOOTH_JACOBI || o.smoother == DEC_SMOOTH_CHEBYSHEV),
           "multigrid: per-RHS shifts (coarse_solver 2) need the Jacobi or Chebyshev smoother");
   require(o.galerkin == 0 || o.galerkin == 1, "multigrid: galerkin must be 0 or 1");
+  require(o.device_loop == 0 || o.device_loop == 1, "multigrid: device_loop must be 0 or 1");
   require(!(o.galerkin && o.coarse_solver == 2),
           "multigrid: per-RHS shifts (coarse_solver 2) need every level's own Laplacian (not GalerkinMode)");
   auto mg = std::make_unique<dec_mg>();
@@ -1685,6 +1711,21 @@ static const CT<T>* pick(const DArr<double>& a64, const DArr<float>& a32) {
 template <class T, int K>
 static dim3 row_grid(int n, int np) {
   return dim3(grid_for((long long)n, Lanes<T, K>::RPB, 8), np);
+}
+
+// R r_f into the coarse level's panels; the unrolled kernel where a coarse vertex has at most six
+// midpoints (every level of the refined icosphere and of the triangulated grids).
+template <class T, int K>
+static void launch_restrict(const Level& L, const Level& Cl, const T* r, T* bc, int np, cudaStream_t s,
+                            bool pdl = true) {
+  auto kern = L.Wq == 6 ? k_restrict<T, K, 6> : k_restrict<T, K>;
+  const dim3 g = row_grid<T, K>(Cl.n, np);
+  const size_t fs = (size_t)L.n * K, cs = (size_t)Cl.n * K;
+  if (pdl)
+    launch_pdl(kern, g, dim3(TB), s, L.nc, L.Wq, (const int32_t*)L.rself.p, (const int32_t*)L.ridx.p,
+               (const double*)L.rs.p, r, bc, fs, cs);
+  else
+    kern<<<g, TB, 0, s>>>(L.nc, L.Wq, L.rself.p, L.ridx.p, L.rs.p, r, bc, fs, cs);
 }
 
 template <class T, int K>
@@ -1844,9 +1885,7 @@ static double* cg_mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs
   launch_sweep<double, K>(L, B.b.p, x, r, nullptr, prm, np, s, B.cs);
   const Level& Cl = mg.lv[l + 1];
   LevelBufs<double>& Cb = bufs[l + 1];
-  launch_pdl(k_restrict<double, K>, row_grid<double, K>(Cl.n, np), dim3(TB), s, L.nc, L.Wq,
-             (const int32_t*)L.rself.p, (const int32_t*)L.ridx.p, (const double*)L.rs.p, (const double*)r, Cb.b.p,
-             (size_t)L.n * K, (size_t)Cl.n * K);
+  launch_restrict<double, K>(L, Cl, (const double*)r, Cb.b.p, np, s);
   double* z = cg_mu_cycle<K>(mg, w, bufs, l + 1, Cb.x.p, true, mu, np, s);
   if (mu > 1) z = cg_mu_cycle<K>(mg, w, bufs, l + 1, z, false, mu - 1, np, s);
   if (zero_x) DEC_CUDA(cudaMemsetAsync(x, 0, (size_t)L.n * K * np * sizeof(double), s));
@@ -1889,9 +1928,7 @@ static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bu
   launch_sweep<T, K>(L, B.b.p, x, r, nullptr, prm, np, s, B.cs);
   const Level& Cl = mg.lv[l + 1];
   LevelBufs<T>& Cb = bufs[l + 1];
-  launch_pdl(k_restrict<T, K>, row_grid<T, K>(Cl.n, np), dim3(TB), s, L.nc, L.Wq, (const int32_t*)L.rself.p,
-             (const int32_t*)L.ridx.p, (const double*)L.rs.p, (const T*)r, Cb.b.p, (size_t)L.n * K,
-             (size_t)Cl.n * K);
+  launch_restrict<T, K>(L, Cl, (const T*)r, Cb.b.p, np, s);
   T* z = mu_cycle<T, K>(mg, w, bufs, l + 1, Cb.x.p, true, mu, np, s);
   if (mu > 1) z = mu_cycle<T, K>(mg, w, bufs, l + 1, z, false, mu - 1, np, s);
   if (zero_x) {  // x is all zero: start it from the prolonged correction
@@ -2306,9 +2343,7 @@ static T* fmg_T(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bufs,
   if (l < last) {
     const Level& Cl = mg.lv[l + 1];
     LevelBufs<T>& Cb = bufs[l + 1];
-    launch_pdl(k_restrict<T, K>, row_grid<T, K>(Cl.n, np), dim3(TB), s, L.nc, L.Wq, (const int32_t*)L.rself.p,
-               (const int32_t*)L.ridx.p, (const double*)L.rs.p, (const T*)B.b.p, Cb.b.p, (size_t)L.n * K,
-               (size_t)Cl.n * K);
+    launch_restrict<T, K>(L, Cl, (const T*)B.b.p, Cb.b.p, np, s);
     T* zc = fmg_T<T, K>(mg, w, bufs, l + 1, cycles, np, s);
     DEC_CUDA(cudaMemsetAsync(z, 0, (size_t)L.n * K * np * sizeof(T), s));
     launch_pdl(k_prolong<T, K>, row_grid<T, K>(L.n, np), dim3(TB), s, L.n, (const int32_t*)L.pa.p,
@@ -2387,7 +2422,7 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
     bd = w.bcm.p;
     ud = w.ucm.p;
   }
-  if (mg->opt.smoother != DEC_SMOOTH_LEARNED) {  // the refinement loop runs on the device
+  if (mg->opt.smoother != DEC_SMOOTH_LEARNED && mg->opt.device_loop) {  // the refinement loop runs on the device
     enqueue_solve(*mg, w, bd, ud, nrhs, rtol, max_iters, use_initial_guess, s);
     if (host_buffers) DEC_CUDA(cudaMemcpyAsync(u, ud, (size_t)n * nrhs * 8, cudaMemcpyDeviceToHost, s));
     DEC_CUDA(cudaEventRecord(e1, s));
@@ -2615,9 +2650,7 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
                                                       rout, w.partial.p, (size_t)F.n * K, nullptr);
     } else if (kernel == DEC_KERNEL_RESTRICT) {
       const Level& Cl = mg.lv[level + 1];
-      k_restrict<T, K><<<row_grid<T, K>(Cl.n, np), TB, 0, s>>>(L.nc, L.Wq, L.rself.p, L.ridx.p, L.rs.p, B.x.p,
-                                                                bufs[level + 1].b.p, (size_t)L.n * K,
-                                                                (size_t)Cl.n * K);
+      launch_restrict<T, K>(L, Cl, (const T*)B.x.p, bufs[level + 1].b.p, np, s, false);
     } else {
       const Level& Cl = mg.lv[level + 1];
       k_prolong<T, K><<<row_grid<T, K>(L.n, np), TB, 0, s>>>(L.n, L.pa.p, L.pb.p, bufs[level + 1].x.p, B.x.p,
