@@ -536,8 +536,10 @@ __global__ void __launch_bounds__(TB) k_restrict(int nc, int Wq, const int32_t* 
 }
 
 // Prolongation and correction x_f += P z (P = Sᵀ, Multigrid.jl:774): every fine row takes
-// ½ z[pa] + ½ z[pb] (pa = pb for a coarse vertex, which gives z exactly).
-template <class T, int K>
+// ½ z[pa] + ½ z[pb] (pa = pb for a coarse vertex, which gives z exactly).  ASSIGN: x_f is known
+// to be zero (a cycle started from x = 0 with no pre-smoothing), so it is neither read nor
+// cleared first; the sum starts from +0 as the cleared buffer's did, which keeps every bit.
+template <class T, int K, bool ASSIGN = false>
 __global__ void __launch_bounds__(TB) k_prolong(int nf, const int32_t* __restrict__ pa, const int32_t* __restrict__ pb,
                                                 const T* __restrict__ z, T* __restrict__ x, size_t fstride,
                                                 size_t cstride) {
@@ -552,7 +554,12 @@ __global__ void __launch_bounds__(TB) k_prolong(int nf, const int32_t* __restric
     C za[V], zb[V], xv[V];
     ldv<T, V>(zc + (size_t)pa[j] * K, za);
     ldv<T, V>(zc + (size_t)pb[j] * K, zb);
-    ldv<T, V>(xf + (size_t)j * K, xv);
+    if constexpr (ASSIGN) {
+#pragma unroll
+      for (int q = 0; q < V; ++q) xv[q] = C(0);
+    } else {
+      ldv<T, V>(xf + (size_t)j * K, xv);
+    }
 #pragma unroll
     for (int q = 0; q < V; ++q) xv[q] += C(0.5) * za[q] + C(0.5) * zb[q];
     stv<T, V>(xf + (size_t)j * K, xv);
@@ -1728,6 +1735,19 @@ static void launch_restrict(const Level& L, const Level& Cl, const T* r, T* bc, 
     kern<<<g, TB, 0, s>>>(L.nc, L.Wq, L.rself.p, L.ridx.p, L.rs.p, r, bc, fs, cs);
 }
 
+// x_f (+)= P z on all panels; assign when x_f is known to be zero (no clear, no read of x_f).
+template <class T, int K>
+static void launch_prolong(const Level& L, const Level& Cl, const T* z, T* x, bool assign, int np, cudaStream_t s,
+                           bool pdl = true) {
+  auto kern = assign ? k_prolong<T, K, true> : k_prolong<T, K, false>;
+  const dim3 g = row_grid<T, K>(L.n, np);
+  const size_t fs = (size_t)L.n * K, cs = (size_t)Cl.n * K;
+  if (pdl)
+    launch_pdl(kern, g, dim3(TB), s, L.n, (const int32_t*)L.pa.p, (const int32_t*)L.pb.p, z, x, fs, cs);
+  else
+    kern<<<g, TB, 0, s>>>(L.n, L.pa.p, L.pb.p, z, x, fs, cs);
+}
+
 template <class T, int K>
 static void launch_sweep(const Level& L, const T* b, const T* x, T* out, T* d, SweepPrm<CT<T>> prm, int np,
                          cudaStream_t s, const CT<T>* cs) {
@@ -1878,19 +1898,21 @@ static double* cg_mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs
     if (zero_x) DEC_CUDA(cudaMemsetAsync(x, 0, (size_t)L.n * K * np * sizeof(double), s));
     return x;
   }
-  double* r = (x == B.x.p) ? B.y.p : B.x.p;
-  SweepPrm<double> prm{};
-  prm.mode = S_RESID;
-  prm.zero_x = zero_x ? 1 : 0;
-  launch_sweep<double, K>(L, B.b.p, x, r, nullptr, prm, np, s, B.cs);
+  // with x = 0 the residual is b itself (the residual sweep would copy it bit for bit)
+  const double* r = B.b.p;
+  if (!zero_x) {
+    double* rr = (x == B.x.p) ? B.y.p : B.x.p;
+    SweepPrm<double> prm{};
+    prm.mode = S_RESID;
+    launch_sweep<double, K>(L, B.b.p, x, rr, nullptr, prm, np, s, B.cs);
+    r = rr;
+  }
   const Level& Cl = mg.lv[l + 1];
   LevelBufs<double>& Cb = bufs[l + 1];
-  launch_restrict<double, K>(L, Cl, (const double*)r, Cb.b.p, np, s);
+  launch_restrict<double, K>(L, Cl, r, Cb.b.p, np, s);
   double* z = cg_mu_cycle<K>(mg, w, bufs, l + 1, Cb.x.p, true, mu, np, s);
   if (mu > 1) z = cg_mu_cycle<K>(mg, w, bufs, l + 1, z, false, mu - 1, np, s);
-  if (zero_x) DEC_CUDA(cudaMemsetAsync(x, 0, (size_t)L.n * K * np * sizeof(double), s));
-  launch_pdl(k_prolong<double, K>, row_grid<double, K>(L.n, np), dim3(TB), s, L.n, (const int32_t*)L.pa.p,
-             (const int32_t*)L.pb.p, (const double*)z, x, (size_t)L.n * K, (size_t)Cl.n * K);
+  launch_prolong<double, K>(L, Cl, (const double*)z, x, zero_x, np, s);
   return cg_smooth<K>(mg, w, L, B, x, false, steps_post, np, s);
 }
 
@@ -1920,22 +1942,24 @@ static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bu
   }
   x = smooth<T, K>(mg, L, B, x, zero_x, mg.opt.pre, np, s);
   zero_x = zero_x && mg.opt.pre == 0;
-  // residual into the free buffer, then restrict into the coarse right-hand side
-  T* r = (x == B.x.p) ? B.y.p : B.x.p;
-  SweepPrm<CT<T>> prm{};
-  prm.mode = S_RESID;
-  prm.zero_x = zero_x ? 1 : 0;
-  launch_sweep<T, K>(L, B.b.p, x, r, nullptr, prm, np, s, B.cs);
+  // residual into the free buffer, then restrict into the coarse right-hand side; with x = 0
+  // (every coarse level, and the finest one on a refinement step's first cycle) the residual is
+  // b itself, which the residual sweep would only copy (bit for bit)
+  const T* r = B.b.p;
+  if (!zero_x) {
+    T* rr = (x == B.x.p) ? B.y.p : B.x.p;
+    SweepPrm<CT<T>> prm{};
+    prm.mode = S_RESID;
+    launch_sweep<T, K>(L, B.b.p, x, rr, nullptr, prm, np, s, B.cs);
+    r = rr;
+  }
   const Level& Cl = mg.lv[l + 1];
   LevelBufs<T>& Cb = bufs[l + 1];
-  launch_restrict<T, K>(L, Cl, (const T*)r, Cb.b.p, np, s);
+  launch_restrict<T, K>(L, Cl, r, Cb.b.p, np, s);
   T* z = mu_cycle<T, K>(mg, w, bufs, l + 1, Cb.x.p, true, mu, np, s);
   if (mu > 1) z = mu_cycle<T, K>(mg, w, bufs, l + 1, z, false, mu - 1, np, s);
-  if (zero_x) {  // x is all zero: start it from the prolonged correction
-    DEC_CUDA(cudaMemsetAsync(x, 0, (size_t)L.n * K * np * sizeof(T), s));
-  }
-  launch_pdl(k_prolong<T, K>, row_grid<T, K>(L.n, np), dim3(TB), s, L.n, (const int32_t*)L.pa.p,
-             (const int32_t*)L.pb.p, (const T*)z, x, (size_t)L.n * K, (size_t)Cl.n * K);
+  // x = 0: the prolonged correction is x (written, not added)
+  launch_prolong<T, K>(L, Cl, (const T*)z, x, zero_x, np, s);
   return smooth<T, K>(mg, L, B, x, false, mg.opt.post, np, s);
 }
 
@@ -2345,9 +2369,7 @@ static T* fmg_T(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bufs,
     LevelBufs<T>& Cb = bufs[l + 1];
     launch_restrict<T, K>(L, Cl, (const T*)B.b.p, Cb.b.p, np, s);
     T* zc = fmg_T<T, K>(mg, w, bufs, l + 1, cycles, np, s);
-    DEC_CUDA(cudaMemsetAsync(z, 0, (size_t)L.n * K * np * sizeof(T), s));
-    launch_pdl(k_prolong<T, K>, row_grid<T, K>(L.n, np), dim3(TB), s, L.n, (const int32_t*)L.pa.p,
-               (const int32_t*)L.pb.p, (const T*)zc, z, (size_t)L.n * K, (size_t)Cl.n * K);
+    launch_prolong<T, K>(L, Cl, (const T*)zc, z, true, np, s);
     zero = false;
   }
   for (int c = 0; c < cycles; ++c) {
@@ -2653,8 +2675,7 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
       launch_restrict<T, K>(L, Cl, (const T*)B.x.p, bufs[level + 1].b.p, np, s, false);
     } else {
       const Level& Cl = mg.lv[level + 1];
-      k_prolong<T, K><<<row_grid<T, K>(L.n, np), TB, 0, s>>>(L.n, L.pa.p, L.pb.p, bufs[level + 1].x.p, B.x.p,
-                                                              (size_t)L.n * K, (size_t)Cl.n * K);
+      launch_prolong<T, K>(L, Cl, (const T*)bufs[level + 1].x.p, B.x.p, false, np, s, false);
     }
   };
   launch();  // warm-up
