@@ -526,21 +526,25 @@ class MultigridData:
         check(lib().dec_mg_time_kernel(self._h, kernel, level, nrhs, reps, _stream(), C.byref(ms), C.byref(by)))
         return ms.value, by.value
 
-    def solve(self, u, b, rtol=1e-8, max_iters=100, shifts=None):
+    def solve(self, u, b, rtol=1e-8, max_iters=100, shifts=None, use_initial_guess=True):
         """FP64-refined solve of A u = b (u in/out); with `shifts` (coarse_solver=2 hierarchies)
-        right-hand side j solves (L + (shift + shifts[j]) I) u_j = b_j."""
+        right-hand side j solves (L + (shift + shifts[j]) I) u_j = b_j.  use_initial_guess=False
+        starts from u = 0 (u is output only; dec_mg_solve_from_zero)."""
         nrhs = 1 if b.dim() == 1 else b.shape[0]
         rep = _capi.SolveReport()
         if shifts is not None:
             sh = np.ascontiguousarray(shifts, np.float64)
             if sh.size != nrhs:
                 raise ValueError("one shift per right-hand side")
+            if not use_initial_guess:
+                u.zero_()
             st = lib().dec_mg_solve_shifted(self._h, _ptr(u), _ptr(b), nrhs, sh.ctypes.data_as(C.c_void_p), rtol,
                                             max_iters, C.byref(rep), _stream())
             if st not in (_capi.DEC_OK, 4):
                 check(st)
             return u, rep
-        st = lib().dec_mg_solve(self._h, _ptr(u), _ptr(b), nrhs, rtol, max_iters, C.byref(rep), _stream())
+        fn = lib().dec_mg_solve if use_initial_guess else lib().dec_mg_solve_from_zero
+        st = fn(self._h, _ptr(u), _ptr(b), nrhs, rtol, max_iters, C.byref(rep), _stream())
         if st not in (_capi.DEC_OK, 4):
             check(st)
         return u, rep

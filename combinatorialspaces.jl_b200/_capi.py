@@ -81,6 +81,7 @@ SIGNATURES = {
     "dec_mg_cycles": (I32, [P, P, P, I32, I32, P]),
     "dec_mg_full_multigrid": (I32, [P, P, P, I32, I32, P]),
     "dec_mg_solve": (I32, [P, P, P, I32, F64, I32, C.POINTER(SolveReport), P]),
+    "dec_mg_solve_from_zero": (I32, [P, P, P, I32, F64, I32, C.POINTER(SolveReport), P]),
     "dec_mg_solve_host": (I32, [P, P, P, I32, F64, I32, I32, C.POINTER(SolveReport), P]),
     "dec_c_wedge_apply": (I32, [I32, I32, I64, P, P, I32, P, P, P, I32, P]),
     "dec_mg_solve_host_submit": (I32, [P, P, P, I32, F64, I32, I32, C.POINTER(C.c_uint64)]),

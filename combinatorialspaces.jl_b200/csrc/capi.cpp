@@ -245,6 +245,13 @@ dec_status dec_mg_solve(dec_mg* mg, double* u, const double* b, int32_t nrhs, do
   return g != DEC_OK ? g : st;
 }
 
+dec_status dec_mg_solve_from_zero(dec_mg* mg, double* u, const double* b, int32_t nrhs, double rtol,
+                                  int32_t max_iters, dec_solve_report* rep, void* stream) {
+  dec_status st = DEC_OK;
+  dec_status g = guard([&] { st = decb::mg_solve(mg, u, b, nrhs, rtol, max_iters, rep, stream, false, false); });
+  return g != DEC_OK ? g : st;
+}
+
 dec_status dec_mg_solve_host(dec_mg* mg, double* u, const double* b, int32_t nrhs, double rtol, int32_t max_iters,
                              int32_t use_initial_guess, dec_solve_report* rep, void* stream) {
   dec_status st = DEC_OK;

@@ -846,6 +846,31 @@ __global__ void __launch_bounds__(TB) k_panel_sumsq(int n, const double* __restr
   if (threadIdx.x < K) partial[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * K + threadIdx.x] = sh[threadIdx.x];
 }
 
+// k_panel_sumsq's partial sums of b², and the first refinement step's right-hand side from a zero
+// initial guess: r = b - A·0 = b, rounded to the V-cycle's storage type as the residual kernel
+// rounds it (so the step is the same bit for bit without the FP64 update and residual passes).
+template <int K, class T>
+__global__ void __launch_bounds__(TB) k_first_rhs(int n, const double* __restrict__ x, double* __restrict__ partial,
+                                                  size_t pstride, T* __restrict__ r) {
+  const int k = threadIdx.x % K;
+  const size_t po = (size_t)blockIdx.y * pstride;
+  double ss = 0.0;
+  for (int i = blockIdx.x * (TB / K) + threadIdx.x / K; i < n; i += gridDim.x * (TB / K)) {
+    const size_t ik = po + (size_t)i * K + k;
+    const double v = x[ik];
+    r[ik] = (T)v;
+    ss += v * v;
+  }
+  __shared__ double sh[TB];
+  sh[threadIdx.x] = ss;
+  __syncthreads();
+  for (int stride = TB / 2; stride >= K; stride >>= 1) {
+    if (threadIdx.x < stride) sh[threadIdx.x] += sh[threadIdx.x + stride];
+    __syncthreads();
+  }
+  if (threadIdx.x < K) partial[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * K + threadIdx.x] = sh[threadIdx.x];
+}
+
 // Power iteration for λmax(D⁻¹A): y = D⁻¹ A x (single vector, FP64).
 __global__ void k_dinv_a(int n, int W, const int32_t* __restrict__ col, const double* __restrict__ off,
                          const double* __restrict__ diag, const double* __restrict__ x, double* __restrict__ y) {
@@ -1160,8 +1185,9 @@ struct Workspace {
   DArr<double> pu[3], pb[3];  // staging slots of pipelined host-buffer solves
   DArr<double> bn2;           // ||b_j||² (device refinement loop)
   DArr<LoopState> loop;       // device refinement loop state
-  cudaGraphExec_t solve_graph = nullptr;  // the whole refinement loop (Jacobi / Chebyshev)
-  int64_t solve_pre = 0, solve_body = 0;  // kernel nodes before / inside its loop
+  // the whole refinement loop (Jacobi / Chebyshev): [0] from a given initial guess, [1] from zero
+  cudaGraphExec_t solve_graph[2] = {nullptr, nullptr};
+  int64_t solve_pre[2] = {0, 0}, solve_body = 0;  // kernel nodes before / inside its loop
   int nblocks = 0;
   DArr<double> Ubak;          // learned smoother: the iterate before a refinement step
   DArr<double> cs64;          // coarse_solver 2: per-RHS total shifts (K * npanels)
@@ -1176,8 +1202,10 @@ struct Workspace {
       if (g) cudaGraphExecDestroy(g);
       g = nullptr;
     }
-    if (solve_graph) cudaGraphExecDestroy(solve_graph);
-    solve_graph = nullptr;
+    for (auto& g : solve_graph) {
+      if (g) cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
   }
   ~Workspace() { drop_graphs(); }
 };
@@ -2224,11 +2252,32 @@ static void zero_correction(const dec_mg& mg, Workspace& w, cudaStream_t s) {
   else DEC_CUDA(cudaMemsetAsync(w.f64[0].x.p, 0, total * sizeof(double), s));
 }
 
+// From a zero initial guess (FP32 / FP64 V-cycles): ||b||² and the first right-hand side r = b in
+// one pass over b, and ||r||² = ||b||² for the first test.
+static void enqueue_first_rhs(const dec_mg& mg, Workspace& w, cudaStream_t s) {
+  const int n = mg.lv[0].n, K = w.K, np = w.npanels;
+  dim3 g(w.nblocks, np);
+  const size_t ps = (size_t)n * K;
+  switch (K) {
+#define DEC_K(KK)                                                                                    \
+  case KK:                                                                                           \
+    if (w.prec == 1) k_first_rhs<KK, float><<<g, TB, 0, s>>>(n, w.B64.p, w.partial.p, ps, w.f32[0].b.p); \
+    else k_first_rhs<KK, double><<<g, TB, 0, s>>>(n, w.B64.p, w.partial.p, ps, w.f64[0].b.p);         \
+    break;
+    DEC_K(1) DEC_K(2) DEC_K(4) DEC_K(8) DEC_K(16) DEC_K(32)
+#undef DEC_K
+  }
+  k_reduce_partials<<<K * np, 256, 0, s>>>(w.nblocks, K, np, w.partial.p, w.bn2.p);
+  DEC_CHECK_LAUNCH();
+  DEC_CUDA(cudaMemcpyAsync(w.norms.p, w.bn2.p, (size_t)K * np * sizeof(double), cudaMemcpyDeviceToDevice, s));
+}
+
 // The whole refinement loop of a Jacobi / Chebyshev solve as one graph, from the FP64 panels
 // (B64, U64) and the loop state (k_loop_init):
 //   ||b||²; e = 0; [u += e; r = b - A u; test]; WHILE (test): { e = V^c(r); u += e; r = b - A u; test }
 // The test (k_ir_check) sets the WHILE node's condition, so the solve needs no host round trip.
-static void capture_solve(dec_mg& mg, Workspace& w) {
+// zero_guess (u = 0; FP32 / FP64 V-cycles): the bracketed first step is r = b with its norms.
+static void capture_solve(dec_mg& mg, Workspace& w, bool zero_guess) {
   if (w.bn2.n < (size_t)w.K * w.npanels) w.bn2.alloc((size_t)w.K * w.npanels);
   if (!w.loop.p) w.loop.alloc(1);
   cudaGraph_t g = nullptr;
@@ -2244,9 +2293,13 @@ static void capture_solve(dec_mg& mg, Workspace& w) {
     cudaGraphConditionalHandle h;
     DEC_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
     DEC_CUDA(cudaStreamBeginCaptureToGraph(mg.cap, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    enqueue_bnorms(mg, w, mg.cap, w.bn2.p);
-    zero_correction(mg, w, mg.cap);
-    dispatch(mg, w, mg.cap, G_RESID);
+    if (zero_guess && w.prec != 2) {
+      enqueue_first_rhs(mg, w, mg.cap);
+    } else {
+      enqueue_bnorms(mg, w, mg.cap, w.bn2.p);
+      zero_correction(mg, w, mg.cap);
+      dispatch(mg, w, mg.cap, G_RESID);
+    }
     k_ir_check<<<1, 256, 0, mg.cap>>>(h, w.norms.p, w.bn2.p, w.loop.p);
     DEC_CHECK_LAUNCH();
     cudaStreamCaptureStatus st;
@@ -2270,11 +2323,11 @@ static void capture_solve(dec_mg& mg, Workspace& w) {
     k_ir_check<<<1, 256, 0, mg.cap>>>(h, w.norms.p, w.bn2.p, w.loop.p);
     DEC_CHECK_LAUNCH();
     DEC_CUDA(cudaStreamEndCapture(mg.cap, &body));
-    w.solve_pre = count_kernel_nodes(g);
+    w.solve_pre[zero_guess] = count_kernel_nodes(g);
     w.solve_body = count_kernel_nodes(body);
     cudaGraphExec_t ex = nullptr;
     DEC_CUDA(cudaGraphInstantiate(&ex, g, 0));
-    w.solve_graph = ex;
+    w.solve_graph[zero_guess] = ex;
   } catch (...) {
     fail();
     throw;
@@ -2289,7 +2342,8 @@ static void enqueue_solve(dec_mg& mg, Workspace& w, const double* bd, double* ud
   const Level& F = mg.lv[0];
   const int n = F.n, K = w.K, np = w.npanels;
   const size_t total = (size_t)n * K * np;
-  if (!w.solve_graph) capture_solve(mg, w);
+  const int z = use_initial_guess ? 0 : 1;
+  if (!w.solve_graph[z]) capture_solve(mg, w, z == 1);
   k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, K, np, F.dperm.p, bd, w.B64.p);
   if (use_initial_guess)
     k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, K, np, F.dperm.p, ud, w.U64.p);
@@ -2297,7 +2351,7 @@ static void enqueue_solve(dec_mg& mg, Workspace& w, const double* bd, double* ud
     DEC_CUDA(cudaMemsetAsync(w.U64.p, 0, total * sizeof(double), s));
   k_loop_init<<<1, 1, 0, s>>>(w.loop.p, nrhs, max_iters, rtol);
   DEC_CHECK_LAUNCH();
-  DEC_CUDA(cudaGraphLaunch(w.solve_graph, s));
+  DEC_CUDA(cudaGraphLaunch(w.solve_graph[z], s));
   k_from_panels<double, double><<<grid_for((long long)n * nrhs, 256), 256, 0, s>>>(n, nrhs, K, F.diperm.p, w.U64.p, ud);
   DEC_CHECK_LAUNCH();
 }
@@ -2309,7 +2363,7 @@ static void fill_report(const Workspace& w, const LoopState& st, bool guess, flo
   rep->max_rel_residual = st.worst;
   rep->seconds = ms * 1e-3;
   // to_panels (b, and u), loop init, the graph's kernels, from_panels
-  rep->launches = (guess ? 2 : 1) + 1 + w.solve_pre + (int64_t)st.it * w.solve_body + 1;
+  rep->launches = (guess ? 2 : 1) + 1 + w.solve_pre[guess ? 0 : 1] + (int64_t)st.it * w.solve_body + 1;
   rep->rhs_block = w.K;
   rep->fallback_iteration = -1;
 }
@@ -2584,7 +2638,7 @@ uint64_t mg_solve_submit(dec_mg* mg, double* u, const double* b, int nrhs, doubl
   cudaStream_t hin = mg->pipe[0], comp = mg->pipe[1], hout = mg->pipe[2];
   Workspace& w = workspace(*mg, nrhs, mg->opt.precision, false);
   set_shifts(*mg, w, nullptr, nrhs, comp);
-  if (!w.solve_graph) capture_solve(*mg, w);
+  if (!w.solve_graph[use_initial_guess ? 0 : 1]) capture_solve(*mg, w, !use_initial_guess);
   const size_t len = (size_t)mg->lv[0].n * nrhs;
   DArr<double>& bs = w.pb[slot];
   DArr<double>& us = w.pu[slot];

@@ -247,6 +247,11 @@ dec_status dec_mg_full_multigrid(dec_mg* mg, double* u, const double* b, int32_t
                                  void* stream);
 dec_status dec_mg_solve(dec_mg* mg, double* u, const double* b, int32_t nrhs, double rtol,
                         int32_t max_iters, dec_solve_report* report, void* stream);
+/* dec_mg_solve from u = 0 (multigrid_vcycles with a zero initial guess): u is output only and
+ * is not read.  The first refinement step's residual is b itself, so it costs one pass over b
+ * instead of the FP64 update and residual passes (the same iterates bit for bit). */
+dec_status dec_mg_solve_from_zero(dec_mg* mg, double* u, const double* b, int32_t nrhs, double rtol,
+                                  int32_t max_iters, dec_solve_report* report, void* stream);
 /* Same solve with host u / b (pinned or pageable); copies are part of the call.  With
  * use_initial_guess = 0 the solve starts from u = 0 and u_host is output only (not copied in). */
 dec_status dec_mg_solve_host(dec_mg* mg, double* u_host, const double* b_host, int32_t nrhs, double rtol,

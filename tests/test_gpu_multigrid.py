@@ -199,6 +199,25 @@ def test_host_driven_loop_matches_device_loop(dec, built):
     assert out[0][1:] == out[1][1:] and out[0][3] == 1
 
 
+@pytest.mark.parametrize("precision,device_loop", [(0, 1), (1, 1), (2, 1), (1, 0)])
+def test_solve_from_zero_matches_zero_guess(dec, built, precision, device_loop):
+    """dec_mg_solve_from_zero (u output only; the first residual is b itself) gives the same bits
+    and steps as dec_mg_solve from a zeroed u, whatever u held before; b = 0 needs no step."""
+    coarse, md, _ = built["ico4_circum"]
+    mg = dec.MultigridData(coarse, 4, shift=1.0, center="circumcenter", project_radius=1.0, precision=precision,
+                           pre=0, post=2, cheb_ratio=3.0, inner_cycles=2, device_loop=device_loop)
+    B = torch.tensor(np.stack([uniform(170 + j, mg.n) for j in range(5)]), device="cuda")
+    B[3] = 0.0
+    U0, r0 = mg.solve(torch.zeros_like(B), B, rtol=1e-10, max_iters=60)
+    for _ in range(2):
+        Uz, rz = mg.solve(torch.full_like(B, float("nan")), B, rtol=1e-10, max_iters=60, use_initial_guess=False)
+        np.testing.assert_array_equal(Uz.cpu().numpy(), U0.cpu().numpy())
+        assert (rz.iterations, rz.converged, rz.max_rel_residual) == (r0.iterations, 1, r0.max_rel_residual)
+    assert float(Uz[3].abs().max()) == 0.0
+    Z, rzz = mg.solve(torch.ones_like(B), torch.zeros_like(B), rtol=1e-10, use_initial_guess=False)
+    assert rzz.iterations == 0 and rzz.converged == 1 and float(Z.abs().max()) == 0.0
+
+
 def test_pipelined_host_solves_match_synchronous(dec, built):
     """solve_host_submit / wait: three solves in flight on the hierarchy's own streams give the
     same bits as the synchronous host-buffer solve; a fourth submit before a wait, a second wait on
