@@ -353,13 +353,15 @@ struct Lanes {
 //   S_CHEB0 : d = D⁻¹ r / θ; out = x + d
 //   S_CHEBN : d = c1 d + c2 D⁻¹ r; out = x + d
 // SH: right-hand side j of panel p has its own operator A + cs[p*K + j] I (D likewise).
-template <class T, int K, int W, bool SH>
+// UPD: the sweep's result is the refinement step's correction e, added straight to the FP64
+// iterate (u += (double) e, the update pass's arithmetic) instead of being stored in out.
+template <class T, int K, int W, bool SH, bool UPD = false>
 __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restrict__ col,
                                            const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
                                            const CT<T>* __restrict__ dinv, const T* __restrict__ b,
                                            const T* __restrict__ x, T* __restrict__ out, T* __restrict__ d,
                                            const SweepPrm<CT<T>>& prm, size_t pstride,
-                                           const CT<T>* __restrict__ shf) {
+                                           const CT<T>* __restrict__ shf, double* __restrict__ u64 = nullptr) {
   using Ln = Lanes<T, K>;
   using C = CT<T>;
   pdl_enter();
@@ -451,7 +453,12 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
       }
       if (prm.write_d) stv<T, V>(d + ik, dn);
     }
-    stv<T, V>(out + ik, o);
+    if constexpr (UPD) {
+#pragma unroll
+      for (int q = 0; q < V; ++q) u64[ik + q] += (double)(T)o[q];
+    } else {
+      stv<T, V>(out + ik, o);
+    }
   }
 }
 
@@ -462,6 +469,18 @@ __global__ void __launch_bounds__(TB) k_sweep(int n, int Wr, const int32_t* __re
                                               const T* __restrict__ x, T* __restrict__ out, T* __restrict__ d,
                                               SweepPrm<CT<T>> prm, size_t pstride, const CT<T>* __restrict__ shf) {
   sweep_rows<T, K, W, SH>(n, Wr, col, off, diag, dinv, b, x, out, d, prm, pstride, shf);
+}
+
+// The last sweep of a refinement step's V-cycles on the finest level with the step's update
+// u += e fused in (FP32 / FP64 storage).
+template <class T, int K, int W, bool SH>
+__global__ void __launch_bounds__(TB) k_sweep_u(int n, int Wr, const int32_t* __restrict__ col,
+                                                const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
+                                                const CT<T>* __restrict__ dinv, const T* __restrict__ b,
+                                                const T* __restrict__ x, T* __restrict__ out, T* __restrict__ d,
+                                                SweepPrm<CT<T>> prm, size_t pstride, const CT<T>* __restrict__ shf,
+                                                double* __restrict__ u64) {
+  sweep_rows<T, K, W, SH, true>(n, Wr, col, off, diag, dinv, b, x, out, d, prm, pstride, shf, u64);
 }
 
 // FP16-stored sweeps carry eight values per 16-byte access; unbounded they took 72 registers
@@ -566,20 +585,37 @@ __global__ void __launch_bounds__(TB) k_prolong(int nf, const int32_t* __restric
   }
 }
 
-// Coarsest level: x = A⁻¹ b with the dense FP64 inverse; one thread per (row, right-hand side),
-// the row of A⁻¹ shared (broadcast) by a row's K lanes.
+// Coarsest level: x = A⁻¹ b with the dense FP64 inverse.  One CTA per (row, panel): its TB threads
+// are S = TB / K segments of the row's dot product for the K right-hand sides (segment g takes
+// columns g, g + S, g + 2S, ... into two FP64 sums), and the segments' sums meet in a fixed-order
+// tree in shared memory.  A thread per (row, right-hand side) running the whole row left a
+// 162-vertex level's solve latency-bound at 21 CTAs.
 template <class T, int K>
 __global__ void __launch_bounds__(TB) k_coarse(int n, const double* __restrict__ ainv, const T* __restrict__ b,
                                                T* __restrict__ x, size_t pstride) {
+  constexpr int S = TB / K;
   pdl_enter();
   const T* bb = b + (size_t)blockIdx.y * pstride;
   T* xx = x + (size_t)blockIdx.y * pstride;
-  const int k = threadIdx.x % K;
-  for (int i = blockIdx.x * (TB / K) + threadIdx.x / K; i < n; i += gridDim.x * (TB / K)) {
+  const int k = threadIdx.x % K, g = threadIdx.x / K;
+  __shared__ double sh[TB];
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
     const double* a = ainv + (size_t)i * n;
-    double s = 0.0;
-    for (int j = 0; j < n; ++j) s += a[j] * to_d(bb[(size_t)j * K + k]);
-    xx[(size_t)i * K + k] = from_d<T>(s);
+    double s0 = 0.0, s1 = 0.0;
+    int j = g;
+    for (; j + S < n; j += 2 * S) {
+      s0 += a[j] * to_d(bb[(size_t)j * K + k]);
+      s1 += a[j + S] * to_d(bb[(size_t)(j + S) * K + k]);
+    }
+    if (j < n) s0 += a[j] * to_d(bb[(size_t)j * K + k]);
+    sh[threadIdx.x] = s0 + s1;
+    __syncthreads();
+    for (int st = S / 2; st > 0; st >>= 1) {
+      if (g < st) sh[threadIdx.x] += sh[threadIdx.x + st * K];
+      __syncthreads();
+    }
+    if (g == 0) xx[(size_t)i * K + k] = from_d<T>(sh[k]);
+    __syncthreads();
   }
 }
 
@@ -1778,7 +1814,7 @@ static void launch_prolong(const Level& L, const Level& Cl, const T* z, T* x, bo
 
 template <class T, int K>
 static void launch_sweep(const Level& L, const T* b, const T* x, T* out, T* d, SweepPrm<CT<T>> prm, int np,
-                         cudaStream_t s, const CT<T>* cs) {
+                         cudaStream_t s, const CT<T>* cs, double* upd = nullptr) {
   size_t ps = (size_t)L.n * K;
   dim3 grid = row_grid<T, K>(L.n, np);
   if constexpr (std::is_same<T, __half>::value) {
@@ -1798,7 +1834,19 @@ static void launch_sweep(const Level& L, const T* b, const T* x, T* out, T* d, S
     const CT<T>* off = pick<T>(L.off64, L.off32);
     const CT<T>* dg = pick<T>(L.diag64, L.diag32);
     const CT<T>* di = pick<T>(L.dinv64, L.dinv32);
-    if (cs) {
+    if (upd) {  // u += (this sweep's result); out is not written
+      auto go = [&](auto kern) {
+        launch_pdl(kern, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs, upd);
+      };
+      if (cs) {
+        if (L.W == 6) go(k_sweep_u<T, K, 6, true>);
+        else go(k_sweep_u<T, K, 0, true>);
+      } else if (L.W == 6) {
+        go(k_sweep_u<T, K, 6, false>);
+      } else {
+        go(k_sweep_u<T, K, 0, false>);
+      }
+    } else if (cs) {
       if (L.W == 6)
         launch_pdl(k_sweep<T, K, 6, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
       else
@@ -1814,7 +1862,7 @@ static void launch_sweep(const Level& L, const T* b, const T* x, T* out, T* d, S
 // Smooth `sweeps` times starting from x (zero if zero_x); returns the buffer holding the result.
 template <class T, int K>
 static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool zero_x, int sweeps, int np,
-                 cudaStream_t s) {
+                 cudaStream_t s, double* upd = nullptr) {
   const dec_mg_options& o = mg.opt;
   T* other = (x == B.x.p) ? B.y.p : B.x.p;
   if constexpr (!std::is_same<T, __half>::value) {
@@ -1861,7 +1909,7 @@ static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool z
       prm.c2 = (C)(2 * rho_new / delta);
       rho = rho_new;
     }
-    launch_sweep<T, K>(L, B.b.p, x, other, B.d.p, prm, np, s, B.cs);
+    launch_sweep<T, K>(L, B.b.p, x, other, B.d.p, prm, np, s, B.cs, it + 1 == sweeps ? upd : nullptr);
     std::swap(x, other);
     zero_x = false;
   }
@@ -1909,7 +1957,7 @@ static double* cg_smooth(const dec_mg& mg, Workspace& w, const Level& L, LevelBu
 
 template <class T, int K>
 static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bufs, int l, T* x, bool zero_x, int mu,
-                   int np, cudaStream_t s);
+                   int np, cudaStream_t s, double* upd = nullptr);
 
 // _multigrid_μ_cycle, Multigrid.jl:857-872, with the Krylov CG smoother: CG (steps) ; if the
 // coarsest level, return ; r = b - A u ; restrict ; recurse (twice for μ = 2) ; u += P z ; CG.
@@ -1945,9 +1993,11 @@ static double* cg_mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs
 }
 
 // One μ-cycle at level l on (b = B[l].b, initial guess x); returns the buffer with the result.
+// upd (finest level, Jacobi / Chebyshev post-smoothing, not FP16): the last sweep adds its result
+// to the FP64 iterate (k_sweep_u) and the returned buffer holds nothing.
 template <class T, int K>
 static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bufs, int l, T* x, bool zero_x, int mu,
-                   int np, cudaStream_t s) {
+                   int np, cudaStream_t s, double* upd) {
   const Level& L = mg.lv[l];
   LevelBufs<T>& B = bufs[l];
   if constexpr (std::is_same<T, double>::value) {
@@ -1964,7 +2014,7 @@ static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bu
                  (size_t)L.n * K);
       return B.x.p;
     }
-    launch_pdl(k_coarse<T, K>, dim3(grid_for(L.n, TB / K, 64), np), dim3(TB), s, L.n, (const double*)mg.ainv.p,
+    launch_pdl(k_coarse<T, K>, dim3(grid_for(L.n, 1, 8), np), dim3(TB), s, L.n, (const double*)mg.ainv.p,
                (const T*)B.b.p, B.x.p, (size_t)L.n * K);
     return B.x.p;
   }
@@ -1988,7 +2038,7 @@ static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bu
   if (mu > 1) z = mu_cycle<T, K>(mg, w, bufs, l + 1, z, false, mu - 1, np, s);
   // x = 0: the prolonged correction is x (written, not added)
   launch_prolong<T, K>(L, Cl, (const T*)z, x, zero_x, np, s);
-  return smooth<T, K>(mg, L, B, x, false, mg.opt.post, np, s);
+  return smooth<T, K>(mg, L, B, x, false, mg.opt.post, np, s, upd);
 }
 
 template <class T>
@@ -2028,7 +2078,8 @@ static int choose_k(const dec_mg& mg, int nrhs, int prec) {
 // Refinement step, part 1: u += e; r = b - A u in FP64 (r stored in the inner precision as the
 // finest right-hand side) with per-RHS squared norms.
 template <class T, int K>
-static void enqueue_resid_T(dec_mg& mg, Workspace& w, cudaStream_t s, std::vector<LevelBufs<T>>& bufs) {
+static void enqueue_resid_T(dec_mg& mg, Workspace& w, cudaStream_t s, std::vector<LevelBufs<T>>& bufs,
+                            bool updated = false) {
   const Level& F = mg.lv[0];
   const int np = w.npanels;
   const size_t total = (size_t)F.n * K * np;
@@ -2040,8 +2091,9 @@ static void enqueue_resid_T(dec_mg& mg, Workspace& w, cudaStream_t s, std::vecto
                (const __half*)bufs[0].x.p, (const double*)w.escale.p, w.U64.p);
     rout = w.r32.p;
   } else {
-    launch_pdl(k_axpy_update<T>, dim3(grid_for((long long)total, 256)), dim3(256), s, total, (const T*)bufs[0].x.p,
-               w.U64.p);
+    if (!updated)  // else the V-cycles' last sweep added e to u already
+      launch_pdl(k_axpy_update<T>, dim3(grid_for((long long)total, 256)), dim3(256), s, total,
+                 (const T*)bufs[0].x.p, w.U64.p);
     rout = bufs[0].b.p;
   }
   dim3 g(w.nblocks, np);
@@ -2069,12 +2121,16 @@ static void enqueue_resid_T(dec_mg& mg, Workspace& w, cudaStream_t s, std::vecto
 
 // Refinement step, part 2: e = V^c(r) (c = inner_cycles) from a zero initial guess, left in
 // bufs[0].x.
+// upd: the last cycle's last sweep adds e to the FP64 iterate (fused_update) and e is not kept.
 template <class T, int K>
-static void enqueue_vcycle_T(dec_mg& mg, Workspace& w, cudaStream_t s, std::vector<LevelBufs<T>>& bufs) {
+static void enqueue_vcycle_T(dec_mg& mg, Workspace& w, cudaStream_t s, std::vector<LevelBufs<T>>& bufs,
+                             double* upd = nullptr) {
   const size_t total = (size_t)mg.lv[0].n * K * w.npanels;
+  const int c_last = mg.opt.inner_cycles - 1;
   T* e = bufs[0].x.p;
-  for (int c = 0; c < mg.opt.inner_cycles; ++c) e = mu_cycle<T, K>(mg, w, bufs, 0, e, c == 0, mg.opt.mu, w.npanels, s);
-  if (e != bufs[0].x.p)
+  for (int c = 0; c <= c_last; ++c)
+    e = mu_cycle<T, K>(mg, w, bufs, 0, e, c == 0, mg.opt.mu, w.npanels, s, c == c_last ? upd : nullptr);
+  if (!upd && e != bufs[0].x.p)
     DEC_CUDA(cudaMemcpyAsync(bufs[0].x.p, e, total * sizeof(T), cudaMemcpyDeviceToDevice, s));
   DEC_CHECK_LAUNCH();
 }
@@ -2094,7 +2150,16 @@ static void enqueue_cycle(dec_mg& mg, Workspace& w, cudaStream_t s) {
 // Vectors a smoothing sweep reads or writes once: Jacobi b, x, out; Chebyshev b, x, d (r/w), out.
 static int prm_vectors(int smoother) { return smoother == DEC_SMOOTH_JACOBI ? 3 : 5; }
 
-enum GraphKind { G_RESID = 0, G_VCYCLE = 1, G_CYCLE = 2, G_VCYCLE_PLAIN = 3 };  // plain: learned-smoother fallback
+// plain: learned-smoother fallback; G_STEP (V-cycles with the update fused into the last sweep,
+// then the residual) is enqueued only inside the device refinement loop, never cached in graph[]
+enum GraphKind { G_RESID = 0, G_VCYCLE = 1, G_CYCLE = 2, G_VCYCLE_PLAIN = 3, G_STEP = 4 };
+
+// The last finest-level sweep can take the refinement update (k_sweep_u): Jacobi / Chebyshev
+// post-smoothing on a finest level that is not the directly solved one, FP32 / FP64 storage.
+static bool fused_update(const dec_mg& mg, const Workspace& w) {
+  const int s = mg.opt.smoother;
+  return (s == DEC_SMOOTH_JACOBI || s == DEC_SMOOTH_CHEBYSHEV) && mg.opt.post > 0 && mg.lc > 0 && w.prec != 2;
+}
 
 template <int K>
 static void enqueue_kind(dec_mg& mg, Workspace& w, cudaStream_t s, int kind) {
@@ -2104,11 +2169,23 @@ static void enqueue_kind(dec_mg& mg, Workspace& w, cudaStream_t s, int kind) {
     if (kind == G_RESID) enqueue_resid_T<__half, K>(mg, w, s, w.f16);
     else enqueue_vcycle_T<__half, K>(mg, w, s, w.f16);
   } else if (w.prec == 1) {
-    if (kind == G_RESID) enqueue_resid_T<float, K>(mg, w, s, w.f32);
-    else enqueue_vcycle_T<float, K>(mg, w, s, w.f32);
+    if (kind == G_STEP) {
+      enqueue_vcycle_T<float, K>(mg, w, s, w.f32, w.U64.p);
+      enqueue_resid_T<float, K>(mg, w, s, w.f32, true);
+    } else if (kind == G_RESID) {
+      enqueue_resid_T<float, K>(mg, w, s, w.f32);
+    } else {
+      enqueue_vcycle_T<float, K>(mg, w, s, w.f32);
+    }
   } else {
-    if (kind == G_RESID) enqueue_resid_T<double, K>(mg, w, s, w.f64);
-    else enqueue_vcycle_T<double, K>(mg, w, s, w.f64);
+    if (kind == G_STEP) {
+      enqueue_vcycle_T<double, K>(mg, w, s, w.f64, w.U64.p);
+      enqueue_resid_T<double, K>(mg, w, s, w.f64, true);
+    } else if (kind == G_RESID) {
+      enqueue_resid_T<double, K>(mg, w, s, w.f64);
+    } else {
+      enqueue_vcycle_T<double, K>(mg, w, s, w.f64);
+    }
   }
 }
 
@@ -2318,8 +2395,12 @@ static void capture_solve(dec_mg& mg, Workspace& w, bool zero_guess) {
     DEC_CUDA(cudaStreamEndCapture(mg.cap, &g));
     cudaGraph_t body = prm.conditional.phGraph_out[0];
     DEC_CUDA(cudaStreamBeginCaptureToGraph(mg.cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    dispatch(mg, w, mg.cap, G_VCYCLE);
-    dispatch(mg, w, mg.cap, G_RESID);
+    if (fused_update(mg, w)) {
+      dispatch(mg, w, mg.cap, G_STEP);
+    } else {
+      dispatch(mg, w, mg.cap, G_VCYCLE);
+      dispatch(mg, w, mg.cap, G_RESID);
+    }
     k_ir_check<<<1, 256, 0, mg.cap>>>(h, w.norms.p, w.bn2.p, w.loop.p);
     DEC_CHECK_LAUNCH();
     DEC_CUDA(cudaStreamEndCapture(mg.cap, &body));
