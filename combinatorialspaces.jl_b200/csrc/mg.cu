@@ -1231,8 +1231,8 @@ struct Workspace {
   DArr<double> ceig;          // coarse_solver 2: FP64 scratch of the coarsest solve
   std::vector<double> hcs64;  // host staging of the shifts
   std::vector<float> hcs32;
-  cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};  // GraphKind
-  int64_t launches[4] = {0, 0, 0, 0};                               // kernel nodes per graph
+  cudaGraphExec_t graph[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // GraphKind
+  int64_t launches[5] = {0, 0, 0, 0, 0};                                     // kernel nodes per graph
   void drop_graphs() {
     for (auto& g : graph) {
       if (g) cudaGraphExecDestroy(g);
@@ -2150,8 +2150,8 @@ static void enqueue_cycle(dec_mg& mg, Workspace& w, cudaStream_t s) {
 // Vectors a smoothing sweep reads or writes once: Jacobi b, x, out; Chebyshev b, x, d (r/w), out.
 static int prm_vectors(int smoother) { return smoother == DEC_SMOOTH_JACOBI ? 3 : 5; }
 
-// plain: learned-smoother fallback; G_STEP (V-cycles with the update fused into the last sweep,
-// then the residual) is enqueued only inside the device refinement loop, never cached in graph[]
+// plain: learned-smoother fallback; G_STEP: V-cycles with the update fused into the last sweep,
+// then the residual (the refinement loops' step when fused_update holds)
 enum GraphKind { G_RESID = 0, G_VCYCLE = 1, G_CYCLE = 2, G_VCYCLE_PLAIN = 3, G_STEP = 4 };
 
 // The last finest-level sweep can take the refinement update (k_sweep_u): Jacobi / Chebyshev
@@ -2599,14 +2599,25 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
     k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, K, np, F.dperm.p, ud, w.U64.p);
   else
     DEC_CUDA(cudaMemsetAsync(w.U64.p, 0, total * sizeof(double), s));
-  // the first refinement step adds e = 0
-  if (w.prec == 2) DEC_CUDA(cudaMemsetAsync(w.f16[0].x.p, 0, total * sizeof(__half), s));
-  else if (w.prec == 1) DEC_CUDA(cudaMemsetAsync(w.f32[0].x.p, 0, total * sizeof(float), s));
-  else DEC_CUDA(cudaMemsetAsync(w.f64[0].x.p, 0, total * sizeof(double), s));
-  DEC_CHECK_LAUNCH();
-  // ||b|| per right-hand side.
+  const bool learned = mg->opt.smoother == DEC_SMOOTH_LEARNED;
+  // the steps the device loop takes: from u = 0 the first residual is b (k_first_rhs), and the
+  // update rides on the last sweep of each step's V-cycles (G_STEP)
+  const bool zero_start = !use_initial_guess && !learned && w.prec != 2;
+  const bool fuse = !learned && fused_update(*mg, w);
   std::vector<double> bn((size_t)K * np), rn((size_t)K * np);
-  {
+  if (zero_start) {
+    if (w.bn2.n < (size_t)K * np) w.bn2.alloc((size_t)K * np);
+    enqueue_first_rhs(*mg, w, s);
+    DEC_CUDA(cudaMemcpyAsync(bn.data(), w.bn2.p, bn.size() * 8, cudaMemcpyDeviceToHost, s));
+    DEC_CUDA(cudaStreamSynchronize(s));
+    for (auto& x : bn) x = std::sqrt(x);
+  } else {
+    // the first refinement step adds e = 0
+    if (w.prec == 2) DEC_CUDA(cudaMemsetAsync(w.f16[0].x.p, 0, total * sizeof(__half), s));
+    else if (w.prec == 1) DEC_CUDA(cudaMemsetAsync(w.f32[0].x.p, 0, total * sizeof(float), s));
+    else DEC_CUDA(cudaMemsetAsync(w.f64[0].x.p, 0, total * sizeof(double), s));
+    DEC_CHECK_LAUNCH();
+    // ||b|| per right-hand side.
     dim3 g(w.nblocks, np);
     switch (K) {
 #define DEC_K(KK) \
@@ -2620,17 +2631,15 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
     DEC_CUDA(cudaStreamSynchronize(s));
     for (auto& x : bn) x = std::sqrt(x);
   }
-  const bool learned = mg->opt.smoother == DEC_SMOOTH_LEARNED;
   if (!w.graph[G_RESID]) w.graph[G_RESID] = capture(*mg, w, G_RESID);
   if (!w.graph[G_VCYCLE]) w.graph[G_VCYCLE] = capture(*mg, w, G_VCYCLE);
+  if (fuse && !w.graph[G_STEP]) w.graph[G_STEP] = capture(*mg, w, G_STEP);
   if (learned) {
     if (!w.graph[G_VCYCLE_PLAIN]) w.graph[G_VCYCLE_PLAIN] = capture(*mg, w, G_VCYCLE_PLAIN);
     if (w.Ubak.n < total) w.Ubak.alloc(total);
   }
   int64_t nl = (use_initial_guess ? 2 : 1) + 2;  // to_panels, ||b|| partials + reduce
-  auto residual = [&]() {                        // u += e; r = b - A u; worst relative residual
-    DEC_CUDA(cudaGraphLaunch(w.graph[G_RESID], s));
-    nl += w.launches[G_RESID];
+  auto worst_rel = [&]() {  // the worst relative residual from the norms on the device
     DEC_CUDA(cudaMemcpyAsync(rn.data(), w.norms.p, rn.size() * 8, cudaMemcpyDeviceToHost, s));
     DEC_CUDA(cudaStreamSynchronize(s));
     double wr = 0.0;
@@ -2641,13 +2650,18 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
     }
     return wr;
   };
+  auto residual = [&]() {  // u += e; r = b - A u; worst relative residual
+    DEC_CUDA(cudaGraphLaunch(w.graph[G_RESID], s));
+    nl += w.launches[G_RESID];
+    return worst_rel();
+  };
   int it = 0, fallback_at = -1;
   double worst = 0.0, prev = 0.0;
   bool conv = false, plain = !learned;
   for (;;) {
     const bool check = !plain && it > 0;
     if (check) DEC_CUDA(cudaMemcpyAsync(w.Ubak.p, w.U64.p, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    worst = residual();
+    worst = (it == 0 ? zero_start : fuse) ? worst_rel() : residual();
     if (check && !(worst <= mg->opt.fallback_rho * prev)) {
       // the learned step fell behind: undo it (u from before the step, e = 0, same residual)
       // and continue with the plain smoother
@@ -2665,8 +2679,8 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
     }
     if (it >= max_iters) break;
     prev = worst;
-    const int kind = learned && plain ? G_VCYCLE_PLAIN : G_VCYCLE;
-    DEC_CUDA(cudaGraphLaunch(w.graph[kind], s));  // e = V(r)
+    const int kind = fuse ? G_STEP : learned && plain ? G_VCYCLE_PLAIN : G_VCYCLE;
+    DEC_CUDA(cudaGraphLaunch(w.graph[kind], s));  // e = V(r) (G_STEP: and u += e, r = b - A u)
     nl += w.launches[kind];
     ++it;
   }
@@ -2992,8 +3006,12 @@ static cudaGraphExec_t batch_capture(dec_batch& bt, int kind) {
       Workspace& w = *bt.used[q];
       cudaStream_t st = bt.streams[q];
       DEC_CUDA(cudaStreamWaitEvent(st, bt.fork, 0));
-      if (kind == 1) dispatch(mg, w, st, G_VCYCLE);
-      dispatch(mg, w, st, G_RESID);
+      if (kind == 1 && fused_update(mg, w)) {
+        dispatch(mg, w, st, G_STEP);  // V-cycles with u += e in the last sweep, then the residual
+      } else {
+        if (kind == 1) dispatch(mg, w, st, G_VCYCLE);
+        dispatch(mg, w, st, G_RESID);
+      }
       DEC_CUDA(cudaMemcpyAsync(bt.norms.p + bt.off[q], w.norms.p, w.norms.bytes(), cudaMemcpyDeviceToDevice, st));
       DEC_CUDA(cudaEventRecord(bt.join[q], st));
       DEC_CUDA(cudaStreamWaitEvent(bt.cap, bt.join[q], 0));

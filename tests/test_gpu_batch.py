@@ -113,6 +113,10 @@ def test_batch_over_uneven_meshes(O, dec):
         for q, (md, mg) in enumerate(pairs):
             assert reps[q].converged == 1 and reps[q].iterations <= tot.iterations
             _check_solutions(csc(md.op(0)), Bs[q], Us[q].cpu().numpy(), shifts[q], 1e-9)
+            # every group takes the batch's steps; its own solve held to as many gives the same bits
+            U1 = torch.zeros_like(Us[q])
+            mg.solve(U1, torch.tensor(Bs[q], device="cuda"), rtol=1e-30, max_iters=tot.iterations, shifts=shifts[q])
+            np.testing.assert_array_equal(U1.cpu().numpy(), Us[q].cpu().numpy())
 
 
 @pytest.mark.parametrize("kind,m,n", [("pp", 0, 1), ("pp", 1, 0), ("pp", 0, 2), ("pp", 2, 0), ("pp", 1, 1),
