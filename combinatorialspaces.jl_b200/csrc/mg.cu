@@ -655,28 +655,77 @@ __global__ void __launch_bounds__(TB) k_coarse_eig2(int n, const double* __restr
   }
 }
 
-// Column-major RHS block (nrhs vectors of length n, reference vertex order) -> panels of K in
-// the level's internal order (perm: internal -> reference), and back.
-template <class T, class S>
-__global__ void k_to_panels(int n, int nrhs, int K, int npanels, const int32_t* __restrict__ perm,
-                            const S* __restrict__ src, T* __restrict__ dst) {
-  size_t total = (size_t)n * K * npanels;
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
-    size_t p = q / ((size_t)n * K), rem = q % ((size_t)n * K);
-    int i = (int)(rem / K), k = (int)(rem % K);
-    int j = (int)p * K + k;
-    dst[q] = j < nrhs ? (T)src[(size_t)j * n + perm[i]] : T(0);
+// Column-major RHS block (nrhs vectors of length n, reference vertex order) <-> panels of K in the
+// level's internal order (iperm: reference -> internal).  A CTA moves a tile of kTile vertices x K
+// right-hand sides of one panel through shared memory, so both sides move in whole runs: a panel
+// row's K contiguous values, and kTile contiguous values of a vector.  (Element by element, one of
+// the two sides was a scattered 8-byte access: 1.7 / 3.3 TB/s at L8 x 32.)  Padding right-hand
+// sides (j >= nrhs) of the last panel are zero.
+constexpr int kTile = 32;
+
+template <int K>
+__global__ void __launch_bounds__(256) k_vectors_to_panels(int n, int nrhs, const int32_t* __restrict__ iperm,
+                                                           const double* __restrict__ src, double* __restrict__ dst) {
+  __shared__ double t[kTile][K + 1];
+  const int p = blockIdx.y;
+  double* dp = dst + (size_t)p * n * K;
+  for (int v0 = blockIdx.x * kTile; v0 < n; v0 += gridDim.x * kTile) {
+    for (int e = threadIdx.x; e < kTile * K; e += blockDim.x) {
+      const int k = e / kTile, dv = e % kTile, v = v0 + dv, j = p * K + k;
+      t[dv][k] = (v < n && j < nrhs) ? src[(size_t)j * n + v] : 0.0;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kTile * K; e += blockDim.x) {
+      const int dv = e / K, k = e % K, v = v0 + dv;
+      if (v < n) dp[(size_t)iperm[v] * K + k] = t[dv][k];
+    }
+    __syncthreads();
   }
 }
 
-template <class T, class S>
-__global__ void k_from_panels(int n, int nrhs, int K, const int32_t* __restrict__ iperm, const S* __restrict__ src,
-                              T* __restrict__ dst) {
-  size_t total = (size_t)n * nrhs;
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
-    int j = (int)(q / n), i = (int)(q % n);
-    int p = j / K, k = j % K;
-    dst[q] = (T)src[(size_t)p * n * K + (size_t)iperm[i] * K + k];
+template <int K>
+__global__ void __launch_bounds__(256) k_panels_to_vectors(int n, int nrhs, const int32_t* __restrict__ iperm,
+                                                           const double* __restrict__ src, double* __restrict__ dst) {
+  __shared__ double t[kTile][K + 1];
+  const int p = blockIdx.y;
+  const double* sp = src + (size_t)p * n * K;
+  for (int v0 = blockIdx.x * kTile; v0 < n; v0 += gridDim.x * kTile) {
+    for (int e = threadIdx.x; e < kTile * K; e += blockDim.x) {
+      const int dv = e / K, k = e % K, v = v0 + dv;
+      if (v < n) t[dv][k] = sp[(size_t)iperm[v] * K + k];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kTile * K; e += blockDim.x) {
+      const int k = e / kTile, dv = e % kTile, v = v0 + dv, j = p * K + k;
+      if (v < n && j < nrhs) dst[(size_t)j * n + v] = t[dv][k];
+    }
+    __syncthreads();
+  }
+}
+
+// src (nrhs x n, reference order) -> dst panels; iperm: reference -> internal row.
+static void to_panels(int n, int nrhs, int K, int np, const int32_t* iperm, const double* src, double* dst,
+                      cudaStream_t s) {
+  const dim3 g(grid_for(n, kTile, 16), np);
+  switch (K) {
+#define DEC_K(KK) \
+  case KK: k_vectors_to_panels<KK><<<g, 256, 0, s>>>(n, nrhs, iperm, src, dst); break;
+    DEC_K(1) DEC_K(2) DEC_K(4) DEC_K(8) DEC_K(16) DEC_K(32)
+#undef DEC_K
+    default: throw Error(DEC_ERR_INVALID_ARG, "multigrid: bad panel width");
+  }
+}
+
+// panels -> dst (nrhs x n, reference order).
+static void from_panels(int n, int nrhs, int K, int np, const int32_t* iperm, const double* src, double* dst,
+                        cudaStream_t s) {
+  const dim3 g(grid_for(n, kTile, 16), np);
+  switch (K) {
+#define DEC_K(KK) \
+  case KK: k_panels_to_vectors<KK><<<g, 256, 0, s>>>(n, nrhs, iperm, src, dst); break;
+    DEC_K(1) DEC_K(2) DEC_K(4) DEC_K(8) DEC_K(16) DEC_K(32)
+#undef DEC_K
+    default: throw Error(DEC_ERR_INVALID_ARG, "multigrid: bad panel width");
   }
 }
 
@@ -2425,15 +2474,15 @@ static void enqueue_solve(dec_mg& mg, Workspace& w, const double* bd, double* ud
   const size_t total = (size_t)n * K * np;
   const int z = use_initial_guess ? 0 : 1;
   if (!w.solve_graph[z]) capture_solve(mg, w, z == 1);
-  k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, K, np, F.dperm.p, bd, w.B64.p);
+  to_panels(n, nrhs, K, np, F.diperm.p, bd, w.B64.p, s);
   if (use_initial_guess)
-    k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, K, np, F.dperm.p, ud, w.U64.p);
+    to_panels(n, nrhs, K, np, F.diperm.p, ud, w.U64.p, s);
   else
     DEC_CUDA(cudaMemsetAsync(w.U64.p, 0, total * sizeof(double), s));
   k_loop_init<<<1, 1, 0, s>>>(w.loop.p, nrhs, max_iters, rtol);
   DEC_CHECK_LAUNCH();
   DEC_CUDA(cudaGraphLaunch(w.solve_graph[z], s));
-  k_from_panels<double, double><<<grid_for((long long)n * nrhs, 256), 256, 0, s>>>(n, nrhs, K, F.diperm.p, w.U64.p, ud);
+  from_panels(n, nrhs, K, w.npanels, F.diperm.p, w.U64.p, ud, s);
   DEC_CHECK_LAUNCH();
 }
 
@@ -2475,15 +2524,12 @@ void mg_cycles(dec_mg* mg, double* u, const double* b, int nrhs, int cycles, voi
   const Level& F = mg->lv[0];
   const int n = F.n;
   const size_t total = (size_t)n * w.K * w.npanels;
-  k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, w.K, w.npanels, F.dperm.p, b,
-                                                                               w.B64.p);
-  k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, w.K, w.npanels, F.dperm.p, u,
-                                                                               w.U64.p);
+  to_panels(n, nrhs, w.K, w.npanels, F.diperm.p, b, w.B64.p, s);
+  to_panels(n, nrhs, w.K, w.npanels, F.diperm.p, u, w.U64.p, s);
   DEC_CHECK_LAUNCH();
   if (!w.graph[G_CYCLE]) w.graph[G_CYCLE] = capture(*mg, w, G_CYCLE);
   for (int c = 0; c < cycles; ++c) DEC_CUDA(cudaGraphLaunch(w.graph[G_CYCLE], s));
-  k_from_panels<double, double><<<grid_for((long long)n * nrhs, 256), 256, 0, s>>>(n, nrhs, w.K, F.diperm.p,
-                                                                                    w.U64.p, u);
+  from_panels(n, nrhs, w.K, w.npanels, F.diperm.p, w.U64.p, u, s);
   DEC_CHECK_LAUNCH();
 }
 
@@ -2536,8 +2582,7 @@ void mg_full_multigrid(dec_mg* mg, double* u, const double* b, int nrhs, int cyc
   const Level& F = mg->lv[0];
   const int n = F.n;
   const size_t total = (size_t)n * w.K * w.npanels;
-  k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, w.K, w.npanels, F.dperm.p, b,
-                                                                               w.B64.p);
+  to_panels(n, nrhs, w.K, w.npanels, F.diperm.p, b, w.B64.p, s);
   DEC_CHECK_LAUNCH();
   switch (w.K) {
 #define DEC_K(KK) \
@@ -2546,8 +2591,7 @@ void mg_full_multigrid(dec_mg* mg, double* u, const double* b, int nrhs, int cyc
 #undef DEC_K
     default: throw Error(DEC_ERR_INVALID_ARG, "multigrid: bad panel width");
   }
-  k_from_panels<double, double><<<grid_for((long long)n * nrhs, 256), 256, 0, s>>>(n, nrhs, w.K, F.diperm.p,
-                                                                                    w.U64.p, u);
+  from_panels(n, nrhs, w.K, w.npanels, F.diperm.p, w.U64.p, u, s);
   DEC_CHECK_LAUNCH();
 }
 
@@ -2594,9 +2638,9 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
     fill_report(w, st, use_initial_guess, ms, rep);
     return st.conv ? DEC_OK : DEC_ERR_NOT_CONVERGED;
   }
-  k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, K, np, F.dperm.p, bd, w.B64.p);
+  to_panels(n, nrhs, K, np, F.diperm.p, bd, w.B64.p, s);
   if (use_initial_guess)
-    k_to_panels<double, double><<<grid_for((long long)total, 256), 256, 0, s>>>(n, nrhs, K, np, F.dperm.p, ud, w.U64.p);
+    to_panels(n, nrhs, K, np, F.diperm.p, ud, w.U64.p, s);
   else
     DEC_CUDA(cudaMemsetAsync(w.U64.p, 0, total * sizeof(double), s));
   const bool learned = mg->opt.smoother == DEC_SMOOTH_LEARNED;
@@ -2684,7 +2728,7 @@ dec_status mg_solve(dec_mg* mg, double* u, const double* b, int nrhs, double rto
     nl += w.launches[kind];
     ++it;
   }
-  k_from_panels<double, double><<<grid_for((long long)n * nrhs, 256), 256, 0, s>>>(n, nrhs, K, F.diperm.p, w.U64.p, ud);
+  from_panels(n, nrhs, K, w.npanels, F.diperm.p, w.U64.p, ud, s);
   DEC_CHECK_LAUNCH();
   if (host_buffers) DEC_CUDA(cudaMemcpyAsync(u, ud, (size_t)n * nrhs * 8, cudaMemcpyDeviceToHost, s));
   DEC_CUDA(cudaEventRecord(e1, s));
@@ -3076,8 +3120,8 @@ dec_status batch_solve(dec_batch* b, double* const* u, const double* const* rhs,
     const Level& F = mg.lv[0];
     const int n = F.n, K = w.K, np = w.npanels;
     const size_t tot = (size_t)n * K * np;
-    k_to_panels<double, double><<<grid_for((long long)tot, 256), 256, 0, s>>>(n, nrhs[q], K, np, F.dperm.p, rhs[q], w.B64.p);
-    k_to_panels<double, double><<<grid_for((long long)tot, 256), 256, 0, s>>>(n, nrhs[q], K, np, F.dperm.p, u[q], w.U64.p);
+    to_panels(n, nrhs[q], K, np, F.diperm.p, rhs[q], w.B64.p, s);
+    to_panels(n, nrhs[q], K, np, F.diperm.p, u[q], w.U64.p, s);
     if (w.prec == 2) DEC_CUDA(cudaMemsetAsync(w.f16[0].x.p, 0, tot * sizeof(__half), s));
     else if (w.prec == 1) DEC_CUDA(cudaMemsetAsync(w.f32[0].x.p, 0, tot * sizeof(float), s));
     else DEC_CUDA(cudaMemsetAsync(w.f64[0].x.p, 0, tot * sizeof(double), s));
@@ -3136,8 +3180,7 @@ dec_status batch_solve(dec_batch* b, double* const* u, const double* const* rhs,
     dec_mg& mg = *b->groups[q];
     Workspace& w = *ws[q];
     const Level& F = mg.lv[0];
-    k_from_panels<double, double><<<grid_for((long long)F.n * nrhs[q], 256), 256, 0, s>>>(F.n, nrhs[q], w.K, F.diperm.p,
-                                                                                           w.U64.p, u[q]);
+    from_panels(F.n, nrhs[q], w.K, w.npanels, F.diperm.p, w.U64.p, u[q], s);
     ++nl;
   }
   DEC_CHECK_LAUNCH();
