@@ -217,8 +217,7 @@ template <class T>
 struct SweepPrm {
   int mode;
   int zero_x;   // x is known to be zero: A x is skipped
-  int write_d;  // Chebyshev: store the direction (not needed after the last sweep)
-  int d_is_x;   // Chebyshev: the direction equals x (first step from zero), so d is not read
+  int d_is_x;   // Chebyshev: the previous iterate is zero (second step from zero), so it is not read
   T omega;      // Jacobi
   T inv_theta;  // Chebyshev first step
   T c1, c2;     // Chebyshev recurrence
@@ -351,7 +350,10 @@ struct Lanes {
 //   S_RESID : out = r
 //   S_JACOBI: out = x + ω D⁻¹ r
 //   S_CHEB0 : d = D⁻¹ r / θ; out = x + d
-//   S_CHEBN : d = c1 d + c2 D⁻¹ r; out = x + d
+//   S_CHEBN : d = c1 (x - x_prev) + c2 D⁻¹ r; out = x + d, where x_prev, the iterate before x, is
+//             what out holds on entry: the last direction is recomputed from the two iterates
+//             (each row reads its own x_prev before writing over it), so no direction vector is
+//             stored, a vector write less per step than keeping d in its own buffer
 // SH: right-hand side j of panel p has its own operator A + cs[p*K + j] I (D likewise).
 // UPD: the sweep's result is the refinement step's correction e, added straight to the FP64
 // iterate (u += (double) e, the update pass's arithmetic) instead of being stored in out.
@@ -359,9 +361,9 @@ template <class T, int K, int W, bool SH, bool UPD = false>
 __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restrict__ col,
                                            const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
                                            const CT<T>* __restrict__ dinv, const T* __restrict__ b,
-                                           const T* __restrict__ x, T* __restrict__ out, T* __restrict__ d,
-                                           const SweepPrm<CT<T>>& prm, size_t pstride,
-                                           const CT<T>* __restrict__ shf, double* __restrict__ u64 = nullptr) {
+                                           const T* __restrict__ x, T* __restrict__ out, const SweepPrm<CT<T>>& prm,
+                                           size_t pstride, const CT<T>* __restrict__ shf,
+                                           double* __restrict__ u64 = nullptr) {
   using Ln = Lanes<T, K>;
   using C = CT<T>;
   pdl_enter();
@@ -437,21 +439,22 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
         dn[q] = (di[q] * r[q]) * prm.inv_theta;
         o[q] = xi[q] + dn[q];
       }
-      if (prm.write_d) stv<T, V>(d + ik, dn);
     } else {
       C dn[V];
       if (prm.d_is_x) {
 #pragma unroll
         for (int q = 0; q < V; ++q) dn[q] = xi[q];
       } else {
-        ldv<T, V>(d + ik, dn);
+        C xp[V];
+        ldv<T, V>(out + ik, xp);
+#pragma unroll
+        for (int q = 0; q < V; ++q) dn[q] = xi[q] - xp[q];
       }
 #pragma unroll
       for (int q = 0; q < V; ++q) {
         dn[q] = prm.c1 * dn[q] + prm.c2 * (di[q] * r[q]);
         o[q] = xi[q] + dn[q];
       }
-      if (prm.write_d) stv<T, V>(d + ik, dn);
     }
     if constexpr (UPD) {
 #pragma unroll
@@ -466,9 +469,9 @@ template <class T, int K, int W, bool SH>
 __global__ void __launch_bounds__(TB) k_sweep(int n, int Wr, const int32_t* __restrict__ col,
                                               const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
                                               const CT<T>* __restrict__ dinv, const T* __restrict__ b,
-                                              const T* __restrict__ x, T* __restrict__ out, T* __restrict__ d,
+                                              const T* __restrict__ x, T* __restrict__ out,
                                               SweepPrm<CT<T>> prm, size_t pstride, const CT<T>* __restrict__ shf) {
-  sweep_rows<T, K, W, SH>(n, Wr, col, off, diag, dinv, b, x, out, d, prm, pstride, shf);
+  sweep_rows<T, K, W, SH>(n, Wr, col, off, diag, dinv, b, x, out, prm, pstride, shf);
 }
 
 // The last sweep of a refinement step's V-cycles on the finest level with the step's update
@@ -477,10 +480,10 @@ template <class T, int K, int W, bool SH>
 __global__ void __launch_bounds__(TB) k_sweep_u(int n, int Wr, const int32_t* __restrict__ col,
                                                 const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
                                                 const CT<T>* __restrict__ dinv, const T* __restrict__ b,
-                                                const T* __restrict__ x, T* __restrict__ out, T* __restrict__ d,
+                                                const T* __restrict__ x, T* __restrict__ out,
                                                 SweepPrm<CT<T>> prm, size_t pstride, const CT<T>* __restrict__ shf,
                                                 double* __restrict__ u64) {
-  sweep_rows<T, K, W, SH, true>(n, Wr, col, off, diag, dinv, b, x, out, d, prm, pstride, shf, u64);
+  sweep_rows<T, K, W, SH, true>(n, Wr, col, off, diag, dinv, b, x, out, prm, pstride, shf, u64);
 }
 
 // FP16-stored sweeps carry eight values per 16-byte access; unbounded they took 72 registers
@@ -492,9 +495,9 @@ template <int K, int W, bool SH>
 __global__ void __launch_bounds__(TB, kSweepHalfBlocks) k_sweep_h(
     int n, int Wr, const int32_t* __restrict__ col, const float* __restrict__ off, const float* __restrict__ diag,
     const float* __restrict__ dinv, const __half* __restrict__ b, const __half* __restrict__ x,
-    __half* __restrict__ out, __half* __restrict__ d, SweepPrm<float> prm, size_t pstride,
+    __half* __restrict__ out, SweepPrm<float> prm, size_t pstride,
     const float* __restrict__ shf) {
-  sweep_rows<__half, K, W, SH>(n, Wr, col, off, diag, dinv, b, x, out, d, prm, pstride, shf);
+  sweep_rows<__half, K, W, SH>(n, Wr, col, off, diag, dinv, b, x, out, prm, pstride, shf);
 }
 
 // Restriction R = row-normalised S (make_restriction, Multigrid.jl:595-612):
@@ -1862,7 +1865,7 @@ static void launch_prolong(const Level& L, const Level& Cl, const T* z, T* x, bo
 }
 
 template <class T, int K>
-static void launch_sweep(const Level& L, const T* b, const T* x, T* out, T* d, SweepPrm<CT<T>> prm, int np,
+static void launch_sweep(const Level& L, const T* b, const T* x, T* out, SweepPrm<CT<T>> prm, int np,
                          cudaStream_t s, const CT<T>* cs, double* upd = nullptr) {
   size_t ps = (size_t)L.n * K;
   dim3 grid = row_grid<T, K>(L.n, np);
@@ -1872,12 +1875,12 @@ static void launch_sweep(const Level& L, const T* b, const T* x, T* out, T* d, S
     const float* dg = L.diag32.p;
     const float* di = L.dinv32.p;
     if (cs) {
-      if (L.W == 6) launch_pdl(k_sweep_h<K, 6, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
-      else launch_pdl(k_sweep_h<K, 0, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+      if (L.W == 6) launch_pdl(k_sweep_h<K, 6, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs);
+      else launch_pdl(k_sweep_h<K, 0, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs);
     } else if (L.W == 6) {
-      launch_pdl(k_sweep_h<K, 6, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+      launch_pdl(k_sweep_h<K, 6, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs);
     } else {
-      launch_pdl(k_sweep_h<K, 0, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+      launch_pdl(k_sweep_h<K, 0, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs);
     }
   } else {
     const CT<T>* off = pick<T>(L.off64, L.off32);
@@ -1885,7 +1888,7 @@ static void launch_sweep(const Level& L, const T* b, const T* x, T* out, T* d, S
     const CT<T>* di = pick<T>(L.dinv64, L.dinv32);
     if (upd) {  // u += (this sweep's result); out is not written
       auto go = [&](auto kern) {
-        launch_pdl(kern, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs, upd);
+        launch_pdl(kern, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs, upd);
       };
       if (cs) {
         if (L.W == 6) go(k_sweep_u<T, K, 6, true>);
@@ -1897,13 +1900,13 @@ static void launch_sweep(const Level& L, const T* b, const T* x, T* out, T* d, S
       }
     } else if (cs) {
       if (L.W == 6)
-        launch_pdl(k_sweep<T, K, 6, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+        launch_pdl(k_sweep<T, K, 6, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs);
       else
-        launch_pdl(k_sweep<T, K, 0, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+        launch_pdl(k_sweep<T, K, 0, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs);
     } else if (L.W == 6) {
-      launch_pdl(k_sweep<T, K, 6, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+      launch_pdl(k_sweep<T, K, 6, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs);
     } else {
-      launch_pdl(k_sweep<T, K, 0, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, d, prm, ps, cs);
+      launch_pdl(k_sweep<T, K, 0, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs);
     }
   }
 }
@@ -1923,7 +1926,7 @@ static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool z
       if (!zero_x) {
         SweepPrm<CT<T>> prm{};
         prm.mode = S_RESID;
-        launch_sweep<T, K>(L, B.b.p, x, B.d.p, nullptr, prm, np, s, B.cs);
+        launch_sweep<T, K>(L, B.b.p, x, B.d.p, prm, np, s, B.cs);
         r = B.d.p;
       }
       launch_mlp_smooth<T, K>(wts, L.n, L.W, L.col.p, L.mtab.p, pick<T>(L.diag64, L.diag32), r, x, zero_x ? 1 : 0,
@@ -1942,8 +1945,8 @@ static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool z
   for (int it = 0; it < sweeps; ++it) {
     SweepPrm<C> prm{};
     prm.zero_x = zero_x ? 1 : 0;
-    // the direction is needed only by a later sweep; after a first step from zero it equals x
-    prm.write_d = (it + 1 < sweeps) && !(it == 0 && started_at_zero) ? 1 : 0;
+    // step k reads x_{k-2} from the buffer it writes (x and other alternate); after a first step
+    // from zero that iterate is zero and the buffer holds nothing
     prm.d_is_x = (it == 1 && started_at_zero) ? 1 : 0;
     if (o.smoother == DEC_SMOOTH_JACOBI) {
       prm.mode = S_JACOBI;
@@ -1958,7 +1961,7 @@ static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool z
       prm.c2 = (C)(2 * rho_new / delta);
       rho = rho_new;
     }
-    launch_sweep<T, K>(L, B.b.p, x, other, B.d.p, prm, np, s, B.cs, it + 1 == sweeps ? upd : nullptr);
+    launch_sweep<T, K>(L, B.b.p, x, other, prm, np, s, B.cs, it + 1 == sweeps ? upd : nullptr);
     std::swap(x, other);
     zero_x = false;
   }
@@ -2029,7 +2032,7 @@ static double* cg_mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs
     double* rr = (x == B.x.p) ? B.y.p : B.x.p;
     SweepPrm<double> prm{};
     prm.mode = S_RESID;
-    launch_sweep<double, K>(L, B.b.p, x, rr, nullptr, prm, np, s, B.cs);
+    launch_sweep<double, K>(L, B.b.p, x, rr, prm, np, s, B.cs);
     r = rr;
   }
   const Level& Cl = mg.lv[l + 1];
@@ -2077,7 +2080,7 @@ static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bu
     T* rr = (x == B.x.p) ? B.y.p : B.x.p;
     SweepPrm<CT<T>> prm{};
     prm.mode = S_RESID;
-    launch_sweep<T, K>(L, B.b.p, x, rr, nullptr, prm, np, s, B.cs);
+    launch_sweep<T, K>(L, B.b.p, x, rr, prm, np, s, B.cs);
     r = rr;
   }
   const Level& Cl = mg.lv[l + 1];
@@ -2197,7 +2200,8 @@ static void enqueue_cycle(dec_mg& mg, Workspace& w, cudaStream_t s) {
 }
 
 // Vectors a smoothing sweep reads or writes once: Jacobi b, x, out; Chebyshev b, x, d (r/w), out.
-static int prm_vectors(int smoother) { return smoother == DEC_SMOOTH_JACOBI ? 3 : 5; }
+// vectors a timed sweep moves: b, x, out (+ the previous iterate in out for a Chebyshev step)
+static int prm_vectors(int smoother) { return smoother == DEC_SMOOTH_JACOBI ? 3 : 4; }
 
 // plain: learned-smoother fallback; G_STEP: V-cycles with the update fused into the last sweep,
 // then the residual (the refinement loops' step when fused_update holds)
@@ -2841,11 +2845,10 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
     if (kernel == DEC_KERNEL_SWEEP) {
       SweepPrm<CT<T>> prm{};
       prm.mode = mg.opt.smoother == DEC_SMOOTH_JACOBI ? S_JACOBI : S_CHEBN;
-      prm.write_d = 1;  // a middle Chebyshev step: reads and writes the direction
-      prm.omega = (CT<T>)mg.opt.omega;
+      prm.omega = (CT<T>)mg.opt.omega;  // a middle Chebyshev step: reads the previous iterate from out
       prm.c1 = (CT<T>)0.5;
       prm.c2 = (CT<T>)0.25;
-      launch_sweep<T, K>(L, B.b.p, B.x.p, B.y.p, B.d.p, prm, np, s, B.cs);
+      launch_sweep<T, K>(L, B.b.p, B.x.p, B.y.p, prm, np, s, B.cs);
     } else if (kernel == DEC_KERNEL_MLP) {
       if constexpr (!std::is_same<T, __half>::value)
         launch_mlp_smooth<T, K>(mlp_weights(mg.mlp), L.n, L.W, L.col.p, L.mtab.p, pick<T>(L.diag64, L.diag32),
