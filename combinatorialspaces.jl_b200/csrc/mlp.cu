@@ -264,6 +264,14 @@ __global__ void __launch_bounds__(kMlpThreads, 3) k_mlp_smooth(MlpWeights w, int
     T xv = T(0);
     if (q < nq) {
       const int i = (int)(q / K), k = (int)(q % K);
+      // every slot's index and residual are loaded without waiting for the valence (padding
+      // slots hold the row itself), then the slots past it are zeroed
+      int cj[6];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) cj[j] = j < W ? col[(size_t)i * W + j] : i;
+      float rv[6];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) rv[j] = (float)r[po + (size_t)cj[j] * K + k];
       const float4 t0 = tab[2 * (size_t)i], t1 = tab[2 * (size_t)i + 1];
       const int nn = __float2int_rn(t1.w * 6.0f);
       const float ri = (float)r[po + q];
@@ -271,7 +279,7 @@ __global__ void __launch_bounds__(kMlpThreads, 3) k_mlp_smooth(MlpWeights w, int
       float s = fabsf(ri);
 #pragma unroll
       for (int j = 0; j < 6; ++j) {
-        nb[j] = j < nn ? (float)r[po + (size_t)col[(size_t)i * W + j] * K + k] : 0.f;
+        nb[j] = j < nn ? rv[j] : 0.f;
         s = fmaxf(s, fabsf(nb[j]));
       }
       if (s == 0.0f) s = 1.0f;
@@ -637,6 +645,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mlp_smooth_tcg(MlpWeights w, 
     T xv = T(0);
     if (q < nq) {
       const int i = (int)(q / K), k = (int)(q % K);
+      // every slot's index and residual are loaded without waiting for the valence (padding
+      // slots hold the row itself), then the slots past it are zeroed
+      int cj[6];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) cj[j] = j < W ? col[(size_t)i * W + j] : i;
+      float rv[6];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) rv[j] = (float)r[po + (size_t)cj[j] * K + k];
       const float4 t0 = tab[2 * (size_t)i], t1 = tab[2 * (size_t)i + 1];
       const int nn = __float2int_rn(t1.w * 6.0f);
       const float ri = (float)r[po + q];
@@ -644,7 +660,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mlp_smooth_tcg(MlpWeights w, 
       float s = fabsf(ri);
 #pragma unroll
       for (int j = 0; j < 6; ++j) {
-        nb[j] = j < nn ? (float)r[po + (size_t)col[(size_t)i * W + j] * K + k] : 0.f;
+        nb[j] = j < nn ? rv[j] : 0.f;
         s = fmaxf(s, fabsf(nb[j]));
       }
       if (s == 0.0f) s = 1.0f;
