@@ -379,6 +379,51 @@ def dist_env():
 
 
 # ------------------------------------------------------------------------------------------
+# Ranks: one process per GPU, each solving its own right-hand sides (replicas, no data-path
+# collective); the process group carries only the barrier and the max-over-ranks timing.
+# ------------------------------------------------------------------------------------------
+def init_dist(world, backend="nccl", timeout_s=300):
+    """The process group of a world > 1 run (rendezvous from MASTER_ADDR / MASTER_PORT), with a
+    short timeout so that ranks waiting on a dead one end with an error."""
+    if world <= 1:
+        return
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+
+
+def rank_seeds(rank, nrhs=NRHS):
+    """The right-hand-side seeds of a rank: rank r solves seeds 2 + r·nrhs .. 1 + (r+1)·nrhs."""
+    return [2 + j + nrhs * rank for j in range(nrhs)]
+
+
+def collectives(world, device):
+    """(barrier, max_over_ranks) for a world of `world` ranks; max_over_ranks reduces a float on
+    `device` ("cuda" under NCCL, "cpu" under gloo).  Identity functions for one rank."""
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world > 1:
+            import torch
+            import torch.distributed as dist
+            t = torch.tensor([x], dtype=torch.float64, device=device)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    return barrier, max_over_ranks
+
+
+def whole_job_rate(nrhs, world, steps, seconds):
+    """Solves per second of the whole job: every rank's right-hand sides over the slowest rank's
+    time (seconds is already the max over ranks)."""
+    return nrhs * world * steps / seconds
+
+
+# ------------------------------------------------------------------------------------------
 # CPU baseline (the oracle, on the host cores)
 # ------------------------------------------------------------------------------------------
 def cpu_reference_solve(O, md, A, b, budget_s=30.0):
@@ -454,12 +499,8 @@ def run_reference(args):
 def run_ours(args):
     import torch
     world, rank, local = dist_env()
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
+    init_dist(world, "nccl")
     dec = load_package()
     ico = dec.meshes.icosahedron()
     t_setup = time.perf_counter()
@@ -472,7 +513,7 @@ def run_ours(args):
     mg64 = dec.MultigridData(ico, LEVEL, precision=0, **common)
     setup_s = time.perf_counter() - t_setup
     n = mg.level_info(0)[0]
-    seeds = [2 + j + NRHS * rank for j in range(NRHS)]
+    seeds = rank_seeds(rank)
     B = torch.tensor(np.stack([dec.meshes.uniform(s, n) for s in seeds]), device="cuda")
     U = torch.zeros_like(B)
     tuned = mg.autotune(NRHS, reps=3) if args.rhs_block == 0 else args.rhs_block
@@ -480,18 +521,7 @@ def run_ours(args):
         mg64.autotune(NRHS, reps=3)
     stream = torch.cuda.current_stream()
 
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([x], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return x
+    barrier, max_over_ranks = collectives(world, "cuda")
 
     def timed(fn, steps, warmup):
         for _ in range(warmup):
@@ -533,12 +563,12 @@ def run_ours(args):
     clocks["window"] = "0.6 s of the same solves before and after the timed region, and the timed region"
     if args.profile:
         if rank == 0:
-            print(json.dumps({"profile_run": True, "solves_per_s": NRHS * world * args.steps / t_ours,
+            print(json.dumps({"profile_run": True, "solves_per_s": whole_job_rate(NRHS, world, args.steps, t_ours),
                               "v_cycles": int(reps[-1].iterations), "rhs_block": int(tuned)}), flush=True)
         return
     rep0 = reps[-1]
     converged = all(r.converged for r in reps)
-    value = NRHS * world * args.steps / t_ours
+    value = whole_job_rate(NRHS, world, args.steps, t_ours)
     launches = int(sum(r.launches for r in reps))
 
     # --- error against an FP64-only solve (GPU, FP64 V-cycles to 1e-12) ---
@@ -561,7 +591,7 @@ def run_ours(args):
         t_plain, reps64 = timed(solve64, max(1, args.steps), 1)
         o = m64.options
         cheb64.append({"cycle": f"V({o.pre},{o.post}) ratio {o.cheb_ratio:g}, {o.inner_cycles} per step",
-                       "solves_per_s": NRHS * world * max(1, args.steps) / t_plain,
+                       "solves_per_s": whole_job_rate(NRHS, world, max(1, args.steps), t_plain),
                        "refinement_steps": int(reps64[-1].iterations)})
         if cfg:
             del m64
@@ -582,7 +612,7 @@ def run_ours(args):
         return mgcg.solve(Ucg, B, rtol=RTOL, max_iters=100, use_initial_guess=False)[1]
 
     t_cg, reps_cg = timed(solve_cg, max(1, args.steps), 1)
-    cg64_value = NRHS * world * max(1, args.steps) / t_cg
+    cg64_value = whole_job_rate(NRHS, world, max(1, args.steps), t_cg)
     assert reps_cg[-1].converged == 1
     del mgcg, Ucg
     torch.cuda.empty_cache()
@@ -611,7 +641,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(time.perf_counter() - t0)
     assert all(r.converged == 1 for r in e2e_reps)
-    e2e_value = NRHS * world * args.steps / t_e2e
+    e2e_value = whole_job_rate(NRHS, world, args.steps, t_e2e)
     bytes_vec = NRHS * n * 8
 
     # --- roofline of the dominant kernel (the finest-level smoothing sweep), timed alone ---
