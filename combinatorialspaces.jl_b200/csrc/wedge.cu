@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(kThreads) k_w02(int nt, const int32_t* __restr
 
 // wedge_kernel_11!, FastDEC.jl:184-191.
 template <class T>
-__global__ void __launch_bounds__(kThreads) k_w11(int nt, const int32_t* __restrict__ te0,
+__global__ void __launch_bounds__(kThreads, 4) k_w11(int nt, const int32_t* __restrict__ te0,
                                                   const int32_t* __restrict__ te1, const int32_t* __restrict__ te2,
                                                   const T* __restrict__ c0, const T* __restrict__ c1,
                                                   const T* __restrict__ c2, const T* __restrict__ a,
