@@ -441,7 +441,7 @@ def cpu_reference_solve(O, md, A, b, budget_s=30.0):
         rel = np.linalg.norm(b - A @ u) / nb
         if rel <= RTOL or time.perf_counter() - t0 > budget_s or cycles >= 50:
             break
-    return time.perf_counter() - t0, cycles, rel, rel <= RTOL
+    return time.perf_counter() - t0, cycles, float(rel), bool(rel <= RTOL)
 
 
 def build_cpu_reference(threads):
