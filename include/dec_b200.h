@@ -248,9 +248,9 @@ dec_status dec_mg_full_multigrid(dec_mg* mg, double* u, const double* b, int32_t
 dec_status dec_mg_solve(dec_mg* mg, double* u, const double* b, int32_t nrhs, double rtol,
                         int32_t max_iters, dec_solve_report* report, void* stream);
 /* dec_mg_solve from u = 0 (multigrid_vcycles(zeros(n), b, md, cycles), src/Multigrid.jl:814, as the
- * refined solve): u is output only and
- * is not read.  The first refinement step's residual is b itself, so it costs one pass over b
- * instead of the FP64 update and residual passes (the same iterates bit for bit). */
+ * refined solve): u is output only and is not read.  The first refinement step's residual is b
+ * itself, so it costs one pass over b instead of the FP64 update and residual passes (the same
+ * iterates bit for bit). */
 dec_status dec_mg_solve_from_zero(dec_mg* mg, double* u, const double* b, int32_t nrhs, double rtol,
                                   int32_t max_iters, dec_solve_report* report, void* stream);
 /* Same solve with host u / b (pinned or pageable); copies are part of the call.  With
