@@ -194,8 +194,8 @@ def measure_operators(dec, peak):
         del g
         torch.cuda.empty_cache()
 
-    # 128 x 128 grid, barycentric duals, FP64, 100 repetitions each
-    # (L2-resident: µs per operation, not an HBM figure).
+    # The plain-operator workload: the 128 x 128 grid, barycentric duals, FP64, 100 repetitions of
+    # each operation (L2-resident: µs per operation, not an HBM figure).
     m = dec.meshes.triangulated_grid(127, 127, 1.0, 1.0, False)
     g = dec.Mesh(m.points, m.ev0, m.ev1, m.te0, m.te1, m.te2, m.edge_orientation, m.tri_orientation,
                  center="barycenter")
@@ -206,7 +206,7 @@ def measure_operators(dec, peak):
                      dec.dec_wedge_product(0, 2, g))
     d1, L = dec.dec_differential(1, g), dec.laplace_beltrami(g)
     d1a = torch.empty(g.nt, dtype=torch.float64, device="cuda")
-    cfg1 = {}
+    grid_ops = {}
     for name, fn in (("wedge01(f,alpha)", lambda: w01(f, al)), ("wedge11(alpha,beta)", lambda: w11(al, be)),
                      ("wedge02(f,d1 alpha)", lambda: w02(f, d1.apply(al, d1a))), ("laplacian f", lambda: L.apply(f))):
         fn()
@@ -218,8 +218,8 @@ def measure_operators(dec, peak):
             fn()
         e1.record()
         torch.cuda.synchronize()
-        cfg1[name] = round(e0.elapsed_time(e1) * 10, 2)  # µs per op (ms / 100 * 1000)
-    out["grid_128x128_config1_us_per_op"] = cfg1
+        grid_ops[name] = round(e0.elapsed_time(e1) * 10, 2)  # µs per op (ms / 100 * 1000)
+    out["grid_128x128_us_per_op"] = grid_ops
     return out
 
 
