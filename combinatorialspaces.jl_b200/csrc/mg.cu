@@ -1836,13 +1836,27 @@ static dim3 row_grid(int n, int np) {
   return dim3(grid_for((long long)n, Lanes<T, K>::RPB, 8), np);
 }
 
+// CTAs of k_restrict<T, K, WQ> resident per SM (queried once): its grid stays within one wave, so
+// no partial second wave of grid-stride CTAs trails the rest.
+template <class T, int K, int WQ>
+static int restrict_ctas() {
+  static const int ctas = [] {
+    int o = 0;
+    DEC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_restrict<T, K, WQ>, TB, 0));
+    return std::max(1, o);
+  }();
+  return ctas;
+}
+
 // R r_f into the coarse level's panels; the unrolled kernel where a coarse vertex has at most six
 // midpoints (every level of the refined icosphere and of the triangulated grids).
 template <class T, int K>
 static void launch_restrict(const Level& L, const Level& Cl, const T* r, T* bc, int np, cudaStream_t s,
                             bool pdl = true) {
   auto kern = L.Wq == 6 ? k_restrict<T, K, 6> : k_restrict<T, K>;
-  const dim3 g = row_grid<T, K>(Cl.n, np);
+  dim3 g = row_grid<T, K>(Cl.n, np);
+  const int ctas = L.Wq == 6 ? restrict_ctas<T, K, 6>() : restrict_ctas<T, K, 0>();
+  g.x = std::min<unsigned>(g.x, (unsigned)(ctas * num_sms()));
   const size_t fs = (size_t)L.n * K, cs = (size_t)Cl.n * K;
   if (pdl)
     launch_pdl(kern, g, dim3(TB), s, L.nc, L.Wq, (const int32_t*)L.rself.p, (const int32_t*)L.ridx.p,
