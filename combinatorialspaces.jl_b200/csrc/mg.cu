@@ -1254,7 +1254,7 @@ struct Level {
 
 template <class T>
 struct LevelBufs {
-  DArr<T> x, y, b, d;  // x / y ping-pong, b right-hand side, d Chebyshev direction
+  DArr<T> x, y, b, d;  // x / y ping-pong, b right-hand side, d the learned sweep's residual / CG direction
   DArr<T> q, e;        // CG smoother: A p and the accumulated correction Δx (CG mode only)
   const CT<T>* cs = nullptr;  // per-RHS shifts (coarse_solver 2), K * npanels, shared by all levels
 };
@@ -2421,6 +2421,8 @@ static void enqueue_first_rhs(const dec_mg& mg, Workspace& w, cudaStream_t s) {
 //   ||b||²; e = 0; [u += e; r = b - A u; test]; WHILE (test): { e = V^c(r); u += e; r = b - A u; test }
 // The test (k_ir_check) sets the WHILE node's condition, so the solve needs no host round trip.
 // zero_guess (u = 0; FP32 / FP64 V-cycles): the bracketed first step is r = b with its norms.
+// When the step ends in a Jacobi / Chebyshev post-sweep (fused_update), the body's u += e is that
+// sweep's epilogue (G_STEP) instead of a pass of its own.
 static void capture_solve(dec_mg& mg, Workspace& w, bool zero_guess) {
   if (w.bn2.n < (size_t)w.K * w.npanels) w.bn2.alloc((size_t)w.K * w.npanels);
   if (!w.loop.p) w.loop.alloc(1);
