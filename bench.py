@@ -254,7 +254,8 @@ def measure_learned(dec, args, B, U64, common, timed):
 
         t, reps = timed(solve, max(1, args.steps), 1)
         rep = reps[-1]
-        res = {"solves_per_s": Bm.shape[0] * max(1, args.steps) / t, "v_cycles_per_solve": int(rep.iterations),
+        res = {"solves_per_s": Bm.shape[0] * max(1, args.steps) / t, "refinement_steps": int(rep.iterations),
+               "v_cycles_per_solve": int(rep.iterations) * opts.get("inner_cycles", common["inner_cycles"]),
                "converged": bool(rep.converged), "fallback_iteration": int(rep.fallback_iteration),
                "sweeps": sweeps}
         if smoother == 3:
@@ -367,6 +368,127 @@ def measure_batched(dec, args):
     res["wedge11_L7_fp32_x1024"] = {"ms": 1e3 * tw, "wedges_per_s": count / tw, "GB/s": by / tw / 1e9,
                                     "bytes": by}
     del a, b, out
+    torch.cuda.empty_cache()
+    return res
+
+
+def oracle_hierarchy(level, threads):
+    """The oracle's icosphere hierarchy of `level` binary subdivisions (checker only: the errors the
+    GPU results are stated against)."""
+    sys.path.insert(0, str(ROOT))
+    import oracle
+    O = oracle.load()
+    O.set_num_threads(threads)
+    return oracle, O, O.build_mg(O.icosahedron(), level, O.CIRCUMCENTER, SHIFT, 1.0, 3)
+
+
+def measure_config2(dec, args):
+    """Plain FP64 multigrid on icosphere L6 (40,962 vertices): (L + I) u = b, b uniform[-1,1] with
+    seed 1, V(3,3) Chebyshev-Jacobi cycles with a dense direct solve on L0 (12 vertices), to 1e-10
+    relative residual.  GPU: the device refinement loop (FP64 V-cycles), one right-hand side and the
+    32-RHS batch; the error is against the oracle's FP64 solve to 1e-13; the CPU figure is the same
+    V-cycle in the oracle on all host threads."""
+    import torch
+    ico = dec.meshes.icosahedron()
+    mg = dec.MultigridData(ico, 6, shift=SHIFT, center="circumcenter", project_radius=1.0, precision=0,
+                           smoother=1, pre=3, post=3, cheb_ratio=4.0, coarse_solver=0, coarse_max=0)
+    n = mg.n
+    b = torch.tensor(dec.meshes.uniform(1, n), device="cuda")
+    U = torch.zeros_like(b)
+    steps = max(3, args.steps)
+
+    def rate(Bm):
+        Um = torch.zeros_like(Bm)
+        for _ in range(3):
+            mg.solve(Um, Bm, rtol=1e-10, max_iters=60, use_initial_guess=False)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        reps = [mg.solve(Um, Bm, rtol=1e-10, max_iters=60, use_initial_guess=False)[1] for _ in range(steps)]
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / steps
+        nr = 1 if Bm.dim() == 1 else Bm.shape[0]
+        return Um, reps[-1], t, nr
+
+    U, rep, t1, _ = rate(b)
+    B32 = torch.tensor(np.stack([dec.meshes.uniform(1 + j, n) for j in range(NRHS)]), device="cuda")
+    _, rep32, t32, _ = rate(B32)
+    res = {"vertices": n, "cycle": "V(3,3) Chebyshev-Jacobi [λ/4, λ], dense FP64 solve on L0 (12 vertices)",
+           "refinement_steps": int(rep.iterations), "v_cycles": int(rep.iterations),
+           "max_rel_residual": rep.max_rel_residual, "converged": bool(rep.converged),
+           "ms_per_solve_1rhs": 1e3 * t1, "solves_per_s_1rhs": 1.0 / t1,
+           "solves_per_s_32rhs": NRHS / t32, "ms_per_32rhs": 1e3 * t32,
+           "bytes_per_solve_1rhs": mg.solve_traffic(1, int(rep.iterations))}
+    if not args.no_cpu:
+        threads = os.cpu_count() or 1
+        oracle, O, md = oracle_hierarchy(6, threads)
+        bh = b.cpu().numpy()
+        ue, rel, cyc, lmax = oracle.fp64_solve(md, bh, rtol=1e-13)
+        u = U.cpu().numpy()
+        res["rel_error_vs_fp64_oracle_solve"] = float(np.linalg.norm(u - ue) / np.linalg.norm(ue))
+        res["oracle_solve"] = f"{cyc} oracle V(3,3) cycles to {rel:.1e}"
+        # the same V-cycle on the host cores (the oracle), to 1e-10
+        import scipy.sparse as sp
+        cp, rv, nz, shape = md.op(0)
+        A = sp.csc_matrix((nz, rv, cp), shape=shape).tocsr()
+        t0 = time.perf_counter()
+        uc, c = np.zeros(n), 0
+        while c < 40:
+            uc = O.plain_vcycles(md, uc, bh, 1, 1, 3, 3, 0.8, 4.0, lmax)
+            c += 1
+            if np.linalg.norm(bh - A @ uc) / np.linalg.norm(bh) <= 1e-10:
+                break
+        tc = time.perf_counter() - t0
+        res["cpu_same_cycle"] = {"seconds_per_solve": tc, "v_cycles": c, "threads": threads,
+                                 "kind": "port (oracle V(3,3) FP64, residual checks included)"}
+    del mg
+    torch.cuda.empty_cache()
+    return res
+
+
+def measure_config3(dec, args, common):
+    """Mixed precision at L8 to 1e-10: 32 right-hand sides (seeds 2..33), FP32 V-cycles (the
+    headline cycle) inside FP64 iterative refinement; errors against the oracle's FP64-only solve
+    (to 1e-13 on the host, for the first `args.oracle_rhs` right-hand sides)."""
+    import torch
+    ico = dec.meshes.icosahedron()
+    mg = dec.MultigridData(ico, LEVEL, precision=1, **common)
+    if args.rhs_block == 0:
+        mg.autotune(NRHS, reps=2)
+    n = mg.n
+    B = torch.tensor(np.stack([dec.meshes.uniform(s, n) for s in range(2, 2 + NRHS)]), device="cuda")
+    U = torch.zeros_like(B)
+    steps = max(1, args.steps)
+    for _ in range(max(1, args.warmup)):
+        mg.solve(U, B, rtol=1e-10, max_iters=60, use_initial_guess=False)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    reps = [mg.solve(U, B, rtol=1e-10, max_iters=60, use_initial_guess=False)[1] for _ in range(steps)]
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / steps
+    rep = reps[-1]
+    res = {"rtol": 1e-10, "solves_per_s": NRHS / t, "ms_per_32rhs": 1e3 * t,
+           "refinement_steps": int(rep.iterations), "v_cycles": int(rep.iterations) * common["inner_cycles"],
+           "converged": bool(rep.converged), "max_rel_residual": rep.max_rel_residual,
+           "bytes_per_step": mg.solve_traffic(NRHS, int(rep.iterations))}
+    if not args.no_cpu and args.oracle_rhs > 0:
+        threads = os.cpu_count() or 1
+        oracle, O, md = oracle_hierarchy(LEVEL, threads)
+        lmax = [oracle.level_lmax(md, l) for l in range(md.nlevels)]
+        Bh, Uh = B.cpu().numpy(), U.cpu().numpy()
+        errs, t0 = [], time.perf_counter()
+        for j in range(min(NRHS, args.oracle_rhs)):
+            ue, rel, _, _ = oracle.fp64_solve(md, Bh[j], rtol=1e-13, lmax=lmax)
+            errs.append(float(np.linalg.norm(Uh[j] - ue) / np.linalg.norm(ue)))
+        res["max_rel_error_vs_fp64_oracle_solve"] = max(errs)
+        res["oracle_rhs_checked"] = len(errs)
+        res["oracle_seconds"] = time.perf_counter() - t0
+    del mg, B, U
     torch.cuda.empty_cache()
     return res
 
@@ -650,6 +772,14 @@ def run_ours(args):
     achieved = algo_bytes / (ms * 1e-3) / 1e9
     traffic = traffic_per_launch("k_sweep")
 
+    # --- the whole step's algorithmic bytes (every kernel of the solve graph) against its time ---
+    step_bytes = mg.solve_traffic(NRHS, int(rep0.iterations))
+    step_gbs = step_bytes / (t_ours / args.steps) / 1e9
+
+    # --- config 2 (L6 FP64 to 1e-10) and config 3 (L8 mixed precision to 1e-10) ---
+    config2 = measure_config2(dec, args) if (rank == 0 and not args.no_configs) else None
+    config3 = measure_config3(dec, args, common) if (rank == 0 and not args.no_configs) else None
+
     # --- batched uneven workload (512 solves over 8 meshes, one graph per step) ---
     batched = measure_batched(dec, args) if (rank == 0 and not args.no_batch) else None
 
@@ -669,6 +799,15 @@ def run_ours(args):
                "sample": f"1 right-hand side (seed 2) of the L8 workload: {c} reference V-cycles "
                          f"(Krylov CG smoother, FP64) to {rel:.2e} in {t:.2f} s on {threads} host threads"}
 
+    learned_ratio = None
+    if learned_res:
+        cands = [(k, c, r) for k in ("L8_learned_fp32", "L8_learned_fp32_mma_sync") for c, r in learned_res[k].items()
+                 if r["converged"]]
+        if cands:
+            k, c, r = max(cands, key=lambda x: x[2]["solves_per_s"])
+            learned_ratio = {"value": r["solves_per_s"] / plain_value, "learned_solves_per_s": r["solves_per_s"],
+                             "plain_fp64_solves_per_s": plain_value, "learned_cycle": f"{k} {c}",
+                             "fallback_iteration": r["fallback_iteration"], "target": 3.0}
     if rank == 0:
         line = {
             "metric": "icosphere-L8 Helmholtz solves/s to 1e-8 relative residual",
@@ -683,13 +822,15 @@ def run_ours(args):
                           f"{args.inner_cycles} per "
                           "FP64 iterative-refinement step, dense FP64 solve on the coarsest level used "
                           f"(coarse_max {args.coarse_max}), locality-ordered levels",
-                "rhs_panel_width": int(tuned), "v_cycles_per_solve": int(rep0.iterations),
+                "rhs_panel_width": int(tuned), "refinement_steps": int(rep0.iterations),
+                "v_cycles_per_solve": int(rep0.iterations) * args.inner_cycles,
                 "converged": converged, "max_rel_residual": rep0.max_rel_residual,
                 "max_rel_error_vs_fp64_solve": err,
                 "l2": "inputs larger than L2 (b: 168 MB FP64 per step)",
                 "parallelism": f"replicas x{world} (independent batches, no collective)",
                 "setup_seconds": setup_s,
             },
+            "learned_fp32_vs_plain_fp64": learned_ratio,
             "comparison": {"plain_fp64_vcycle_solves_per_s": plain_value,
                            "speedup_vs_plain_fp64": value / plain_value,
                            "plain_fp64_chebyshev": best64,
@@ -701,7 +842,9 @@ def run_ours(args):
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": f"k_sweep<float,{int(tuned)},6> finest level",
                          "algorithmic_bytes_per_launch": algo_bytes, "ms_per_launch": ms,
-                         "peak_kind": f"{peak_kind} (HBM copy, burst)"},
+                         "peak_kind": f"{peak_kind} (HBM copy, burst)",
+                         "step_algorithmic_bytes": step_bytes, "step_GB/s": step_gbs,
+                         "step_frac": step_gbs / peak},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": bytes_vec,
                     "d2h_bytes_per_step": bytes_vec,
@@ -711,6 +854,8 @@ def run_ours(args):
             "clocks": clocks,
             "operators": operators,
             "learned_smoother": learned_res,
+            "config2_L6_fp64": config2,
+            "config3_L8_mixed_1e-10": config3,
             "batched": batched,
         }
         print(json.dumps(line), flush=True)
@@ -820,6 +965,11 @@ def main():
                     help="time one DEC operator kernel alone (steps launches after warmup) and exit")
     ap.add_argument("--dtype", default="float64", choices=["float64", "float32"])
     ap.add_argument("--no-batch", action="store_true", dest="no_batch", help="skip the batched-workload section")
+    ap.add_argument("--no-configs", action="store_true", dest="no_configs",
+                    help="skip the L6 FP64 and L8 1e-10 sections")
+    ap.add_argument("--oracle-rhs", type=int, default=8, dest="oracle_rhs",
+                    help="right-hand sides of the L8 1e-10 section whose error is checked against the oracle's "
+                         "FP64 solve on the host")
     ap.add_argument("--mlp-engine", default="tcgen05", choices=["mma", "tcgen05"], dest="mlp_engine",
                     help="kernel engine of the learned smoothing step for --kernel mlp")
     ap.add_argument("--train-steps", type=int, default=20000, dest="train_steps",

@@ -515,6 +515,13 @@ class MultigridData:
         check(lib().dec_mg_autotune(self._h, nrhs, reps, _stream(), C.byref(k)))
         return k.value
 
+    def solve_traffic(self, nrhs, iterations, from_zero=True):
+        """Algorithmic bytes of a device-loop solve of `nrhs` right-hand sides that ran `iterations`
+        refinement steps (dec_mg_solve_traffic)."""
+        by = C.c_double()
+        check(lib().dec_mg_solve_traffic(self._h, nrhs, 1 if from_zero else 0, iterations, C.byref(by)))
+        return by.value
+
     def set_smoother_mlp(self, mlp):
         """Attach the learned smoother network used by smoother=DEC_SMOOTH_LEARNED (None detaches)."""
         check(lib().dec_mg_set_smoother_mlp(self._h, None if mlp is None else mlp._h))

@@ -279,6 +279,13 @@ dec_status dec_mg_time_kernel(dec_mg* mg, int32_t kernel, int32_t level, int32_t
   return guard([&] { decb::mg_time_kernel(mg, kernel, level, nrhs, reps, stream, ms, bytes); });
 }
 
+dec_status dec_mg_solve_traffic(dec_mg* mg, int32_t nrhs, int32_t from_zero, int32_t iterations, double* bytes) {
+  return guard([&] {
+    double b = decb::mg_solve_traffic(mg, nrhs, from_zero, iterations);
+    if (bytes) *bytes = b;
+  });
+}
+
 dec_status dec_mg_autotune(dec_mg* mg, int32_t nrhs, int32_t reps, void* stream, int32_t* rhs_block) {
   return guard([&] {
     int k = decb::mg_autotune(mg, nrhs, reps, stream);

@@ -337,6 +337,14 @@ template <class T> __device__ __forceinline__ T from_d(double v) { return (T)v; 
 template <> __device__ __forceinline__ __half from_d<__half>(double v) { return __float2half_rn((float)v); }
 
 // Lanes per row: each lane moves one 16-byte vector (or the whole row when K is smaller).
+// Algorithmic bytes of the kernels enqueued while a solve graph is captured (every streamed array
+// read or written once, each gathered vector once, int32 indices; reduction partials of under a
+// megabyte are not counted).  Set only around a capture, on the capturing thread.
+static thread_local double* t_bytes = nullptr;
+static inline void add_bytes(double b) {
+  if (t_bytes) *t_bytes += b;
+}
+
 template <class T, int K>
 struct Lanes {
   static constexpr int V = std::is_same<T, float>::value    ? (K >= 4 ? 4 : K)
@@ -1276,6 +1284,7 @@ struct Workspace {
   // the whole refinement loop (Jacobi / Chebyshev): [0] from a given initial guess, [1] from zero
   cudaGraphExec_t solve_graph[2] = {nullptr, nullptr};
   int64_t solve_pre[2] = {0, 0}, solve_body = 0;  // kernel nodes before / inside its loop
+  double solve_pre_bytes[2] = {0.0, 0.0}, solve_body_bytes = 0.0;  // their algorithmic bytes
   int nblocks = 0;
   DArr<double> Ubak;          // learned smoother: the iterate before a refinement step
   DArr<double> cs64;          // coarse_solver 2: per-RHS total shifts (K * npanels)
@@ -1858,6 +1867,7 @@ static void launch_restrict(const Level& L, const Level& Cl, const T* r, T* bc, 
   const int ctas = L.Wq == 6 ? restrict_ctas<T, K, 6>() : restrict_ctas<T, K, 0>();
   g.x = std::min<unsigned>(g.x, (unsigned)(ctas * num_sms()));
   const size_t fs = (size_t)L.n * K, cs = (size_t)Cl.n * K;
+  add_bytes((double)Cl.n * ((L.Wq + 1) * 4.0 + 8) + (double)(fs + cs) * np * sizeof(T));
   if (pdl)
     launch_pdl(kern, g, dim3(TB), s, L.nc, L.Wq, (const int32_t*)L.rself.p, (const int32_t*)L.ridx.p,
                (const double*)L.rs.p, r, bc, fs, cs);
@@ -1872,6 +1882,7 @@ static void launch_prolong(const Level& L, const Level& Cl, const T* z, T* x, bo
   auto kern = assign ? k_prolong<T, K, true> : k_prolong<T, K, false>;
   const dim3 g = row_grid<T, K>(L.n, np);
   const size_t fs = (size_t)L.n * K, cs = (size_t)Cl.n * K;
+  add_bytes((double)L.n * 8.0 + (double)(cs + (assign ? 1 : 2) * fs) * np * sizeof(T));
   if (pdl)
     launch_pdl(kern, g, dim3(TB), s, L.n, (const int32_t*)L.pa.p, (const int32_t*)L.pb.p, z, x, fs, cs);
   else
@@ -1883,6 +1894,15 @@ static void launch_sweep(const Level& L, const T* b, const T* x, T* out, SweepPr
                          cudaStream_t s, const CT<T>* cs, double* upd = nullptr) {
   size_t ps = (size_t)L.n * K;
   dim3 grid = row_grid<T, K>(L.n, np);
+  {
+    const double c = sizeof(CT<T>), v = (double)ps * np * sizeof(T);
+    double by = v;                                                       // b
+    if (!prm.zero_x) by += (double)L.n * (L.W * (4.0 + c) + c) + v;      // operator row, x
+    if (prm.mode != S_RESID && !cs) by += (double)L.n * c;               // 1/diagonal
+    if (prm.mode == S_CHEBN && !prm.d_is_x) by += v;                     // previous iterate
+    by += upd ? 2.0 * (double)ps * np * sizeof(double) : v;              // out, or u read + written
+    add_bytes(by);
+  }
   if constexpr (std::is_same<T, __half>::value) {
     grid.x = std::min<unsigned>(grid.x, (unsigned)(kSweepHalfBlocks * num_sms()));
     const float* off = L.off32.p;
@@ -1943,6 +1963,8 @@ static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool z
         launch_sweep<T, K>(L, B.b.p, x, B.d.p, prm, np, s, B.cs);
         r = B.d.p;
       }
+      add_bytes((double)L.n * (L.W * 4.0 + 32.0 + sizeof(CT<T>)) +
+                (double)L.n * K * np * sizeof(T) * (zero_x ? 2.0 : 3.0));  // indices, couplings, diag; r, x, out
       launch_mlp_smooth<T, K>(wts, L.n, L.W, L.col.p, L.mtab.p, pick<T>(L.diag64, L.diag32), r, x, zero_x ? 1 : 0,
                               other, np, s);
       std::swap(x, other);
@@ -2074,12 +2096,14 @@ static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bu
       return smooth<T, K>(mg, L, B, x, zero_x, std::max(1, mg.opt.pre + mg.opt.post), np, s);
     if (mg.opt.coarse_solver == 2) {  // per-RHS shifted solve through the eigendecomposition
       const dim3 g(grid_for(L.n, TB / K, 64), np);
+      add_bytes(2.0 * (double)L.n * L.n * 8.0 + (double)L.n * K * np * (2.0 * sizeof(T) + 16.0));
       launch_pdl(k_coarse_eig1<T, K>, g, dim3(TB), s, L.n, (const double*)mg.eigF.p, (const double*)mg.eigL.p,
                  (const double*)w.cs64.p, (const T*)B.b.p, w.ceig.p, (size_t)L.n * K);
       launch_pdl(k_coarse_eig2<T, K>, g, dim3(TB), s, L.n, (const double*)mg.eigE.p, (const double*)w.ceig.p, B.x.p,
                  (size_t)L.n * K);
       return B.x.p;
     }
+    add_bytes((double)L.n * L.n * 8.0 + 2.0 * (double)L.n * K * np * sizeof(T));
     launch_pdl(k_coarse<T, K>, dim3(grid_for(L.n, 1, 8), np), dim3(TB), s, L.n, (const double*)mg.ainv.p,
                (const T*)B.b.p, B.x.p, (size_t)L.n * K);
     return B.x.p;
@@ -2153,17 +2177,21 @@ static void enqueue_resid_T(dec_mg& mg, Workspace& w, cudaStream_t s, std::vecto
   using R = typename std::conditional<H, float, T>::type;  // the residual kernel's output type
   R* rout;
   if constexpr (H) {
+    add_bytes((double)total * (sizeof(__half) + 16.0));
     launch_pdl(k_axpy_scaled<K>, dim3(grid_for((long long)total, 256)), dim3(256), s, total, (size_t)F.n * K,
                (const __half*)bufs[0].x.p, (const double*)w.escale.p, w.U64.p);
     rout = w.r32.p;
   } else {
-    if (!updated)  // else the V-cycles' last sweep added e to u already
+    if (!updated) {  // else the V-cycles' last sweep added e to u already
+      add_bytes((double)total * (sizeof(T) + 16.0));
       launch_pdl(k_axpy_update<T>, dim3(grid_for((long long)total, 256)), dim3(256), s, total,
                  (const T*)bufs[0].x.p, w.U64.p);
+    }
     rout = bufs[0].b.p;
   }
   dim3 g(w.nblocks, np);
   const double* cs = w.cs64.p;
+  add_bytes((double)F.n * (F.W * 12.0 + 8.0) + (double)total * (16.0 + sizeof(R)));  // A (FP64), b, u; r out
   auto go = [&](auto kern) {
     launch_pdl(kern, g, dim3(TB), s, F.n, F.W, (const int32_t*)F.col.p, (const double*)F.off64.p,
                (const double*)F.diag64.p, (const double*)w.B64.p, (const double*)w.U64.p, rout, w.partial.p,
@@ -2179,6 +2207,7 @@ static void enqueue_resid_T(dec_mg& mg, Workspace& w, cudaStream_t s, std::vecto
   }
   launch_pdl(k_reduce_partials, dim3(K * np), dim3(256), s, w.nblocks, K, np, (const double*)w.partial.p,
              w.norms.p);
+  if constexpr (H) add_bytes((double)total * (4.0 + sizeof(__half)));
   if constexpr (H)
     launch_pdl(k_scale_half<K>, dim3(grid_for((long long)total, 256)), dim3(256), s, F.n, np, (const float*)w.r32.p,
                (const double*)w.norms.p, (__half*)bufs[0].b.p, w.escale.p);
@@ -2196,8 +2225,10 @@ static void enqueue_vcycle_T(dec_mg& mg, Workspace& w, cudaStream_t s, std::vect
   T* e = bufs[0].x.p;
   for (int c = 0; c <= c_last; ++c)
     e = mu_cycle<T, K>(mg, w, bufs, 0, e, c == 0, mg.opt.mu, w.npanels, s, c == c_last ? upd : nullptr);
-  if (!upd && e != bufs[0].x.p)
+  if (!upd && e != bufs[0].x.p) {
+    add_bytes(2.0 * (double)total * sizeof(T));
     DEC_CUDA(cudaMemcpyAsync(bufs[0].x.p, e, total * sizeof(T), cudaMemcpyDeviceToDevice, s));
+  }
   DEC_CHECK_LAUNCH();
 }
 
@@ -2378,6 +2409,7 @@ static Workspace& workspace(dec_mg& mg, int nrhs, int prec, bool drain = true) {
 static void enqueue_bnorms(const dec_mg& mg, Workspace& w, cudaStream_t s, double* out) {
   const int n = mg.lv[0].n, K = w.K, np = w.npanels;
   dim3 g(w.nblocks, np);
+  add_bytes((double)n * K * np * 8.0);
   switch (K) {
 #define DEC_K(KK) \
   case KK: k_panel_sumsq<KK><<<g, TB, 0, s>>>(n, w.B64.p, w.partial.p, (size_t)n * KK); break;
@@ -2391,6 +2423,7 @@ static void enqueue_bnorms(const dec_mg& mg, Workspace& w, cudaStream_t s, doubl
 // e = 0 on the finest level (the correction the first refinement step adds).
 static void zero_correction(const dec_mg& mg, Workspace& w, cudaStream_t s) {
   const size_t total = (size_t)mg.lv[0].n * w.K * w.npanels;
+  add_bytes((double)total * (w.prec == 2 ? 2.0 : w.prec == 1 ? 4.0 : 8.0));
   if (w.prec == 2) DEC_CUDA(cudaMemsetAsync(w.f16[0].x.p, 0, total * sizeof(__half), s));
   else if (w.prec == 1) DEC_CUDA(cudaMemsetAsync(w.f32[0].x.p, 0, total * sizeof(float), s));
   else DEC_CUDA(cudaMemsetAsync(w.f64[0].x.p, 0, total * sizeof(double), s));
@@ -2402,6 +2435,7 @@ static void enqueue_first_rhs(const dec_mg& mg, Workspace& w, cudaStream_t s) {
   const int n = mg.lv[0].n, K = w.K, np = w.npanels;
   dim3 g(w.nblocks, np);
   const size_t ps = (size_t)n * K;
+  add_bytes((double)ps * np * (8.0 + (w.prec == 1 ? 4.0 : 8.0)));  // b read, r = b written
   switch (K) {
 #define DEC_K(KK)                                                                                    \
   case KK:                                                                                           \
@@ -2439,6 +2473,8 @@ static void capture_solve(dec_mg& mg, Workspace& w, bool zero_guess) {
     cudaGraphConditionalHandle h;
     DEC_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
     DEC_CUDA(cudaStreamBeginCaptureToGraph(mg.cap, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    w.solve_pre_bytes[zero_guess] = 0.0;
+    t_bytes = &w.solve_pre_bytes[zero_guess];
     if (zero_guess && w.prec != 2) {
       enqueue_first_rhs(mg, w, mg.cap);
     } else {
@@ -2448,6 +2484,7 @@ static void capture_solve(dec_mg& mg, Workspace& w, bool zero_guess) {
     }
     k_ir_check<<<1, 256, 0, mg.cap>>>(h, w.norms.p, w.bn2.p, w.loop.p);
     DEC_CHECK_LAUNCH();
+    t_bytes = nullptr;
     cudaStreamCaptureStatus st;
     cudaGraph_t cg = nullptr;
     const cudaGraphNode_t* deps = nullptr;
@@ -2464,6 +2501,8 @@ static void capture_solve(dec_mg& mg, Workspace& w, bool zero_guess) {
     DEC_CUDA(cudaStreamEndCapture(mg.cap, &g));
     cudaGraph_t body = prm.conditional.phGraph_out[0];
     DEC_CUDA(cudaStreamBeginCaptureToGraph(mg.cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    w.solve_body_bytes = 0.0;
+    t_bytes = &w.solve_body_bytes;
     if (fused_update(mg, w)) {
       dispatch(mg, w, mg.cap, G_STEP);
     } else {
@@ -2472,6 +2511,7 @@ static void capture_solve(dec_mg& mg, Workspace& w, bool zero_guess) {
     }
     k_ir_check<<<1, 256, 0, mg.cap>>>(h, w.norms.p, w.bn2.p, w.loop.p);
     DEC_CHECK_LAUNCH();
+    t_bytes = nullptr;
     DEC_CUDA(cudaStreamEndCapture(mg.cap, &body));
     w.solve_pre[zero_guess] = count_kernel_nodes(g);
     w.solve_body = count_kernel_nodes(body);
@@ -2479,6 +2519,7 @@ static void capture_solve(dec_mg& mg, Workspace& w, bool zero_guess) {
     DEC_CUDA(cudaGraphInstantiate(&ex, g, 0));
     w.solve_graph[zero_guess] = ex;
   } catch (...) {
+    t_bytes = nullptr;
     fail();
     throw;
   }
@@ -2942,6 +2983,26 @@ void mg_time_kernel(dec_mg* mg, int kernel, int level, int nrhs, int reps, void*
     DEC_K(1) DEC_K(2) DEC_K(4) DEC_K(8) DEC_K(16) DEC_K(32)
 #undef DEC_K
   }
+}
+
+// Algorithmic bytes of a device-loop solve of nrhs right-hand sides that ran `iterations`
+// refinement steps: b (and u) into panels, the graph's part before its loop, `iterations` loop
+// bodies, u out of panels.  Captures the solve graph if no solve of this shape ran yet.
+double mg_solve_traffic(dec_mg* mg, int nrhs, int from_zero, int iterations) {
+  require(mg != nullptr && nrhs >= 1 && iterations >= 0, "multigrid: bad solve-traffic arguments");
+  require((mg->opt.smoother == DEC_SMOOTH_JACOBI || mg->opt.smoother == DEC_SMOOTH_CHEBYSHEV) &&
+              mg->opt.device_loop == 1,
+          "multigrid: solve traffic is counted for the device refinement loop (Jacobi / Chebyshev smoothers)");
+  require(!from_zero || mg->opt.precision != 2, "multigrid: FP16 storage has no solve from zero");
+  Workspace& w = workspace(*mg, nrhs, mg->opt.precision);
+  const int z = from_zero ? 1 : 0;
+  if (!w.solve_graph[z]) capture_solve(*mg, w, z == 1);
+  const double n = mg->lv[0].n, cm = n * nrhs * 8.0, pan = n * w.K * w.npanels * 8.0;
+  double by = cm + pan + n * 4.0;                  // b into panels (with the row permutation)
+  by += from_zero ? pan : cm + pan + n * 4.0;      // U cleared, or u into panels
+  by += w.solve_pre_bytes[z] + iterations * w.solve_body_bytes;
+  by += pan + cm + n * 4.0;                        // u out of panels
+  return by;
 }
 
 void mg_set_smoother_mlp(dec_mg* mg, const dec_mlp* mlp) {

@@ -21,6 +21,7 @@ dec_status mg_solve_wait(dec_mg* mg, uint64_t ticket, dec_solve_report* rep);
 void mg_time_kernel(dec_mg* mg, int kernel, int level, int nrhs, int reps, void* stream, double* ms,
                     double* bytes);
 int mg_autotune(dec_mg* mg, int nrhs, int reps, void* stream);
+double mg_solve_traffic(dec_mg* mg, int nrhs, int from_zero, int iterations);
 void mg_set_smoother_mlp(dec_mg* mg, const dec_mlp* mlp);
 dec_batch* batch_create(dec_mg* const* groups, int ngroups);
 void batch_destroy(dec_batch* b);

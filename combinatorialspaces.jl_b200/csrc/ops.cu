@@ -7,6 +7,7 @@
 // increasing column order, the order of the reference's CSC SpMV, and this file is compiled
 // without FMA contraction, so results reproduce the reference CPU arithmetic.
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <type_traits>
 
@@ -949,23 +950,32 @@ void op_residual_norms_impl(dec_op* op, const double* x, const double* b, int nr
 // side) followed by the 2 * nrhs norms, in a file-scope device array.  Every device that loads
 // the library holds it until the process exits.  In host code `g_resid_scratch` only names the
 // symbol; its device address is looked up once per device with that device current.
-static __device__ __align__(256) double
-    g_resid_scratch[2 * kResidBlocks * DEC_RESIDUAL_NOALLOC_MAX_RHS + 2 * DEC_RESIDUAL_NOALLOC_MAX_RHS];
+static __device__ __align__(256) double g_resid_scratch[DEC_RESIDUAL_NOALLOC_SCRATCH_DOUBLES];
+static_assert(DEC_RESIDUAL_NOALLOC_SCRATCH_DOUBLES ==
+                  2 * kResidBlocks * DEC_RESIDUAL_NOALLOC_MAX_RHS + 2 * DEC_RESIDUAL_NOALLOC_MAX_RHS,
+              "the header's scratch size must match the reduction's partial sums and norms");
 
+#define DEC_STR_(x) #x
+#define DEC_STR(x) DEC_STR_(x)
+
+// Device address of the scratch on the current device.  A filled slot is read without a lock;
+// the mutex only serialises first lookups.  The addresses are kept for the life of the process
+// (a cudaDeviceReset is not followed).
 static double* resid_scratch_for_current_device() {
   constexpr int kMaxDevices = 64;
   static std::mutex mu;
-  static double* ptrs[kMaxDevices] = {};
+  static std::atomic<double*> ptrs[kMaxDevices] = {};
   int dev = 0;
   DEC_CUDA(cudaGetDevice(&dev));
   require(dev >= 0 && dev < kMaxDevices, "residual norms (no-alloc): device ordinal out of range");
+  if (double* p = ptrs[dev].load(std::memory_order_acquire)) return p;
   std::lock_guard<std::mutex> lock(mu);
-  if (ptrs[dev] == nullptr) {
+  if (ptrs[dev].load(std::memory_order_relaxed) == nullptr) {
     void* p = nullptr;
     DEC_CUDA(cudaGetSymbolAddress(&p, g_resid_scratch));
-    ptrs[dev] = static_cast<double*>(p);
+    ptrs[dev].store(static_cast<double*>(p), std::memory_order_release);
   }
-  return ptrs[dev];
+  return ptrs[dev].load(std::memory_order_relaxed);
 }
 
 void op_residual_norms_noalloc_impl(dec_op* op, const double* x, const double* b, int nrhs, double* norms,
@@ -974,8 +984,8 @@ void op_residual_norms_noalloc_impl(dec_op* op, const double* x, const double* b
   require(op->kind == DEC_OP_LAPLACE0 || op->kind == DEC_OP_HELMHOLTZ0,
           "residual norms (no-alloc): the operator must be the Laplacian or a Helmholtz operator");
   require(nrhs >= 1 && nrhs <= DEC_RESIDUAL_NOALLOC_MAX_RHS,
-          "residual norms (no-alloc): nrhs must be in [1, " + std::to_string(DEC_RESIDUAL_NOALLOC_MAX_RHS) +
-              "], the size of its static scratch");
+          "residual norms (no-alloc): nrhs must be in [1, " DEC_STR(DEC_RESIDUAL_NOALLOC_MAX_RHS)
+          "], the size of its static scratch");
   cudaStream_t s = as_stream(stream);
   double* partial = resid_scratch_for_current_device();
   double* dn = partial + (size_t)2 * kResidBlocks * DEC_RESIDUAL_NOALLOC_MAX_RHS;

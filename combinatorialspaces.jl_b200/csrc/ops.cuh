@@ -25,7 +25,7 @@ template <class T>
 void cast_array(const DArr<double>& a, DArr<T>& b);
 
 // Blocks of the residual-norm reduction (each block reduces a strided set of rows).
-constexpr int kResidBlocks = 256;
+constexpr int kResidBlocks = DEC_RESIDUAL_BLOCKS;
 constexpr int kResidThreads = 256;
 // Residual-norm kernels on caller-provided scratch: partial holds 2 * kResidBlocks * nrhs doubles,
 // dnorms 2 * nrhs.  Every partial slot is written before it is read, so the scratch needs no

@@ -155,16 +155,21 @@ dec_status dec_op_residual_norms(dec_op* op, const double* x, const double* b, i
  * For callers that cannot allocate device memory at the point of the call: an application
  * that hands the device a fixed memory budget up front, a real-time loop that must not enter
  * the allocator, or code running while another thread captures a CUDA graph.  It calls no
- * cudaMalloc / cudaFree: its scratch (the per-block partial sums) is a file-scope device array
- * of DEC_RESIDUAL_NOALLOC_MAX_RHS * 2 * 256 + 2 * DEC_RESIDUAL_NOALLOC_MAX_RHS doubles (about
- * 264 KiB) that every GPU which loads the library holds until the process exits.
+ * cudaMalloc / cudaFree: its scratch (the per-block partial sums, then the norms) is a file-scope
+ * device array of DEC_RESIDUAL_NOALLOC_SCRATCH_DOUBLES doubles (about 264 KiB) that every GPU
+ * which loads the library holds until the process exits.
  *  - nrhs above DEC_RESIDUAL_NOALLOC_MAX_RHS is rejected with DEC_ERR_INVALID_ARG.
  *  - The first call on a device looks up the array's device address (cudaGetSymbolAddress);
- *    make that first call before any stream capture on that device.
+ *    make that first call before any stream capture on that device.  The address is kept for
+ *    the life of the process: after cudaDeviceReset on a device, do not call it on that device
+ *    again.
  *  - All calls share the one array, which keeps the last call's contents (every slot a call
  *    reads it has written first, so nothing needs clearing): calls that overlap on the GPU
  *    (concurrent streams or host threads) race. */
 #define DEC_RESIDUAL_NOALLOC_MAX_RHS 64
+#define DEC_RESIDUAL_BLOCKS 256 /* blocks of the residual-norm reduction: 2 partial sums each per RHS */
+#define DEC_RESIDUAL_NOALLOC_SCRATCH_DOUBLES \
+  (2 * DEC_RESIDUAL_BLOCKS * DEC_RESIDUAL_NOALLOC_MAX_RHS + 2 * DEC_RESIDUAL_NOALLOC_MAX_RHS)
 dec_status dec_op_residual_norms_noalloc(dec_op* op, const double* x, const double* b, int32_t nrhs,
                                          double* norms, double* bnorms, void* stream);
 /* CSR export to host, two-phase: call with rowptr == NULL to get nnz. */
@@ -359,6 +364,12 @@ typedef enum dec_mg_kernel {
  * launch and the algorithmic bytes one launch moves (every array read or written once). */
 dec_status dec_mg_time_kernel(dec_mg* mg, int32_t kernel, int32_t level, int32_t nrhs, int32_t reps,
                               void* stream, double* ms_per_launch, double* bytes_per_launch);
+/* Algorithmic bytes of a whole dec_mg_solve / dec_mg_solve_from_zero (from_zero = 1) of nrhs
+ * right-hand sides that ran `iterations` refinement steps (the report's iterations), with the
+ * refinement loop on the device (Jacobi / Chebyshev smoothers): every kernel's streamed arrays
+ * read or written once and each gathered vector once, summed over the solve graph's kernels, plus
+ * the layout changes of b and u.  Captures the solve graph if no solve of this shape ran yet. */
+dec_status dec_mg_solve_traffic(dec_mg* mg, int32_t nrhs, int32_t from_zero, int32_t iterations, double* bytes);
 /* Times each candidate panel width on one V-cycle and keeps the fastest for `nrhs` right-hand
  * sides (used when rhs_block = 0).  Returns the chosen width. */
 dec_status dec_mg_autotune(dec_mg* mg, int32_t nrhs, int32_t reps, void* stream, int32_t* rhs_block);

@@ -416,3 +416,23 @@ def test_galerkin_mixed_precision_solve(O, dec):
     with pytest.raises(dec.DecError, match="Galerkin"):
         dec.MultigridData(coarse, 2, shift=1.0, center="circumcenter", project_radius=1.0, coarse_solver=2,
                           mode="galerkin")
+
+
+def test_solve_traffic_counts_the_graph(dec, built):
+    """dec_mg_solve_traffic: linear in the refinement steps; a loop body moves at least its
+    finest-level sweeps' bytes (dec_mg_time_kernel's figure for a middle Chebyshev step) and at most
+    a few times a whole cycle's worth; a solve from zero moves fewer bytes than one from a guess."""
+    coarse, md, _ = built["ico4_circum"]
+    mg = dec.MultigridData(coarse, 4, shift=1.0, center="circumcenter", project_radius=1.0, precision=1,
+                           pre=0, post=2, cheb_ratio=3.0, inner_cycles=2, rhs_block=4)
+    B = torch.tensor(np.stack([uniform(180 + j, mg.n) for j in range(4)]), device="cuda")
+    _, rep = mg.solve(torch.zeros_like(B), B, rtol=1e-9, use_initial_guess=False)
+    t1, t2, t3 = (mg.solve_traffic(4, k) for k in (1, 2, 3))
+    body = t2 - t1
+    assert body > 0 and abs((t3 - t2) - body) <= 1e-9 * body
+    _, sweep_bytes = mg.time_kernel(0, 0, 4, reps=1)
+    assert body >= 2 * 2 * 0.9 * sweep_bytes          # inner_cycles x post finest sweeps
+    assert body <= 8 * 2 * sweep_bytes
+    assert mg.solve_traffic(4, 2, from_zero=True) < mg.solve_traffic(4, 2, from_zero=False)
+    with pytest.raises(dec.DecError):
+        dec.MultigridData(coarse, 2, shift=1.0, center="circumcenter", project_radius=1.0, smoother=2).solve_traffic(1, 1)
