@@ -238,11 +238,11 @@ def dec_c_wedge_product(j, k, a, b, p, c, n_out, out=None, index_base=0):
 class Operator:
     """A sparse DEC operator on the device: ``op(x)`` / ``op @ x`` returns Op x."""
 
-    def __init__(self, sd, kind, dtype="float64", shift=0.0, handle=None):
+    def __init__(self, sd, kind, dtype="float64", shift=0.0, handle=None, owned=False, code=None):
         self.sd = sd
         if handle is not None:
-            self._h, self._owned = handle, False
-            self.code = _capi.DEC_F64
+            self._h, self._owned = handle, owned
+            self.code = _capi.DEC_F64 if code is None else code
         else:
             self.code = _dtype_code(dtype)
             h = C.c_void_p()
@@ -292,6 +292,35 @@ class Operator:
         check(lib().dec_op_export_csr(self._h, C.byref(nnz), rp.ctypes.data_as(C.c_void_p),
                                       ci.ctypes.data_as(C.c_void_p), v.ctypes.data_as(C.c_void_p)))
         return rp, ci, v, self.shape
+
+
+def _csc_struct(A, keep, index_base=0):
+    """dec_csc of a scipy sparse matrix or an (colptr, rowval, nzval, (m, n)) tuple (0-based)."""
+    if isinstance(A, tuple):
+        cp, rv, nz, shape = A
+    else:
+        A = A.tocsc()
+        A.sort_indices()
+        cp, rv, nz, shape = A.indptr, A.indices, A.data, A.shape
+    cp = np.ascontiguousarray(np.asarray(cp) + index_base, np.int32)
+    rv = np.ascontiguousarray(np.asarray(rv) + index_base, np.int32)
+    nz = np.ascontiguousarray(nz, np.float64)
+    keep += [cp, rv, nz]
+    c = _capi.Csc()
+    c.m, c.n, c.index_base = int(shape[0]), int(shape[1]), index_base
+    c.colptr, c.rowval, c.nzval = (cp.ctypes.data_as(C.c_void_p), rv.ctypes.data_as(C.c_void_p),
+                                   nz.ctypes.data_as(C.c_void_p))
+    return c
+
+
+def sparse_operator(A, dtype="float64", index_base=0):
+    """A caller's sparse matrix (scipy sparse, or a CSC tuple) as a device operator
+    (dec_op_create_csc): ``op @ x`` is the reference's ``A * x`` on a SparseMatrixCSC."""
+    keep = []
+    c = _csc_struct(A, keep, index_base)
+    h = C.c_void_p()
+    check(lib().dec_op_create_csc(C.byref(c), _dtype_code(dtype), C.byref(h)))
+    return Operator(None, 0, handle=h, owned=True, code=_dtype_code(dtype))
 
 
 def dec_differential(n, sd, dtype="float64"):
@@ -479,6 +508,49 @@ class MultigridData:
         if h and _capi is not None and _capi._lib is not None:
             _capi._lib.dec_mg_destroy(h)
             self._h = None
+
+    @classmethod
+    def from_matrices(cls, operators, restrictions, prolongations, steps=None, index_base=0, **opts):
+        """MultigridData(g, r, p, s) (Multigrid.jl:538-546) from caller matrices, finest first:
+        square operators, restrictions (n_{k+1} x n_k), prolongations (n_k x n_{k+1}), each a scipy
+        sparse matrix or a CSC tuple; steps: one int for every level, a list per level, or None
+        (opts pre / post).  dec_mg_create_from_csc."""
+        o = default_mg_options()
+        for k, v in opts.items():
+            if not hasattr(o, k):
+                raise TypeError(f"unknown multigrid option {k}")
+            setattr(o, k, v)
+        nl = len(operators)
+        if len(restrictions) != nl - 1 or len(prolongations) != nl - 1:
+            raise ValueError("one restriction and one prolongation per level pair")
+        keep = []
+        ops = (_capi.Csc * nl)(*[_csc_struct(A, keep, index_base) for A in operators])
+        rs = (_capi.Csc * max(1, nl - 1))(*[_csc_struct(A, keep, index_base) for A in restrictions])
+        ps = (_capi.Csc * max(1, nl - 1))(*[_csc_struct(A, keep, index_base) for A in prolongations])
+        st = None
+        if steps is not None:
+            sv = [int(steps)] * nl if np.isscalar(steps) else [int(x) for x in steps]
+            if len(sv) != nl:
+                raise ValueError("one steps entry per level")
+            st = (C.c_int32 * nl)(*sv)
+        h = C.c_void_p()
+        check(lib().dec_mg_create_from_csc(nl, ops, rs, ps, st, C.byref(o), C.byref(h)))
+        self = cls.__new__(cls)
+        self.options = o
+        self._h = h
+        self.nlevels = nl
+        return self
+
+    def set_level_steps(self, steps):
+        """MultigridData.steps: smoother steps before and after the coarse correction per level
+        (None restores the options' pre / post).  dec_mg_set_level_steps."""
+        if steps is None:
+            check(lib().dec_mg_set_level_steps(self._h, None))
+            return
+        sv = [int(steps)] * self.nlevels if np.isscalar(steps) else [int(x) for x in steps]
+        if len(sv) != self.nlevels:
+            raise ValueError("one steps entry per level")
+        check(lib().dec_mg_set_level_steps(self._h, (C.c_int32 * len(sv))(*sv)))
 
     def level_info(self, level):
         nv, ne, nt, lm = C.c_int64(), C.c_int64(), C.c_int64(), C.c_double()

@@ -14,7 +14,7 @@ DEC_WEDGE_PP, DEC_WEDGE_PD, DEC_WEDGE_DP, DEC_WEDGE_DD = 0, 1, 2, 3
 (DEC_OP_D0, DEC_OP_D1, DEC_OP_BOUNDARY1, DEC_OP_BOUNDARY2, DEC_OP_DUAL_D0, DEC_OP_DUAL_D1,
  DEC_OP_STAR0, DEC_OP_STAR1, DEC_OP_STAR2, DEC_OP_INV_STAR0, DEC_OP_INV_STAR1, DEC_OP_INV_STAR2,
  DEC_OP_LAPLACE0, DEC_OP_HELMHOLTZ0, DEC_OP_STAR1_GEOMETRIC, DEC_OP_INV_STAR1_GEOMETRIC,
- DEC_OP_FLAT_SHARP) = range(17)
+ DEC_OP_FLAT_SHARP, DEC_OP_GENERAL) = range(18)
 DEC_GEOM_LENGTH, DEC_GEOM_AREA, DEC_GEOM_DUAL_AREA, DEC_GEOM_DUAL_LENGTH_TE, DEC_GEOM_DUAL_POINT = range(5)
 DEC_SMOOTH_JACOBI, DEC_SMOOTH_CHEBYSHEV, DEC_SMOOTH_CG, DEC_SMOOTH_LEARNED = 0, 1, 2, 3
 DEC_KERNEL_SWEEP, DEC_KERNEL_RESIDUAL, DEC_KERNEL_RESTRICT, DEC_KERNEL_PROLONG, DEC_KERNEL_MLP = range(5)
@@ -36,6 +36,12 @@ class MGOptions(C.Structure):
                 ("precision", C.c_int32), ("rhs_block", C.c_int32), ("mu", C.c_int32),
                 ("inner_cycles", C.c_int32), ("reorder", C.c_int32), ("coarse_max", C.c_int32),
                 ("fallback_rho", C.c_double), ("galerkin", C.c_int32), ("device_loop", C.c_int32)]
+
+
+class Csc(C.Structure):
+    """dec_csc: a SparseMatrixCSC{Float64, Int32} in host memory."""
+    _fields_ = [("m", C.c_int32), ("n", C.c_int32), ("index_base", C.c_int32),
+                ("colptr", C.c_void_p), ("rowval", C.c_void_p), ("nzval", C.c_void_p)]
 
 
 class SolveReport(C.Structure):
@@ -66,6 +72,7 @@ SIGNATURES = {
     "dec_wedge_apply_batched": (I32, [P, P, P, P, I32, P]),
     "dec_wedge_plan_destroy": (I32, [P]),
     "dec_op_create": (I32, [P, I32, F64, I32, PP]),
+    "dec_op_create_csc": (I32, [C.POINTER(Csc), I32, PP]),
     "dec_op_shape": (I32, [P, PI64, PI64]),
     "dec_op_apply": (I32, [P, P, P, F64, F64, P]),
     "dec_op_export_csr": (I32, [P, PI64, P, P, P]),
@@ -74,6 +81,9 @@ SIGNATURES = {
     "dec_op_destroy": (I32, [P]),
     "dec_mg_default_options": (None, [C.POINTER(MGOptions)]),
     "dec_mg_create": (I32, [C.POINTER(MeshDesc), C.POINTER(MGOptions), PP]),
+    "dec_mg_create_from_csc": (I32, [I32, C.POINTER(Csc), C.POINTER(Csc), C.POINTER(Csc), C.POINTER(C.c_int32),
+                                     C.POINTER(MGOptions), PP]),
+    "dec_mg_set_level_steps": (I32, [P, C.POINTER(C.c_int32)]),
     "dec_mg_destroy": (I32, [P]),
     "dec_mg_level_info": (I32, [P, I32, PI64, PI64, PI64, PF64]),
     "dec_mg_level_mesh": (I32, [P, I32, PP]),

@@ -38,6 +38,7 @@ void mlp_set_engine_impl(dec_mlp* m, int engine);
 void mlp_load_impl(dec_mlp* m, const char* path);
 void op_residual_norms_noalloc_impl(dec_op* op, const double* x, const double* b, int nrhs, double* norms,
                                     double* bnorms, void* stream);
+dec_op* op_create_csc_impl(const dec_csc* a, dec_dtype dt);
 
 namespace {
 thread_local std::string g_err;
@@ -172,6 +173,14 @@ dec_status dec_op_create(dec_mesh* m, int32_t kind, double shift, dec_dtype dt, 
   });
 }
 
+dec_status dec_op_create_csc(const dec_csc* a, dec_dtype dt, dec_op** out) {
+  return guard([&] {
+    decb::require(out != nullptr, "dec_op_create_csc: null output");
+    *out = nullptr;
+    *out = op_create_csc_impl(a, dt);
+  });
+}
+
 dec_status dec_op_shape(const dec_op* op, int64_t* rows, int64_t* cols) {
   return guard([&] {
     decb::require(op != nullptr, "dec_op_shape: null operator");
@@ -212,6 +221,20 @@ dec_status dec_mg_create(const dec_mesh_desc* coarse, const dec_mg_options* opts
     *out = nullptr;
     *out = decb::mg_create(*coarse, *opts);
   });
+}
+
+dec_status dec_mg_create_from_csc(int32_t nlevels, const dec_csc* operators, const dec_csc* restrictions,
+                                  const dec_csc* prolongations, const int32_t* steps, const dec_mg_options* opts,
+                                  dec_mg** out) {
+  return guard([&] {
+    decb::require(opts && out, "dec_mg_create_from_csc: null argument");
+    *out = nullptr;
+    *out = decb::mg_create_from_csc(nlevels, operators, restrictions, prolongations, steps, *opts);
+  });
+}
+
+dec_status dec_mg_set_level_steps(dec_mg* mg, const int32_t* steps) {
+  return guard([&] { decb::mg_set_level_steps(mg, steps); });
 }
 
 dec_status dec_mg_destroy(dec_mg* mg) {

@@ -37,6 +37,7 @@
 dec_op* op_create_impl(dec_mesh* mh, int kind, double shift, dec_dtype dt);
 dec_op* op_from_csr_impl(dec_mesh* mh, int n, const std::vector<int32_t>& rowptr, const std::vector<int32_t>& colind,
                          const std::vector<double>& val);
+void csc_to_csr(const dec_csc& a, std::vector<int32_t>& rp, std::vector<int32_t>& ci, std::vector<double>& vv);
 decb::MlpWeights mlp_weights(const dec_mlp* m);
 void mlp_check_error(const dec_mlp* m, cudaStream_t s);
 
@@ -593,6 +594,46 @@ __global__ void __launch_bounds__(TB) k_prolong(int nf, const int32_t* __restric
 #pragma unroll
     for (int q = 0; q < V; ++q) xv[q] += C(0.5) * za[q] + C(0.5) * zb[q];
     stv<T, V>(xf + (size_t)j * K, xv);
+  }
+}
+
+// General transfers (a hierarchy from caller matrices): dst (+)= M src on all panels, M row-major
+// ELL with each row's columns increasing and -1 after the last, so a row's terms are added in the
+// column order of SparseArrays' CSC product (from zero); ADD: the sum is then added to dst, as
+// u += p * z adds the finished product.
+template <class T, int K, bool ADD>
+__global__ void __launch_bounds__(TB) k_transfer(int rows, int W, const int32_t* __restrict__ col,
+                                                 const CT<T>* __restrict__ val, const T* __restrict__ src,
+                                                 T* __restrict__ dst, size_t sstride, size_t dstride) {
+  using Ln = Lanes<T, K>;
+  using C = CT<T>;
+  pdl_enter();
+  constexpr int V = Ln::V;
+  const int lane = threadIdx.x % Ln::LPR;
+  const T* sp = src + (size_t)blockIdx.y * sstride + (size_t)lane * V;
+  T* dp = dst + (size_t)blockIdx.y * dstride + (size_t)lane * V;
+  for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < rows; i += gridDim.x * Ln::RPB) {
+    C acc[V];
+#pragma unroll
+    for (int q = 0; q < V; ++q) acc[q] = C(0);
+    for (int e = 0; e < W; ++e) {
+      const int c = col[(size_t)i * W + e];
+      if (c < 0) break;
+      const C w = val[(size_t)i * W + e];
+      C v[V];
+      ldv<T, V>(sp + (size_t)c * K, v);
+#pragma unroll
+      for (int q = 0; q < V; ++q) acc[q] += w * v[q];
+    }
+    if constexpr (ADD) {
+      C xv[V];
+      ldv<T, V>(dp + (size_t)i * K, xv);
+#pragma unroll
+      for (int q = 0; q < V; ++q) xv[q] += acc[q];
+      stv<T, V>(dp + (size_t)i * K, xv);
+    } else {
+      stv<T, V>(dp + (size_t)i * K, acc);
+    }
   }
 }
 
@@ -1258,6 +1299,12 @@ struct Level {
   int nc = 0, Wq = 0;
   DArr<int32_t> rself, ridx, pa, pb;
   DArr<double> rs;
+  // a hierarchy from caller matrices: general R (nc x n) and P (n x nc) as row-major ELL
+  bool gen = false;
+  int Wr = 0, Wp = 0;
+  DArr<int32_t> rcol, pcol;
+  DArr<double> rval64, pval64;
+  DArr<float> rval32, pval32;
 };
 
 template <class T>
@@ -1312,6 +1359,10 @@ struct Workspace {
 struct dec_mg {
   dec_mg_options opt{};
   std::vector<decb::Level> lv;  // 0 = finest
+  std::vector<int> steps;       // per-level smoother steps before and after the coarse correction
+                                // (MultigridData.steps); empty: opt.pre / opt.post everywhere
+  int pre_at(int l) const { return steps.empty() ? opt.pre : steps[l]; }
+  int post_at(int l) const { return steps.empty() ? opt.post : steps[l]; }
   decb::DArr<double> ainv;      // dense inverse of level lc (FP64, internal order)
   decb::DArr<double> eigE, eigF, eigL;  // coarse_solver 2: (L + c I)⁻¹ = E (Λ + c)⁻¹ F on level lc
   int lc = 0;                   // level at which cycles solve directly
@@ -1641,8 +1692,8 @@ static void galerkin_product(const dec_op& A, const HostLevel& c, std::vector<in
 static void build_level_operator(Level& L, double shift, bool reorder, dec_op* given = nullptr) {
   if (given) L.op.reset(given);
   else L.op.reset(op_create_impl(L.mesh.get(), DEC_OP_HELMHOLTZ0, shift, DEC_F64));
-  L.n = L.mesh->m.nv;
-  if (reorder) {
+  L.n = L.mesh ? L.mesh->m.nv : (int)L.op->rows;
+  if (reorder && L.mesh) {
     L.perm = morton_order(L.mesh->m.h_pts, L.mesh->m.pts.p, L.n);
   } else {
     L.perm.resize(L.n);
@@ -1653,7 +1704,7 @@ static void build_level_operator(Level& L, double shift, bool reorder, dec_op* g
   L.dperm.upload(L.perm);
   L.diperm.upload(L.iperm);
   // off-diagonal slots: the maximum vertex degree (a Galerkin operator: its widest row)
-  L.W = given ? std::max(1, L.op->W) : std::max(1, L.mesh->m.max_v2e);
+  L.W = given || !L.mesh ? std::max(1, L.op->W) : std::max(1, L.mesh->m.max_v2e);
   L.col.alloc((size_t)L.n * L.W);
   L.off64.alloc((size_t)L.n * L.W);
   L.diag64.alloc(L.n);
@@ -1811,6 +1862,105 @@ dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
   return mg.release();
 }
 
+// Row-major ELL (rows x W, -1 padding) of a CSR, for the general transfers.
+static int ell_rows(const std::vector<int32_t>& rp, const std::vector<int32_t>& ci, const std::vector<double>& vv,
+                    DArr<int32_t>& col, DArr<double>& val64, DArr<float>& val32) {
+  const int rows = (int)rp.size() - 1;
+  int W = 1;
+  for (int i = 0; i < rows; ++i) W = std::max(W, rp[i + 1] - rp[i]);
+  std::vector<int32_t> c((size_t)rows * W, -1);
+  std::vector<double> v((size_t)rows * W, 0.0);
+  for (int i = 0; i < rows; ++i)
+    for (int q = rp[i]; q < rp[i + 1]; ++q) {
+      c[(size_t)i * W + (q - rp[i])] = ci[q];
+      v[(size_t)i * W + (q - rp[i])] = vv[q];
+    }
+  col.upload(c);
+  val64.upload(v);
+  cast_array(val64, val32);
+  return W;
+}
+
+// MultigridData(g, r, p, s) (Multigrid.jl:538-546): levels from the caller's operators,
+// restrictions and prolongations, in the caller's numbering (no locality order: there are no points).
+dec_mg* mg_create_from_csc(int nl, const dec_csc* ops, const dec_csc* rs, const dec_csc* ps, const int* steps,
+                           const dec_mg_options& o) {
+  require(nl >= 1 && nl <= 32, "multigrid: the number of levels must be in [1, 32]");
+  require(ops != nullptr && (nl == 1 || (rs != nullptr && ps != nullptr)),
+          "multigrid: null operators / restrictions / prolongations");
+  require(o.smoother == DEC_SMOOTH_JACOBI || o.smoother == DEC_SMOOTH_CHEBYSHEV || o.smoother == DEC_SMOOTH_CG,
+          "multigrid: a hierarchy from matrices takes the CG, Jacobi or Chebyshev smoother");
+  require(o.smoother != DEC_SMOOTH_CG || o.precision == 0, "multigrid: the CG smoother runs in FP64 (precision 0)");
+  require(o.pre >= 0 && o.post >= 0 && o.pre <= 16 && o.post <= 16, "multigrid: sweeps must be in [0, 16]");
+  require(o.mu == 1 || o.mu == 2, "multigrid: mu must be 1 (V) or 2 (W)");
+  require(o.precision >= 0 && o.precision <= 2, "multigrid: precision must be 0, 1 or 2");
+  require(o.precision != 2 || o.smoother != DEC_SMOOTH_CG,
+          "multigrid: FP16 storage (precision 2) needs the Jacobi or Chebyshev smoother");
+  require(o.cheb_ratio > 1.0, "multigrid: cheb_ratio must exceed 1");
+  require(o.inner_cycles >= 1 && o.inner_cycles <= 8, "multigrid: inner_cycles must be in [1, 8]");
+  require(o.coarse_max >= 0 && o.coarse_max <= 1024, "multigrid: coarse_max must be in [0, 1024]");
+  require(o.coarse_solver == 0 || o.coarse_solver == 1,
+          "multigrid: a hierarchy from matrices takes coarse_solver 0 (dense) or 1 (the smoother)");
+  require(o.device_loop == 0 || o.device_loop == 1, "multigrid: device_loop must be 0 or 1");
+  if (steps)
+    for (int k = 0; k < nl; ++k) require(steps[k] >= 0 && steps[k] <= 16, "multigrid: steps must be in [0, 16]");
+  for (int k = 0; k < nl; ++k) require(ops[k].m == ops[k].n && ops[k].m >= 1, "multigrid: operators must be square");
+  for (int k = 0; k + 1 < nl; ++k) {
+    require(rs[k].m == ops[k + 1].m && rs[k].n == ops[k].m,
+            "multigrid: restriction k must be (size of level k+1) x (size of level k)");
+    require(ps[k].m == ops[k].m && ps[k].n == ops[k + 1].m,
+            "multigrid: prolongation k must be (size of level k) x (size of level k+1)");
+  }
+  auto mg = std::make_unique<dec_mg>();
+  mg->opt = o;
+  mg->opt.levels = nl - 1;
+  mg->opt.reorder = 0;
+  mg->opt.galerkin = 0;
+  mg->lv.resize(nl);
+  if (steps) mg->steps.assign(steps, steps + nl);
+  for (int k = 0; k < nl; ++k) {
+    std::vector<int32_t> rp, ci;
+    std::vector<double> vv;
+    csc_to_csr(ops[k], rp, ci, vv);
+    dec_op* A = op_from_csr_impl(nullptr, ops[k].m, rp, ci, vv);
+    A->kind = DEC_OP_GENERAL;
+    build_level_operator(mg->lv[k], 0.0, false, A);
+    if (o.smoother != DEC_SMOOTH_CG) {
+      for (double d : mg->lv[k].diag64.download())
+        require(d != 0.0 && std::isfinite(d),
+                "multigrid: the Jacobi / Chebyshev smoothers need a nonzero diagonal on every level");
+    }
+  }
+  for (int k = 0; k + 1 < nl; ++k) {
+    Level& L = mg->lv[k];
+    L.gen = true;
+    L.nc = mg->lv[k + 1].n;
+    std::vector<int32_t> rp, ci;
+    std::vector<double> vv;
+    csc_to_csr(rs[k], rp, ci, vv);
+    L.Wr = ell_rows(rp, ci, vv, L.rcol, L.rval64, L.rval32);
+    csc_to_csr(ps[k], rp, ci, vv);
+    L.Wp = ell_rows(rp, ci, vv, L.pcol, L.pval64, L.pval32);
+  }
+  for (Level& L : mg->lv) L.lmax = power_lmax(L);
+  mg->lc = nl - 1;
+  if (o.coarse_max > 0)
+    for (int l = 0; l < nl; ++l)
+      if (mg->lv[l].n <= o.coarse_max) {
+        mg->lc = l;
+        break;
+      }
+  if (o.smoother == DEC_SMOOTH_CG) mg->lc = nl - 1;
+  const Level& C = mg->lv[mg->lc];
+  if (o.coarse_solver == 0 && o.smoother != DEC_SMOOTH_CG) {
+    require(C.n <= 8192, "multigrid: the dense coarsest solve takes at most 8192 unknowns (coarse_max)");
+    mg->ainv.upload(dense_inverse(*C.op, C.n));  // identity order: internal = caller numbering
+  }
+  DEC_CUDA(cudaStreamCreateWithFlags(&mg->cap, cudaStreamNonBlocking));
+  DEC_CUDA(cudaDeviceSynchronize());
+  return mg.release();
+}
+
 void mg_destroy(dec_mg* mg) { delete mg; }
 
 static const Level& level_at(const dec_mg* mg, int level) {
@@ -1821,13 +1971,17 @@ static const Level& level_at(const dec_mg* mg, int level) {
 
 void mg_level_info(const dec_mg* mg, int level, int64_t* nv, int64_t* ne, int64_t* nt, double* lmax) {
   const Level& L = level_at(mg, level);
-  if (nv) *nv = L.mesh->m.nv;
-  if (ne) *ne = L.mesh->m.ne;
-  if (nt) *nt = L.mesh->m.nt;
+  if (nv) *nv = L.n;
+  if (ne) *ne = L.mesh ? L.mesh->m.ne : 0;
+  if (nt) *nt = L.mesh ? L.mesh->m.nt : 0;
   if (lmax) *lmax = L.lmax;
 }
 
-const dec_mesh* mg_level_mesh(const dec_mg* mg, int level) { return level_at(mg, level).mesh.get(); }
+const dec_mesh* mg_level_mesh(const dec_mg* mg, int level) {
+  const Level& L = level_at(mg, level);
+  require(L.mesh != nullptr, "multigrid: a hierarchy built from matrices has no level meshes");
+  return L.mesh.get();
+}
 const dec_op* mg_level_op(const dec_mg* mg, int level) { return level_at(mg, level).op.get(); }
 
 // ---------------------------------------------------------------------------------------------
@@ -1862,6 +2016,17 @@ static int restrict_ctas() {
 template <class T, int K>
 static void launch_restrict(const Level& L, const Level& Cl, const T* r, T* bc, int np, cudaStream_t s,
                             bool pdl = true) {
+  if (L.gen) {
+    const dim3 g = row_grid<T, K>(Cl.n, np);
+    const size_t fs = (size_t)L.n * K, cs = (size_t)Cl.n * K;
+    add_bytes((double)Cl.n * L.Wr * (4.0 + sizeof(CT<T>)) + (double)(fs + cs) * np * sizeof(T));
+    const CT<T>* v = pick<T>(L.rval64, L.rval32);
+    if (pdl)
+      launch_pdl(k_transfer<T, K, false>, g, dim3(TB), s, Cl.n, L.Wr, (const int32_t*)L.rcol.p, v, r, bc, fs, cs);
+    else
+      k_transfer<T, K, false><<<g, TB, 0, s>>>(Cl.n, L.Wr, L.rcol.p, v, r, bc, fs, cs);
+    return;
+  }
   auto kern = L.Wq == 6 ? k_restrict<T, K, 6> : k_restrict<T, K>;
   dim3 g = row_grid<T, K>(Cl.n, np);
   const int ctas = L.Wq == 6 ? restrict_ctas<T, K, 6>() : restrict_ctas<T, K, 0>();
@@ -1879,6 +2044,18 @@ static void launch_restrict(const Level& L, const Level& Cl, const T* r, T* bc, 
 template <class T, int K>
 static void launch_prolong(const Level& L, const Level& Cl, const T* z, T* x, bool assign, int np, cudaStream_t s,
                            bool pdl = true) {
+  if (L.gen) {
+    const dim3 g = row_grid<T, K>(L.n, np);
+    const size_t fs = (size_t)L.n * K, cs = (size_t)Cl.n * K;
+    add_bytes((double)L.n * L.Wp * (4.0 + sizeof(CT<T>)) + (double)(cs + (assign ? 1 : 2) * fs) * np * sizeof(T));
+    const CT<T>* v = pick<T>(L.pval64, L.pval32);
+    auto kern = assign ? k_transfer<T, K, false> : k_transfer<T, K, true>;
+    if (pdl)
+      launch_pdl(kern, g, dim3(TB), s, L.n, L.Wp, (const int32_t*)L.pcol.p, v, z, x, cs, fs);
+    else
+      kern<<<g, TB, 0, s>>>(L.n, L.Wp, L.pcol.p, v, z, x, cs, fs);
+    return;
+  }
   auto kern = assign ? k_prolong<T, K, true> : k_prolong<T, K, false>;
   const dim3 g = row_grid<T, K>(L.n, np);
   const size_t fs = (size_t)L.n * K, cs = (size_t)Cl.n * K;
@@ -2055,7 +2232,7 @@ static double* cg_mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs
   const Level& L = mg.lv[l];
   LevelBufs<double>& B = bufs[l];
   const int last = (int)mg.lv.size() - 1;
-  const int steps_pre = mg.opt.pre, steps_post = mg.opt.post;
+  const int steps_pre = mg.pre_at(l), steps_post = mg.post_at(l);
   x = cg_smooth<K>(mg, w, L, B, x, zero_x, steps_pre, np, s);
   if (steps_pre > 0) zero_x = false;
   if (l >= last) {
@@ -2093,7 +2270,7 @@ static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bu
   }
   if (l == mg.lc) {
     if (mg.opt.coarse_solver == 1)  // the smoother on the coarsest level (pre + post sweeps)
-      return smooth<T, K>(mg, L, B, x, zero_x, std::max(1, mg.opt.pre + mg.opt.post), np, s);
+      return smooth<T, K>(mg, L, B, x, zero_x, std::max(1, mg.pre_at(l) + mg.post_at(l)), np, s);
     if (mg.opt.coarse_solver == 2) {  // per-RHS shifted solve through the eigendecomposition
       const dim3 g(grid_for(L.n, TB / K, 64), np);
       add_bytes(2.0 * (double)L.n * L.n * 8.0 + (double)L.n * K * np * (2.0 * sizeof(T) + 16.0));
@@ -2108,8 +2285,8 @@ static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bu
                (const T*)B.b.p, B.x.p, (size_t)L.n * K);
     return B.x.p;
   }
-  x = smooth<T, K>(mg, L, B, x, zero_x, mg.opt.pre, np, s);
-  zero_x = zero_x && mg.opt.pre == 0;
+  x = smooth<T, K>(mg, L, B, x, zero_x, mg.pre_at(l), np, s);
+  zero_x = zero_x && mg.pre_at(l) == 0;
   // residual into the free buffer, then restrict into the coarse right-hand side; with x = 0
   // (every coarse level, and the finest one on a refinement step's first cycle) the residual is
   // b itself, which the residual sweep would only copy (bit for bit)
@@ -2128,7 +2305,7 @@ static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bu
   if (mu > 1) z = mu_cycle<T, K>(mg, w, bufs, l + 1, z, false, mu - 1, np, s);
   // x = 0: the prolonged correction is x (written, not added)
   launch_prolong<T, K>(L, Cl, (const T*)z, x, zero_x, np, s);
-  return smooth<T, K>(mg, L, B, x, false, mg.opt.post, np, s, upd);
+  return smooth<T, K>(mg, L, B, x, false, mg.post_at(l), np, s, upd);
 }
 
 template <class T>
@@ -2256,7 +2433,7 @@ enum GraphKind { G_RESID = 0, G_VCYCLE = 1, G_CYCLE = 2, G_VCYCLE_PLAIN = 3, G_S
 // post-smoothing on a finest level that is not the directly solved one, FP32 / FP64 storage.
 static bool fused_update(const dec_mg& mg, const Workspace& w) {
   const int s = mg.opt.smoother;
-  return (s == DEC_SMOOTH_JACOBI || s == DEC_SMOOTH_CHEBYSHEV) && mg.opt.post > 0 && mg.lc > 0 && w.prec != 2;
+  return (s == DEC_SMOOTH_JACOBI || s == DEC_SMOOTH_CHEBYSHEV) && mg.post_at(0) > 0 && mg.lc > 0 && w.prec != 2;
 }
 
 template <int K>
@@ -2953,10 +3130,12 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
     *bytes = mat + (double)F.n * K * np * (8 + 8 + sz);
   } else if (kernel == DEC_KERNEL_RESTRICT) {
     const Level& Cl = mg.lv[level + 1];
-    *bytes = (double)Cl.n * ((L.Wq + 1) * 4.0 + 8) + (double)nk * sz + (double)Cl.n * K * np * sz;
+    const double idx = L.gen ? (double)Cl.n * L.Wr * (4.0 + sizeof(CT<T>)) : (double)Cl.n * ((L.Wq + 1) * 4.0 + 8);
+    *bytes = idx + (double)nk * sz + (double)Cl.n * K * np * sz;
   } else {
     const Level& Cl = mg.lv[level + 1];
-    *bytes = (double)L.n * 8.0 + (double)Cl.n * K * np * sz + 2.0 * nk * sz;
+    const double idx = L.gen ? (double)L.n * L.Wp * (4.0 + sizeof(CT<T>)) : (double)L.n * 8.0;
+    *bytes = idx + (double)Cl.n * K * np * sz + 2.0 * nk * sz;
   }
 }
 
@@ -3005,8 +3184,25 @@ double mg_solve_traffic(dec_mg* mg, int nrhs, int from_zero, int iterations) {
   return by;
 }
 
+// MultigridData.steps per level (pre = post = steps[l]); null restores the options' pre / post.
+void mg_set_level_steps(dec_mg* mg, const int* steps) {
+  require(mg != nullptr, "multigrid: null handle");
+  drain_pipeline(*mg);
+  const int nl = (int)mg->lv.size();
+  if (steps) {
+    for (int k = 0; k < nl; ++k) require(steps[k] >= 0 && steps[k] <= 16, "multigrid: steps must be in [0, 16]");
+    mg->steps.assign(steps, steps + nl);
+  } else {
+    mg->steps.clear();
+  }
+  for (auto& kv : mg->ws) kv.second->drop_graphs();  // captured cycles hold the old sweep counts
+  ++mg->epoch;
+}
+
 void mg_set_smoother_mlp(dec_mg* mg, const dec_mlp* mlp) {
   require(mg != nullptr, "multigrid: null argument");
+  require(mlp == nullptr || mg->lv[0].mesh != nullptr,
+          "multigrid: the learned smoother needs mesh levels (not a hierarchy built from matrices)");
   if (mg->mlp == mlp) return;
   if (mlp)  // the per-row coupling features the network reads on every level
     for (Level& L : mg->lv)

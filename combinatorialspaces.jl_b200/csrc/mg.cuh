@@ -6,6 +6,9 @@
 namespace decb {
 void mg_default_options(dec_mg_options& o);
 dec_mg* mg_create(const dec_mesh_desc& coarse, const dec_mg_options& opts);
+dec_mg* mg_create_from_csc(int nl, const dec_csc* ops, const dec_csc* rs, const dec_csc* ps, const int* steps,
+                           const dec_mg_options& o);
+void mg_set_level_steps(dec_mg* mg, const int* steps);
 void mg_destroy(dec_mg* mg);
 void mg_level_info(const dec_mg* mg, int level, int64_t* nv, int64_t* ne, int64_t* nt, double* lmax);
 const dec_mesh* mg_level_mesh(const dec_mg* mg, int level);

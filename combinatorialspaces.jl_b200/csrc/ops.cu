@@ -567,9 +567,8 @@ __global__ void k_resid_finish(int nblocks, int nrhs, const double* __restrict__
 
 void launch_residual_norms(const dec_op& op, const double* x, const double* b, int nrhs, double* partial,
                            double* dnorms, cudaStream_t s) {
-  const Mesh& m = *op.m;
   dim3 g(kResidBlocks, nrhs);
-  k_resid_partials<<<g, kResidThreads, 0, s>>>(m.nv, op.W, op.col.p, op.val64.p, x, b, partial, nrhs);
+  k_resid_partials<<<g, kResidThreads, 0, s>>>((int)op.rows, op.W, op.col.p, op.val64.p, x, b, partial, nrhs);
   k_resid_finish<<<(2 * nrhs + 127) / 128, 128, 0, s>>>(kResidBlocks, nrhs, partial, dnorms);
   DEC_CHECK_LAUNCH();
 }
@@ -709,11 +708,17 @@ static void inverse_geometric_star(dec_op& op, const void* vx, void* vy, double 
 
 template <class T>
 static void launch_op(const dec_op& op, const void* vx, void* vy, double alpha, double beta, cudaStream_t s) {
-  const Mesh& m = *op.m;
   const T* x = (const T*)vx;
   T* y = (T*)vy;
   const T a = (T)alpha, b = (T)beta;
   const bool hb = beta != 0.0;
+  if (op.kind == DEC_OP_GENERAL) {  // a caller's matrix: no mesh
+    const T* val = std::is_same<T, double>::value ? (const T*)op.val64.p : (const T*)op.val32.p;
+    if (op.rows) launch_ell<T>((int)op.rows, op.W, op.col.p, val, x, y, a, b, hb, s);
+    DEC_CHECK_LAUNCH();
+    return;
+  }
+  const Mesh& m = *op.m;
   const int TH = 256;
   switch (op.kind) {
     case DEC_OP_D0:
@@ -816,9 +821,9 @@ dec_op* op_create_impl(dec_mesh* mh, int kind, double shift, dec_dtype dt) {
 // slot-major ELL of the Laplacian kind (apply, residual norms and export as for L + shift I).
 dec_op* op_from_csr_impl(dec_mesh* mh, int n, const std::vector<int32_t>& rowptr, const std::vector<int32_t>& colind,
                          const std::vector<double>& val) {
-  require(mh != nullptr && (int)rowptr.size() == n + 1, "op: bad CSR");
+  require((int)rowptr.size() == n + 1, "op: bad CSR");
   auto* op = new dec_op();
-  op->m = &mh->m;
+  op->m = mh ? &mh->m : nullptr;
   op->kind = DEC_OP_HELMHOLTZ0;
   op->dtype = DEC_F64;
   op->rows = op->cols = n;
@@ -842,6 +847,72 @@ dec_op* op_from_csr_impl(dec_mesh* mh, int n, const std::vector<int32_t>& rowptr
   return op;
 }
 
+// CSC (the reference's SparseMatrixCSC layout, any index base) -> 0-based CSR with each row's
+// columns increasing (the order a CSC SpMV adds a row's terms in), validated.
+void csc_to_csr(const dec_csc& a, std::vector<int32_t>& rp, std::vector<int32_t>& ci, std::vector<double>& vv) {
+  require(a.m >= 0 && a.n >= 0, "csc: negative dimensions");
+  require(a.index_base == 0 || a.index_base == 1, "csc: index_base must be 0 or 1");
+  require(a.colptr != nullptr, "csc: null colptr");
+  const int32_t base = a.index_base;
+  require(a.colptr[0] == base, "csc: colptr[0] must equal index_base");
+  for (int j = 0; j < a.n; ++j) require(a.colptr[j + 1] >= a.colptr[j], "csc: colptr must be nondecreasing");
+  const int64_t nnz = (int64_t)a.colptr[a.n] - base;
+  require(nnz == 0 || (a.rowval != nullptr && a.nzval != nullptr), "csc: null rowval / nzval");
+  rp.assign((size_t)a.m + 1, 0);
+  for (int j = 0; j < a.n; ++j)
+    for (int32_t q = a.colptr[j] - base; q < a.colptr[j + 1] - base; ++q) {
+      const int32_t r = a.rowval[q] - base;
+      require(r >= 0 && r < a.m, "csc: row index out of range");
+      require(q == a.colptr[j] - base || a.rowval[q] > a.rowval[q - 1],
+              "csc: row indices must be strictly increasing within a column");
+      rp[(size_t)r + 1]++;
+    }
+  for (int i = 0; i < a.m; ++i) rp[(size_t)i + 1] += rp[i];
+  ci.resize((size_t)nnz);
+  vv.resize((size_t)nnz);
+  std::vector<int32_t> pos(rp.begin(), rp.end() - 1);
+  for (int j = 0; j < a.n; ++j)
+    for (int32_t q = a.colptr[j] - base; q < a.colptr[j + 1] - base; ++q) {
+      const int32_t r = a.rowval[q] - base;
+      ci[pos[r]] = j;
+      vv[pos[r]++] = a.nzval[q];
+    }
+}
+
+dec_op* op_create_csc_impl(const dec_csc* a, dec_dtype dt) {
+  require(a != nullptr, "op: null matrix");
+  require(dt == DEC_F64 || dt == DEC_F32, "op: dtype must be DEC_F64 or DEC_F32");
+  std::vector<int32_t> rp, ci;
+  std::vector<double> vv;
+  csc_to_csr(*a, rp, ci, vv);
+  const int n = a->m;
+  auto* op = new dec_op();
+  op->m = nullptr;
+  op->kind = DEC_OP_GENERAL;
+  op->dtype = dt;
+  op->rows = a->m;
+  op->cols = a->n;
+  int W = 1;
+  for (int i = 0; i < n; ++i) W = std::max(W, rp[i + 1] - rp[i]);
+  op->W = W;
+  std::vector<int32_t> c((size_t)W * n, -1);
+  std::vector<double> v((size_t)W * n, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int q = rp[i]; q < rp[i + 1]; ++q) {
+      c[(size_t)(q - rp[i]) * n + i] = ci[q];
+      v[(size_t)(q - rp[i]) * n + i] = vv[q];
+    }
+  try {
+    op->col.upload(c);
+    op->val64.upload(v);
+    if (dt == DEC_F32) cast_array(op->val64, op->val32);
+  } catch (...) {
+    delete op;
+    throw;
+  }
+  return op;
+}
+
 void op_apply_impl(dec_op* op, const void* x, void* y, double alpha, double beta, void* stream) {
   require(op != nullptr && x != nullptr && y != nullptr, "op: null argument");
   if (op->dtype == DEC_F64) launch_op<double>(*op, x, y, alpha, beta, as_stream(stream));
@@ -851,7 +922,8 @@ void op_apply_impl(dec_op* op, const void* x, void* y, double alpha, double beta
 // CSR of the operator on the host (exact integers for d / ∂ / dual d).
 void op_export_csr_impl(const dec_op* op, int64_t* nnz, int32_t* rowptr, int32_t* colind, double* val) {
   require(op != nullptr && nnz != nullptr, "op: null argument");
-  const Mesh& m = *op->m;
+  static const Mesh kNoMesh;
+  const Mesh& m = op->m ? *op->m : kNoMesh;
   std::vector<int32_t> rp(op->rows + 1, 0), ci;
   std::vector<double> vv;
   auto push = [&](int c, double v) { ci.push_back(c); vv.push_back(v); };
@@ -886,7 +958,8 @@ void op_export_csr_impl(const dec_op* op, int64_t* nnz, int32_t* rowptr, int32_t
       }
       break;
     }
-    case DEC_OP_LAPLACE0: case DEC_OP_HELMHOLTZ0: case DEC_OP_STAR1_GEOMETRIC: case DEC_OP_FLAT_SHARP: {
+    case DEC_OP_LAPLACE0: case DEC_OP_HELMHOLTZ0: case DEC_OP_STAR1_GEOMETRIC: case DEC_OP_FLAT_SHARP:
+    case DEC_OP_GENERAL: {
       auto c = op->col.download();
       auto v = op->val64.download();
       const size_t n = (size_t)op->rows;
@@ -931,8 +1004,9 @@ void hodge_diag_impl(const dec_mesh* mh, int k, int inverse, dec_dtype dt, void*
 void op_residual_norms_impl(dec_op* op, const double* x, const double* b, int nrhs, double* norms, double* bnorms,
                             void* stream) {
   require(op != nullptr && x != nullptr && b != nullptr && norms != nullptr, "residual norms: null argument");
-  require(op->kind == DEC_OP_LAPLACE0 || op->kind == DEC_OP_HELMHOLTZ0,
-          "residual norms: the operator must be the Laplacian or a Helmholtz operator");
+  require(op->kind == DEC_OP_LAPLACE0 || op->kind == DEC_OP_HELMHOLTZ0 ||
+              (op->kind == DEC_OP_GENERAL && op->rows == op->cols),
+          "residual norms: the operator must be the Laplacian, a Helmholtz operator or a square matrix");
   require(nrhs >= 1 && nrhs <= 65535, "residual norms: nrhs must be in [1, 65535]");
   cudaStream_t s = as_stream(stream);
   DArr<double> partial((size_t)2 * kResidBlocks * nrhs), dn((size_t)2 * nrhs);
@@ -981,8 +1055,9 @@ static double* resid_scratch_for_current_device() {
 void op_residual_norms_noalloc_impl(dec_op* op, const double* x, const double* b, int nrhs, double* norms,
                                     double* bnorms, void* stream) {
   require(op != nullptr && x != nullptr && b != nullptr && norms != nullptr, "residual norms (no-alloc): null argument");
-  require(op->kind == DEC_OP_LAPLACE0 || op->kind == DEC_OP_HELMHOLTZ0,
-          "residual norms (no-alloc): the operator must be the Laplacian or a Helmholtz operator");
+  require(op->kind == DEC_OP_LAPLACE0 || op->kind == DEC_OP_HELMHOLTZ0 ||
+              (op->kind == DEC_OP_GENERAL && op->rows == op->cols),
+          "residual norms (no-alloc): the operator must be the Laplacian, a Helmholtz operator or a square matrix");
   require(nrhs >= 1 && nrhs <= DEC_RESIDUAL_NOALLOC_MAX_RHS,
           "residual norms (no-alloc): nrhs must be in [1, " DEC_STR(DEC_RESIDUAL_NOALLOC_MAX_RHS)
           "], the size of its static scratch");

@@ -138,9 +138,26 @@ typedef enum dec_op_kind {
                                       read-back per reduction; not capturable in a CUDA graph) */,
   DEC_OP_FLAT_SHARP = 16           /* ♭♯_mat(sd) (DiscreteExteriorCalculus.jl:1992; ♭ :687-714, ♯ :876-909):
                                       dual 1-form -> primal 1-form, ne x ne, <= 6 nnz per row (the
-                                      matrix inside dec_wedge_product_pd/dp(1,1), FastDEC.jl:391-401) */
+                                      matrix inside dec_wedge_product_pd/dp(1,1), FastDEC.jl:391-401) */,
+  DEC_OP_GENERAL = 17              /* a caller's sparse matrix (dec_op_create_csc): the reference's A * x on a
+                                      SparseMatrixCSC / CuSparseMatrixCSC (e.g. an operator of
+                                      MultigridData.operators, src/Multigrid.jl:538-543) */
 } dec_op_kind;
+
+/* A sparse matrix in the layout of the reference's SparseMatrixCSC{Float64, Int32}
+ * (src/Multigrid.jl:538-543): host arrays, column pointers and row indices with a selectable base. */
+typedef struct dec_csc {
+  int32_t m, n;            /* rows, columns */
+  int32_t index_base;      /* 1 (Julia) or 0 */
+  const int32_t* colptr;   /* n + 1 entries, colptr[0] == index_base */
+  const int32_t* rowval;   /* row indices, strictly increasing within each column */
+  const double* nzval;     /* values */
+} dec_csc;
 dec_status dec_op_create(dec_mesh* m, int32_t kind, double shift, dec_dtype dtype, dec_op** out);
+/* A DEC_OP_GENERAL operator from a caller's sparse matrix (stored on the device as a slot-major ELL
+ * with each row's columns in increasing order, so a row sums in SparseArrays' column order).
+ * dec_op_apply, dec_op_shape and dec_op_export_csr work on it. */
+dec_status dec_op_create_csc(const dec_csc* a, dec_dtype dtype, dec_op** out);
 dec_status dec_op_shape(const dec_op* op, int64_t* rows, int64_t* cols);
 /* y = alpha * Op x + beta * y  (beta == 0 overwrites y). */
 dec_status dec_op_apply(dec_op* op, const void* x, void* y, double alpha, double beta, void* stream);
@@ -238,6 +255,24 @@ typedef struct dec_solve_report {
 void dec_mg_default_options(dec_mg_options* o);
 dec_status dec_mg_create(const dec_mesh_desc* coarse, const dec_mg_options* opts, dec_mg** out);
 dec_status dec_mg_destroy(dec_mg* mg);
+/* MultigridData(g, r, p, s) (src/Multigrid.jl:538-546): a hierarchy from the caller's matrices --
+ * nlevels square operators, finest first (operators[k] n_k x n_k), nlevels - 1 restrictions
+ * (restrictions[k] n_{k+1} x n_k) and prolongations (prolongations[k] n_k x n_{k+1}), and steps[k]
+ * smoother steps before and after the coarse correction on level k (NULL: opts->pre / opts->post on
+ * every level).  The cycle is _multigrid_μ_cycle (src/Multigrid.jl:857-872): smooth, r = b - A u,
+ * r_c = R r, recurse (twice for μ = 2), u += P z, smooth, with each restriction and prolongation a
+ * sparse product summed in SparseArrays' column order.  Smoothers: DEC_SMOOTH_CG (the reference's
+ * Krylov cg, FP64), Jacobi and Chebyshev (every operator needs a nonzero diagonal; any precision);
+ * coarse_solver 0 (dense) or 1.  opts->levels, center, project_radius, shift, galerkin and reorder
+ * are not used: the operators are taken as given, in the caller's numbering.  Levels have no mesh
+ * (dec_mg_level_mesh fails; dec_mg_level_info reports ne = nt = 0). */
+dec_status dec_mg_create_from_csc(int32_t nlevels, const dec_csc* operators, const dec_csc* restrictions,
+                                  const dec_csc* prolongations, const int32_t* steps, const dec_mg_options* opts,
+                                  dec_mg** out);
+/* The steps field of MultigridData (src/Multigrid.jl:542, :858-871): smoother steps before and after the
+ * coarse correction on each level (steps[k] for level k, finest first, as many as the hierarchy has
+ * levels; each in [0, 16]); NULL restores opts->pre / opts->post.  Any hierarchy, any smoother. */
+dec_status dec_mg_set_level_steps(dec_mg* mg, const int32_t* steps);
 /* level 0 = finest. */
 dec_status dec_mg_level_info(const dec_mg* mg, int32_t level, int64_t* nv, int64_t* ne, int64_t* nt,
                              double* lmax);

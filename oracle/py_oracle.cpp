@@ -252,8 +252,37 @@ PYBIND11_MODULE(dec_oracle, mod) {
       .def("restriction", [](const MGData& md, int k) { return csc_tuple(md.rs.at(k)); })
       .def("prolongation", [](const MGData& md, int k) { return csc_tuple(md.ps.at(k)); })
       .def("mesh", [](const MGData& md, int k) { return md.meshes.at(k); })
-      .def("set_steps", [](MGData& md, int s) { for (auto& x : md.steps) x = s; });
+      .def("set_steps", [](MGData& md, int s) { for (auto& x : md.steps) x = s; })
+      .def("set_level_steps", [](MGData& md, std::vector<int> s) {
+        if (s.size() != md.steps.size()) throw std::runtime_error("set_level_steps: one entry per level");
+        md.steps = s;
+      });
 
+  mod.def("mgdata_from_csc", [](py::list ops, py::list rs, py::list ps, std::vector<int> steps) {
+    // MultigridData(g, r, p, s) (Multigrid.jl:538-546) from CSC tuples (0-based), finest first
+    auto csc_of = [](py::handle h) {
+      auto t = h.cast<py::tuple>();
+      CSC a;
+      a.colptr = from_np(t[0].cast<py::array_t<int32_t, py::array::c_style | py::array::forcecast>>());
+      a.rowval = from_np(t[1].cast<py::array_t<int32_t, py::array::c_style | py::array::forcecast>>());
+      a.nzval = from_np(t[2].cast<py::array_t<double, py::array::c_style | py::array::forcecast>>());
+      auto shape = t[3].cast<py::tuple>();
+      a.m = shape[0].cast<int>();
+      a.n = shape[1].cast<int>();
+      return a;
+    };
+    MGData md;
+    for (auto h : ops) md.ops.push_back(csc_of(h));
+    for (auto h : rs) md.rs.push_back(csc_of(h));
+    for (auto h : ps) md.ps.push_back(csc_of(h));
+    if (md.rs.size() + 1 != md.ops.size() || md.ps.size() + 1 != md.ops.size() || steps.size() != md.ops.size())
+      throw std::runtime_error("mgdata_from_csc: level counts do not match");
+    md.steps = steps;
+    for (auto& a : md.ops) md.ops_t.push_back(transpose(a));
+    for (auto& a : md.rs) md.rs_t.push_back(transpose(a));
+    for (auto& a : md.ps) md.ps_t.push_back(transpose(a));
+    return md;
+  });
   mod.def("build_mg", &build_mg, py::arg("coarse"), py::arg("levels"), py::arg("center"),
           py::arg("shift"), py::arg("radius"), py::arg("steps") = 3, py::arg("galerkin") = false);
   mod.def("krylov_cg", [](const MGData& md, int lvl, py::array_t<double, py::array::c_style | py::array::forcecast> b,

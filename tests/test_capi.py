@@ -115,3 +115,102 @@ def test_null_arguments(dec):
     assert L.dec_mesh_create(None, C.byref(h)) == 1
     assert L.dec_wedge_apply(None, None, None, None, None) == 1
     assert L.dec_op_apply(None, None, None, 1.0, 0.0, None) == 1
+
+
+def _csc(capi, m, n, colptr, rowval, nzval, base=0, keep=None):
+    keep = keep if keep is not None else []
+    cp = np.ascontiguousarray(colptr, np.int32)
+    rv = np.ascontiguousarray(rowval, np.int32)
+    nz = np.ascontiguousarray(nzval, np.float64)
+    keep += [cp, rv, nz]
+    c = capi.Csc()
+    c.m, c.n, c.index_base = m, n, base
+    c.colptr, c.rowval, c.nzval = (cp.ctypes.data_as(C.c_void_p), rv.ctypes.data_as(C.c_void_p),
+                                   nz.ctypes.data_as(C.c_void_p))
+    return c, keep
+
+
+@pytest.mark.parametrize("case,msg", [
+    (dict(colptr=[1, 2, 3], rowval=[0, 1], nzval=[1.0, 2.0]), b"colptr[0]"),          # base 0, colptr[0] = 1
+    (dict(colptr=[0, 2, 1], rowval=[0, 1], nzval=[1.0, 2.0]), b"nondecreasing"),
+    (dict(colptr=[0, 1, 2], rowval=[0, 5], nzval=[1.0, 2.0]), b"out of range"),
+    (dict(colptr=[0, 2, 2], rowval=[1, 0], nzval=[1.0, 2.0]), b"strictly increasing"),
+])
+def test_csc_operator_rejects_malformed_matrices(dec, case, msg):
+    """dec_op_create_csc checks the SparseMatrixCSC layout on the host before any device work."""
+    from importlib import import_module
+    capi = import_module("dec_b200._capi")
+    L = dec.lib()
+    c, keep = _csc(capi, 2, 2, **case)
+    h = C.c_void_p()
+    assert L.dec_op_create_csc(C.byref(c), 0, C.byref(h)) == 1
+    assert msg in L.dec_last_error()
+
+
+def test_mg_from_csc_rejects_mismatched_levels(dec):
+    """dec_mg_create_from_csc checks the options and every matrix's dimensions before any device work."""
+    from importlib import import_module
+    capi = import_module("dec_b200._capi")
+    L = dec.lib()
+    keep = []
+    a0, _ = _csc(capi, 3, 3, [0, 1, 2, 3], [0, 1, 2], [1.0, 1.0, 1.0], keep=keep)
+    a1, _ = _csc(capi, 2, 2, [0, 1, 2], [0, 1], [1.0, 1.0], keep=keep)
+    r_bad, _ = _csc(capi, 3, 2, [0, 1, 2], [0, 1], [1.0, 1.0], keep=keep)   # should be 2 x 3
+    p0, _ = _csc(capi, 3, 2, [0, 1, 2], [0, 1], [1.0, 1.0], keep=keep)
+    ops = (capi.Csc * 2)(a0, a1)
+    rs = (capi.Csc * 1)(r_bad)
+    ps = (capi.Csc * 1)(p0)
+    o = capi.MGOptions()
+    L.dec_mg_default_options(C.byref(o))
+    h = C.c_void_p()
+    assert L.dec_mg_create_from_csc(2, ops, rs, ps, None, C.byref(o), C.byref(h)) == 1
+    assert b"restriction" in L.dec_last_error()
+    o.smoother = 3
+    assert L.dec_mg_create_from_csc(2, ops, rs, ps, None, C.byref(o), C.byref(h)) == 1
+    L.dec_mg_default_options(C.byref(o))
+    steps = (C.c_int32 * 2)(3, 17)
+    assert L.dec_mg_create_from_csc(2, ops, rs, ps, steps, C.byref(o), C.byref(h)) == 1
+    assert b"steps" in L.dec_last_error()
+
+
+def _c_struct_fields(name):
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    body = re.search(r"typedef struct " + name + r" \{(.*?)\}", text, flags=re.S).group(1)
+    fields = []
+    for decl in body.split(";"):
+        decl = re.sub(r"\bconst\b", " ", decl).replace("*", " ").strip()
+        if decl:
+            fields += [f.strip() for f in decl.split(None, 1)[1].split(",")]
+    return [f for f in fields if f]
+
+
+def _julia_struct_fields(text, name):
+    body = re.search(r"struct " + name + r"\n(.*?)\nend", text, flags=re.S).group(1)
+    fields = []
+    for line in body.splitlines():
+        line = line.split("#")[0]
+        if "()" in line:
+            continue
+        fields += re.findall(r"(\w+)::", line)
+    return fields
+
+
+def test_julia_extension_matches_the_header(dec):
+    """ext/CombinatorialSpacesB200Ext.jl (the Val(:B200) backend a Julia caller loads) ccalls only
+    symbols that the header declares and the library exports, and mirrors the C structs field for
+    field (Julia is not installed here, so this is the check that runs)."""
+    jl = (ROOT / "ext" / "CombinatorialSpacesB200Ext.jl").read_text()
+    called = set(re.findall(r":(dec_[a-z0-9_]+)", jl))
+    declared = set(declared_functions())
+    assert called and called <= declared, called - declared
+    L = dec.lib()
+    for name in called:
+        assert hasattr(L, name)
+    for cname, jname in (("dec_mesh_desc", "DecMeshDesc"), ("dec_csc", "DecCsc"),
+                         ("dec_mg_options", "DecMGOptions"), ("dec_solve_report", "DecSolveReport")):
+        assert _julia_struct_fields(jl, jname) == _c_struct_fields(cname), cname
+    # the reference CUDA extension's entry points all have Val(:B200) methods
+    for fn in ("cache_wedge", "dec_boundary", "dec_dual_derivative", "dec_differential", "dec_hodge_star",
+               "dec_inv_hodge_star", "dec_wedge_product", "multigrid_vcycles", "full_multigrid"):
+        assert re.search(r"\n" + fn + r"\(.*Val\{:B200\}|function " + fn + r"\(.*Val\{:B200\}|\n" + fn +
+                         r"\(u::CuVecOrMat|function " + fn + r"\(b::CuVecOrMat", jl), fn
