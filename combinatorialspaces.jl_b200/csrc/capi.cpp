@@ -98,6 +98,7 @@ dec_status dec_mesh_counts(const dec_mesh* m, int64_t* nv, int64_t* ne, int64_t*
 dec_status dec_mesh_orientation(const dec_mesh* m, int8_t* eo, int8_t* to) {
   return guard([&] {
     decb::require(m != nullptr, "dec_mesh_orientation: null mesh");
+    m->m.ensure_host();
     if (eo) std::memcpy(eo, m->m.h_eo.data(), m->m.h_eo.size());
     if (to) std::memcpy(to, m->m.h_to.data(), m->m.h_to.size());
   });
@@ -114,6 +115,7 @@ dec_status dec_mesh_geometry(const dec_mesh* mh, int32_t which, double* out, int
       case DEC_GEOM_DUAL_AREA: v = m.dual_area.download(); break;
       case DEC_GEOM_DUAL_LENGTH_TE: v = m.dual_len_te.download(); break;
       case DEC_GEOM_DUAL_POINT: {
+        m.ensure_host();
         auto tc = m.tri_center.download();
         v.resize(3 * ((size_t)m.nv + m.ne + m.nt));
         std::copy(m.h_pts.begin(), m.h_pts.end(), v.begin());

@@ -376,6 +376,125 @@ void Mesh::build(const dec_mesh_desc& d) {
   esign.upload(es);
   tsign.upload(ts);
   pts.upload(h_pts);
+  host_ready = true;
+  derive();
+}
+
+// refine(::BinarySubdivision) on the device (Multigrid.jl:130-183, 0-based): coarse edge e splits
+// into fine edge 2e (midpoint -> ∂v0) and 2e+1 (midpoint -> ∂v1), its midpoint vertex nv + e placed by
+// propagate_points (:111-122) and optionally projected onto the sphere of the given radius
+// (the arithmetic of the host statement, uncontracted).
+__global__ void k_refine_edges(int nvc, int nec, const int32_t* __restrict__ cev0, const int32_t* __restrict__ cev1,
+                               const double* __restrict__ cpts, double radius, int32_t* __restrict__ fev0,
+                               int32_t* __restrict__ fev1, double* __restrict__ fpts) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nec; e += gridDim.x * blockDim.x) {
+    const int a = cev0[e], b = cev1[e], m = nvc + e;
+    fev0[2 * e] = m;
+    fev1[2 * e] = a;
+    fev0[2 * e + 1] = m;
+    fev1[2 * e + 1] = b;
+    double o[3];
+    for (int k = 0; k < 3; ++k) o[k] = (cpts[3 * (size_t)a + k] + cpts[3 * (size_t)b + k]) / 2;
+    if (radius > 0) {
+      const double nrm = sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+      for (int k = 0; k < 3; ++k) o[k] = o[k] / nrm * radius;
+    }
+    for (int k = 0; k < 3; ++k) fpts[3 * (size_t)m + k] = o[k];
+  }
+}
+
+// The triangles' part of refine: per coarse triangle t its three interior edges 2ne + 3t + (0, 1, 2)
+// and its four children 4t .. 4t+3 with their ∂e wiring (Multigrid.jl:160-179), and the children's
+// orientation in closed form (o, ¬o, o, ¬o), o the coarse triangle's (flipped where flip[t] is set:
+// the first refinement follows orient!'s DFS seeded true at each component's first triangle).
+__global__ void k_refine_tris(int nvc, int nec, int ntc, const int32_t* __restrict__ cte0,
+                              const int32_t* __restrict__ cte1, const int32_t* __restrict__ cte2,
+                              const int8_t* __restrict__ ctsign, const int8_t* __restrict__ flip,
+                              int32_t* __restrict__ fev0, int32_t* __restrict__ fev1, int32_t* __restrict__ fte0,
+                              int32_t* __restrict__ fte1, int32_t* __restrict__ fte2, int8_t* __restrict__ ftsign) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntc; t += gridDim.x * blockDim.x) {
+    const int e0 = cte0[t], e1 = cte1[t], e2 = cte2[t];
+    const int m0 = e0 + nvc, m1 = e1 + nvc, m2 = e2 + nvc;
+    const int m0_m1 = 2 * nec + 3 * t, m1_m2 = m0_m1 + 1, m0_m2 = m0_m1 + 2;
+    fev0[m0_m1] = m1;
+    fev1[m0_m1] = m0;
+    fev0[m1_m2] = m2;
+    fev1[m1_m2] = m1;
+    fev0[m0_m2] = m2;
+    fev1[m0_m2] = m0;
+    const int m0_v1 = 2 * e0 + 1, v2_m0 = 2 * e0, m1_v0 = 2 * e1 + 1, v2_m1 = 2 * e1, m2_v0 = 2 * e2 + 1,
+              v1_m2 = 2 * e2;
+    const int b = 4 * t;
+    fte0[b] = m1_m2;
+    fte1[b] = m0_m2;
+    fte2[b] = m0_m1;
+    fte0[b + 1] = m1_m2;
+    fte1[b + 1] = m2_v0;
+    fte2[b + 1] = m1_v0;
+    fte0[b + 2] = m0_m2;
+    fte1[b + 2] = v1_m2;
+    fte2[b + 2] = m0_v1;
+    fte0[b + 3] = m0_m1;
+    fte1[b + 3] = v2_m1;
+    fte2[b + 3] = v2_m0;
+    bool o = ctsign[t] > 0;
+    if (flip && flip[t]) o = !o;
+    const int8_t so = o ? 1 : -1;
+    ftsign[b] = so;
+    ftsign[b + 1] = (int8_t)-so;
+    ftsign[b + 2] = so;
+    ftsign[b + 3] = (int8_t)-so;
+  }
+}
+
+void Mesh::refine_from(const Mesh& c, double radius, const int8_t* dflip, int center_kind) {
+  require(4LL * c.nt < (1LL << 30) && 2LL * c.ne + 3LL * c.nt < (1LL << 30) && (long long)c.nv + c.ne < (1LL << 30),
+          "multigrid: hierarchy too large");
+  nv = c.nv + c.ne;
+  ne = 2 * c.ne + 3 * c.nt;
+  nt = 4 * c.nt;
+  center = center_kind;
+  ev0.alloc(ne);
+  ev1.alloc(ne);
+  te0.alloc(nt);
+  te1.alloc(nt);
+  te2.alloc(nt);
+  esign.alloc(ne);
+  tsign.alloc(nt);
+  pts.alloc(3 * (size_t)nv);
+  const int T = 256;
+  // the coarse vertices keep their places; unset edge orientations become false (DEC.jl:311-320)
+  DEC_CUDA(cudaMemcpy(pts.p, c.pts.p, 3 * (size_t)c.nv * sizeof(double), cudaMemcpyDeviceToDevice));
+  if (ne) DEC_CUDA(cudaMemset(esign.p, 0xFF, (size_t)ne));
+  if (c.ne)
+    k_refine_edges<<<grid_for(c.ne, T), T>>>(c.nv, c.ne, c.ev0.p, c.ev1.p, c.pts.p, radius, ev0.p, ev1.p, pts.p);
+  if (c.nt)
+    k_refine_tris<<<grid_for(c.nt, T), T>>>(c.nv, c.ne, c.nt, c.te0.p, c.te1.p, c.te2.p, c.tsign.p, dflip, ev0.p,
+                                            ev1.p, te0.p, te1.p, te2.p, tsign.p);
+  DEC_CHECK_LAUNCH();
+  host_ready = false;
+  derive();
+}
+
+void Mesh::ensure_host() const {
+  if (host_ready) return;
+  h_ev0 = ev0.download();
+  h_ev1 = ev1.download();
+  h_te0 = te0.download();
+  h_te1 = te1.download();
+  h_te2 = te2.download();
+  h_pts = pts.download();
+  auto es = esign.download();
+  auto ts = tsign.download();
+  h_eo.resize(ne);
+  h_to.resize(nt);
+  for (int e = 0; e < ne; ++e) h_eo[e] = es[e] > 0 ? 1 : 0;
+  for (int t = 0; t < nt; ++t) h_to[t] = ts[t] > 0 ? 1 : 0;
+  host_ready = true;
+}
+
+// Derived topology, incidence and geometry, on the device from the raw arrays only.
+void Mesh::derive() {
   tv0.alloc(nt);
   tv1.alloc(nt);
   tv2.alloc(nt);

@@ -8,11 +8,12 @@ namespace decb {
 struct Mesh {
   int nv = 0, ne = 0, nt = 0, center = 0;
 
-  // Host copies of the (0-based) topology and points: used to build incidence lists, CSR
-  // exports and the refined levels of a multigrid hierarchy.
-  std::vector<int32_t> h_ev0, h_ev1, h_te0, h_te1, h_te2;
-  std::vector<int8_t> h_eo, h_to;  // 1 / 0
-  std::vector<double> h_pts;       // 3 * nv
+  // Host copies of the (0-based) topology and points, for CSR exports and host-side products:
+  // filled by build(); a level refined on the device fills them on first use (ensure_host).
+  mutable std::vector<int32_t> h_ev0, h_ev1, h_te0, h_te1, h_te2;
+  mutable std::vector<int8_t> h_eo, h_to;  // 1 / 0
+  mutable std::vector<double> h_pts;       // 3 * nv
+  mutable bool host_ready = false;
 
   // Topology.
   DArr<int32_t> ev0, ev1;            // ∂v0, ∂v1 per edge
@@ -44,6 +45,16 @@ struct Mesh {
   DArr<double> star0, star1, star2;  // diagonal Hodge stars
 
   void build(const dec_mesh_desc& desc);
+  // The binary subdivision of coarse mesh c, built on the device (refine + propagate_points, new
+  // vertices projected onto the sphere of `radius` when it is positive); dflip: device per coarse
+  // triangle, nonzero where the children's orientation follows the flipped coarse one (or null).
+  void refine_from(const Mesh& c, double radius, const int8_t* dflip, int center);
+  void ensure_host() const;
+
+ private:
+  void derive();
+
+ public:
 };
 
 }  // namespace decb

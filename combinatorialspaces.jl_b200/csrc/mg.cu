@@ -44,7 +44,8 @@ void mlp_check_error(const dec_mlp* m, cudaStream_t s);
 namespace decb {
 
 // ---------------------------------------------------------------------------------------------
-// Host topology refinement (Multigrid.jl:111-219)
+// Host topology: the coarse mesh's orientation flips and GalerkinMode's sparse products
+// (the refinement itself runs on the device, Mesh::refine_from)
 // ---------------------------------------------------------------------------------------------
 struct HostLevel {
   int nv = 0, ne = 0, nt = 0;
@@ -52,62 +53,6 @@ struct HostLevel {
   std::vector<int8_t> eo, to;
   std::vector<double> pts;
 };
-
-// refine(::BinarySubdivision, topo), Multigrid.jl:130-183 (0-based: coarse edge e -> fine
-// edges 2e, 2e+1; triangle t -> interior edges 2ne+3t.., children 4t..4t+3).
-static HostLevel refine_level(const HostLevel& c, double radius, const std::vector<int8_t>* flip) {
-  HostLevel f;
-  f.nv = c.nv + c.ne;
-  f.ne = 2 * c.ne + 3 * c.nt;
-  f.nt = 4 * c.nt;
-  f.ev0.resize(f.ne);
-  f.ev1.resize(f.ne);
-  for (int e = 0; e < c.ne; ++e) {
-    int m = c.nv + e;
-    f.ev0[2 * e] = m;
-    f.ev1[2 * e] = c.ev0[e];
-    f.ev0[2 * e + 1] = m;
-    f.ev1[2 * e + 1] = c.ev1[e];
-  }
-  f.te0.resize(f.nt);
-  f.te1.resize(f.nt);
-  f.te2.resize(f.nt);
-  f.to.resize(f.nt);
-  for (int t = 0; t < c.nt; ++t) {
-    int e0 = c.te0[t], e1 = c.te1[t], e2 = c.te2[t];
-    int m0 = e0 + c.nv, m1 = e1 + c.nv, m2 = e2 + c.nv;
-    int m0_m1 = 2 * c.ne + 3 * t, m1_m2 = m0_m1 + 1, m0_m2 = m0_m1 + 2;
-    f.ev0[m0_m1] = m1; f.ev1[m0_m1] = m0;
-    f.ev0[m1_m2] = m2; f.ev1[m1_m2] = m1;
-    f.ev0[m0_m2] = m2; f.ev1[m0_m2] = m0;
-    int m0_v1 = 2 * e0 + 1, v2_m0 = 2 * e0, m1_v0 = 2 * e1 + 1, v2_m1 = 2 * e1, m2_v0 = 2 * e2 + 1,
-        v1_m2 = 2 * e2;
-    int b = 4 * t;
-    f.te0[b] = m1_m2;     f.te1[b] = m0_m2;     f.te2[b] = m0_m1;
-    f.te0[b + 1] = m1_m2; f.te1[b + 1] = m2_v0; f.te2[b + 1] = m1_v0;
-    f.te0[b + 2] = m0_m2; f.te1[b + 2] = v1_m2; f.te2[b + 2] = m0_v1;
-    f.te0[b + 3] = m0_m1; f.te1[b + 3] = v2_m1; f.te2[b + 3] = v2_m0;
-    int8_t o = c.to[t];
-    if (flip && (*flip)[t]) o = (int8_t)!o;
-    f.to[b] = o;
-    f.to[b + 1] = (int8_t)!o;
-    f.to[b + 2] = o;
-    f.to[b + 3] = (int8_t)!o;
-  }
-  f.eo.assign(f.ne, 0);  // unset edge orientations become false (DEC.jl:311-320)
-  // propagate_points(::BinarySubdivision), :111-122, optionally projected onto a sphere.
-  f.pts.resize(3 * (size_t)f.nv);
-  std::copy(c.pts.begin(), c.pts.end(), f.pts.begin());
-  for (int e = 0; e < c.ne; ++e) {
-    double* o = &f.pts[3 * ((size_t)c.nv + e)];
-    for (int k = 0; k < 3; ++k) o[k] = (c.pts[3 * (size_t)c.ev0[e] + k] + c.pts[3 * (size_t)c.ev1[e] + k]) / 2;
-    if (radius > 0) {
-      double n = std::sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
-      for (int k = 0; k < 3; ++k) o[k] = o[k] / n * radius;
-    }
-  }
-  return f;
-}
 
 // Per coarse triangle: does its component's DFS seed (first triangle) carry `false`?  Then the
 // fine level's orient! (seeded true at that triangle's first child) flips the component.
@@ -143,24 +88,22 @@ static std::vector<int8_t> component_flips(const HostLevel& c) {
   return flip;
 }
 
-static std::unique_ptr<dec_mesh> make_mesh(const HostLevel& h, int center) {
-  dec_mesh_desc d{};
-  d.nv = h.nv;
-  d.ne = h.ne;
-  d.nt = h.nt;
-  d.index_base = 0;
-  d.points = h.pts.data();
-  d.e_v0 = h.ev0.data();
-  d.e_v1 = h.ev1.data();
-  d.t_e0 = h.te0.data();
-  d.t_e1 = h.te1.data();
-  d.t_e2 = h.te2.data();
-  d.edge_orientation = h.eo.data();
-  d.tri_orientation = h.to.data();
-  d.center = center;
-  auto m = std::make_unique<dec_mesh>();
-  m->m.build(d);
-  return m;
+// The host topology of a mesh (downloaded once if the mesh was refined on the device).
+static HostLevel host_level(const Mesh& m) {
+  m.ensure_host();
+  HostLevel h;
+  h.nv = m.nv;
+  h.ne = m.ne;
+  h.nt = m.nt;
+  h.ev0 = m.h_ev0;
+  h.ev1 = m.h_ev1;
+  h.te0 = m.h_te0;
+  h.te1 = m.h_te1;
+  h.te2 = m.h_te2;
+  h.eo = m.h_eo;
+  h.to = m.h_to;
+  h.pts = m.h_pts;
+  return h;
 }
 
 // Locality order: vertices sorted by the 3D Morton code of their (bounding-box normalised)
@@ -190,13 +133,42 @@ __global__ void k_morton_keys(int n, const double* __restrict__ pts, double3 lo,
   }
 }
 
-static std::vector<int32_t> morton_order(const std::vector<double>& h_pts, const double* d_pts, int n) {
-  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  for (int i = 0; i < n; ++i)
+// Bounding box of the points: per block the minima and maxima of x, y, z (part[6 b + k]).
+__global__ void __launch_bounds__(256) k_bbox(int n, const double* __restrict__ pts, double* __restrict__ part) {
+  __shared__ double sh[6][256];
+  double v[6] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     for (int k = 0; k < 3; ++k) {
-      lo[k] = std::min(lo[k], h_pts[3 * (size_t)i + k]);
-      hi[k] = std::max(hi[k], h_pts[3 * (size_t)i + k]);
+      const double p = pts[3 * (size_t)i + k];
+      v[k] = fmin(v[k], p);
+      v[3 + k] = fmax(v[3 + k], p);
     }
+  for (int k = 0; k < 6; ++k) sh[k][threadIdx.x] = v[k];
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int k = 0; k < 6; ++k)
+        sh[k][threadIdx.x] = k < 3 ? fmin(sh[k][threadIdx.x], sh[k][threadIdx.x + st])
+                                   : fmax(sh[k][threadIdx.x], sh[k][threadIdx.x + st]);
+    __syncthreads();
+  }
+  if (threadIdx.x < 6) part[6 * (size_t)blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+static std::vector<int32_t> morton_order(const double* d_pts, int n) {
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  {
+    const int nb = (int)grid_for(n, 256, 4);
+    DArr<double> part(6 * (size_t)nb);
+    k_bbox<<<nb, 256>>>(n, d_pts, part.p);
+    DEC_CHECK_LAUNCH();
+    auto h = part.download();
+    for (int b = 0; b < nb; ++b)
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(lo[k], h[6 * (size_t)b + k]);
+        hi[k] = std::max(hi[k], h[6 * (size_t)b + 3 + k]);
+      }
+  }
   DArr<uint64_t> key(n), ks(n);
   DArr<int32_t> idx(n), is(n);
   k_morton_keys<<<grid_for(n, 256), 256>>>(n, d_pts, make_double3(lo[0], lo[1], lo[2]),
@@ -1694,7 +1666,7 @@ static void build_level_operator(Level& L, double shift, bool reorder, dec_op* g
   else L.op.reset(op_create_impl(L.mesh.get(), DEC_OP_HELMHOLTZ0, shift, DEC_F64));
   L.n = L.mesh ? L.mesh->m.nv : (int)L.op->rows;
   if (reorder && L.mesh) {
-    L.perm = morton_order(L.mesh->m.h_pts, L.mesh->m.pts.p, L.n);
+    L.perm = morton_order(L.mesh->m.pts.p, L.n);
   } else {
     L.perm.resize(L.n);
     std::iota(L.perm.begin(), L.perm.end(), 0);
@@ -1717,56 +1689,61 @@ static void build_level_operator(Level& L, double shift, bool reorder, dec_op* g
   cast_array(L.dinv64, L.dinv32);
 }
 
-// Transfers between fine level F and its coarse level C (host topology c of the coarse mesh),
-// in the internal numbering of both.
-static void build_transfers(Level& F, const Level& C, const HostLevel& c) {
-  F.nc = c.nv;
-  // coarse vertex -> fine midpoints (reference numbering) in increasing edge order, as CSR
-  std::vector<int32_t> iptr(c.nv + 1, 0), inc;
-  for (int e = 0; e < c.ne; ++e) {
-    iptr[c.ev0[e] + 1]++;
-    if (c.ev1[e] != c.ev0[e]) iptr[c.ev1[e] + 1]++;
-  }
-  for (int i = 0; i < c.nv; ++i) iptr[i + 1] += iptr[i];
-  inc.resize(iptr[c.nv]);
-  {
-    std::vector<int32_t> pos(iptr.begin(), iptr.end() - 1);
-    for (int e = 0; e < c.ne; ++e) {
-      inc[pos[c.ev0[e]]++] = c.nv + e;
-      if (c.ev1[e] != c.ev0[e]) inc[pos[c.ev1[e]]++] = c.nv + e;
-    }
-  }
-  int Wq = 1;
-  for (int i = 0; i < c.nv; ++i) Wq = std::max<int>(Wq, iptr[i + 1] - iptr[i]);
-  std::vector<int32_t> rself(c.nv), ridx((size_t)c.nv * Wq, -1);
-  std::vector<double> rs(c.nv);
-  for (int ic = 0; ic < c.nv; ++ic) {   // internal coarse row
-    int i = C.perm[ic];                 // reference coarse vertex
-    rself[ic] = F.iperm[i];             // the vertex's copy on the fine level (reference index i)
-    double s = 1.0;                     // row sum of S in column order: 1.0 then 0.5 per edge
-    for (int q = iptr[i]; q < iptr[i + 1]; ++q) {
-      ridx[(size_t)ic * Wq + (q - iptr[i])] = F.iperm[inc[q]];
+// Restriction lists, on the device: per internal coarse row ic (reference vertex i = cperm[ic])
+// its copy on the fine level, the fine midpoints of its incident edges in increasing edge order
+// (the coarse mesh's d0ᵀ rows, sorted by edge; -1 after them in the Wq slots) and the row sum of S
+// (1.0, then 0.5 per edge, in column order).
+__global__ void k_restrict_lists(int nc, int Wq, const int32_t* __restrict__ cperm, const int32_t* __restrict__ fiperm,
+                                 const int32_t* __restrict__ v2e_ptr, const int32_t* __restrict__ v2e,
+                                 int32_t* __restrict__ rself, int32_t* __restrict__ ridx, double* __restrict__ rs) {
+  for (int ic = blockIdx.x * blockDim.x + threadIdx.x; ic < nc; ic += gridDim.x * blockDim.x) {
+    const int i = cperm[ic];
+    rself[ic] = fiperm[i];
+    double s = 1.0;
+    int q = 0;
+    for (int p = v2e_ptr[i]; p < v2e_ptr[i + 1] && q < Wq; ++p, ++q) {
+      const int e = abs(v2e[p]) - 1;
+      ridx[(size_t)ic * Wq + q] = fiperm[nc + e];
       s += 0.5;
     }
+    for (; q < Wq; ++q) ridx[(size_t)ic * Wq + q] = -1;
     rs[ic] = s;
   }
-  std::vector<int32_t> pa(F.n), pb(F.n);
-  for (int jf = 0; jf < F.n; ++jf) {    // internal fine row
-    int j = F.perm[jf];
-    if (j < c.nv) {
-      pa[jf] = pb[jf] = C.iperm[j];
+}
+
+// Prolongation lists: fine row jf (reference vertex j = fperm[jf]) takes ½ z[pa] + ½ z[pb], pa = pb
+// = the coarse vertex itself for j < nc, else the endpoints of coarse edge j - nc, lower first.
+__global__ void k_prolong_lists(int nf, int nc, const int32_t* __restrict__ fperm, const int32_t* __restrict__ ciperm,
+                                const int32_t* __restrict__ cev0, const int32_t* __restrict__ cev1,
+                                int32_t* __restrict__ pa, int32_t* __restrict__ pb) {
+  for (int jf = blockIdx.x * blockDim.x + threadIdx.x; jf < nf; jf += gridDim.x * blockDim.x) {
+    const int j = fperm[jf];
+    if (j < nc) {
+      pa[jf] = pb[jf] = ciperm[j];
     } else {
-      int e = j - c.nv;
-      pa[jf] = C.iperm[std::min(c.ev0[e], c.ev1[e])];
-      pb[jf] = C.iperm[std::max(c.ev0[e], c.ev1[e])];
+      const int e = j - nc;
+      pa[jf] = ciperm[min(cev0[e], cev1[e])];
+      pb[jf] = ciperm[max(cev0[e], cev1[e])];
     }
   }
-  F.Wq = Wq;
-  F.rself.upload(rself);
-  F.ridx.upload(ridx);
-  F.rs.upload(rs);
-  F.pa.upload(pa);
-  F.pb.upload(pb);
+}
+
+// Transfers between fine level F and its coarse level C, in the internal numbering of both, from
+// the coarse mesh's device topology (a simplicial complex: no edge has ∂v0 = ∂v1).
+static void build_transfers(Level& F, const Level& C) {
+  const Mesh& c = C.mesh->m;
+  F.nc = c.nv;
+  F.Wq = std::max(1, c.max_v2e);
+  F.rself.alloc(c.nv);
+  F.ridx.alloc((size_t)c.nv * F.Wq);
+  F.rs.alloc(c.nv);
+  F.pa.alloc(F.n);
+  F.pb.alloc(F.n);
+  const int T = 256;
+  k_restrict_lists<<<grid_for(c.nv, T), T>>>(c.nv, F.Wq, C.dperm.p, F.diperm.p, c.v2e_ptr.p, c.v2e.p, F.rself.p,
+                                             F.ridx.p, F.rs.p);
+  k_prolong_lists<<<grid_for(F.n, T), T>>>(F.n, c.nv, F.dperm.p, C.diperm.p, c.ev0.p, c.ev1.p, F.pa.p, F.pb.p);
+  DEC_CHECK_LAUNCH();
 }
 
 dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
@@ -1792,41 +1769,31 @@ dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
           "multigrid: per-RHS shifts (coarse_solver 2) need every level's own Laplacian (not GalerkinMode)");
   auto mg = std::make_unique<dec_mg>();
   mg->opt = o;
-  std::vector<HostLevel> hl(o.levels + 1);
   {
     auto m = std::make_unique<dec_mesh>();
     dec_mesh_desc d = cd;
     d.center = o.center;
     m->m.build(d);
-    HostLevel& h = hl[0];
-    h.nv = m->m.nv;
-    h.ne = m->m.ne;
-    h.nt = m->m.nt;
-    h.ev0 = m->m.h_ev0;
-    h.ev1 = m->m.h_ev1;
-    h.te0 = m->m.h_te0;
-    h.te1 = m->m.h_te1;
-    h.te2 = m->m.h_te2;
-    h.eo = m->m.h_eo;
-    h.to = m->m.h_to;
-    h.pts = m->m.h_pts;
     mg->lv.resize(o.levels + 1);
     mg->lv[o.levels].mesh = std::move(m);
   }
+  // every finer level is the binary subdivision of the one below it, refined on the device; the
+  // first refinement carries the coarse mesh's orientation flips (orient!'s seeds)
+  DArr<int8_t> dflip;
+  if (o.levels >= 1) dflip.upload(component_flips(host_level(mg->lv[o.levels].mesh->m)));
   for (int l = 1; l <= o.levels; ++l) {
-    std::vector<int8_t> flip;
-    if (l == 1) flip = component_flips(hl[0]);
-    require(4LL * hl[l - 1].nt < (1LL << 30), "multigrid: hierarchy too large");
-    hl[l] = refine_level(hl[l - 1], o.project_radius, l == 1 ? &flip : nullptr);
-    mg->lv[o.levels - l].mesh = make_mesh(hl[l], o.center);
+    auto fm = std::make_unique<dec_mesh>();
+    fm->m.refine_from(mg->lv[o.levels - l + 1].mesh->m, o.project_radius, l == 1 ? dflip.p : nullptr, o.center);
+    mg->lv[o.levels - l].mesh = std::move(fm);
   }
   // coarse_solver 2 keeps every level's operator the Laplacian; the shifts come per RHS
   for (int l = 0; l <= o.levels; ++l) {
     if (o.galerkin && l > 0) {  // A_l = R A_{l-1} P over the coarse topology of level l
       std::vector<int32_t> rp, ci;
       std::vector<double> vv;
-      galerkin_product(*mg->lv[l - 1].op, hl[o.levels - l], rp, ci, vv);
-      dec_op* A = op_from_csr_impl(mg->lv[l].mesh.get(), hl[o.levels - l].nv, rp, ci, vv);
+      const HostLevel hc = host_level(mg->lv[l].mesh->m);
+      galerkin_product(*mg->lv[l - 1].op, hc, rp, ci, vv);
+      dec_op* A = op_from_csr_impl(mg->lv[l].mesh.get(), hc.nv, rp, ci, vv);
       build_level_operator(mg->lv[l], 0.0, o.reorder != 0, A);
     } else {
       build_level_operator(mg->lv[l], o.coarse_solver == 2 ? 0.0 : o.shift, o.reorder != 0);
@@ -1834,7 +1801,7 @@ dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
   }
   for (int l = 0; l <= o.levels; ++l) {
     Level& L = mg->lv[l];
-    if (l < o.levels) build_transfers(L, mg->lv[l + 1], hl[o.levels - l - 1]);
+    if (l < o.levels) build_transfers(L, mg->lv[l + 1]);
     L.lmax = power_lmax(L);
   }
   mg->lc = o.levels;
@@ -3262,23 +3229,36 @@ int mg_autotune(dec_mg* mg, int nrhs, int reps, void* stream) {
 // groups is one CUDA graph whose branches (one per group, on forked streams) run concurrently;
 // the host reads all groups' residual norms with one copy per step.
 // ---------------------------------------------------------------------------------------------
+// The state of a batched solve's refinement loop (one graph with a conditional WHILE node).
+struct BatchState {
+  int it;         // refinement steps run
+  int max_iters;
+  int all;        // every group converged
+  int pad;
+  double rtol;
+};
+
 struct dec_batch {
   std::vector<dec_mg*> groups;                 // not owned
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> join;
   cudaEvent_t fork = nullptr;
   cudaStream_t cap = nullptr;
-  decb::DArr<double> norms;                    // all groups' squared residual norms
+  decb::DArr<double> norms, bn2;               // all groups' squared residual / right-hand-side norms
+  decb::DArr<int32_t> meta;                    // per group: offset into norms, right-hand sides
+  decb::DArr<int32_t> conv_at;                 // per group: step at which it converged, -1 before
+  decb::DArr<double> worst;                    // per group: worst relative residual at the last test
+  decb::DArr<BatchState> state;
   std::vector<size_t> off;                     // group g's norms at norms[off[g]]
-  std::vector<decb::Workspace*> used;          // workspaces the graphs were captured on
+  std::vector<decb::Workspace*> used;          // workspaces the graph was captured on
   std::vector<uint64_t> epochs;
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // 0: residual of all groups, 1: V-cycle + residual
-  int64_t launches[2] = {0, 0};
+  std::vector<const void*> bufs;               // the caller's u / rhs pointers baked into the graph
+  std::vector<int> nrhs;
+  cudaGraphExec_t graph = nullptr;             // the whole solve: panels in, loop, panels out
+  int64_t launches_pre = 0, launches_body = 0; // kernel nodes outside / inside the WHILE body
   void drop_graphs() {
-    for (auto& g : graph) {
-      if (g) cudaGraphExecDestroy(g);
-      g = nullptr;
-    }
+    if (graph) cudaGraphExecDestroy(graph);
+    graph = nullptr;
   }
   ~dec_batch() {
     drop_graphs();
@@ -3309,45 +3289,150 @@ dec_batch* batch_create(dec_mg* const* groups, int ngroups) {
   }
   DEC_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
   DEC_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+  b->conv_at.alloc(ngroups);
+  b->worst.alloc(ngroups);
+  b->state.alloc(1);
   return b.release();
 }
 
 void batch_destroy(dec_batch* b) { delete b; }
 
-// kind 0: the residual step of every group; kind 1: V-cycle then residual of every group.  Each
-// group's norms are copied into the batch's array at the end of its branch.
-static cudaGraphExec_t batch_capture(dec_batch& bt, int kind) {
+__global__ void k_batch_init(BatchState* st, int* conv_at, int G, int max_iters, double rtol) {
+  for (int q = threadIdx.x; q < G; q += blockDim.x) conv_at[q] = -1;
+  if (threadIdx.x == 0) {
+    st->it = 0;
+    st->max_iters = max_iters;
+    st->all = 0;
+    st->rtol = rtol;
+  }
+}
+
+// The batch's residual test after step `it` (+1 inside the loop body): per group the worst
+// ||b_j - A u_j|| / ||b_j|| over its right-hand sides, the step at which it first reached rtol, and
+// the WHILE node's condition: not every group converged and fewer than max_iters steps.
+__global__ void __launch_bounds__(256) k_batch_check(cudaGraphConditionalHandle h, int G,
+                                                     const int32_t* __restrict__ meta, const double* __restrict__ n2,
+                                                     const double* __restrict__ bn2, BatchState* st, int* conv_at,
+                                                     double* worst, int step) {
+  __shared__ int all;
+  if (threadIdx.x == 0) all = 1;
+  __syncthreads();
+  const int it = st->it + step;
+  const double rtol = st->rtol;
+  for (int q = threadIdx.x; q < G; q += blockDim.x) {
+    const int off = meta[2 * q], nr = meta[2 * q + 1];
+    double wr = 0.0;
+    for (int j = 0; j < nr; ++j) {
+      const double r = sqrt(n2[off + j]), bn = sqrt(bn2[off + j]);
+      const double rel = bn > 0 ? r / bn : r;
+      wr = isfinite(rel) ? fmax(wr, rel) : HUGE_VAL;
+    }
+    worst[q] = wr;
+    if (conv_at[q] < 0 && wr <= rtol) conv_at[q] = it;
+    if (conv_at[q] < 0) atomicAnd(&all, 0);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    st->it = it;
+    st->all = all;
+    cudaGraphSetConditional(h, (!all && it < st->max_iters) ? 1u : 0u);
+  }
+}
+
+// Every group's branch of one phase on its own stream, forked from and joined back to bt.cap.
+template <class F>
+static void per_group(dec_batch& bt, F&& f) {
+  DEC_CUDA(cudaEventRecord(bt.fork, bt.cap));
+  for (size_t q = 0; q < bt.groups.size(); ++q) {
+    cudaStream_t st = bt.streams[q];
+    DEC_CUDA(cudaStreamWaitEvent(st, bt.fork, 0));
+    f(q, st);
+    DEC_CUDA(cudaEventRecord(bt.join[q], st));
+    DEC_CUDA(cudaStreamWaitEvent(bt.cap, bt.join[q], 0));
+  }
+}
+
+// The whole batched solve as one graph (caller buffers u / rhs baked in):
+//   per group: b and u into panels, e = 0, ||b||², r = b - A u and its norms;  test (step 0);
+//   WHILE (test): { per group: V-cycles, u += e, r = b - A u, norms;  test }
+//   per group: u out of panels.
+static cudaGraphExec_t batch_capture(dec_batch& bt, double* const* u, const double* const* rhs, const int* nrhs) {
   cudaGraph_t g = nullptr;
-  DEC_CUDA(cudaStreamBeginCapture(bt.cap, cudaStreamCaptureModeThreadLocal));
+  DEC_CUDA(cudaGraphCreate(&g, 0));
+  const int G = (int)bt.groups.size();
+  auto fail = [&]() {
+    cudaGraph_t junk = nullptr;
+    cudaStreamCaptureStatus cs;
+    if (cudaStreamIsCapturing(bt.cap, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+      cudaStreamEndCapture(bt.cap, &junk);
+    cudaGraphDestroy(g);
+  };
   try {
-    DEC_CUDA(cudaEventRecord(bt.fork, bt.cap));
-    for (size_t q = 0; q < bt.groups.size(); ++q) {
+    cudaGraphConditionalHandle h;
+    DEC_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+    DEC_CUDA(cudaStreamBeginCaptureToGraph(bt.cap, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    per_group(bt, [&](size_t q, cudaStream_t st) {
       dec_mg& mg = *bt.groups[q];
       Workspace& w = *bt.used[q];
-      cudaStream_t st = bt.streams[q];
-      DEC_CUDA(cudaStreamWaitEvent(st, bt.fork, 0));
-      if (kind == 1 && fused_update(mg, w)) {
+      const Level& F = mg.lv[0];
+      const int n = F.n, K = w.K, np = w.npanels;
+      to_panels(n, nrhs[q], K, np, F.diperm.p, rhs[q], w.B64.p, st);
+      to_panels(n, nrhs[q], K, np, F.diperm.p, u[q], w.U64.p, st);
+      zero_correction(mg, w, st);
+      enqueue_bnorms(mg, w, st, bt.bn2.p + bt.off[q]);
+      dispatch(mg, w, st, G_RESID);
+      DEC_CUDA(cudaMemcpyAsync(bt.norms.p + bt.off[q], w.norms.p, w.norms.bytes(), cudaMemcpyDeviceToDevice, st));
+    });
+    k_batch_check<<<1, 256, 0, bt.cap>>>(h, G, bt.meta.p, bt.norms.p, bt.bn2.p, bt.state.p, bt.conv_at.p,
+                                         bt.worst.p, 0);
+    DEC_CHECK_LAUNCH();
+    cudaStreamCaptureStatus cst;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    DEC_CUDA(cudaStreamGetCaptureInfo(bt.cap, &cst, nullptr, &cg, &deps, &ndeps));
+    cudaGraphNodeParams prm = {};
+    prm.type = cudaGraphNodeTypeConditional;
+    prm.conditional.handle = h;
+    prm.conditional.type = cudaGraphCondTypeWhile;
+    prm.conditional.size = 1;
+    cudaGraphNode_t loop_node;
+    DEC_CUDA(cudaGraphAddNode(&loop_node, cg, deps, ndeps, &prm));
+    DEC_CUDA(cudaStreamUpdateCaptureDependencies(bt.cap, &loop_node, 1, cudaStreamSetCaptureDependencies));
+    per_group(bt, [&](size_t q, cudaStream_t st) {
+      dec_mg& mg = *bt.groups[q];
+      Workspace& w = *bt.used[q];
+      const Level& F = mg.lv[0];
+      from_panels(F.n, nrhs[q], w.K, w.npanels, F.diperm.p, w.U64.p, u[q], st);
+    });
+    DEC_CUDA(cudaStreamEndCapture(bt.cap, &g));
+    cudaGraph_t body = prm.conditional.phGraph_out[0];
+    DEC_CUDA(cudaStreamBeginCaptureToGraph(bt.cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    per_group(bt, [&](size_t q, cudaStream_t st) {
+      dec_mg& mg = *bt.groups[q];
+      Workspace& w = *bt.used[q];
+      if (fused_update(mg, w)) {
         dispatch(mg, w, st, G_STEP);  // V-cycles with u += e in the last sweep, then the residual
       } else {
-        if (kind == 1) dispatch(mg, w, st, G_VCYCLE);
+        dispatch(mg, w, st, G_VCYCLE);
         dispatch(mg, w, st, G_RESID);
       }
       DEC_CUDA(cudaMemcpyAsync(bt.norms.p + bt.off[q], w.norms.p, w.norms.bytes(), cudaMemcpyDeviceToDevice, st));
-      DEC_CUDA(cudaEventRecord(bt.join[q], st));
-      DEC_CUDA(cudaStreamWaitEvent(bt.cap, bt.join[q], 0));
-    }
+    });
+    k_batch_check<<<1, 256, 0, bt.cap>>>(h, G, bt.meta.p, bt.norms.p, bt.bn2.p, bt.state.p, bt.conv_at.p,
+                                         bt.worst.p, 1);
+    DEC_CHECK_LAUNCH();
+    DEC_CUDA(cudaStreamEndCapture(bt.cap, &body));
+    bt.launches_pre = count_kernel_nodes(g);
+    bt.launches_body = count_kernel_nodes(body);
+    cudaGraphExec_t ex = nullptr;
+    DEC_CUDA(cudaGraphInstantiate(&ex, g, 0));
+    cudaGraphDestroy(g);
+    return ex;
   } catch (...) {
-    cudaStreamEndCapture(bt.cap, &g);
-    if (g) cudaGraphDestroy(g);
+    fail();
     throw;
   }
-  DEC_CUDA(cudaStreamEndCapture(bt.cap, &g));
-  bt.launches[kind] = count_kernel_nodes(g);
-  cudaGraphExec_t ex = nullptr;
-  cudaError_t err = cudaGraphInstantiate(&ex, g, 0);
-  cudaGraphDestroy(g);
-  DEC_CUDA(err);
-  return ex;
 }
 
 void batch_autotune(dec_batch* b, const int* nrhs, int reps, void* stream) {
@@ -3363,9 +3448,11 @@ dec_status batch_solve(dec_batch* b, double* const* u, const double* const* rhs,
   require(max_iters >= 1 && rtol > 0, "batch: bad max_iters / rtol");
   const size_t G = b->groups.size();
   cudaStream_t s = as_stream(stream);
-  // workspaces (autotuned panel widths), shifts, panels, initial e = 0
+  // workspaces (autotuned panel widths) and the graph's identity: any change recaptures it
   std::vector<Workspace*> ws(G);
   std::vector<uint64_t> ep(G);
+  std::vector<const void*> bufs(2 * G);
+  std::vector<int> nr(nrhs, nrhs + G);
   size_t nn = 0;
   std::vector<size_t> off(G);
   for (size_t q = 0; q < G; ++q) {
@@ -3375,93 +3462,44 @@ dec_status batch_solve(dec_batch* b, double* const* u, const double* const* rhs,
     ep[q] = mg.epoch;
     off[q] = nn;
     nn += ws[q]->norms.n;
+    bufs[2 * q] = u[q];
+    bufs[2 * q + 1] = rhs[q];
   }
-  if (ws != b->used || ep != b->epochs || b->off != off) {
+  if (ws != b->used || ep != b->epochs || b->off != off || bufs != b->bufs || nr != b->nrhs) {
     b->drop_graphs();
     b->used = ws;
     b->epochs = ep;
     b->off = off;
-    if (b->norms.n < nn) b->norms.alloc(nn);
+    b->bufs = bufs;
+    b->nrhs = nr;
+    if (b->norms.n < nn) {
+      b->norms.alloc(nn);
+      b->bn2.alloc(nn);
+    }
+    std::vector<int32_t> meta(2 * G);
+    for (size_t q = 0; q < G; ++q) {
+      meta[2 * q] = (int32_t)off[q];
+      meta[2 * q + 1] = nrhs[q];
+    }
+    b->meta.upload(meta);
   }
   cudaEvent_t e0, e1;
   DEC_CUDA(cudaEventCreate(&e0));
   DEC_CUDA(cudaEventCreate(&e1));
   DEC_CUDA(cudaEventRecord(e0, s));
-  std::vector<std::vector<double>> bn(G);
-  int64_t nl = 0;
-  for (size_t q = 0; q < G; ++q) {
-    dec_mg& mg = *b->groups[q];
-    Workspace& w = *ws[q];
-    set_shifts(mg, w, shifts ? shifts[q] : nullptr, nrhs[q], s);
-    const Level& F = mg.lv[0];
-    const int n = F.n, K = w.K, np = w.npanels;
-    const size_t tot = (size_t)n * K * np;
-    to_panels(n, nrhs[q], K, np, F.diperm.p, rhs[q], w.B64.p, s);
-    to_panels(n, nrhs[q], K, np, F.diperm.p, u[q], w.U64.p, s);
-    if (w.prec == 2) DEC_CUDA(cudaMemsetAsync(w.f16[0].x.p, 0, tot * sizeof(__half), s));
-    else if (w.prec == 1) DEC_CUDA(cudaMemsetAsync(w.f32[0].x.p, 0, tot * sizeof(float), s));
-    else DEC_CUDA(cudaMemsetAsync(w.f64[0].x.p, 0, tot * sizeof(double), s));
-    dim3 g(w.nblocks, np);
-    switch (K) {
-#define DEC_K(KK) \
-  case KK: k_panel_sumsq<KK><<<g, TB, 0, s>>>(n, w.B64.p, w.partial.p, (size_t)n * KK); break;
-      DEC_K(1) DEC_K(2) DEC_K(4) DEC_K(8) DEC_K(16) DEC_K(32)
-#undef DEC_K
-    }
-    k_reduce_partials<<<K * np, 256, 0, s>>>(w.nblocks, K, np, w.partial.p, b->norms.p + off[q]);
-    DEC_CHECK_LAUNCH();
-    nl += 5;
-  }
-  std::vector<double> hn(nn);
-  auto fetch = [&]() {
-    DEC_CUDA(cudaMemcpyAsync(hn.data(), b->norms.p, nn * sizeof(double), cudaMemcpyDeviceToHost, s));
-    DEC_CUDA(cudaStreamSynchronize(s));
-  };
-  fetch();
-  for (size_t q = 0; q < G; ++q) {
-    bn[q].resize(nrhs[q]);
-    for (int j = 0; j < nrhs[q]; ++j) bn[q][j] = std::sqrt(hn[off[q] + j]);
-  }
-  if (!b->graph[0]) b->graph[0] = batch_capture(*b, 0);
-  if (!b->graph[1]) b->graph[1] = batch_capture(*b, 1);
-  std::vector<double> worst(G, 0.0);
-  std::vector<int> conv_at(G, -1);
-  auto check = [&](int it) {
-    fetch();
-    bool all = true;
-    for (size_t q = 0; q < G; ++q) {
-      double wr = 0.0;
-      for (int j = 0; j < nrhs[q]; ++j) {
-        const double r = std::sqrt(hn[off[q] + j]);
-        const double rel = bn[q][j] > 0 ? r / bn[q][j] : r;
-        wr = std::isfinite(rel) ? std::max(wr, rel) : HUGE_VAL;
-      }
-      worst[q] = wr;
-      if (conv_at[q] < 0 && wr <= rtol) conv_at[q] = it;
-      all = all && conv_at[q] >= 0;
-    }
-    return all;
-  };
-  DEC_CUDA(cudaGraphLaunch(b->graph[0], s));
-  nl += b->launches[0];
-  int it = 0;
-  bool all = check(0);
-  while (!all && it < max_iters) {
-    DEC_CUDA(cudaGraphLaunch(b->graph[1], s));
-    nl += b->launches[1];
-    ++it;
-    all = check(it);
-  }
-  for (size_t q = 0; q < G; ++q) {
-    dec_mg& mg = *b->groups[q];
-    Workspace& w = *ws[q];
-    const Level& F = mg.lv[0];
-    from_panels(F.n, nrhs[q], w.K, w.npanels, F.diperm.p, w.U64.p, u[q], s);
-    ++nl;
-  }
+  for (size_t q = 0; q < G; ++q) set_shifts(*b->groups[q], *ws[q], shifts ? shifts[q] : nullptr, nrhs[q], s);
+  if (!b->graph) b->graph = batch_capture(*b, u, rhs, nrhs);
+  k_batch_init<<<1, 256, 0, s>>>(b->state.p, b->conv_at.p, (int)G, max_iters, rtol);
   DEC_CHECK_LAUNCH();
+  DEC_CUDA(cudaGraphLaunch(b->graph, s));
   DEC_CUDA(cudaEventRecord(e1, s));
-  DEC_CUDA(cudaEventSynchronize(e1));
+  BatchState st;
+  std::vector<int32_t> conv(G);
+  std::vector<double> worst(G);
+  DEC_CUDA(cudaMemcpyAsync(&st, b->state.p, sizeof(BatchState), cudaMemcpyDeviceToHost, s));
+  DEC_CUDA(cudaMemcpyAsync(conv.data(), b->conv_at.p, G * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  DEC_CUDA(cudaMemcpyAsync(worst.data(), b->worst.p, G * sizeof(double), cudaMemcpyDeviceToHost, s));
+  DEC_CUDA(cudaStreamSynchronize(s));
   float ms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
@@ -3470,8 +3508,8 @@ dec_status batch_solve(dec_batch* b, double* const* u, const double* const* rhs,
   for (size_t q = 0; q < G; ++q) {
     wmax = std::max(wmax, worst[q]);
     if (reps) {
-      reps[q].iterations = conv_at[q] >= 0 ? conv_at[q] : it;
-      reps[q].converged = conv_at[q] >= 0 ? 1 : 0;
+      reps[q].iterations = conv[q] >= 0 ? conv[q] : st.it;
+      reps[q].converged = conv[q] >= 0 ? 1 : 0;
       reps[q].max_rel_residual = worst[q];
       reps[q].seconds = ms * 1e-3;
       reps[q].launches = 0;
@@ -3480,15 +3518,15 @@ dec_status batch_solve(dec_batch* b, double* const* u, const double* const* rhs,
     }
   }
   if (total) {
-    total->iterations = it;
-    total->converged = all ? 1 : 0;
+    total->iterations = st.it;
+    total->converged = st.all ? 1 : 0;
     total->max_rel_residual = wmax;
     total->seconds = ms * 1e-3;
-    total->launches = nl;
+    total->launches = 1 + b->launches_pre + (int64_t)st.it * b->launches_body;  // init kernel, graph
     total->rhs_block = 0;
     total->fallback_iteration = -1;
   }
-  return all ? DEC_OK : DEC_ERR_NOT_CONVERGED;
+  return st.all ? DEC_OK : DEC_ERR_NOT_CONVERGED;
 }
 
 }  // namespace decb

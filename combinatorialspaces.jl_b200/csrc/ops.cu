@@ -929,6 +929,7 @@ void op_export_csr_impl(const dec_op* op, int64_t* nnz, int32_t* rowptr, int32_t
   auto push = [&](int c, double v) { ci.push_back(c); vv.push_back(v); };
   switch (op->kind) {
     case DEC_OP_D0:
+      m.ensure_host();
       for (int e = 0; e < m.ne; ++e) {
         double s = m.h_eo[e] ? 1.0 : -1.0;
         int a = m.h_ev0[e], b = m.h_ev1[e];

@@ -317,9 +317,12 @@ dec_status dec_mg_solve_shifted(dec_mg* mg, double* u, const double* b, int32_t 
                                 double rtol, int32_t max_iters, dec_solve_report* report, void* stream);
 
 /* ---- batched solves over several hierarchies (meshes of uneven sizes; no counterpart in the
- *      reference): every refinement step of all groups is one CUDA graph with a concurrent branch
- *      per group (FP32 or FP64 V-cycles per each hierarchy's options, FP64 refinement), one
- *      residual-norm read-back per step for all groups.  Groups use the Jacobi or Chebyshev smoother.
+ *      reference): the whole solve of all groups is one CUDA graph -- a concurrent branch per group
+ *      (FP32 or FP64 V-cycles per each hierarchy's options, FP64 refinement) and the refinement loop
+ *      as a conditional WHILE node that a residual-test kernel over all groups sets, so a batch is one
+ *      graph launch and one read-back of the loop state.  The graph holds the caller's u / rhs
+ *      pointers: it is reused while a call passes the same buffers and sizes, and rebuilt otherwise.
+ *      Groups use the Jacobi or Chebyshev smoother.
  * ------------------------------------------------------------------------------------------ */
 /* The hierarchies are not owned and must outlive the batch. */
 dec_status dec_batch_create(dec_mg* const* groups, int32_t ngroups, dec_batch** out);

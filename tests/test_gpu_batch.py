@@ -117,6 +117,16 @@ def test_batch_over_uneven_meshes(O, dec):
             U1 = torch.zeros_like(Us[q])
             mg.solve(U1, torch.tensor(Bs[q], device="cuda"), rtol=1e-30, max_iters=tot.iterations, shifts=shifts[q])
             np.testing.assert_array_equal(U1.cpu().numpy(), Us[q].cpu().numpy())
+    # the batch is one graph launch: its kernels are the graph's nodes outside the loop plus the
+    # loop body's per step, and new caller buffers rebuild the graph with the same result
+    again = [torch.zeros_like(U) for U in Us]
+    reps2, tot2 = batch.solve(again, [torch.tensor(B, device="cuda") for B in Bs], shifts=shifts, rtol=1e-9)
+    assert tot2.iterations == tot.iterations and tot2.launches == tot.launches
+    for q in range(3):
+        np.testing.assert_array_equal(again[q].cpu().numpy(), Us[q].cpu().numpy())
+    capped, totc = batch.solve([torch.zeros_like(U) for U in Us], [torch.tensor(B, device="cuda") for B in Bs],
+                               shifts=shifts, rtol=1e-30, max_iters=2)
+    assert totc.converged == 0 and totc.iterations == 2
 
 
 @pytest.mark.parametrize("kind,m,n", [("pp", 0, 1), ("pp", 1, 0), ("pp", 0, 2), ("pp", 2, 0), ("pp", 1, 1),
