@@ -273,7 +273,7 @@ def test_residual_norms(O, dec, cases, name):
     ref_b = np.linalg.norm(B, axis=1)
     np.testing.assert_allclose(r, ref_r, rtol=1e-12)
     np.testing.assert_allclose(bn, ref_b, rtol=1e-13)
-    with pytest.raises(dec.DecError, match="Laplacian or a Helmholtz"):
+    with pytest.raises(dec.DecError, match="Laplacian, a Helmholtz operator or a square matrix"):
         dec.dec_differential(0, g).residual_norms(cuda(X), cuda(B))   # rejected before any device work
 
 
