@@ -126,7 +126,31 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def measure_operators(dec, peak):
+def cpu_operator_baseline(reps=100):
+    """The plain-operator workload on the host cores: the oracle's statement of the reference's CPU
+    kernels (FastDEC's wedge kernels, SparseArrays' products) on the 128 x 128 grid, µs per operation,
+    on one thread and on every host thread (a thread per slice of rows, started per call)."""
+    sys.path.insert(0, str(ROOT))
+    import oracle
+    O = oracle.load()
+    m = O.triangulated_grid(127, 127, 1.0, 1.0, compress=False)
+    d = O.dualize(m, O.BARYCENTER)
+    dec = load_package()
+    f, a, b = dec.meshes.uniform(0, d.nv), dec.meshes.uniform(1, d.ne), dec.meshes.uniform(2, d.ne)
+    out = {}
+    for threads in sorted({1, os.cpu_count() or 1}):
+        O.set_num_threads(threads)
+        t = O.time_operators(d, f, a, b, reps)
+        out[f"{threads}_threads"] = {"wedge01(f,alpha)": round(t["wedge01"] * 1e6, 2),
+                                     "wedge11(alpha,beta)": round(t["wedge11"] * 1e6, 2),
+                                     "wedge02(f,d1 alpha)": round(t["wedge02_d1"] * 1e6, 2),
+                                     "laplacian f": round(t["laplacian"] * 1e6, 2)}
+    O.set_num_threads(1)
+    out["kind"] = "port (the oracle's C++ statement, -O2; µs per operation, mean of 100 after one warm-up)"
+    return out
+
+
+def measure_operators(dec, peak, cpu=True):
     """HBM roofline of the DEC operator kernels: each kernel timed alone with CUDA events, L2
     flushed before every launch by reading a 256 MB buffer (a read leaves L2 holding clean lines,
     so the timed kernel pays no write-back of the flush), on icosphere L9 (circumcentric duals) and a
@@ -220,6 +244,8 @@ def measure_operators(dec, peak):
         torch.cuda.synchronize()
         grid_ops[name] = round(e0.elapsed_time(e1) * 10, 2)  # µs per op (ms / 100 * 1000)
     out["grid_128x128_us_per_op"] = grid_ops
+    if cpu:
+        out["grid_128x128_cpu_us_per_op"] = cpu_operator_baseline()
     return out
 
 
@@ -787,7 +813,7 @@ def run_ours(args):
     learned_res = measure_learned(dec, args, B, U64, common, timed) if args.train_steps > 0 else None
 
     # --- DEC operator kernels (wedges, d, star, Laplacian) at full size ---
-    operators = measure_operators(dec, peak) if (rank == 0 and not args.no_ops) else None
+    operators = measure_operators(dec, peak, cpu=not args.no_cpu) if (rank == 0 and not args.no_ops) else None
 
     # --- CPU baseline (rank 0, N = 1 only): the reference algorithm on the host cores ---
     cpu = None

@@ -206,6 +206,35 @@ PYBIND11_MODULE(dec_oracle, mod) {
     return std::chrono::duration<double>(t1 - t0).count() / reps;
   });
 
+  mod.def("time_operators", [](const Dual& d, py::array_t<double, py::array::c_style | py::array::forcecast> f,
+                                py::array_t<double, py::array::c_style | py::array::forcecast> a,
+                                py::array_t<double, py::array::c_style | py::array::forcecast> b, int reps) {
+    // Seconds per evaluation on the current thread count (caches and matrices built once, outside
+    // the timing): ∧(0,1)(f, α), ∧(1,1)(α, β), ∧(0,2)(f, d1 α) (the d1 SpMV, then the wedge) and
+    // Δ0 f = L f (the Laplacian SpMV: SparseArrays' column-order product on one thread, rows in
+    // parallel on several).
+    auto c02 = wedge02_cache(d);
+    auto c11 = wedge11_cache(d);
+    CSC d1 = dec_differential(d, 1), L = laplace_beltrami0(d);
+    CSC d1t = transpose(d1), Lt = transpose(L);
+    std::vector<double> oe(d.ne), ot(d.nt), ov(d.nv), t1(d.nt);
+    auto time = [&](auto fn) {
+      fn();
+      auto t0 = std::chrono::steady_clock::now();
+      for (int r = 0; r < reps; ++r) fn();
+      auto t1c = std::chrono::steady_clock::now();
+      return std::chrono::duration<double>(t1c - t0).count() / reps;
+    };
+    py::dict out;
+    out["wedge01"] = time([&] { wedge01<double>(d, f.data(), a.data(), oe.data()); });
+    out["wedge11"] = time([&] { wedge11<double>(d, c11, a.data(), b.data(), ot.data()); });
+    out["wedge02_d1"] = time([&] {
+      apply(d1, &d1t, a.data(), t1.data());
+      wedge02<double>(d, c02, f.data(), t1.data(), ot.data());
+    });
+    out["laplacian"] = time([&] { apply(L, &Lt, f.data(), ov.data()); });
+    return out;
+  });
   mod.def("csc_matvec", [](py::tuple t, py::array_t<double, py::array::c_style | py::array::forcecast> x) {
     // y = A x in the column order of the reference's SparseMatrixCSC SpMV
     CSC a;
