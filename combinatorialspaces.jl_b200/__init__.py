@@ -282,6 +282,13 @@ class Operator:
                                           bn.ctypes.data_as(C.POINTER(C.c_double)), _stream()))
         return r, bn
 
+    def autotune(self, reps=10):
+        """Time the apply's rows-per-thread variants and record the fastest in the tuning table
+        (dec_op_autotune); returns the choice (0: this operator's kernel has no variants)."""
+        c = C.c_int32()
+        check(lib().dec_op_autotune(self._h, reps, _stream(), C.byref(c)))
+        return c.value
+
     def csr(self):
         """(indptr, indices, data, shape) of the operator, exported to the host."""
         nnz = C.c_int64()
@@ -321,6 +328,34 @@ def sparse_operator(A, dtype="float64", index_base=0):
     h = C.c_void_p()
     check(lib().dec_op_create_csc(C.byref(c), _dtype_code(dtype), C.byref(h)))
     return Operator(None, 0, handle=h, owned=True, code=_dtype_code(dtype))
+
+
+def tune_set(key, value):
+    """Set an entry of the autotuner's table (dec_tune_set)."""
+    check(lib().dec_tune_set(key.encode(), int(value)))
+
+
+def tune_get(key):
+    """The tuning table's entry for `key`, or None (dec_tune_get)."""
+    v, found = C.c_int32(), C.c_int32()
+    check(lib().dec_tune_get(key.encode(), C.byref(v), C.byref(found)))
+    return v.value if found.value else None
+
+
+def tune_clear():
+    check(lib().dec_tune_clear())
+
+
+def tune_save(path):
+    """Write the autotuner's table as JSON (dec_tune_save)."""
+    check(lib().dec_tune_save(str(path).encode()))
+
+
+def tune_load(path):
+    """Merge a saved tuning table into the current one; returns the entries read (dec_tune_load)."""
+    n = C.c_int32()
+    check(lib().dec_tune_load(str(path).encode(), C.byref(n)))
+    return n.value
 
 
 def dec_differential(n, sd, dtype="float64"):

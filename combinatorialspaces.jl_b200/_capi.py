@@ -99,6 +99,12 @@ SIGNATURES = {
     "dec_mg_time_kernel": (I32, [P, I32, I32, I32, I32, P, PF64, PF64]),
     "dec_mg_autotune": (I32, [P, I32, I32, P, C.POINTER(C.c_int32)]),
     "dec_mg_solve_traffic": (I32, [P, I32, I32, I32, PF64]),
+    "dec_op_autotune": (I32, [P, I32, P, C.POINTER(C.c_int32)]),
+    "dec_tune_set": (I32, [C.c_char_p, I32]),
+    "dec_tune_get": (I32, [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "dec_tune_clear": (I32, []),
+    "dec_tune_save": (I32, [C.c_char_p]),
+    "dec_tune_load": (I32, [C.c_char_p, C.POINTER(C.c_int32)]),
     "dec_mg_set_smoother_mlp": (I32, [P, P]),
     "dec_mg_solve_shifted": (I32, [P, P, P, I32, P, F64, I32, C.POINTER(SolveReport), P]),
     "dec_batch_create": (I32, [P, I32, PP]),

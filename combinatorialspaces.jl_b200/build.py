@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", f"-I{INCLUDE}", f"-I{CSRC}",
           "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 EXACT = {"mesh.cu", "wedge.cu", "ops.cu"}   # no FMA contraction
-SOURCES = ["mesh.cu", "wedge.cu", "ops.cu", "mg.cu", "mlp.cu", "capi.cpp"]
+SOURCES = ["mesh.cu", "wedge.cu", "ops.cu", "mg.cu", "mlp.cu", "tune.cpp", "capi.cpp"]
 
 
 def nvcc() -> str:

@@ -9,6 +9,7 @@
 #include "mesh.cuh"
 #include "mg.cuh"
 #include "ops.cuh"
+#include "tune.cuh"
 
 // Implementations (wedge.cu, ops.cu).
 dec_wedge_plan* wedge_plan_create_impl(dec_mesh* mh, int kind, int da, int db, dec_dtype dt);
@@ -39,6 +40,7 @@ void mlp_load_impl(dec_mlp* m, const char* path);
 void op_residual_norms_noalloc_impl(dec_op* op, const double* x, const double* b, int nrhs, double* norms,
                                     double* bnorms, void* stream);
 dec_op* op_create_csc_impl(const dec_csc* a, dec_dtype dt);
+int op_autotune_impl(dec_op* op, int reps, void* stream);
 
 namespace {
 thread_local std::string g_err;
@@ -308,6 +310,49 @@ dec_status dec_mg_solve_traffic(dec_mg* mg, int32_t nrhs, int32_t from_zero, int
   return guard([&] {
     double b = decb::mg_solve_traffic(mg, nrhs, from_zero, iterations);
     if (bytes) *bytes = b;
+  });
+}
+
+dec_status dec_op_autotune(dec_op* op, int32_t reps, void* stream, int32_t* choice) {
+  return guard([&] {
+    int c = op_autotune_impl(op, reps, stream);
+    if (choice) *choice = c;
+  });
+}
+
+dec_status dec_tune_set(const char* key, int32_t value) {
+  return guard([&] {
+    decb::require(key != nullptr && key[0] != 0, "dec_tune_set: empty key");
+    decb::tune_set(key, value);
+  });
+}
+
+dec_status dec_tune_get(const char* key, int32_t* value, int32_t* found) {
+  return guard([&] {
+    decb::require(key != nullptr && value != nullptr && found != nullptr, "dec_tune_get: null argument");
+    constexpr int kMissing = -2147483647 - 1;
+    const int v = decb::tune_get(key, kMissing);
+    *found = v != kMissing;
+    if (*found) *value = v;
+  });
+}
+
+dec_status dec_tune_clear(void) {
+  return guard([&] { decb::tune_clear(); });
+}
+
+dec_status dec_tune_save(const char* path) {
+  return guard([&] {
+    decb::require(path != nullptr, "dec_tune_save: null path");
+    decb::tune_save(path);
+  });
+}
+
+dec_status dec_tune_load(const char* path, int32_t* entries) {
+  return guard([&] {
+    decb::require(path != nullptr, "dec_tune_load: null path");
+    const int n = decb::tune_load(path);
+    if (entries) *entries = n;
   });
 }
 

@@ -33,6 +33,7 @@
 
 #include "mg.cuh"
 #include "mlp.cuh"
+#include "tune.cuh"
 
 dec_op* op_create_impl(dec_mesh* mh, int kind, double shift, dec_dtype dt);
 dec_op* op_from_csr_impl(dec_mesh* mh, int n, const std::vector<int32_t>& rowptr, const std::vector<int32_t>& colind,
@@ -318,9 +319,12 @@ static inline void add_bytes(double b) {
   if (t_bytes) *t_bytes += b;
 }
 
-template <class T, int K>
+// VV > 0 overrides the vector width (a tuned variant: VV = 2 on FP32 panels of K >= 8 puts twice the
+// lanes on a row).
+template <class T, int K, int VV = 0>
 struct Lanes {
-  static constexpr int V = std::is_same<T, float>::value    ? (K >= 4 ? 4 : K)
+  static constexpr int V = VV > 0 ? VV
+                           : std::is_same<T, float>::value  ? (K >= 4 ? 4 : K)
                            : std::is_same<T, __half>::value ? (K >= 8 ? 8 : K)
                                                             : (K >= 2 ? 2 : 1);
   static constexpr int LPR = K / V;        // lanes per row
@@ -338,14 +342,14 @@ struct Lanes {
 // SH: right-hand side j of panel p has its own operator A + cs[p*K + j] I (D likewise).
 // UPD: the sweep's result is the refinement step's correction e, added straight to the FP64
 // iterate (u += (double) e, the update pass's arithmetic) instead of being stored in out.
-template <class T, int K, int W, bool SH, bool UPD = false>
+template <class T, int K, int W, bool SH, bool UPD = false, int VV = 0>
 __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restrict__ col,
                                            const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
                                            const CT<T>* __restrict__ dinv, const T* __restrict__ b,
                                            const T* __restrict__ x, T* __restrict__ out, const SweepPrm<CT<T>>& prm,
                                            size_t pstride, const CT<T>* __restrict__ shf,
                                            double* __restrict__ u64 = nullptr) {
-  using Ln = Lanes<T, K>;
+  using Ln = Lanes<T, K, VV>;
   using C = CT<T>;
   pdl_enter();
   constexpr int V = Ln::V;
@@ -446,25 +450,25 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
   }
 }
 
-template <class T, int K, int W, bool SH>
+template <class T, int K, int W, bool SH, int VV = 0>
 __global__ void __launch_bounds__(TB) k_sweep(int n, int Wr, const int32_t* __restrict__ col,
                                               const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
                                               const CT<T>* __restrict__ dinv, const T* __restrict__ b,
                                               const T* __restrict__ x, T* __restrict__ out,
                                               SweepPrm<CT<T>> prm, size_t pstride, const CT<T>* __restrict__ shf) {
-  sweep_rows<T, K, W, SH>(n, Wr, col, off, diag, dinv, b, x, out, prm, pstride, shf);
+  sweep_rows<T, K, W, SH, false, VV>(n, Wr, col, off, diag, dinv, b, x, out, prm, pstride, shf);
 }
 
 // The last sweep of a refinement step's V-cycles on the finest level with the step's update
 // u += e fused in (FP32 / FP64 storage).
-template <class T, int K, int W, bool SH>
+template <class T, int K, int W, bool SH, int VV = 0>
 __global__ void __launch_bounds__(TB) k_sweep_u(int n, int Wr, const int32_t* __restrict__ col,
                                                 const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
                                                 const CT<T>* __restrict__ dinv, const T* __restrict__ b,
                                                 const T* __restrict__ x, T* __restrict__ out,
                                                 SweepPrm<CT<T>> prm, size_t pstride, const CT<T>* __restrict__ shf,
                                                 double* __restrict__ u64) {
-  sweep_rows<T, K, W, SH, true>(n, Wr, col, off, diag, dinv, b, x, out, prm, pstride, shf, u64);
+  sweep_rows<T, K, W, SH, true, VV>(n, Wr, col, off, diag, dinv, b, x, out, prm, pstride, shf, u64);
 }
 
 // FP16-stored sweeps carry eight values per 16-byte access; unbounded they took 72 registers
@@ -1277,6 +1281,9 @@ struct Level {
   DArr<int32_t> rcol, pcol;
   DArr<double> rval64, pval64;
   DArr<float> rval32, pval32;
+  // tuned FP32 sweep variant per panel width 8 / 16 / 32 (index 3 / 4 / 5), cached per table version
+  mutable unsigned sweep_tuned_at[6] = {0, 0, 0, 0, 0, 0};
+  mutable int sweep_vv[6] = {0, 0, 0, 0, 0, 0};
 };
 
 template <class T>
@@ -2033,6 +2040,60 @@ static void launch_prolong(const Level& L, const Level& Cl, const T* z, T* x, bo
     kern<<<g, TB, 0, s>>>(L.n, L.pa.p, L.pb.p, z, x, fs, cs);
 }
 
+// Tuning key of the FP32 sweep's lanes per row (panel widths of 8 or more: vector width 4, the
+// default, or 2, twice the lanes on a row), per panel width, row width and size bucket.
+static std::string sweep_key(int K, int W, int n) {
+  return "sweep/f32/K" + std::to_string(K) + "/W" + std::to_string(W) + "/n" + std::to_string(size_bucket(n));
+}
+
+// The tuned vector width override of level L's FP32 sweep at panel width K (0: the default),
+// looked up once per change of the tuning table.
+template <int K>
+static int sweep_variant(const Level& L) {
+  constexpr int k = K >= 32 ? 5 : K >= 16 ? 4 : 3;
+  if (L.sweep_tuned_at[k] != tune_version()) {
+    L.sweep_tuned_at[k] = tune_version();
+    const int v = tune_get(sweep_key(K, L.W, L.n), 4);
+    L.sweep_vv[k] = v == 2 ? 2 : 0;
+  }
+  return L.sweep_vv[k];
+}
+
+template <class T, int K, int VV>
+static void launch_sweep_fp(const Level& L, const T* b, const T* x, T* out, SweepPrm<CT<T>> prm, int np,
+                            cudaStream_t s, const CT<T>* cs, double* upd) {
+  size_t ps = (size_t)L.n * K;
+  const dim3 grid(grid_for((long long)L.n, Lanes<T, K, VV>::RPB, 8), np);
+  const CT<T>* off = pick<T>(L.off64, L.off32);
+  const CT<T>* dg = pick<T>(L.diag64, L.diag32);
+  const CT<T>* di = pick<T>(L.dinv64, L.dinv32);
+  if (upd) {  // u += (this sweep's result); out is not written
+    auto go = [&](auto kern) {
+      launch_pdl(kern, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs, upd);
+    };
+    if (cs) {
+      if (L.W == 6) go(k_sweep_u<T, K, 6, true, VV>);
+      else go(k_sweep_u<T, K, 0, true, VV>);
+    } else if (L.W == 6) {
+      go(k_sweep_u<T, K, 6, false, VV>);
+    } else {
+      go(k_sweep_u<T, K, 0, false, VV>);
+    }
+  } else {
+    auto go = [&](auto kern) {
+      launch_pdl(kern, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs);
+    };
+    if (cs) {
+      if (L.W == 6) go(k_sweep<T, K, 6, true, VV>);
+      else go(k_sweep<T, K, 0, true, VV>);
+    } else if (L.W == 6) {
+      go(k_sweep<T, K, 6, false, VV>);
+    } else {
+      go(k_sweep<T, K, 0, false, VV>);
+    }
+  }
+}
+
 template <class T, int K>
 static void launch_sweep(const Level& L, const T* b, const T* x, T* out, SweepPrm<CT<T>> prm, int np,
                          cudaStream_t s, const CT<T>* cs, double* upd = nullptr) {
@@ -2061,31 +2122,13 @@ static void launch_sweep(const Level& L, const T* b, const T* x, T* out, SweepPr
       launch_pdl(k_sweep_h<K, 0, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs);
     }
   } else {
-    const CT<T>* off = pick<T>(L.off64, L.off32);
-    const CT<T>* dg = pick<T>(L.diag64, L.diag32);
-    const CT<T>* di = pick<T>(L.dinv64, L.dinv32);
-    if (upd) {  // u += (this sweep's result); out is not written
-      auto go = [&](auto kern) {
-        launch_pdl(kern, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs, upd);
-      };
-      if (cs) {
-        if (L.W == 6) go(k_sweep_u<T, K, 6, true>);
-        else go(k_sweep_u<T, K, 0, true>);
-      } else if (L.W == 6) {
-        go(k_sweep_u<T, K, 6, false>);
-      } else {
-        go(k_sweep_u<T, K, 0, false>);
+    if constexpr (std::is_same<T, float>::value && K >= 8) {
+      if (sweep_variant<K>(L) == 2) {
+        launch_sweep_fp<T, K, 2>(L, b, x, out, prm, np, s, cs, upd);
+        return;
       }
-    } else if (cs) {
-      if (L.W == 6)
-        launch_pdl(k_sweep<T, K, 6, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs);
-      else
-        launch_pdl(k_sweep<T, K, 0, true>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs);
-    } else if (L.W == 6) {
-      launch_pdl(k_sweep<T, K, 6, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs);
-    } else {
-      launch_pdl(k_sweep<T, K, 0, false>, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs);
     }
+    launch_sweep_fp<T, K, 0>(L, b, x, out, prm, np, s, cs, upd);
   }
 }
 
@@ -3209,6 +3252,38 @@ int mg_autotune(dec_mg* mg, int nrhs, int reps, void* stream) {
       best_t = t;
       best = K;
     }
+  }
+  // FP32 panels of 8 or more: the sweep's lanes per row (vector width 4, the default, or 2), timed
+  // on the same V-cycle with the variant on every level, kept in the tuning table per level
+  if (prec == 1 && best >= 8) {
+    Workspace& w = workspace_k(*mg, nrhs, prec, best);
+    auto set_all = [&](int v) {
+      for (const Level& L : mg->lv) tune_set(sweep_key(best, L.W, L.n), v);
+      w.drop_graphs();
+    };
+    int best_v = 4;
+    double best_vt = 1e300;
+    for (int v : {4, 2}) {
+      set_all(v);
+      w.graph[G_VCYCLE] = capture(*mg, w, G_VCYCLE);
+      DEC_CUDA(cudaGraphLaunch(w.graph[G_VCYCLE], s));
+      std::vector<float> ts;
+      for (int r = 0; r < std::max(3, reps); ++r) {
+        DEC_CUDA(cudaEventRecord(e0, s));
+        DEC_CUDA(cudaGraphLaunch(w.graph[G_VCYCLE], s));
+        DEC_CUDA(cudaEventRecord(e1, s));
+        DEC_CUDA(cudaEventSynchronize(e1));
+        float t = 0;
+        cudaEventElapsedTime(&t, e0, e1);
+        ts.push_back(t);
+      }
+      std::sort(ts.begin(), ts.end());
+      if (ts[ts.size() / 2] < best_vt) {
+        best_vt = ts[ts.size() / 2];
+        best_v = v;
+      }
+    }
+    set_all(best_v);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

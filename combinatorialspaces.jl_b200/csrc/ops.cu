@@ -13,6 +13,7 @@
 
 #include "mesh.cuh"
 #include "ops.cuh"
+#include "tune.cuh"
 
 namespace decb {
 
@@ -248,6 +249,42 @@ __global__ void __launch_bounds__(kOpThreads) k_ell(int n, int W, const int32_t*
       }
     }
     y[i] = epilogue(s, hb ? y[i] : T(0), alpha, beta, hb);
+  }
+}
+
+// The same with R rows per thread, a block apart (FP32: half the bytes per row of FP64, so a thread
+// keeps two rows' loads in flight); every row sums in slot order as above.
+template <class T, int WC, int R>
+__global__ void __launch_bounds__(kOpThreads) k_ell_rows(int n, const int32_t* __restrict__ col,
+                                                         const T* __restrict__ val, const T* __restrict__ x,
+                                                         T* __restrict__ y, T alpha, T beta, bool hb) {
+  for (long long base = (long long)blockIdx.x * blockDim.x * R + threadIdx.x; base < n;
+       base += (long long)gridDim.x * blockDim.x * R) {
+    int c[R][WC];
+    T v[R][WC], g[R][WC];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const long long i = base + (long long)r * blockDim.x;
+#pragma unroll
+      for (int q = 0; q < WC; ++q) {
+        c[r][q] = i < n ? __ldcs(col + (size_t)q * n + i) : -1;
+        v[r][q] = i < n ? __ldcs(val + (size_t)q * n + i) : T(0);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int q = 0; q < WC; ++q) g[r][q] = c[r][q] >= 0 ? __ldg(x + c[r][q]) : T(0);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const long long i = base + (long long)r * blockDim.x;
+      if (i >= n) break;
+      T s = T(0);
+#pragma unroll
+      for (int q = 0; q < WC; ++q)
+        if (c[r][q] >= 0) s += v[r][q] * g[r][q];
+      y[i] = epilogue(s, hb ? y[i] : T(0), alpha, beta, hb);
+    }
   }
 }
 
@@ -615,10 +652,20 @@ template void cast_array<float>(const DArr<double>&, DArr<float>&);
 
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
+// Tuning key of the ELL apply: rows-per-thread variants exist for rows of 7 slots (the Laplacian /
+// Helmholtz operators of triangle meshes), per dtype and size bucket.
+static std::string ell_key(int n, int W, bool f32) {
+  return std::string("ell/") + (f32 ? "f32" : "f64") + "/W" + std::to_string(W) + "/n" + std::to_string(size_bucket(n));
+}
+
 template <class T>
 static void launch_ell(int n, int W, const int32_t* col, const T* val, const T* x, T* y, T a, T b, bool hb,
-                       cudaStream_t s) {
-  if (W == 7) k_ell<T, 7><<<grid_for(n, kOpThreads), kOpThreads, 0, s>>>(n, W, col, val, x, y, a, b, hb);
+                       cudaStream_t s, int rows = 1) {
+  if (W == 7 && rows == 2)
+    k_ell_rows<T, 7, 2><<<grid_for(n, kOpThreads * 2), kOpThreads, 0, s>>>(n, col, val, x, y, a, b, hb);
+  else if (W == 7 && rows == 4)
+    k_ell_rows<T, 7, 4><<<grid_for(n, kOpThreads * 4), kOpThreads, 0, s>>>(n, col, val, x, y, a, b, hb);
+  else if (W == 7) k_ell<T, 7><<<grid_for(n, kOpThreads), kOpThreads, 0, s>>>(n, W, col, val, x, y, a, b, hb);
   else if (W == 6) k_ell<T, 6><<<grid_for(n, kOpThreads), kOpThreads, 0, s>>>(n, W, col, val, x, y, a, b, hb);
   else k_ell<T, 0><<<grid_for(n, kOpThreads), kOpThreads, 0, s>>>(n, W, col, val, x, y, a, b, hb);
 }
@@ -712,9 +759,13 @@ static void launch_op(const dec_op& op, const void* vx, void* vy, double alpha, 
   T* y = (T*)vy;
   const T a = (T)alpha, b = (T)beta;
   const bool hb = beta != 0.0;
+  if (op.W == 7 && op.tuned_at != tune_version()) {  // the table changed since the last lookup
+    op.tuned_at = tune_version();
+    op.ell_rows = tune_get(ell_key((int)op.rows, op.W, std::is_same<T, float>::value), 1);
+  }
   if (op.kind == DEC_OP_GENERAL) {  // a caller's matrix: no mesh
     const T* val = std::is_same<T, double>::value ? (const T*)op.val64.p : (const T*)op.val32.p;
-    if (op.rows) launch_ell<T>((int)op.rows, op.W, op.col.p, val, x, y, a, b, hb, s);
+    if (op.rows) launch_ell<T>((int)op.rows, op.W, op.col.p, val, x, y, a, b, hb, s, op.ell_rows);
     DEC_CHECK_LAUNCH();
     return;
   }
@@ -752,7 +803,7 @@ static void launch_op(const dec_op& op, const void* vx, void* vy, double alpha, 
     case DEC_OP_STAR1_GEOMETRIC:
     case DEC_OP_FLAT_SHARP: {
       const T* val = std::is_same<T, double>::value ? (const T*)op.val64.p : (const T*)op.val32.p;
-      if (op.rows) launch_ell<T>((int)op.rows, op.W, op.col.p, val, x, y, a, b, hb, s);
+      if (op.rows) launch_ell<T>((int)op.rows, op.W, op.col.p, val, x, y, a, b, hb, s, op.ell_rows);
       break;
     }
     case DEC_OP_INV_STAR1_GEOMETRIC:
@@ -917,6 +968,52 @@ void op_apply_impl(dec_op* op, const void* x, void* y, double alpha, double beta
   require(op != nullptr && x != nullptr && y != nullptr, "op: null argument");
   if (op->dtype == DEC_F64) launch_op<double>(*op, x, y, alpha, beta, as_stream(stream));
   else launch_op<float>(*op, x, y, alpha, beta, as_stream(stream));
+}
+
+// Times each rows-per-thread variant of the operator's ELL apply (rows of 7 slots) on scratch
+// vectors and records the fastest in the tuning table; returns the chosen rows per thread, or 0 when
+// the operator's kernel has no variants.
+int op_autotune_impl(dec_op* op, int reps, void* stream) {
+  require(op != nullptr && reps >= 1, "op autotune: bad arguments");
+  const bool ell = op->kind == DEC_OP_LAPLACE0 || op->kind == DEC_OP_HELMHOLTZ0 || op->kind == DEC_OP_GENERAL ||
+                   op->kind == DEC_OP_STAR1_GEOMETRIC || op->kind == DEC_OP_FLAT_SHARP;
+  if (!ell || op->W != 7 || op->rows == 0) return 0;
+  cudaStream_t s = as_stream(stream);
+  const bool f32 = op->dtype == DEC_F32;
+  const size_t es = f32 ? 4 : 8;
+  DArr<unsigned char> xb((size_t)op->cols * es), yb((size_t)op->rows * es);
+  DEC_CUDA(cudaMemsetAsync(xb.p, 0, xb.bytes(), s));
+  cudaEvent_t e0, e1;
+  DEC_CUDA(cudaEventCreate(&e0));
+  DEC_CUDA(cudaEventCreate(&e1));
+  const int n = (int)op->rows;
+  int best = 1;
+  float best_ms = 1e30f;
+  for (int rows : {1, 2, 4}) {
+    auto go = [&]() {
+      if (f32)
+        launch_ell<float>(n, op->W, op->col.p, op->val32.p, (const float*)xb.p, (float*)yb.p, 1.f, 0.f, false, s, rows);
+      else
+        launch_ell<double>(n, op->W, op->col.p, op->val64.p, (const double*)xb.p, (double*)yb.p, 1.0, 0.0, false, s,
+                           rows);
+    };
+    go();
+    DEC_CUDA(cudaEventRecord(e0, s));
+    for (int r = 0; r < reps; ++r) go();
+    DEC_CUDA(cudaEventRecord(e1, s));
+    DEC_CHECK_LAUNCH();
+    DEC_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = rows;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  tune_set(ell_key(n, op->W, f32), best);
+  return best;
 }
 
 // CSR of the operator on the host (exact integers for d / ∂ / dual d).

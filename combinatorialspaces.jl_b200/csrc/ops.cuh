@@ -15,6 +15,8 @@ struct dec_op {
   decb::DArr<double> val64;
   decb::DArr<float> val32;
   decb::DArr<double> kry;     // inverse geometric ⋆1: Krylov vectors, 1/diag and reduction scratch
+  mutable unsigned tuned_at = 0;  // tuning-table version of ell_rows
+  mutable int ell_rows = 1;       // rows per thread of the ELL apply (autotuned)
 };
 
 namespace decb {

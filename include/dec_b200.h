@@ -408,8 +408,29 @@ dec_status dec_mg_time_kernel(dec_mg* mg, int32_t kernel, int32_t level, int32_t
  * read or written once and each gathered vector once, summed over the solve graph's kernels, plus
  * the layout changes of b and u.  Captures the solve graph if no solve of this shape ran yet. */
 dec_status dec_mg_solve_traffic(dec_mg* mg, int32_t nrhs, int32_t from_zero, int32_t iterations, double* bytes);
+/* ---- the autotuner's table (no counterpart in the reference): the variant chosen per (kernel,
+ *      dtype, shape, size bucket), process-wide, consulted when a kernel is launched or a solve graph
+ *      captured.  Keys read "<kernel>/<dtype>/<shape>/n<floor(log2 size)>":
+ *        ell/f32|f64/W7/n<rows>          rows per thread of the ELL apply (1, 2 or 4; 1 by default)
+ *        sweep/f32/K<width>/W<slots>/n<rows>  lanes per row of the FP32 smoothing sweep: the vector
+ *                                        width 4 (default) or 2 (twice the lanes on a row)
+ *      Every variant computes the same bits; only the time differs. ------------------------------ */
+/* Times each rows-per-thread variant of the operator's apply (operators stored as rows of 7 slots:
+ * the Laplacian / Helmholtz operators of triangle meshes, a caller matrix of that width) on scratch
+ * vectors, records the fastest in the table and returns it in *choice (0: the kernel has no variants). */
+dec_status dec_op_autotune(dec_op* op, int32_t reps, void* stream, int32_t* choice);
+dec_status dec_tune_set(const char* key, int32_t value);
+/* *found = 0 (and *value untouched) when the key was never measured or set. */
+dec_status dec_tune_get(const char* key, int32_t* value, int32_t* found);
+dec_status dec_tune_clear(void);
+/* The table as JSON ({"format": "dec_b200 tuning table", "version": 1, "device": ..., "entries": {...}});
+ * loading merges a saved table into the current one (its entries win) and returns how many it read. */
+dec_status dec_tune_save(const char* path);
+dec_status dec_tune_load(const char* path, int32_t* entries);
 /* Times each candidate panel width on one V-cycle and keeps the fastest for `nrhs` right-hand
- * sides (used when rhs_block = 0).  Returns the chosen width. */
+ * sides (used when rhs_block = 0); for FP32 V-cycles on panels of 8 or more it then times the sweep's
+ * lanes-per-row variants on the same cycle and records the winner in the tuning table for every
+ * level.  Returns the chosen width. */
 dec_status dec_mg_autotune(dec_mg* mg, int32_t nrhs, int32_t reps, void* stream, int32_t* rhs_block);
 
 #ifdef __cplusplus

@@ -214,3 +214,28 @@ def test_julia_extension_matches_the_header(dec):
                "dec_inv_hodge_star", "dec_wedge_product", "multigrid_vcycles", "full_multigrid"):
         assert re.search(r"\n" + fn + r"\(.*Val\{:B200\}|function " + fn + r"\(.*Val\{:B200\}|\n" + fn +
                          r"\(u::CuVecOrMat|function " + fn + r"\(b::CuVecOrMat", jl), fn
+
+
+def test_tuning_table_round_trip(dec, tmp_path):
+    """The autotuner's table: set / get, saved as JSON and merged back after a clear; a file that is
+    not a tuning table is refused (host only, no device work)."""
+    import json
+    dec.tune_clear()
+    assert dec.tune_get("ell/f32/W7/n21") is None
+    dec.tune_set("ell/f32/W7/n21", 2)
+    dec.tune_set("sweep/f32/K32/W6/n19", 4)
+    assert dec.tune_get("ell/f32/W7/n21") == 2
+    path = tmp_path / "tune.json"
+    dec.tune_save(path)
+    d = json.loads(path.read_text())
+    assert d["format"] == "dec_b200 tuning table" and d["version"] == 1
+    assert d["entries"] == {"ell/f32/W7/n21": 2, "sweep/f32/K32/W6/n19": 4}
+    dec.tune_clear()
+    assert dec.tune_get("sweep/f32/K32/W6/n19") is None
+    assert dec.tune_load(path) == 2
+    assert dec.tune_get("sweep/f32/K32/W6/n19") == 4
+    bad = tmp_path / "bad.json"
+    bad.write_text('{"entries": {"x": 1}}')
+    with pytest.raises(dec.DecError, match="tuning table"):
+        dec.tune_load(bad)
+    dec.tune_clear()
