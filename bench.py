@@ -200,6 +200,7 @@ def measure_operators(dec, peak, cpu=True):
             d0 = dec.dec_differential(0, g, dt)
             d1 = dec.dec_differential(1, g, dt)
             L = dec.laplace_beltrami(g, dt)
+            ell_rows = L.autotune(reps=10)   # rows per thread of the ELL apply, recorded in the tuning table
             s1 = dec.hodge_operator(1, g, dtype=dt)
             ops = {
                 "wedge01": (lambda: w01(f, a, oe), ne * (8 + 2 * sz) + nv * sz),
@@ -214,6 +215,8 @@ def measure_operators(dec, peak, cpu=True):
                 ms = time_op(fn)
                 gbs = by / (ms * 1e-3) / 1e9
                 res[f"{op}_{dt}"] = {"us": round(ms * 1e3, 2), "GB/s": round(gbs, 1), "frac": round(gbs / peak, 3)}
+                if op == "laplacian":
+                    res[f"{op}_{dt}"]["rows_per_thread"] = ell_rows
         out[name] = res
         del g
         torch.cuda.empty_cache()
@@ -913,9 +916,17 @@ def run_op(args):
     wedges = {"wedge01": (dec.dec_wedge_product(0, 1, g, args.dtype), f, a),
               "wedge11": (dec.dec_wedge_product(1, 1, g, args.dtype), a, b),
               "wedge02": (dec.dec_wedge_product(0, 2, g, args.dtype), f, t)}
+    variant = None
     if args.op in ops:
         op, x = ops[args.op]
         y = torch.empty(op.shape[0], dtype=tdt, device="cuda")
+        if args.op == "laplacian":
+            key = f"ell/{'f64' if args.dtype == 'float64' else 'f32'}/W7/n{int(np.log2(g.nv))}"
+            if args.variant:
+                dec.tune_set(key, args.variant)
+            elif args.autotune:
+                op.autotune(reps=10)
+            variant = {key: dec.tune_get(key)}
         fn = lambda: op.apply(x, y)
     else:
         w, x1, x2 = wedges[args.op]
@@ -932,7 +943,8 @@ def run_op(args):
     e1.record()
     torch.cuda.synchronize()
     print(json.dumps({"op": args.op, "dtype": args.dtype, "mesh_level": args.mesh_level, "nv": g.nv, "ne": g.ne,
-                      "nt": g.nt, "us_per_launch": 1e3 * e0.elapsed_time(e1) / args.steps}), flush=True)
+                      "nt": g.nt, "us_per_launch": 1e3 * e0.elapsed_time(e1) / args.steps, "variant": variant}),
+          flush=True)
 
 
 def run_kernel(args):
@@ -990,6 +1002,8 @@ def main():
     ap.add_argument("--op", choices=["laplacian", "d0", "d1", "star1_geometric", "wedge01", "wedge11", "wedge02"],
                     help="time one DEC operator kernel alone (steps launches after warmup) and exit")
     ap.add_argument("--dtype", default="float64", choices=["float64", "float32"])
+    ap.add_argument("--autotune", action="store_true", help="--op laplacian: autotune the apply's variant first")
+    ap.add_argument("--variant", type=int, default=0, help="--op laplacian: rows per thread (1, 2, 4)")
     ap.add_argument("--no-batch", action="store_true", dest="no_batch", help="skip the batched-workload section")
     ap.add_argument("--no-configs", action="store_true", dest="no_configs",
                     help="skip the L6 FP64 and L8 1e-10 sections")

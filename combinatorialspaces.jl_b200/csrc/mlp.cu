@@ -343,6 +343,12 @@ struct __align__(128) TcGroup {
 struct __align__(128) TcSmem {
   __nv_bfloat16 w1[kMlpH * kMlpIn];
   __nv_bfloat16 w2[kMlpH * kMlpH];
+  // The biases as an MMA: ones (128 x 16, columns 0..2 one, the rest zero) times bb1 / bb2 (64 x 16,
+  // row j = the exact three-part BF16 split hi + mid + lo of b1_j / b2_j) puts b into the
+  // accumulator before the layer's products add onto it.
+  __nv_bfloat16 ones[kTcRows * kMlpIn];
+  __nv_bfloat16 bb1[kMlpH * kMlpIn];
+  __nv_bfloat16 bb2[kMlpH * kMlpIn];
   uint32_t tmem;
   uint64_t mbar[kTcGroups];
   TcGroup g[kTcGroups];
@@ -441,9 +447,33 @@ __device__ __forceinline__ void tc_store_features(__nv_bfloat16* a1, int r, cons
   *reinterpret_cast<uint4*>(base + kmaj(r, 8, kMlpIn)) = hi;
 }
 
+// b = hi + mid + lo exactly (each part the round-to-nearest BF16 of what the previous ones leave:
+// 8 of FP32's 24 significant bits per part), part k of value v.
+__device__ __forceinline__ __nv_bfloat16 bf16_part(float v, int k) {
+  const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+  if (k == 0) return hi;
+  const float r1 = v - __bfloat162float(hi);
+  const __nv_bfloat16 mid = __float2bfloat16_rn(r1);
+  if (k == 1) return mid;
+  return __float2bfloat16_rn(r1 - __bfloat162float(mid));
+}
+
 __device__ void tc_setup(TcSmem& sm, const MlpWeights& w) {
   char* w1 = reinterpret_cast<char*>(sm.w1);
   char* w2 = reinterpret_cast<char*>(sm.w2);
+  char* ones = reinterpret_cast<char*>(sm.ones);
+  char* bb1 = reinterpret_cast<char*>(sm.bb1);
+  char* bb2 = reinterpret_cast<char*>(sm.bb2);
+  for (int i = threadIdx.x; i < kTcRows * kMlpIn; i += blockDim.x)
+    *reinterpret_cast<__nv_bfloat16*>(ones + kmaj(i / kMlpIn, i % kMlpIn, kMlpIn)) =
+        __float2bfloat16_rn(i % kMlpIn < 3 ? 1.f : 0.f);
+  for (int i = threadIdx.x; i < kMlpH * kMlpIn; i += blockDim.x) {
+    const int j = i / kMlpIn, k = i % kMlpIn;
+    *reinterpret_cast<__nv_bfloat16*>(bb1 + kmaj(j, k, kMlpIn)) =
+        k < 3 ? bf16_part(w.hs.b1[j], k) : __float2bfloat16_rn(0.f);
+    *reinterpret_cast<__nv_bfloat16*>(bb2 + kmaj(j, k, kMlpIn)) =
+        k < 3 ? bf16_part(w.hs.b2[j], k) : __float2bfloat16_rn(0.f);
+  }
   for (int i = threadIdx.x; i < kMlpH * kMlpIn; i += blockDim.x)
     *reinterpret_cast<__nv_bfloat16*>(w1 + kmaj(i / kMlpIn, i % kMlpIn, kMlpIn)) = w.w1[i];
   for (int i = threadIdx.x; i < kMlpH * kMlpH; i += blockDim.x)
@@ -488,25 +518,25 @@ __device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
 __device__ __forceinline__ float lo_of(uint64_t v) { return __uint_as_float((uint32_t)v); }
 __device__ __forceinline__ float hi_of(uint64_t v) { return __uint_as_float((uint32_t)(v >> 32)); }
 
-// Layer-1 epilogue of one 16-column chunk: A2[r, c0 .. c0+15] = bf16(ReLU(D + b1)), the ReLU and
-// the round-to-nearest BF16 pair in one conversion (a NaN stays NaN there, where max(x, 0) gave 0).
-__device__ __forceinline__ void tc_epi1(const MlpSmall& hs, char* a2, int r, int c0, const uint32_t (&z)[16]) {
+// Layer-1 epilogue of one 16-column chunk: A2[r, c0 .. c0+15] = bf16(ReLU(D)), D = b1 + A1 W1ᵀ (the
+// bias is in the accumulator), the ReLU and the round-to-nearest BF16 pair in one conversion (a NaN
+// stays NaN there, where max(x, 0) gave 0).
+__device__ __forceinline__ void tc_epi1(char* a2, int r, int c0, const uint32_t (&z)[16]) {
   uint32_t pk[8];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const uint64_t v = add2(f2(z[2 * j], z[2 * j + 1]), f2(hs.b1[c0 + 2 * j], hs.b1[c0 + 2 * j + 1]));
-    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(pk[j]) : "f"(hi_of(v)), "f"(lo_of(v)));
-  }
+  for (int j = 0; j < 8; ++j)
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;"
+        : "=r"(pk[j])
+        : "f"(__uint_as_float(z[2 * j + 1])), "f"(__uint_as_float(z[2 * j])));
   *reinterpret_cast<uint4*>(a2 + kmaj(r, c0, kMlpH)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
   *reinterpret_cast<uint4*>(a2 + kmaj(r, c0 + 8, kMlpH)) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
 }
-// Layer-3 partial sums of one chunk, two lanes: acc.lo += w3_j ReLU(D_j + b2_j) over even j,
-// acc.hi over odd j.
+// Layer-3 partial sums of one chunk, two lanes: acc.lo += w3_j ReLU(D_j) over even j, acc.hi over
+// odd j, D = b2 + A2 W2ᵀ.
 __device__ __forceinline__ void tc_epi2(const MlpSmall& hs, int c0, const uint32_t (&z)[16], uint64_t& acc) {
 #pragma unroll
   for (int j = 0; j < 16; j += 2) {
-    const uint64_t v = add2(f2(z[j], z[j + 1]), f2(hs.b2[c0 + j], hs.b2[c0 + j + 1]));
-    const uint64_t h = f2(fmaxf(lo_of(v), 0.f), fmaxf(hi_of(v), 0.f));
+    const uint64_t h = f2(fmaxf(__uint_as_float(z[j]), 0.f), fmaxf(__uint_as_float(z[j + 1]), 0.f));
     acc = fma2(f2(hs.w3[c0 + j], hs.w3[c0 + j + 1]), h, acc);
   }
 }
@@ -524,7 +554,8 @@ __device__ __forceinline__ bool tc_tile(TcSmem& sm, const MlpSmall& hs, int g, i
   group_sync(bar);
   if (r == 0) {
     tc_fence_after();
-    tc_mma(dcol, smem_desc(smem_u32(G.a1), 128, 256), smem_desc(smem_u32(sm.w1), 128, 256), 0);
+    tc_mma(dcol, smem_desc(smem_u32(sm.ones), 128, 256), smem_desc(smem_u32(sm.bb1), 128, 256), 0);
+    tc_mma(dcol, smem_desc(smem_u32(G.a1), 128, 256), smem_desc(smem_u32(sm.w1), 128, 256), 1);
     tc_commit(mbar);
   }
   bool ok = group_all(bar, mbar_wait(mbar, phase));
@@ -539,24 +570,25 @@ __device__ __forceinline__ bool tc_tile(TcSmem& sm, const MlpSmall& hs, int g, i
   tc_ld16(lane, za);
   tc_wait16(za);
   tc_ld16(lane + 16, zb);
-  tc_epi1(hs, a2, r, 0, za);
+  tc_epi1(a2, r, 0, za);
   tc_wait16(zb);
   tc_ld16(lane + 32, za);
-  tc_epi1(hs, a2, r, 16, zb);
+  tc_epi1(a2, r, 16, zb);
   tc_wait16(za);
   tc_ld16(lane + 48, zb);
-  tc_epi1(hs, a2, r, 32, za);
+  tc_epi1(a2, r, 32, za);
   tc_wait16(zb);
-  tc_epi1(hs, a2, r, 48, zb);
+  tc_epi1(a2, r, 48, zb);
   fence_async_smem();
   tc_fence_before();
   group_sync(bar);  // every lane has read D1 and written its A2 row
   if (r == 0) {
     tc_fence_after();
+    tc_mma(dcol, smem_desc(smem_u32(sm.ones), 128, 256), smem_desc(smem_u32(sm.bb2), 128, 256), 0);
 #pragma unroll
     for (int ks = 0; ks < 4; ++ks)
       tc_mma(dcol, smem_desc(smem_u32(G.a2) + 256 * ks, 128, 1024), smem_desc(smem_u32(sm.w2) + 256 * ks, 128, 1024),
-             ks > 0 ? 1u : 0u);
+             1u);
     tc_commit(mbar);
   }
   ok = group_all(bar, mbar_wait(mbar, phase));
