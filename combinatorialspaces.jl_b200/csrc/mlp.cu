@@ -806,43 +806,202 @@ __global__ void k_mlp_eval_cc(int64_t n, const float* __restrict__ x, float* __r
 // h1 = bf16(relu(z1)) (64), relu(z2) (64), dz1 (64), dz2 (64).
 constexpr int kActX0 = 0, kActH1 = 16, kActR2 = 80, kActDz1 = 144, kActDz2 = 208, kActRows = 272;
 
-// Forward + backward of one sample: stores its activations in batch column j and dL/dy in dyb[j].
-// The ReLU masks are z1 > 0 and z2 > 0.
-__device__ void backward_sample(const float* f, float d, const __nv_bfloat16* __restrict__ w1b,
-                                const __nv_bfloat16* __restrict__ w2b, const float* __restrict__ p,
-                                float* __restrict__ act, int64_t j, int64_t B, float* __restrict__ dyb) {
-  float x0[kMlpIn], z1[kMlpH], h1[kMlpH], dz2[kMlpH];
-  for (int k = 0; k < kMlpIn; ++k) x0[k] = __bfloat162float(__float2bfloat16_rn(f[k]));
-  for (int jj = 0; jj < kMlpH; ++jj) {
-    float s = p[kOffB1 + jj];
+// (a, b) as BF16 pairs hi (round to nearest) and lo (the remainders rounded): hi + lo keeps 16 of
+// FP32's 24 significant bits.
+__device__ __forceinline__ void split_pair(float a, float b, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = pack_bf16(a - __low2float(h), b - __high2float(h));
+}
+
+// ---- backward on the tensor cores -----------------------------------------------------------
+// A warp takes 32 samples (rows of its feature tile xs, lane L's sample in row L, dL/dy d in lane L)
+// through the forward of mlp_tile32 (mma.sync m16n8k16, the inference roundings: x0 and h1 BF16,
+// FP32 accumulation), keeping the ReLU masks as bits, and the backward
+//   dz2 = d w3 [z2 > 0],  dh1 = W2ᵀ dz2 (mma.sync: dz2 as hi + lo BF16 A fragments against W2ᵀ),
+//   dz1 = dh1 [z1 > 0],
+// and stores the batch columns jbase .. jbase + 31 of the activations x0, h1, relu(z2), dz1, dz2
+// (structure of arrays [row][B], the layout of the gradient contractions) and dy.
+struct MlpBwdSmem {
+  MlpSmem f;                                              // W1, W2, b1, b2, w3, b3
+  __align__(16) __nv_bfloat16 w2t[kMlpH * kW2Stride];    // W2ᵀ: row i = column i of W2
+};
+
+__device__ void load_bwd_weights(MlpBwdSmem& sm, const MlpWeights& w) {
+  for (int i = threadIdx.x; i < kMlpH * kMlpH; i += blockDim.x)
+    sm.w2t[(i % kMlpH) * kW2Stride + i / kMlpH] = w.w2[i];  // w2[j][i] -> w2t[i][j]
+  load_weights(sm.f, w);  // ends with __syncthreads
+}
+
+__device__ __noinline__ void bwd_tile_tc(const MlpBwdSmem& sm, const __nv_bfloat16* xs, float d, float* __restrict__ act,
+                                            float* __restrict__ dyb, int64_t jbase, int64_t B, int64_t valid) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const uint32_t* X = reinterpret_cast<const uint32_t*>(xs);
+  const uint32_t* W1 = reinterpret_cast<const uint32_t*>(sm.f.w1);
+  const uint32_t* W2 = reinterpret_cast<const uint32_t*>(sm.f.w2);
+  const uint32_t* W2T = reinterpret_cast<const uint32_t*>(sm.w2t);
+  constexpr int XW = kXsStride / 2, W1W = kW1Stride / 2, W2W = kW2Stride / 2;
+  // column jbase + s of the activation rows; samples past `valid` are not stored
+  auto put = [&](int row, int smp, float v) {
+    if (smp < valid) act[(size_t)row * B + jbase + smp] = v;
+  };
+  {  // x0 = bf16(features) and dy, one sample per lane
+    const uint4* xr = reinterpret_cast<const uint4*>(xs + lane * kXsStride);
+    const uint4 lo = xr[0], hi = xr[1];
+    const uint32_t wv[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
 #pragma unroll
-    for (int k = 0; k < kMlpIn; ++k) s += __bfloat162float(w1b[jj * kMlpIn + k]) * x0[k];
-    z1[jj] = s;
-    h1[jj] = __bfloat162float(__float2bfloat16_rn(fmaxf(s, 0.f)));
+    for (int k = 0; k < 8; ++k) {
+      put(kActX0 + 2 * k, lane, __uint_as_float(wv[k] << 16));
+      put(kActX0 + 2 * k + 1, lane, __uint_as_float(wv[k] & 0xffff0000u));
+    }
+    if (lane < valid) dyb[jbase + lane] = d;
   }
-  for (int k = 0; k < kMlpIn; ++k) act[(size_t)(kActX0 + k) * B + j] = x0[k];
-  for (int jj = 0; jj < kMlpH; ++jj) {
-    float s = p[kOffB2 + jj];
-    for (int i = 0; i < kMlpH; ++i) s += __bfloat162float(w2b[jj * kMlpH + i]) * h1[i];
-    dz2[jj] = s > 0.f ? d * p[kOffW3 + jj] : 0.f;
-    act[(size_t)(kActH1 + jj) * B + j] = h1[jj];
-    act[(size_t)(kActR2 + jj) * B + j] = fmaxf(s, 0.f);
-    act[(size_t)(kActDz2 + jj) * B + j] = dz2[jj];
+  // dL/dy of the rows this thread's fragments hold: 16 m + g (+ 8)
+  float dr[2][2];
+#pragma unroll
+  for (int m = 0; m < 2; ++m)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) dr[m][h] = __shfl_sync(0xffffffffu, d, 16 * m + 8 * h + g);
+  uint32_t a[2][4];
+#pragma unroll
+  for (int m = 0; m < 2; ++m) {
+    const int r0 = 16 * m + g;
+    a[m][0] = X[r0 * XW + t];
+    a[m][1] = X[(r0 + 8) * XW + t];
+    a[m][2] = X[r0 * XW + t + 4];
+    a[m][3] = X[(r0 + 8) * XW + t + 4];
   }
-  for (int i = 0; i < kMlpH; ++i) {
-    float dh = 0.f;
-    for (int jj = 0; jj < kMlpH; ++jj) dh += __bfloat162float(w2b[jj * kMlpH + i]) * dz2[jj];
-    act[(size_t)(kActDz1 + i) * B + j] = z1[i] > 0.f ? dh : 0.f;
+  // layer 1: h1 = bf16(relu(b1 + x W1ᵀ)) as layer-2 A fragments; mask bit (m, j, e) = z1 > 0
+  uint32_t a2[2][4][4];
+  uint64_t mask1 = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const uint32_t b0 = W1[(8 * j + g) * W1W + t], b1 = W1[(8 * j + g) * W1W + t + 4];
+    const float bb0 = sm.f.b1[8 * j + 2 * t], bb1 = sm.f.b1[8 * j + 2 * t + 1];
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      float c[4] = {bb0, bb1, bb0, bb1};
+      mma16816(c, a[m], b0, b1);
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (c[e] > 0.f) mask1 |= 1ull << (m * 32 + j * 4 + e);
+      const uint32_t lo = pack_bf16(fmaxf(c[0], 0.f), fmaxf(c[1], 0.f));
+      const uint32_t hi = pack_bf16(fmaxf(c[2], 0.f), fmaxf(c[3], 0.f));
+      const int col = 8 * j + 2 * t, s0 = 16 * m + g;
+      put(kActH1 + col, s0, __uint_as_float(lo << 16));
+      put(kActH1 + col + 1, s0, __uint_as_float(lo & 0xffff0000u));
+      put(kActH1 + col, s0 + 8, __uint_as_float(hi << 16));
+      put(kActH1 + col + 1, s0 + 8, __uint_as_float(hi & 0xffff0000u));
+      if ((j & 1) == 0) {
+        a2[m][j >> 1][0] = lo;
+        a2[m][j >> 1][1] = hi;
+      } else {
+        a2[m][j >> 1][2] = lo;
+        a2[m][j >> 1][3] = hi;
+      }
+    }
   }
-  dyb[j] = d;
+  // layer 2 and dz2 = d w3 [z2 > 0], packed as the A fragments (hi, lo) of dh1 = dz2 W2
+  uint32_t dh[2][4][4], dl[2][4][4];
+#pragma unroll
+  for (int jt = 0; jt < 8; ++jt) {
+    const float bb0 = sm.f.b2[8 * jt + 2 * t], bb1 = sm.f.b2[8 * jt + 2 * t + 1];
+    const float w0 = sm.f.w3[8 * jt + 2 * t], w1 = sm.f.w3[8 * jt + 2 * t + 1];
+    float c[2][4];
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      c[m][0] = bb0;
+      c[m][1] = bb1;
+      c[m][2] = bb0;
+      c[m][3] = bb1;
+    }
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      const uint32_t b0 = W2[(8 * jt + g) * W2W + 8 * kk + t], b1 = W2[(8 * jt + g) * W2W + 8 * kk + t + 4];
+#pragma unroll
+      for (int m = 0; m < 2; ++m) mma16816(c[m], a2[m][kk], b0, b1);
+    }
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      const int col = 8 * jt + 2 * t, s0 = 16 * m + g;
+      const float z[4] = {c[m][0], c[m][1], c[m][2], c[m][3]};
+      const float dd[4] = {z[0] > 0.f ? dr[m][0] * w0 : 0.f, z[1] > 0.f ? dr[m][0] * w1 : 0.f,
+                           z[2] > 0.f ? dr[m][1] * w0 : 0.f, z[3] > 0.f ? dr[m][1] * w1 : 0.f};
+      put(kActR2 + col, s0, fmaxf(z[0], 0.f));
+      put(kActR2 + col + 1, s0, fmaxf(z[1], 0.f));
+      put(kActR2 + col, s0 + 8, fmaxf(z[2], 0.f));
+      put(kActR2 + col + 1, s0 + 8, fmaxf(z[3], 0.f));
+      put(kActDz2 + col, s0, dd[0]);
+      put(kActDz2 + col + 1, s0, dd[1]);
+      put(kActDz2 + col, s0 + 8, dd[2]);
+      put(kActDz2 + col + 1, s0 + 8, dd[3]);
+      uint32_t h01, l01, h23, l23;
+      split_pair(dd[0], dd[1], h01, l01);
+      split_pair(dd[2], dd[3], h23, l23);
+      const int kk = jt >> 1, e = (jt & 1) * 2;
+      dh[m][kk][e] = h01;
+      dl[m][kk][e] = l01;
+      dh[m][kk][e + 1] = h23;
+      dl[m][kk][e + 1] = l23;
+    }
+  }
+  // dh1 = dz2 W2 (K = the 64 units of layer 2), then dz1 = dh1 [z1 > 0]
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    float c[2][4] = {};
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      const uint32_t b0 = W2T[(8 * it + g) * W2W + 8 * kk + t], b1 = W2T[(8 * it + g) * W2W + 8 * kk + t + 4];
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        mma16816(c[m], dh[m][kk], b0, b1);
+        mma16816(c[m], dl[m][kk], b0, b1);
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      const int col = 8 * it + 2 * t, s0 = 16 * m + g;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const bool on = (mask1 >> (m * 32 + it * 4 + e)) & 1ull;
+        put(kActDz1 + col + (e & 1), s0 + 8 * (e >> 1), on ? c[m][e] : 0.f);
+      }
+    }
+  }
 }
 
 // Backward of n given feature rows with given dL/dy (the gradient check entry point).
-__global__ void k_bwd_direct(int64_t n, const float* __restrict__ x, const float* __restrict__ dy,
-                             const __nv_bfloat16* __restrict__ w1b, const __nv_bfloat16* __restrict__ w2b,
-                             const float* __restrict__ p, float* __restrict__ act, float* __restrict__ dyb) {
-  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
-    backward_sample(x + q * 16, dy[q], w1b, w2b, p, act, q, n, dyb);
+__global__ void __launch_bounds__(kMlpThreads) k_bwd_direct_tc(int64_t n, const float* __restrict__ x,
+                                                               const float* __restrict__ dy, MlpWeights w,
+                                                               float* __restrict__ act, float* __restrict__ dyb) {
+  __shared__ MlpBwdSmem sm;
+  __shared__ __align__(16) __nv_bfloat16 xs[kMlpWarps][kTile * kXsStride];
+  load_bwd_weights(sm, w);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t ntiles = (n + kTile - 1) / kTile;
+  for (int64_t tile = (int64_t)blockIdx.x * kMlpWarps + warp; tile < ntiles; tile += (int64_t)gridDim.x * kMlpWarps) {
+    const int64_t q = tile * kTile + lane;
+    float f[16], d = 0.f;
+    if (q < n) {
+      const float4* src = reinterpret_cast<const float4*>(x + q * 16);
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const float4 t4 = src[v];
+        f[4 * v] = t4.x;
+        f[4 * v + 1] = t4.y;
+        f[4 * v + 2] = t4.z;
+        f[4 * v + 3] = t4.w;
+      }
+      d = dy[q];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) f[k] = 0.f;
+    }
+    store_row(xs[warp], lane, f);
+    __syncwarp();
+    bwd_tile_tc(sm, xs[warp], d, act, dyb, tile * kTile, n, n - tile * kTile);
+    __syncwarp();
+  }
 }
 
 // Features of sample (vertex i, field rs) on a reference-ordered Laplacian / Helmholtz operator of
@@ -869,6 +1028,15 @@ __device__ void op_features(int i, int n, int Wf, const int32_t* __restrict__ co
   float scale;
   mlp_features((float)rs[i], nb, cp, nn, 1.f - sabs / dif, f, &scale);
   *dsc = scale / dif;
+}
+
+// The features alone, out of line: the backward tile that follows keeps its registers for the MMA
+// fragments.
+__device__ __noinline__ void op_features_only(int i, int n, int Wf, const int32_t* __restrict__ col,
+                                              const double* __restrict__ val, const double* __restrict__ rs,
+                                              float* f) {
+  float dsc;
+  op_features(i, n, Wf, col, val, rs, f, &dsc);
 }
 
 __global__ void k_op_features(int n, int S, int Wf, const int32_t* __restrict__ col, const double* __restrict__ val,
@@ -915,13 +1083,16 @@ __global__ void __launch_bounds__(kMlpThreads) k_train_fwd(int n, int S, int Wf,
   }
 }
 
-// n_s = Σ_i ⋆0_i r_si² / a_ii per field (one CTA per field).
-__global__ void __launch_bounds__(256) k_train_norms(int n, int Wf, const int32_t* __restrict__ col,
-                                                     const double* __restrict__ val, const double* __restrict__ star0,
-                                                     const double* __restrict__ r, double* __restrict__ nrm) {
-  const double* rs = r + (size_t)blockIdx.x * n;
+// n_s = Σ_i ⋆0_i r_si² / a_ii per field: kNormBlocks CTAs per field write partial sums over strided
+// rows (lpart[s * kNormBlocks + b]), then one CTA per field adds them in block order.
+constexpr int kNormBlocks = 64;
+__global__ void __launch_bounds__(256) k_train_norm_parts(int n, int Wf, const int32_t* __restrict__ col,
+                                                          const double* __restrict__ val,
+                                                          const double* __restrict__ star0,
+                                                          const double* __restrict__ r, double* __restrict__ part) {
+  const double* rs = r + (size_t)blockIdx.y * n;
   double acc = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double di = 0.0;
     for (int q = 0; q < Wf; ++q)
       if (col[(size_t)q * n + i] == i) di += val[(size_t)q * n + i];
@@ -934,7 +1105,23 @@ __global__ void __launch_bounds__(256) k_train_norms(int n, int Wf, const int32_
     if (threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
     __syncthreads();
   }
-  if (threadIdx.x == 0) nrm[blockIdx.x] = sh[0] > 0 ? sh[0] : 1.0;
+  if (threadIdx.x == 0) part[(size_t)blockIdx.y * kNormBlocks + blockIdx.x] = sh[0];
+}
+
+__global__ void k_train_norm_sum(const double* __restrict__ part, double* __restrict__ nrm) {
+  if (threadIdx.x != 0) return;
+  double s = 0.0;
+  for (int b = 0; b < kNormBlocks; ++b) s += part[(size_t)blockIdx.x * kNormBlocks + b];
+  nrm[blockIdx.x] = s > 0 ? s : 1.0;
+}
+
+static void train_norms(dec_mlp& m, const dec_op* op, const double* r, int S, cudaStream_t s) {
+  if (m.npart.n < (size_t)S * kNormBlocks) m.npart.alloc((size_t)S * kNormBlocks);
+  const int n = op->m->nv;
+  k_train_norm_parts<<<dim3(kNormBlocks, S), 256, 0, s>>>(n, op->W, op->col.p, op->val64.p, op->m->star0.p, r,
+                                                          m.npart.p);
+  k_train_norm_sum<<<S, 32, 0, s>>>(m.npart.p, m.nrm.p);
+  DEC_CHECK_LAUNCH();
 }
 
 // dL/dδ = 2 w (A δ - r), w = ⋆0_i / (S n_s); dy = dL/dδ · dscale; loss partials Σ w δ (A δ - 2 r).
@@ -971,89 +1158,149 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
 // Backward over the batch: column j is sample j when the fields hold at most B samples, else a
 // sample drawn uniformly with replacement from (seed, step, j); dL/dy is scaled by N / B so the
 // batch gradient estimates the full one.
-__global__ void k_train_bwd(int n, int S, int64_t B, uint64_t seed, int64_t step, int Wf,
-                            const int32_t* __restrict__ col, const double* __restrict__ val,
-                            const double* __restrict__ r, const __nv_bfloat16* __restrict__ w1b,
-                            const __nv_bfloat16* __restrict__ w2b, const float* __restrict__ p,
-                            const double* __restrict__ dy, float* __restrict__ act, float* __restrict__ dyb) {
+__global__ void __launch_bounds__(kMlpThreads) k_train_bwd_tc(int n, int S, int64_t B, uint64_t seed, int64_t step,
+                                                              int Wf, const int32_t* __restrict__ col,
+                                                              const double* __restrict__ val,
+                                                              const double* __restrict__ r, MlpWeights w,
+                                                              const double* __restrict__ dy, float* __restrict__ act,
+                                                              float* __restrict__ dyb) {
+  __shared__ MlpBwdSmem sm;
+  __shared__ __align__(16) __nv_bfloat16 xs[kMlpWarps][kTile * kXsStride];
+  load_bwd_weights(sm, w);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t N = (int64_t)n * S;
   const bool sample = N > B;
   const int64_t Bn = sample ? B : N;
   const double scale = sample ? (double)N / (double)B : 1.0;
-  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < Bn; j += (int64_t)gridDim.x * blockDim.x) {
-    int64_t q = j;
-    if (sample) {
-      const uint64_t h = mix64(seed + 0x9E3779B97F4A7C15ull * (uint64_t)(step + 1) + 0xD1B54A32D192ED03ull * (uint64_t)j);
-      q = (int64_t)(h % (uint64_t)N);
+  const int64_t ntiles = (Bn + kTile - 1) / kTile;
+  for (int64_t tile = (int64_t)blockIdx.x * kMlpWarps + warp; tile < ntiles; tile += (int64_t)gridDim.x * kMlpWarps) {
+    const int64_t j = tile * kTile + lane;
+    float f[16], d = 0.f;
+    if (j < Bn) {
+      int64_t q = j;
+      if (sample) {
+        const uint64_t h = mix64(seed + 0x9E3779B97F4A7C15ull * (uint64_t)(step + 1) + 0xD1B54A32D192ED03ull * (uint64_t)j);
+        q = (int64_t)(h % (uint64_t)N);
+      }
+      const int s = (int)(q / n), i = (int)(q % n);
+      op_features_only(i, n, Wf, col, val, r + (size_t)s * n, f);
+      d = (float)(dy[q] * scale);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) f[k] = 0.f;
     }
-    const int s = (int)(q / n), i = (int)(q % n);
-    float f[16], dsc;
-    op_features(i, n, Wf, col, val, r + (size_t)s * n, f, &dsc);
-    backward_sample(f, (float)(dy[q] * scale), w1b, w2b, p, act, j, Bn, dyb);
+    store_row(xs[warp], lane, f);
+    __syncwarp();
+    bwd_tile_tc(sm, xs[warp], d, act, dyb, tile * kTile, Bn, Bn - tile * kTile);
+    __syncwarp();
   }
+}
+
+static unsigned bwd_grid(int64_t samples) {
+  const long long tiles = (samples + kTile - 1) / kTile;
+  return (unsigned)std::max<long long>(1, std::min<long long>((tiles + kMlpWarps - 1) / kMlpWarps, num_sms() * 4LL));
 }
 
 // Parameter gradient partials over one chunk of batch columns per CTA, in a fixed order:
 // dW1 = Σ dz1 x0ᵀ, db1 = Σ dz1, dW2 = Σ dz2 h1ᵀ, db2 = Σ dz2, dw3 = Σ dy relu(z2), db3 = Σ dy.
-constexpr int kGradThreads = 256, kGradTile = 16, kGradChunk = 256, kMaxChunks = 1024;
-__global__ void __launch_bounds__(kGradThreads) k_train_grad(int64_t B, int64_t chunk, const float* __restrict__ act,
-                                                             const float* __restrict__ dyb, float* __restrict__ gpart) {
-  __shared__ float sx0[kMlpIn][kGradTile], sh1[kMlpH][kGradTile], sr2[kMlpH][kGradTile];
-  __shared__ float sdz1[kMlpH][kGradTile], sdz2[kMlpH][kGradTile], sdy[kGradTile];
-  constexpr int kPer = (kMlpNParam + kGradThreads - 1) / kGradThreads;
-  float acc[kPer];
-#pragma unroll
-  for (int m = 0; m < kPer; ++m) acc[m] = 0.f;
+constexpr int kGradThreads = 256, kGradChunk = 256, kMaxChunks = 1024;
+
+// The two contractions run on the tensor cores (mma.sync m16n8k16, BF16 operands,
+// FP32 accumulation): dW2 = Σ_s dz2_s h1_sᵀ and dW1 = Σ_s dz1_s x0_sᵀ over the batch, K = the batch
+// samples.  x0 and h1 are BF16 values already; dz1 and dz2 enter as hi + lo BF16 pairs (hi = the
+// round-to-nearest BF16, lo = that of the remainder), so each product carries 16 of FP32's 24 bits
+// of dz.  A CTA stages 32 samples of every activation row in shared memory at a time; warp w owns
+// the output tiles dW2 rows 16 (w / 2) .. +15, columns 32 (w % 2) .. +31 (four n8 tiles) and dW1
+// rows 16 (w / 2) .., columns 8 (w % 2) .. +7.  db1, db2, dw3 and db3 are sums on the CUDA cores.
+constexpr int kGradStage = 32;
+
+__global__ void __launch_bounds__(kGradThreads) k_train_grad_tc(int64_t B, int64_t chunk,
+                                                                const float* __restrict__ act,
+                                                                const float* __restrict__ dyb,
+                                                                float* __restrict__ gpart) {
+  // rows of the staged batch slice: the activation rows then dy, kGradStage samples each (+1 pad)
+  constexpr int kRows = kActRows + 1, kLd = kGradStage + 1;
+  __shared__ float sa[kRows * kLd];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int mt = warp >> 1, nh = warp & 1;
+  float c2[4][4] = {}, c1[4] = {};
+  float sacc = 0.f;  // this thread's bias / w3 sum (threads 0 .. 192)
   const int64_t lo = blockIdx.x * chunk, hi = min(B, lo + chunk);
-  for (int64_t b = lo; b < hi; b += kGradTile) {
-    for (int e = threadIdx.x; e < kGradTile * (kActRows + 1); e += kGradThreads) {
-      const int c = e % kGradTile, row = e / kGradTile;
-      const int64_t q = b + c;
-      const bool ok = q < hi;
-      const float v = ok ? (row < kActRows ? act[(size_t)row * B + q] : dyb[q]) : 0.f;
-      if (row < kActH1) sx0[row][c] = v;
-      else if (row < kActR2) sh1[row - kActH1][c] = v;
-      else if (row < kActDz1) sr2[row - kActR2][c] = v;
-      else if (row < kActDz2) sdz1[row - kActDz1][c] = v;
-      else if (row < kActRows) sdz2[row - kActDz2][c] = v;
-      else sdy[c] = v;
+  for (int64_t b0 = lo; b0 < hi; b0 += kGradStage) {
+    for (int e = threadIdx.x; e < kRows * kGradStage; e += kGradThreads) {
+      const int row = e / kGradStage, c = e % kGradStage;
+      const int64_t q = b0 + c;
+      float v = 0.f;
+      if (q < hi) v = row < kActRows ? act[(size_t)row * B + q] : dyb[q];
+      sa[row * kLd + c] = v;
     }
     __syncthreads();
 #pragma unroll
-    for (int m = 0; m < kPer; ++m) {
-      const int pi = threadIdx.x + m * kGradThreads;
-      if (pi >= kMlpNParam) break;
-      float s = 0.f;
-      if (pi < kOffB1) {
-        const int i = pi / kMlpIn, k = pi % kMlpIn;
+    for (int ks = 0; ks < kGradStage; ks += 16) {
+      // A fragments of dz2 rows 16 mt .. (and dz1 for dW1), hi and lo parts
+      auto afrag = [&](int base, uint32_t (&ah)[4], uint32_t (&al)[4]) {
+        const float* r0 = sa + (base + 16 * mt + g) * kLd + ks;
+        const float* r8 = r0 + 8 * kLd;
+        split_pair(r0[2 * t], r0[2 * t + 1], ah[0], al[0]);
+        split_pair(r8[2 * t], r8[2 * t + 1], ah[1], al[1]);
+        split_pair(r0[2 * t + 8], r0[2 * t + 9], ah[2], al[2]);
+        split_pair(r8[2 * t + 8], r8[2 * t + 9], ah[3], al[3]);
+      };
+      uint32_t ah[4], al[4];
+      afrag(kActDz2, ah, al);
 #pragma unroll
-        for (int c = 0; c < kGradTile; ++c) s += sdz1[i][c] * sx0[k][c];
-      } else if (pi < kOffW2) {
-#pragma unroll
-        for (int c = 0; c < kGradTile; ++c) s += sdz1[pi - kOffB1][c];
-      } else if (pi < kOffB2) {
-        const int j = (pi - kOffW2) / kMlpH, i = (pi - kOffW2) % kMlpH;
-#pragma unroll
-        for (int c = 0; c < kGradTile; ++c) s += sdz2[j][c] * sh1[i][c];
-      } else if (pi < kOffW3) {
-#pragma unroll
-        for (int c = 0; c < kGradTile; ++c) s += sdz2[pi - kOffB2][c];
-      } else if (pi < kOffB3) {
-#pragma unroll
-        for (int c = 0; c < kGradTile; ++c) s += sdy[c] * sr2[pi - kOffW3][c];
-      } else {
-#pragma unroll
-        for (int c = 0; c < kGradTile; ++c) s += sdy[c];
+      for (int u = 0; u < 4; ++u) {
+        const float* h = sa + (kActH1 + 32 * nh + 8 * u + g) * kLd + ks;
+        const uint32_t b0r = pack_bf16(h[2 * t], h[2 * t + 1]), b1r = pack_bf16(h[2 * t + 8], h[2 * t + 9]);
+        mma16816(c2[u], ah, b0r, b1r);
+        mma16816(c2[u], al, b0r, b1r);
       }
-      acc[m] += s;
+      afrag(kActDz1, ah, al);
+      {
+        const float* x = sa + (kActX0 + 8 * nh + g) * kLd + ks;
+        const uint32_t b0r = pack_bf16(x[2 * t], x[2 * t + 1]), b1r = pack_bf16(x[2 * t + 8], x[2 * t + 9]);
+        mma16816(c1, ah, b0r, b1r);
+        mma16816(c1, al, b0r, b1r);
+      }
+    }
+    // db1 (threads 0..63), db2 (64..127), dw3 = Σ dy relu(z2) (128..191), db3 = Σ dy (192)
+    if (threadIdx.x < 3 * kMlpH + 1) {
+      const int p = threadIdx.x;
+      const float* row = p < kMlpH         ? sa + (kActDz1 + p) * kLd
+                         : p < 2 * kMlpH   ? sa + (kActDz2 + p - kMlpH) * kLd
+                         : p < 3 * kMlpH   ? sa + (kActR2 + p - 2 * kMlpH) * kLd
+                                           : sa + kActRows * kLd;
+      const float* dy = sa + kActRows * kLd;
+      float s = 0.f;
+      if (p >= 2 * kMlpH && p < 3 * kMlpH) {
+        for (int c = 0; c < kGradStage; ++c) s += dy[c] * row[c];
+      } else {
+        for (int c = 0; c < kGradStage; ++c) s += row[c];
+      }
+      sacc += s;
     }
     __syncthreads();
   }
+  float* out = gpart + (size_t)blockIdx.x * kMlpNParam;
 #pragma unroll
-  for (int m = 0; m < kPer; ++m) {
-    const int pi = threadIdx.x + m * kGradThreads;
-    if (pi < kMlpNParam) gpart[(size_t)blockIdx.x * kMlpNParam + pi] = acc[m];
+  for (int u = 0; u < 4; ++u) {
+    const int j = 16 * mt + g, i = 32 * nh + 8 * u + 2 * t;
+    out[kOffW2 + j * kMlpH + i] = c2[u][0];
+    out[kOffW2 + j * kMlpH + i + 1] = c2[u][1];
+    out[kOffW2 + (j + 8) * kMlpH + i] = c2[u][2];
+    out[kOffW2 + (j + 8) * kMlpH + i + 1] = c2[u][3];
   }
+  {
+    const int j = 16 * mt + g, k = 8 * nh + 2 * t;
+    out[kOffW1 + j * kMlpIn + k] = c1[0];
+    out[kOffW1 + j * kMlpIn + k + 1] = c1[1];
+    out[kOffW1 + (j + 8) * kMlpIn + k] = c1[2];
+    out[kOffW1 + (j + 8) * kMlpIn + k + 1] = c1[3];
+  }
+  if (threadIdx.x < kMlpH) out[kOffB1 + threadIdx.x] = sacc;
+  else if (threadIdx.x < 2 * kMlpH) out[kOffB2 + threadIdx.x - kMlpH] = sacc;
+  else if (threadIdx.x < 3 * kMlpH) out[kOffW3 + threadIdx.x - 2 * kMlpH] = sacc;
+  else if (threadIdx.x == 3 * kMlpH) out[kOffB3] = sacc;
 }
 
 __global__ void k_grad_reduce(int nchunks, const float* __restrict__ gpart, float* __restrict__ grad) {
@@ -1126,7 +1373,7 @@ static int grad_chunks(int64_t B, int64_t* chunk) {
 static void reduce_grad(dec_mlp& m, int64_t B, float* grad, cudaStream_t s) {
   int64_t chunk;
   const int nch = grad_chunks(B, &chunk);
-  k_train_grad<<<nch, kGradThreads, 0, s>>>(B, chunk, m.act.p, m.dyb.p, m.gpart.p);
+  k_train_grad_tc<<<nch, kGradThreads, 0, s>>>(B, chunk, m.act.p, m.dyb.p, m.gpart.p);
   k_grad_reduce<<<(kMlpNParam + 255) / 256, 256, 0, s>>>(nch, m.gpart.p, grad);
   DEC_CHECK_LAUNCH();
 }
@@ -1286,7 +1533,7 @@ void mlp_grad_impl(dec_mlp* m, const float* x, const float* dy, int64_t n, float
   require(m != nullptr && x != nullptr && dy != nullptr && grad != nullptr && n > 0, "mlp: bad grad arguments");
   cudaStream_t s = as_stream(stream);
   ensure_scratch(*m, 1, (size_t)n, 1);
-  k_bwd_direct<<<grid_for(n, 128), 128, 0, s>>>(n, x, dy, m->w1b.p, m->w2b.p, m->master.p, m->act.p, m->dyb.p);
+  k_bwd_direct_tc<<<bwd_grid(n), kMlpThreads, 0, s>>>(n, x, dy, mlp_weights(m), m->act.p, m->dyb.p);
   DEC_CHECK_LAUNCH();
   reduce_grad(*m, n, grad, s);
 }
@@ -1307,11 +1554,11 @@ void mlp_loss_grad_impl(dec_mlp* m, dec_op* op, const double* r, int S, double* 
   const int n = op->m->nv;
   const int64_t N = (int64_t)n * S;
   ensure_scratch(*m, (size_t)N, (size_t)N, S);
-  k_train_norms<<<S, 256, 0, s>>>(n, op->W, op->col.p, op->val64.p, op->m->star0.p, r, m->nrm.p);
+  train_norms(*m, op, r, S, s);
   loss_and_dy(*m, op, r, S, s);
   if (grad) {
-    k_train_bwd<<<grid_for(N, 128), 128, 0, s>>>(n, S, N, 0, 0, op->W, op->col.p, op->val64.p, r, m->w1b.p, m->w2b.p,
-                                                 m->master.p, m->dy.p, m->act.p, m->dyb.p);
+    k_train_bwd_tc<<<bwd_grid(N), kMlpThreads, 0, s>>>(n, S, N, 0, 0, op->W, op->col.p, op->val64.p, r,
+                                                         mlp_weights(m), m->dy.p, m->act.p, m->dyb.p);
     DEC_CHECK_LAUNCH();
     reduce_grad(*m, N, grad, s);
   }
@@ -1327,11 +1574,11 @@ void mlp_train_impl(dec_mlp* m, dec_op* op, const double* r, int S, int steps, d
   const int64_t N = (int64_t)n * S;
   const int64_t Bn = std::min<int64_t>(batch, N);
   ensure_scratch(*m, (size_t)N, (size_t)Bn, S);
-  k_train_norms<<<S, 256, 0, s>>>(n, op->W, op->col.p, op->val64.p, op->m->star0.p, r, m->nrm.p);
+  train_norms(*m, op, r, S, s);
   for (int it = 0; it < steps; ++it) {
     loss_and_dy(*m, op, r, S, s);
-    k_train_bwd<<<grid_for(Bn, 128), 128, 0, s>>>(n, S, batch, seed, m->step, op->W, op->col.p, op->val64.p, r,
-                                                  m->w1b.p, m->w2b.p, m->master.p, m->dy.p, m->act.p, m->dyb.p);
+    k_train_bwd_tc<<<bwd_grid(Bn), kMlpThreads, 0, s>>>(n, S, batch, seed, m->step, op->W, op->col.p, op->val64.p,
+                                                          r, mlp_weights(m), m->dy.p, m->act.p, m->dyb.p);
     DEC_CHECK_LAUNCH();
     reduce_grad(*m, Bn, m->grad.p, s);
     ++m->step;

@@ -70,7 +70,7 @@ struct dec_mlp {
   decb::DArr<float> dsc;            // per sample: s_i / a_ii
   decb::DArr<float> dyb;      // dL/dy of the backward batch
   decb::DArr<float> gpart;    // per-chunk gradient partials
-  decb::DArr<double> lpart, nrm;
+  decb::DArr<double> lpart, nrm, npart;
   decb::DArr<int> err;        // device error flag of the tcgen05 kernels
   int engine = 1;             // tcgen05 (1) by default; mma.sync (0) on request
   decb::MlpSmall hsmall{};    // host copy of b1, b2, w3, b3 (refreshed with every parameter change)
