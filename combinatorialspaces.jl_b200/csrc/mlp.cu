@@ -558,9 +558,11 @@ __device__ __forceinline__ bool tc_tile(TcSmem& sm, const MlpSmall& hs, int g, i
     tc_mma(dcol, smem_desc(smem_u32(G.a1), 128, 256), smem_desc(smem_u32(sm.w1), 128, 256), 1);
     tc_commit(mbar);
   }
-  bool ok = group_all(bar, mbar_wait(mbar, phase));
+  // one thread polls the MMA's mbarrier; the others block on the named barrier, which hands them its
+  // result and orders their TMEM reads after the wait (tcgen05.fence::after_thread_sync below)
+  bool ok = group_all(bar, r == 0 ? mbar_wait(mbar, phase) : true);
   if (!ok) {  // one more bounded wait for the MMA in flight before the TMEM is freed
-    mbar_wait(mbar, phase);
+    if (r == 0) mbar_wait(mbar, phase);
     return false;
   }
   phase ^= 1;
@@ -591,9 +593,9 @@ __device__ __forceinline__ bool tc_tile(TcSmem& sm, const MlpSmall& hs, int g, i
              1u);
     tc_commit(mbar);
   }
-  ok = group_all(bar, mbar_wait(mbar, phase));
+  ok = group_all(bar, r == 0 ? mbar_wait(mbar, phase) : true);
   if (!ok) {
-    mbar_wait(mbar, phase);
+    if (r == 0) mbar_wait(mbar, phase);
     return false;
   }
   phase ^= 1;
@@ -667,11 +669,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mlp_smooth_tcg(MlpWeights w, 
   const int g = threadIdx.x / kTcRows, rr = threadIdx.x % kTcRows;
   uint32_t phase = 0;
   const int64_t nq = (int64_t)n * K;
-  const int64_t tiles_per_panel = (nq + kTcRows - 1) / kTcRows;
-  const int64_t ntiles = tiles_per_panel * np;
-  for (int64_t tile = (int64_t)blockIdx.x * kTcGroups + g; tile < ntiles; tile += (int64_t)gridDim.x * kTcGroups) {
-    const size_t po = (size_t)(tile / tiles_per_panel) * pstride;
-    const int64_t q = (tile % tiles_per_panel) * kTcRows + rr;
+  // 32-bit tile arithmetic (the launch checks that the tiles fit): one panel / offset division per
+  // tile instead of a 64-bit one
+  const uint32_t tiles_per_panel = (uint32_t)((nq + kTcRows - 1) / kTcRows);
+  const uint32_t ntiles = tiles_per_panel * (uint32_t)np;
+  for (uint32_t tile = blockIdx.x * kTcGroups + g; tile < ntiles; tile += gridDim.x * kTcGroups) {
+    const uint32_t panel = tile / tiles_per_panel;
+    const size_t po = (size_t)panel * pstride;
+    const int64_t q = (int64_t)(tile - panel * tiles_per_panel) * kTcRows + rr;
     float f[16];
     float dsc = 0.f;
     T xv = T(0);
@@ -742,6 +747,7 @@ void launch_mlp_smooth(const MlpWeights& w, int n, int W, const int32_t* col, co
                        const T* r, const T* x, int zero_x, T* out, int np, cudaStream_t s) {
   if (w.engine == 1) {
     const long long tiles = ((long long)n * K + kTcRows - 1) / kTcRows * np;
+    require(tiles < (1LL << 31), "mlp: too many sample tiles for one launch");
     k_mlp_smooth_tcg<T, K><<<tc_grid(tiles), kTcThreads, kTcSmemBytes, s>>>(w, n, W, col, tab, diag, r, x, zero_x,
                                                                           out, (size_t)n * K, np, w.err);
     DEC_CHECK_LAUNCH();
@@ -1227,13 +1233,22 @@ __global__ void __launch_bounds__(kGradThreads) k_train_grad_tc(int64_t B, int64
   float sacc = 0.f;  // this thread's bias / w3 sum (threads 0 .. 192)
   const int64_t lo = blockIdx.x * chunk, hi = min(B, lo + chunk);
   for (int64_t b0 = lo; b0 < hi; b0 += kGradStage) {
+    // the slice arrives by asynchronous copies, all in flight before the one wait (a load and a
+    // store per element serialised the staging on the load latency)
     for (int e = threadIdx.x; e < kRows * kGradStage; e += kGradThreads) {
       const int row = e / kGradStage, c = e % kGradStage;
       const int64_t q = b0 + c;
-      float v = 0.f;
-      if (q < hi) v = row < kActRows ? act[(size_t)row * B + q] : dyb[q];
-      sa[row * kLd + c] = v;
+      float* dst = sa + row * kLd + c;
+      if (q < hi) {
+        const float* src = row < kActRows ? act + (size_t)row * B + q : dyb + q;
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                     "l"(src)
+                     : "memory");
+      } else {
+        *dst = 0.f;
+      }
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
 #pragma unroll
     for (int ks = 0; ks < kGradStage; ks += 16) {
@@ -1306,7 +1321,15 @@ __global__ void __launch_bounds__(kGradThreads) k_train_grad_tc(int64_t B, int64
 __global__ void k_grad_reduce(int nchunks, const float* __restrict__ gpart, float* __restrict__ grad) {
   for (int pi = blockIdx.x * blockDim.x + threadIdx.x; pi < kMlpNParam; pi += gridDim.x * blockDim.x) {
     float s = 0.f;
-    for (int c = 0; c < nchunks; ++c) s += gpart[(size_t)c * kMlpNParam + pi];
+    int c = 0;
+    for (; c + 8 <= nchunks; c += 8) {  // eight loads in flight, added in chunk order
+      float v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = gpart[(size_t)(c + u) * kMlpNParam + pi];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) s += v[u];
+    }
+    for (; c < nchunks; ++c) s += gpart[(size_t)c * kMlpNParam + pi];
     grad[pi] = s;
   }
 }
