@@ -1318,18 +1318,23 @@ __global__ void __launch_bounds__(kGradThreads) k_train_grad_tc(int64_t B, int64
   else if (threadIdx.x == 3 * kMlpH) out[kOffB3] = sacc;
 }
 
-__global__ void k_grad_reduce(int nchunks, const float* __restrict__ gpart, float* __restrict__ grad) {
+// The chunk partials summed in a fixed order, in two levels: group g of kReduceGroups adds chunks
+// g, g + G, g + 2G, ... (in increasing order) into red[g]; then the groups are added in order.
+constexpr int kReduceGroups = 16;
+__global__ void k_grad_reduce(int nchunks, const float* __restrict__ gpart, float* __restrict__ red) {
+  const int g = blockIdx.y;
   for (int pi = blockIdx.x * blockDim.x + threadIdx.x; pi < kMlpNParam; pi += gridDim.x * blockDim.x) {
     float s = 0.f;
-    int c = 0;
-    for (; c + 8 <= nchunks; c += 8) {  // eight loads in flight, added in chunk order
-      float v[8];
+    for (int c = g; c < nchunks; c += kReduceGroups) s += gpart[(size_t)c * kMlpNParam + pi];
+    red[(size_t)g * kMlpNParam + pi] = s;
+  }
+}
+
+__global__ void k_grad_reduce2(const float* __restrict__ red, float* __restrict__ grad) {
+  for (int pi = blockIdx.x * blockDim.x + threadIdx.x; pi < kMlpNParam; pi += gridDim.x * blockDim.x) {
+    float s = 0.f;
 #pragma unroll
-      for (int u = 0; u < 8; ++u) v[u] = gpart[(size_t)(c + u) * kMlpNParam + pi];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) s += v[u];
-    }
-    for (; c < nchunks; ++c) s += gpart[(size_t)c * kMlpNParam + pi];
+    for (int g = 0; g < kReduceGroups; ++g) s += red[(size_t)g * kMlpNParam + pi];
     grad[pi] = s;
   }
 }
@@ -1384,7 +1389,8 @@ static void ensure_scratch(dec_mlp& m, size_t N, size_t B, int S) {
   }
   if (m.nrm.n < (size_t)S) m.nrm.alloc(std::max<size_t>(S, 64));
   if (m.lpart.n < (size_t)kLossBlocks) m.lpart.alloc(kLossBlocks);
-  if (m.gpart.n < (size_t)kMaxChunks * kMlpNParam) m.gpart.alloc((size_t)kMaxChunks * kMlpNParam);
+  if (m.gpart.n < (size_t)(kMaxChunks + kReduceGroups) * kMlpNParam)
+    m.gpart.alloc((size_t)(kMaxChunks + kReduceGroups) * kMlpNParam);
 }
 
 static int grad_chunks(int64_t B, int64_t* chunk) {
@@ -1397,7 +1403,9 @@ static void reduce_grad(dec_mlp& m, int64_t B, float* grad, cudaStream_t s) {
   int64_t chunk;
   const int nch = grad_chunks(B, &chunk);
   k_train_grad_tc<<<nch, kGradThreads, 0, s>>>(B, chunk, m.act.p, m.dyb.p, m.gpart.p);
-  k_grad_reduce<<<(kMlpNParam + 255) / 256, 256, 0, s>>>(nch, m.gpart.p, grad);
+  float* red = m.gpart.p + (size_t)kMaxChunks * kMlpNParam;  // after the chunk partials
+  k_grad_reduce<<<dim3((kMlpNParam + 255) / 256, kReduceGroups), 256, 0, s>>>(nch, m.gpart.p, red);
+  k_grad_reduce2<<<(kMlpNParam + 255) / 256, 256, 0, s>>>(red, grad);
   DEC_CHECK_LAUNCH();
 }
 
