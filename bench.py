@@ -252,6 +252,38 @@ def measure_operators(dec, peak, cpu=True):
     return out
 
 
+def training_tensor_flop(steps, batch=65536, levels=(5, 6, 7), block=10):
+    """Tensor-core FLOP of `steps` training steps of learned.train_smoother's schedule: per step the
+    forward over every sample of its fields (2·(16·64 + 64·64) = 10,240 per sample), and per batch
+    sample the recomputed forward (10,240), dh1 = W2ᵀ dz2 with dz2 as two BF16 parts (2·2·64·64 =
+    16,384) and the weight gradients with dz as two parts (dW2 16,384, dW1 4,096)."""
+    n = {lv: 10 * 4 ** lv + 2 for lv in levels}
+    per_step = {5: 6, 6: 2, 7: 1}
+    total, t = 0.0, 0
+    while t < steps:
+        for lv in levels:
+            if t >= steps:
+                break
+            nb = min(block, steps - t)
+            N = n[lv] * per_step.get(lv, 1)
+            total += nb * (N * 10240.0 + min(batch, N) * (10240.0 + 16384.0 + 16384.0 + 4096.0))
+            t += nb
+    return total
+
+
+def run_train(args):
+    """The learned smoother's training alone (the entry point for the training launch list)."""
+    import torch
+    dec = load_package()
+    from dec_b200 import learned
+    t0 = time.perf_counter()
+    mlp, losses = learned.train_smoother(steps=args.train_steps, lr=1e-3, batch=65536, seed=4, shift=SHIFT)
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    print(json.dumps({"train_steps": args.train_steps, "seconds": t, "final_loss": losses[-1][2],
+                      "tensor_TFLOP": training_tensor_flop(args.train_steps) / 1e12}), flush=True)
+
+
 def measure_learned(dec, args, B, U64, common, timed):
     """The learned smoother: trained on the GPU (Adam, lr 1e-3, batch 65,536 vertex samples, seed
     4) on V-cycle (residual, error) pairs of icospheres L5-L7, then used as the smoother at every
@@ -265,7 +297,10 @@ def measure_learned(dec, args, B, U64, common, timed):
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     ico = dec.meshes.icosahedron()
-    out = {"train": {"steps": args.train_steps, "seconds": train_s, "final_losses": [round(l, 4) for _, _, l in losses[-3:]]}}
+    flop = training_tensor_flop(args.train_steps)
+    out = {"train": {"steps": args.train_steps, "seconds": train_s, "final_losses": [round(l, 4) for _, _, l in losses[-3:]],
+                     "tensor_TFLOP": flop / 1e12, "tensor_TFLOP/s_incl_setup": flop / train_s / 1e12,
+                     "engine": "mma.sync m16n8k16 (forward, backward, weight gradients)"}}
 
     def run(level, smoother, sweeps, Bm, Uref=None, engine="tcgen05"):
         # the learned V(1,1) solve is fastest with 2 cycles per refinement step (measured 1, 2, 3)
@@ -1012,12 +1047,15 @@ def main():
                          "FP64 solve on the host")
     ap.add_argument("--mlp-engine", default="tcgen05", choices=["mma", "tcgen05"], dest="mlp_engine",
                     help="kernel engine of the learned smoothing step for --kernel mlp")
+    ap.add_argument("--train", action="store_true", help="train the learned smoother alone (--train-steps) and exit")
     ap.add_argument("--train-steps", type=int, default=20000, dest="train_steps",
                     help="Adam steps of the learned smoother (0 skips the learned-smoother section)")
     args = ap.parse_args()
     if args.sweeps is not None:
         args.pre = args.post = args.sweeps
-    if args.op:
+    if args.train:
+        run_train(args)
+    elif args.op:
         run_op(args)
     elif args.kernel:
         run_kernel(args)
