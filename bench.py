@@ -893,6 +893,7 @@ def run_ours(args):
                 "l2": "inputs larger than L2 (b: 168 MB FP64 per step)",
                 "parallelism": f"replicas x{world} (independent batches, no collective)",
                 "setup_seconds": setup_s,
+                "tuned_variants": {k: v for k, v in dec.tune_entries().items() if k.startswith(("sweep/", "cheb2/"))},
             },
             "learned_fp32_vs_plain_fp64": learned_ratio,
             "comparison": {"plain_fp64_vcycle_solves_per_s": plain_value,

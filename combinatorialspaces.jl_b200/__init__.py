@@ -346,6 +346,21 @@ def tune_clear():
     check(lib().dec_tune_clear())
 
 
+def tune_entries():
+    """The autotuner's table as a dict (through dec_tune_save into a temporary file)."""
+    import json
+    import os
+    import tempfile
+    fd, path = tempfile.mkstemp(suffix=".json")
+    os.close(fd)
+    try:
+        tune_save(path)
+        with open(path) as f:
+            return json.load(f)["entries"]
+    finally:
+        os.unlink(path)
+
+
 def tune_save(path):
     """Write the autotuner's table as JSON (dec_tune_save)."""
     check(lib().dec_tune_save(str(path).encode()))

@@ -247,6 +247,22 @@ static void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStre
   DEC_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
 }
 
+template <class... KArgs, class... Args>
+static void launch_pdl_smem(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                            Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  DEC_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
+}
+
 // Storage type T of the panel vectors and the type C the kernels compute in: FP16 storage
 // (precision 2) computes in FP32.
 template <class T> struct Cmp { using t = T; };
@@ -469,6 +485,120 @@ __global__ void __launch_bounds__(TB) k_sweep_u(int n, int Wr, const int32_t* __
                                                 SweepPrm<CT<T>> prm, size_t pstride, const CT<T>* __restrict__ shf,
                                                 double* __restrict__ u64) {
   sweep_rows<T, K, W, SH, true, VV>(n, Wr, col, off, diag, dinv, b, x, out, prm, pstride, shf, u64);
+}
+
+// Two Chebyshev steps in one pass (post-smoothing from a given iterate x0, FP32 panels): step 1
+// (S_CHEB0) on the rows of a patch and of its 1-ring from x0 staged in shared memory with the 2-ring,
+// then step 2 (S_CHEBN, x_prev = x0) on the patch rows from step 1's result, also in shared memory.
+// x0 is read once with its halo, b once per step, and only the second step's result is written, where
+// two sweeps move the operator twice and seven vectors.  A CTA takes one patch and KS of the panel's K
+// right-hand sides (grid.y), four per lane.  The per-element arithmetic is sweep_rows', statement for
+// statement, so the result is the two sweeps' bit for bit.  UPD: u += (double) x2 as k_sweep_u.
+constexpr int kTwoStepRows = 512;
+template <int K, int KS, int W, bool UPD>
+__global__ void __launch_bounds__(TB) k_cheb2(int n, int P, int max_local, const int32_t* __restrict__ hptr,
+                                              const int32_t* __restrict__ h1n, const int32_t* __restrict__ halo,
+                                              const int32_t* __restrict__ lptr, const uint16_t* __restrict__ lcol,
+                                              const float* __restrict__ off, const float* __restrict__ diag,
+                                              const float* __restrict__ dinv, const float* __restrict__ b,
+                                              const float* __restrict__ x0, float* __restrict__ out, float inv_theta,
+                                              float c1, float c2, size_t pstride, double* __restrict__ u64) {
+  static_assert(KS % 4 == 0 && K % KS == 0, "slices of whole float4 lanes");
+  constexpr int LPR = KS / 4, RPP = TB / LPR;
+  extern __shared__ float4 tsm[];
+  pdl_enter();
+  const int patch = blockIdx.x;
+  const int lane = threadIdx.x % LPR, sub = threadIdx.x / LPR;
+  const size_t po = (size_t)blockIdx.z * pstride + (size_t)blockIdx.y * KS + (size_t)lane * 4;
+  const int a = patch * P, pr = min(P, n - a);
+  const int hb = hptr[patch], nh = hptr[patch + 1] - hb, n1 = h1n[patch];
+  const int nloc = pr + nh, nl1 = pr + n1;
+  float4* X0 = tsm;
+  float4* X1 = tsm + (size_t)max_local * LPR;
+  const uint16_t* lc = lcol + (size_t)lptr[patch] * W;
+  for (int lr = sub; lr < nloc; lr += RPP) {
+    const int g = lr < pr ? a + lr : halo[hb + lr - pr];
+    X0[lr * LPR + lane] = *reinterpret_cast<const float4*>(x0 + po + (size_t)g * K);
+  }
+  __syncthreads();
+  for (int lr = sub; lr < nl1; lr += RPP) {  // step 1
+    const int g = lr < pr ? a + lr : halo[hb + lr - pr];
+    const float4 b4 = *reinterpret_cast<const float4*>(b + po + (size_t)g * K);
+    const float4 x4 = X0[lr * LPR + lane];
+    float r[4] = {b4.x, b4.y, b4.z, b4.w}, xi[4] = {x4.x, x4.y, x4.z, x4.w}, acc[4];
+    const float dg = diag[g];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = dg * xi[q];
+    int cs[W];
+    float vs[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      cs[k] = lc[lr * W + k];
+      vs[k] = off[(size_t)g * W + k];
+    }
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      const float4 nb4 = X0[cs[k] * LPR + lane];
+      const float nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] += vs[k] * nb[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) r[q] = r[q] - acc[q];
+    float di[4], o[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) di[q] = dinv[g];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float dn = (di[q] * r[q]) * inv_theta;
+      o[q] = xi[q] + dn;
+    }
+    X1[lr * LPR + lane] = make_float4(o[0], o[1], o[2], o[3]);
+  }
+  __syncthreads();
+  for (int lr = sub; lr < pr; lr += RPP) {  // step 2
+    const int g = a + lr;
+    const size_t ik = po + (size_t)g * K;
+    const float4 b4 = *reinterpret_cast<const float4*>(b + ik);
+    const float4 x4 = X1[lr * LPR + lane], p4 = X0[lr * LPR + lane];
+    float r[4] = {b4.x, b4.y, b4.z, b4.w}, xi[4] = {x4.x, x4.y, x4.z, x4.w}, xp[4] = {p4.x, p4.y, p4.z, p4.w};
+    float acc[4];
+    const float dg = diag[g];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = dg * xi[q];
+    int cs[W];
+    float vs[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      cs[k] = lc[lr * W + k];
+      vs[k] = off[(size_t)g * W + k];
+    }
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      const float4 nb4 = X1[cs[k] * LPR + lane];
+      const float nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] += vs[k] * nb[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) r[q] = r[q] - acc[q];
+    float di[4], o[4], dn[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) di[q] = dinv[g];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) dn[q] = xi[q] - xp[q];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      dn[q] = c1 * dn[q] + c2 * (di[q] * r[q]);
+      o[q] = xi[q] + dn[q];
+    }
+    if constexpr (UPD) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) u64[ik + q] += (double)(float)o[q];
+    } else {
+      *reinterpret_cast<float4*>(out + ik) = make_float4(o[0], o[1], o[2], o[3]);
+    }
+  }
 }
 
 // FP16-stored sweeps carry eight values per 16-byte access; unbounded they took 72 registers
@@ -1284,6 +1414,16 @@ struct Level {
   // tuned FP32 sweep variant per panel width 8 / 16 / 32 (index 3 / 4 / 5), cached per table version
   mutable unsigned sweep_tuned_at[6] = {0, 0, 0, 0, 0, 0};
   mutable int sweep_vv[6] = {0, 0, 0, 0, 0, 0};
+  // The two-step Chebyshev pair (k_cheb2): patches of P consecutive internal rows, each with its
+  // 1-ring halo H1 then its 2-ring halo H2 (internal row ids in halo[hptr[p] ..], |H1| = h1n[p]), and
+  // the local column of every slot of the patch and H1 rows (lcol, rows from lptr[p]; local numbering:
+  // patch rows, then H1, then H2).  Built on the host the first time it is used.
+  struct TwoStep {
+    int P = 0, npatch = 0, max_local = 0, max_l1 = 0;
+    double sum_local = 0, sum_l1 = 0;
+    DArr<int32_t> hptr, h1n, halo, lptr;
+    DArr<uint16_t> lcol;
+  } ts;
 };
 
 template <class T>
@@ -2132,6 +2272,127 @@ static void launch_sweep(const Level& L, const T* b, const T* x, T* out, SweepPr
   }
 }
 
+// ---- the two-step Chebyshev pair ----------------------------------------------------------------
+// Tuning key: 1 = the post-smoothing pair of this level runs as k_cheb2, 0 (default) = two sweeps.
+static std::string cheb2_key(int K, int W, int n) {
+  return "cheb2/f32/K" + std::to_string(K) + "/W" + std::to_string(W) + "/n" + std::to_string(size_bucket(n));
+}
+constexpr int kCheb2MinRows = 1 << 14;  // smaller levels stay with the sweeps (launch-bound)
+
+// The patches and halos of level L (host, from the internal slot-major operator columns).
+static void build_two_step(Level& L) {
+  const int n = L.n, W = L.W, P = kTwoStepRows;
+  const std::vector<int32_t> col = L.col.download();
+  const int npatch = (n + P - 1) / P;
+  std::vector<int32_t> hptr(npatch + 1, 0), h1n(npatch, 0), lptr(npatch + 1, 0), halo, loc(n, 0), stamp(n, -1);
+  std::vector<uint16_t> lcol;
+  halo.reserve((size_t)n);
+  lcol.reserve((size_t)n * W * 5 / 4);
+  int max_local = 0, max_l1 = 0;
+  double sum_local = 0, sum_l1 = 0;
+  for (int p = 0; p < npatch; ++p) {
+    const int a = p * P, e = std::min(n, a + P), pr = e - a;
+    auto local = [&](int g) { return stamp[g] == p ? loc[g] : -1; };
+    auto add = [&](int g, int id) {
+      stamp[g] = p;
+      loc[g] = id;
+    };
+    for (int r = a; r < e; ++r) add(r, r - a);
+    int next = pr;
+    hptr[p] = (int)halo.size();
+    for (int r = a; r < e; ++r)
+      for (int k = 0; k < W; ++k) {
+        const int c = col[(size_t)r * W + k];
+        if (local(c) < 0) {
+          add(c, next++);
+          halo.push_back(c);
+        }
+      }
+    const int n1 = next - pr;
+    h1n[p] = n1;
+    for (int h = hptr[p]; h < hptr[p] + n1; ++h)
+      for (int k = 0; k < W; ++k) {
+        const int c = col[(size_t)halo[h] * W + k];
+        if (local(c) < 0) {
+          add(c, next++);
+          halo.push_back(c);
+        }
+      }
+    hptr[p + 1] = (int)halo.size();
+    require(next <= 65535, "multigrid: a two-step patch's halo exceeds 16-bit local indices");
+    lptr[p] = (int)(lcol.size() / W);
+    for (int lr = 0; lr < pr + n1; ++lr) {
+      const int g = lr < pr ? a + lr : halo[hptr[p] + lr - pr];
+      for (int k = 0; k < W; ++k) lcol.push_back((uint16_t)local(col[(size_t)g * W + k]));
+    }
+    lptr[p + 1] = (int)(lcol.size() / W);
+    max_local = std::max(max_local, next);
+    max_l1 = std::max(max_l1, pr + n1);
+    sum_local += next;
+    sum_l1 += pr + n1;
+  }
+  L.ts.P = P;
+  L.ts.npatch = npatch;
+  L.ts.max_local = max_local;
+  L.ts.max_l1 = max_l1;
+  L.ts.sum_local = sum_local;
+  L.ts.sum_l1 = sum_l1;
+  L.ts.hptr.upload(hptr);
+  L.ts.h1n.upload(h1n);
+  L.ts.lptr.upload(lptr);
+  L.ts.halo.upload(halo.empty() ? std::vector<int32_t>(1, 0) : halo);
+  L.ts.lcol.upload(lcol);
+}
+
+template <int K>
+static size_t cheb2_smem(const Level& L) {
+  constexpr int KS = K >= 16 ? 16 : K;
+  return (size_t)(L.ts.max_local + L.ts.max_l1) * KS * sizeof(float);
+}
+
+// Can level L's post-smoothing pair of panel width K run as k_cheb2 (FP32, rows of 6 off-diagonal
+// slots, no per-RHS shifts, built patches that fit the shared memory), and does the table ask for it?
+template <class T, int K>
+static bool cheb2_on(const Level& L, const CT<T>* cs) {
+  if constexpr (!std::is_same<T, float>::value || K < 16) {
+    return false;
+  } else {
+    if (cs || L.W != 6 || L.n < kCheb2MinRows || !L.ts.npatch) return false;
+    if (cheb2_smem<K>(L) > 200 * 1024) return false;
+    return tune_get(cheb2_key(K, L.W, L.n), 0) == 1;
+  }
+}
+
+template <class T, int K>
+static void launch_cheb2(const Level& L, const T* b, const T* x, T* out, double inv_theta, double c1, double c2,
+                         int np, cudaStream_t s, double* upd) {
+  if constexpr (std::is_same<T, float>::value && K >= 16) {
+    constexpr int KS = 16;
+    const size_t smem = cheb2_smem<K>(L);
+    const size_t ps = (size_t)L.n * K;
+    {
+      const double v = KS * 4.0, opr = L.W * (2.0 + 4.0) + 8.0;  // local columns, values, diag, 1/diag
+      const double per_slice = L.ts.sum_local * v + L.ts.sum_l1 * (v + opr) + (double)L.n * (v + opr) +
+                               (double)L.n * (upd ? 2.0 * KS * 8.0 : v);
+      add_bytes((double)(K / KS) * np * per_slice + (double)L.ts.sum_local * 4.0);
+    }
+    auto go = [&](auto kern) {
+      static bool opted = false;  // per kernel instance: the dynamic shared memory above 48 KB
+      if (!opted) {
+        DEC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        opted = true;
+      }
+      launch_pdl_smem(kern, dim3(L.ts.npatch, K / KS, np), dim3(TB), smem, s, L.n, L.ts.P, L.ts.max_local,
+                      (const int32_t*)L.ts.hptr.p, (const int32_t*)L.ts.h1n.p, (const int32_t*)L.ts.halo.p,
+                      (const int32_t*)L.ts.lptr.p, (const uint16_t*)L.ts.lcol.p, (const float*)L.off32.p,
+                      (const float*)L.diag32.p, (const float*)L.dinv32.p, b, x, out, (float)inv_theta, (float)c1,
+                      (float)c2, ps, upd);
+    };
+    if (upd) go(k_cheb2<K, KS, 6, true>);
+    else go(k_cheb2<K, KS, 6, false>);
+  }
+}
+
 // Smooth `sweeps` times starting from x (zero if zero_x); returns the buffer holding the result.
 template <class T, int K>
 static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool zero_x, int sweeps, int np,
@@ -2165,6 +2426,12 @@ static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool z
   const double theta = (hi + lo) / 2, delta = (hi - lo) / 2, sigma = theta / delta;
   double rho = 1 / sigma;
   const bool started_at_zero = zero_x;
+  if (o.smoother == DEC_SMOOTH_CHEBYSHEV && sweeps == 2 && !zero_x && cheb2_on<T, K>(L, B.cs)) {
+    // the two steps in one pass: the coefficients of the loop below for it = 0 and it = 1
+    const double rho_new = 1 / (2 * sigma - rho);
+    launch_cheb2<T, K>(L, B.b.p, x, other, 1.0 / theta, rho_new * rho, 2 * rho_new / delta, np, s, upd);
+    return other;
+  }
   for (int it = 0; it < sweeps; ++it) {
     SweepPrm<C> prm{};
     prm.zero_x = zero_x ? 1 : 0;
@@ -2503,7 +2770,17 @@ static int64_t count_kernel_nodes(cudaGraph_t g) {
   return k;
 }
 
+// Builds the two-step patches of every level whose table entry asks for the pair at panel width K
+// (host work and uploads: before a capture starts).
+static void ensure_two_step(dec_mg& mg, int K) {
+  if (mg.opt.smoother != DEC_SMOOTH_CHEBYSHEV || mg.opt.precision != 1 || K < 16) return;
+  for (Level& L : mg.lv)
+    if (!L.ts.npatch && L.W == 6 && L.n >= kCheb2MinRows && tune_get(cheb2_key(K, L.W, L.n), 0) == 1)
+      build_two_step(L);
+}
+
 static cudaGraphExec_t capture(dec_mg& mg, Workspace& w, int kind) {
+  ensure_two_step(mg, w.K);
   cudaGraph_t g = nullptr;
   require(mg.opt.smoother != DEC_SMOOTH_LEARNED || mg.mlp != nullptr || kind == G_VCYCLE_PLAIN || kind == G_RESID,
           "multigrid: the learned smoother needs a network (dec_mg_set_smoother_mlp)");
@@ -2645,6 +2922,7 @@ static void enqueue_first_rhs(const dec_mg& mg, Workspace& w, cudaStream_t s) {
 // When the step ends in a Jacobi / Chebyshev post-sweep (fused_update), the body's u += e is that
 // sweep's epilogue (G_STEP) instead of a pass of its own.
 static void capture_solve(dec_mg& mg, Workspace& w, bool zero_guess) {
+  ensure_two_step(mg, w.K);
   if (w.bn2.n < (size_t)w.K * w.npanels) w.bn2.alloc((size_t)w.K * w.npanels);
   if (!w.loop.p) w.loop.alloc(1);
   cudaGraph_t g = nullptr;
@@ -3285,6 +3563,40 @@ int mg_autotune(dec_mg* mg, int nrhs, int reps, void* stream) {
     }
     set_all(best_v);
   }
+  // Chebyshev post-smoothing pairs (post = 2) on FP32 panels of 16 or more: the two steps as one
+  // temporal-blocked pass (k_cheb2) or as two sweeps, timed on the same V-cycle with the choice on every
+  // level of at least kCheb2MinRows rows
+  if (prec == 1 && best >= 16 && mg->opt.smoother == DEC_SMOOTH_CHEBYSHEV && mg->post_at(0) == 2) {
+    Workspace& w = workspace_k(*mg, nrhs, prec, best);
+    auto set_all = [&](int v) {
+      for (const Level& L : mg->lv)
+        if (L.W == 6 && L.n >= kCheb2MinRows) tune_set(cheb2_key(best, L.W, L.n), v);
+      w.drop_graphs();
+    };
+    int best_c = 0;
+    double best_ct = 1e300;
+    for (int v : {0, 1}) {
+      set_all(v);
+      w.graph[G_VCYCLE] = capture(*mg, w, G_VCYCLE);
+      DEC_CUDA(cudaGraphLaunch(w.graph[G_VCYCLE], s));
+      std::vector<float> ts;
+      for (int r = 0; r < std::max(3, reps); ++r) {
+        DEC_CUDA(cudaEventRecord(e0, s));
+        DEC_CUDA(cudaGraphLaunch(w.graph[G_VCYCLE], s));
+        DEC_CUDA(cudaEventRecord(e1, s));
+        DEC_CUDA(cudaEventSynchronize(e1));
+        float t = 0;
+        cudaEventElapsedTime(&t, e0, e1);
+        ts.push_back(t);
+      }
+      std::sort(ts.begin(), ts.end());
+      if (ts[ts.size() / 2] < best_ct) {
+        best_ct = ts[ts.size() / 2];
+        best_c = v;
+      }
+    }
+    set_all(best_c);
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   for (int K = 1; K <= 32; K <<= 1) {
@@ -3432,6 +3744,7 @@ static void per_group(dec_batch& bt, F&& f) {
 //   WHILE (test): { per group: V-cycles, u += e, r = b - A u, norms;  test }
 //   per group: u out of panels.
 static cudaGraphExec_t batch_capture(dec_batch& bt, double* const* u, const double* const* rhs, const int* nrhs) {
+  for (size_t q = 0; q < bt.groups.size(); ++q) ensure_two_step(*bt.groups[q], bt.used[q]->K);
   cudaGraph_t g = nullptr;
   DEC_CUDA(cudaGraphCreate(&g, 0));
   const int G = (int)bt.groups.size();

@@ -65,3 +65,37 @@ def test_sweep_lane_variants_same_cycles(dec, tmp_path):
     np.testing.assert_array_equal(res[0][0], res[1][0])
     assert res[0][1] == res[1][1]
     dec.tune_clear()
+
+
+def _cheb2_keys(levels, K=32):
+    return [f"cheb2/f32/K{K}/W6/n{int(np.log2(10 * 4 ** k + 2))}" for k in range(levels + 1)
+            if 10 * 4 ** k + 2 >= 1 << 14]
+
+
+def test_two_step_chebyshev_pair_same_bits(dec):
+    """The temporal-blocked post-smoothing pair (k_cheb2: both Chebyshev steps in one pass over patches
+    with their halos in shared memory) gives the two sweeps' results bit for bit: V-cycles from a
+    given iterate, and the refined solve whose last sweep adds into the FP64 iterate."""
+    dec.tune_clear()
+    ico = dec.meshes.icosahedron()
+    kw = dict(shift=1.0, center="circumcenter", project_radius=1.0, precision=1, pre=0, post=2, cheb_ratio=3.0,
+              inner_cycles=3, rhs_block=32)
+    n = 10 * 4 ** 7 + 2
+    B = torch.tensor(np.stack([uniform(90 + j, n) for j in range(32)]), device="cuda")
+    U0 = torch.tensor(np.stack([uniform(190 + j, n) for j in range(32)]) * 0.1, device="cuda")
+    out = []
+    for v in (0, 1):
+        for k in _cheb2_keys(7):
+            dec.tune_set(k, v)
+        h = dec.MultigridData(ico, 7, **kw)
+        U = h.cycles(U0.clone(), B, 2).cpu().numpy()
+        X, rep = h.solve(torch.zeros_like(B), B, rtol=1e-9, use_initial_guess=False)
+        assert rep.converged == 1
+        out.append((U, X.cpu().numpy(), rep.iterations))
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2]
+    mg = dec.MultigridData(ico, 7, **kw)
+    mg.autotune(32, reps=2)
+    assert all(dec.tune_get(k) in (0, 1) for k in _cheb2_keys(7))
+    dec.tune_clear()
