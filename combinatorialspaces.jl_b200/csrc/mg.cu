@@ -25,6 +25,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <numeric>
 
@@ -2331,6 +2332,13 @@ static void build_two_step(Level& L) {
     sum_local += next;
     sum_l1 += pr + n1;
   }
+  // every local column of a patch row or H1 row lies inside its patch's local rows (patch, H1, H2)
+  for (int p = 0; p < npatch; ++p) {
+    const int pr = std::min(n, (p + 1) * P) - p * P, nloc = pr + hptr[p + 1] - hptr[p];
+    for (size_t q = (size_t)lptr[p] * W; q < (size_t)lptr[p + 1] * W; ++q)
+      require(lcol[q] < nloc, "multigrid: a two-step patch's local column falls outside its rows");
+    require(lptr[p + 1] - lptr[p] == pr + h1n[p], "multigrid: two-step local rows do not match the patch");
+  }
   L.ts.P = P;
   L.ts.npatch = npatch;
   L.ts.max_local = max_local;
@@ -2342,6 +2350,24 @@ static void build_two_step(Level& L) {
   L.ts.lptr.upload(lptr);
   L.ts.halo.upload(halo.empty() ? std::vector<int32_t>(1, 0) : halo);
   L.ts.lcol.upload(lcol);
+}
+
+// The dynamic shared memory above 48 KB that k_cheb2 needs, for both of its instances at panel widths
+// 16 and 32, once per device (a host call that must not run inside a stream capture).
+static void cheb2_opt_in() {
+  static std::mutex mu;
+  static uint64_t done = 0;  // bit per device ordinal
+  int dev = 0;
+  DEC_CUDA(cudaGetDevice(&dev));
+  require(dev >= 0 && dev < 64, "multigrid: device ordinal out of range");
+  std::lock_guard<std::mutex> lock(mu);
+  if (done & (1ull << dev)) return;
+  constexpr int kMax = 200 * 1024;
+  DEC_CUDA(cudaFuncSetAttribute(k_cheb2<16, 16, 6, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMax));
+  DEC_CUDA(cudaFuncSetAttribute(k_cheb2<16, 16, 6, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMax));
+  DEC_CUDA(cudaFuncSetAttribute(k_cheb2<32, 16, 6, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMax));
+  DEC_CUDA(cudaFuncSetAttribute(k_cheb2<32, 16, 6, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMax));
+  done |= 1ull << dev;
 }
 
 template <int K>
@@ -2376,12 +2402,7 @@ static void launch_cheb2(const Level& L, const T* b, const T* x, T* out, double 
                                (double)L.n * (upd ? 2.0 * KS * 8.0 : v);
       add_bytes((double)(K / KS) * np * per_slice + (double)L.ts.sum_local * 4.0);
     }
-    auto go = [&](auto kern) {
-      static bool opted = false;  // per kernel instance: the dynamic shared memory above 48 KB
-      if (!opted) {
-        DEC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        opted = true;
-      }
+    auto go = [&](auto kern) {  // both instances were opted in before the capture (cheb2_opt_in)
       launch_pdl_smem(kern, dim3(L.ts.npatch, K / KS, np), dim3(TB), smem, s, L.n, L.ts.P, L.ts.max_local,
                       (const int32_t*)L.ts.hptr.p, (const int32_t*)L.ts.h1n.p, (const int32_t*)L.ts.halo.p,
                       (const int32_t*)L.ts.lptr.p, (const uint16_t*)L.ts.lcol.p, (const float*)L.off32.p,
@@ -2775,8 +2796,10 @@ static int64_t count_kernel_nodes(cudaGraph_t g) {
 static void ensure_two_step(dec_mg& mg, int K) {
   if (mg.opt.smoother != DEC_SMOOTH_CHEBYSHEV || mg.opt.precision != 1 || K < 16) return;
   for (Level& L : mg.lv)
-    if (!L.ts.npatch && L.W == 6 && L.n >= kCheb2MinRows && tune_get(cheb2_key(K, L.W, L.n), 0) == 1)
-      build_two_step(L);
+    if (L.W == 6 && L.n >= kCheb2MinRows && tune_get(cheb2_key(K, L.W, L.n), 0) == 1) {
+      cheb2_opt_in();
+      if (!L.ts.npatch) build_two_step(L);
+    }
 }
 
 static cudaGraphExec_t capture(dec_mg& mg, Workspace& w, int kind) {
