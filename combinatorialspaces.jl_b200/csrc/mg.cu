@@ -336,6 +336,17 @@ static inline void add_bytes(double b) {
   if (t_bytes) *t_bytes += b;
 }
 
+// The sweep's row arithmetic with each rounding pinned (no contraction choices left to the compiler),
+// so the one-step sweeps and the two-step pair (k_cheb2) compute the same bits.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 // VV > 0 overrides the vector width (a tuned variant: VV = 2 on FP32 panels of K >= 8 puts twice the
 // lanes on a row).
 template <class T, int K, int VV = 0>
@@ -385,8 +396,8 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
       C acc[V];
 #pragma unroll
       for (int q = 0; q < V; ++q) {
-        if constexpr (SH) acc[q] = (dg + csv[q]) * xi[q];
-        else acc[q] = dg * xi[q];
+        if constexpr (SH) acc[q] = mul_rn(add_rn(dg, csv[q]), xi[q]);
+        else acc[q] = mul_rn(dg, xi[q]);
       }
       const int32_t* c = col + (size_t)i * w;
       const C* v = off + (size_t)i * w;
@@ -403,7 +414,7 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
           C nb[V];
           ldv<T, V>(x + po + (size_t)cs[s] * K, nb);
 #pragma unroll
-          for (int q = 0; q < V; ++q) acc[q] += vs[s] * nb[q];
+          for (int q = 0; q < V; ++q) acc[q] = fma_rn(vs[s], nb[q], acc[q]);
         }
       } else {
         for (int s = 0; s < w; ++s) {
@@ -411,11 +422,11 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
           ldv<T, V>(x + po + (size_t)c[s] * K, nb);
           const C vv = v[s];
 #pragma unroll
-          for (int q = 0; q < V; ++q) acc[q] += vv * nb[q];
+          for (int q = 0; q < V; ++q) acc[q] = fma_rn(vv, nb[q], acc[q]);
         }
       }
 #pragma unroll
-      for (int q = 0; q < V; ++q) r[q] = r[q] - acc[q];
+      for (int q = 0; q < V; ++q) r[q] = sub_rn(r[q], acc[q]);
     } else {
 #pragma unroll
       for (int q = 0; q < V; ++q) xi[q] = C(0);
@@ -438,8 +449,8 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
       C dn[V];
 #pragma unroll
       for (int q = 0; q < V; ++q) {
-        dn[q] = (di[q] * r[q]) * prm.inv_theta;
-        o[q] = xi[q] + dn[q];
+        dn[q] = mul_rn(mul_rn(di[q], r[q]), prm.inv_theta);
+        o[q] = add_rn(xi[q], dn[q]);
       }
     } else {
       C dn[V];
@@ -450,12 +461,12 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
         C xp[V];
         ldv<T, V>(out + ik, xp);
 #pragma unroll
-        for (int q = 0; q < V; ++q) dn[q] = xi[q] - xp[q];
+        for (int q = 0; q < V; ++q) dn[q] = sub_rn(xi[q], xp[q]);
       }
 #pragma unroll
       for (int q = 0; q < V; ++q) {
-        dn[q] = prm.c1 * dn[q] + prm.c2 * (di[q] * r[q]);
-        o[q] = xi[q] + dn[q];
+        dn[q] = fma_rn(prm.c1, dn[q], mul_rn(prm.c2, mul_rn(di[q], r[q])));
+        o[q] = add_rn(xi[q], dn[q]);
       }
     }
     if constexpr (UPD) {
@@ -494,7 +505,8 @@ __global__ void __launch_bounds__(TB) k_sweep_u(int n, int Wr, const int32_t* __
 // x0 is read once with its halo, b once per step, and only the second step's result is written, where
 // two sweeps move the operator twice and seven vectors.  A CTA takes one patch and KS of the panel's K
 // right-hand sides (grid.y), four per lane.  The per-element arithmetic is sweep_rows', statement for
-// statement, so the result is the two sweeps' bit for bit.  UPD: u += (double) x2 as k_sweep_u.
+// statement with every rounding pinned (mul_rn / fma_rn ...), so the result is the two sweeps' bit for
+// bit.  UPD: u += (double) x2 as k_sweep_u.
 constexpr int kTwoStepRows = 512;
 template <int K, int KS, int W, bool UPD>
 __global__ void __launch_bounds__(TB) k_cheb2(int n, int P, int max_local, const int32_t* __restrict__ hptr,
@@ -529,7 +541,7 @@ __global__ void __launch_bounds__(TB) k_cheb2(int n, int P, int max_local, const
     float r[4] = {b4.x, b4.y, b4.z, b4.w}, xi[4] = {x4.x, x4.y, x4.z, x4.w}, acc[4];
     const float dg = diag[g];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) acc[q] = dg * xi[q];
+    for (int q = 0; q < 4; ++q) acc[q] = mul_rn(dg, xi[q]);
     int cs[W];
     float vs[W];
 #pragma unroll
@@ -542,17 +554,17 @@ __global__ void __launch_bounds__(TB) k_cheb2(int n, int P, int max_local, const
       const float4 nb4 = X0[cs[k] * LPR + lane];
       const float nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
 #pragma unroll
-      for (int q = 0; q < 4; ++q) acc[q] += vs[k] * nb[q];
+      for (int q = 0; q < 4; ++q) acc[q] = fma_rn(vs[k], nb[q], acc[q]);
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) r[q] = r[q] - acc[q];
+    for (int q = 0; q < 4; ++q) r[q] = sub_rn(r[q], acc[q]);
     float di[4], o[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) di[q] = dinv[g];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const float dn = (di[q] * r[q]) * inv_theta;
-      o[q] = xi[q] + dn;
+      const float dn = mul_rn(mul_rn(di[q], r[q]), inv_theta);
+      o[q] = add_rn(xi[q], dn);
     }
     X1[lr * LPR + lane] = make_float4(o[0], o[1], o[2], o[3]);
   }
@@ -566,7 +578,7 @@ __global__ void __launch_bounds__(TB) k_cheb2(int n, int P, int max_local, const
     float acc[4];
     const float dg = diag[g];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) acc[q] = dg * xi[q];
+    for (int q = 0; q < 4; ++q) acc[q] = mul_rn(dg, xi[q]);
     int cs[W];
     float vs[W];
 #pragma unroll
@@ -579,19 +591,19 @@ __global__ void __launch_bounds__(TB) k_cheb2(int n, int P, int max_local, const
       const float4 nb4 = X1[cs[k] * LPR + lane];
       const float nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
 #pragma unroll
-      for (int q = 0; q < 4; ++q) acc[q] += vs[k] * nb[q];
+      for (int q = 0; q < 4; ++q) acc[q] = fma_rn(vs[k], nb[q], acc[q]);
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) r[q] = r[q] - acc[q];
+    for (int q = 0; q < 4; ++q) r[q] = sub_rn(r[q], acc[q]);
     float di[4], o[4], dn[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) di[q] = dinv[g];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) dn[q] = xi[q] - xp[q];
+    for (int q = 0; q < 4; ++q) dn[q] = sub_rn(xi[q], xp[q]);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      dn[q] = c1 * dn[q] + c2 * (di[q] * r[q]);
-      o[q] = xi[q] + dn[q];
+      dn[q] = fma_rn(c1, dn[q], mul_rn(c2, mul_rn(di[q], r[q])));
+      o[q] = add_rn(xi[q], dn[q]);
     }
     if constexpr (UPD) {
 #pragma unroll
