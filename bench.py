@@ -988,12 +988,15 @@ def run_kernel(args):
     right-hand sides: the entry point for ncu captures of a single kernel."""
     import torch
     dec = load_package()
-    kinds = {"sweep": 0, "residual": 1, "restrict": 2, "prolong": 3, "mlp": 4}
+    kinds = {"sweep": 0, "residual": 1, "restrict": 2, "prolong": 3, "mlp": 4, "pair": 5}
     kind = kinds[args.kernel]
     mg = dec.MultigridData(dec.meshes.icosahedron(), args.mesh_level, shift=SHIFT, center="circumcenter",
                            project_radius=1.0, smoother=3 if kind == 4 else 1, pre=max(1, args.pre),
                            post=max(1, args.post),
                            precision=args.precision, rhs_block=32, coarse_max=args.coarse_max)
+    if kind == 5 and args.variant:  # patch rows of the pair
+        n = mg.level_info(0)[0]
+        dec.tune_set(f"cheb2/f32/K32/W6/n{int(np.log2(n))}", args.variant)
     if kind == 4:
         mlp = dec.SmootherMLP(4)
         mlp.set_engine(args.mlp_engine)
@@ -1030,7 +1033,7 @@ def main():
     ap.add_argument("--no-ops", action="store_true", help="skip the operator-kernel roofline section")
     ap.add_argument("--profile", action="store_true",
                     help="run only the timed mixed-precision solves (inside an NVTX range 'timed')")
-    ap.add_argument("--kernel", choices=["sweep", "residual", "restrict", "prolong", "mlp"],
+    ap.add_argument("--kernel", choices=["sweep", "residual", "restrict", "prolong", "mlp", "pair"],
                     help="time one V-cycle kernel alone (steps launches after warmup) and exit")
     ap.add_argument("--mesh-level", type=int, default=LEVEL, dest="mesh_level")
     ap.add_argument("--precision", type=int, default=1, choices=[1, 2],
@@ -1039,7 +1042,8 @@ def main():
                     help="time one DEC operator kernel alone (steps launches after warmup) and exit")
     ap.add_argument("--dtype", default="float64", choices=["float64", "float32"])
     ap.add_argument("--autotune", action="store_true", help="--op laplacian: autotune the apply's variant first")
-    ap.add_argument("--variant", type=int, default=0, help="--op laplacian: rows per thread (1, 2, 4)")
+    ap.add_argument("--variant", type=int, default=0,
+                    help="--op laplacian: rows per thread (1, 2, 4); --kernel pair: patch rows (128, 256, 512)")
     ap.add_argument("--no-batch", action="store_true", dest="no_batch", help="skip the batched-workload section")
     ap.add_argument("--no-configs", action="store_true", dest="no_configs",
                     help="skip the L6 FP64 and L8 1e-10 sections")

@@ -507,7 +507,7 @@ __global__ void __launch_bounds__(TB) k_sweep_u(int n, int Wr, const int32_t* __
 // right-hand sides (grid.y), four per lane.  The per-element arithmetic is sweep_rows', statement for
 // statement with every rounding pinned (mul_rn / fma_rn ...), so the result is the two sweeps' bit for
 // bit.  UPD: u += (double) x2 as k_sweep_u.
-constexpr int kTwoStepRows = 512;
+constexpr int kTwoStepRows = 512;  // the largest patch (the tuned value picks 128, 256 or 512)
 template <int K, int KS, int W, bool UPD>
 __global__ void __launch_bounds__(TB) k_cheb2(int n, int P, int max_local, const int32_t* __restrict__ hptr,
                                               const int32_t* __restrict__ h1n, const int32_t* __restrict__ halo,
@@ -529,10 +529,13 @@ __global__ void __launch_bounds__(TB) k_cheb2(int n, int P, int max_local, const
   float4* X0 = tsm;
   float4* X1 = tsm + (size_t)max_local * LPR;
   const uint16_t* lc = lcol + (size_t)lptr[patch] * W;
-  for (int lr = sub; lr < nloc; lr += RPP) {
+  for (int lr = sub; lr < nloc; lr += RPP) {  // x0 by asynchronous 16-byte copies, all in flight
     const int g = lr < pr ? a + lr : halo[hb + lr - pr];
-    X0[lr * LPR + lane] = *reinterpret_cast<const float4*>(x0 + po + (size_t)g * K);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(X0 + lr * LPR + lane)),
+                 "l"(x0 + po + (size_t)g * K)
+                 : "memory");
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");
   __syncthreads();
   for (int lr = sub; lr < nl1; lr += RPP) {  // step 1
     const int g = lr < pr ? a + lr : halo[hb + lr - pr];
@@ -2286,15 +2289,17 @@ static void launch_sweep(const Level& L, const T* b, const T* x, T* out, SweepPr
 }
 
 // ---- the two-step Chebyshev pair ----------------------------------------------------------------
-// Tuning key: 1 = the post-smoothing pair of this level runs as k_cheb2, 0 (default) = two sweeps.
+// Tuning key: P > 0 = the post-smoothing pair of this level runs as k_cheb2 over patches of P rows
+// (128, 256 or 512), 0 (default) = two sweeps.
 static std::string cheb2_key(int K, int W, int n) {
   return "cheb2/f32/K" + std::to_string(K) + "/W" + std::to_string(W) + "/n" + std::to_string(size_bucket(n));
 }
 constexpr int kCheb2MinRows = 1 << 14;  // smaller levels stay with the sweeps (launch-bound)
 
-// The patches and halos of level L (host, from the internal slot-major operator columns).
-static void build_two_step(Level& L) {
-  const int n = L.n, W = L.W, P = kTwoStepRows;
+// The patches of P rows and their halos of level L (host, from the internal operator columns).
+static void build_two_step(Level& L, int P) {
+  require(P >= 32 && P <= kTwoStepRows, "multigrid: two-step patches of 32 to 512 rows");
+  const int n = L.n, W = L.W;
   const std::vector<int32_t> col = L.col.download();
   const int npatch = (n + P - 1) / P;
   std::vector<int32_t> hptr(npatch + 1, 0), h1n(npatch, 0), lptr(npatch + 1, 0), halo, loc(n, 0), stamp(n, -1);
@@ -2397,7 +2402,7 @@ static bool cheb2_on(const Level& L, const CT<T>* cs) {
   } else {
     if (cs || L.W != 6 || L.n < kCheb2MinRows || !L.ts.npatch) return false;
     if (cheb2_smem<K>(L) > 200 * 1024) return false;
-    return tune_get(cheb2_key(K, L.W, L.n), 0) == 1;
+    return tune_get(cheb2_key(K, L.W, L.n), 0) == L.ts.P;
   }
 }
 
@@ -2808,9 +2813,11 @@ static int64_t count_kernel_nodes(cudaGraph_t g) {
 static void ensure_two_step(dec_mg& mg, int K) {
   if (mg.opt.smoother != DEC_SMOOTH_CHEBYSHEV || mg.opt.precision != 1 || K < 16) return;
   for (Level& L : mg.lv)
-    if (L.W == 6 && L.n >= kCheb2MinRows && tune_get(cheb2_key(K, L.W, L.n), 0) == 1) {
+    if (L.W == 6 && L.n >= kCheb2MinRows) {
+      const int P = tune_get(cheb2_key(K, L.W, L.n), 0);
+      if (P <= 0) continue;
       cheb2_opt_in();
-      if (!L.ts.npatch) build_two_step(L);
+      if (!L.ts.npatch || L.ts.P != P) build_two_step(L, P);
     }
 }
 
@@ -3406,6 +3413,8 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
       prm.c1 = (CT<T>)0.5;
       prm.c2 = (CT<T>)0.25;
       launch_sweep<T, K>(L, B.b.p, B.x.p, B.y.p, prm, np, s, B.cs);
+    } else if (kernel == DEC_KERNEL_SWEEP_PAIR) {
+      launch_cheb2<T, K>(L, B.b.p, B.x.p, B.y.p, 0.5, 0.5, 0.25, np, s, nullptr);
     } else if (kernel == DEC_KERNEL_MLP) {
       if constexpr (!std::is_same<T, __half>::value)
         launch_mlp_smooth<T, K>(mlp_weights(mg.mlp), L.n, L.W, L.col.p, L.mtab.p, pick<T>(L.diag64, L.diag32),
@@ -3445,6 +3454,8 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
   if (kernel == DEC_KERNEL_SWEEP) {
     double mat = (double)L.n * (L.W * (4.0 + sz) + 2 * sz);
     *bytes = mat + prm_vectors(mg.opt.smoother) * (double)nk * sz;
+  } else if (kernel == DEC_KERNEL_SWEEP_PAIR) {
+    *bytes = (double)L.n * (L.W * (4.0 + sz) + 2 * sz) + 3.0 * (double)nk * sz;  // operator, x, b, out once
   } else if (kernel == DEC_KERNEL_MLP) {
     *bytes = (double)L.n * (L.W * (4.0 + sz) + sz) + 3.0 * (double)nk * sz;  // operator, r, x, out
   } else if (kernel == DEC_KERNEL_RESIDUAL) {
@@ -3472,7 +3483,17 @@ static void time_kernel_K(dec_mg& mg, Workspace& w, int kernel, int level, int r
 
 void mg_time_kernel(dec_mg* mg, int kernel, int level, int nrhs, int reps, void* stream, double* ms, double* bytes) {
   require(mg != nullptr && ms != nullptr && bytes != nullptr, "multigrid: null argument");
-  require(kernel >= 0 && kernel <= 4, "multigrid: unknown kernel");
+  require(kernel >= 0 && kernel <= 5, "multigrid: unknown kernel");
+  if (kernel == DEC_KERNEL_SWEEP_PAIR) {
+    Level& L = mg->lv[level];
+    const int K = choose_k(*mg, nrhs, mg->opt.precision);
+    require(mg->opt.precision == 1 && K >= 16 && L.W == 6 && L.n >= kCheb2MinRows,
+            "multigrid: the sweep pair runs on FP32 panels of 16 or more over rows of 6 slots");
+    cheb2_opt_in();
+    const int tuned = tune_get(cheb2_key(K, L.W, L.n), 0);
+    const int P = tuned > 0 ? tuned : kTwoStepRows;  // the table's patch size, else the largest
+    if (!L.ts.npatch || L.ts.P != P) build_two_step(L, P);
+  }
   require(kernel != DEC_KERNEL_MLP || mg->mlp != nullptr, "multigrid: no learned smoother network set");
   require(level >= 0 && level < (int)mg->lv.size() - (kernel == 2 || kernel == 3 ? 1 : 0),
           "multigrid: level out of range");
@@ -3610,7 +3631,7 @@ int mg_autotune(dec_mg* mg, int nrhs, int reps, void* stream) {
     };
     int best_c = 0;
     double best_ct = 1e300;
-    for (int v : {0, 1}) {
+    for (int v : {0, 512, 256, 128}) {
       set_all(v);
       w.graph[G_VCYCLE] = capture(*mg, w, G_VCYCLE);
       DEC_CUDA(cudaGraphLaunch(w.graph[G_VCYCLE], s));
