@@ -233,9 +233,14 @@ def measure_operators(dec, peak, cpu=True):
                      dec.dec_wedge_product(0, 2, g))
     d1, L = dec.dec_differential(1, g), dec.laplace_beltrami(g)
     d1a = torch.empty(g.nt, dtype=torch.float64, device="cuda")
-    grid_ops = {}
-    for name, fn in (("wedge01(f,alpha)", lambda: w01(f, al)), ("wedge11(alpha,beta)", lambda: w11(al, be)),
-                     ("wedge02(f,d1 alpha)", lambda: w02(f, d1.apply(al, d1a))), ("laplacian f", lambda: L.apply(f))):
+    o01 = torch.empty(g.ne, dtype=torch.float64, device="cuda")
+    o11 = torch.empty(g.nt, dtype=torch.float64, device="cuda")
+    o02 = torch.empty(g.nt, dtype=torch.float64, device="cuda")
+    oL = torch.empty(g.nv, dtype=torch.float64, device="cuda")
+    grid_ops, grid_graph = {}, {}
+    for name, fn in (("wedge01(f,alpha)", lambda: w01(f, al, o01)), ("wedge11(alpha,beta)", lambda: w11(al, be, o11)),
+                     ("wedge02(f,d1 alpha)", lambda: w02(f, d1.apply(al, d1a), o02)),
+                     ("laplacian f", lambda: L.apply(f, oL))):
         fn()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -246,7 +251,21 @@ def measure_operators(dec, peak, cpu=True):
         e1.record()
         torch.cuda.synchronize()
         grid_ops[name] = round(e0.elapsed_time(e1) * 10, 2)  # µs per op (ms / 100 * 1000)
+        # the same 100 repetitions captured in one CUDA graph: the device time per operation
+        gr = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(gr):
+            for _ in range(100):
+                fn()
+        gr.replay()
+        torch.cuda.synchronize()
+        e0.record()
+        gr.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        grid_graph[name] = round(e0.elapsed_time(e1) * 10, 2)
+        del gr
     out["grid_128x128_us_per_op"] = grid_ops
+    out["grid_128x128_us_per_op_graph"] = grid_graph
     if cpu:
         out["grid_128x128_cpu_us_per_op"] = cpu_operator_baseline()
     return out
@@ -401,7 +420,11 @@ def measure_batched(dec, args):
     for (name, _, _, _), mg, r, k in zip(types, mgs, reps, nrhs):
         groups[name] = {"vertices": mg.n, "solves": k, "refinement_steps": int(r.iterations),
                         "converged": bool(r.converged), "panel_width": int(r.rhs_block)}
+    peak, peak_kind = measured_peaks()
+    by_batch = batch.traffic(int(tot.iterations))
     res = {"solves": 512, "solves_per_s": 512 * steps / t, "ms_per_batch": 1e3 * t / steps,
+           "bytes_per_batch": by_batch, "GB/s": by_batch / (t / steps) / 1e9,
+           "frac": by_batch / (t / steps) / 1e9 / peak, "peak": peak_kind,
            "refinement_steps": int(tot.iterations), "converged": bool(tot.converged),
            "max_rel_residual": tot.max_rel_residual, "kernels_per_batch": int(tot.launches),
            "setup_seconds": setup_s, "groups": groups}
@@ -420,6 +443,7 @@ def measure_batched(dec, args):
     a = torch.rand((count, ne), dtype=torch.float32, device="cuda", generator=gen) * 2 - 1
     b = torch.rand((count, ne), dtype=torch.float32, device="cuda", generator=gen) * 2 - 1
     out = torch.empty((count, nt), dtype=torch.float32, device="cuda")
+    pairs = w11.autotune(count, reps=3)  # form pairs per thread, from the project autotuner
     w11.batched(a, b, out)
     torch.cuda.synchronize()
     e0.record()
@@ -430,7 +454,8 @@ def measure_batched(dec, args):
     tw = e0.elapsed_time(e1) / 1e3 / steps
     by = count * (2.0 * ne * 4 + nt * 4) + nt * (12 + 3 * 4)
     res["wedge11_L7_fp32_x1024"] = {"ms": 1e3 * tw, "wedges_per_s": count / tw, "GB/s": by / tw / 1e9,
-                                    "bytes": by}
+                                    "bytes": by, "frac": by / tw / 1e9 / peak, "peak": peak_kind,
+                                    "pairs_per_thread": pairs}
     del a, b, out
     torch.cuda.empty_cache()
     return res

@@ -190,6 +190,13 @@ class WedgePlan:
         check(lib().dec_wedge_apply_batched(self._h, _ptr(a), _ptr(b), _ptr(out), count, _stream()))
         return out
 
+    def autotune(self, count, reps=5):
+        """Time the batched FP32 ∧(1,1)'s pairs-per-thread variants on min(count, 256) pairs and record
+        the fastest in the tuning table (dec_wedge_autotune); returns the choice (0: nothing tuned)."""
+        c = C.c_int32()
+        check(lib().dec_wedge_autotune(self._h, count, reps, _stream(), C.byref(c)))
+        return c.value
+
 
 def dec_wedge_product(m, n, sd, dtype="float64"):
     """Primal-primal wedge of an m-form and an n-form (FastDEC.jl:255-289)."""
@@ -772,6 +779,13 @@ class Batch:
         if st not in (_capi.DEC_OK, 4):
             check(st)
         return list(reps), tot
+
+    def traffic(self, iterations):
+        """Algorithmic bytes of the captured batch graph run for `iterations` refinement steps
+        (dec_batch_traffic)."""
+        by = C.c_double()
+        check(lib().dec_batch_traffic(self._h, iterations, C.byref(by)))
+        return by.value
 
 
 class SmootherMLP:

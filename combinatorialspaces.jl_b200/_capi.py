@@ -70,6 +70,7 @@ SIGNATURES = {
     "dec_wedge_apply": (I32, [P, P, P, P, P]),
     "dec_wedge_lengths": (I32, [P, PI64, PI64, PI64]),
     "dec_wedge_apply_batched": (I32, [P, P, P, P, I32, P]),
+    "dec_wedge_autotune": (I32, [P, I32, I32, P, C.POINTER(C.c_int32)]),
     "dec_wedge_plan_destroy": (I32, [P]),
     "dec_op_create": (I32, [P, I32, F64, I32, PP]),
     "dec_op_create_csc": (I32, [C.POINTER(Csc), I32, PP]),
@@ -110,6 +111,7 @@ SIGNATURES = {
     "dec_batch_create": (I32, [P, I32, PP]),
     "dec_batch_destroy": (I32, [P]),
     "dec_batch_autotune": (I32, [P, P, I32, P]),
+    "dec_batch_traffic": (I32, [P, I32, C.POINTER(C.c_double)]),
     "dec_batch_solve": (I32, [P, P, P, P, P, F64, I32, P, C.POINTER(SolveReport), P]),
     "dec_mlp_create": (I32, [C.c_uint64, PP]),
     "dec_mlp_destroy": (I32, [P]),

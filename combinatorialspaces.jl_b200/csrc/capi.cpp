@@ -14,6 +14,7 @@
 // Implementations (wedge.cu, ops.cu).
 dec_wedge_plan* wedge_plan_create_impl(dec_mesh* mh, int kind, int da, int db, dec_dtype dt);
 void wedge_apply_impl(dec_wedge_plan* P, const void* a, const void* b, void* out, int count, void* stream);
+int wedge_autotune_impl(dec_wedge_plan* P, int count, int reps, void* stream);
 void wedge_plan_destroy_impl(dec_wedge_plan* P);
 void wedge_lengths_impl(const dec_wedge_plan* P, int64_t* la, int64_t* lb, int64_t* lo);
 void c_wedge_apply_impl(int j, int k, int64_t n, const int32_t* p, const void* c, dec_dtype dt, const void* a,
@@ -154,6 +155,13 @@ dec_status dec_wedge_apply(dec_wedge_plan* p, const void* a, const void* b, void
 dec_status dec_wedge_apply_batched(dec_wedge_plan* p, const void* a, const void* b, void* out, int32_t count,
                                    void* stream) {
   return guard([&] { wedge_apply_impl(p, a, b, out, count, stream); });
+}
+
+dec_status dec_wedge_autotune(dec_wedge_plan* p, int32_t count, int32_t reps, void* stream, int32_t* choice) {
+  return guard([&] {
+    const int c = wedge_autotune_impl(p, count, reps, stream);
+    if (choice) *choice = c;
+  });
 }
 
 dec_status dec_c_wedge_apply(int32_t j, int32_t k, int64_t n_out, const int32_t* p, const void* c, dec_dtype dtype,
@@ -387,6 +395,13 @@ dec_status dec_batch_destroy(dec_batch* batch) {
 
 dec_status dec_batch_autotune(dec_batch* batch, const int32_t* nrhs, int32_t reps, void* stream) {
   return guard([&] { decb::batch_autotune(batch, nrhs, reps, stream); });
+}
+
+dec_status dec_batch_traffic(const dec_batch* batch, int32_t iterations, double* bytes) {
+  return guard([&] {
+    decb::require(bytes != nullptr, "batch: null output");
+    *bytes = decb::batch_traffic(batch, iterations);
+  });
 }
 
 dec_status dec_batch_solve(dec_batch* batch, double* const* u, const double* const* rhs, const int32_t* nrhs,

@@ -3699,6 +3699,7 @@ struct dec_batch {
   std::vector<int> nrhs;
   cudaGraphExec_t graph = nullptr;             // the whole solve: panels in, loop, panels out
   int64_t launches_pre = 0, launches_body = 0; // kernel nodes outside / inside the WHILE body
+  double bytes_pre = 0.0, bytes_body = 0.0;     // algorithmic bytes outside / inside the WHILE body
   void drop_graphs() {
     if (graph) cudaGraphExecDestroy(graph);
     graph = nullptr;
@@ -3815,6 +3816,8 @@ static cudaGraphExec_t batch_capture(dec_batch& bt, double* const* u, const doub
     cudaGraphConditionalHandle h;
     DEC_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
     DEC_CUDA(cudaStreamBeginCaptureToGraph(bt.cap, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    bt.bytes_pre = bt.bytes_body = 0.0;
+    t_bytes = &bt.bytes_pre;
     per_group(bt, [&](size_t q, cudaStream_t st) {
       dec_mg& mg = *bt.groups[q];
       Workspace& w = *bt.used[q];
@@ -3822,6 +3825,8 @@ static cudaGraphExec_t batch_capture(dec_batch& bt, double* const* u, const doub
       const int n = F.n, K = w.K, np = w.npanels;
       to_panels(n, nrhs[q], K, np, F.diperm.p, rhs[q], w.B64.p, st);
       to_panels(n, nrhs[q], K, np, F.diperm.p, u[q], w.U64.p, st);
+      // b and u into panels, u out of panels at the end: caller vectors, panels, the row permutation
+      add_bytes(3.0 * ((double)n * nrhs[q] * 8.0 + (double)n * K * np * 8.0 + n * 4.0));
       zero_correction(mg, w, st);
       enqueue_bnorms(mg, w, st, bt.bn2.p + bt.off[q]);
       dispatch(mg, w, st, G_RESID);
@@ -3830,6 +3835,7 @@ static cudaGraphExec_t batch_capture(dec_batch& bt, double* const* u, const doub
     k_batch_check<<<1, 256, 0, bt.cap>>>(h, G, bt.meta.p, bt.norms.p, bt.bn2.p, bt.state.p, bt.conv_at.p,
                                          bt.worst.p, 0);
     DEC_CHECK_LAUNCH();
+    t_bytes = nullptr;
     cudaStreamCaptureStatus cst;
     cudaGraph_t cg = nullptr;
     const cudaGraphNode_t* deps = nullptr;
@@ -3852,6 +3858,7 @@ static cudaGraphExec_t batch_capture(dec_batch& bt, double* const* u, const doub
     DEC_CUDA(cudaStreamEndCapture(bt.cap, &g));
     cudaGraph_t body = prm.conditional.phGraph_out[0];
     DEC_CUDA(cudaStreamBeginCaptureToGraph(bt.cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    t_bytes = &bt.bytes_body;
     per_group(bt, [&](size_t q, cudaStream_t st) {
       dec_mg& mg = *bt.groups[q];
       Workspace& w = *bt.used[q];
@@ -3866,6 +3873,7 @@ static cudaGraphExec_t batch_capture(dec_batch& bt, double* const* u, const doub
     k_batch_check<<<1, 256, 0, bt.cap>>>(h, G, bt.meta.p, bt.norms.p, bt.bn2.p, bt.state.p, bt.conv_at.p,
                                          bt.worst.p, 1);
     DEC_CHECK_LAUNCH();
+    t_bytes = nullptr;
     DEC_CUDA(cudaStreamEndCapture(bt.cap, &body));
     bt.launches_pre = count_kernel_nodes(g);
     bt.launches_body = count_kernel_nodes(body);
@@ -3874,9 +3882,16 @@ static cudaGraphExec_t batch_capture(dec_batch& bt, double* const* u, const doub
     cudaGraphDestroy(g);
     return ex;
   } catch (...) {
+    t_bytes = nullptr;
     fail();
     throw;
   }
+}
+
+double batch_traffic(const dec_batch* b, int iterations) {
+  require(b != nullptr && iterations >= 0, "batch: bad traffic arguments");
+  require(b->graph != nullptr, "batch: no captured solve (call dec_batch_solve first)");
+  return b->bytes_pre + iterations * b->bytes_body;
 }
 
 void batch_autotune(dec_batch* b, const int* nrhs, int reps, void* stream) {

@@ -29,6 +29,7 @@ void mg_set_smoother_mlp(dec_mg* mg, const dec_mlp* mlp);
 dec_batch* batch_create(dec_mg* const* groups, int ngroups);
 void batch_destroy(dec_batch* b);
 void batch_autotune(dec_batch* b, const int* nrhs, int reps, void* stream);
+double batch_traffic(const dec_batch* b, int iterations);
 dec_status batch_solve(dec_batch* b, double* const* u, const double* const* rhs, const int* nrhs,
                        const double* const* shifts, double rtol, int max_iters, dec_solve_report* reps,
                        dec_solve_report* total, void* stream);

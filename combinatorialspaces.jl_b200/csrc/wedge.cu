@@ -16,6 +16,7 @@
 #include <algorithm>
 
 #include "mesh.cuh"
+#include "tune.cuh"
 
 namespace decb {
 
@@ -296,6 +297,66 @@ __global__ void __launch_bounds__(kThreads) k_w11v(int nt, const int32_t* __rest
     const float be0 = __ldg(b + te0[t]), be1 = __ldg(b + te1[t]), be2 = __ldg(b + te2[t]);
     out[t] = (cf0[t] * (ae2 * be1 - ae1 * be2) + cf1[t] * (ae2 * be0 - ae0 * be2) + cf2[t] * (ae1 * be0 - ae0 * be1));
   }
+}
+
+// Batched FP32 ∧11, P form pairs per thread: the four triangles' edge indices and coefficients are
+// loaded once (cached, so the next chunk of pairs finds them in L2) and serve pairs p0 .. p0 + P - 1,
+// p0 = P blockIdx.y.  Each output keeps the single-pair expression, so every pair equals its single
+// application bit for bit.  Needs the streamed pointers of every pair 16-byte aligned, like k_w11v.
+template <int P>
+__global__ void __launch_bounds__(kThreads) k_w11v_pairs(int nt, int count, const int32_t* __restrict__ te0,
+                                                         const int32_t* __restrict__ te1,
+                                                         const int32_t* __restrict__ te2,
+                                                         const float* __restrict__ cf0, const float* __restrict__ cf1,
+                                                         const float* __restrict__ cf2, const float* __restrict__ a,
+                                                         const float* __restrict__ b, float* __restrict__ out,
+                                                         size_t sa, size_t sb, size_t so) {
+  const int p0 = (int)blockIdx.y * P;
+  const int np = min(P, count - p0);
+  a += (size_t)p0 * sa;
+  b += (size_t)p0 * sb;
+  out += (size_t)p0 * so;
+  const int n4 = nt / 4;
+  for (int g = blockIdx.x * kThreads + threadIdx.x; g < n4; g += gridDim.x * kThreads) {
+    int e0[4], e1[4], e2[4];
+    float c0[4], c1[4], c2[4];
+    i4(__ldg(reinterpret_cast<const int4*>(te0) + g), e0);
+    i4(__ldg(reinterpret_cast<const int4*>(te1) + g), e1);
+    i4(__ldg(reinterpret_cast<const int4*>(te2) + g), e2);
+    f4(__ldg(reinterpret_cast<const float4*>(cf0) + g), c0);
+    f4(__ldg(reinterpret_cast<const float4*>(cf1) + g), c1);
+    f4(__ldg(reinterpret_cast<const float4*>(cf2) + g), c2);
+#pragma unroll 1
+    for (int p = 0; p < np; ++p) {
+      const float* ap = a + (size_t)p * sa;
+      const float* bp = b + (size_t)p * sb;
+      float ae[3][4], be[3][4], o[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        ae[0][k] = __ldg(ap + e0[k]);
+        ae[1][k] = __ldg(ap + e1[k]);
+        ae[2][k] = __ldg(ap + e2[k]);
+        be[0][k] = __ldg(bp + e0[k]);
+        be[1][k] = __ldg(bp + e1[k]);
+        be[2][k] = __ldg(bp + e2[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        o[k] = (c0[k] * (ae[2][k] * be[1][k] - ae[1][k] * be[2][k]) +
+                c1[k] * (ae[2][k] * be[0][k] - ae[0][k] * be[2][k]) +
+                c2[k] * (ae[1][k] * be[0][k] - ae[0][k] * be[1][k]));
+      __stcs(reinterpret_cast<float4*>(out + (size_t)p * so) + g, make_float4(o[0], o[1], o[2], o[3]));
+    }
+  }
+  for (int t = 4 * n4 + blockIdx.x * kThreads + threadIdx.x; t < nt; t += gridDim.x * kThreads)
+    for (int p = 0; p < np; ++p) {
+      const float* ap = a + (size_t)p * sa;
+      const float* bp = b + (size_t)p * sb;
+      const float ae0 = __ldg(ap + te0[t]), ae1 = __ldg(ap + te1[t]), ae2 = __ldg(ap + te2[t]);
+      const float be0 = __ldg(bp + te0[t]), be1 = __ldg(bp + te1[t]), be2 = __ldg(bp + te2[t]);
+      out[(size_t)p * so + t] =
+          (cf0[t] * (ae2 * be1 - ae1 * be2) + cf1[t] * (ae2 * be0 - ae0 * be2) + cf2[t] * (ae1 * be0 - ae0 * be1));
+    }
 }
 
 // (M x) .* y with M a row-major ELL matrix (columns sorted, -1 = padding): the
@@ -674,10 +735,31 @@ static void build_plan(dec_wedge_plan& P) {
   DEC_CUDA(cudaDeviceSynchronize());
 }
 
-// `count` form pairs (a, b, out consecutive with the plan's lengths), one launch per kind.
+// The batched FP32 ∧11's pairs per thread (k_w11v_pairs), per triangle-count bucket.
+static std::string w11_pairs_key(int nt) { return "w11pairs/f32/n" + std::to_string(size_bucket(nt)); }
+constexpr int kW11PairsDefault = 4;
+
+static void launch_w11v_pairs(int pairs, const Mesh& m, const CoefSet<float>& c, const float* a, const float* b,
+                              float* o, size_t sa, size_t sb, size_t so, int cnt, cudaStream_t s) {
+  auto go = [&](auto kernel, int per) {
+    const dim3 grid(grid_for(m.nt / 4 + 1, kThreads), (unsigned)((cnt + per - 1) / per));
+    kernel<<<grid, kThreads, 0, s>>>(m.nt, cnt, m.te0.p, m.te1.p, m.te2.p, c.c[0].p, c.c[1].p, c.c[2].p, a, b, o, sa,
+                                     sb, so);
+  };
+  switch (pairs) {
+    case 2: go(k_w11v_pairs<2>, 2); break;
+    case 4: go(k_w11v_pairs<4>, 4); break;
+    case 8: go(k_w11v_pairs<8>, 8); break;
+    case 16: go(k_w11v_pairs<16>, 16); break;
+    default: go(k_w11v_pairs<1>, 1); break;
+  }
+}
+
+// `count` form pairs (a, b, out consecutive with the plan's lengths), one launch per kind.  pairs:
+// the batched FP32 ∧11's pairs per thread (0 = the tuning table's choice).
 template <class T>
 static void launch_plan(dec_wedge_plan& P, const CoefSet<T>& c, const void* va, const void* vb, void* vo, int count,
-                        cudaStream_t s) {
+                        cudaStream_t s, int pairs = 0) {
   Mesh& m = *P.m;
   const T* a = (const T*)va;
   const T* b = (const T*)vb;
@@ -744,6 +826,11 @@ static void launch_plan(dec_wedge_plan& P, const CoefSet<T>& c, const void* va, 
       case W11:
         if (!m.nt) break;
         if constexpr (sizeof(T) == 4) {
+          if (vec && cnt > 1) {
+            const int per = pairs > 0 ? pairs : tune_get(w11_pairs_key(m.nt), kW11PairsDefault);
+            launch_w11v_pairs(per, m, c, ab, bb, ob, sa, sb, so, cnt, s);
+            break;
+          }
           if (vec) {
             k_w11v<<<grid2(m.nt / 4 + 1, kThreads, cnt), kThreads, 0, s>>>(m.nt, m.te0.p, m.te1.p, m.te2.p, c.c[0].p,
                                                                              c.c[1].p, c.c[2].p, ab, bb, ob, sa, sb, so);
@@ -934,6 +1021,42 @@ void wedge_apply_impl(dec_wedge_plan* P, const void* a, const void* b, void* out
   cudaStream_t s = as_stream(stream);
   if (P->dtype == DEC_F64) launch_plan<double>(*P, P->c64, a, b, out, count, s);
   else launch_plan<float>(*P, P->c32, a, b, out, count, s);
+}
+
+// Times the batched FP32 ∧11 with 1, 2, 4, 8 and 16 pairs per thread on min(count, 256) pairs of
+// zero forms (reps launches each after one untimed) and stores the fastest under the plan's size
+// bucket.
+int wedge_autotune_impl(dec_wedge_plan* P, int count, int reps, void* stream) {
+  require(P != nullptr && count >= 1 && reps >= 1, "wedge autotune: bad arguments");
+  if (P->op != W11 || P->dtype != DEC_F32 || count < 2 || P->m->nt == 0) return 0;
+  count = std::min(count, 256);
+  cudaStream_t s = as_stream(stream);
+  DArr<float> a((size_t)count * P->len_a), b((size_t)count * P->len_b), o((size_t)count * P->len_out);
+  DEC_CUDA(cudaMemsetAsync(a.p, 0, a.bytes(), s));
+  DEC_CUDA(cudaMemsetAsync(b.p, 0, b.bytes(), s));
+  cudaEvent_t e0, e1;
+  DEC_CUDA(cudaEventCreate(&e0));
+  DEC_CUDA(cudaEventCreate(&e1));
+  int best = 1;
+  float best_ms = 1e30f;
+  for (int pairs : {1, 2, 4, 8, 16}) {
+    launch_plan<float>(*P, P->c32, a.p, b.p, o.p, count, s, pairs);
+    DEC_CUDA(cudaEventRecord(e0, s));
+    for (int r = 0; r < reps; ++r) launch_plan<float>(*P, P->c32, a.p, b.p, o.p, count, s, pairs);
+    DEC_CUDA(cudaEventRecord(e1, s));
+    DEC_CHECK_LAUNCH();
+    DEC_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = pairs;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  tune_set(w11_pairs_key(P->m->nt), best);
+  return best;
 }
 
 void wedge_plan_destroy_impl(dec_wedge_plan* P) { delete P; }

@@ -105,6 +105,11 @@ dec_status dec_wedge_lengths(const dec_wedge_plan* p, int64_t* len_a, int64_t* l
 /* Batched launch: out_i = a_i ∧ b_i for `count` form pairs laid out back to back. */
 dec_status dec_wedge_apply_batched(dec_wedge_plan* p, const void* a, const void* b, void* out,
                                    int32_t count, void* stream);
+/* Autotuner (no reference counterpart): times the batched FP32 ∧(1,1) with 1, 2, 4, 8 and 16 form
+ * pairs per thread on min(count, 256) pairs and stores the fastest in the tuning table under the
+ * plan's triangle-count bucket (dec_tune_save keeps it); *choice = the pairs per thread, or 0 when
+ * the plan is not an FP32 ∧(1,1) or count < 2 (nothing tuned).  Untuned batches use 4. */
+dec_status dec_wedge_autotune(dec_wedge_plan* p, int32_t count, int32_t reps, void* stream, int32_t* choice);
 dec_status dec_wedge_plan_destroy(dec_wedge_plan* p);
 /* dec_c_wedge_product!(Val(j), Val(k), res, α, β, p, c) (FastDEC.jl:217-232): a wedge kernel on
  * caller caches in the reference's layout (cache_wedge output, Julia column-major), for
@@ -336,6 +341,10 @@ dec_status dec_batch_autotune(dec_batch* batch, const int32_t* nrhs, int32_t rep
 dec_status dec_batch_solve(dec_batch* batch, double* const* u, const double* const* rhs, const int32_t* nrhs,
                            const double* const* shifts, double rtol, int32_t max_iters,
                            dec_solve_report* reports, dec_solve_report* total, void* stream);
+/* Algorithmic bytes of the captured batch graph run for `iterations` refinement steps (total.iterations
+ * of the last dec_batch_solve): every kernel's compulsory reads and writes, the caller vectors
+ * into and out of the panels included; errors if no solve has been captured. */
+dec_status dec_batch_traffic(const dec_batch* batch, int32_t iterations, double* bytes);
 
 /* Learned smoother for DEC_SMOOTH_LEARNED: the hierarchy reads the network's weights at every
  * cycle (the network must outlive its use; retraining takes effect at the next cycle).  NULL

@@ -100,3 +100,25 @@ def test_two_step_chebyshev_pair_same_bits(dec):
     mg.autotune(32, reps=2)
     assert all(dec.tune_get(k) in (0, 128, 256, 512) for k in _cheb2_keys(7))
     dec.tune_clear()
+
+
+def test_batched_wedge11_pairs_variants_same_bits(dec):
+    """The batched FP32 ∧(1,1) with 1, 2, 4, 8 and 16 form pairs per thread (a count that no variant
+    divides) equals the single applications bit for bit; dec_wedge_autotune records one of them."""
+    m = dec.meshes.icosphere(4)
+    g = dec.Mesh(m.points, m.ev0, m.ev1, m.te0, m.te1, m.te2, m.edge_orientation, m.tri_orientation,
+                 center="circumcenter")
+    w = dec.dec_wedge_product(1, 1, g, "float32")
+    count = 37
+    a = torch.tensor(np.stack([uniform(700 + j, w.len_a) for j in range(count)]), dtype=torch.float32, device="cuda")
+    b = torch.tensor(np.stack([uniform(800 + j, w.len_b) for j in range(count)]), dtype=torch.float32, device="cuda")
+    single = np.stack([w(a[j], b[j]).cpu().numpy() for j in range(count)])
+    key = f"w11pairs/f32/n{int(np.log2(g.nt))}"
+    for pairs in (1, 2, 4, 8, 16):
+        dec.tune_set(key, pairs)
+        out = torch.full((count, w.len_out), float("nan"), dtype=torch.float32, device="cuda")
+        w.batched(a, b, out)
+        np.testing.assert_array_equal(out.cpu().numpy(), single)
+    choice = w.autotune(count, reps=2)
+    assert choice in (1, 2, 4, 8, 16) and dec.tune_get(key) == choice
+    assert dec.dec_wedge_product(0, 1, g, "float32").autotune(count) == 0

@@ -110,6 +110,10 @@ def test_batch_over_uneven_meshes(O, dec):
         Us = [torch.zeros((nrhs[q], pairs[q][1].n), dtype=torch.float64, device="cuda") for q in range(3)]
         reps, tot = batch.solve(Us, [torch.tensor(B, device="cuda") for B in Bs], shifts=shifts, rtol=1e-9)
         assert tot.converged == 1 and tot.launches > 0
+        # algorithmic bytes: at least every caller vector in and out, and linear in the steps
+        by0, by1, byk = batch.traffic(0), batch.traffic(1), batch.traffic(tot.iterations)
+        assert by0 > 3 * 8 * sum(nrhs[q] * pairs[q][1].n for q in range(3)) and by1 > by0
+        assert byk == pytest.approx(by0 + tot.iterations * (by1 - by0), rel=1e-12)
         for q, (md, mg) in enumerate(pairs):
             assert reps[q].converged == 1 and reps[q].iterations <= tot.iterations
             _check_solutions(csc(md.op(0)), Bs[q], Us[q].cpu().numpy(), shifts[q], 1e-9)
