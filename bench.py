@@ -978,7 +978,20 @@ def run_op(args):
               "wedge11": (dec.dec_wedge_product(1, 1, g, args.dtype), a, b),
               "wedge02": (dec.dec_wedge_product(0, 2, g, args.dtype), f, t)}
     variant = None
-    if args.op in ops:
+    if args.op == "wedge11_batched":
+        # `count` FP32 pairs in one batched launch, pairs per thread from --variant or the autotuner
+        w = dec.dec_wedge_product(1, 1, g, "float32")
+        A = torch.rand((args.count, g.ne), dtype=torch.float32, device="cuda")
+        B = torch.rand((args.count, g.ne), dtype=torch.float32, device="cuda")
+        y = torch.empty((args.count, g.nt), dtype=torch.float32, device="cuda")
+        key = f"w11pairs/f32/n{int(np.log2(g.nt))}"
+        if args.variant:
+            dec.tune_set(key, args.variant)
+        else:
+            w.autotune(args.count, reps=3)
+        variant = {key: dec.tune_get(key)}
+        fn = lambda: w.batched(A, B, y)
+    elif args.op in ops:
         op, x = ops[args.op]
         y = torch.empty(op.shape[0], dtype=tdt, device="cuda")
         if args.op == "laplacian":
@@ -1003,9 +1016,13 @@ def run_op(args):
         fn()
     e1.record()
     torch.cuda.synchronize()
-    print(json.dumps({"op": args.op, "dtype": args.dtype, "mesh_level": args.mesh_level, "nv": g.nv, "ne": g.ne,
-                      "nt": g.nt, "us_per_launch": 1e3 * e0.elapsed_time(e1) / args.steps, "variant": variant}),
-          flush=True)
+    us = 1e3 * e0.elapsed_time(e1) / args.steps
+    rec = {"op": args.op, "dtype": args.dtype, "mesh_level": args.mesh_level, "nv": g.nv, "ne": g.ne, "nt": g.nt,
+           "us_per_launch": us, "variant": variant}
+    if args.op == "wedge11_batched":
+        by = args.count * (2.0 * g.ne * 4 + g.nt * 4) + g.nt * (12 + 3 * 4)
+        rec.update({"count": args.count, "bytes": by, "GB/s": by / us / 1e3})
+    print(json.dumps(rec), flush=True)
 
 
 def run_kernel(args):
@@ -1063,9 +1080,11 @@ def main():
     ap.add_argument("--mesh-level", type=int, default=LEVEL, dest="mesh_level")
     ap.add_argument("--precision", type=int, default=1, choices=[1, 2],
                     help="V-cycle storage for --kernel: 1 FP32, 2 FP16 (FP32 arithmetic)")
-    ap.add_argument("--op", choices=["laplacian", "d0", "d1", "star1_geometric", "wedge01", "wedge11", "wedge02"],
+    ap.add_argument("--op", choices=["laplacian", "d0", "d1", "star1_geometric", "wedge01", "wedge11", "wedge02",
+                                     "wedge11_batched"],
                     help="time one DEC operator kernel alone (steps launches after warmup) and exit")
     ap.add_argument("--dtype", default="float64", choices=["float64", "float32"])
+    ap.add_argument("--count", type=int, default=64, help="--op wedge11_batched: form pairs per launch")
     ap.add_argument("--autotune", action="store_true", help="--op laplacian: autotune the apply's variant first")
     ap.add_argument("--variant", type=int, default=0,
                     help="--op laplacian: rows per thread (1, 2, 4); --kernel pair: patch rows (128, 256, 512)")
