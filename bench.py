@@ -1017,7 +1017,8 @@ def run_op(args):
     e1.record()
     torch.cuda.synchronize()
     us = 1e3 * e0.elapsed_time(e1) / args.steps
-    rec = {"op": args.op, "dtype": args.dtype, "mesh_level": args.mesh_level, "nv": g.nv, "ne": g.ne, "nt": g.nt,
+    rec = {"op": args.op, "dtype": "float32" if args.op == "wedge11_batched" else args.dtype,
+           "mesh_level": args.mesh_level, "nv": g.nv, "ne": g.ne, "nt": g.nt,
            "us_per_launch": us, "variant": variant}
     if args.op == "wedge11_batched":
         by = args.count * (2.0 * g.ne * 4 + g.nt * 4) + g.nt * (12 + 3 * 4)
