@@ -1031,7 +1031,8 @@ def run_kernel(args):
     right-hand sides: the entry point for ncu captures of a single kernel."""
     import torch
     dec = load_package()
-    kinds = {"sweep": 0, "residual": 1, "restrict": 2, "prolong": 3, "mlp": 4, "pair": 5}
+    kinds = {"sweep": 0, "residual": 1, "restrict": 2, "prolong": 3, "mlp": 4, "pair": 5, "sweep_p0": 6,
+             "sweep_p1": 7}
     kind = kinds[args.kernel]
     mg = dec.MultigridData(dec.meshes.icosahedron(), args.mesh_level, shift=SHIFT, center="circumcenter",
                            project_radius=1.0, smoother=3 if kind == 4 else 1, pre=max(1, args.pre),
@@ -1076,7 +1077,8 @@ def main():
     ap.add_argument("--no-ops", action="store_true", help="skip the operator-kernel roofline section")
     ap.add_argument("--profile", action="store_true",
                     help="run only the timed mixed-precision solves (inside an NVTX range 'timed')")
-    ap.add_argument("--kernel", choices=["sweep", "residual", "restrict", "prolong", "mlp", "pair"],
+    ap.add_argument("--kernel", choices=["sweep", "residual", "restrict", "prolong", "mlp", "pair", "sweep_p0",
+                                         "sweep_p1"],
                     help="time one V-cycle kernel alone (steps launches after warmup) and exit")
     ap.add_argument("--mesh-level", type=int, default=LEVEL, dest="mesh_level")
     ap.add_argument("--precision", type=int, default=1, choices=[1, 2],

@@ -17,7 +17,8 @@ DEC_WEDGE_PP, DEC_WEDGE_PD, DEC_WEDGE_DP, DEC_WEDGE_DD = 0, 1, 2, 3
  DEC_OP_FLAT_SHARP, DEC_OP_GENERAL) = range(18)
 DEC_GEOM_LENGTH, DEC_GEOM_AREA, DEC_GEOM_DUAL_AREA, DEC_GEOM_DUAL_LENGTH_TE, DEC_GEOM_DUAL_POINT = range(5)
 DEC_SMOOTH_JACOBI, DEC_SMOOTH_CHEBYSHEV, DEC_SMOOTH_CG, DEC_SMOOTH_LEARNED = 0, 1, 2, 3
-DEC_KERNEL_SWEEP, DEC_KERNEL_RESIDUAL, DEC_KERNEL_RESTRICT, DEC_KERNEL_PROLONG, DEC_KERNEL_MLP, DEC_KERNEL_SWEEP_PAIR = range(6)
+(DEC_KERNEL_SWEEP, DEC_KERNEL_RESIDUAL, DEC_KERNEL_RESTRICT, DEC_KERNEL_PROLONG, DEC_KERNEL_MLP, DEC_KERNEL_SWEEP_PAIR,
+ DEC_KERNEL_SWEEP_PROLONGED0, DEC_KERNEL_SWEEP_PROLONGED1) = range(8)
 DEC_MLP_NPARAM = 5313
 
 

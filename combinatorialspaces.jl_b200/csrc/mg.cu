@@ -198,6 +198,16 @@ struct SweepPrm {
   T c1, c2;     // Chebyshev recurrence
 };
 
+// The coarse correction a fused sweep prolongs: fine row j's parents pa[j], pb[j] (equal for a kept
+// vertex) and the coarse panels z.
+template <class T>
+struct ProlongSrc {
+  const int32_t* pa;
+  const int32_t* pb;
+  const T* z;
+  size_t cstride;
+};
+
 constexpr int TB = 256;
 
 // State of the refinement loop that runs on the device (graph with a conditional WHILE node).
@@ -346,6 +356,12 @@ __device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, 
 __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+// ½ za + ½ zb, one rounding (both halvings are exact): the prolongation's per-row term, shared by
+// k_prolong and the sweeps that prolong on the fly so both give the same bits.
+template <class C>
+__device__ __forceinline__ C prolong_term(C za, C zb) {
+  return fma_rn(C(0.5), zb, mul_rn(C(0.5), za));
+}
 
 // VV > 0 overrides the vector width (a tuned variant: VV = 2 on FP32 panels of K >= 8 puts twice the
 // lanes on a row).
@@ -370,13 +386,16 @@ struct Lanes {
 // SH: right-hand side j of panel p has its own operator A + cs[p*K + j] I (D likewise).
 // UPD: the sweep's result is the refinement step's correction e, added straight to the FP64
 // iterate (u += (double) e, the update pass's arithmetic) instead of being stored in out.
-template <class T, int K, int W, bool SH, bool UPD = false, int VV = 0>
+// PV (k_sweep_p, a Chebyshev step after the first): the previous iterate is formed from the coarse
+// correction z as the prolongation would have stored it (prolong_term, same bits): 1: P z (the level's
+// iterate was zero), 2: out + P z (out still holds the iterate before the correction).
+template <class T, int K, int W, bool SH, bool UPD = false, int VV = 0, int PV = 0>
 __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restrict__ col,
                                            const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
                                            const CT<T>* __restrict__ dinv, const T* __restrict__ b,
                                            const T* __restrict__ x, T* __restrict__ out, const SweepPrm<CT<T>>& prm,
                                            size_t pstride, const CT<T>* __restrict__ shf,
-                                           double* __restrict__ u64 = nullptr) {
+                                           double* __restrict__ u64 = nullptr, ProlongSrc<T> pz = {}) {
   using Ln = Lanes<T, K, VV>;
   using C = CT<T>;
   pdl_enter();
@@ -459,7 +478,15 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
         for (int q = 0; q < V; ++q) dn[q] = xi[q];
       } else {
         C xp[V];
-        ldv<T, V>(out + ik, xp);
+        if constexpr (PV != 1) ldv<T, V>(out + ik, xp);
+        if constexpr (PV != 0) {  // + ½ z[pa_i] + ½ z[pb_i], k_prolong's arithmetic
+          const T* zc = pz.z + (size_t)blockIdx.y * pz.cstride + (size_t)lane * V;
+          C za[V], zb[V];
+          ldv<T, V>(zc + (size_t)__ldg(pz.pa + i) * K, za);
+          ldv<T, V>(zc + (size_t)__ldg(pz.pb + i) * K, zb);
+#pragma unroll
+          for (int q = 0; q < V; ++q) xp[q] = add_rn(PV == 2 ? xp[q] : C(0), prolong_term(za[q], zb[q]));
+        }
 #pragma unroll
         for (int q = 0; q < V; ++q) dn[q] = sub_rn(xi[q], xp[q]);
       }
@@ -497,6 +524,115 @@ __global__ void __launch_bounds__(TB) k_sweep_u(int n, int Wr, const int32_t* __
                                                 SweepPrm<CT<T>> prm, size_t pstride, const CT<T>* __restrict__ shf,
                                                 double* __restrict__ u64) {
   sweep_rows<T, K, W, SH, true, VV>(n, Wr, col, off, diag, dinv, b, x, out, prm, pstride, shf, u64);
+}
+
+// The second Chebyshev step after x (+)= P z with its previous iterate formed from z (PV = 1: P z,
+// 2: out + P z), so the prolonged iterate is never read back.  UPD as k_sweep_u.
+template <class T, int K, int W, bool SH, bool UPD, int PV, int VV = 0>
+__global__ void __launch_bounds__(TB) k_sweep_p(int n, int Wr, const int32_t* __restrict__ col,
+                                                const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
+                                                const CT<T>* __restrict__ dinv, const T* __restrict__ b,
+                                                const T* __restrict__ x, T* __restrict__ out,
+                                                SweepPrm<CT<T>> prm, size_t pstride, const CT<T>* __restrict__ shf,
+                                                double* __restrict__ u64, ProlongSrc<T> pz) {
+  sweep_rows<T, K, W, SH, UPD, VV, PV>(n, Wr, col, off, diag, dinv, b, x, out, prm, pstride, shf, u64, pz);
+}
+
+// Width of a level's A P rows (fine row -> coarse columns; at most 7 on binary-subdivision levels of
+// rows with 6 off-diagonal slots: a kept vertex's own coarse copy and its neighbours', a midpoint's
+// four coarse vertices), padded with weight 0.
+constexpr int kApW = 8;
+
+// The first Chebyshev step after the prolongation, from x0 = P z (ADD: x0 = e + P z, e the iterate
+// before the correction), without x0 stored: r = b - A x0 with A x0 = (A P) z (+ A e), the product
+// A P precomputed per level (apc / apv, kApW slots per row); out = x0 + D⁻¹ r / θ.  SH: A + cs I per
+// right-hand side (A P then holds the unshifted product and cs x0 is added).
+template <class T, int K, bool SH, bool ADD, int VV = 0>
+__global__ void __launch_bounds__(TB) k_sweep_ap(int n, const int32_t* __restrict__ col, const CT<T>* __restrict__ off,
+                                                 const CT<T>* __restrict__ diag, const CT<T>* __restrict__ dinv,
+                                                 const int32_t* __restrict__ apc, const CT<T>* __restrict__ apv,
+                                                 const T* __restrict__ b, const T* __restrict__ e,
+                                                 T* __restrict__ out, CT<T> inv_theta, size_t pstride,
+                                                 const CT<T>* __restrict__ shf, ProlongSrc<T> pz) {
+  using Ln = Lanes<T, K, VV>;
+  using C = CT<T>;
+  pdl_enter();
+  constexpr int V = Ln::V;
+  const int lane = threadIdx.x % Ln::LPR;
+  const size_t po = (size_t)blockIdx.y * pstride + (size_t)lane * V;
+  const T* zc = pz.z + (size_t)blockIdx.y * pz.cstride + (size_t)lane * V;
+  C csv[V];
+  if constexpr (SH) ldv<C, V>(shf + (size_t)blockIdx.y * K + (size_t)lane * V, csv);
+  for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < n; i += gridDim.x * Ln::RPB) {
+    const size_t ik = po + (size_t)i * K;
+    int pc[kApW];
+    C pw[kApW];
+#pragma unroll
+    for (int k = 0; k < kApW; ++k) {
+      pc[k] = apc[(size_t)i * kApW + k];
+      pw[k] = apv[(size_t)i * kApW + k];
+    }
+    C r[V], pzi[V], x0[V], acc[V];
+    ldv<T, V>(b + ik, r);
+    // the row's own parents are A P's first slots (slot 1 only when they differ), so P z at this row
+    // comes from the same gathers
+    const bool kept = pz.pa[i] == pz.pb[i];
+    C zk[kApW][V];
+#pragma unroll
+    for (int k = 0; k < kApW; ++k) ldv<T, V>(zc + (size_t)pc[k] * K, zk[k]);
+#pragma unroll
+    for (int q = 0; q < V; ++q) {
+      pzi[q] = prolong_term(zk[0][q], kept ? zk[0][q] : zk[1][q]);  // P z at this row
+      x0[q] = add_rn(C(0), pzi[q]);                                // k_prolong's assignment (from +0)
+    }
+    if constexpr (ADD) {  // A e, as the sweep forms it
+      C ei[V];
+      ldv<T, V>(e + ik, ei);
+      const C dg = diag[i];
+#pragma unroll
+      for (int q = 0; q < V; ++q) {
+        if constexpr (SH) acc[q] = mul_rn(add_rn(dg, csv[q]), ei[q]);
+        else acc[q] = mul_rn(dg, ei[q]);
+      }
+      int cs[6];
+      C vs[6];
+#pragma unroll
+      for (int s = 0; s < 6; ++s) {
+        cs[s] = col[(size_t)i * 6 + s];
+        vs[s] = off[(size_t)i * 6 + s];
+      }
+#pragma unroll
+      for (int s = 0; s < 6; ++s) {
+        C nb[V];
+        ldv<T, V>(e + po + (size_t)cs[s] * K, nb);
+#pragma unroll
+        for (int q = 0; q < V; ++q) acc[q] = fma_rn(vs[s], nb[q], acc[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < V; ++q) x0[q] = add_rn(ei[q], pzi[q]);
+    } else {
+#pragma unroll
+      for (int q = 0; q < V; ++q) acc[q] = C(0);
+    }
+#pragma unroll
+    for (int k = 0; k < kApW; ++k)  // + (A P) z
+#pragma unroll
+      for (int q = 0; q < V; ++q) acc[q] = fma_rn(pw[k], zk[k][q], acc[q]);
+    if constexpr (SH) {  // + cs (P z) at this row (A e already carries its cs e)
+#pragma unroll
+      for (int q = 0; q < V; ++q) acc[q] = fma_rn(csv[q], pzi[q], acc[q]);
+    }
+    C o[V];
+#pragma unroll
+    for (int q = 0; q < V; ++q) {
+      C di;
+      if constexpr (SH) di = C(1) / (diag[i] + csv[q]);
+      else di = dinv[i];
+      const C rr = sub_rn(r[q], acc[q]);
+      o[q] = add_rn(x0[q], mul_rn(mul_rn(di, rr), inv_theta));
+    }
+    stv<T, V>(out + ik, o);
+  }
 }
 
 // Two Chebyshev steps in one pass (post-smoothing from a given iterate x0, FP32 panels): step 1
@@ -714,7 +850,7 @@ __global__ void __launch_bounds__(TB) k_prolong(int nf, const int32_t* __restric
       ldv<T, V>(xf + (size_t)j * K, xv);
     }
 #pragma unroll
-    for (int q = 0; q < V; ++q) xv[q] += C(0.5) * za[q] + C(0.5) * zb[q];
+    for (int q = 0; q < V; ++q) xv[q] = add_rn(xv[q], prolong_term(za[q], zb[q]));
     stv<T, V>(xf + (size_t)j * K, xv);
   }
 }
@@ -1421,6 +1557,12 @@ struct Level {
   int nc = 0, Wq = 0;
   DArr<int32_t> rself, ridx, pa, pb;
   DArr<double> rs;
+  // A P (kApW coarse columns per fine row) for the first sweep after a prolongation (k_sweep_ap);
+  // built for binary-subdivision levels with rows of 6 off-diagonal slots
+  bool ap_ok = false;
+  DArr<int32_t> apc;
+  DArr<double> apv64;
+  DArr<float> apv32;
   // a hierarchy from caller matrices: general R (nc x n) and P (n x nc) as row-major ELL
   bool gen = false;
   int Wr = 0, Wp = 0;
@@ -1909,6 +2051,67 @@ static void build_transfers(Level& F, const Level& C) {
   DEC_CHECK_LAUNCH();
 }
 
+// Row i of A P (A the level operator, P the prolongation from the next coarser level): the parents
+// of the row itself (½ a_ii each) and of its six neighbours (½ a_ij each), equal coarse columns
+// merged in order of first appearance (FP64 sums); kApW slots, padded with the row's first parent at
+// weight 0.  *bad = 1 if a row has more than kApW distinct coarse columns.
+__global__ void k_ap_build(int n, const int32_t* __restrict__ col, const double* __restrict__ off,
+                           const double* __restrict__ diag, const int32_t* __restrict__ pa,
+                           const int32_t* __restrict__ pb, int32_t* __restrict__ apc, double* __restrict__ apv,
+                           int* __restrict__ bad) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int c[14];
+    double w[14];
+    int m = 0;
+    auto put = [&](int p, double v) {
+      for (int k = 0; k < m; ++k)
+        if (c[k] == p) {
+          w[k] += v;
+          return;
+        }
+      c[m] = p;
+      w[m] = v;
+      ++m;
+    };
+    const double h = 0.5 * diag[i];
+    put(pa[i], h);
+    put(pb[i], h);
+    for (int s = 0; s < 6; ++s) {
+      const int j = col[(size_t)i * 6 + s];
+      const double hj = 0.5 * off[(size_t)i * 6 + s];
+      put(pa[j], hj);
+      put(pb[j], hj);
+    }
+    if (m > kApW) {
+      atomicExch(bad, 1);
+      m = kApW;
+    }
+    for (int k = 0; k < kApW; ++k) {
+      apc[(size_t)i * kApW + k] = k < m ? c[k] : pa[i];
+      apv[(size_t)i * kApW + k] = k < m ? w[k] : 0.0;
+    }
+  }
+}
+
+static void build_ap(Level& L) {
+  L.ap_ok = false;
+  if (L.W != 6 || L.gen || !L.pa.p) return;
+  L.apc.alloc((size_t)L.n * kApW);
+  L.apv64.alloc((size_t)L.n * kApW);
+  DArr<int> bad(1);
+  DEC_CUDA(cudaMemset(bad.p, 0, sizeof(int)));
+  k_ap_build<<<grid_for(L.n, 256), 256>>>(L.n, L.col.p, L.off64.p, L.diag64.p, L.pa.p, L.pb.p, L.apc.p, L.apv64.p,
+                                          bad.p);
+  DEC_CHECK_LAUNCH();
+  if (bad.download()[0]) {  // wider rows than the slots: this level keeps the stored prolongation
+    L.apc.release();
+    L.apv64.release();
+    return;
+  }
+  cast_array(L.apv64, L.apv32);
+  L.ap_ok = true;
+}
+
 dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
   require(o.levels >= 0 && o.levels <= 12, "multigrid: levels must be in [0, 12]");
   require(o.smoother >= 0 && o.smoother <= 3, "multigrid: unknown smoother");
@@ -1964,7 +2167,10 @@ dec_mg* mg_create(const dec_mesh_desc& cd, const dec_mg_options& o) {
   }
   for (int l = 0; l <= o.levels; ++l) {
     Level& L = mg->lv[l];
-    if (l < o.levels) build_transfers(L, mg->lv[l + 1]);
+    if (l < o.levels) {
+      build_transfers(L, mg->lv[l + 1]);
+      build_ap(L);
+    }
     L.lmax = power_lmax(L);
   }
   mg->lc = o.levels;
@@ -2288,6 +2494,123 @@ static void launch_sweep(const Level& L, const T* b, const T* x, T* out, SweepPr
   }
 }
 
+// ---- sweeps fused with the prolongation ----------------------------------------------------------
+// CTAs of a kernel instance resident per SM (queried once per instance; the tag types keep the
+// instances' counters apart): the grid-stride grids stay within one wave.
+template <class Tag, class F>
+static int resident_ctas(F* kern) {
+  static const int ctas = [kern] {
+    int o = 0;
+    DEC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, TB, 0));
+    return std::min(8, std::max(1, o));
+  }();
+  return ctas;
+}
+template <class T, int K, bool SH, bool UPD, int PV, int VV>
+struct SweepPTag {};
+template <class T, int K, bool SH, bool ADD, int VV>
+struct SweepApTag {};
+
+// The second Chebyshev step after x (+)= P z with its previous iterate P z (PV 1) or out + P z (PV 2)
+// formed from the coarse panels z of level Cl.
+template <class T, int K, int PV, int VV>
+static void launch_sweep_p_vv(const Level& L, const Level& Cl, const T* b, const T* x, T* out, SweepPrm<CT<T>> prm,
+                              const T* z, int np, cudaStream_t s, const CT<T>* cs, double* upd) {
+  const size_t ps = (size_t)L.n * K;
+  const CT<T>* off = pick<T>(L.off64, L.off32);
+  const CT<T>* dg = pick<T>(L.diag64, L.diag32);
+  const CT<T>* di = pick<T>(L.dinv64, L.dinv32);
+  const ProlongSrc<T> pz{L.pa.p, L.pb.p, z, (size_t)Cl.n * K};
+  auto go = [&](auto kern, int per_sm) {
+    const dim3 grid(grid_for((long long)L.n, Lanes<T, K, VV>::RPB, per_sm), np);
+    launch_pdl(kern, grid, dim3(TB), s, L.n, L.W, L.col.p, off, dg, di, b, x, out, prm, ps, cs, upd, pz);
+  };
+#define DEC_GO(SHV, UPDV) \
+  go(k_sweep_p<T, K, 6, SHV, UPDV, PV, VV>, \
+     resident_ctas<SweepPTag<T, K, SHV, UPDV, PV, VV>>(k_sweep_p<T, K, 6, SHV, UPDV, PV, VV>))
+  if (cs) {
+    if (upd) DEC_GO(true, true);
+    else DEC_GO(true, false);
+  } else {
+    if (upd) DEC_GO(false, true);
+    else DEC_GO(false, false);
+  }
+#undef DEC_GO
+}
+
+template <class T, int K>
+static void launch_sweep_p(const Level& L, const Level& Cl, const T* b, const T* x, T* out, SweepPrm<CT<T>> prm,
+                           int pv, const T* z, int np, cudaStream_t s, const CT<T>* cs, double* upd) {
+  {
+    const size_t ps = (size_t)L.n * K;
+    const double c = sizeof(CT<T>), v = (double)ps * np * sizeof(T), vc = (double)Cl.n * K * np * sizeof(T);
+    double by = 2.0 * v + (double)L.n * (L.W * (4.0 + c) + c);        // b, x, operator row
+    by += vc + (double)L.n * 8.0;                                      // coarse correction, parent indices
+    if (!cs) by += (double)L.n * c;                                    // 1/diagonal
+    if (pv == 2) by += v;                                              // the iterate before the correction
+    by += upd ? 2.0 * (double)ps * np * sizeof(double) : v;            // out, or u read + written
+    add_bytes(by);
+  }
+  auto run = [&](auto vv) {
+    constexpr int VV = decltype(vv)::value;
+    if (pv == 1) launch_sweep_p_vv<T, K, 1, VV>(L, Cl, b, x, out, prm, z, np, s, cs, upd);
+    else launch_sweep_p_vv<T, K, 2, VV>(L, Cl, b, x, out, prm, z, np, s, cs, upd);
+  };
+  if constexpr (std::is_same<T, float>::value && K >= 8) {
+    if (sweep_variant<K>(L) == 2) {
+      run(std::integral_constant<int, 2>());
+      return;
+    }
+  }
+  run(std::integral_constant<int, 0>());
+}
+
+// The first Chebyshev step after the prolongation (k_sweep_ap): out = x0 + D⁻¹ (b - A x0) / θ with
+// x0 = P z (add: e + P z, e in x) from the coarse panels z of level Cl and A P precomputed.
+template <class T, int K>
+static void launch_sweep_ap(const Level& L, const Level& Cl, const T* b, const T* x, T* out, double inv_theta,
+                            bool add, const T* z, int np, cudaStream_t s, const CT<T>* cs) {
+  const size_t ps = (size_t)L.n * K;
+  {
+    const double c = sizeof(CT<T>), v = (double)ps * np * sizeof(T), vc = (double)Cl.n * K * np * sizeof(T);
+    double by = 2.0 * v + (double)L.n * kApW * (4.0 + c);              // b, out, A P rows
+    by += vc + (double)L.n * 8.0;                                      // coarse correction, parent indices
+    by += cs ? (double)L.n * c : (double)L.n * c;                      // diagonal or 1/diagonal
+    if (add) by += v + (double)L.n * L.W * (4.0 + c);                  // e, the operator's off-diagonals
+    add_bytes(by);
+  }
+  const CT<T>* off = pick<T>(L.off64, L.off32);
+  const CT<T>* dg = pick<T>(L.diag64, L.diag32);
+  const CT<T>* di = pick<T>(L.dinv64, L.dinv32);
+  const CT<T>* apv = pick<T>(L.apv64, L.apv32);
+  const ProlongSrc<T> pz{L.pa.p, L.pb.p, z, (size_t)Cl.n * K};
+  auto run = [&](auto vv) {
+    constexpr int VV = decltype(vv)::value;
+    auto go = [&](auto kern, int per_sm) {
+      const dim3 grid(grid_for((long long)L.n, Lanes<T, K, VV>::RPB, per_sm), np);
+      launch_pdl(kern, grid, dim3(TB), s, L.n, (const int32_t*)L.col.p, off, dg, di, (const int32_t*)L.apc.p, apv,
+                 b, x, out, (CT<T>)inv_theta, ps, cs, pz);
+    };
+#define DEC_GO(SHV, ADDV) \
+  go(k_sweep_ap<T, K, SHV, ADDV, VV>, resident_ctas<SweepApTag<T, K, SHV, ADDV, VV>>(k_sweep_ap<T, K, SHV, ADDV, VV>))
+    if (cs) {
+      if (add) DEC_GO(true, true);
+      else DEC_GO(true, false);
+    } else {
+      if (add) DEC_GO(false, true);
+      else DEC_GO(false, false);
+    }
+#undef DEC_GO
+  };
+  if constexpr (std::is_same<T, float>::value && K >= 8) {
+    if (sweep_variant<K>(L) == 2) {
+      run(std::integral_constant<int, 2>());
+      return;
+    }
+  }
+  run(std::integral_constant<int, 0>());
+}
+
 // ---- the two-step Chebyshev pair ----------------------------------------------------------------
 // Tuning key: P > 0 = the post-smoothing pair of this level runs as k_cheb2 over patches of P rows
 // (128, 256 or 512), 0 (default) = two sweeps.
@@ -2497,6 +2820,55 @@ static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool z
 }
 
 
+// The prolongation x (+)= P z fused into the two Chebyshev steps that follow it (tuning key "pfuse":
+// 1, the default, where the level's iterate was zero (x0 = P z); 2 also onto an iterate; 0 never):
+// the first step forms A x0 from the coarse panels through A P (k_sweep_ap), the second its previous
+// iterate x0 from them (k_sweep_p), so x0 is never stored.  FP32 / FP64 panels,
+// binary-subdivision transfers, rows of 6 off-diagonal slots, two or more post-smoothing steps; a
+// level whose post-smoothing pair runs as k_cheb2 keeps the stored prolongation.
+template <class T, int K>
+static bool prolong_fused(const dec_mg& mg, const Level& L, const CT<T>* cs, int sweeps, bool assign) {
+  if constexpr (std::is_same<T, __half>::value) {
+    return false;
+  } else {
+    if (mg.opt.smoother != DEC_SMOOTH_CHEBYSHEV || sweeps < 2 || !L.ap_ok) return false;
+    if (sweeps == 2 && cheb2_on<T, K>(L, cs)) return false;
+    const int mode = tune_get("pfuse", 1);
+    return mode == 2 || (mode == 1 && assign);
+  }
+}
+
+// smooth() from x0 = P z (assign) or x + P z, the prolongation fused into the first two steps;
+// returns the buffer holding the result, as smooth() after launch_prolong would.
+template <class T, int K>
+static T* smooth_prolonged(const dec_mg& mg, const Level& L, const Level& Cl, LevelBufs<T>& B, T* x, const T* z,
+                           bool assign, int sweeps, int np, cudaStream_t s, double* upd) {
+  const dec_mg_options& o = mg.opt;
+  using C = CT<T>;
+  T* other = (x == B.x.p) ? B.y.p : B.x.p;
+  const double hi = L.lmax, lo = L.lmax / o.cheb_ratio;
+  const double theta = (hi + lo) / 2, delta = (hi - lo) / 2, sigma = theta / delta;
+  double rho = 1 / sigma;
+  // step 1: x (the iterate before the correction, unread when assign) -> other
+  launch_sweep_ap<T, K>(L, Cl, B.b.p, x, other, 1.0 / theta, !assign, z, np, s, B.cs);
+  std::swap(x, other);
+  for (int it = 1; it < sweeps; ++it) {
+    SweepPrm<C> prm{};
+    const double rho_new = 1 / (2 * sigma - rho);
+    prm.mode = S_CHEBN;
+    prm.c1 = (C)(rho_new * rho);
+    prm.c2 = (C)(2 * rho_new / delta);
+    rho = rho_new;
+    double* u = it + 1 == sweeps ? upd : nullptr;
+    if (it == 1)  // previous iterate x0: P z, or (out, still the iterate before the correction) + P z
+      launch_sweep_p<T, K>(L, Cl, B.b.p, x, other, prm, assign ? 1 : 2, z, np, s, B.cs, u);
+    else
+      launch_sweep<T, K>(L, B.b.p, x, other, prm, np, s, B.cs, u);
+    std::swap(x, other);
+  }
+  return x;
+}
+
 // steps iterations of the Krylov CG smoother on level L from x (zero if zero_x); returns the
 // buffer holding x.  FP64 only.
 template <int K>
@@ -2618,6 +2990,10 @@ static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bu
   launch_restrict<T, K>(L, Cl, r, Cb.b.p, np, s);
   T* z = mu_cycle<T, K>(mg, w, bufs, l + 1, Cb.x.p, true, mu, np, s);
   if (mu > 1) z = mu_cycle<T, K>(mg, w, bufs, l + 1, z, false, mu - 1, np, s);
+  if constexpr (!std::is_same<T, __half>::value) {
+    if (prolong_fused<T, K>(mg, L, B.cs, mg.post_at(l), zero_x))
+      return smooth_prolonged<T, K>(mg, L, Cl, B, x, z, zero_x, mg.post_at(l), np, s, upd);
+  }
   // x = 0: the prolonged correction is x (written, not added)
   launch_prolong<T, K>(L, Cl, (const T*)z, x, zero_x, np, s);
   return smooth<T, K>(mg, L, B, x, false, mg.post_at(l), np, s, upd);
@@ -3415,6 +3791,19 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
       launch_sweep<T, K>(L, B.b.p, B.x.p, B.y.p, prm, np, s, B.cs);
     } else if (kernel == DEC_KERNEL_SWEEP_PAIR) {
       launch_cheb2<T, K>(L, B.b.p, B.x.p, B.y.p, 0.5, 0.5, 0.25, np, s, nullptr);
+    } else if (kernel == DEC_KERNEL_SWEEP_PROLONGED0 || kernel == DEC_KERNEL_SWEEP_PROLONGED1) {
+      if constexpr (!std::is_same<T, __half>::value) {
+        const Level& Cl = mg.lv[level + 1];
+        if (kernel == DEC_KERNEL_SWEEP_PROLONGED0) {  // first step from x0 = P z
+          launch_sweep_ap<T, K>(L, Cl, B.b.p, B.x.p, B.y.p, 0.5, false, bufs[level + 1].x.p, np, s, B.cs);
+        } else {  // second step: x from the buffer, the previous iterate P z
+          SweepPrm<CT<T>> prm{};
+          prm.mode = S_CHEBN;
+          prm.c1 = (CT<T>)0.5;
+          prm.c2 = (CT<T>)0.25;
+          launch_sweep_p<T, K>(L, Cl, B.b.p, B.x.p, B.y.p, prm, 1, bufs[level + 1].x.p, np, s, B.cs, nullptr);
+        }
+      }
     } else if (kernel == DEC_KERNEL_MLP) {
       if constexpr (!std::is_same<T, __half>::value)
         launch_mlp_smooth<T, K>(mlp_weights(mg.mlp), L.n, L.W, L.col.p, L.mtab.p, pick<T>(L.diag64, L.diag32),
@@ -3456,6 +3845,13 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
     *bytes = mat + prm_vectors(mg.opt.smoother) * (double)nk * sz;
   } else if (kernel == DEC_KERNEL_SWEEP_PAIR) {
     *bytes = (double)L.n * (L.W * (4.0 + sz) + 2 * sz) + 3.0 * (double)nk * sz;  // operator, x, b, out once
+  } else if (kernel == DEC_KERNEL_SWEEP_PROLONGED0 || kernel == DEC_KERNEL_SWEEP_PROLONGED1) {
+    // step 1: A P rows, 1/diagonal, parents, the coarse correction, b and out; step 2: the operator
+    // row with 1/diagonal, parents, the coarse correction, x, b and out
+    const Level& Cl = mg.lv[level + 1];
+    const double rows = kernel == DEC_KERNEL_SWEEP_PROLONGED0 ? (double)L.n * (kApW * (4.0 + sz) + sz + 8.0)
+                                                               : (double)L.n * (L.W * (4.0 + sz) + 2 * sz + 8.0);
+    *bytes = rows + (double)Cl.n * K * np * sz + (kernel == DEC_KERNEL_SWEEP_PROLONGED0 ? 2.0 : 3.0) * (double)nk * sz;
   } else if (kernel == DEC_KERNEL_MLP) {
     *bytes = (double)L.n * (L.W * (4.0 + sz) + sz) + 3.0 * (double)nk * sz;  // operator, r, x, out
   } else if (kernel == DEC_KERNEL_RESIDUAL) {
@@ -3483,7 +3879,13 @@ static void time_kernel_K(dec_mg& mg, Workspace& w, int kernel, int level, int r
 
 void mg_time_kernel(dec_mg* mg, int kernel, int level, int nrhs, int reps, void* stream, double* ms, double* bytes) {
   require(mg != nullptr && ms != nullptr && bytes != nullptr, "multigrid: null argument");
-  require(kernel >= 0 && kernel <= 5, "multigrid: unknown kernel");
+  require(kernel >= 0 && kernel <= 7, "multigrid: unknown kernel");
+  if (kernel == DEC_KERNEL_SWEEP_PROLONGED0 || kernel == DEC_KERNEL_SWEEP_PROLONGED1) {
+    require(level >= 0 && level + 1 < (int)mg->lv.size(), "multigrid: level out of range");
+    const Level& L = mg->lv[level];
+    require(mg->opt.precision != 2 && L.ap_ok,
+            "multigrid: the prolonged sweeps run on FP32 / FP64 panels over rows of 6 slots with subdivision transfers");
+  }
   if (kernel == DEC_KERNEL_SWEEP_PAIR) {
     Level& L = mg->lv[level];
     const int K = choose_k(*mg, nrhs, mg->opt.precision);
@@ -3495,7 +3897,7 @@ void mg_time_kernel(dec_mg* mg, int kernel, int level, int nrhs, int reps, void*
     if (!L.ts.npatch || L.ts.P != P) build_two_step(L, P);
   }
   require(kernel != DEC_KERNEL_MLP || mg->mlp != nullptr, "multigrid: no learned smoother network set");
-  require(level >= 0 && level < (int)mg->lv.size() - (kernel == 2 || kernel == 3 ? 1 : 0),
+  require(level >= 0 && level < (int)mg->lv.size() - (kernel == 2 || kernel == 3 || kernel >= 6 ? 1 : 0),
           "multigrid: level out of range");
   require(reps >= 1 && nrhs >= 1, "multigrid: reps and nrhs must be positive");
   Workspace& w = workspace(*mg, nrhs, mg->opt.precision);

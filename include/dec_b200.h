@@ -405,9 +405,13 @@ typedef enum dec_mg_kernel {
   DEC_KERNEL_PROLONG = 3,
   DEC_KERNEL_MLP = 4,       /* learned smoothing step (the MLP kernel alone; 10,368 FLOP per sample,
                                10,240 of them on the tensor cores) */
-  DEC_KERNEL_SWEEP_PAIR = 5 /* two Chebyshev steps as one temporal-blocked pass (FP32 panels of 16 or more,
+  DEC_KERNEL_SWEEP_PAIR = 5, /* two Chebyshev steps as one temporal-blocked pass (FP32 panels of 16 or more,
                                rows of 6 slots); bytes: the pair's one-pass minimum (operator, x, b and the
                                result once) */
+  DEC_KERNEL_SWEEP_PROLONGED0 = 6, /* first post-smoothing step from x = P z, the prolongation fused in
+                                      (reads the coarse correction of level + 1; rows of 6 slots) */
+  DEC_KERNEL_SWEEP_PROLONGED1 = 7  /* second Chebyshev step with its previous iterate P z formed the same
+                                      way */
 } dec_mg_kernel;
 /* Times `reps` back-to-back launches of one V-cycle kernel at `level`, configured as in a solve
  * of `nrhs` right-hand sides, with CUDA events on `stream`.  Returns the mean milliseconds per

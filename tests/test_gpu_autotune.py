@@ -75,8 +75,10 @@ def _cheb2_keys(levels, K=32):
 def test_two_step_chebyshev_pair_same_bits(dec):
     """The temporal-blocked post-smoothing pair (k_cheb2: both Chebyshev steps in one pass over patches
     with their halos in shared memory) gives the two sweeps' results bit for bit: V-cycles from a
-    given iterate, and the refined solve whose last sweep adds into the FP64 iterate."""
+    given iterate, and the refined solve whose last sweep adds into the FP64 iterate.  The two sweeps
+    here follow a stored prolongation (tuning key "pfuse" 0), as the pair does."""
     dec.tune_clear()
+    dec.tune_set("pfuse", 0)
     ico = dec.meshes.icosahedron()
     kw = dict(shift=1.0, center="circumcenter", project_radius=1.0, precision=1, pre=0, post=2, cheb_ratio=3.0,
               inner_cycles=3, rhs_block=32)
@@ -96,6 +98,7 @@ def test_two_step_chebyshev_pair_same_bits(dec):
         np.testing.assert_array_equal(out[0][0], o[0])
         np.testing.assert_array_equal(out[0][1], o[1])
         assert out[0][2] == o[2]
+    dec.tune_clear()
     mg = dec.MultigridData(ico, 7, **kw)
     mg.autotune(32, reps=2)
     assert all(dec.tune_get(k) in (0, 128, 256, 512) for k in _cheb2_keys(7))

@@ -436,3 +436,38 @@ def test_solve_traffic_counts_the_graph(dec, built):
     assert mg.solve_traffic(4, 2, from_zero=True) < mg.solve_traffic(4, 2, from_zero=False)
     with pytest.raises(dec.DecError):
         dec.MultigridData(coarse, 2, shift=1.0, center="circumcenter", project_radius=1.0, smoother=2).solve_traffic(1, 1)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("smoother,pre,post", [(1, 0, 2), (1, 2, 2), (1, 1, 3), (0, 1, 1), (1, 0, 1)])
+@pytest.mark.parametrize("nrhs,shifts", [(3, False), (32, False), (5, True)])
+def test_prolongation_fused_into_sweeps(O, dec, precision, smoother, pre, post, nrhs, shifts):
+    """The two Chebyshev steps after a prolongation with the prolonged iterate never stored
+    (k_sweep_ap: A x0 = (A P) z; k_sweep_p: the previous iterate P z formed from the coarse panels;
+    tuning key "pfuse": 1 where the level's iterate was zero, 2 also onto an iterate) against
+    x (+)= P z stored by k_prolong and then swept: the same iterates up to the rounding of the
+    regrouped products, on cycles from zero and from a guess, with per-RHS shifts, FP32 and FP64
+    panels; the same refinement steps to 1e-9."""
+    coarse = O.icosahedron()
+    outs = []
+    try:
+        for fuse in (0, 1, 2):
+            dec.tune_set("pfuse", fuse)
+            kw = dict(coarse_solver=2, coarse_max=170) if shifts else {}
+            mg = dec.MultigridData(coarse, 4, shift=1.0, center="circumcenter", project_radius=1.0,
+                                   precision=precision, smoother=smoother, pre=pre, post=post, omega=0.7,
+                                   cheb_ratio=3.0, inner_cycles=2, **kw)
+            B = torch.tensor(np.stack([uniform(300 + j, mg.n) for j in range(nrhs)]), device="cuda")
+            sh = np.exp(np.linspace(-1.0, 1.0, nrhs)) if shifts else None
+            U = torch.tensor(np.stack([uniform(400 + j, mg.n) * 0.1 for j in range(nrhs)]), device="cuda")
+            U, _ = mg.solve(U, B, rtol=1e-30, max_iters=3, shifts=sh)
+            Uz, rep = mg.solve(torch.zeros_like(B), B, rtol=1e-9, max_iters=40, shifts=sh, use_initial_guess=False)
+            assert rep.converged == 1
+            outs.append((U.cpu().numpy(), Uz.cpu().numpy(), rep.iterations))
+    finally:
+        dec.tune_set("pfuse", 1)
+    tol = 1e-12 if precision == 0 else 1e-5
+    for o in outs[1:]:
+        for a, b in ((outs[0][0], o[0]), (outs[0][1], o[1])):
+            assert np.abs(a - b).max() <= tol * np.abs(a).max()
+        assert outs[0][2] == o[2]
