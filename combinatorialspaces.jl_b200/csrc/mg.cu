@@ -574,16 +574,14 @@ __global__ void __launch_bounds__(TB) k_sweep_ap(int n, const int32_t* __restric
     }
     C r[V], pzi[V], x0[V], acc[V];
     ldv<T, V>(b + ik, r);
-    // the row's own parents are A P's first slots (slot 1 only when they differ), so P z at this row
-    // comes from the same gathers
-    const bool kept = pz.pa[i] == pz.pb[i];
+    // A P's slots 0 and 1 are the row's own parents, so P z at this row comes from the same gathers
     C zk[kApW][V];
 #pragma unroll
     for (int k = 0; k < kApW; ++k) ldv<T, V>(zc + (size_t)pc[k] * K, zk[k]);
 #pragma unroll
     for (int q = 0; q < V; ++q) {
-      pzi[q] = prolong_term(zk[0][q], kept ? zk[0][q] : zk[1][q]);  // P z at this row
-      x0[q] = add_rn(C(0), pzi[q]);                                // k_prolong's assignment (from +0)
+      pzi[q] = prolong_term(zk[0][q], zk[1][q]);  // P z at this row
+      x0[q] = add_rn(C(0), pzi[q]);              // k_prolong's assignment (from +0)
     }
     if constexpr (ADD) {  // A e, as the sweep forms it
       C ei[V];
@@ -2051,18 +2049,22 @@ static void build_transfers(Level& F, const Level& C) {
   DEC_CHECK_LAUNCH();
 }
 
-// Row i of A P (A the level operator, P the prolongation from the next coarser level): the parents
-// of the row itself (½ a_ii each) and of its six neighbours (½ a_ij each), equal coarse columns
-// merged in order of first appearance (FP64 sums); kApW slots, padded with the row's first parent at
-// weight 0.  *bad = 1 if a row has more than kApW distinct coarse columns.
+// Row i of A P (A the level operator, P the prolongation from the next coarser level): slots 0 and 1
+// are the row's own parents pa_i, pb_i (for a kept vertex pa_i twice, the second at weight 0, so a
+// sweep reads P z at the row from slots 0 and 1), then the parents of its six neighbours; equal coarse
+// columns merged into their first slot (FP64 sums of ½ a_ij); kApW slots, padded with pa_i at weight
+// 0.  *bad = 1 if a row has more than kApW slots.
 __global__ void k_ap_build(int n, const int32_t* __restrict__ col, const double* __restrict__ off,
                            const double* __restrict__ diag, const int32_t* __restrict__ pa,
                            const int32_t* __restrict__ pb, int32_t* __restrict__ apc, double* __restrict__ apv,
                            int* __restrict__ bad) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    int c[14];
-    double w[14];
-    int m = 0;
+    int c[16];
+    double w[16];
+    c[0] = pa[i];
+    c[1] = pb[i];
+    w[0] = w[1] = 0.0;
+    int m = 2;
     auto put = [&](int p, double v) {
       for (int k = 0; k < m; ++k)
         if (c[k] == p) {
@@ -2574,7 +2576,7 @@ static void launch_sweep_ap(const Level& L, const Level& Cl, const T* b, const T
   {
     const double c = sizeof(CT<T>), v = (double)ps * np * sizeof(T), vc = (double)Cl.n * K * np * sizeof(T);
     double by = 2.0 * v + (double)L.n * kApW * (4.0 + c);              // b, out, A P rows
-    by += vc + (double)L.n * 8.0;                                      // coarse correction, parent indices
+    by += vc;                                                          // the coarse correction
     by += cs ? (double)L.n * c : (double)L.n * c;                      // diagonal or 1/diagonal
     if (add) by += v + (double)L.n * L.W * (4.0 + c);                  // e, the operator's off-diagonals
     add_bytes(by);
@@ -3846,10 +3848,10 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
   } else if (kernel == DEC_KERNEL_SWEEP_PAIR) {
     *bytes = (double)L.n * (L.W * (4.0 + sz) + 2 * sz) + 3.0 * (double)nk * sz;  // operator, x, b, out once
   } else if (kernel == DEC_KERNEL_SWEEP_PROLONGED0 || kernel == DEC_KERNEL_SWEEP_PROLONGED1) {
-    // step 1: A P rows, 1/diagonal, parents, the coarse correction, b and out; step 2: the operator
-    // row with 1/diagonal, parents, the coarse correction, x, b and out
+    // step 1: A P rows, 1/diagonal, the coarse correction, b and out; step 2: the operator row with
+    // 1/diagonal, parents, the coarse correction, x, b and out
     const Level& Cl = mg.lv[level + 1];
-    const double rows = kernel == DEC_KERNEL_SWEEP_PROLONGED0 ? (double)L.n * (kApW * (4.0 + sz) + sz + 8.0)
+    const double rows = kernel == DEC_KERNEL_SWEEP_PROLONGED0 ? (double)L.n * (kApW * (4.0 + sz) + sz)
                                                                : (double)L.n * (L.W * (4.0 + sz) + 2 * sz + 8.0);
     *bytes = rows + (double)Cl.n * K * np * sz + (kernel == DEC_KERNEL_SWEEP_PROLONGED0 ? 2.0 : 3.0) * (double)nk * sz;
   } else if (kernel == DEC_KERNEL_MLP) {
