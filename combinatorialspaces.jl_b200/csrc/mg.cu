@@ -409,6 +409,11 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
     const size_t ik = po + (size_t)i * K;
     C r[V], xi[V];
     ldv<T, V>(b + ik, r);
+    int pai = 0, pbi = 0;  // PV: the row's parents, loaded with the row's other indices
+    if constexpr (PV != 0) {
+      pai = __ldg(pz.pa + i);
+      pbi = __ldg(pz.pb + i);
+    }
     if (!prm.zero_x) {
       ldv<T, V>(x + ik, xi);
       const C dg = diag[i];
@@ -482,8 +487,8 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
         if constexpr (PV != 0) {  // + ½ z[pa_i] + ½ z[pb_i], k_prolong's arithmetic
           const T* zc = pz.z + (size_t)blockIdx.y * pz.cstride + (size_t)lane * V;
           C za[V], zb[V];
-          ldv<T, V>(zc + (size_t)__ldg(pz.pa + i) * K, za);
-          ldv<T, V>(zc + (size_t)__ldg(pz.pb + i) * K, zb);
+          ldv<T, V>(zc + (size_t)pai * K, za);
+          ldv<T, V>(zc + (size_t)pbi * K, zb);
 #pragma unroll
           for (int q = 0; q < V; ++q) xp[q] = add_rn(PV == 2 ? xp[q] : C(0), prolong_term(za[q], zb[q]));
         }
