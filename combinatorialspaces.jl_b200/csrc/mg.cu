@@ -388,7 +388,9 @@ struct Lanes {
 // iterate (u += (double) e, the update pass's arithmetic) instead of being stored in out.
 // PV (k_sweep_p, a Chebyshev step after the first): the previous iterate is formed from the coarse
 // correction z as the prolongation would have stored it (prolong_term, same bits): 1: P z (the level's
-// iterate was zero), 2: out + P z (out still holds the iterate before the correction).
+// iterate was zero), 2: out + P z (out still holds the iterate before the correction); 3: P z, and the
+// step's result is added to out (the iterate e the correction δ = the smoothed P z belongs to:
+// out = e + δ, each row reading its e before writing; with UPD u += e + δ).
 template <class T, int K, int W, bool SH, bool UPD = false, int VV = 0, int PV = 0>
 __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restrict__ col,
                                            const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
@@ -483,7 +485,7 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
         for (int q = 0; q < V; ++q) dn[q] = xi[q];
       } else {
         C xp[V];
-        if constexpr (PV != 1) ldv<T, V>(out + ik, xp);
+        if constexpr (PV == 0 || PV == 2) ldv<T, V>(out + ik, xp);
         if constexpr (PV != 0) {  // + ½ z[pa_i] + ½ z[pb_i], k_prolong's arithmetic
           const T* zc = pz.z + (size_t)blockIdx.y * pz.cstride + (size_t)lane * V;
           C za[V], zb[V];
@@ -500,6 +502,12 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
         dn[q] = fma_rn(prm.c1, dn[q], mul_rn(prm.c2, mul_rn(di[q], r[q])));
         o[q] = add_rn(xi[q], dn[q]);
       }
+    }
+    if constexpr (PV == 3) {  // out = e + δ
+      C ev[V];
+      ldv<T, V>(out + ik, ev);
+#pragma unroll
+      for (int q = 0; q < V; ++q) o[q] = add_rn(ev[q], o[q]);
     }
     if constexpr (UPD) {
 #pragma unroll
@@ -2554,14 +2562,15 @@ static void launch_sweep_p(const Level& L, const Level& Cl, const T* b, const T*
     double by = 2.0 * v + (double)L.n * (L.W * (4.0 + c) + c);        // b, x, operator row
     by += vc + (double)L.n * 8.0;                                      // coarse correction, parent indices
     if (!cs) by += (double)L.n * c;                                    // 1/diagonal
-    if (pv == 2) by += v;                                              // the iterate before the correction
+    if (pv >= 2) by += v;                                              // the iterate before the correction
     by += upd ? 2.0 * (double)ps * np * sizeof(double) : v;            // out, or u read + written
     add_bytes(by);
   }
   auto run = [&](auto vv) {
     constexpr int VV = decltype(vv)::value;
     if (pv == 1) launch_sweep_p_vv<T, K, 1, VV>(L, Cl, b, x, out, prm, z, np, s, cs, upd);
-    else launch_sweep_p_vv<T, K, 2, VV>(L, Cl, b, x, out, prm, z, np, s, cs, upd);
+    else if (pv == 2) launch_sweep_p_vv<T, K, 2, VV>(L, Cl, b, x, out, prm, z, np, s, cs, upd);
+    else launch_sweep_p_vv<T, K, 3, VV>(L, Cl, b, x, out, prm, z, np, s, cs, upd);
   };
   if constexpr (std::is_same<T, float>::value && K >= 8) {
     if (sweep_variant<K>(L) == 2) {
@@ -2828,11 +2837,14 @@ static T* smooth(const dec_mg& mg, const Level& L, LevelBufs<T>& B, T* x, bool z
 
 
 // The prolongation x (+)= P z fused into the two Chebyshev steps that follow it (tuning key "pfuse":
-// 1, the default, where the level's iterate was zero (x0 = P z); 2 also onto an iterate; 0 never):
-// the first step forms A x0 from the coarse panels through A P (k_sweep_ap), the second its previous
-// iterate x0 from them (k_sweep_p), so x0 is never stored.  FP32 / FP64 panels,
+// 1 where the level's iterate was zero (x0 = P z); 2 also onto an iterate e (x0 = e + P z); 3, the
+// default, 1 and onto an iterate in correction form (two post-smoothing steps: the steps smooth δ on
+// A δ = r, r = b - A e the residual the cycle restricted, from δ0 = P z, and the second stores e + δ);
+// 0 never): the first step forms A x0 from the coarse panels through A P (k_sweep_ap), the second its
+// previous iterate from them (k_sweep_p), so x0 is never stored.  FP32 / FP64 panels,
 // binary-subdivision transfers, rows of 6 off-diagonal slots, two or more post-smoothing steps; a
 // level whose post-smoothing pair runs as k_cheb2 keeps the stored prolongation.
+constexpr int kPfuseDefault = 3;
 template <class T, int K>
 static bool prolong_fused(const dec_mg& mg, const Level& L, const CT<T>* cs, int sweeps, bool assign) {
   if constexpr (std::is_same<T, __half>::value) {
@@ -2840,8 +2852,8 @@ static bool prolong_fused(const dec_mg& mg, const Level& L, const CT<T>* cs, int
   } else {
     if (mg.opt.smoother != DEC_SMOOTH_CHEBYSHEV || sweeps < 2 || !L.ap_ok) return false;
     if (sweeps == 2 && cheb2_on<T, K>(L, cs)) return false;
-    const int mode = tune_get("pfuse", 1);
-    return mode == 2 || (mode == 1 && assign);
+    const int mode = tune_get("pfuse", kPfuseDefault);
+    return assign ? mode != 0 : (mode == 2 || (mode == 3 && sweeps == 2));
   }
 }
 
@@ -2873,6 +2885,26 @@ static T* smooth_prolonged(const dec_mg& mg, const Level& L, const Level& Cl, Le
       launch_sweep<T, K>(L, B.b.p, x, other, prm, np, s, B.cs, u);
     std::swap(x, other);
   }
+  return x;
+}
+
+// Two post-smoothing Chebyshev steps from e + P z in correction form: δ1 from δ0 = P z on A δ = r
+// (k_sweep_ap into B.d), then δ2 and the stored e + δ2 (k_sweep_p, PV 3, into e's buffer x or added to
+// the FP64 iterate with upd).  r: the residual b - A e the cycle restricted.  Returns x.
+template <class T, int K>
+static T* smooth_correction(const dec_mg& mg, const Level& L, const Level& Cl, LevelBufs<T>& B, T* x, const T* r,
+                            const T* z, int np, cudaStream_t s, double* upd) {
+  const dec_mg_options& o = mg.opt;
+  using C = CT<T>;
+  const double hi = L.lmax, lo = L.lmax / o.cheb_ratio;
+  const double theta = (hi + lo) / 2, delta = (hi - lo) / 2, sigma = theta / delta;
+  const double rho = 1 / sigma, rho_new = 1 / (2 * sigma - rho);
+  launch_sweep_ap<T, K>(L, Cl, r, nullptr, B.d.p, 1.0 / theta, false, z, np, s, B.cs);
+  SweepPrm<C> prm{};
+  prm.mode = S_CHEBN;
+  prm.c1 = (C)(rho_new * rho);
+  prm.c2 = (C)(2 * rho_new / delta);
+  launch_sweep_p<T, K>(L, Cl, r, B.d.p, x, prm, 3, z, np, s, B.cs, upd);
   return x;
 }
 
@@ -2998,8 +3030,11 @@ static T* mu_cycle(const dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& bu
   T* z = mu_cycle<T, K>(mg, w, bufs, l + 1, Cb.x.p, true, mu, np, s);
   if (mu > 1) z = mu_cycle<T, K>(mg, w, bufs, l + 1, z, false, mu - 1, np, s);
   if constexpr (!std::is_same<T, __half>::value) {
-    if (prolong_fused<T, K>(mg, L, B.cs, mg.post_at(l), zero_x))
+    if (prolong_fused<T, K>(mg, L, B.cs, mg.post_at(l), zero_x)) {
+      if (!zero_x && tune_get("pfuse", kPfuseDefault) == 3)  // r: the restricted residual b - A x
+        return smooth_correction<T, K>(mg, L, Cl, B, x, r, z, np, s, upd);
       return smooth_prolonged<T, K>(mg, L, Cl, B, x, z, zero_x, mg.post_at(l), np, s, upd);
+    }
   }
   // x = 0: the prolonged correction is x (written, not added)
   launch_prolong<T, K>(L, Cl, (const T*)z, x, zero_x, np, s);

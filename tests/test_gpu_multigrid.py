@@ -444,14 +444,15 @@ def test_solve_traffic_counts_the_graph(dec, built):
 def test_prolongation_fused_into_sweeps(O, dec, precision, smoother, pre, post, nrhs, shifts):
     """The two Chebyshev steps after a prolongation with the prolonged iterate never stored
     (k_sweep_ap: A x0 = (A P) z; k_sweep_p: the previous iterate P z formed from the coarse panels;
-    tuning key "pfuse": 1 where the level's iterate was zero, 2 also onto an iterate) against
+    tuning key "pfuse": 1 where the level's iterate was zero, 2 also onto an iterate, 3 onto an iterate
+    in correction form) against
     x (+)= P z stored by k_prolong and then swept: the same iterates up to the rounding of the
     regrouped products, on cycles from zero and from a guess, with per-RHS shifts, FP32 and FP64
     panels; the same refinement steps to 1e-9."""
     coarse = O.icosahedron()
     outs = []
     try:
-        for fuse in (0, 1, 2):
+        for fuse in (0, 1, 2, 3):
             dec.tune_set("pfuse", fuse)
             kw = dict(coarse_solver=2, coarse_max=170) if shifts else {}
             mg = dec.MultigridData(coarse, 4, shift=1.0, center="circumcenter", project_radius=1.0,
@@ -465,7 +466,7 @@ def test_prolongation_fused_into_sweeps(O, dec, precision, smoother, pre, post, 
             assert rep.converged == 1
             outs.append((U.cpu().numpy(), Uz.cpu().numpy(), rep.iterations))
     finally:
-        dec.tune_set("pfuse", 1)
+        dec.tune_set("pfuse", 3)
     tol = 1e-12 if precision == 0 else 1e-5
     for o in outs[1:]:
         for a, b in ((outs[0][0], o[0]), (outs[0][1], o[1])):
