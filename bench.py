@@ -855,11 +855,14 @@ def run_ours(args):
     e2e_value = whole_job_rate(NRHS, world, args.steps, t_e2e)
     bytes_vec = NRHS * n * 8
 
-    # --- roofline of the dominant kernel (the finest-level smoothing sweep), timed alone ---
-    ms, algo_bytes = mg.time_kernel(0, 0, NRHS, reps=20)
+    # --- roofline of the dominant kernel, timed alone: the first Chebyshev step after the fused
+    # prolongation on the finest level (k_sweep_ap, the largest share of the solve's launch list);
+    # beside it the plain Chebyshev step (k_sweep) ---
+    ms, algo_bytes = mg.time_kernel(6, 0, NRHS, reps=20)
+    ms_sw, bytes_sw = mg.time_kernel(0, 0, NRHS, reps=20)
     peak, peak_kind = measured_peaks()
     achieved = algo_bytes / (ms * 1e-3) / 1e9
-    traffic = traffic_per_launch("k_sweep")
+    traffic = traffic_per_launch("k_sweep_ap")
 
     # --- the whole step's algorithmic bytes (every kernel of the solve graph) against its time ---
     step_bytes = mg.solve_traffic(NRHS, int(rep0.iterations))
@@ -930,9 +933,14 @@ def run_ours(args):
                            "plain": "the faster of the two FP64 V-cycle solves"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": f"k_sweep<float,{int(tuned)},6> finest level",
+                         "kernel": f"k_sweep_ap<float,{int(tuned)}> finest level (first step after the prolongation)",
                          "algorithmic_bytes_per_launch": algo_bytes, "ms_per_launch": ms,
                          "peak_kind": f"{peak_kind} (HBM copy, burst)",
+                         "plain_step": {"kernel": f"k_sweep<float,{int(tuned)},6> finest level (middle Chebyshev step)",
+                                        "ms_per_launch": ms_sw, "algorithmic_bytes_per_launch": bytes_sw,
+                                        "achieved": bytes_sw / (ms_sw * 1e-3) / 1e9,
+                                        "frac": bytes_sw / (ms_sw * 1e-3) / 1e9 / peak,
+                                        "traffic": traffic_per_launch("k_sweep")},
                          "step_algorithmic_bytes": step_bytes, "step_GB/s": step_gbs,
                          "step_frac": step_gbs / peak},
             "cpu_baseline": cpu,

@@ -587,10 +587,18 @@ __global__ void __launch_bounds__(TB) k_sweep_ap(int n, const int32_t* __restric
     }
     C r[V], pzi[V], x0[V], acc[V];
     ldv<T, V>(b + ik, r);
-    // A P's slots 0 and 1 are the row's own parents, so P z at this row comes from the same gathers
+    // A P's slots 0 and 1 are the row's own parents, so P z at this row comes from the same gathers;
+    // the padding slots (column -1: a midpoint row has four columns) are not gathered
     C zk[kApW][V];
 #pragma unroll
-    for (int k = 0; k < kApW; ++k) ldv<T, V>(zc + (size_t)pc[k] * K, zk[k]);
+    for (int k = 0; k < kApW; ++k) {
+      if (k < 2 || pc[k] >= 0) {
+        ldv<T, V>(zc + (size_t)pc[k] * K, zk[k]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < V; ++q) zk[k][q] = C(0);
+      }
+    }
 #pragma unroll
     for (int q = 0; q < V; ++q) {
       pzi[q] = prolong_term(zk[0][q], zk[1][q]);  // P z at this row
@@ -2065,8 +2073,8 @@ static void build_transfers(Level& F, const Level& C) {
 // Row i of A P (A the level operator, P the prolongation from the next coarser level): slots 0 and 1
 // are the row's own parents pa_i, pb_i (for a kept vertex pa_i twice, the second at weight 0, so a
 // sweep reads P z at the row from slots 0 and 1), then the parents of its six neighbours; equal coarse
-// columns merged into their first slot (FP64 sums of ½ a_ij); kApW slots, padded with pa_i at weight
-// 0.  *bad = 1 if a row has more than kApW slots.
+// columns merged into their first slot (FP64 sums of ½ a_ij); kApW slots, padded with column -1 at
+// weight 0.  *bad = 1 if a row has more than kApW slots.
 __global__ void k_ap_build(int n, const int32_t* __restrict__ col, const double* __restrict__ off,
                            const double* __restrict__ diag, const int32_t* __restrict__ pa,
                            const int32_t* __restrict__ pb, int32_t* __restrict__ apc, double* __restrict__ apv,
@@ -2102,7 +2110,7 @@ __global__ void k_ap_build(int n, const int32_t* __restrict__ col, const double*
       m = kApW;
     }
     for (int k = 0; k < kApW; ++k) {
-      apc[(size_t)i * kApW + k] = k < m ? c[k] : pa[i];
+      apc[(size_t)i * kApW + k] = k < m ? c[k] : -1;
       apv[(size_t)i * kApW + k] = k < m ? w[k] : 0.0;
     }
   }
