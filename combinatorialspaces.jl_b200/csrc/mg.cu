@@ -320,6 +320,18 @@ __device__ __forceinline__ void ldv(const S* p, C (&r)[V]) {
 }
 template <class S, int V, class C>
 __device__ __forceinline__ void stv(S* p, const C (&r)[V]) {
+  if constexpr (!std::is_same<S, __half>::value && sizeof(S) * V > 16) {  // several 16-byte stores
+    constexpr int H = 16 / sizeof(S);
+    static_assert(V % H == 0, "vector width");
+#pragma unroll
+    for (int c = 0; c < V / H; ++c) {
+      C t[H];
+#pragma unroll
+      for (int k = 0; k < H; ++k) t[k] = r[c * H + k];
+      stv<S, H>(p + c * H, t);
+    }
+    return;
+  } else {
   using VT = typename VecT<S, V>::t;
   VT t;
   if constexpr (std::is_same<S, __half>::value) {
@@ -331,6 +343,7 @@ __device__ __forceinline__ void stv(S* p, const C (&r)[V]) {
     memcpy(&t, r, sizeof(VT));
   }
   *reinterpret_cast<VT*>(p) = t;
+  }
 }
 template <class T> __device__ __forceinline__ double to_d(T v) { return (double)v; }
 template <> __device__ __forceinline__ double to_d<__half>(__half v) { return (double)__half2float(v); }
