@@ -801,13 +801,14 @@ __global__ void __launch_bounds__(TB, kSweepHalfBlocks) k_sweep_h(
 
 // Restriction R = row-normalised S (make_restriction, Multigrid.jl:595-612):
 // rc[i] = (1/rs_i) rf[self_i] + Σ_e (0.5/rs_i) rf[mid_e], rs_i = 1 + deg_i / 2, terms in the
-// reference's column order.  A row's midpoints fill the front of its ridx slots (-1 after them).
+// reference's column order; the two weights per row come rounded to the compute type from setup
+// (rw: (C)(1.0 / rs_i), (C)(0.5 / rs_i)).  A row's midpoints fill the front of its ridx slots (-1 after them).
 // WQ > 0 (the slot count, known at compile time) loads every midpoint index first and issues all
 // the row's gathers before the first sum, instead of one index -> gather -> sum chain per slot;
 // the sums keep the same order, so the result is the same bit for bit.
 template <class T, int K, int WQ = 0>
 __global__ void __launch_bounds__(TB) k_restrict(int nc, int Wq, const int32_t* __restrict__ rself,
-                                                 const int32_t* __restrict__ ridx, const double* __restrict__ rs,
+                                                 const int32_t* __restrict__ ridx, const CT<T>* __restrict__ rw,
                                                  const T* __restrict__ rf, T* __restrict__ rc, size_t fstride,
                                                  size_t cstride) {
   using Ln = Lanes<T, K>;
@@ -818,8 +819,7 @@ __global__ void __launch_bounds__(TB) k_restrict(int nc, int Wq, const int32_t* 
   const T* f = rf + (size_t)blockIdx.y * fstride + (size_t)lane * V;
   T* c = rc + (size_t)blockIdx.y * cstride + (size_t)lane * V;
   for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < nc; i += gridDim.x * Ln::RPB) {
-    const double s = rs[i];
-    const C w1 = (C)(1.0 / s), wh = (C)(0.5 / s);
+    const C w1 = rw[2 * (size_t)i], wh = rw[2 * (size_t)i + 1];  // (C)(1 / rs_i), (C)(0.5 / rs_i)
     C acc[V], v[V];
     if constexpr (WQ > 0) {
       int m[WQ];
@@ -1589,6 +1589,8 @@ struct Level {
   int nc = 0, Wq = 0;
   DArr<int32_t> rself, ridx, pa, pb;
   DArr<double> rs;
+  DArr<double> rw64;  // per coarse row (1 / rs, 0.5 / rs), FP64 and rounded to FP32
+  DArr<float> rw32;
   // A P (kApW coarse columns per fine row) for the first sweep after a prolongation (k_sweep_ap);
   // built for binary-subdivision levels with rows of 6 off-diagonal slots
   bool ap_ok = false;
@@ -2065,6 +2067,18 @@ __global__ void k_prolong_lists(int nf, int nc, const int32_t* __restrict__ fper
   }
 }
 
+// The restriction's two weights per coarse row, (1 / rs, 0.5 / rs), in FP64 and rounded to FP32.
+__global__ void k_restrict_weights(int nc, const double* __restrict__ rs, double* __restrict__ w64,
+                                   float* __restrict__ w32) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nc; i += gridDim.x * blockDim.x) {
+    const double a = 1.0 / rs[i], h = 0.5 / rs[i];
+    w64[2 * (size_t)i] = a;
+    w64[2 * (size_t)i + 1] = h;
+    w32[2 * (size_t)i] = (float)a;
+    w32[2 * (size_t)i + 1] = (float)h;
+  }
+}
+
 // Transfers between fine level F and its coarse level C, in the internal numbering of both, from
 // the coarse mesh's device topology (a simplicial complex: no edge has ∂v0 = ∂v1).
 static void build_transfers(Level& F, const Level& C) {
@@ -2079,6 +2093,9 @@ static void build_transfers(Level& F, const Level& C) {
   const int T = 256;
   k_restrict_lists<<<grid_for(c.nv, T), T>>>(c.nv, F.Wq, C.dperm.p, F.diperm.p, c.v2e_ptr.p, c.v2e.p, F.rself.p,
                                              F.ridx.p, F.rs.p);
+  F.rw64.alloc(2 * (size_t)c.nv);
+  F.rw32.alloc(2 * (size_t)c.nv);
+  k_restrict_weights<<<grid_for(c.nv, T), T>>>(c.nv, F.rs.p, F.rw64.p, F.rw32.p);
   k_prolong_lists<<<grid_for(F.n, T), T>>>(F.n, c.nv, F.dperm.p, C.diperm.p, c.ev0.p, c.ev1.p, F.pa.p, F.pb.p);
   DEC_CHECK_LAUNCH();
 }
@@ -2404,12 +2421,13 @@ static void launch_restrict(const Level& L, const Level& Cl, const T* r, T* bc, 
   const int ctas = L.Wq == 6 ? restrict_ctas<T, K, 6>() : restrict_ctas<T, K, 0>();
   g.x = std::min<unsigned>(g.x, (unsigned)(ctas * num_sms()));
   const size_t fs = (size_t)L.n * K, cs = (size_t)Cl.n * K;
-  add_bytes((double)Cl.n * ((L.Wq + 1) * 4.0 + 8) + (double)(fs + cs) * np * sizeof(T));
+  add_bytes((double)Cl.n * ((L.Wq + 1) * 4.0 + 2 * sizeof(CT<T>)) + (double)(fs + cs) * np * sizeof(T));
+  const CT<T>* rw = pick<T>(L.rw64, L.rw32);
   if (pdl)
-    launch_pdl(kern, g, dim3(TB), s, L.nc, L.Wq, (const int32_t*)L.rself.p, (const int32_t*)L.ridx.p,
-               (const double*)L.rs.p, r, bc, fs, cs);
+    launch_pdl(kern, g, dim3(TB), s, L.nc, L.Wq, (const int32_t*)L.rself.p, (const int32_t*)L.ridx.p, rw, r, bc,
+               fs, cs);
   else
-    kern<<<g, TB, 0, s>>>(L.nc, L.Wq, L.rself.p, L.ridx.p, L.rs.p, r, bc, fs, cs);
+    kern<<<g, TB, 0, s>>>(L.nc, L.Wq, L.rself.p, L.ridx.p, rw, r, bc, fs, cs);
 }
 
 // x_f (+)= P z on all panels; assign when x_f is known to be zero (no clear, no read of x_f).
@@ -3923,7 +3941,7 @@ static void time_kernel_T(dec_mg& mg, Workspace& w, std::vector<LevelBufs<T>>& b
     *bytes = mat + (double)F.n * K * np * (8 + 8 + sz);
   } else if (kernel == DEC_KERNEL_RESTRICT) {
     const Level& Cl = mg.lv[level + 1];
-    const double idx = L.gen ? (double)Cl.n * L.Wr * (4.0 + sizeof(CT<T>)) : (double)Cl.n * ((L.Wq + 1) * 4.0 + 8);
+    const double idx = L.gen ? (double)Cl.n * L.Wr * (4.0 + sizeof(CT<T>)) : (double)Cl.n * ((L.Wq + 1) * 4.0 + 2 * sizeof(CT<T>));
     *bytes = idx + (double)nk * sz + (double)Cl.n * K * np * sz;
   } else {
     const Level& Cl = mg.lv[level + 1];
