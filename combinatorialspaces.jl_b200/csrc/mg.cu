@@ -222,23 +222,24 @@ struct LoopState {
 
 
 // Programmatic dependent launch: every kernel of a cycle is launched with the
-// programmatic-serialization attribute, waits for its predecessor's results with
-// griddepcontrol.wait before touching memory, and lets its successor start launching at once.
-// The launches of a cycle then overlap the tails of the kernels before them.
+// programmatic-serialization attribute and waits for its predecessor's results with
+// griddepcontrol.wait before touching memory.  A kernel does not trigger its dependents early: the
+// trigger is the implicit one as its blocks exit, so the next launch is prepared during the tail of
+// the kernel before it without taking SM slots from the kernel's own blocks.
 __device__ __forceinline__ void pdl_enter() {
 #if __CUDA_ARCH__ >= 900
   asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;");
 #endif
 }
 
-// The attribute is off unless DEC_B200_PDL=1: measured on B200, the early launch of dependents
-// overlaps small kernels' launch latency but takes SM slots from the large finest-level kernels,
-// and the whole solve ran about 4% slower with it.
+// On unless DEC_B200_PDL=0.  Measured on B200 (same process, 10 L8 solves of 32 RHS; 20 L6
+// single-RHS FP64 solves): without the attribute 10,440 solves/s and 0.928 ms; with dependents
+// triggered at each kernel's start 10,250 and 0.891 ms (their blocks took SM slots from the large
+// finest-level kernels); with the implicit trigger at exit 10,525 and 0.840 ms.
 static bool pdl_enabled() {
   static const bool on = [] {
     const char* v = std::getenv("DEC_B200_PDL");
-    return v && v[0] == '1';
+    return !(v && v[0] == '0');
   }();
   return on;
 }
