@@ -232,6 +232,18 @@ __device__ __forceinline__ void pdl_enter() {
 #endif
 }
 
+// An L2 prefetch of the bytes [p, p + bytes) as one bulk request (cp.async.bulk.prefetch, no register
+// held while it is in flight), trimmed inward to 16-byte boundaries so nothing outside the range is
+// touched.  The row kernels issue it for the rows their CTA takes next, so those rows' streamed loads
+// (b, the iterate, the operator rows) hit L2 instead of starting a DRAM round trip in front of the
+// gathers that depend on them.
+__device__ __forceinline__ void l2_prefetch(const void* p, size_t bytes) {
+  size_t a = __cvta_generic_to_global(p), e = a + bytes;
+  a = (a + 15) & ~size_t(15);
+  e &= ~size_t(15);
+  if (e > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)));
+}
+
 // On unless DEC_B200_PDL=0.  Measured on B200 (same process, 10 L8 solves of 32 RHS; 20 L6
 // single-RHS FP64 solves): without the attribute 10,440 solves/s and 0.928 ms; with dependents
 // triggered at each kernel's start 10,250 and 0.891 ms (their blocks took SM slots from the large
@@ -389,6 +401,20 @@ struct Lanes {
   static constexpr int RPB = TB / LPR;     // rows per block
 };
 
+// The row kernels' FP32 forms (unshifted, fixed width, not adding an iterate) are compiled for 8
+// resident CTAs of 256 threads per SM (32 registers a thread: every warp slot holds a warp waiting on
+// its loads) and prefetch the rows their CTA takes next (l2_prefetch).  The other forms keep the code
+// and the register counts they have without either: forced to 32 registers they spill, and with the
+// prefetch alone their counts rose (FP64 panels 32-40 -> 70-124) and their occupancy fell.  Measured on
+// B200 at icosphere L8 with 32 FP32 right-hand sides: k_sweep_ap 47.1 -> 44.0 us, the second step after
+// the prolongation 67.4 -> 59.8 us (40 registers and 6 CTAs per SM before), the FP64 residual
+// 103.5 -> 91.3 us, a middle Chebyshev step 64.6 -> 62.8 us (the cap alone), the solve 10,525 ->
+// 10,705 solves/s with every iterate bit for bit.
+template <class T, bool KEEP>
+constexpr int kRowCtas = (sizeof(T) == 4 && !KEEP) ? 8 : 0;  // 0: no bound given
+template <class T, bool KEEP>
+constexpr bool kRowPrefetch = sizeof(T) == 4 && !KEEP;
+
 // One smoothing sweep / residual on all panels: r = b - A x, then
 //   S_RESID : out = r
 //   S_JACOBI: out = x + ω D⁻¹ r
@@ -423,6 +449,28 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
   if constexpr (SH) ldv<C, V>(shf + (size_t)blockIdx.y * K + (size_t)lane * V, csv);
   for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < n; i += gridDim.x * Ln::RPB) {
     const size_t ik = po + (size_t)i * K;
+    // the CTA's next rows (i is their first row here), except in a plain middle Chebyshev step
+    // (measured slower with it: 64.2 -> 69.7 us at L8, 32 FP32 right-hand sides)
+    if (kRowPrefetch<T, SH || W == 0> && threadIdx.x == 0 && i + gridDim.x * Ln::RPB < n &&
+        (PV != 0 || UPD || prm.mode != S_CHEBN)) {
+      const int j = i + gridDim.x * Ln::RPB, m = min(Ln::RPB, n - j);
+      const size_t pj = (size_t)blockIdx.y * pstride + (size_t)j * K, vb = (size_t)m * K * sizeof(T);
+      l2_prefetch(b + pj, vb);
+      if (!prm.zero_x) {
+        l2_prefetch(x + pj, vb);
+        l2_prefetch(col + (size_t)j * w, (size_t)m * w * sizeof(int32_t));
+        l2_prefetch(off + (size_t)j * w, (size_t)m * w * sizeof(C));
+        l2_prefetch(diag + j, (size_t)m * sizeof(C));
+      }
+      if (!SH && prm.mode != S_RESID) l2_prefetch(dinv + j, (size_t)m * sizeof(C));
+      if ((PV == 0 || PV == 2) && prm.mode == S_CHEBN && !prm.d_is_x) l2_prefetch(out + pj, vb);
+      if constexpr (PV == 3) l2_prefetch(out + pj, vb);
+      if constexpr (UPD) l2_prefetch(u64 + pj, (size_t)m * K * sizeof(double));
+      if constexpr (PV != 0) {
+        l2_prefetch(pz.pa + j, (size_t)m * sizeof(int32_t));
+        l2_prefetch(pz.pb + j, (size_t)m * sizeof(int32_t));
+      }
+    }
     C r[V], xi[V];
     ldv<T, V>(b + ik, r);
     int pai = 0, pbi = 0;  // PV: the row's parents, loaded with the row's other indices
@@ -533,7 +581,8 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
 }
 
 template <class T, int K, int W, bool SH, int VV = 0>
-__global__ void __launch_bounds__(TB) k_sweep(int n, int Wr, const int32_t* __restrict__ col,
+__global__ void __launch_bounds__(TB, kRowCtas<T, SH || W == 0>)
+    k_sweep(int n, int Wr, const int32_t* __restrict__ col,
                                               const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
                                               const CT<T>* __restrict__ dinv, const T* __restrict__ b,
                                               const T* __restrict__ x, T* __restrict__ out,
@@ -544,7 +593,8 @@ __global__ void __launch_bounds__(TB) k_sweep(int n, int Wr, const int32_t* __re
 // The last sweep of a refinement step's V-cycles on the finest level with the step's update
 // u += e fused in (FP32 / FP64 storage).
 template <class T, int K, int W, bool SH, int VV = 0>
-__global__ void __launch_bounds__(TB) k_sweep_u(int n, int Wr, const int32_t* __restrict__ col,
+__global__ void __launch_bounds__(TB, kRowCtas<T, SH || W == 0>)
+    k_sweep_u(int n, int Wr, const int32_t* __restrict__ col,
                                                 const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
                                                 const CT<T>* __restrict__ dinv, const T* __restrict__ b,
                                                 const T* __restrict__ x, T* __restrict__ out,
@@ -556,7 +606,8 @@ __global__ void __launch_bounds__(TB) k_sweep_u(int n, int Wr, const int32_t* __
 // The second Chebyshev step after x (+)= P z with its previous iterate formed from z (PV = 1: P z,
 // 2: out + P z), so the prolonged iterate is never read back.  UPD as k_sweep_u.
 template <class T, int K, int W, bool SH, bool UPD, int PV, int VV = 0>
-__global__ void __launch_bounds__(TB) k_sweep_p(int n, int Wr, const int32_t* __restrict__ col,
+__global__ void __launch_bounds__(TB, kRowCtas<T, SH || W == 0>)
+    k_sweep_p(int n, int Wr, const int32_t* __restrict__ col,
                                                 const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
                                                 const CT<T>* __restrict__ dinv, const T* __restrict__ b,
                                                 const T* __restrict__ x, T* __restrict__ out,
@@ -575,7 +626,8 @@ constexpr int kApW = 8;
 // A P precomputed per level (apc / apv, kApW slots per row); out = x0 + D⁻¹ r / θ.  SH: A + cs I per
 // right-hand side (A P then holds the unshifted product and cs x0 is added).
 template <class T, int K, bool SH, bool ADD, int VV = 0>
-__global__ void __launch_bounds__(TB) k_sweep_ap(int n, const int32_t* __restrict__ col, const CT<T>* __restrict__ off,
+__global__ void __launch_bounds__(TB, kRowCtas<T, SH || ADD>)
+    k_sweep_ap(int n, const int32_t* __restrict__ col, const CT<T>* __restrict__ off,
                                                  const CT<T>* __restrict__ diag, const CT<T>* __restrict__ dinv,
                                                  const int32_t* __restrict__ apc, const CT<T>* __restrict__ apv,
                                                  const T* __restrict__ b, const T* __restrict__ e,
@@ -592,6 +644,14 @@ __global__ void __launch_bounds__(TB) k_sweep_ap(int n, const int32_t* __restric
   if constexpr (SH) ldv<C, V>(shf + (size_t)blockIdx.y * K + (size_t)lane * V, csv);
   for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < n; i += gridDim.x * Ln::RPB) {
     const size_t ik = po + (size_t)i * K;
+    if (kRowPrefetch<T, SH || ADD> && threadIdx.x == 0 && i + gridDim.x * Ln::RPB < n) {  // the CTA's next rows
+      const int j = i + gridDim.x * Ln::RPB, m = min(Ln::RPB, n - j);            // (i: their first)
+      l2_prefetch(b + (size_t)blockIdx.y * pstride + (size_t)j * K, (size_t)m * K * sizeof(T));
+      l2_prefetch(apc + (size_t)j * kApW, (size_t)m * kApW * sizeof(int32_t));
+      l2_prefetch(apv + (size_t)j * kApW, (size_t)m * kApW * sizeof(C));
+      if constexpr (!SH) l2_prefetch(dinv + j, (size_t)m * sizeof(C));
+      if constexpr (ADD) l2_prefetch(e + (size_t)blockIdx.y * pstride + (size_t)j * K, (size_t)m * K * sizeof(T));
+    }
     int pc[kApW];
     C pw[kApW];
 #pragma unroll
@@ -1112,7 +1172,8 @@ __global__ void k_scale_half(int n, int np, const float* __restrict__ r, const d
 // FP64 residual r = b - A u on the panels, written in the inner precision T, with per-block
 // partial sums of r² per right-hand side (deterministic two-stage reduction).
 template <class T, int K, int W, bool SH>
-__global__ void __launch_bounds__(TB) k_residual64(int n, int Wr, const int32_t* __restrict__ col,
+__global__ void __launch_bounds__(TB, kRowCtas<T, SH || W == 0>)
+    k_residual64(int n, int Wr, const int32_t* __restrict__ col,
                                                    const double* __restrict__ off, const double* __restrict__ diag,
                                                    const double* __restrict__ b, const double* __restrict__ u,
                                                    T* __restrict__ rT, double* __restrict__ partial, size_t pstride,
@@ -1129,6 +1190,15 @@ __global__ void __launch_bounds__(TB) k_residual64(int n, int Wr, const int32_t*
   if constexpr (SH) ldv<double, V>(cs + (size_t)blockIdx.y * K + (size_t)lane * V, csv);
   for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < n; i += gridDim.x * Ln::RPB) {
     const size_t ik = po + (size_t)i * K;
+    if (kRowPrefetch<T, SH || W == 0> && threadIdx.x == 0 && i + gridDim.x * Ln::RPB < n) {  // the CTA's next rows
+      const int j = i + gridDim.x * Ln::RPB, m = min(Ln::RPB, n - j);            // (i: their first)
+      const size_t pj = (size_t)blockIdx.y * pstride + (size_t)j * K, vb = (size_t)m * K * sizeof(double);
+      l2_prefetch(u + pj, vb);
+      l2_prefetch(b + pj, vb);
+      l2_prefetch(col + (size_t)j * w, (size_t)m * w * sizeof(int32_t));
+      l2_prefetch(off + (size_t)j * w, (size_t)m * w * sizeof(double));
+      l2_prefetch(diag + j, (size_t)m * sizeof(double));
+    }
     double ui[V], acc[V], bv[V];
     ldv<double, V>(u + ik, ui);
     ldv<double, V>(b + ik, bv);
