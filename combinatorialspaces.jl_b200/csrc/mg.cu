@@ -403,13 +403,14 @@ struct Lanes {
 
 // The row kernels' FP32 forms (unshifted, fixed width, not adding an iterate) are compiled for 8
 // resident CTAs of 256 threads per SM (32 registers a thread: every warp slot holds a warp waiting on
-// its loads) and prefetch the rows their CTA takes next (l2_prefetch).  The other forms keep the code
-// and the register counts they have without either: forced to 32 registers they spill, and with the
-// prefetch alone their counts rose (FP64 panels 32-40 -> 70-124) and their occupancy fell.  Measured on
-// B200 at icosphere L8 with 32 FP32 right-hand sides: k_sweep_ap 47.1 -> 44.0 us, the second step after
-// the prolongation 67.4 -> 59.8 us (40 registers and 6 CTAs per SM before), the FP64 residual
-// 103.5 -> 91.3 us, a middle Chebyshev step 64.6 -> 62.8 us (the cap alone), the solve 10,525 ->
-// 10,705 solves/s with every iterate bit for bit.
+// its loads) and, except the step that adds into the FP64 iterate (UPD) and a plain middle Chebyshev
+// step, prefetch the rows their CTA takes next (l2_prefetch).  The other forms keep the code and the
+// register counts they have without either: forced to 32 registers they spill, and with the prefetch
+// alone their counts rose (FP64 panels 32-40 -> 70-124) and their occupancy fell.  Measured on B200 at
+// icosphere L8 with 32 FP32 right-hand sides: k_sweep_ap 47.1 -> 44.0 us, the second step after the
+// prolongation 67.4 -> 60.3 us (40 registers and 6 CTAs per SM before), the FP64 residual 103.5 -> 91.0
+// us, a middle Chebyshev step 64.6 -> 62.6 us (the bound alone; 69.7 us with the prefetch), the solve
+// 10,525 -> 10,980 solves/s (10,715 with the UPD step prefetching too) with every iterate bit for bit.
 template <class T, bool KEEP>
 constexpr int kRowCtas = (sizeof(T) == 4 && !KEEP) ? 8 : 0;  // 0: no bound given
 template <class T, bool KEEP>
@@ -449,9 +450,8 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
   if constexpr (SH) ldv<C, V>(shf + (size_t)blockIdx.y * K + (size_t)lane * V, csv);
   for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < n; i += gridDim.x * Ln::RPB) {
     const size_t ik = po + (size_t)i * K;
-    // the CTA's next rows (i is their first row here), except in a plain middle Chebyshev step
-    // (measured slower with it: 64.2 -> 69.7 us at L8, 32 FP32 right-hand sides)
-    if (kRowPrefetch<T, SH || W == 0> && threadIdx.x == 0 && i + gridDim.x * Ln::RPB < n &&
+    // the CTA's next rows (i is their first row here), not in a plain middle Chebyshev step
+    if (kRowPrefetch<T, SH || W == 0 || UPD> && threadIdx.x == 0 && i + gridDim.x * Ln::RPB < n &&
         (PV != 0 || UPD || prm.mode != S_CHEBN)) {
       const int j = i + gridDim.x * Ln::RPB, m = min(Ln::RPB, n - j);
       const size_t pj = (size_t)blockIdx.y * pstride + (size_t)j * K, vb = (size_t)m * K * sizeof(T);
