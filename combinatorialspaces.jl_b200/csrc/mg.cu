@@ -401,18 +401,19 @@ struct Lanes {
   static constexpr int RPB = TB / LPR;     // rows per block
 };
 
-// The row kernels' FP32 forms (unshifted, fixed width, not adding an iterate) are compiled for 8
-// resident CTAs of 256 threads per SM (32 registers a thread: every warp slot holds a warp waiting on
-// its loads) and, except the step that adds into the FP64 iterate (UPD) and a plain middle Chebyshev
-// step, prefetch the rows their CTA takes next (l2_prefetch).  The other forms keep the code and the
-// register counts they have without either: forced to 32 registers they spill, and with the prefetch
-// alone their counts rose (FP64 panels 32-40 -> 70-124) and their occupancy fell.  Measured on B200 at
-// icosphere L8 with 32 FP32 right-hand sides: k_sweep_ap 47.1 -> 44.0 us, the second step after the
-// prolongation 67.4 -> 60.3 us (40 registers and 6 CTAs per SM before), the FP64 residual 103.5 -> 91.0
-// us, a middle Chebyshev step 64.6 -> 62.6 us (the bound alone; 69.7 us with the prefetch), the solve
-// 10,525 -> 10,980 solves/s (10,715 with the UPD step prefetching too) with every iterate bit for bit.
-template <class T, bool KEEP>
-constexpr int kRowCtas = (sizeof(T) == 4 && !KEEP) ? 8 : 0;  // 0: no bound given
+// The row kernels' FP32 forms of fixed width that do not add an iterate are compiled for 8 resident
+// CTAs of 256 threads per SM (32 registers a thread: every warp slot holds a warp waiting on its loads),
+// 6 for the shifted forms (SH, 40 registers), and, except the step that adds into the FP64 iterate (UPD)
+// and a plain middle Chebyshev step, prefetch the rows their CTA takes next (l2_prefetch).  The other
+// forms keep the code and the register counts they have without either: forced to 32 registers they
+// spill, and with the prefetch alone their counts rose (FP64 panels 32-40 -> 70-124) and their occupancy
+// fell.  Measured on B200 at icosphere L8 with 32 FP32 right-hand sides: k_sweep_ap 47.1 -> 44.0 us,
+// the second step after the prolongation 67.4 -> 60.3 us (40 registers and 6 CTAs per SM before), the
+// FP64 residual 103.5 -> 91.0 us, a middle Chebyshev step 64.6 -> 62.6 us (the bound alone; 69.7 us with
+// the prefetch), the solve 10,525 -> 10,980 solves/s (10,715 with the UPD step prefetching too) with
+// every iterate bit for bit; the batch of 512 shifted solves 57,900 -> 58,400-59,800 solves/s.
+template <class T, bool KEEP, bool SHV = false>
+constexpr int kRowCtas = (sizeof(T) == 4 && !KEEP) ? (SHV ? 6 : 8) : 0;  // 0: no bound given
 template <class T, bool KEEP>
 constexpr bool kRowPrefetch = sizeof(T) == 4 && !KEEP;
 
@@ -451,7 +452,7 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
   for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < n; i += gridDim.x * Ln::RPB) {
     const size_t ik = po + (size_t)i * K;
     // the CTA's next rows (i is their first row here), not in a plain middle Chebyshev step
-    if (kRowPrefetch<T, SH || W == 0 || UPD> && threadIdx.x == 0 && i + gridDim.x * Ln::RPB < n &&
+    if (kRowPrefetch<T, W == 0 || UPD> && threadIdx.x == 0 && i + gridDim.x * Ln::RPB < n &&
         (PV != 0 || UPD || prm.mode != S_CHEBN)) {
       const int j = i + gridDim.x * Ln::RPB, m = min(Ln::RPB, n - j);
       const size_t pj = (size_t)blockIdx.y * pstride + (size_t)j * K, vb = (size_t)m * K * sizeof(T);
@@ -465,7 +466,6 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
       if (!SH && prm.mode != S_RESID) l2_prefetch(dinv + j, (size_t)m * sizeof(C));
       if ((PV == 0 || PV == 2) && prm.mode == S_CHEBN && !prm.d_is_x) l2_prefetch(out + pj, vb);
       if constexpr (PV == 3) l2_prefetch(out + pj, vb);
-      if constexpr (UPD) l2_prefetch(u64 + pj, (size_t)m * K * sizeof(double));
       if constexpr (PV != 0) {
         l2_prefetch(pz.pa + j, (size_t)m * sizeof(int32_t));
         l2_prefetch(pz.pb + j, (size_t)m * sizeof(int32_t));
@@ -581,7 +581,7 @@ __device__ __forceinline__ void sweep_rows(int n, int Wr, const int32_t* __restr
 }
 
 template <class T, int K, int W, bool SH, int VV = 0>
-__global__ void __launch_bounds__(TB, kRowCtas<T, SH || W == 0>)
+__global__ void __launch_bounds__(TB, kRowCtas<T, W == 0, SH>)
     k_sweep(int n, int Wr, const int32_t* __restrict__ col,
                                               const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
                                               const CT<T>* __restrict__ dinv, const T* __restrict__ b,
@@ -593,7 +593,7 @@ __global__ void __launch_bounds__(TB, kRowCtas<T, SH || W == 0>)
 // The last sweep of a refinement step's V-cycles on the finest level with the step's update
 // u += e fused in (FP32 / FP64 storage).
 template <class T, int K, int W, bool SH, int VV = 0>
-__global__ void __launch_bounds__(TB, kRowCtas<T, SH || W == 0>)
+__global__ void __launch_bounds__(TB, kRowCtas<T, W == 0, SH>)
     k_sweep_u(int n, int Wr, const int32_t* __restrict__ col,
                                                 const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
                                                 const CT<T>* __restrict__ dinv, const T* __restrict__ b,
@@ -606,7 +606,7 @@ __global__ void __launch_bounds__(TB, kRowCtas<T, SH || W == 0>)
 // The second Chebyshev step after x (+)= P z with its previous iterate formed from z (PV = 1: P z,
 // 2: out + P z), so the prolonged iterate is never read back.  UPD as k_sweep_u.
 template <class T, int K, int W, bool SH, bool UPD, int PV, int VV = 0>
-__global__ void __launch_bounds__(TB, kRowCtas<T, SH || W == 0>)
+__global__ void __launch_bounds__(TB, kRowCtas<T, W == 0, SH>)
     k_sweep_p(int n, int Wr, const int32_t* __restrict__ col,
                                                 const CT<T>* __restrict__ off, const CT<T>* __restrict__ diag,
                                                 const CT<T>* __restrict__ dinv, const T* __restrict__ b,
@@ -626,7 +626,7 @@ constexpr int kApW = 8;
 // A P precomputed per level (apc / apv, kApW slots per row); out = x0 + D⁻¹ r / θ.  SH: A + cs I per
 // right-hand side (A P then holds the unshifted product and cs x0 is added).
 template <class T, int K, bool SH, bool ADD, int VV = 0>
-__global__ void __launch_bounds__(TB, kRowCtas<T, SH || ADD>)
+__global__ void __launch_bounds__(TB, kRowCtas<T, ADD, SH>)
     k_sweep_ap(int n, const int32_t* __restrict__ col, const CT<T>* __restrict__ off,
                                                  const CT<T>* __restrict__ diag, const CT<T>* __restrict__ dinv,
                                                  const int32_t* __restrict__ apc, const CT<T>* __restrict__ apv,
@@ -644,7 +644,7 @@ __global__ void __launch_bounds__(TB, kRowCtas<T, SH || ADD>)
   if constexpr (SH) ldv<C, V>(shf + (size_t)blockIdx.y * K + (size_t)lane * V, csv);
   for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < n; i += gridDim.x * Ln::RPB) {
     const size_t ik = po + (size_t)i * K;
-    if (kRowPrefetch<T, SH || ADD> && threadIdx.x == 0 && i + gridDim.x * Ln::RPB < n) {  // the CTA's next rows
+    if (kRowPrefetch<T, ADD> && threadIdx.x == 0 && i + gridDim.x * Ln::RPB < n) {  // the CTA's next rows
       const int j = i + gridDim.x * Ln::RPB, m = min(Ln::RPB, n - j);            // (i: their first)
       l2_prefetch(b + (size_t)blockIdx.y * pstride + (size_t)j * K, (size_t)m * K * sizeof(T));
       l2_prefetch(apc + (size_t)j * kApW, (size_t)m * kApW * sizeof(int32_t));
@@ -1172,7 +1172,7 @@ __global__ void k_scale_half(int n, int np, const float* __restrict__ r, const d
 // FP64 residual r = b - A u on the panels, written in the inner precision T, with per-block
 // partial sums of r² per right-hand side (deterministic two-stage reduction).
 template <class T, int K, int W, bool SH>
-__global__ void __launch_bounds__(TB, kRowCtas<T, SH || W == 0>)
+__global__ void __launch_bounds__(TB, kRowCtas<T, W == 0, SH>)
     k_residual64(int n, int Wr, const int32_t* __restrict__ col,
                                                    const double* __restrict__ off, const double* __restrict__ diag,
                                                    const double* __restrict__ b, const double* __restrict__ u,
@@ -1190,7 +1190,7 @@ __global__ void __launch_bounds__(TB, kRowCtas<T, SH || W == 0>)
   if constexpr (SH) ldv<double, V>(cs + (size_t)blockIdx.y * K + (size_t)lane * V, csv);
   for (int i = blockIdx.x * Ln::RPB + threadIdx.x / Ln::LPR; i < n; i += gridDim.x * Ln::RPB) {
     const size_t ik = po + (size_t)i * K;
-    if (kRowPrefetch<T, SH || W == 0> && threadIdx.x == 0 && i + gridDim.x * Ln::RPB < n) {  // the CTA's next rows
+    if (kRowPrefetch<T, W == 0> && threadIdx.x == 0 && i + gridDim.x * Ln::RPB < n) {  // the CTA's next rows
       const int j = i + gridDim.x * Ln::RPB, m = min(Ln::RPB, n - j);            // (i: their first)
       const size_t pj = (size_t)blockIdx.y * pstride + (size_t)j * K, vb = (size_t)m * K * sizeof(double);
       l2_prefetch(u + pj, vb);
